@@ -1,0 +1,156 @@
+/* C ABI of libstopeps_gpu.so: the B200 engine for the StoPEPS sample-ensemble
+ * hot path (row boundary-MPS contraction, full update, Born sampling,
+ * energy/weight contraction).
+ *
+ * Every entry point returns 0 on success or a nonzero sps_status; the message
+ * of the last failure is available through sps_last_error.  The library owns
+ * all device tensors behind integer ids; callers pass and receive plain host
+ * arrays, which are borrowed for the duration of the call only.  A handle
+ * owns one CUDA stream and must not be shared between threads.
+ *
+ * Each declaration names the reference interface (StoPEPS.jl v0.2.0, path
+ * relative to the project root) that it replaces.
+ */
+#ifndef STOPEPS_GPU_H
+#define STOPEPS_GPU_H
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+typedef struct sps_handle sps_handle;
+
+enum sps_status {
+  SPS_OK = 0,
+  SPS_ERR_ARGUMENT = 1,    /* ArgumentError / DimensionMismatch */
+  SPS_ERR_CUDA = 2,        /* CUDA runtime failure */
+  SPS_ERR_NUMERIC = 3,     /* "nonfinite boundary norm" (src/contraction/boundary_mps.jl:131) and
+                              the other error(...) paths on nonfinite / nonpositive values */
+  SPS_ERR_BORN = 4,        /* "invalid Born conditional ... increase chi_sampling",
+                              "zero total mass" (src/sampling/born.jl:140-142) */
+  SPS_ERR_CONVERGENCE = 5, /* device iteration cap reached (Jacobi SVD / eigh) */
+  SPS_ERR_REPAIR = 6,      /* "PSD repair did not remove the FU residual failure"
+                              (src/evolution/full_update.jl:500) */
+  SPS_ERR_STATE = 7        /* unknown handle / state / cache id */
+};
+
+/* Model and solver controls: the RunConfig fields this path reads
+ * (src/driver/config.jl:28-62), TFIM (src/models/tfim.jl:9-19) and
+ * FullUpdate (src/evolution/full_update.jl:11-17). */
+typedef struct sps_config {
+  int32_t Lx, Ly;
+  double J, h;
+  int32_t trotter_order;
+  int32_t fu_max_iterations;
+  double fu_error_tolerance;
+  double fu_diagonal_shift;
+  int32_t fu_linear_max_iterations;
+  double fu_linear_tolerance;
+  int32_t record_boundary_entropy;
+  int32_t device;
+} sps_config;
+
+/* BoundaryMPS(chi, sector_space) (src/contraction/boundary_mps.jl:11-18);
+ * space0/space1 < 0 means sector_space = nothing. */
+typedef struct sps_boundary {
+  int32_t chi;
+  int32_t space0, space1;
+} sps_boundary;
+
+/* Report of evolution_step! (src/evolution/full_update.jl:580-596). */
+typedef struct sps_step_report {
+  double beta;
+  double max_state_truncation;
+  double max_environment_truncation;
+  double max_boundary_entropy;
+  double max_solver_residual;
+  double max_iteration_limit_error;
+  int32_t bond_updates;
+  int32_t iteration_limit_hits;
+  int32_t stop_error_tolerance, stop_iteration_limit, stop_residual_fallback, stop_disabled;
+  int32_t linear_unconverged_updates;
+  int32_t repairs;
+  int32_t fallbacks;
+  double log_normalization_sum;
+} sps_step_report;
+
+/* lognorm (src/contraction/boundary_mps.jl:180-186). */
+typedef struct sps_lognorm_result {
+  double log_norm, tensor_log_norm, max_environment_truncation;
+} sps_lognorm_result;
+
+/* measure_energy (src/measurement/energy.jl:31-78); x_sum is the on-site
+ * ratio sum the reference forms at energy.jl:43-46, exposed as <sum X_i>. */
+typedef struct sps_energy {
+  double energy_total, energy_per_site;
+  double log_norm, tensor_log_norm;
+  double max_environment_truncation;
+  double x_sum, zz_sum;
+} sps_energy;
+
+/* sample_configuration result (src/sampling/born.jl:86-163). */
+typedef struct sps_sample_report {
+  double log_probability;
+  double max_environment_truncation;
+  int32_t near_boundary; /* draws whose uniform lay within 1e-12 of a cumulative probability */
+} sps_sample_report;
+
+/* --- lifetime ------------------------------------------------------------ */
+int sps_create(const sps_config* cfg, sps_handle** out);
+void sps_destroy(sps_handle* h);
+int sps_last_error(const sps_handle* h, char* buf, size_t n);
+int sps_counters(sps_handle* h, long long* kernel_launches, double* flops);
+
+/* --- states: FiniteState (src/states/finite.jl:27-49) ---------------------
+ * Site tensors have legs (W,N,Pout,Paux,E,S); each leg is described by its
+ * even and odd multiplicities (n0,n1), even states first.  leg_dims holds
+ * Lx*Ly*6*2 int32 in site order x + y*Lx; data holds every site's dense
+ * row-major block back to back in the same order. */
+int sps_identity_pepo(sps_handle* h, int32_t* state_id);           /* identity_pepo, finite.jl:80-86 */
+int sps_state_upload(sps_handle* h, int32_t is_pepo, double beta, double log_amplitude,
+                     const int32_t* leg_dims, const double* data, int32_t* state_id);
+int sps_state_layout(sps_handle* h, int32_t state_id, int32_t* leg_dims, int64_t* total);
+int sps_state_download(sps_handle* h, int32_t state_id, double* data, int64_t capacity);
+int sps_state_info(sps_handle* h, int32_t state_id, double* beta, double* log_amplitude, int32_t* is_pepo);
+int sps_state_set_beta(sps_handle* h, int32_t state_id, double beta);
+int sps_state_copy(sps_handle* h, int32_t state_id, int32_t* new_id);           /* Base.copy, finite.jl:41 */
+int sps_state_free(sps_handle* h, int32_t state_id);
+int sps_normalize_state(sps_handle* h, int32_t state_id, double* log_normalizations); /* finite.jl:89-100 */
+
+/* --- hot path -------------------------------------------------------------- */
+/* evolution_step!(state, model, delta, D, FullUpdate, BoundaryMPS; order,
+ * sector_space) (src/evolution/full_update.jl:559-597).  space: bond sector
+ * budget (n0,n1) or NULL. */
+int sps_evolution_step(sps_handle* h, int32_t state_id, double delta, int32_t D, const int32_t* space,
+                       const sps_boundary* environment, sps_step_report* report);
+/* lognorm(state, BoundaryMPS) (src/contraction/boundary_mps.jl:180-186) */
+int sps_lognorm(sps_handle* h, int32_t state_id, const sps_boundary* method, sps_lognorm_result* out);
+/* measure_energy(state, model, BoundaryMPS; record_entropy)
+ * (src/measurement/energy.jl:31-78).  site_x (Lx*Ly), se_north/se_south
+ * ((Ly-1)*(Lx-1), Se profile) may be NULL. */
+int sps_measure_energy(sps_handle* h, int32_t state_id, const sps_boundary* method, sps_energy* out,
+                       double* site_x, double* se_north, double* se_south);
+/* SamplingCache(state, BoundaryMPS; kind=:auxiliary) (src/sampling/born.jl:56-73) */
+int sps_sampling_cache(sps_handle* h, int32_t pepo_id, const sps_boundary* method, int32_t* cache_id);
+int sps_sampling_cache_free(sps_handle* h, int32_t cache_id);
+/* sample_configuration(cache; rng) with the Lx*Ly uniforms (row-major site
+ * order) in place of rand(rng) (src/sampling/born.jl:86-163).  configuration
+ * receives SymmetryBasis labels 1 (even) / 2 (odd), index x + y*Lx. */
+int sps_sample(sps_handle* h, int32_t cache_id, const double* uniforms, int32_t* configuration,
+               sps_sample_report* report);
+/* sample_configuration(cache; configuration) : probability of a given draw */
+int sps_sample_probability(sps_handle* h, int32_t cache_id, const int32_t* configuration,
+                           sps_sample_report* report);
+/* n draws in one call (the MPI sample loop of src/driver/run.jl:45-49 on one device) */
+int sps_sample_batch(sps_handle* h, int32_t cache_id, int32_t n, const double* uniforms,
+                     int32_t* configurations, double* log_probabilities);
+/* project_configuration(checkpoint, configuration) (src/sampling/born.jl:27-36) */
+int sps_project(sps_handle* h, int32_t pepo_id, const int32_t* configuration, int32_t* state_id,
+                double* log_normalizations);
+
+#ifdef __cplusplus
+}
+#endif
+#endif

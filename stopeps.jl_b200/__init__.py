@@ -1,0 +1,25 @@
+"""stopeps_b200: the StoPEPS sample-ensemble hot path on one B200.
+
+The public names mirror the reference package StoPEPS.jl v0.2.0
+(``src/StoPEPS.jl:32-42``) for the row boundary-MPS path: the configuration
+types, the two drivers, the hot-path functions and the ensemble statistics.
+The numerical work runs in ``libstopeps_gpu.so`` (C ABI in
+``include/stopeps_gpu.h``).
+"""
+from .config import (Z2Space, Lattice, TFIM, FullUpdate, BoundaryMPS, BoundaryMPSRow, ResamplingOptions,
+                     SymmetryBasis, RunConfig, validate_config, temperature_nodes, parameter_dict)
+from .engine import (Engine, DeviceState, SamplingCache, normalize_state, evolution_step, lognorm,
+                     measure_energy, sample_configuration, sample_batch, project_configuration)
+from .driver import (run_purification, run_stochastic, ensemble_statistics, group_configurations,
+                     sample_uniforms, step_schedule, ThermalCheckpoint, Particle, RESULT_SCHEMA_VERSION)
+from . import _lib
+from .build import build, LIB as LIBRARY_PATH
+
+__all__ = [
+    "Z2Space", "Lattice", "TFIM", "FullUpdate", "BoundaryMPS", "BoundaryMPSRow", "ResamplingOptions",
+    "SymmetryBasis", "RunConfig", "validate_config", "temperature_nodes", "parameter_dict", "Engine",
+    "DeviceState", "SamplingCache", "normalize_state", "evolution_step", "lognorm", "measure_energy",
+    "sample_configuration", "sample_batch", "project_configuration", "run_purification", "run_stochastic",
+    "ensemble_statistics", "group_configurations", "sample_uniforms", "step_schedule", "ThermalCheckpoint",
+    "Particle", "RESULT_SCHEMA_VERSION", "build", "LIBRARY_PATH",
+]

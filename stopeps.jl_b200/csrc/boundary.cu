@@ -1,0 +1,544 @@
+// Row boundary-MPS contraction, Born sampling and energy measurement on the
+// Z2 engine.  Restates src/contraction/boundary_mps.jl (whole file),
+// src/sampling/born.jl:27-163 (auxiliary kind, SymmetryBasis) and
+// src/measurement/energy.jl.
+#include "pipeline.h"
+#include <algorithm>
+#include <cfloat>
+
+namespace sps {
+
+static const double EPS = DBL_EPSILON;
+
+Tensor unit_tensor(Engine& E, const std::vector<Par>& legs) {
+  for (auto& p : legs)
+    if (p->size() != 1 || (*p)[0] != 0) throw Error(SPS_ERR_ARGUMENT, "nontrivial OBC leg");
+  double one = 1.0;
+  return E.upload(legs, &one);
+}
+
+// double_layer (boundary_mps.jl:65-73): legs (w,n,e,s), each fused (ket,bra)
+Tensor double_layer(Engine& E, const Tensor& ket, const Tensor& bra, const Tensor* physical) {
+  Tensor A = physical ? ein(E, "pu,wnuaes->wnpaes", *physical, ket) : ket;
+  Tensor raw = ein(E, "wnpaes,WNpaES->wWnNeEsS", A, bra);
+  for (int axis : {6, 4, 2, 0}) raw = fuse(E, raw, axis, 2);
+  return raw;
+}
+
+std::vector<Tensor> row_layers(Engine& E, const State& s) {
+  std::vector<Tensor> out;
+  out.reserve(s.sites.size());
+  for (auto& A : s.sites) out.push_back(double_layer(E, A, A));
+  return out;
+}
+
+static std::vector<Tensor> column(const std::vector<Tensor>& layers, int Lx, int y) {
+  return std::vector<Tensor>(layers.begin() + y * Lx, layers.begin() + (y + 1) * Lx);
+}
+
+Env trivial_boundary(Engine& E, const std::vector<Tensor>& row, bool north) {
+  Env env;
+  Par triv = make_par(1, 0);
+  int axis = north ? 1 : 3;
+  for (auto& A : row) env.t.push_back(unit_tensor(E, {triv, A.legs[axis], triv}));
+  return env;
+}
+
+// compress_boundary! (boundary_mps.jl:94-134)
+CompressReport compress_boundary(Engine& E, std::vector<Tensor>& B, const BMPS& m, bool reverse,
+                                 Entropy* ent, bool south_side, int row_cut) {
+  if (m.chi < 1) throw Error(SPS_ERR_ARGUMENT, "chi must be positive");
+  const int N = (int)B.size();
+  double max_error = 0;
+  Trunc tr;
+  tr.chi = m.chi;
+  tr.space[0] = m.space[0];
+  tr.space[1] = m.space[1];
+  if (!reverse) {
+    for (int x = N - 1; x >= 1; --x) {
+      LQres f = lq(E, B[x], {0}, {1, 2});
+      B[x] = f.Q;
+      B[x - 1] = ein(E, "lpk,kr->lpr", B[x - 1], f.L);
+    }
+    for (int x = 0; x < N - 1; ++x) {
+      SVDres f = svd(E, B[x], {0, 1}, {2}, tr, ent != nullptr);
+      if (ent) ent->record(south_side, row_cut, x + 1, f.entropy);
+      max_error = std::max(max_error, f.norm == 0 ? 0.0 : (f.err / f.norm) * (f.err / f.norm));
+      B[x] = f.U;
+      std::vector<double> s(f.S[0]);
+      s.insert(s.end(), f.S[1].begin(), f.S[1].end());
+      Tensor R = scale_leg(E, f.V, 0, s);
+      B[x + 1] = ein(E, "lk,kpr->lpr", R, B[x + 1]);
+    }
+  } else {
+    for (int x = 0; x < N - 1; ++x) {
+      QRres f = qr(E, B[x], {0, 1}, {2});
+      B[x] = f.Q;
+      B[x + 1] = ein(E, "lk,kpr->lpr", f.R, B[x + 1]);
+    }
+    for (int x = N - 1; x >= 1; --x) {
+      SVDres f = svd(E, B[x], {0}, {1, 2}, tr, ent != nullptr);
+      if (ent) ent->record(south_side, row_cut, x, f.entropy);
+      max_error = std::max(max_error, f.norm == 0 ? 0.0 : (f.err / f.norm) * (f.err / f.norm));
+      B[x] = f.V;
+      std::vector<double> s(f.S[0]);
+      s.insert(s.end(), f.S[1].begin(), f.S[1].end());
+      Tensor L = scale_leg(E, f.U, 1, s);
+      B[x - 1] = ein(E, "lpk,kr->lpr", B[x - 1], L);
+    }
+  }
+  int center = reverse ? 0 : N - 1;
+  double scale = norm(E, B[center]);
+  if (!std::isfinite(scale)) throw Error(SPS_ERR_NUMERIC, "nonfinite boundary norm");
+  if (scale != 0) scale_inplace(E, B[center], 1.0 / scale);
+  return {max_error, scale == 0 ? -INFINITY : std::log(scale)};
+}
+
+// _absorb for the row method (boundary_mps.jl:136-151)
+Env absorb(Engine& E, const Env& env, const std::vector<Tensor>& row, const BMPS& m, bool north,
+           Entropy* ent, int row_cut) {
+  std::vector<Tensor> B;
+  B.reserve(row.size());
+  for (size_t x = 0; x < row.size(); ++x) {
+    Tensor C = north ? ein(E, "lnr,wnep->lwpre", env.t[x], row[x]) : ein(E, "lsr,wpes->lwpre", env.t[x], row[x]);
+    B.push_back(fuse(E, fuse(E, C, 3, 2), 0, 2));
+  }
+  CompressReport rep = compress_boundary(E, B, m, !north, ent, !north, row_cut);
+  Env out;
+  out.t = std::move(B);
+  out.log_scale = env.log_scale + rep.log_scale;
+  out.max_trunc = std::max(env.max_trunc, rep.max_trunc);
+  return out;
+}
+
+// _close_boundary (boundary_mps.jl:153-163)
+double close_boundary(Engine& E, const std::vector<Tensor>& B) {
+  Tensor V = unit_tensor(E, {B[0].legs[0]});
+  for (auto& A : B) {
+    if (A.dims[1] != 1) throw Error(SPS_ERR_ARGUMENT, "close_boundary: open physical leg");
+    Tensor P = unit_tensor(E, {A.legs[1]});
+    Tensor W = ein(E, "l,lpr->pr", V, A);
+    V = ein(E, "p,pr->r", P, W);
+  }
+  return sum_all(E, V);
+}
+
+static double positive_real(double z, const char* name) {
+  if (!(std::isfinite(z) && z > 0))
+    throw Error(SPS_ERR_NUMERIC, std::string(name) + " requires a finite positive real value; received " +
+                                     std::to_string(z));
+  return z;
+}
+
+// lognorm / contract_layers (boundary_mps.jl:165-186)
+LogNorm lognorm(Engine& E, const State& s, const BMPS& m) {
+  auto layers = row_layers(E, s);
+  Env env = trivial_boundary(E, column(layers, s.Lx, 0), true);
+  for (int y = 0; y < s.Ly; ++y) env = absorb(E, env, column(layers, s.Lx, y), m, true);
+  double v = positive_real(close_boundary(E, env.t), "norm");
+  return {std::log(v) + env.log_scale + 2 * s.log_amplitude, std::log(v) + env.log_scale, env.max_trunc};
+}
+
+// boundary_environments (boundary_mps.jl:193-209)
+Envs boundary_environments(Engine& E, const std::vector<Tensor>& layers, int Lx, int Ly, const BMPS& m,
+                           int side, Entropy* ent) {
+  Envs r;
+  r.north.resize(Ly + 1);
+  r.south.resize(Ly + 1);
+  r.north[0] = trivial_boundary(E, column(layers, Lx, 0), true);
+  r.south[Ly] = trivial_boundary(E, column(layers, Lx, Ly - 1), false);
+  if (side != 2)
+    for (int y = 0; y < Ly; ++y) r.north[y + 1] = absorb(E, r.north[y], column(layers, Lx, y), m, true, ent, y + 1);
+  if (side != 1)
+    for (int y = Ly - 1; y >= 0; --y) r.south[y] = absorb(E, r.south[y + 1], column(layers, Lx, y), m, false, ent, y);
+  r.max_trunc = std::max(side == 2 ? 0.0 : r.north[Ly].max_trunc, side == 1 ? 0.0 : r.south[0].max_trunc);
+  return r;
+}
+
+// _left_step / _right_step, plain and slab (boundary_mps.jl:216-246)
+Tensor left_step(Engine& E, const Tensor& L, const Tensor& T, const Layer& row, const Tensor& B) {
+  if (row.slab) {
+    Tensor X = ein(E, "awvb,anc->wvbnc", L, T);
+    Tensor Y = ein(E, "wvbnc,wnek->vbcek", X, row.a);
+    Tensor Z = ein(E, "vbcek,vkfs->bcefs", Y, row.b);
+    return ein(E, "bcefs,bsd->cefd", Z, B);
+  }
+  Tensor X = ein(E, "awb,anc->wbnc", L, T);
+  Tensor Y = ein(E, "wbnc,wnes->bces", X, row.a);
+  return ein(E, "bces,bsd->ced", Y, B);
+}
+
+Tensor right_step(Engine& E, const Tensor& T, const Layer& row, const Tensor& B, const Tensor& R) {
+  if (row.slab) {
+    Tensor X = ein(E, "anc,cefd->anefd", T, R);
+    Tensor Y = ein(E, "anefd,wnek->awkfd", X, row.a);
+    Tensor Z = ein(E, "awkfd,vkfs->awvsd", Y, row.b);
+    return ein(E, "awvsd,bsd->awvb", Z, B);
+  }
+  Tensor X = ein(E, "anc,ced->aned", T, R);
+  Tensor Y = ein(E, "aned,wnes->awsd", X, row.a);
+  return ein(E, "awsd,bsd->awb", Y, B);
+}
+
+Tensor row_edge(Engine& E, const std::vector<Tensor>& top, const std::vector<Layer>& row,
+                const std::vector<Tensor>& bottom, bool left) {
+  int i = left ? 0 : (int)row.size() - 1;
+  int a = left ? 0 : 2;
+  if (row[i].slab)
+    return unit_tensor(E, {top[i].legs[a], row[i].a.legs[a], row[i].b.legs[a], bottom[i].legs[a]});
+  return unit_tensor(E, {top[i].legs[a], row[i].a.legs[a], bottom[i].legs[a]});
+}
+
+// row_environments (boundary_mps.jl:261-273)
+RowEnvs row_environments(Engine& E, const std::vector<Tensor>& top, const std::vector<Layer>& row,
+                         const std::vector<Tensor>& bottom, int side) {
+  int N = (int)row.size();
+  RowEnvs r;
+  r.left.resize(N + 1);
+  r.right.resize(N + 1);
+  r.left[0] = row_edge(E, top, row, bottom, true);
+  r.right[N] = row_edge(E, top, row, bottom, false);
+  if (side != 2)
+    for (int x = 0; x < N; ++x) {
+      r.left[x + 1] = left_step(E, r.left[x], top[x], row[x], bottom[x]);
+      safe_scale_inplace(E, r.left[x + 1]);
+    }
+  if (side != 1)
+    for (int x = N - 1; x >= 0; --x) {
+      r.right[x] = right_step(E, top[x], row[x], bottom[x], r.right[x + 1]);
+      safe_scale_inplace(E, r.right[x]);
+    }
+  return r;
+}
+
+void row_scalar_to(Engine& E, const Tensor& L, const Tensor& T, const Layer& row, const Tensor& B,
+                   const Tensor& R, int slot) {
+  Tensor X = left_step(E, L, T, row, B);
+  dot_to(E, X, R, slot);
+}
+
+// ---------------------------------------------------------------------------
+// states
+// ---------------------------------------------------------------------------
+State identity_pepo(Engine& E, int Lx, int Ly) {
+  State s;
+  s.Lx = Lx;
+  s.Ly = Ly;
+  Par t = make_par(1, 0), p2 = make_par(1, 1);
+  double a[4] = {1, 0, 0, 1};   // A[0,0,p,a,0,0] = delta_pa
+  for (int i = 0; i < Lx * Ly; ++i) s.sites.push_back(E.upload({t, t, p2, p2, t, t}, a));
+  s.beta = 0;
+  s.log_amplitude = 0;
+  s.pepo = true;
+  return s;
+}
+
+// normalize_state! (src/states/finite.jl:89-100), row-major site order
+std::vector<double> normalize_state(Engine& E, State& s) {
+  int n = s.Lx * s.Ly;
+  if (n > Engine::NSCAL) throw Error(SPS_ERR_ARGUMENT, "lattice too large");
+  for (int i = 0; i < n; ++i) norm2_to(E, s.sites[i], i);
+  SPS_CUDA(cudaMemcpyAsync(E.hscal, E.dscal, sizeof(double) * n, cudaMemcpyDeviceToHost, E.stream));
+  E.sync();
+  std::vector<double> inc(n);
+  for (int y = 0; y < s.Ly; ++y)
+    for (int x = 0; x < s.Lx; ++x) {
+      int i = x + y * s.Lx;
+      double v = std::sqrt(E.hscal[i]);
+      if (!(std::isfinite(v) && v > 0))
+        throw Error(SPS_ERR_NUMERIC, "zero or nonfinite tensor at (" + std::to_string(x + 1) + "," +
+                                         std::to_string(y + 1) + ")");
+      scale_inplace(E, s.sites[i], 1.0 / v);
+      inc[i] = std::log(v);
+      s.log_amplitude += inc[i];
+    }
+  return inc;
+}
+
+// ---------------------------------------------------------------------------
+// Born sampling (src/sampling/born.jl:56-163), kind = :auxiliary
+// ---------------------------------------------------------------------------
+static Tensor project_aux(Engine& E, const Tensor& A, int k) {
+  return slice_leg(E, A, 3, k, k == 0 ? make_par(1, 0) : make_par(0, 1));
+}
+
+SamplingCache make_sampling_cache(Engine& E, const State& s, const BMPS& m) {
+  SamplingCache c;
+  c.Lx = s.Lx;
+  c.Ly = s.Ly;
+  c.method = m;
+  c.state_ref = &s;
+  c.layers = row_layers(E, s);
+  for (auto& A : s.sites) {
+    std::array<Tensor, 2> cand;
+    for (int k = 0; k < 2; ++k) {
+      Tensor P = project_aux(E, A, k);
+      cand[k] = double_layer(E, P, P);
+    }
+    c.candidates.push_back(cand);
+  }
+  c.south.resize(s.Ly + 1);
+  c.south[s.Ly] = trivial_boundary(E, column(c.layers, s.Lx, s.Ly - 1), false);
+  for (int y = s.Ly - 1; y >= 0; --y)
+    c.south[y] = absorb(E, c.south[y + 1], column(c.layers, s.Lx, y), m, false, nullptr, y);
+  return c;
+}
+
+// _rs_logsumexp and _categorical (src/resample/selection.jl:1-7, 68-80)
+static double logsumexp(const std::vector<double>& x) {
+  if (x.empty()) return -INFINITY;
+  double pivot = *std::max_element(x.begin(), x.end());
+  if (pivot == -INFINITY) return -INFINITY;
+  if (!std::isfinite(pivot)) throw Error(SPS_ERR_NUMERIC, "nonfinite positive log mass");
+  double s = 0;
+  for (double v : x) s += std::exp(v - pivot);
+  return pivot + std::log(s);
+}
+
+static int categorical(const std::vector<double>& lm, double u, int* near) {
+  double z = logsumexp(lm);
+  if (!std::isfinite(z)) throw Error(SPS_ERR_NUMERIC, "proposal requires positive total probability");
+  double cum = 0;
+  int last = -1;
+  for (int j = 0; j < (int)lm.size(); ++j) {
+    if (lm[j] == -INFINITY) continue;
+    last = j;
+    cum += std::exp(lm[j] - z);
+    if (std::fabs(u - cum) < 1e-12 && near) ++*near;
+    if (u < cum) return j;
+  }
+  return last;
+}
+
+SampleResult sample_configuration(Engine& E, const SamplingCache& c, const double* uniforms,
+                                  const int* configuration) {
+  const int Lx = c.Lx, Ly = c.Ly;
+  SampleResult res;
+  res.config.assign(Lx * Ly, 0);
+  Env north = trivial_boundary(E, column(c.layers, Lx, 0), true);
+  double maxtr = 0;
+  for (auto& e : c.south) maxtr = std::max(maxtr, e.max_trunc);
+  double logp = 0;
+  for (int y = 0; y < Ly; ++y) {
+    std::vector<Layer> row(Lx);
+    std::vector<Tensor> rowt = column(c.layers, Lx, y);
+    for (int x = 0; x < Lx; ++x) row[x].a = rowt[x];
+    const auto& top = north.t;
+    const auto& bottom = c.south[y + 1].t;
+    RowEnvs e = row_environments(E, top, row, bottom, 2);
+    Tensor left = e.left[0];
+    for (int x = 0; x < Lx; ++x) {
+      const auto& cand = c.candidates[x + y * Lx];
+      for (int k = 0; k < 2; ++k) {
+        Layer l;
+        l.a = cand[k];
+        row_scalar_to(E, left, top[x], l, bottom[x], e.right[x + 1], 10 + k);
+      }
+      SPS_CUDA(cudaMemcpyAsync(E.hscal + 10, E.dscal + 10, 2 * sizeof(double), cudaMemcpyDeviceToHost, E.stream));
+      E.sync();
+      E.check_flag("sample_configuration");
+      double raw[2] = {E.hscal[10], E.hscal[11]};
+      double scale = std::max(std::fabs(raw[0]), std::fabs(raw[1]));
+      for (double z : raw)
+        if (!(std::isfinite(z) && z >= -64 * EPS * scale))
+          throw Error(SPS_ERR_BORN, "invalid Born conditional at (" + std::to_string(x + 1) + "," +
+                                        std::to_string(y + 1) + "); increase chi_sampling");
+      double v0 = std::max(raw[0], 0.0), v1 = std::max(raw[1], 0.0);
+      double total = v0 + v1;
+      if (!(total > 0))
+        throw Error(SPS_ERR_BORN, "Born conditional has zero total mass at (" + std::to_string(x + 1) + "," +
+                                      std::to_string(y + 1) + ")");
+      double p[2] = {v0 / total, v1 / total};
+      int k;
+      if (configuration) {
+        k = configuration[x + y * Lx] - 1;
+        if (k < 0 || k > 1) throw Error(SPS_ERR_ARGUMENT, "configuration contains an unknown basis label");
+      } else {
+        std::vector<double> lm{p[0] > 0 ? std::log(p[0]) : -INFINITY, p[1] > 0 ? std::log(p[1]) : -INFINITY};
+        k = categorical(lm, uniforms[x + y * Lx], &res.near_boundary);
+      }
+      res.config[x + y * Lx] = k + 1;
+      res.conditionals.push_back(p[k]);
+      if (p[k] == 0.0) {
+        res.log_probability = -INFINITY;
+        res.max_env_trunc = maxtr;
+        return res;
+      }
+      logp += std::log(p[k]);
+      row[x].a = cand[k];
+      if (x < Lx - 1) {
+        left = left_step(E, left, top[x], row[x], bottom[x]);
+        safe_scale_inplace(E, left);
+      }
+    }
+    std::vector<Tensor> rt(Lx);
+    for (int x = 0; x < Lx; ++x) rt[x] = row[x].a;
+    north = absorb(E, north, rt, c.method, true, nullptr, y + 1);
+    maxtr = std::max(maxtr, north.max_trunc);
+  }
+  res.log_probability = logp;
+  res.max_env_trunc = maxtr;
+  return res;
+}
+
+// project_configuration (born.jl:27-36)
+State project_configuration(Engine& E, const State& pepo, const int* configuration,
+                            std::vector<double>* log_norms) {
+  State s;
+  s.Lx = pepo.Lx;
+  s.Ly = pepo.Ly;
+  s.beta = pepo.beta;
+  s.log_amplitude = pepo.log_amplitude;
+  s.pepo = false;
+  for (int i = 0; i < pepo.Lx * pepo.Ly; ++i) {
+    int k = configuration[i] - 1;
+    if (k < 0 || k > 1) throw Error(SPS_ERR_ARGUMENT, "configuration contains an unknown basis label");
+    s.sites.push_back(project_aux(E, pepo.sites[i], k));
+  }
+  auto inc = normalize_state(E, s);
+  if (log_norms) *log_norms = inc;
+  return s;
+}
+
+// ---------------------------------------------------------------------------
+// energy (src/measurement/energy.jl)
+// ---------------------------------------------------------------------------
+// _operator_factors(ZZ) for the Z2 TFIM: M[(p,u),(q,v)] = z[p,u] z[q,v] is
+// rank one in the odd block with singular value 2, so F = sqrt(2) z and
+// G = z / sqrt(2) on a one-state odd leg r (energy.jl:8-12).
+static void operator_factors(Engine& E, Tensor& F, Tensor& G) {
+  Par p2 = make_par(1, 1), r = make_par(0, 1);
+  double s2 = std::sqrt(2.0);
+  double f[4] = {0, s2, s2, 0};          // F[p,u,r]: (0,1)->s2, (1,0)->s2
+  double g[4] = {0, 1 / s2, 1 / s2, 0};  // G[r,q,v]
+  F = E.upload({p2, p2, r}, f);
+  G = E.upload({r, p2, p2}, g);
+}
+
+static void operator_pair(Engine& E, const Tensor& A, const Tensor& B, const Tensor& F, const Tensor& G,
+                          bool horizontal, Tensor& C, Tensor& D) {
+  if (horizontal) {
+    C = fuse(E, ein(E, "wnuaes,pur->wnpaers", A, F), 4, 2);
+    D = fuse(E, ein(E, "wnvaes,rqv->wrnqaes", B, G), 0, 2);
+  } else {
+    C = fuse(E, ein(E, "wnuaes,pur->wnpaesr", A, F), 5, 2);
+    D = fuse(E, ein(E, "wnvaes,rqv->wnrqaes", B, G), 1, 2);
+  }
+}
+
+static double real_ratio(double a, double b) {
+  if (b == 0) throw Error(SPS_ERR_NUMERIC, "zero local norm environment");
+  double z = a / b;
+  if (!std::isfinite(z)) throw Error(SPS_ERR_NUMERIC, "nonreal observable");
+  return z;
+}
+
+EnergyResult measure_energy(Engine& E, const State& s, const Model& m, const BMPS& method,
+                            bool record_entropy) {
+  const int Lx = s.Lx, Ly = s.Ly;
+  EnergyResult out;
+  out.entropy.profile = record_entropy;
+  out.entropy.Lx = Lx;
+  out.entropy.Ly = Ly;
+  if (record_entropy) {
+    out.entropy.north.assign(std::max(0, (Ly - 1) * (Lx - 1)), NAN);
+    out.entropy.south.assign(std::max(0, (Ly - 1) * (Lx - 1)), NAN);
+  }
+  auto layers = row_layers(E, s);
+  Envs env = boundary_environments(E, layers, Lx, Ly, method, 0, record_entropy ? &out.entropy : nullptr);
+  Par p2 = make_par(1, 1);
+  double xo[4] = {1, 0, 0, -1};
+  Tensor X = E.upload({p2, p2}, xo);
+  Tensor F, G;
+  operator_factors(E, F, G);
+  // slot layout: [100 + 2*k] numerator, [101 + 2*k] denominator
+  int nterm = Lx * Ly + Ly * (Lx - 1) + (Ly - 1) * Lx;
+  if (100 + 2 * nterm > Engine::NSCAL) throw Error(SPS_ERR_ARGUMENT, "lattice too large for measurement");
+  int term = 0;
+  for (int y = 0; y < Ly; ++y) {
+    std::vector<Layer> row(Lx);
+    for (int x = 0; x < Lx; ++x) row[x].a = layers[x + y * Lx];
+    const auto& top = env.north[y].t;
+    const auto& bottom = env.south[y + 1].t;
+    RowEnvs e = row_environments(E, top, row, bottom, 0);
+    for (int x = 0; x < Lx; ++x) {
+      Layer xl;
+      xl.a = double_layer(E, s.at(x, y), s.at(x, y), &X);
+      row_scalar_to(E, e.left[x], top[x], xl, bottom[x], e.right[x + 1], 100 + 2 * term);
+      row_scalar_to(E, e.left[x], top[x], row[x], bottom[x], e.right[x + 1], 101 + 2 * term);
+      ++term;
+    }
+    for (int x = 0; x < Lx - 1; ++x) {
+      const Tensor& A = s.at(x, y);
+      const Tensor& B = s.at(x + 1, y);
+      Tensor C, D;
+      operator_pair(E, A, B, F, G, true, C, D);
+      Layer lc, ld;
+      lc.a = double_layer(E, C, A);
+      ld.a = double_layer(E, D, B);
+      Tensor left = left_step(E, e.left[x], top[x], lc, bottom[x]);
+      row_scalar_to(E, left, top[x + 1], ld, bottom[x + 1], e.right[x + 2], 100 + 2 * term);
+      left = left_step(E, e.left[x], top[x], row[x], bottom[x]);
+      row_scalar_to(E, left, top[x + 1], row[x + 1], bottom[x + 1], e.right[x + 2], 101 + 2 * term);
+      ++term;
+    }
+  }
+  int first_vertical = term;
+  for (int y = 0; y < Ly - 1; ++y) {
+    std::vector<Layer> row(Lx);
+    for (int x = 0; x < Lx; ++x) {
+      row[x].a = layers[x + y * Lx];
+      row[x].b = layers[x + (y + 1) * Lx];
+      row[x].slab = true;
+    }
+    const auto& top = env.north[y].t;
+    const auto& bottom = env.south[y + 2].t;
+    RowEnvs e = row_environments(E, top, row, bottom, 0);
+    for (int x = 0; x < Lx; ++x) {
+      const Tensor& A = s.at(x, y);
+      const Tensor& B = s.at(x, y + 1);
+      Tensor C, D;
+      operator_pair(E, A, B, F, G, false, C, D);
+      Layer imp;
+      imp.a = double_layer(E, C, A);
+      imp.b = double_layer(E, D, B);
+      imp.slab = true;
+      row_scalar_to(E, e.left[x], top[x], row[x], bottom[x], e.right[x + 1], 101 + 2 * term);
+      row_scalar_to(E, e.left[x], top[x], imp, bottom[x], e.right[x + 1], 100 + 2 * term);
+      ++term;
+    }
+  }
+  SPS_CUDA(cudaMemcpyAsync(E.hscal + 100, E.dscal + 100, sizeof(double) * 2 * nterm, cudaMemcpyDeviceToHost,
+                           E.stream));
+  E.sync();
+  E.check_flag("measure_energy");
+  std::vector<double> vals(E.hscal + 100, E.hscal + 100 + 2 * nterm);
+  double xsum = 0, zzsum = 0;
+  out.site_x.assign(Lx * Ly, 0);
+  term = 0;
+  for (int y = 0; y < Ly; ++y) {
+    for (int x = 0; x < Lx; ++x) {
+      double r = real_ratio(vals[2 * term], vals[2 * term + 1]);
+      out.site_x[x + y * Lx] = r;
+      xsum += r;
+      ++term;
+    }
+    for (int x = 0; x < Lx - 1; ++x) {
+      zzsum += real_ratio(vals[2 * term], vals[2 * term + 1]);
+      ++term;
+    }
+  }
+  for (term = first_vertical; term < nterm; ++term) zzsum += real_ratio(vals[2 * term], vals[2 * term + 1]);
+  const Env& fin = env.north[Ly];
+  double ln = std::log(positive_real(close_boundary(E, fin.t), "norm")) + fin.log_scale;
+  out.energy_total = -m.J * zzsum - m.h * xsum;
+  out.energy_per_site = out.energy_total / (Lx * Ly);
+  out.log_norm = ln + 2 * s.log_amplitude;
+  out.tensor_log_norm = ln;
+  out.max_env_trunc = env.max_trunc;
+  out.x_sum = xsum;
+  out.zz_sum = zzsum;
+  return out;
+}
+
+}  // namespace sps

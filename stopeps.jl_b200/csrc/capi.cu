@@ -1,0 +1,379 @@
+// C ABI (include/stopeps_gpu.h) over the engine: opaque handles, integer
+// state / cache ids, status codes and the last error message.
+#include "stopeps_gpu.h"
+#include "pipeline.h"
+#include <cstring>
+#include <memory>
+#include <unordered_map>
+
+using namespace sps;
+
+struct sps_handle {
+  std::unique_ptr<Engine> E;
+  sps_config cfg;
+  std::unordered_map<int, State> states;
+  std::unordered_map<int, SamplingCache> caches;
+  std::unordered_map<int, int> cache_state;   // cache -> pinned state copy id
+  int next_id = 1;
+  std::string err;
+};
+
+namespace {
+
+template <class F>
+int guarded(sps_handle* h, F&& f) {
+  if (!h) return SPS_ERR_STATE;
+  try {
+    f();
+    h->err.clear();
+    return SPS_OK;
+  } catch (const Error& e) {
+    h->err = e.what();
+    return e.code;
+  } catch (const std::exception& e) {
+    h->err = e.what();
+    return SPS_ERR_ARGUMENT;
+  }
+}
+
+State& get_state(sps_handle* h, int id) {
+  auto it = h->states.find(id);
+  if (it == h->states.end()) throw Error(SPS_ERR_STATE, "unknown state id " + std::to_string(id));
+  return it->second;
+}
+
+BMPS to_bmps(const sps_boundary* b) {
+  if (!b) throw Error(SPS_ERR_ARGUMENT, "missing boundary method");
+  BMPS m;
+  m.chi = b->chi;
+  m.space[0] = b->space0 >= 0 && b->space1 >= 0 ? b->space0 : -1;
+  m.space[1] = b->space0 >= 0 && b->space1 >= 0 ? b->space1 : -1;
+  return m;
+}
+
+Model model_of(const sps_handle* h) { return Model{h->cfg.J, h->cfg.h}; }
+
+FUOptions fu_of(const sps_handle* h) {
+  FUOptions o;
+  o.max_iterations = h->cfg.fu_max_iterations;
+  o.error_tolerance = h->cfg.fu_error_tolerance;
+  o.diagonal_shift = h->cfg.fu_diagonal_shift;
+  o.linear_max_iterations = h->cfg.fu_linear_max_iterations;
+  o.linear_tolerance = h->cfg.fu_linear_tolerance;
+  return o;
+}
+
+int leg_sector(const Par& p, int c) { return par_count(p, c); }
+
+bool sorted_leg(const Par& p) {
+  for (size_t i = 1; i < p->size(); ++i)
+    if ((*p)[i] < (*p)[i - 1]) return false;
+  return true;
+}
+
+}  // namespace
+
+extern "C" {
+
+int sps_create(const sps_config* cfg, sps_handle** out) {
+  if (!cfg || !out) return SPS_ERR_ARGUMENT;
+  *out = nullptr;
+  auto h = new sps_handle();
+  h->cfg = *cfg;
+  if (cfg->Lx < 1 || cfg->Ly < 1 || (cfg->trotter_order != 1 && cfg->trotter_order != 2) ||
+      cfg->fu_max_iterations < 0 || cfg->fu_linear_max_iterations < 1) {
+    delete h;
+    return SPS_ERR_ARGUMENT;
+  }
+  try {
+    h->E.reset(new Engine(cfg->device));
+  } catch (const Error& e) {
+    delete h;
+    return e.code;
+  }
+  *out = h;
+  return SPS_OK;
+}
+
+void sps_destroy(sps_handle* h) {
+  if (!h) return;
+  h->caches.clear();
+  h->states.clear();
+  delete h;
+}
+
+int sps_last_error(const sps_handle* h, char* buf, size_t n) {
+  if (!h || !buf || n == 0) return SPS_ERR_ARGUMENT;
+  std::strncpy(buf, h->err.c_str(), n - 1);
+  buf[n - 1] = 0;
+  return SPS_OK;
+}
+
+int sps_counters(sps_handle* h, long long* launches, double* flops) {
+  return guarded(h, [&] {
+    if (launches) *launches = h->E->launches;
+    if (flops) *flops = h->E->flops;
+  });
+}
+
+int sps_identity_pepo(sps_handle* h, int32_t* state_id) {
+  return guarded(h, [&] {
+    int id = h->next_id++;
+    h->states[id] = identity_pepo(*h->E, h->cfg.Lx, h->cfg.Ly);
+    *state_id = id;
+  });
+}
+
+int sps_state_upload(sps_handle* h, int32_t is_pepo, double beta, double log_amplitude, const int32_t* leg_dims,
+                     const double* data, int32_t* state_id) {
+  return guarded(h, [&] {
+    if (!leg_dims || !data || !state_id) throw Error(SPS_ERR_ARGUMENT, "null pointer");
+    State s;
+    s.Lx = h->cfg.Lx;
+    s.Ly = h->cfg.Ly;
+    s.beta = beta;
+    s.log_amplitude = log_amplitude;
+    s.pepo = is_pepo != 0;
+    const double* ptr = data;
+    for (int i = 0; i < s.Lx * s.Ly; ++i) {
+      std::vector<Par> legs;
+      for (int k = 0; k < 6; ++k) {
+        int n0 = leg_dims[(i * 6 + k) * 2], n1 = leg_dims[(i * 6 + k) * 2 + 1];
+        if (n0 < 0 || n1 < 0 || n0 + n1 == 0) throw Error(SPS_ERR_ARGUMENT, "invalid leg dimensions");
+        legs.push_back(make_par(n0, n1));
+      }
+      Tensor t = h->E->upload(legs, ptr);
+      ptr += t.size();
+      s.sites.push_back(t);
+    }
+    int id = h->next_id++;
+    h->states[id] = std::move(s);
+    *state_id = id;
+  });
+}
+
+int sps_state_layout(sps_handle* h, int32_t state_id, int32_t* leg_dims, int64_t* total) {
+  return guarded(h, [&] {
+    State& s = get_state(h, state_id);
+    int64_t tot = 0;
+    for (int i = 0; i < s.Lx * s.Ly; ++i) {
+      const Tensor& t = s.sites[i];
+      for (int k = 0; k < 6; ++k) {
+        if (!sorted_leg(t.legs[k])) throw Error(SPS_ERR_STATE, "site leg is not sector sorted");
+        if (leg_dims) {
+          leg_dims[(i * 6 + k) * 2] = leg_sector(t.legs[k], 0);
+          leg_dims[(i * 6 + k) * 2 + 1] = leg_sector(t.legs[k], 1);
+        }
+      }
+      tot += t.size();
+    }
+    if (total) *total = tot;
+  });
+}
+
+int sps_state_download(sps_handle* h, int32_t state_id, double* data, int64_t capacity) {
+  return guarded(h, [&] {
+    State& s = get_state(h, state_id);
+    int64_t off = 0;
+    for (auto& t : s.sites) {
+      if (off + t.size() > capacity) throw Error(SPS_ERR_ARGUMENT, "buffer too small");
+      auto v = h->E->download(t);
+      std::memcpy(data + off, v.data(), v.size() * sizeof(double));
+      off += t.size();
+    }
+  });
+}
+
+int sps_state_info(sps_handle* h, int32_t state_id, double* beta, double* log_amplitude, int32_t* is_pepo) {
+  return guarded(h, [&] {
+    State& s = get_state(h, state_id);
+    if (beta) *beta = s.beta;
+    if (log_amplitude) *log_amplitude = s.log_amplitude;
+    if (is_pepo) *is_pepo = s.pepo ? 1 : 0;
+  });
+}
+
+int sps_state_set_beta(sps_handle* h, int32_t state_id, double beta) {
+  return guarded(h, [&] { get_state(h, state_id).beta = beta; });
+}
+
+int sps_state_copy(sps_handle* h, int32_t state_id, int32_t* new_id) {
+  return guarded(h, [&] {
+    State c = get_state(h, state_id);
+    for (auto& t : c.sites) t = clone(*h->E, t);
+    int id = h->next_id++;
+    h->states[id] = std::move(c);
+    *new_id = id;
+  });
+}
+
+int sps_state_free(sps_handle* h, int32_t state_id) {
+  return guarded(h, [&] {
+    if (!h->states.erase(state_id)) throw Error(SPS_ERR_STATE, "unknown state id");
+  });
+}
+
+int sps_normalize_state(sps_handle* h, int32_t state_id, double* log_normalizations) {
+  return guarded(h, [&] {
+    auto v = normalize_state(*h->E, get_state(h, state_id));
+    if (log_normalizations) std::memcpy(log_normalizations, v.data(), v.size() * sizeof(double));
+  });
+}
+
+int sps_evolution_step(sps_handle* h, int32_t state_id, double delta, int32_t D, const int32_t* space,
+                       const sps_boundary* environment, sps_step_report* report) {
+  return guarded(h, [&] {
+    State& s = get_state(h, state_id);
+    int sp[2] = {-1, -1};
+    if (space) {
+      sp[0] = space[0];
+      sp[1] = space[1];
+    }
+    StepReport r = evolution_step(*h->E, s, model_of(h), delta, D, fu_of(h), to_bmps(environment),
+                                  h->cfg.trotter_order, sp, h->cfg.record_boundary_entropy != 0);
+    if (report) {
+      sps_step_report& o = *report;
+      o.beta = r.beta;
+      o.max_state_truncation = r.max_state_truncation;
+      o.max_environment_truncation = r.max_environment_truncation;
+      o.max_boundary_entropy = r.max_boundary_entropy;
+      o.max_solver_residual = r.max_solver_residual;
+      o.max_iteration_limit_error = r.max_iteration_limit_error;
+      o.bond_updates = r.bond_updates;
+      o.iteration_limit_hits = r.iteration_limit_hits;
+      o.stop_error_tolerance = r.stop_reasons[0];
+      o.stop_iteration_limit = r.stop_reasons[1];
+      o.stop_residual_fallback = r.stop_reasons[2];
+      o.stop_disabled = r.stop_reasons[3];
+      o.linear_unconverged_updates = r.linear_unconverged;
+      o.repairs = r.repairs;
+      o.fallbacks = r.fallbacks;
+      double sum = 0;
+      for (double v : r.log_normalizations) sum += v;
+      o.log_normalization_sum = sum;
+    }
+  });
+}
+
+int sps_lognorm(sps_handle* h, int32_t state_id, const sps_boundary* method, sps_lognorm_result* out) {
+  return guarded(h, [&] {
+    LogNorm r = lognorm(*h->E, get_state(h, state_id), to_bmps(method));
+    if (out) {
+      out->log_norm = r.log_norm;
+      out->tensor_log_norm = r.tensor_log_norm;
+      out->max_environment_truncation = r.max_env_trunc;
+    }
+  });
+}
+
+int sps_measure_energy(sps_handle* h, int32_t state_id, const sps_boundary* method, sps_energy* out,
+                       double* site_x, double* se_north, double* se_south) {
+  return guarded(h, [&] {
+    State& s = get_state(h, state_id);
+    EnergyResult r = measure_energy(*h->E, s, model_of(h), to_bmps(method), h->cfg.record_boundary_entropy != 0);
+    if (out) {
+      out->energy_total = r.energy_total;
+      out->energy_per_site = r.energy_per_site;
+      out->log_norm = r.log_norm;
+      out->tensor_log_norm = r.tensor_log_norm;
+      out->max_environment_truncation = r.max_env_trunc;
+      out->x_sum = r.x_sum;
+      out->zz_sum = r.zz_sum;
+    }
+    if (site_x) std::memcpy(site_x, r.site_x.data(), r.site_x.size() * sizeof(double));
+    if (se_north && r.entropy.profile)
+      std::memcpy(se_north, r.entropy.north.data(), r.entropy.north.size() * sizeof(double));
+    if (se_south && r.entropy.profile)
+      std::memcpy(se_south, r.entropy.south.data(), r.entropy.south.size() * sizeof(double));
+  });
+}
+
+int sps_sampling_cache(sps_handle* h, int32_t pepo_id, const sps_boundary* method, int32_t* cache_id) {
+  return guarded(h, [&] {
+    State& s = get_state(h, pepo_id);
+    if (!s.pepo) throw Error(SPS_ERR_ARGUMENT, "auxiliary sampling requires a PEPO");
+    // the cache keeps its own reference to the PEPO tensors
+    int sid = h->next_id++;
+    h->states[sid] = s;
+    int id = h->next_id++;
+    h->caches[id] = make_sampling_cache(*h->E, h->states[sid], to_bmps(method));
+    h->cache_state[id] = sid;
+    *cache_id = id;
+  });
+}
+
+int sps_sampling_cache_free(sps_handle* h, int32_t cache_id) {
+  return guarded(h, [&] {
+    auto it = h->caches.find(cache_id);
+    if (it == h->caches.end()) throw Error(SPS_ERR_STATE, "unknown cache id");
+    h->caches.erase(it);
+    h->states.erase(h->cache_state[cache_id]);
+    h->cache_state.erase(cache_id);
+  });
+}
+
+static SamplingCache& get_cache(sps_handle* h, int id) {
+  auto it = h->caches.find(id);
+  if (it == h->caches.end()) throw Error(SPS_ERR_STATE, "unknown cache id");
+  return it->second;
+}
+
+int sps_sample(sps_handle* h, int32_t cache_id, const double* uniforms, int32_t* configuration,
+               sps_sample_report* report) {
+  return guarded(h, [&] {
+    if (!uniforms) throw Error(SPS_ERR_ARGUMENT, "an explicit RNG is required");
+    SamplingCache& c = get_cache(h, cache_id);
+    SampleResult r = sample_configuration(*h->E, c, uniforms, nullptr);
+    if (configuration)
+      for (size_t i = 0; i < r.config.size(); ++i) configuration[i] = r.config[i];
+    if (report) {
+      report->log_probability = r.log_probability;
+      report->max_environment_truncation = r.max_env_trunc;
+      report->near_boundary = r.near_boundary;
+    }
+  });
+}
+
+int sps_sample_probability(sps_handle* h, int32_t cache_id, const int32_t* configuration,
+                           sps_sample_report* report) {
+  return guarded(h, [&] {
+    if (!configuration) throw Error(SPS_ERR_ARGUMENT, "missing configuration");
+    SamplingCache& c = get_cache(h, cache_id);
+    std::vector<int> cfg(configuration, configuration + c.Lx * c.Ly);
+    SampleResult r = sample_configuration(*h->E, c, nullptr, cfg.data());
+    if (report) {
+      report->log_probability = r.log_probability;
+      report->max_environment_truncation = r.max_env_trunc;
+      report->near_boundary = 0;
+    }
+  });
+}
+
+int sps_sample_batch(sps_handle* h, int32_t cache_id, int32_t n, const double* uniforms, int32_t* configurations,
+                     double* log_probabilities) {
+  return guarded(h, [&] {
+    SamplingCache& c = get_cache(h, cache_id);
+    int L = c.Lx * c.Ly;
+    for (int i = 0; i < n; ++i) {
+      SampleResult r = sample_configuration(*h->E, c, uniforms + (size_t)i * L, nullptr);
+      for (int k = 0; k < L; ++k) configurations[(size_t)i * L + k] = r.config[k];
+      log_probabilities[i] = r.log_probability;
+    }
+  });
+}
+
+int sps_project(sps_handle* h, int32_t pepo_id, const int32_t* configuration, int32_t* state_id,
+                double* log_normalizations) {
+  return guarded(h, [&] {
+    State& p = get_state(h, pepo_id);
+    std::vector<int> cfg(configuration, configuration + p.Lx * p.Ly);
+    std::vector<double> ln;
+    State s = project_configuration(*h->E, p, cfg.data(), &ln);
+    int id = h->next_id++;
+    h->states[id] = std::move(s);
+    *state_id = id;
+    if (log_normalizations) std::memcpy(log_normalizations, ln.data(), ln.size() * sizeof(double));
+  });
+}
+
+}  // extern "C"

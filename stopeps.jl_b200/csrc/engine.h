@@ -1,0 +1,218 @@
+// Z2 block-tensor engine on one B200: device buffers, strided Z2 tensors and
+// the table-driven contraction / factorization primitives the hot path is
+// written in.
+//
+// A tensor is a dense float64 array (arbitrary strides) plus one parity bit
+// per basis state of every leg.  Entries whose parities sum to an odd number
+// are structural zeros: kernels never read them as operands of a parity
+// block and always leave them zero in outputs.  A matrix view of a tensor
+// for (row legs | column legs) has two parity blocks; block c lists the
+// row-major fused indices of parity c in increasing order (rows and columns
+// alike).  Every GEMM, QR, LQ, SVD and eigendecomposition works on those
+// blocks, which is what TensorKit does per coupled sector of a Z2 TensorMap.
+#pragma once
+#include <cuda_runtime.h>
+#include <cstdint>
+#include <cstdio>
+#include <map>
+#include <memory>
+#include <stdexcept>
+#include <string>
+#include <vector>
+
+#include "stopeps_gpu.h"   // status codes shared with the C ABI
+
+namespace sps {
+
+struct Error : std::runtime_error {
+  int code;
+  Error(int c, const std::string& m) : std::runtime_error(m), code(c) {}
+};
+
+#define SPS_CUDA(x)                                                              \
+  do {                                                                           \
+    cudaError_t e_ = (x);                                                        \
+    if (e_ != cudaSuccess)                                                       \
+      throw ::sps::Error(SPS_ERR_CUDA,                                  \
+                         std::string(#x) + ": " + cudaGetErrorString(e_));       \
+  } while (0)
+
+// ---------------------------------------------------------------------------
+// device memory pool (stream-ordered reuse on the engine's single stream)
+// ---------------------------------------------------------------------------
+class Pool {
+ public:
+  void* get(size_t bytes);
+  void put(void* p, size_t bytes);
+  void trim();
+  ~Pool();
+  size_t held() const { return held_; }
+ private:
+  std::multimap<size_t, void*> free_;
+  size_t held_ = 0;
+};
+
+struct DevBuf {
+  Pool* pool = nullptr;
+  void* ptr = nullptr;
+  size_t bytes = 0;
+  ~DevBuf() {
+    if (ptr && pool) pool->put(ptr, bytes);
+  }
+};
+using Buf = std::shared_ptr<DevBuf>;
+
+using Par = std::shared_ptr<const std::vector<uint8_t>>;  // parity of each basis state
+Par make_par(int n0, int n1);
+Par make_par(std::vector<uint8_t> v);
+Par fused_par(const std::vector<Par>& parts);
+int par_count(const Par& p, int c);
+
+struct Tensor {
+  std::vector<Par> legs;
+  std::vector<int64_t> dims;
+  std::vector<int64_t> strides;   // in elements
+  Buf buf;
+  int64_t offset = 0;             // element offset into buf
+
+  int rank() const { return (int)legs.size(); }
+  int64_t size() const {
+    int64_t s = 1;
+    for (auto d : dims) s *= d;
+    return s;
+  }
+  double* ptr() const { return buf ? (double*)buf->ptr + offset : nullptr; }
+  bool contiguous() const;
+};
+
+// Scratch for values the host reads back after a sync.
+struct HostScalars {
+  double* h = nullptr;     // pinned host
+  double* d = nullptr;     // device
+  int n = 0;
+};
+
+class Engine {
+ public:
+  explicit Engine(int device);
+  ~Engine();
+  cudaStream_t stream = nullptr;
+  int device = 0;
+  int num_sms = 148;
+  Pool pool;
+
+  Buf alloc(size_t bytes);
+  Tensor empty(const std::vector<Par>& legs);      // row-major, uninitialised
+  Tensor zeros(const std::vector<Par>& legs);      // row-major, zero-filled
+  Tensor upload(const std::vector<Par>& legs, const double* host);
+  std::vector<double> download(const Tensor& t);   // row-major dense copy
+
+  // device tables (int64) uploaded through a pinned staging ring
+  int64_t* upload_i64(const std::vector<int64_t>& v, Buf& keep);
+  int* upload_i32(const std::vector<int>& v, Buf& keep);
+
+  // Copy small host data to the device through a pinned staging ring, so the
+  // copy stays asynchronous (pageable-source copies serialise the stream).
+  void stage(const void* src, size_t bytes, void* dst);
+  char* ring = nullptr;
+  size_t ring_size = 0, ring_pos = 0;
+
+  void sync();
+  // device-side error flag written by kernels (nonfinite values, iteration caps)
+  int* dflag = nullptr;
+  void check_flag(const char* where);
+
+  // pinned scalar scratch
+  double* hscal = nullptr;
+  double* dscal = nullptr;
+  static constexpr int NSCAL = 4096;
+
+  // counters
+  long long launches = 0;
+  double flops = 0;
+};
+
+// ---------------------------------------------------------------------------
+// tensor primitives (tensor_ops.cu)
+// ---------------------------------------------------------------------------
+// einsum with two operands: "abc,cde->abde" style labels (single chars).
+Tensor ein(Engine& E, const std::string& spec, const Tensor& A, const Tensor& B, double alpha = 1.0);
+// single-operand relabel / permutation (materialised contiguous)
+Tensor perm(Engine& E, const Tensor& A, const std::vector<int>& order);
+Tensor perm_view(const Tensor& A, const std::vector<int>& order);
+Tensor contiguous(Engine& E, const Tensor& A);
+Tensor fuse(Engine& E, const Tensor& A, int first, int count);
+Tensor split(Engine& E, const Tensor& A, int axis, const std::vector<Par>& parts);
+Tensor clone(Engine& E, const Tensor& A);
+Tensor slice_leg(Engine& E, const Tensor& A, int axis, int index, Par newpar);
+
+void scale_inplace(Engine& E, Tensor& A, double s);
+// A := A / ||A|| computed on device (no host sync); flags nonfinite norms.
+void safe_scale_inplace(Engine& E, Tensor& A);
+Tensor axpby(Engine& E, double a, const Tensor& X, double b, const Tensor& Y);  // a X + b Y (same legs)
+// Reductions into device scalar slot `slot` of E.dscal (read after E.sync()).
+void norm2_to(Engine& E, const Tensor& A, int slot);   // sum of squares
+void dot_to(Engine& E, const Tensor& A, const Tensor& B, int slot);
+double norm(Engine& E, const Tensor& A);   // syncs
+double dot(Engine& E, const Tensor& A, const Tensor& B);   // syncs
+double sum_all(Engine& E, const Tensor& A);  // syncs
+bool all_finite(Engine& E, const Tensor& A);  // syncs
+
+// factorizations on the parity blocks of (rows | cols)
+struct QRres { Tensor Q, R; };
+QRres qr(Engine& E, const Tensor& A, const std::vector<int>& rows, const std::vector<int>& cols);
+struct LQres { Tensor L, Q; };
+LQres lq(Engine& E, const Tensor& A, const std::vector<int>& rows, const std::vector<int>& cols);
+
+struct Trunc {
+  int chi = -1;             // truncrank (-1: none)
+  int space[2] = {-1, -1};  // truncspace per sector (-1: none)
+  double atol = -1;         // trunctol (<0: none)
+};
+struct SVDres {
+  Tensor U, V;                    // U (rows..., new), V (new, cols...)
+  std::vector<double> S[2];       // kept singular values per sector (descending)
+  double err = 0;                 // 2-norm of discarded values
+  double entropy = 0;             // pretruncation Schmidt entropy (if asked)
+  double norm = 0;                // Frobenius norm of the input
+};
+SVDres svd(Engine& E, const Tensor& A, const std::vector<int>& rows, const std::vector<int>& cols,
+           const Trunc& tr, bool want_entropy = false);
+// eigendecomposition of a symmetric block matrix (rows | cols must match)
+struct EIGres {
+  std::vector<double> w[2];   // eigenvalues (ascending) per block
+  Tensor V;                   // (rows..., new)
+};
+EIGres eigh(Engine& E, const Tensor& A, const std::vector<int>& rows, const std::vector<int>& cols);
+// block inverse of a square 2-leg tensor (out,in) -> (in,out)
+Tensor block_inverse(Engine& E, const Tensor& R);
+// multiply a leg by a per-state diagonal (values in leg order) : A[..k..] *= d[k]
+Tensor scale_leg(Engine& E, const Tensor& A, int axis, const std::vector<double>& d);
+
+// host view of parity blocks (for tests / small control decisions)
+std::vector<int64_t> block_index(const std::vector<Par>& legs, const std::vector<int64_t>& strides,
+                                 int c);
+
+// Householder / Jacobi kernels (linalg.cu)
+namespace la {
+// column-major m x n blocks, batched over `count` problems given by descriptor arrays
+struct MatDesc {
+  double* a;       // input (overwritten), column-major, lda
+  double* q;       // output Q (column-major, ldq) for QR / U for SVD / V for eig
+  double* r;       // output R (column-major, ldr) / V for SVD
+  double* s;       // singular / eigen values
+  int m, n, lda, ldq, ldr;
+};
+void qr_batched(Engine& E, const std::vector<MatDesc>& d);
+void svd_batched(Engine& E, const std::vector<MatDesc>& d);    // m >= n required
+void eigh_batched(Engine& E, const std::vector<MatDesc>& d);   // symmetric n x n
+void inv_batched(Engine& E, const std::vector<MatDesc>& d);    // general square
+}  // namespace la
+
+// gather/scatter between tensors and dense column-major block matrices
+void gather_block(Engine& E, const Tensor& A, const int64_t* rt, const int64_t* ct, int M, int N,
+                  double* dst, int ld, bool transpose);
+void scatter_block(Engine& E, Tensor& A, const int64_t* rt, const int64_t* ct, int M, int N,
+                   const double* src, int ld, bool transpose);
+
+}  // namespace sps

@@ -1,0 +1,144 @@
+// The sample-ensemble hot path on the Z2 engine: row boundary-MPS
+// contraction, full update, Born sampling and energy measurement.  Each
+// function restates the reference function named beside it.
+#pragma once
+#include "engine.h"
+#include <array>
+#include <cmath>
+
+namespace sps {
+
+struct Model {
+  double J = 1.0, h = 0.7;
+};
+
+struct FUOptions {   // FullUpdate (src/evolution/full_update.jl:11-17)
+  int max_iterations = 4;
+  double error_tolerance = 1e-8;
+  double diagonal_shift = 1e-10;
+  int linear_max_iterations = 24;
+  double linear_tolerance = 1e-9;
+};
+
+struct BMPS {        // BoundaryMPS (src/contraction/boundary_mps.jl:11-18)
+  int chi = 32;
+  int space[2] = {-1, -1};
+};
+
+struct State {       // FiniteState (src/states/finite.jl:27-49)
+  int Lx = 0, Ly = 0;
+  std::vector<Tensor> sites;   // x + y*Lx, legs (W,N,Pout,Paux,E,S)
+  double beta = 0, log_amplitude = 0;
+  bool pepo = true;
+  Tensor& at(int x, int y) { return sites[x + y * Lx]; }
+  const Tensor& at(int x, int y) const { return sites[x + y * Lx]; }
+};
+
+struct Env {         // BoundaryEnvironment (boundary_mps.jl:79-83)
+  std::vector<Tensor> t;
+  double log_scale = 0, max_trunc = 0;
+};
+
+struct Entropy {     // BoundaryEntropy (boundary_mps.jl:44-57)
+  double maximum = 0;
+  bool profile = false;
+  int Lx = 0, Ly = 0;
+  std::vector<double> north, south;   // (Ly-1) x (Lx-1), row-major [row][bond]
+  void record(bool south_side, int row, int bond, double v) {
+    maximum = std::max(maximum, v);
+    if (profile && row >= 1 && row <= Ly - 1) (south_side ? south : north)[(row - 1) * (Lx - 1) + bond - 1] = v;
+  }
+};
+
+struct Layer {       // a row entry: plain double layer or SlabColumn (boundary_mps.jl:212-215)
+  Tensor a, b;
+  bool slab = false;
+};
+
+// contraction
+Tensor unit_tensor(Engine& E, const std::vector<Par>& legs);
+Tensor double_layer(Engine& E, const Tensor& ket, const Tensor& bra, const Tensor* physical = nullptr);
+std::vector<Tensor> row_layers(Engine& E, const State& s);
+Env trivial_boundary(Engine& E, const std::vector<Tensor>& row, bool north);
+struct CompressReport { double max_trunc, log_scale; };
+CompressReport compress_boundary(Engine& E, std::vector<Tensor>& B, const BMPS& m, bool reverse,
+                                 Entropy* ent, bool south_side, int row_cut);
+Env absorb(Engine& E, const Env& env, const std::vector<Tensor>& row, const BMPS& m, bool north,
+           Entropy* ent = nullptr, int row_cut = 0);
+double close_boundary(Engine& E, const std::vector<Tensor>& B);
+struct LogNorm { double log_norm, tensor_log_norm, max_env_trunc; };
+LogNorm lognorm(Engine& E, const State& s, const BMPS& m);
+struct Envs { std::vector<Env> north, south; double max_trunc = 0; };
+Envs boundary_environments(Engine& E, const std::vector<Tensor>& layers, int Lx, int Ly, const BMPS& m,
+                           int side /*0 both,1 north,2 south*/, Entropy* ent);
+Tensor left_step(Engine& E, const Tensor& L, const Tensor& T, const Layer& row, const Tensor& B);
+Tensor right_step(Engine& E, const Tensor& T, const Layer& row, const Tensor& B, const Tensor& R);
+Tensor row_edge(Engine& E, const std::vector<Tensor>& top, const std::vector<Layer>& row,
+                const std::vector<Tensor>& bottom, bool left);
+struct RowEnvs { std::vector<Tensor> left, right; };
+RowEnvs row_environments(Engine& E, const std::vector<Tensor>& top, const std::vector<Layer>& row,
+                         const std::vector<Tensor>& bottom, int side /*0 both,1 left,2 right*/);
+// full contraction of a row position; result accumulated into device slot
+void row_scalar_to(Engine& E, const Tensor& L, const Tensor& T, const Layer& row, const Tensor& B,
+                   const Tensor& R, int slot);
+
+// full update
+struct BondReport {
+  double initial_cost = 0, final_cost = 0, residual = 0;
+  int iterations = 0;
+  bool iteration_limit_reached = false;
+  int stop_reason = 0;   // 0 error_tolerance, 1 iteration_limit, 2 residual_fallback, 3 disabled
+  int repairs = 0;
+  int fallbacks = 0;
+  double max_env_trunc = 0;
+};
+struct StepReport {
+  double beta = 0;
+  std::vector<double> log_normalizations;
+  int bond_updates = 0, iteration_limit_hits = 0;
+  double max_state_truncation = 0, max_environment_truncation = 0, max_boundary_entropy = NAN;
+  double max_solver_residual = 0, max_iteration_limit_error = 0;
+  int stop_reasons[4] = {0, 0, 0, 0};
+  int repairs = 0, fallbacks = 0, linear_unconverged = 0;
+};
+Tensor trotter_gate(Engine& E, const Model& m, int Lx, int Ly, int ax, int ay, int bx, int by, double delta);
+StepReport evolution_step(Engine& E, State& s, const Model& m, double delta, int D, const FUOptions& o,
+                          const BMPS& env_method, int order, const int space[2], bool record_entropy,
+                          bool force_repair = false);
+std::vector<double> normalize_state(Engine& E, State& s);
+
+// sampling
+struct SamplingCache {
+  int Lx, Ly;
+  std::vector<Tensor> layers;
+  std::vector<std::array<Tensor, 2>> candidates;
+  std::vector<Env> south;
+  BMPS method;
+  const State* state_ref = nullptr;
+};
+SamplingCache make_sampling_cache(Engine& E, const State& s, const BMPS& m);
+struct SampleResult {
+  std::vector<int> config;   // labels 1/2, index x + y*Lx
+  double log_probability = 0;
+  double max_env_trunc = 0;
+  std::vector<double> conditionals;
+  int near_boundary = 0;     // draws within 1e-12 of a cumulative boundary
+};
+SampleResult sample_configuration(Engine& E, const SamplingCache& c, const double* uniforms,
+                                  const int* configuration);
+State project_configuration(Engine& E, const State& pepo, const int* configuration,
+                            std::vector<double>* log_norms);
+
+// measurement
+struct EnergyResult {
+  double energy_total, energy_per_site, log_norm, tensor_log_norm, max_env_trunc;
+  double x_sum, zz_sum;
+  std::vector<double> site_x;
+  Entropy entropy;
+};
+EnergyResult measure_energy(Engine& E, const State& s, const Model& m, const BMPS& method,
+                            bool record_entropy);
+
+State identity_pepo(Engine& E, int Lx, int Ly);
+
+}  // namespace sps

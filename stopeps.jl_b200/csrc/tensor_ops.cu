@@ -1,0 +1,1195 @@
+// Engine plumbing and the Z2 tensor primitives: table-driven block GEMM
+// (the contraction of every @tensor/ncon in the reference), strided
+// permutes, reductions, and the block gather/scatter around the
+// factorization kernels of linalg.cu.
+#include "engine.h"
+#include <algorithm>
+#include <cmath>
+#include <cstring>
+#include <numeric>
+
+namespace sps {
+
+// ---------------------------------------------------------------------------
+// pool
+// ---------------------------------------------------------------------------
+static size_t round_bytes(size_t b) {
+  if (b < 256) return 256;
+  if (b < (1u << 20)) {
+    size_t r = 256;
+    while (r < b) r <<= 1;
+    return r;
+  }
+  size_t mb = (size_t)1 << 20;
+  return ((b + mb - 1) / mb) * mb;
+}
+
+void* Pool::get(size_t bytes) {
+  auto it = free_.lower_bound(bytes);
+  if (it != free_.end() && it->first <= bytes + bytes / 4 + 4096) {
+    void* p = it->second;
+    held_ -= it->first;
+    free_.erase(it);
+    return p;
+  }
+  void* p = nullptr;
+  cudaError_t e = cudaMalloc(&p, bytes);
+  if (e != cudaSuccess) {
+    (void)cudaGetLastError();
+    trim();
+    SPS_CUDA(cudaMalloc(&p, bytes));
+  }
+  return p;
+}
+
+void Pool::put(void* p, size_t bytes) {
+  free_.emplace(bytes, p);
+  held_ += bytes;
+}
+
+void Pool::trim() {
+  cudaDeviceSynchronize();
+  for (auto& kv : free_) cudaFree(kv.second);
+  free_.clear();
+  held_ = 0;
+}
+
+Pool::~Pool() {
+  for (auto& kv : free_) cudaFree(kv.second);
+}
+
+// ---------------------------------------------------------------------------
+// parities
+// ---------------------------------------------------------------------------
+Par make_par(int n0, int n1) {
+  std::vector<uint8_t> v(n0 + n1, 0);
+  for (int i = n0; i < n0 + n1; ++i) v[i] = 1;
+  return std::make_shared<const std::vector<uint8_t>>(std::move(v));
+}
+Par make_par(std::vector<uint8_t> v) { return std::make_shared<const std::vector<uint8_t>>(std::move(v)); }
+Par fused_par(const std::vector<Par>& parts) {
+  std::vector<uint8_t> out(1, 0);
+  for (auto& p : parts) {
+    std::vector<uint8_t> nx;
+    nx.reserve(out.size() * p->size());
+    for (auto a : out)
+      for (auto b : *p) nx.push_back(a ^ b);
+    out.swap(nx);
+  }
+  return make_par(std::move(out));
+}
+int par_count(const Par& p, int c) {
+  int n = 0;
+  for (auto x : *p) n += (x == c);
+  return n;
+}
+
+bool Tensor::contiguous() const {
+  int64_t s = 1;
+  for (int k = rank() - 1; k >= 0; --k) {
+    if (dims[k] != 1 && strides[k] != s) return false;
+    s *= dims[k];
+  }
+  return true;
+}
+
+static std::vector<int64_t> rowmajor_strides(const std::vector<int64_t>& dims) {
+  std::vector<int64_t> s(dims.size());
+  int64_t acc = 1;
+  for (int k = (int)dims.size() - 1; k >= 0; --k) {
+    s[k] = acc;
+    acc *= dims[k];
+  }
+  return s;
+}
+
+// ---------------------------------------------------------------------------
+// engine
+// ---------------------------------------------------------------------------
+Engine::Engine(int dev) : device(dev) {
+  SPS_CUDA(cudaSetDevice(dev));
+  SPS_CUDA(cudaStreamCreateWithFlags(&stream, cudaStreamNonBlocking));
+  cudaDeviceProp prop;
+  SPS_CUDA(cudaGetDeviceProperties(&prop, dev));
+  num_sms = prop.multiProcessorCount;
+  SPS_CUDA(cudaMalloc(&dflag, sizeof(int) * 4));
+  SPS_CUDA(cudaMemset(dflag, 0, sizeof(int) * 4));
+  SPS_CUDA(cudaMallocHost(&hscal, sizeof(double) * NSCAL));
+  ring_size = (size_t)64 << 20;
+  SPS_CUDA(cudaMallocHost(&ring, ring_size));
+  SPS_CUDA(cudaMalloc(&dscal, sizeof(double) * NSCAL));
+}
+
+Engine::~Engine() {
+  cudaStreamSynchronize(stream);
+  cudaFree(dflag);
+  cudaFree(dscal);
+  cudaFreeHost(hscal);
+  cudaFreeHost(ring);
+  cudaStreamDestroy(stream);
+}
+
+Buf Engine::alloc(size_t bytes) {
+  auto b = std::make_shared<DevBuf>();
+  b->pool = &pool;
+  b->bytes = round_bytes(std::max<size_t>(bytes, 1));
+  b->ptr = pool.get(b->bytes);
+  return b;
+}
+
+Tensor Engine::empty(const std::vector<Par>& legs) {
+  Tensor t;
+  t.legs = legs;
+  for (auto& p : legs) t.dims.push_back((int64_t)p->size());
+  t.strides = rowmajor_strides(t.dims);
+  t.buf = alloc(std::max<int64_t>(t.size(), 1) * sizeof(double));
+  return t;
+}
+
+Tensor Engine::zeros(const std::vector<Par>& legs) {
+  Tensor t = empty(legs);
+  SPS_CUDA(cudaMemsetAsync(t.ptr(), 0, std::max<int64_t>(t.size(), 1) * sizeof(double), stream));
+  return t;
+}
+
+Tensor Engine::upload(const std::vector<Par>& legs, const double* host) {
+  Tensor t = empty(legs);
+  stage(host, t.size() * sizeof(double), t.ptr());
+  return t;
+}
+
+std::vector<double> Engine::download(const Tensor& t0) {
+  Tensor t = contiguous(*this, t0);
+  std::vector<double> h(t.size());
+  SPS_CUDA(cudaMemcpyAsync(h.data(), t.ptr(), t.size() * sizeof(double), cudaMemcpyDeviceToHost,
+                           stream));
+  sync();
+  return h;
+}
+
+void Engine::stage(const void* src, size_t bytes, void* dst) {
+  if (bytes == 0) return;
+  size_t need = (bytes + 255) & ~(size_t)255;
+  if (need > ring_size) {   // too large for the ring: synchronous copy
+    SPS_CUDA(cudaMemcpyAsync(dst, src, bytes, cudaMemcpyHostToDevice, stream));
+    return;
+  }
+  if (ring_pos + need > ring_size) sync();   // every earlier staged copy has completed
+  std::memcpy(ring + ring_pos, src, bytes);
+  SPS_CUDA(cudaMemcpyAsync(dst, ring + ring_pos, bytes, cudaMemcpyHostToDevice, stream));
+  ring_pos += need;
+}
+
+int64_t* Engine::upload_i64(const std::vector<int64_t>& v, Buf& keep) {
+  keep = alloc(std::max<size_t>(v.size(), 1) * sizeof(int64_t));
+  stage(v.data(), v.size() * sizeof(int64_t), keep->ptr);
+  return (int64_t*)keep->ptr;
+}
+
+int* Engine::upload_i32(const std::vector<int>& v, Buf& keep) {
+  keep = alloc(std::max<size_t>(v.size(), 1) * sizeof(int));
+  stage(v.data(), v.size() * sizeof(int), keep->ptr);
+  return (int*)keep->ptr;
+}
+
+void Engine::sync() {
+  SPS_CUDA(cudaStreamSynchronize(stream));
+  ring_pos = 0;
+}
+
+void Engine::check_flag(const char* where) {
+  int h = 0;
+  SPS_CUDA(cudaMemcpyAsync(&h, dflag, sizeof(int), cudaMemcpyDeviceToHost, stream));
+  sync();
+  if (h) {
+    SPS_CUDA(cudaMemsetAsync(dflag, 0, sizeof(int), stream));
+    if (h & 2) throw Error(SPS_ERR_CONVERGENCE, std::string(where) + ": device iteration cap reached");
+    throw Error(SPS_ERR_NUMERIC, std::string(where) + ": nonfinite or singular value on device");
+  }
+}
+
+// ---------------------------------------------------------------------------
+// index tables: offsets of the parity-c fused indices (row-major order)
+// ---------------------------------------------------------------------------
+std::vector<int64_t> block_index(const std::vector<Par>& legs, const std::vector<int64_t>& strides,
+                                 int c) {
+  std::vector<int64_t> out;
+  const int r = (int)legs.size();
+  if (r == 0) {
+    if (c == 0) out.push_back(0);
+    return out;
+  }
+  int64_t total = 1;
+  for (auto& p : legs) total *= (int64_t)p->size();
+  if (total == 0) return out;
+  out.reserve(total / 2 + 1);
+  std::vector<int> idx(r, 0);
+  int par = 0;
+  int64_t off = 0;
+  for (int k = 0; k < r; ++k) par ^= (*legs[k])[0];
+  while (true) {
+    if (par == c) out.push_back(off);
+    int k = r - 1;
+    while (k >= 0) {
+      const auto& p = *legs[k];
+      par ^= p[idx[k]];
+      off -= (int64_t)idx[k] * strides[k];
+      idx[k]++;
+      if (idx[k] < (int)p.size()) {
+        par ^= p[idx[k]];
+        off += (int64_t)idx[k] * strides[k];
+        break;
+      }
+      idx[k] = 0;
+      par ^= p[0];
+      --k;
+    }
+    if (k < 0) break;
+  }
+  return out;
+}
+
+// ---------------------------------------------------------------------------
+// kernels: gather GEMM, permute, elementwise, reductions
+// ---------------------------------------------------------------------------
+struct GemmProb {
+  const double* A;
+  const double* B;
+  double* C;
+  const int64_t *ra, *ca, *rb, *cb, *rc, *cc;
+  int M, N, K;
+  int a_kfast, b_jfast;
+};
+
+static constexpr int TM = 64, TN = 64, TK = 16, GT = 256;
+
+__global__ void __launch_bounds__(GT) gemm_gather_kernel(const GemmProb* probs, double alpha) {
+  const GemmProb P = probs[blockIdx.z];
+  const int i0 = blockIdx.y * TM, j0 = blockIdx.x * TN;
+  if (i0 >= P.M || j0 >= P.N) return;
+  __shared__ double As[TK][TM + 1];
+  __shared__ double Bs[TK][TN + 1];
+  __shared__ int64_t rA[TM], cB[TN];
+  const int t = threadIdx.x;
+  if (t < TM) rA[t] = (i0 + t < P.M) ? P.ra[i0 + t] : 0;
+  else if (t < TM + TN) cB[t - TM] = (j0 + t - TM < P.N) ? P.cb[j0 + t - TM] : 0;
+  const int tx = t % 16, ty = t / 16;
+  double acc[4][4] = {};
+  for (int k0 = 0; k0 < P.K; k0 += TK) {
+    __syncthreads();
+    // A tile: 64 x 16
+    if (P.a_kfast) {
+      int kk = t % 16;
+      int64_t ck = (k0 + kk < P.K) ? P.ca[k0 + kk] : -1;
+#pragma unroll
+      for (int r = 0; r < 4; ++r) {
+        int ii = t / 16 + 16 * r;
+        As[kk][ii] = (ck >= 0 && i0 + ii < P.M) ? P.A[rA[ii] + ck] : 0.0;
+      }
+    } else {
+      int ii = t % 64;
+#pragma unroll
+      for (int r = 0; r < 4; ++r) {
+        int kk = t / 64 + 4 * r;
+        As[kk][ii] = (k0 + kk < P.K && i0 + ii < P.M) ? P.A[rA[ii] + P.ca[k0 + kk]] : 0.0;
+      }
+    }
+    // B tile: 16 x 64
+    if (P.b_jfast) {
+      int jj = t % 64;
+#pragma unroll
+      for (int r = 0; r < 4; ++r) {
+        int kk = t / 64 + 4 * r;
+        Bs[kk][jj] = (k0 + kk < P.K && j0 + jj < P.N) ? P.B[P.rb[k0 + kk] + cB[jj]] : 0.0;
+      }
+    } else {
+      int kk = t % 16;
+      int64_t rk = (k0 + kk < P.K) ? P.rb[k0 + kk] : -1;
+#pragma unroll
+      for (int r = 0; r < 4; ++r) {
+        int jj = t / 16 + 16 * r;
+        Bs[kk][jj] = (rk >= 0 && j0 + jj < P.N) ? P.B[rk + cB[jj]] : 0.0;
+      }
+    }
+    __syncthreads();
+#pragma unroll
+    for (int kk = 0; kk < TK; ++kk) {
+      double a[4], b[4];
+#pragma unroll
+      for (int u = 0; u < 4; ++u) a[u] = As[kk][ty + 16 * u];
+#pragma unroll
+      for (int v = 0; v < 4; ++v) b[v] = Bs[kk][tx + 16 * v];
+#pragma unroll
+      for (int u = 0; u < 4; ++u)
+#pragma unroll
+        for (int v = 0; v < 4; ++v) acc[u][v] = fma(a[u], b[v], acc[u][v]);
+    }
+  }
+#pragma unroll
+  for (int u = 0; u < 4; ++u) {
+    int i = i0 + ty + 16 * u;
+    if (i >= P.M) continue;
+    int64_t ro = P.rc[i];
+#pragma unroll
+    for (int v = 0; v < 4; ++v) {
+      int j = j0 + tx + 16 * v;
+      if (j < P.N) P.C[ro + P.cc[j]] = alpha * acc[u][v];
+    }
+  }
+}
+
+struct PermDesc {
+  int rank;
+  int64_t dims[16];
+  int64_t istr[16];
+};
+
+__global__ void permute_kernel(const double* __restrict__ in, double* __restrict__ out, PermDesc d,
+                               int64_t total) {
+  for (int64_t o = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; o < total;
+       o += (int64_t)gridDim.x * blockDim.x) {
+    int64_t rem = o, off = 0;
+    for (int k = d.rank - 1; k >= 0; --k) {
+      int64_t q = rem / d.dims[k];
+      off += (rem - q * d.dims[k]) * d.istr[k];
+      rem = q;
+    }
+    out[o] = in[off];
+  }
+}
+
+__global__ void scale_kernel(double* a, int64_t n, double s) {
+  for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n;
+       i += (int64_t)gridDim.x * blockDim.x)
+    a[i] *= s;
+}
+
+__global__ void axpby_kernel(const double* x, const double* y, double* z, int64_t n, double a,
+                             double b) {
+  for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n;
+       i += (int64_t)gridDim.x * blockDim.x)
+    z[i] = a * x[i] + b * y[i];
+}
+
+static constexpr int RED_BLOCKS = 256;
+
+// per-block partial sums of x*y (y == nullptr: x*x), then a final pass.
+__global__ void dot_partial_kernel(const double* x, const double* y, int64_t n, double* partial) {
+  __shared__ double red[32];
+  double v = 0;
+  for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n;
+       i += (int64_t)gridDim.x * blockDim.x)
+    v += x[i] * (y ? y[i] : x[i]);
+  for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+  if ((threadIdx.x & 31) == 0) red[threadIdx.x >> 5] = v;
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    double s = 0;
+    for (int w = 0; w < (int)(blockDim.x >> 5); ++w) s += red[w];
+    partial[blockIdx.x] = s;
+  }
+}
+
+__global__ void final_sum_kernel(const double* partial, int nb, double* out) {
+  if (threadIdx.x == 0 && blockIdx.x == 0) {
+    double s = 0;
+    for (int i = 0; i < nb; ++i) s += partial[i];
+    *out = s;
+  }
+}
+
+__global__ void sum_partial_kernel(const double* x, int64_t n, double* partial) {
+  __shared__ double red[9];
+  double v = 0;
+  for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n;
+       i += (int64_t)gridDim.x * blockDim.x)
+    v += x[i];
+  for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+  if ((threadIdx.x & 31) == 0) red[threadIdx.x >> 5] = v;
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    double s = 0;
+    for (int w = 0; w < (int)(blockDim.x >> 5); ++w) s += red[w];
+    partial[blockIdx.x] = s;
+  }
+}
+
+__global__ void finite_partial_kernel(const double* x, int64_t n, double* partial) {
+  __shared__ int bad;
+  if (threadIdx.x == 0) bad = 0;
+  __syncthreads();
+  int b = 0;
+  for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n;
+       i += (int64_t)gridDim.x * blockDim.x)
+    b |= !isfinite(x[i]);
+  if (b) bad = 1;
+  __syncthreads();
+  if (threadIdx.x == 0) partial[blockIdx.x] = bad;
+}
+
+// A /= sqrt(*nrm2) when finite and nonzero; flags nonfinite.
+__global__ void safe_scale_kernel(double* a, int64_t n, const double* nrm2, int* flag) {
+  double s2 = *nrm2;
+  double s = sqrt(s2);
+  if (!isfinite(s)) {
+    if (blockIdx.x == 0 && threadIdx.x == 0) atomicOr(flag, 1);
+    return;
+  }
+  if (s == 0.0) return;
+  double inv = 1.0 / s;
+  for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n;
+       i += (int64_t)gridDim.x * blockDim.x)
+    a[i] *= inv;
+}
+
+__global__ void gather_kernel(const double* __restrict__ A, const int64_t* rt, const int64_t* ct,
+                              int M, int N, double* dst, int ld, int transpose) {
+  int64_t total = (int64_t)M * N;
+  for (int64_t e = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; e < total;
+       e += (int64_t)gridDim.x * blockDim.x) {
+    int i, j;
+    if (transpose) { j = (int)(e % N); i = (int)(e / N); }
+    else { i = (int)(e % M); j = (int)(e / M); }
+    double v = A[rt[i] + ct[j]];
+    if (transpose) dst[j + (int64_t)i * ld] = v;
+    else dst[i + (int64_t)j * ld] = v;
+  }
+}
+
+__global__ void scatter_kernel(double* __restrict__ A, const int64_t* rt, const int64_t* ct, int M,
+                               int N, const double* src, int ld, int transpose) {
+  int64_t total = (int64_t)M * N;
+  for (int64_t e = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; e < total;
+       e += (int64_t)gridDim.x * blockDim.x) {
+    int i, j;
+    if (transpose) { j = (int)(e % N); i = (int)(e / N); }
+    else { i = (int)(e % M); j = (int)(e / M); }
+    A[rt[i] + ct[j]] = transpose ? src[j + (int64_t)i * ld] : src[i + (int64_t)j * ld];
+  }
+}
+
+__global__ void scale_leg_kernel(const double* in, double* out, const double* d, int64_t total,
+                                 int64_t stride, int64_t dim) {
+  for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < total;
+       i += (int64_t)gridDim.x * blockDim.x)
+    out[i] = in[i] * d[(i / stride) % dim];
+}
+
+static int grid_for(int64_t n, int threads = 256) {
+  int64_t g = (n + threads - 1) / threads;
+  return (int)std::max<int64_t>(1, std::min<int64_t>(g, 148 * 16));
+}
+
+// ---------------------------------------------------------------------------
+// views / permutes
+// ---------------------------------------------------------------------------
+Tensor perm_view(const Tensor& A, const std::vector<int>& order) {
+  Tensor t;
+  t.buf = A.buf;
+  t.offset = A.offset;
+  for (int k : order) {
+    t.legs.push_back(A.legs[k]);
+    t.dims.push_back(A.dims[k]);
+    t.strides.push_back(A.strides[k]);
+  }
+  return t;
+}
+
+Tensor contiguous(Engine& E, const Tensor& A) {
+  if (A.contiguous()) return A;
+  Tensor out = E.empty(A.legs);
+  int64_t n = out.size();
+  if (n == 0) return out;
+  PermDesc d;
+  d.rank = A.rank();
+  if (d.rank > 16) throw Error(SPS_ERR_ARGUMENT, "rank > 16");
+  for (int k = 0; k < d.rank; ++k) {
+    d.dims[k] = A.dims[k];
+    d.istr[k] = A.strides[k];
+  }
+  permute_kernel<<<grid_for(n), 256, 0, E.stream>>>(A.ptr(), out.ptr(), d, n);
+  SPS_CUDA(cudaGetLastError());
+  E.launches++;
+  return out;
+}
+
+Tensor perm(Engine& E, const Tensor& A, const std::vector<int>& order) {
+  return contiguous(E, perm_view(A, order));
+}
+
+Tensor clone(Engine& E, const Tensor& A) {
+  Tensor c = contiguous(E, A);
+  if (c.buf != A.buf) return c;
+  Tensor out = E.empty(A.legs);
+  if (out.size())
+    SPS_CUDA(cudaMemcpyAsync(out.ptr(), c.ptr(), out.size() * sizeof(double),
+                             cudaMemcpyDeviceToDevice, E.stream));
+  return out;
+}
+
+Tensor fuse(Engine& E, const Tensor& A0, int first, int count) {
+  if (count == 1) return A0;
+  bool ok = true;
+  for (int k = first; k < first + count - 1; ++k)
+    if (A0.strides[k] != A0.strides[k + 1] * A0.dims[k + 1]) ok = false;
+  Tensor A = ok ? A0 : contiguous(E, A0);
+  Tensor t;
+  t.buf = A.buf;
+  t.offset = A.offset;
+  std::vector<Par> parts(A.legs.begin() + first, A.legs.begin() + first + count);
+  int64_t d = 1;
+  for (int k = first; k < first + count; ++k) d *= A.dims[k];
+  for (int k = 0; k < A.rank(); ++k) {
+    if (k == first) {
+      t.legs.push_back(fused_par(parts));
+      t.dims.push_back(d);
+      t.strides.push_back(A.strides[first + count - 1]);
+      k = first + count - 1;
+      continue;
+    }
+    t.legs.push_back(A.legs[k]);
+    t.dims.push_back(A.dims[k]);
+    t.strides.push_back(A.strides[k]);
+  }
+  return t;
+}
+
+Tensor split(Engine& E, const Tensor& A, int axis, const std::vector<Par>& parts) {
+  (void)E;
+  Tensor t;
+  t.buf = A.buf;
+  t.offset = A.offset;
+  for (int k = 0; k < A.rank(); ++k) {
+    if (k == axis) {
+      int64_t s = A.strides[k];
+      std::vector<int64_t> ps(parts.size());
+      for (int q = (int)parts.size() - 1; q >= 0; --q) {
+        ps[q] = s;
+        s *= (int64_t)parts[q]->size();
+      }
+      for (size_t q = 0; q < parts.size(); ++q) {
+        t.legs.push_back(parts[q]);
+        t.dims.push_back((int64_t)parts[q]->size());
+        t.strides.push_back(ps[q]);
+      }
+      continue;
+    }
+    t.legs.push_back(A.legs[k]);
+    t.dims.push_back(A.dims[k]);
+    t.strides.push_back(A.strides[k]);
+  }
+  return t;
+}
+
+Tensor slice_leg(Engine& E, const Tensor& A, int axis, int index, Par newpar) {
+  Tensor t = A;
+  t.offset += (int64_t)index * A.strides[axis];
+  t.dims[axis] = 1;
+  t.legs[axis] = newpar;
+  return contiguous(E, t);
+}
+
+// ---------------------------------------------------------------------------
+// elementwise and reductions
+// ---------------------------------------------------------------------------
+void scale_inplace(Engine& E, Tensor& A, double s) {
+  A = contiguous(E, A);
+  int64_t n = A.size();
+  if (!n) return;
+  scale_kernel<<<grid_for(n), 256, 0, E.stream>>>(A.ptr(), n, s);
+  SPS_CUDA(cudaGetLastError());
+  E.launches++;
+}
+
+static void reduce_dot(Engine& E, const double* x, const double* y, int64_t n, double* out) {
+  Buf part = E.alloc(RED_BLOCKS * sizeof(double));
+  int nb = (int)std::max<int64_t>(1, std::min<int64_t>(RED_BLOCKS, (n + 255) / 256));
+  dot_partial_kernel<<<nb, 256, 0, E.stream>>>(x, y, n, (double*)part->ptr);
+  final_sum_kernel<<<1, 32, 0, E.stream>>>((double*)part->ptr, nb, out);
+  SPS_CUDA(cudaGetLastError());
+  E.launches += 2;
+}
+
+void norm2_to(Engine& E, const Tensor& A0, int slot) {
+  Tensor A = contiguous(E, A0);
+  reduce_dot(E, A.ptr(), nullptr, A.size(), E.dscal + slot);
+}
+
+void dot_to(Engine& E, const Tensor& A0, const Tensor& B0, int slot) {
+  Tensor A = contiguous(E, A0), B = contiguous(E, B0);
+  if (A.size() != B.size()) throw Error(SPS_ERR_ARGUMENT, "dot: size mismatch");
+  reduce_dot(E, A.ptr(), B.ptr(), A.size(), E.dscal + slot);
+}
+
+static double read_slot(Engine& E, int slot) {
+  SPS_CUDA(cudaMemcpyAsync(E.hscal + slot, E.dscal + slot, sizeof(double), cudaMemcpyDeviceToHost,
+                           E.stream));
+  E.sync();
+  return E.hscal[slot];
+}
+
+double norm(Engine& E, const Tensor& A) {
+  norm2_to(E, A, 0);
+  return std::sqrt(read_slot(E, 0));
+}
+
+double dot(Engine& E, const Tensor& A, const Tensor& B) {
+  dot_to(E, A, B, 0);
+  return read_slot(E, 0);
+}
+
+double sum_all(Engine& E, const Tensor& A0) {
+  Tensor A = contiguous(E, A0);
+  Buf part = E.alloc(RED_BLOCKS * sizeof(double));
+  int64_t n = A.size();
+  int nb = (int)std::max<int64_t>(1, std::min<int64_t>(RED_BLOCKS, (n + 255) / 256));
+  sum_partial_kernel<<<nb, 256, 0, E.stream>>>(A.ptr(), n, (double*)part->ptr);
+  final_sum_kernel<<<1, 32, 0, E.stream>>>((double*)part->ptr, nb, E.dscal);
+  E.launches += 2;
+  return read_slot(E, 0);
+}
+
+bool all_finite(Engine& E, const Tensor& A0) {
+  Tensor A = contiguous(E, A0);
+  Buf part = E.alloc(RED_BLOCKS * sizeof(double));
+  int64_t n = A.size();
+  int nb = (int)std::max<int64_t>(1, std::min<int64_t>(RED_BLOCKS, (n + 255) / 256));
+  finite_partial_kernel<<<nb, 256, 0, E.stream>>>(A.ptr(), n, (double*)part->ptr);
+  sum_partial_kernel<<<1, 256, 0, E.stream>>>((double*)part->ptr, nb, E.dscal + 1);
+  E.launches += 2;
+  return read_slot(E, 1) == 0.0;
+}
+
+void safe_scale_inplace(Engine& E, Tensor& A) {
+  A = contiguous(E, A);
+  norm2_to(E, A, 2);
+  int64_t n = A.size();
+  safe_scale_kernel<<<grid_for(n), 256, 0, E.stream>>>(A.ptr(), n, E.dscal + 2, E.dflag);
+  SPS_CUDA(cudaGetLastError());
+  E.launches++;
+}
+
+Tensor axpby(Engine& E, double a, const Tensor& X0, double b, const Tensor& Y0) {
+  Tensor X = contiguous(E, X0), Y = contiguous(E, Y0);
+  if (X.size() != Y.size()) throw Error(SPS_ERR_ARGUMENT, "axpby: size mismatch");
+  Tensor Z = E.empty(X.legs);
+  int64_t n = Z.size();
+  if (n) {
+    axpby_kernel<<<grid_for(n), 256, 0, E.stream>>>(X.ptr(), Y.ptr(), Z.ptr(), n, a, b);
+    SPS_CUDA(cudaGetLastError());
+    E.launches++;
+  }
+  return Z;
+}
+
+Tensor scale_leg(Engine& E, const Tensor& A0, int axis, const std::vector<double>& d) {
+  Tensor A = contiguous(E, A0);
+  Tensor out = E.empty(A.legs);
+  Buf kd = E.alloc(std::max<size_t>(d.size(), 1) * sizeof(double));
+  E.stage(d.data(), d.size() * sizeof(double), kd->ptr);
+  int64_t n = A.size();
+  if (n) {
+    scale_leg_kernel<<<grid_for(n), 256, 0, E.stream>>>(A.ptr(), out.ptr(), (double*)kd->ptr, n,
+                                                         A.strides[axis], A.dims[axis]);
+    SPS_CUDA(cudaGetLastError());
+    E.launches++;
+  }
+  return out;
+}
+
+void gather_block(Engine& E, const Tensor& A, const int64_t* rt, const int64_t* ct, int M, int N,
+                  double* dst, int ld, bool transpose) {
+  int64_t n = (int64_t)M * N;
+  if (!n) return;
+  gather_kernel<<<grid_for(n), 256, 0, E.stream>>>(A.ptr(), rt, ct, M, N, dst, ld, transpose);
+  SPS_CUDA(cudaGetLastError());
+  E.launches++;
+}
+
+void scatter_block(Engine& E, Tensor& A, const int64_t* rt, const int64_t* ct, int M, int N,
+                   const double* src, int ld, bool transpose) {
+  int64_t n = (int64_t)M * N;
+  if (!n) return;
+  scatter_kernel<<<grid_for(n), 256, 0, E.stream>>>(A.ptr(), rt, ct, M, N, src, ld, transpose);
+  SPS_CUDA(cudaGetLastError());
+  E.launches++;
+}
+
+// ---------------------------------------------------------------------------
+// einsum (two operands)
+// ---------------------------------------------------------------------------
+static bool same_par(const Par& a, const Par& b) { return a == b || *a == *b; }
+
+Tensor ein(Engine& E, const std::string& spec, const Tensor& A, const Tensor& B, double alpha) {
+  auto arrow = spec.find("->");
+  auto comma = spec.find(',');
+  if (arrow == std::string::npos || comma == std::string::npos || comma > arrow)
+    throw Error(SPS_ERR_ARGUMENT, "ein: bad spec " + spec);
+  std::string la = spec.substr(0, comma), lb = spec.substr(comma + 1, arrow - comma - 1),
+              lo = spec.substr(arrow + 2);
+  if ((int)la.size() != A.rank() || (int)lb.size() != B.rank())
+    throw Error(SPS_ERR_ARGUMENT, "ein: rank mismatch in " + spec);
+  std::vector<int> fa, fb, ka, kb;   // free A, free B, contracted (A idx, B idx)
+  for (int i = 0; i < (int)la.size(); ++i) {
+    char ch = la[i];
+    auto pb = lb.find(ch);
+    auto po = lo.find(ch);
+    if (pb != std::string::npos && po == std::string::npos) {
+      ka.push_back(i);
+      kb.push_back((int)pb);
+      if (A.dims[i] != B.dims[pb] || !same_par(A.legs[i], B.legs[pb]))
+        throw Error(SPS_ERR_ARGUMENT, std::string("ein: leg mismatch on '") + ch + "' in " + spec);
+    } else if (po != std::string::npos && pb == std::string::npos) {
+      fa.push_back(i);
+    } else {
+      throw Error(SPS_ERR_ARGUMENT, "ein: unsupported label use in " + spec);
+    }
+  }
+  for (int j = 0; j < (int)lb.size(); ++j) {
+    char ch = lb[j];
+    if (la.find(ch) != std::string::npos) continue;
+    if (lo.find(ch) == std::string::npos) throw Error(SPS_ERR_ARGUMENT, "ein: trace in " + spec);
+    fb.push_back(j);
+  }
+  if (fa.size() + fb.size() != lo.size()) throw Error(SPS_ERR_ARGUMENT, "ein: output mismatch " + spec);
+  std::vector<Par> olegs;
+  for (char ch : lo) {
+    auto p = la.find(ch);
+    if (p != std::string::npos) olegs.push_back(A.legs[p]);
+    else olegs.push_back(B.legs[lb.find(ch)]);
+  }
+  Tensor C = E.zeros(olegs);
+  if (C.size() == 0 || A.size() == 0 || B.size() == 0) return C;
+  auto pick = [](const Tensor& T, const std::vector<int>& ix, std::vector<Par>& L,
+                 std::vector<int64_t>& S) {
+    for (int k : ix) {
+      L.push_back(T.legs[k]);
+      S.push_back(T.strides[k]);
+    }
+  };
+  std::vector<Par> LfA, LfB, Lk;
+  std::vector<int64_t> SfA, SfB, SkA, SkB, ScA, ScB;
+  pick(A, fa, LfA, SfA);
+  pick(B, fb, LfB, SfB);
+  {
+    std::vector<Par> dummy;
+    pick(A, ka, Lk, SkA);
+    pick(B, kb, dummy, SkB);
+  }
+  for (int k : fa) ScA.push_back(C.strides[lo.find(la[k])]);
+  for (int k : fb) ScB.push_back(C.strides[lo.find(lb[k])]);
+  std::vector<GemmProb> probs;
+  std::vector<Buf> keep;
+  int maxM = 0, maxN = 0;
+  for (int c = 0; c < 2; ++c) {
+    auto ra = block_index(LfA, SfA, c), rc = block_index(LfA, ScA, c);
+    auto ca = block_index(Lk, SkA, c), rb = block_index(Lk, SkB, c);
+    auto cb = block_index(LfB, SfB, c), cc = block_index(LfB, ScB, c);
+    if (ra.empty() || cb.empty() || ca.empty()) continue;
+    GemmProb P;
+    P.A = A.ptr();
+    P.B = B.ptr();
+    P.C = C.ptr();
+    Buf b1, b2, b3, b4, b5, b6;
+    P.ra = E.upload_i64(ra, b1);
+    P.ca = E.upload_i64(ca, b2);
+    P.rb = E.upload_i64(rb, b3);
+    P.cb = E.upload_i64(cb, b4);
+    P.rc = E.upload_i64(rc, b5);
+    P.cc = E.upload_i64(cc, b6);
+    keep.insert(keep.end(), {b1, b2, b3, b4, b5, b6});
+    P.M = (int)ra.size();
+    P.N = (int)cb.size();
+    P.K = (int)ca.size();
+    P.a_kfast = (ca.size() > 1 && ca[1] - ca[0] == 1) ? 1 : 0;
+    P.b_jfast = (cb.size() > 1 && cb[1] - cb[0] == 1) ? 1 : (rb.size() > 1 && rb[1] - rb[0] == 1 ? 0 : 1);
+    maxM = std::max(maxM, P.M);
+    maxN = std::max(maxN, P.N);
+    E.flops += 2.0 * P.M * P.N * P.K;
+    probs.push_back(P);
+  }
+  if (probs.empty()) return C;
+  Buf kp = E.alloc(probs.size() * sizeof(GemmProb));
+  E.stage(probs.data(), probs.size() * sizeof(GemmProb), kp->ptr);
+  dim3 grid((maxN + TN - 1) / TN, (maxM + TM - 1) / TM, (unsigned)probs.size());
+  gemm_gather_kernel<<<grid, GT, 0, E.stream>>>((const GemmProb*)kp->ptr, alpha);
+  SPS_CUDA(cudaGetLastError());
+  E.launches++;
+  return C;
+}
+
+// ---------------------------------------------------------------------------
+// factorizations
+// ---------------------------------------------------------------------------
+namespace {
+struct BlockTables {
+  std::vector<Par> rp, cp;
+  std::vector<int64_t> rs, cs;
+  std::vector<int64_t> rt[2], ct[2];
+};
+
+BlockTables tables_of(const Tensor& A, const std::vector<int>& rows, const std::vector<int>& cols) {
+  BlockTables t;
+  for (int k : rows) {
+    t.rp.push_back(A.legs[k]);
+    t.rs.push_back(A.strides[k]);
+  }
+  for (int k : cols) {
+    t.cp.push_back(A.legs[k]);
+    t.cs.push_back(A.strides[k]);
+  }
+  for (int c = 0; c < 2; ++c) {
+    t.rt[c] = block_index(t.rp, t.rs, c);
+    t.ct[c] = block_index(t.cp, t.cs, c);
+  }
+  return t;
+}
+
+std::vector<int64_t> leg_offsets(int c, int k0, int k1, int64_t stride) {
+  std::vector<int64_t> v;
+  int base = c == 0 ? 0 : k0;
+  int k = c == 0 ? k0 : k1;
+  for (int i = 0; i < k; ++i) v.push_back((int64_t)(base + i) * stride);
+  return v;
+}
+
+std::vector<int64_t> tensor_rows(const Tensor& T, int first, int count, int c) {
+  std::vector<Par> L(T.legs.begin() + first, T.legs.begin() + first + count);
+  std::vector<int64_t> S(T.strides.begin() + first, T.strides.begin() + first + count);
+  return block_index(L, S, c);
+}
+}  // namespace
+
+QRres qr(Engine& E, const Tensor& A, const std::vector<int>& rows, const std::vector<int>& cols) {
+  BlockTables bt = tables_of(A, rows, cols);
+  int m[2], n[2], k[2];
+  for (int c = 0; c < 2; ++c) {
+    m[c] = (int)bt.rt[c].size();
+    n[c] = (int)bt.ct[c].size();
+    k[c] = std::min(m[c], n[c]);
+  }
+  Par nl = make_par(k[0], k[1]);
+  std::vector<Par> ql = bt.rp;
+  ql.push_back(nl);
+  std::vector<Par> rl{nl};
+  rl.insert(rl.end(), bt.cp.begin(), bt.cp.end());
+  QRres res{E.zeros(ql), E.zeros(rl)};
+  std::vector<la::MatDesc> ds;
+  std::vector<Buf> keep;
+  for (int c = 0; c < 2; ++c) {
+    if (k[c] == 0) continue;
+    Buf ba = E.alloc(sizeof(double) * ((size_t)m[c] * n[c] + (size_t)m[c] * k[c] + (size_t)k[c] * n[c] + k[c]));
+    double* a = (double*)ba->ptr;
+    double* q = a + (size_t)m[c] * n[c];
+    double* r = q + (size_t)m[c] * k[c];
+    double* s = r + (size_t)k[c] * n[c];
+    Buf t1, t2;
+    int64_t* rt = E.upload_i64(bt.rt[c], t1);
+    int64_t* ct = E.upload_i64(bt.ct[c], t2);
+    gather_block(E, A, rt, ct, m[c], n[c], a, m[c], false);
+    ds.push_back({a, q, r, s, m[c], n[c], m[c], m[c], k[c]});
+    keep.insert(keep.end(), {ba, t1, t2});
+  }
+  la::qr_batched(E, ds);
+  int di = 0;
+  for (int c = 0; c < 2; ++c) {
+    if (k[c] == 0) continue;
+    auto& d = ds[di++];
+    Buf t1, t2, t3, t4;
+    int nr = (int)rows.size();
+    auto qrow = tensor_rows(res.Q, 0, nr, c);
+    auto qcol = leg_offsets(c, k[0], k[1], res.Q.strides[nr]);
+    scatter_block(E, res.Q, E.upload_i64(qrow, t1), E.upload_i64(qcol, t2), m[c], k[c], d.q, m[c], false);
+    auto rrow = leg_offsets(c, k[0], k[1], res.R.strides[0]);
+    auto rcol = tensor_rows(res.R, 1, (int)cols.size(), c);
+    scatter_block(E, res.R, E.upload_i64(rrow, t3), E.upload_i64(rcol, t4), k[c], n[c], d.r, k[c], false);
+    keep.insert(keep.end(), {t1, t2, t3, t4});
+  }
+  return res;
+}
+
+LQres lq(Engine& E, const Tensor& A, const std::vector<int>& rows, const std::vector<int>& cols) {
+  BlockTables bt = tables_of(A, rows, cols);
+  int m[2], n[2], k[2];
+  for (int c = 0; c < 2; ++c) {
+    m[c] = (int)bt.rt[c].size();
+    n[c] = (int)bt.ct[c].size();
+    k[c] = std::min(m[c], n[c]);
+  }
+  Par nl = make_par(k[0], k[1]);
+  std::vector<Par> ll = bt.rp;
+  ll.push_back(nl);
+  std::vector<Par> qlg{nl};
+  qlg.insert(qlg.end(), bt.cp.begin(), bt.cp.end());
+  LQres res{E.zeros(ll), E.zeros(qlg)};
+  std::vector<la::MatDesc> ds;
+  std::vector<Buf> keep;
+  for (int c = 0; c < 2; ++c) {
+    if (k[c] == 0) continue;
+    // QR of the transpose: a = M^T (n x m)
+    Buf ba = E.alloc(sizeof(double) * ((size_t)m[c] * n[c] + (size_t)n[c] * k[c] + (size_t)k[c] * m[c] + k[c]));
+    double* a = (double*)ba->ptr;
+    double* q = a + (size_t)m[c] * n[c];
+    double* r = q + (size_t)n[c] * k[c];
+    double* s = r + (size_t)k[c] * m[c];
+    Buf t1, t2;
+    gather_block(E, A, E.upload_i64(bt.rt[c], t1), E.upload_i64(bt.ct[c], t2), m[c], n[c], a, n[c], true);
+    ds.push_back({a, q, r, s, n[c], m[c], n[c], n[c], k[c]});
+    keep.insert(keep.end(), {ba, t1, t2});
+  }
+  la::qr_batched(E, ds);
+  int di = 0;
+  for (int c = 0; c < 2; ++c) {
+    if (k[c] == 0) continue;
+    auto& d = ds[di++];
+    Buf t1, t2, t3, t4;
+    int nr = (int)rows.size();
+    // L (m x k) = R'^T, R' is k x m col-major (ld k)
+    auto lrow = tensor_rows(res.L, 0, nr, c);
+    auto lcol = leg_offsets(c, k[0], k[1], res.L.strides[nr]);
+    scatter_block(E, res.L, E.upload_i64(lrow, t1), E.upload_i64(lcol, t2), m[c], k[c], d.r, k[c], true);
+    // Q (k x n) = Q'^T, Q' is n x k col-major (ld n)
+    auto qrow = leg_offsets(c, k[0], k[1], res.Q.strides[0]);
+    auto qcol = tensor_rows(res.Q, 1, (int)cols.size(), c);
+    scatter_block(E, res.Q, E.upload_i64(qrow, t3), E.upload_i64(qcol, t4), k[c], n[c], d.q, n[c], true);
+    keep.insert(keep.end(), {t1, t2, t3, t4});
+  }
+  return res;
+}
+
+static std::vector<char> select_truncation(const std::vector<double> s[2], const Trunc& tr,
+                                           std::vector<char> keep[2]) {
+  for (int c = 0; c < 2; ++c) keep[c].assign(s[c].size(), 1);
+  if (tr.chi >= 0) {
+    struct E3 { double v; int c, i; };
+    std::vector<E3> all;
+    for (int c = 0; c < 2; ++c)
+      for (int i = 0; i < (int)s[c].size(); ++i) all.push_back({s[c][i], c, i});
+    std::stable_sort(all.begin(), all.end(), [](const E3& a, const E3& b) {
+      if (a.v != b.v) return a.v > b.v;
+      if (a.c != b.c) return a.c < b.c;
+      return a.i < b.i;
+    });
+    std::vector<char> sel[2];
+    for (int c = 0; c < 2; ++c) sel[c].assign(s[c].size(), 0);
+    for (int q = 0; q < (int)all.size() && q < tr.chi; ++q) sel[all[q].c][all[q].i] = 1;
+    for (int c = 0; c < 2; ++c)
+      for (size_t i = 0; i < s[c].size(); ++i) keep[c][i] &= sel[c][i];
+  }
+  for (int c = 0; c < 2; ++c) {
+    if (tr.space[0] >= 0)
+      for (size_t i = 0; i < s[c].size(); ++i)
+        if ((int)i >= tr.space[c]) keep[c][i] = 0;
+    if (tr.atol >= 0)
+      for (size_t i = 0; i < s[c].size(); ++i)
+        if (!(s[c][i] > tr.atol)) keep[c][i] = 0;
+  }
+  return {};
+}
+
+SVDres svd(Engine& E, const Tensor& A, const std::vector<int>& rows, const std::vector<int>& cols,
+           const Trunc& tr, bool want_entropy) {
+  BlockTables bt = tables_of(A, rows, cols);
+  int m[2], n[2], k[2];
+  bool tall[2];
+  for (int c = 0; c < 2; ++c) {
+    m[c] = (int)bt.rt[c].size();
+    n[c] = (int)bt.ct[c].size();
+    k[c] = std::min(m[c], n[c]);
+    tall[c] = m[c] >= n[c];
+  }
+  std::vector<la::MatDesc> ds;
+  std::vector<Buf> keep;
+  int dmap[2] = {-1, -1};
+  for (int c = 0; c < 2; ++c) {
+    if (k[c] == 0) continue;
+    int mm = tall[c] ? m[c] : n[c], nn = tall[c] ? n[c] : m[c];
+    Buf ba = E.alloc(sizeof(double) * ((size_t)mm * nn * 2 + (size_t)nn * nn + nn));
+    double* a = (double*)ba->ptr;
+    double* q = a + (size_t)mm * nn;
+    double* r = q + (size_t)mm * nn;
+    double* s = r + (size_t)nn * nn;
+    Buf t1, t2;
+    gather_block(E, A, E.upload_i64(bt.rt[c], t1), E.upload_i64(bt.ct[c], t2), m[c], n[c], a,
+                 tall[c] ? m[c] : n[c], !tall[c]);
+    dmap[c] = (int)ds.size();
+    ds.push_back({a, q, r, s, mm, nn, mm, mm, nn});
+    keep.insert(keep.end(), {ba, t1, t2});
+  }
+  la::svd_batched(E, ds);
+  SVDres res;
+  std::vector<double> sv[2];
+  // copy singular values back
+  int off = 0;
+  for (int c = 0; c < 2; ++c) {
+    if (dmap[c] < 0) continue;
+    SPS_CUDA(cudaMemcpyAsync(E.hscal + off, ds[dmap[c]].s, sizeof(double) * k[c], cudaMemcpyDeviceToHost,
+                             E.stream));
+    off += k[c];
+  }
+  if (off > Engine::NSCAL) throw Error(SPS_ERR_ARGUMENT, "svd: too many singular values");
+  E.sync();
+  E.check_flag("svd");
+  off = 0;
+  for (int c = 0; c < 2; ++c) {
+    if (dmap[c] < 0) continue;
+    sv[c].assign(E.hscal + off, E.hscal + off + k[c]);
+    off += k[c];
+  }
+  double tot2 = 0;
+  for (int c = 0; c < 2; ++c)
+    for (double x : sv[c]) tot2 += x * x;
+  res.norm = std::sqrt(tot2);
+  if (want_entropy) {
+    double scale = res.norm;
+    if (scale == 0) res.entropy = NAN;
+    else {
+      double ent = 0;
+      for (int c = 0; c < 2; ++c)
+        for (double x : sv[c]) {
+          double p = (x / scale) * (x / scale);
+          if (p != 0) ent -= p * std::log(p);
+        }
+      res.entropy = std::max(0.0, ent);
+    }
+  }
+  std::vector<char> kp[2];
+  select_truncation(sv, tr, kp);
+  int kk[2] = {0, 0};
+  double disc = 0;
+  for (int c = 0; c < 2; ++c) {
+    for (size_t i = 0; i < sv[c].size(); ++i) {
+      if (kp[c][i]) {
+        if ((int)i != kk[c]) throw Error(SPS_ERR_NUMERIC, "svd: non-prefix truncation");
+        kk[c]++;
+        res.S[c].push_back(sv[c][i]);
+      } else {
+        disc += sv[c][i] * sv[c][i];
+      }
+    }
+  }
+  res.err = std::sqrt(disc);
+  Par nl = make_par(kk[0], kk[1]);
+  std::vector<Par> ul = bt.rp;
+  ul.push_back(nl);
+  std::vector<Par> vl{nl};
+  vl.insert(vl.end(), bt.cp.begin(), bt.cp.end());
+  res.U = E.zeros(ul);
+  res.V = E.zeros(vl);
+  int nr = (int)rows.size();
+  for (int c = 0; c < 2; ++c) {
+    if (dmap[c] < 0 || kk[c] == 0) continue;
+    auto& d = ds[dmap[c]];
+    Buf t1, t2, t3, t4;
+    auto urow = tensor_rows(res.U, 0, nr, c);
+    auto ucol = leg_offsets(c, kk[0], kk[1], res.U.strides[nr]);
+    auto vrow = leg_offsets(c, kk[0], kk[1], res.V.strides[0]);
+    auto vcol = tensor_rows(res.V, 1, (int)cols.size(), c);
+    int64_t* urd = E.upload_i64(urow, t1);
+    int64_t* ucd = E.upload_i64(ucol, t2);
+    int64_t* vrd = E.upload_i64(vrow, t3);
+    int64_t* vcd = E.upload_i64(vcol, t4);
+    if (tall[c]) {
+      // U = q (m x n, ld m), V rows = columns of r (n x n, ld n)
+      scatter_block(E, res.U, urd, ucd, m[c], kk[c], d.q, m[c], false);
+      scatter_block(E, res.V, vrd, vcd, kk[c], n[c], d.r, n[c], true);
+    } else {
+      // M^T = U' S V'^T: U = V' (r, m x m, ld m); V rows = columns of U' (q, n x m, ld n)
+      scatter_block(E, res.U, urd, ucd, m[c], kk[c], d.r, m[c], false);
+      scatter_block(E, res.V, vrd, vcd, kk[c], n[c], d.q, n[c], true);
+    }
+    keep.insert(keep.end(), {t1, t2, t3, t4});
+  }
+  return res;
+}
+
+EIGres eigh(Engine& E, const Tensor& A, const std::vector<int>& rows, const std::vector<int>& cols) {
+  BlockTables bt = tables_of(A, rows, cols);
+  int n[2];
+  for (int c = 0; c < 2; ++c) {
+    n[c] = (int)bt.rt[c].size();
+    if ((int)bt.ct[c].size() != n[c]) throw Error(SPS_ERR_ARGUMENT, "eigh: non-square block");
+  }
+  std::vector<la::MatDesc> ds;
+  std::vector<Buf> keep;
+  int dmap[2] = {-1, -1};
+  for (int c = 0; c < 2; ++c) {
+    if (n[c] == 0) continue;
+    Buf ba = E.alloc(sizeof(double) * ((size_t)n[c] * n[c] * 2 + n[c]));
+    double* a = (double*)ba->ptr;
+    double* q = a + (size_t)n[c] * n[c];
+    double* s = q + (size_t)n[c] * n[c];
+    Buf t1, t2;
+    gather_block(E, A, E.upload_i64(bt.rt[c], t1), E.upload_i64(bt.ct[c], t2), n[c], n[c], a, n[c], false);
+    dmap[c] = (int)ds.size();
+    ds.push_back({a, q, nullptr, s, n[c], n[c], n[c], n[c], 0});
+    keep.insert(keep.end(), {ba, t1, t2});
+  }
+  la::eigh_batched(E, ds);
+  EIGres res;
+  int off = 0;
+  for (int c = 0; c < 2; ++c) {
+    if (dmap[c] < 0) continue;
+    SPS_CUDA(cudaMemcpyAsync(E.hscal + off, ds[dmap[c]].s, sizeof(double) * n[c], cudaMemcpyDeviceToHost,
+                             E.stream));
+    off += n[c];
+  }
+  if (off > Engine::NSCAL) throw Error(SPS_ERR_ARGUMENT, "eigh: too large");
+  E.sync();
+  E.check_flag("eigh");
+  off = 0;
+  for (int c = 0; c < 2; ++c) {
+    if (dmap[c] < 0) continue;
+    res.w[c].assign(E.hscal + off, E.hscal + off + n[c]);
+    off += n[c];
+  }
+  Par nl = make_par(n[0], n[1]);
+  std::vector<Par> vl = bt.rp;
+  vl.push_back(nl);
+  res.V = E.zeros(vl);
+  int nr = (int)rows.size();
+  for (int c = 0; c < 2; ++c) {
+    if (dmap[c] < 0) continue;
+    Buf t1, t2;
+    auto vr = tensor_rows(res.V, 0, nr, c);
+    auto vc = leg_offsets(c, n[0], n[1], res.V.strides[nr]);
+    scatter_block(E, res.V, E.upload_i64(vr, t1), E.upload_i64(vc, t2), n[c], n[c], ds[dmap[c]].q, n[c],
+                  false);
+    keep.insert(keep.end(), {t1, t2});
+  }
+  return res;
+}
+
+Tensor block_inverse(Engine& E, const Tensor& R) {
+  BlockTables bt = tables_of(R, {0}, {1});
+  Tensor out = E.zeros({R.legs[1], R.legs[0]});
+  std::vector<la::MatDesc> ds;
+  std::vector<Buf> keep;
+  int dmap[2] = {-1, -1};
+  for (int c = 0; c < 2; ++c) {
+    int m = (int)bt.rt[c].size(), n = (int)bt.ct[c].size();
+    if (m != n) throw Error(SPS_ERR_ARGUMENT, "block_inverse: non-square block");
+    if (n == 0) continue;
+    Buf ba = E.alloc(sizeof(double) * (size_t)n * n * 2);
+    double* a = (double*)ba->ptr;
+    double* q = a + (size_t)n * n;
+    Buf t1, t2;
+    gather_block(E, R, E.upload_i64(bt.rt[c], t1), E.upload_i64(bt.ct[c], t2), n, n, a, n, false);
+    dmap[c] = (int)ds.size();
+    ds.push_back({a, q, nullptr, nullptr, n, n, n, n, 0});
+    keep.insert(keep.end(), {ba, t1, t2});
+  }
+  la::inv_batched(E, ds);
+  for (int c = 0; c < 2; ++c) {
+    if (dmap[c] < 0) continue;
+    int n = ds[dmap[c]].n;
+    Buf t1, t2;
+    auto rr = tensor_rows(out, 0, 1, c);
+    auto cc = tensor_rows(out, 1, 1, c);
+    scatter_block(E, out, E.upload_i64(rr, t1), E.upload_i64(cc, t2), n, n, ds[dmap[c]].q, n, false);
+    keep.insert(keep.end(), {t1, t2});
+  }
+  return out;
+}
+
+}  // namespace sps

@@ -1,0 +1,295 @@
+"""``run_purification`` / ``run_stochastic`` over the device engine.
+
+Restates the control flow of ``src/driver/run.jl:2-66,76-134``,
+``src/driver/particles.jl:27-119`` and ``src/statistics/ensemble.jl``: the
+same temperature grid, step schedule, particle weights, ensemble statistics
+and result record (schema 2.7.0 field names).  Born draws take their
+uniforms from ``sample_uniforms(seed, index, n)``, the explicit replacement
+of the reference's ``sample_rng(seed, index)`` stream.  File output (JLD2,
+run.log) and annealed resampling are not part of this engine: a run whose
+ensemble would trigger resampling stops with an error.
+"""
+from __future__ import annotations
+
+import math
+import time
+from dataclasses import dataclass, field
+
+import numpy as np
+
+from .config import (RunConfig, validate_config, temperature_nodes, measure_at, same_beta, parameter_dict)
+from . import engine as eng
+
+RESULT_SCHEMA_VERSION = "2.7.0"
+
+
+def sample_uniforms(seed: int, index: int, n: int) -> np.ndarray:
+    """The n uniforms of Born draw ``index`` (1-based) of run ``seed``."""
+    if seed < 0 or index < 1:
+        raise ValueError("invalid random stream identity")
+    return np.random.default_rng([int(seed), int(index)]).random(n)
+
+
+def step_schedule(start, target, delta_tau):
+    """``_step_schedule`` (``particles.jl:55-64``)."""
+    steps = []
+    b = float(start)
+    while not same_beta(b, target):
+        if not target > b:
+            raise ValueError("evolution requires increasing beta endpoints")
+        b = min(target, b + 2 * delta_tau)
+        if same_beta(b, target):
+            b = float(target)
+        steps.append(b)
+    return steps
+
+
+def ensemble_statistics(relative, multiplicity, energy, Ns, log_scale=0.0, nsites=1):
+    """``ensemble_statistics`` (``src/statistics/ensemble.jl:8-25``)."""
+    relative = np.asarray(relative, float)
+    multiplicity = np.asarray(multiplicity, float)
+    energy = np.asarray(energy, float)
+    if not (len(relative) == len(multiplicity) == len(energy) > 0):
+        raise ValueError("empty or inconsistent ensemble")
+    if not (np.all(np.isfinite(relative)) and np.all(multiplicity > 0)):
+        raise ValueError("invalid particle weights/counts")
+    Nv = multiplicity.sum()
+    pivot = relative.max()
+    w = np.exp(relative - pivot)
+    mass = multiplicity * w
+    total = mass.sum()
+    mu1 = total / Nv
+    mu2 = float(np.sum(multiplicity * w ** 2) / Nv)
+    eta = min(max(mu1 ** 2 / mu2, 1 / Nv), 1.0)
+
+    def sem(f):
+        return math.nan if Nv <= 1 else math.sqrt(max(0.0, float(np.sum(multiplicity * f ** 2)) / (Nv * (Nv - 1))))
+
+    measured = bool(np.all(np.isfinite(energy)))
+    E = float(np.sum(mass * energy) / total) if measured else math.nan
+    Eerr = sem(w * (energy - E) / mu1) if measured else math.nan
+    return dict(energy_total=nsites * E, energy_per_site=E, energy_per_site_error=Eerr,
+                lnZ=log_scale + pivot + math.log(mu1), lnZ_error=sem((w - mu1) / mu1), eta=eta,
+                eta_error=sem((2 * mu1 / mu2) * (w - mu1) - (mu1 ** 2 / mu2 ** 2) * (w ** 2 - mu2)),
+                ESS=Nv * eta,
+                eta_p=min(max(total ** 2 / (Ns * float(np.sum(mass ** 2))), 1 / Ns), len(relative) / Ns),
+                target_samples=Ns, virtual_samples=Nv, representatives=len(relative))
+
+
+def group_configurations(configurations):
+    """``_group_configurations`` (``src/resample/selection.jl:122-140``), 1-based draws."""
+    first, mult, d2g = [], [], []
+    lookup = {}
+    for d, x in enumerate(configurations, start=1):
+        key = tuple(np.asarray(x).reshape(-1).tolist())
+        j = lookup.get(key)
+        if j is None:
+            first.append(d)
+            mult.append(0)
+            j = len(first)
+            lookup[key] = j
+        mult[j - 1] += 1
+        d2g.append(j)
+    return dict(first_draw=first, multiplicity=mult, draw_to_group=d2g)
+
+
+@dataclass
+class ThermalCheckpoint:
+    """Thermal PEPO at beta0 plus preparation records (``src/io/run_output.jl:4-11``)."""
+    state: eng.DeviceState
+    preparation: dict
+    purification: list
+    history: list
+    run_id: str
+
+
+@dataclass
+class Particle:
+    """A Born sample with its normalisation and estimator weight (``particles.jl:2-25``)."""
+    id: int
+    count: int
+    configuration: np.ndarray
+    state: eng.DeviceState
+    log_p0: float
+    log_q_proposal: float
+    relative_log_weight: float
+    weight_log_scale: float
+    physical_log_norm: float
+    tensor_log_norm: float
+    energy_total: float
+    energy_per_site: float
+    magnetization: float
+    max_state_truncation: float = 0.0
+    max_environment_truncation: float = 0.0
+    max_boundary_entropy: float = math.nan
+    time_seconds: float = 0.0
+    measurement_seconds: float = 0.0
+    generation: int = 0
+    sample_index: int = 0
+    seed: int = 0
+
+
+def _observe(state, c: RunConfig, energy: bool):
+    """``_observe`` (``particles.jl:35-40``)."""
+    t = time.perf_counter()
+    if energy:
+        m = eng.measure_energy(state, c.boundary("measurement"))
+    else:
+        m = eng.lognorm(state, c.boundary("measurement"))
+        m.update(energy_total=math.nan, energy_per_site=math.nan, magnetization=math.nan)
+    m["measurement_seconds"] = time.perf_counter() - t
+    return m
+
+
+def _evolve(state, c: RunConfig, steps, D, space, on_step=None):
+    """``_evolve!`` (``particles.jl:66-85``)."""
+    total = maxstate = maxenv = normalization = 0.0
+    maxent = 0.0 if (c.record_boundary_entropy and steps) else math.nan
+    for beta in steps:
+        t = time.perf_counter()
+        r = eng.evolution_step(state, (beta - state.beta) / 2, D, c.boundary("environment"), space)
+        elapsed = time.perf_counter() - t
+        state.beta = beta
+        normalization += r["log_normalization_sum"]
+        total += elapsed
+        maxstate = max(maxstate, r["max_state_truncation"])
+        maxenv = max(maxenv, r["max_environment_truncation"])
+        maxent = max(maxent, r["max_boundary_entropy"])
+        if on_step:
+            on_step(dict(r, beta=beta, time_seconds=elapsed))
+    return dict(time_seconds=total, max_state_truncation=maxstate, max_environment_truncation=maxenv,
+                max_boundary_entropy=maxent, normalization=normalization)
+
+
+def run_purification(c: RunConfig, engine: eng.Engine | None = None) -> ThermalCheckpoint:
+    """Prepare the beta0 thermal PEPO (``run.jl:2-43``)."""
+    validate_config(c)
+    e = engine or eng.Engine.from_config(c)
+    state = e.identity_pepo()
+    initial = eng.normalize_state(state)
+    history = [dict(phase="initialization", beta=0.0, normalizations=initial.tolist())]
+    rows = []
+    for beta in [b for b in temperature_nodes(c) if b <= c.beta0]:
+        steps = step_schedule(state.beta, beta, c.delta_tau_pur)
+        rep = _evolve(state, c, steps, c.D_pur, c.bond_space_pur, on_step=history.append)
+        m = _observe(state, c, measure_at(c, beta))
+        rows.append(dict(beta=beta, source="purification", energy_total=m["energy_total"],
+                         energy_per_site=m["energy_per_site"],
+                         energy_per_site_error=0.0 if measure_at(c, beta) else math.nan,
+                         lnZ=m["log_norm"], lnZ_error=0.0, eta=math.nan, eta_error=math.nan,
+                         magnetization=m["magnetization"],
+                         max_state_truncation=rep["max_state_truncation"],
+                         max_environment_truncation=max(rep["max_environment_truncation"],
+                                                        m["max_environment_truncation"]),
+                         max_boundary_entropy=rep["max_boundary_entropy"],
+                         time_seconds=rep["time_seconds"], measurement_seconds=m["measurement_seconds"]))
+    return ThermalCheckpoint(state, parameter_dict(c), rows, history, f"run-{time.time_ns()}")
+
+
+def _particle_record(p: Particle):
+    """``_particle_scalar`` (``particles.jl:103-115``)."""
+    return dict(id=p.id, generation=p.generation, sample_index=p.sample_index, seed=p.seed, count=p.count,
+                configuration=p.configuration.copy(), owner=0, beta=p.state.beta, log_p0=p.log_p0,
+                log_q_proposal=p.log_q_proposal, relative_log_weight=p.relative_log_weight,
+                weight_log_scale=p.weight_log_scale, log_weight=p.weight_log_scale + p.relative_log_weight,
+                physical_log_norm=p.physical_log_norm, log_amplitude=p.state.log_amplitude,
+                energy_total=p.energy_total, energy_per_site=p.energy_per_site, magnetization=p.magnetization,
+                max_state_truncation=p.max_state_truncation,
+                max_environment_truncation=p.max_environment_truncation,
+                max_boundary_entropy=p.max_boundary_entropy, time_seconds=p.time_seconds,
+                measurement_seconds=p.measurement_seconds)
+
+
+def _statistics(records, Ns, nsites):
+    """``_statistics`` (``ensemble.jl:31-40``)."""
+    scale = max(r["weight_log_scale"] for r in records)
+    rel = [r["relative_log_weight"] + (r["weight_log_scale"] - scale) for r in records]
+    s = ensemble_statistics(rel, [r["count"] for r in records], [r["energy_per_site"] for r in records], Ns,
+                            log_scale=scale, nsites=nsites)
+    s.update(beta=records[0]["beta"],
+             max_state_truncation=max(r["max_state_truncation"] for r in records),
+             max_environment_truncation=max(r["max_environment_truncation"] for r in records),
+             max_boundary_entropy=max(r["max_boundary_entropy"] for r in records),
+             distinct_configurations=len({tuple(np.asarray(r["configuration"]).reshape(-1)) for r in records}))
+    mags = [r["magnetization"] for r in records]
+    if all(math.isfinite(x) for x in mags):
+        w = np.exp(np.asarray(rel) - max(rel)) * np.asarray([r["count"] for r in records])
+        s["magnetization"] = float(np.sum(w * np.asarray(mags)) / np.sum(w))
+    else:
+        s["magnetization"] = math.nan
+    return s
+
+
+def run_stochastic(c: RunConfig, checkpoint: ThermalCheckpoint, uniforms_fn=None):
+    """Draw Born samples from the beta0 checkpoint and evolve the weighted ensemble (``run.jl:76-134``).
+
+    Returns the result record: ``observables`` (curve, purification, samples),
+    ``diagnostics`` (born draws and grouping), ``metadata`` and ``parameters``.
+    """
+    validate_config(c)
+    if not (same_beta(checkpoint.state.beta, c.beta0)):
+        raise ValueError("checkpoint model, lattice or beta0 mismatch")
+    L = c.lattice.Lx * c.lattice.Ly
+    if uniforms_fn is None:
+        uniforms_fn = lambda i: sample_uniforms(c.seed, i, L)
+    cache = eng.SamplingCache(checkpoint.state, c.boundary("sampling"))
+    draws = []
+    for i in range(1, c.Ns + 1):
+        d = eng.sample_configuration(cache, uniforms=uniforms_fn(i))
+        d["index"] = i
+        draws.append(d)
+    del cache
+    grouping = group_configurations([d["configuration"] for d in draws])
+    particles = []
+    for u, i in enumerate(grouping["first_draw"]):
+        d = draws[i - 1]
+        state, _ = eng.project_configuration(checkpoint.state, d["configuration"])
+        m = _observe(state, c, measure_at(c, c.beta0))
+        particles.append(Particle(id=i, count=grouping["multiplicity"][u], configuration=d["configuration"],
+                                  state=state, log_p0=d["log_probability"], log_q_proposal=d["log_probability"],
+                                  relative_log_weight=m["log_norm"] - d["log_probability"],
+                                  weight_log_scale=0.0, physical_log_norm=m["log_norm"],
+                                  tensor_log_norm=m["tensor_log_norm"], energy_total=m["energy_total"],
+                                  energy_per_site=m["energy_per_site"], magnetization=m["magnetization"],
+                                  max_environment_truncation=max(d["max_environment_truncation"],
+                                                                 m["max_environment_truncation"]),
+                                  measurement_seconds=m["measurement_seconds"], sample_index=i, seed=c.seed))
+    curve = [r for r in checkpoint.purification if r["beta"] < c.beta0 and not same_beta(r["beta"], c.beta0)]
+    samples = []
+    nodes = [b for b in temperature_nodes(c) if b >= c.beta0]
+    for node, beta in enumerate(nodes):
+        if node > 0:
+            steps = step_schedule(nodes[node - 1], beta, c.delta_tau_peps)
+            for p in particles:
+                old = p.tensor_log_norm
+                rep = _evolve(p.state, c, steps, c.D_peps, c.bond_space_peps)
+                m = _observe(p.state, c, measure_at(c, beta))
+                p.relative_log_weight += 2 * rep["normalization"] + (m["tensor_log_norm"] - old)
+                p.physical_log_norm = m["log_norm"]
+                p.tensor_log_norm = m["tensor_log_norm"]
+                p.energy_total = m["energy_total"]
+                p.energy_per_site = m["energy_per_site"]
+                p.magnetization = m["magnetization"]
+                p.max_state_truncation = rep["max_state_truncation"]
+                p.max_environment_truncation = max(rep["max_environment_truncation"],
+                                                   m["max_environment_truncation"])
+                p.max_boundary_entropy = rep["max_boundary_entropy"]
+                p.time_seconds = rep["time_seconds"]
+                p.measurement_seconds = m["measurement_seconds"]
+        records = [_particle_record(p) for p in particles]
+        stats = _statistics(records, c.Ns, L)
+        stats.update(source="sampling", time_seconds=sum(p.time_seconds for p in particles))
+        if c.resampling.enabled and stats["eta"] < c.resampling.eta_th:
+            raise NotImplementedError("annealed Born resampling is not part of this engine; "
+                                      "run with resampling=ResamplingOptions(enabled=False)")
+        curve.append(stats)
+        samples.extend(records)
+    return {"schema_version": RESULT_SCHEMA_VERSION, "method": "stoPEPS",
+            "parameters": parameter_dict(c), "model": parameter_dict(c)["model"],
+            "observables": {"curve": curve, "purification": list(checkpoint.purification),
+                            "samples": samples, "replay": []},
+            "diagnostics": {"born_draws": draws, "born_grouping": grouping, "events": [],
+                            "history": list(checkpoint.history)},
+            "metadata": {"run_id": checkpoint.run_id, "stage": "stochastic", "complete": True,
+                         "mpi_size": 1, "restart_supported": False,
+                         "uncertainty": "conditional_particle_delta_method; shared_history_scale_fixed"}}

@@ -1,0 +1,284 @@
+"""Device-resident states and the hot-path calls, through the C ABI.
+
+Each function here keeps the name, argument meaning and error behaviour of
+the reference function it stands for (``lognorm``, ``measure_energy``,
+``evolution_step!``, ``SamplingCache``, ``sample_configuration``,
+``project_configuration``, ``normalize_state!``, ``identity_pepo``).  The
+work runs in ``libstopeps_gpu.so``; there is no host fallback.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import math
+
+import numpy as np
+
+from . import _lib
+from .config import BoundaryMPS, RunConfig, TFIM, FullUpdate, Z2Space
+
+
+def _arr(a, ctype):
+    return a.ctypes.data_as(C.POINTER(ctype))
+
+
+def _boundary(m: BoundaryMPS):
+    b = _lib.sps_boundary()
+    b.chi = int(m.chi)
+    if m.sector_space is None:
+        b.space0 = b.space1 = -1
+    else:
+        b.space0, b.space1 = int(m.sector_space.n0), int(m.sector_space.n1)
+    return b
+
+
+class Engine:
+    """One device handle for a lattice, model, full-update options and Trotter order."""
+
+    def __init__(self, Lx, Ly, model: TFIM = TFIM(), update: FullUpdate = FullUpdate(), trotter_order=2,
+                 record_boundary_entropy=True, device=0):
+        self.lib = _lib.load()
+        cfg = _lib.sps_config()
+        cfg.Lx, cfg.Ly = int(Lx), int(Ly)
+        cfg.J, cfg.h = float(model.J), float(model.h)
+        cfg.trotter_order = int(trotter_order)
+        cfg.fu_max_iterations = int(update.max_iterations)
+        cfg.fu_error_tolerance = float(update.error_tolerance)
+        cfg.fu_diagonal_shift = float(update.diagonal_shift)
+        cfg.fu_linear_max_iterations = int(update.linear_max_iterations)
+        cfg.fu_linear_tolerance = float(update.linear_tolerance)
+        cfg.record_boundary_entropy = 1 if record_boundary_entropy else 0
+        cfg.device = int(device)
+        h = C.c_void_p()
+        code = self.lib.sps_create(C.byref(cfg), C.byref(h))
+        if code != 0:
+            raise _lib.EngineError(code, "sps_create failed (is a CUDA device visible?)")
+        self.h = h
+        self.Lx, self.Ly = int(Lx), int(Ly)
+        self.model = model
+        self.update = update
+
+    @classmethod
+    def from_config(cls, c: RunConfig, device=0):
+        return cls(c.lattice.Lx, c.lattice.Ly, c.model, c.update, c.trotter_order, c.record_boundary_entropy,
+                   device)
+
+    def check(self, code):
+        if code != 0:
+            buf = C.create_string_buffer(4096)
+            self.lib.sps_last_error(self.h, buf, 4096)
+            raise _lib.EngineError(code, buf.value.decode(errors="replace"))
+
+    def counters(self):
+        n = C.c_longlong()
+        f = C.c_double()
+        self.check(self.lib.sps_counters(self.h, C.byref(n), C.byref(f)))
+        return n.value, f.value
+
+    def close(self):
+        if getattr(self, "h", None):
+            self.lib.sps_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    # --- states -----------------------------------------------------------
+    def identity_pepo(self) -> "DeviceState":
+        sid = C.c_int32()
+        self.check(self.lib.sps_identity_pepo(self.h, C.byref(sid)))
+        return DeviceState(self, sid.value)
+
+    def upload_state(self, sites, leg_dims, is_pepo, beta=0.0, log_amplitude=0.0) -> "DeviceState":
+        """Upload site tensors (x + y*Lx order) with per-leg (n0,n1) multiplicities."""
+        dims = np.ascontiguousarray(np.asarray(leg_dims, np.int32).reshape(-1))
+        data = np.ascontiguousarray(np.concatenate([np.asarray(s, np.float64).reshape(-1) for s in sites]))
+        sid = C.c_int32()
+        self.check(self.lib.sps_state_upload(self.h, 1 if is_pepo else 0, float(beta), float(log_amplitude),
+                                             _arr(dims, C.c_int32), _arr(data, C.c_double), C.byref(sid)))
+        return DeviceState(self, sid.value)
+
+
+class DeviceState:
+    """``FiniteState`` held on the device (``src/states/finite.jl:27-49``)."""
+
+    def __init__(self, engine: Engine, sid: int):
+        self.engine = engine
+        self.id = sid
+
+    def _info(self):
+        b, la, p = C.c_double(), C.c_double(), C.c_int32()
+        self.engine.check(self.engine.lib.sps_state_info(self.engine.h, self.id, C.byref(b), C.byref(la),
+                                                         C.byref(p)))
+        return b.value, la.value, bool(p.value)
+
+    @property
+    def beta(self):
+        return self._info()[0]
+
+    @beta.setter
+    def beta(self, v):
+        self.engine.check(self.engine.lib.sps_state_set_beta(self.engine.h, self.id, float(v)))
+
+    @property
+    def log_amplitude(self):
+        return self._info()[1]
+
+    @property
+    def is_pepo(self):
+        return self._info()[2]
+
+    @property
+    def lattice(self):
+        return (self.engine.Lx, self.engine.Ly)
+
+    def copy(self) -> "DeviceState":
+        nid = C.c_int32()
+        self.engine.check(self.engine.lib.sps_state_copy(self.engine.h, self.id, C.byref(nid)))
+        return DeviceState(self.engine, nid.value)
+
+    def download(self):
+        """Site tensors (x + y*Lx order) and their leg multiplicities."""
+        L = self.engine.Lx * self.engine.Ly
+        dims = np.zeros(L * 12, np.int32)
+        tot = C.c_int64()
+        self.engine.check(self.engine.lib.sps_state_layout(self.engine.h, self.id, _arr(dims, C.c_int32),
+                                                           C.byref(tot)))
+        data = np.zeros(tot.value, np.float64)
+        self.engine.check(self.engine.lib.sps_state_download(self.engine.h, self.id, _arr(data, C.c_double),
+                                                             tot.value))
+        dims = dims.reshape(L, 6, 2)
+        sites, off = [], 0
+        for i in range(L):
+            shape = [int(a + b) for a, b in dims[i]]
+            n = int(np.prod(shape))
+            sites.append(data[off:off + n].reshape(shape))
+            off += n
+        return sites, dims
+
+    def __del__(self):
+        try:
+            if self.engine.h:
+                self.engine.lib.sps_state_free(self.engine.h, self.id)
+        except Exception:
+            pass
+
+
+def normalize_state(state: DeviceState):
+    """``normalize_state!``: per-site log normalisations in row-major order."""
+    L = state.engine.Lx * state.engine.Ly
+    out = np.zeros(L)
+    state.engine.check(state.engine.lib.sps_normalize_state(state.engine.h, state.id, _arr(out, C.c_double)))
+    return out
+
+
+def evolution_step(state: DeviceState, delta, D, contraction: BoundaryMPS, sector_space: Z2Space | None = None):
+    """``evolution_step!(state, model, delta, D, FullUpdate, contraction)``."""
+    e = state.engine
+    rep = _lib.sps_step_report()
+    b = _boundary(contraction)
+    if sector_space is None:
+        e.check(e.lib.sps_evolution_step(e.h, state.id, float(delta), int(D), None, C.byref(b), C.byref(rep)))
+    else:
+        sp = (C.c_int32 * 2)(sector_space.n0, sector_space.n1)
+        e.check(e.lib.sps_evolution_step(e.h, state.id, float(delta), int(D), sp, C.byref(b), C.byref(rep)))
+    return {f: getattr(rep, f) for f, _ in rep._fields_}
+
+
+def lognorm(state: DeviceState, contraction: BoundaryMPS):
+    e = state.engine
+    r = _lib.sps_lognorm_result()
+    b = _boundary(contraction)
+    e.check(e.lib.sps_lognorm(e.h, state.id, C.byref(b), C.byref(r)))
+    return dict(log_norm=r.log_norm, tensor_log_norm=r.tensor_log_norm,
+                max_environment_truncation=r.max_environment_truncation)
+
+
+def measure_energy(state: DeviceState, contraction: BoundaryMPS, site_profile=False):
+    """``measure_energy``; also returns ``magnetization`` = <sum_i X_i>/N."""
+    e = state.engine
+    r = _lib.sps_energy()
+    b = _boundary(contraction)
+    L = e.Lx * e.Ly
+    sx = np.zeros(L)
+    nb = max(0, (e.Ly - 1) * (e.Lx - 1))
+    sn = np.zeros(max(nb, 1))
+    ss = np.zeros(max(nb, 1))
+    e.check(e.lib.sps_measure_energy(e.h, state.id, C.byref(b), C.byref(r), _arr(sx, C.c_double),
+                                     _arr(sn, C.c_double), _arr(ss, C.c_double)))
+    out = dict(energy_total=r.energy_total, energy_per_site=r.energy_per_site, log_norm=r.log_norm,
+               tensor_log_norm=r.tensor_log_norm, max_environment_truncation=r.max_environment_truncation,
+               x_sum=r.x_sum, zz_sum=r.zz_sum, magnetization=r.x_sum / L)
+    if site_profile:
+        out["site_x"] = sx.reshape(e.Ly, e.Lx).T.copy()
+        out["Se"] = {"north": sn[:nb].reshape(e.Ly - 1, e.Lx - 1) if nb else np.zeros((0, 0)),
+                     "south": ss[:nb].reshape(e.Ly - 1, e.Lx - 1) if nb else np.zeros((0, 0))}
+    return out
+
+
+class SamplingCache:
+    """``SamplingCache(state, contraction; kind=:auxiliary)`` on the device."""
+
+    def __init__(self, state: DeviceState, contraction: BoundaryMPS):
+        self.engine = state.engine
+        cid = C.c_int32()
+        b = _boundary(contraction)
+        self.engine.check(self.engine.lib.sps_sampling_cache(self.engine.h, state.id, C.byref(b), C.byref(cid)))
+        self.id = cid.value
+
+    def __del__(self):
+        try:
+            if self.engine.h:
+                self.engine.lib.sps_sampling_cache_free(self.engine.h, self.id)
+        except Exception:
+            pass
+
+
+def sample_configuration(cache: SamplingCache, uniforms=None, configuration=None):
+    """``sample_configuration(cache; rng | configuration)`` with explicit uniforms.
+
+    ``configuration`` / the returned configuration is an (Lx, Ly) int array of
+    SymmetryBasis labels (1 even, 2 odd).
+    """
+    e = cache.engine
+    L = e.Lx * e.Ly
+    rep = _lib.sps_sample_report()
+    if configuration is not None:
+        cfg = np.ascontiguousarray(np.asarray(configuration, np.int32).T.reshape(-1))
+        e.check(e.lib.sps_sample_probability(e.h, cache.id, _arr(cfg, C.c_int32), C.byref(rep)))
+        return dict(configuration=np.asarray(configuration), log_probability=rep.log_probability,
+                    max_environment_truncation=rep.max_environment_truncation)
+    if uniforms is None:
+        raise ValueError("an explicit RNG is required")
+    u = np.ascontiguousarray(np.asarray(uniforms, np.float64).reshape(-1))
+    if u.size != L:
+        raise ValueError("one uniform per site is required")
+    out = np.zeros(L, np.int32)
+    e.check(e.lib.sps_sample(e.h, cache.id, _arr(u, C.c_double), _arr(out, C.c_int32), C.byref(rep)))
+    return dict(configuration=out.reshape(e.Ly, e.Lx).T.copy(), log_probability=rep.log_probability,
+                max_environment_truncation=rep.max_environment_truncation, near_boundary=rep.near_boundary)
+
+
+def sample_batch(cache: SamplingCache, uniforms):
+    """Many draws in one call: uniforms (n, Lx*Ly) -> configurations (n, Lx, Ly), log_p (n,)."""
+    e = cache.engine
+    L = e.Lx * e.Ly
+    u = np.ascontiguousarray(np.asarray(uniforms, np.float64).reshape(-1, L))
+    n = u.shape[0]
+    cfg = np.zeros((n, L), np.int32)
+    lp = np.zeros(n)
+    e.check(e.lib.sps_sample_batch(e.h, cache.id, n, _arr(u, C.c_double), _arr(cfg, C.c_int32),
+                                   _arr(lp, C.c_double)))
+    return cfg.reshape(n, e.Ly, e.Lx).transpose(0, 2, 1).copy(), lp
+
+
+def project_configuration(pepo: DeviceState, configuration):
+    """``project_configuration(checkpoint, configuration)`` -> (PEPS state, log normalisations)."""
+    e = pepo.engine
+    cfg = np.ascontiguousarray(np.asarray(configuration, np.int32).T.reshape(-1))
+    sid = C.c_int32()
+    ln = np.zeros(e.Lx * e.Ly)
+    e.check(e.lib.sps_project(e.h, pepo.id, _arr(cfg, C.c_int32), C.byref(sid), _arr(ln, C.c_double)))
+    return DeviceState(e, sid.value), ln
