@@ -1,0 +1,86 @@
+"""Host logic of the engine package (no GPU): configuration, schedules,
+statistics and the C-ABI library's exported symbols."""
+import ctypes
+import math
+import os
+import re
+
+import numpy as np
+import pytest
+
+from oracle import driver as odr
+
+ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+
+
+def test_validate_config_defaults_and_errors(sps):
+    c = sps.RunConfig()
+    assert sps.validate_config(c) is c
+    assert c.chi_sampling == c.chi_environment == c.chi_measurement == 32
+    with pytest.raises(ValueError):
+        sps.validate_config(sps.RunConfig(delta_tau_pur=0.0))
+    with pytest.raises(ValueError):
+        sps.validate_config(sps.RunConfig(Ns=1))          # resampling needs Ns >= 2
+    with pytest.raises(ValueError):
+        sps.validate_config(sps.RunConfig(trotter_order=3))
+    with pytest.raises(ValueError):
+        sps.TFIM(physical_space=sps.Z2Space(2, 2))
+
+
+def test_temperature_nodes_and_schedule_match_oracle(sps):
+    c = sps.RunConfig(beta0=0.5, beta_log=[1.0, 2.0, 3.0, 4.0], beta_measure=[0.5, 1.0, 2.0, 3.0, 4.0])
+    oc = odr.RunConfig(beta0=0.5, beta_log=[1.0, 2.0, 3.0, 4.0], beta_measure=[0.5, 1.0, 2.0, 3.0, 4.0])
+    assert sps.temperature_nodes(c) == odr.temperature_nodes(oc) == [0.0, 0.5, 1.0, 2.0, 3.0, 4.0]
+    s = sps.step_schedule(0.5, 1.0, 0.05)
+    assert s == odr.step_schedule(0.5, 1.0, 0.05)
+    assert len(s) == 5 and s[-1] == 1.0
+    assert sps.step_schedule(0.0, 0.07, 0.025) == [0.05, 0.07]
+    with pytest.raises(ValueError):
+        sps.step_schedule(1.0, 0.5, 0.05)
+
+
+def test_ensemble_statistics_matches_oracle(sps):
+    rng = np.random.default_rng(0)
+    rel = rng.normal(size=9)
+    mult = rng.integers(1, 4, size=9)
+    en = rng.normal(size=9)
+    a = sps.ensemble_statistics(rel, mult, en, 12, log_scale=0.3, nsites=16)
+    b = odr.ensemble_statistics(rel, mult, en, 12, log_scale=0.3, nsites=16)
+    for k in b:
+        assert (math.isnan(a[k]) and math.isnan(b[k])) or abs(a[k] - b[k]) < 1e-14, k
+    with pytest.raises(ValueError):
+        sps.ensemble_statistics([], [], [], 1)
+    with pytest.raises(ValueError):
+        sps.ensemble_statistics([np.inf], [1], [0.0], 1)
+
+
+def test_group_configurations(sps):
+    cfgs = [np.array([[1, 2], [1, 1]]), np.array([[1, 1], [1, 1]]), np.array([[1, 2], [1, 1]])]
+    g = sps.group_configurations(cfgs)
+    assert g == dict(first_draw=[1, 2], multiplicity=[2, 1], draw_to_group=[1, 2, 1])
+
+
+def test_sample_uniforms_are_reproducible(sps):
+    a = sps.sample_uniforms(7, 3, 16)
+    assert np.array_equal(a, sps.sample_uniforms(7, 3, 16))
+    assert np.array_equal(a, odr.sample_uniforms(7, 3, 16))
+    assert not np.array_equal(a, sps.sample_uniforms(7, 4, 16))
+    with pytest.raises(ValueError):
+        sps.sample_uniforms(-1, 1, 4)
+
+
+def test_library_exports_every_declared_symbol(sps):
+    header = open(os.path.join(ROOT, "include", "stopeps_gpu.h")).read()
+    declared = set(re.findall(r"\b(sps_[a-z_0-9]+)\s*\(", header))
+    lib = ctypes.CDLL(sps.LIBRARY_PATH)
+    missing = [n for n in sorted(declared) if not hasattr(lib, n)]
+    assert not missing, missing
+    assert declared >= set(sps._lib.EXPORTS)
+
+
+def test_create_without_device_fails_loudly(sps):
+    import torch
+    if torch.cuda.is_available():
+        pytest.skip("a CUDA device is present")
+    with pytest.raises(sps._lib.EngineError):
+        sps.Engine(2, 2)

@@ -1,0 +1,117 @@
+"""The CPU oracle pinned against exact diagonalization and structural invariants.
+
+The reference ships no golden vectors (its only test checks RunConfig
+validation), so exact diagonalization (``src/models/tfim.jl:72-76``,
+restated in ``oracle/model.py``) and the identities below are the pins.
+"""
+import itertools
+import math
+
+import numpy as np
+import pytest
+
+from oracle import driver as dr, model as md, sampling as sp, boundary as bm, full_update as fu
+from util import golden
+
+
+def _cfg(**kw):
+    base = dict(Lx=2, Ly=2, J=1.0, h=0.7, beta0=0.2, beta_log=[0.1, 0.2], beta_measure=[0.0, 0.2],
+                delta_tau_pur=0.025, delta_tau_peps=0.025, D_pur=4, D_peps=4, chi_environment=16, Ns=4, seed=1)
+    base.update(kw)
+    return dr.RunConfig(**base)
+
+
+def test_identity_pepo_norm_is_hilbert_dimension():
+    st = md.identity_pepo(3, 2)
+    md.normalize_state(st)
+    ln = bm.lognorm(st, bm.BoundaryMPS(4))
+    assert abs(ln["log_norm"] - 6 * math.log(2)) < 1e-13
+    assert abs(sp.measure_energy(st, md.TFIM(1.0, 0.7), bm.BoundaryMPS(4))["energy_per_site"]) < 1e-14
+
+
+@pytest.mark.parametrize("h", [0.7, 3.0])
+def test_purification_matches_exact_diagonalization(h):
+    c = _cfg(h=h)
+    st, rows = dr.run_purification(c)
+    for r in rows:
+        ex = md.exact_thermal_observables(2, 2, md.TFIM(1.0, h), r["beta"])
+        tol = 2e-5 * max(1.0, h * h)   # second-order Trotter error at delta_tau = 0.025
+        assert abs(r["lnZ"] - ex["lnZ"]) < tol
+        if not math.isnan(r["energy_per_site"]):
+            assert abs(r["energy_per_site"] - ex["energy_per_site"]) < tol
+            mx = md.exact_thermal_magnetization(2, 2, md.TFIM(1.0, h), r["beta"])
+            assert abs(r["magnetization"] - mx) < tol
+
+
+def test_born_probabilities_sum_to_one_and_weights_give_Z():
+    """Exhaustive 2x2: sum_k p_k = 1 and sum_k ||psi_k||^2 = Z(beta0) = ||PEPO||^2."""
+    c = _cfg()
+    st, rows = dr.run_purification(c)
+    cache = sp.SamplingCache(st, bm.BoundaryMPS(16))
+    total_p, total_w = 0.0, 0.0
+    for bits in itertools.product([1, 2], repeat=4):
+        cfg = [[bits[0], bits[2]], [bits[1], bits[3]]]
+        d = sp.sample_configuration(cache, configuration=cfg)
+        total_p += math.exp(d["log_probability"])
+        ps, _ = sp.project_configuration(st, cfg)
+        total_w += math.exp(bm.lognorm(ps, bm.BoundaryMPS(16))["log_norm"])
+    assert abs(total_p - 1.0) < 1e-12
+    assert abs(math.log(total_w) - rows[-1]["lnZ"]) < 1e-12
+
+
+def test_exhaustive_ensemble_reproduces_exact_energy():
+    """Weighting every configuration by its evolved norm reproduces the ED energy at beta."""
+    c = _cfg(beta0=0.1, beta_log=[0.1], beta_measure=[0.1])
+    st, _ = dr.run_purification(c)
+    beta = 0.3
+    num = den = 0.0
+    for bits in itertools.product([1, 2], repeat=4):
+        cfg = [[bits[0], bits[2]], [bits[1], bits[3]]]
+        ps, _ = sp.project_configuration(st, cfg)
+        rep = dr.evolve(ps, c, dr.step_schedule(0.1, beta, 0.025), 4, None)
+        m = sp.measure_energy(ps, md.TFIM(1.0, 0.7), bm.BoundaryMPS(16))
+        w = math.exp(m["log_norm"])
+        num += w * m["energy_per_site"]
+        den += w
+    ex = md.exact_thermal_observables(2, 2, md.TFIM(1.0, 0.7), beta)
+    assert abs(num / den - ex["energy_per_site"]) < 5e-5
+
+
+def test_stochastic_estimate_is_consistent_with_exact():
+    c = _cfg(Ns=24, beta_log=[0.2, 0.4], beta_measure=[0.2, 0.4], delta_tau_pur=0.05, delta_tau_peps=0.05)
+    st, _ = dr.run_purification(c)
+    res = dr.run_stochastic(c, st)
+    for r in res["curve"]:
+        ex = md.exact_thermal_observables(2, 2, md.TFIM(1.0, 0.7), r["beta"])
+        assert abs(r["energy_per_site"] - ex["energy_per_site"]) < 4 * r["energy_per_site_error"] + 1e-3
+
+
+def test_categorical_matches_reference_rule():
+    lm = [math.log(0.25), math.log(0.75)]
+    assert sp.categorical(lm, 0.2) == 0
+    assert sp.categorical(lm, 0.3) == 1
+    assert sp.categorical([-math.inf, 0.0], 0.99) == 1
+
+
+def test_truncation_is_an_intersection():
+    from oracle.z2 import select_truncation
+    s = [np.array([10.0, 9, 8, 7]), np.array([1.0, 0.5])]
+    keep = select_truncation(s, chi=5, space=(3, 3))
+    assert keep[0].tolist() == [True, True, True, False] and keep[1].tolist() == [True, False]
+
+
+@pytest.mark.parametrize("name", ["pepo_3x3_D4.npz", "pepo_2x3_D2.npz"])
+def test_golden_fixture_is_reproducible(name):
+    """The committed fixtures are what the oracle computes today."""
+    from util import oracle_state, space
+    g = golden(name)
+    st = oracle_state(g)
+    for k in range(2):
+        a, b, cc = g[f"chi{k}"]
+        m = bm.BoundaryMPS(int(a), space(b, cc))
+        ln = bm.lognorm(st, m)
+        assert abs(ln["log_norm"] - g[f"lognorm{k}"][0]) < 1e-11
+    a, b, cc = g["chi0"]
+    cache = sp.SamplingCache(st, bm.BoundaryMPS(int(a), space(b, cc)))
+    d = sp.sample_configuration(cache, uniforms=g["uniforms"][0])
+    assert np.array_equal(np.asarray(d["configuration"]), g["configs"][0])
