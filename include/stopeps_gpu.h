@@ -102,6 +102,14 @@ int sps_create(const sps_config* cfg, sps_handle** out);
 void sps_destroy(sps_handle* h);
 int sps_last_error(const sps_handle* h, char* buf, size_t n);
 int sps_counters(sps_handle* h, long long* kernel_launches, double* flops);
+/* Measurement support (no reference counterpart): per-kernel CUDA-event
+ * timing on the handle's stream, reported as JSON
+ * {"kernel": {"ms":..,"count":..,"flops":..,"bytes":..}, ...}; and a
+ * device-side stopwatch (events on the handle's stream; stop synchronizes). */
+int sps_set_profile(sps_handle* h, int32_t enable);
+int sps_kernel_stats_json(sps_handle* h, char* buf, size_t n);
+int sps_timer_start(sps_handle* h);
+int sps_timer_stop(sps_handle* h, double* milliseconds);
 
 /* --- states: FiniteState (src/states/finite.jl:27-49) ---------------------
  * Site tensors have legs (W,N,Pout,Paux,E,S); each leg is described by its

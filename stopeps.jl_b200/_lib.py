@@ -18,7 +18,8 @@ EXPORTS = [
     "sps_state_info", "sps_state_set_beta", "sps_state_copy", "sps_state_free",
     "sps_normalize_state", "sps_evolution_step", "sps_lognorm", "sps_measure_energy",
     "sps_sampling_cache", "sps_sampling_cache_free", "sps_sample", "sps_sample_probability",
-    "sps_sample_batch", "sps_project",
+    "sps_sample_batch", "sps_project", "sps_set_profile", "sps_kernel_stats_json", "sps_timer_start",
+    "sps_timer_stop",
 ]
 
 STATUS = {0: "SPS_OK", 1: "SPS_ERR_ARGUMENT", 2: "SPS_ERR_CUDA", 3: "SPS_ERR_NUMERIC",
@@ -100,6 +101,10 @@ def load():
         "sps_sample_probability": ([vp, i32, P(i32), P(sps_sample_report)], C.c_int),
         "sps_sample_batch": ([vp, i32, i32, P(dbl), P(i32), P(dbl)], C.c_int),
         "sps_project": ([vp, i32, P(i32), P(i32), P(dbl)], C.c_int),
+        "sps_set_profile": ([vp, i32], C.c_int),
+        "sps_kernel_stats_json": ([vp, C.c_char_p, C.c_size_t], C.c_int),
+        "sps_timer_start": ([vp], C.c_int),
+        "sps_timer_stop": ([vp, P(dbl)], C.c_int),
     }
     for name, (args, res) in sig.items():
         f = getattr(lib, name)

@@ -1,0 +1,596 @@
+// Multi-CTA factorizations for the large parity blocks of the boundary
+// compression (e.g. 23328 x 648 and 648 x 648 at chi=36, D=6):
+//
+//  * blocked Householder QR: a cooperative panel kernel (one pass over the
+//    panel rows per column, two grid barriers per column) and compact-WY
+//    trailing updates / Q formation as dense FP64 GEMMs with split-K;
+//  * one-sided Jacobi SVD with every column pair of a round rotated by its
+//    own warp across the whole GPU and a grid barrier between rounds.
+//
+// Grid barriers are software barriers inside cooperative launches (all CTAs
+// co-resident); every spin is bounded and reports through the device flag.
+#include "engine.h"
+#include <cfloat>
+#include <cstring>
+#include <algorithm>
+#include <initializer_list>
+
+namespace sps {
+namespace la {
+
+static constexpr int BT = 256;
+static constexpr int BW = BT / 32;
+static constexpr int FLAG_BARRIER = 4;
+static constexpr int FLAG_CONV = 2;
+
+__device__ __forceinline__ double wsum(double v) {
+  for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+  return v;
+}
+
+__device__ double bsum(double v, double* red) {
+  v = wsum(v);
+  __syncthreads();
+  if ((threadIdx.x & 31) == 0) red[threadIdx.x >> 5] = v;
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    double s = 0;
+    for (int w = 0; w < BW; ++w) s += red[w];
+    red[BW] = s;
+  }
+  __syncthreads();
+  return red[BW];
+}
+
+// bar[0] = arrival count, bar[1] = generation.  Bounded spin (~seconds).
+__device__ void grid_barrier(unsigned* bar, int* flag) {
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    volatile unsigned* gen = bar + 1;
+    unsigned g = *gen;
+    __threadfence();
+    unsigned arrived = atomicAdd(bar, 1u);
+    if (arrived == gridDim.x - 1) {
+      atomicExch(bar, 0u);
+      __threadfence();
+      atomicAdd(bar + 1, 1u);
+    } else {
+      long long spins = 0;
+      while (*gen == g) {
+        if (++spins > (1ll << 26)) {
+          atomicOr(flag, FLAG_BARRIER);
+          break;
+        }
+        __nanosleep(40);
+      }
+    }
+    __threadfence();
+  }
+  __syncthreads();
+}
+
+// ---------------------------------------------------------------------------
+// dense column-major GEMM: C = alpha op(A) B + beta C, split-K into partials
+// ---------------------------------------------------------------------------
+static constexpr int GM = 64, GN = 64, GK = 16;
+
+template <bool TA>
+__global__ void __launch_bounds__(BT) dgemm_cm_kernel(int M, int N, int K, const double* __restrict__ A, int lda,
+                                                      const double* __restrict__ B, int ldb, double* __restrict__ C,
+                                                      int ldc, double alpha, double beta, int kchunk,
+                                                      double* __restrict__ partial) {
+  const int i0 = blockIdx.y * GM, j0 = blockIdx.x * GN;
+  const int kbeg = blockIdx.z * kchunk, kend = min(K, kbeg + kchunk);
+  __shared__ double As[GK][GM + 1];
+  __shared__ double Bs[GK][GN + 1];
+  const int t = threadIdx.x, tx = t % 16, ty = t / 16;
+  double acc[4][4] = {};
+  for (int k0 = kbeg; k0 < kend; k0 += GK) {
+    if (TA) {   // op(A)(i,k) = A[k + i*lda]: k contiguous
+      int kk = t % 16;
+#pragma unroll
+      for (int r = 0; r < 4; ++r) {
+        int ii = t / 16 + 16 * r;
+        int i = i0 + ii, k = k0 + kk;
+        As[kk][ii] = (i < M && k < kend) ? A[k + (size_t)i * lda] : 0.0;
+      }
+    } else {    // A[i + k*lda]: i contiguous
+      int ii = t % 64;
+#pragma unroll
+      for (int r = 0; r < 4; ++r) {
+        int kk = t / 64 + 4 * r;
+        int i = i0 + ii, k = k0 + kk;
+        As[kk][ii] = (i < M && k < kend) ? A[i + (size_t)k * lda] : 0.0;
+      }
+    }
+    {
+      int kk = t % 16;
+#pragma unroll
+      for (int r = 0; r < 4; ++r) {
+        int jj = t / 16 + 16 * r;
+        int j = j0 + jj, k = k0 + kk;
+        Bs[kk][jj] = (j < N && k < kend) ? B[k + (size_t)j * ldb] : 0.0;
+      }
+    }
+    __syncthreads();
+#pragma unroll
+    for (int kk = 0; kk < GK; ++kk) {
+      double a[4], b[4];
+#pragma unroll
+      for (int u = 0; u < 4; ++u) a[u] = As[kk][ty + 16 * u];
+#pragma unroll
+      for (int v = 0; v < 4; ++v) b[v] = Bs[kk][tx + 16 * v];
+#pragma unroll
+      for (int u = 0; u < 4; ++u)
+#pragma unroll
+        for (int v = 0; v < 4; ++v) acc[u][v] = fma(a[u], b[v], acc[u][v]);
+    }
+    __syncthreads();
+  }
+#pragma unroll
+  for (int u = 0; u < 4; ++u) {
+    int i = i0 + ty + 16 * u;
+    if (i >= M) continue;
+#pragma unroll
+    for (int v = 0; v < 4; ++v) {
+      int j = j0 + tx + 16 * v;
+      if (j >= N) continue;
+      if (partial) partial[(size_t)blockIdx.z * M * N + i + (size_t)j * M] = acc[u][v];
+      else C[i + (size_t)j * ldc] = alpha * acc[u][v] + (beta == 0.0 ? 0.0 : beta * C[i + (size_t)j * ldc]);
+    }
+  }
+}
+
+__global__ void splitk_reduce_kernel(int M, int N, int splits, const double* __restrict__ partial, double* C, int ldc,
+                                     double alpha, double beta) {
+  size_t total = (size_t)M * N;
+  for (size_t e = blockIdx.x * (size_t)blockDim.x + threadIdx.x; e < total; e += (size_t)gridDim.x * blockDim.x) {
+    double s = 0;
+    for (int z = 0; z < splits; ++z) s += partial[(size_t)z * total + e];
+    int i = (int)(e % M), j = (int)(e / M);
+    double* c = C + i + (size_t)j * ldc;
+    *c = alpha * s + (beta == 0.0 ? 0.0 : beta * *c);
+  }
+}
+
+void dgemm_cm(Engine& E, bool ta, int M, int N, int K, double alpha, const double* A, int lda, const double* B,
+              int ldb, double beta, double* C, int ldc) {
+  if (M <= 0 || N <= 0) return;
+  int tiles = ((M + GM - 1) / GM) * ((N + GN - 1) / GN);
+  int splits = 1, kchunk = std::max(K, 0);
+  if (K > 256 && tiles < 2 * E.num_sms) {
+    splits = std::min((K + 255) / 256, std::max(1, (4 * E.num_sms) / tiles));
+    kchunk = (K + splits - 1) / splits;
+    kchunk = ((kchunk + GK - 1) / GK) * GK;
+    splits = (K + kchunk - 1) / kchunk;
+  }
+  dim3 grid((N + GN - 1) / GN, (M + GM - 1) / GM, splits);
+  Buf part;
+  double* partial = nullptr;
+  if (splits > 1) {
+    part = E.alloc(sizeof(double) * (size_t)splits * M * N);
+    partial = (double*)part->ptr;
+  }
+  int tk = E.tic("dgemm_cm");
+  if (ta)
+    dgemm_cm_kernel<true><<<grid, BT, 0, E.stream>>>(M, N, K, A, lda, B, ldb, C, ldc, alpha, beta, kchunk, partial);
+  else
+    dgemm_cm_kernel<false><<<grid, BT, 0, E.stream>>>(M, N, K, A, lda, B, ldb, C, ldc, alpha, beta, kchunk, partial);
+  E.toc(tk, 2.0 * M * N * (double)K, 8.0 * ((double)M * K + (double)K * N + 2.0 * M * N));
+  SPS_CUDA(cudaGetLastError());
+  E.launches++;
+  if (splits > 1) {
+    size_t total = (size_t)M * N;
+    int g = (int)std::min<size_t>((total + 255) / 256, 4096);
+    splitk_reduce_kernel<<<g, 256, 0, E.stream>>>(M, N, splits, partial, C, ldc, alpha, beta);
+    SPS_CUDA(cudaGetLastError());
+    E.launches++;
+  }
+  E.flops += 2.0 * M * N * (double)K;
+}
+
+// ---------------------------------------------------------------------------
+// cooperative panel factorization
+// ---------------------------------------------------------------------------
+struct PanelArgs {
+  double* A;
+  int lda, m, j0, jb;
+  double* tau;       // tau[j0 .. j0+jb)
+  double* V;         // explicit V (m x n, ld m): panel columns written
+  double* T;         // jb x jb (col-major) compact-WY factor of this panel
+  double* acc;       // scratch: accn[jb], alpha[jb], accw[jb*jb], gram[jb*jb] (zeroed)
+  unsigned* bar;
+  int* flag;
+  int rpc;           // rows per CTA
+};
+
+__global__ void __launch_bounds__(BT) panel_qr_kernel(PanelArgs p) {
+  extern __shared__ double sm[];   // rpc x jb, row-major in shared memory
+  __shared__ double red[BW + 1];
+  const int jb = p.jb;
+  const int r0 = p.j0 + blockIdx.x * p.rpc;
+  const int r1 = min(p.m, r0 + p.rpc);
+  const int nr = max(0, r1 - r0);
+  double* accn = p.acc;
+  double* alph = accn + jb;
+  double* accw = alph + jb;
+  double* gram = accw + jb * jb;
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  for (int e = threadIdx.x; e < nr * jb; e += BT) {
+    int r = e / jb, c = e % jb;
+    sm[e] = p.A[(size_t)(r0 + r) + (size_t)(p.j0 + c) * p.lda];
+  }
+  __syncthreads();
+  for (int jj = 0; jj < jb; ++jj) {
+    const int j = p.j0 + jj;
+    const bool owner = (j >= r0 && j < r1);
+    double part = 0;
+    for (int r = threadIdx.x; r < nr; r += BT)
+      if (r0 + r > j) {
+        double x = sm[r * jb + jj];
+        part += x * x;
+      }
+    part = bsum(part, red);
+    if (threadIdx.x == 0) {
+      if (part != 0.0) atomicAdd(&accn[jj], part);
+      if (owner) alph[jj] = sm[(j - r0) * jb + jj];
+    }
+    grid_barrier(p.bar, p.flag);
+    const double sumsq = __ldcg(&accn[jj]);
+    const double alpha = __ldcg(&alph[jj]);
+    double tau = 0.0, scal = 0.0, beta = alpha;
+    if (sumsq != 0.0) {
+      beta = -copysign(sqrt(alpha * alpha + sumsq), alpha);
+      tau = (beta - alpha) / beta;
+      scal = 1.0 / (alpha - beta);
+    }
+    if (blockIdx.x == 0 && threadIdx.x == 0) p.tau[j] = tau;
+    if (tau != 0.0) {
+      for (int r = threadIdx.x; r < nr; r += BT)
+        if (r0 + r > j) sm[r * jb + jj] *= scal;
+      if (owner && threadIdx.x == 0) sm[(j - r0) * jb + jj] = beta;
+      __syncthreads();
+      for (int kk = jj + 1 + warp; kk < jb; kk += BW) {
+        double w = 0;
+        for (int r = lane; r < nr; r += 32) {
+          int gr = r0 + r;
+          if (gr > j) w += sm[r * jb + jj] * sm[r * jb + kk];
+          else if (gr == j) w += sm[r * jb + kk];
+        }
+        w = wsum(w);
+        if (lane == 0 && w != 0.0) atomicAdd(&accw[jj * jb + kk], w);
+      }
+      grid_barrier(p.bar, p.flag);
+      for (int kk = jj + 1 + warp; kk < jb; kk += BW) {
+        double w = __ldcg(&accw[jj * jb + kk]) * tau;
+        for (int r = lane; r < nr; r += 32) {
+          int gr = r0 + r;
+          if (gr > j) sm[r * jb + kk] -= sm[r * jb + jj] * w;
+          else if (gr == j) sm[r * jb + kk] -= w;
+        }
+      }
+    }
+    __syncthreads();
+  }
+  // write back, explicit V and partial Gram V^T V
+  for (int e = threadIdx.x; e < nr * jb; e += BT) {
+    int r = e / jb, c = e % jb;
+    int gr = r0 + r, gc = p.j0 + c;
+    double x = sm[e];
+    p.A[(size_t)gr + (size_t)gc * p.lda] = x;
+    double v = gr < gc ? 0.0 : (gr == gc ? 1.0 : x);
+    p.V[(size_t)gr + (size_t)gc * p.m] = v;
+    sm[e] = v;
+  }
+  __syncthreads();
+  for (int e = threadIdx.x; e < jb * jb; e += BT) {
+    int a = e / jb, b = e % jb;
+    if (b < a) continue;
+    double s = 0;
+    for (int r = 0; r < nr; ++r) s += sm[r * jb + a] * sm[r * jb + b];
+    if (s != 0.0) atomicAdd(&gram[a * jb + b], s);
+  }
+  grid_barrier(p.bar, p.flag);
+  if (blockIdx.x == 0 && threadIdx.x == 0) {
+    // T(i,i) = tau_i ; T(0:i, i) = -tau_i T(0:i,0:i) V(:,0:i)^T v_i  (dlarft, forward, columnwise)
+    for (int i = 0; i < jb; ++i) {
+      double ti = p.tau[p.j0 + i];
+      for (int a = 0; a < i; ++a) {
+        double s = 0;
+        for (int b = a; b < i; ++b) s += p.T[a + b * jb] * __ldcg(&gram[b * jb + i]);
+        p.T[a + i * jb] = -ti * s;
+      }
+      p.T[i + i * jb] = ti;
+      for (int a = i + 1; a < jb; ++a) p.T[a + i * jb] = 0.0;
+    }
+  }
+}
+
+void copy_upper_and_identity(Engine& E, const double* a, int m, int n, int lda, double* r, int ldr, double* q,
+                             int ldq);
+
+static int coop_blocks(const void* kernel, int threads, size_t smem, Engine& E) {
+  int per_sm = 0;
+  SPS_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kernel, threads, smem));
+  return std::max(1, per_sm) * E.num_sms;
+}
+
+// Householder QR of a (m x n, col-major lda), m >= n: q (m x n, ldq), r (n x n, ldr).
+void qr_big(Engine& E, double* a, int m, int n, int lda, double* q, int ldq, double* r, int ldr) {
+  const int jb_max = 32;
+  const int np = (n + jb_max - 1) / jb_max;
+  Buf vb = E.alloc(sizeof(double) * (size_t)m * n);
+  Buf tb = E.alloc(sizeof(double) * (size_t)np * jb_max * jb_max);
+  Buf taub = E.alloc(sizeof(double) * n);
+  Buf accb = E.alloc(sizeof(double) * (size_t)np * (2 * jb_max + 2 * jb_max * jb_max));
+  Buf barb = E.alloc(sizeof(unsigned) * 2 * np);
+  Buf wb = E.alloc(sizeof(double) * (size_t)jb_max * n * 2);
+  double* V = (double*)vb->ptr;
+  double* T = (double*)tb->ptr;
+  double* W = (double*)wb->ptr;
+  double* W2 = W + (size_t)jb_max * n;
+  SPS_CUDA(cudaMemsetAsync(accb->ptr, 0, sizeof(double) * (size_t)np * (2 * jb_max + 2 * jb_max * jb_max), E.stream));
+  SPS_CUDA(cudaMemsetAsync(barb->ptr, 0, sizeof(unsigned) * 2 * np, E.stream));
+  SPS_CUDA(cudaMemsetAsync(T, 0, sizeof(double) * (size_t)np * jb_max * jb_max, E.stream));
+  for (int pi = 0; pi < np; ++pi) {
+    int j0 = pi * jb_max, jb = std::min(jb_max, n - j0);
+    int mrows = m - j0;
+    int maxg = coop_blocks((const void*)panel_qr_kernel, BT, 0, E);
+    int G = std::min({E.num_sms, maxg, std::max(1, (mrows + 63) / 64)});
+    int rpc = (mrows + G - 1) / G;
+    size_t smem = sizeof(double) * (size_t)rpc * jb;
+    if (smem > 200 * 1024) {
+      G = std::min(maxg, (int)((mrows * (size_t)jb * 8 + 200 * 1024 - 1) / (200 * 1024)));
+      rpc = (mrows + G - 1) / G;
+      smem = sizeof(double) * (size_t)rpc * jb;
+      if (smem > 200 * 1024) throw Error(SPS_ERR_ARGUMENT, "qr_big: panel too tall for shared memory");
+    }
+    SPS_CUDA(cudaFuncSetAttribute((const void*)panel_qr_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                  (int)std::max<size_t>(smem, 1)));
+    PanelArgs pa;
+    pa.A = a;
+    pa.lda = lda;
+    pa.m = m;
+    pa.j0 = j0;
+    pa.jb = jb;
+    pa.tau = (double*)taub->ptr;
+    pa.V = V;
+    pa.T = T + (size_t)pi * jb_max * jb_max;
+    pa.acc = (double*)accb->ptr + (size_t)pi * (2 * jb_max + 2 * jb_max * jb_max);
+    pa.bar = (unsigned*)barb->ptr + 2 * pi;
+    pa.flag = E.dflag;
+    pa.rpc = rpc;
+    void* args[] = {&pa};
+    int tk = E.tic("qr_panel");
+    SPS_CUDA(cudaLaunchCooperativeKernel((const void*)panel_qr_kernel, dim3(G), dim3(BT), args, smem, E.stream));
+    E.toc(tk, 2.0 * mrows * jb * (double)jb, 16.0 * mrows * jb);
+    E.launches++;
+    int n2 = n - j0 - jb;
+    if (n2 > 0) {
+      const double* Vp = V + j0 + (size_t)j0 * m;
+      double* A2 = a + j0 + (size_t)(j0 + jb) * lda;
+      dgemm_cm(E, true, jb, n2, mrows, 1.0, Vp, m, A2, lda, 0.0, W, jb);                      // W = V^T A2
+      dgemm_cm(E, true, jb, n2, jb, 1.0, pa.T, jb, W, jb, 0.0, W2, jb);                       // W2 = T^T W
+      dgemm_cm(E, false, mrows, n2, jb, -1.0, Vp, m, W2, jb, 1.0, A2, lda);                   // A2 -= V W2
+    }
+  }
+  // R (upper triangle of a) and Q = H_1 ... H_np [I; 0]
+  copy_upper_and_identity(E, a, m, n, lda, r, ldr, q, ldq);
+  for (int pi = np - 1; pi >= 0; --pi) {
+    int j0 = pi * jb_max, jb = std::min(jb_max, n - j0);
+    int mrows = m - j0, nc = n - j0;
+    const double* Vp = V + j0 + (size_t)j0 * m;
+    const double* Tp = T + (size_t)pi * jb_max * jb_max;
+    double* Q2 = q + j0 + (size_t)j0 * ldq;
+    dgemm_cm(E, true, jb, nc, mrows, 1.0, Vp, m, Q2, ldq, 0.0, W, jb);       // W = V^T Q2
+    dgemm_cm(E, false, jb, nc, jb, 1.0, Tp, jb, W, jb, 0.0, W2, jb);         // W2 = T W
+    dgemm_cm(E, false, mrows, nc, jb, -1.0, Vp, m, W2, jb, 1.0, Q2, ldq);    // Q2 -= V W2
+  }
+}
+
+__global__ void upper_identity_kernel(const double* a, int m, int n, int lda, double* r, int ldr, double* q, int ldq) {
+  size_t tr = (size_t)n * n, tq = (size_t)m * n;
+  for (size_t e = blockIdx.x * (size_t)blockDim.x + threadIdx.x; e < tr + tq; e += (size_t)gridDim.x * blockDim.x) {
+    if (e < tr) {
+      int i = (int)(e % n), j = (int)(e / n);
+      r[i + (size_t)j * ldr] = i <= j ? a[i + (size_t)j * lda] : 0.0;
+    } else {
+      size_t f = e - tr;
+      int i = (int)(f % m), j = (int)(f / m);
+      q[i + (size_t)j * ldq] = i == j ? 1.0 : 0.0;
+    }
+  }
+}
+
+void copy_upper_and_identity(Engine& E, const double* a, int m, int n, int lda, double* r, int ldr, double* q,
+                             int ldq) {
+  size_t total = (size_t)n * n + (size_t)m * n;
+  int g = (int)std::min<size_t>((total + 255) / 256, 8192);
+  upper_identity_kernel<<<g, 256, 0, E.stream>>>(a, m, n, lda, r, ldr, q, ldq);
+  SPS_CUDA(cudaGetLastError());
+  E.launches++;
+}
+
+// ---------------------------------------------------------------------------
+// cooperative one-sided Jacobi SVD over several problems (m >= n each)
+// ---------------------------------------------------------------------------
+struct JacProb {
+  double* U;     // m x n (ld m), rotated in place
+  double* V;     // n x n (ld n) workspace
+  double* q;     // output U sorted (ld m)
+  double* r;     // output V sorted (ld n)
+  double* s;     // output singular values (descending)
+  double* sig;   // n scratch
+  int* rank;     // n scratch
+  int m, n;
+  int pair_base; // first global pair index of this problem
+};
+
+__device__ __forceinline__ int rr_idx(int i, int round, int np) {
+  return i == 0 ? 0 : ((i - 1 + round) % (np - 1)) + 1;
+}
+
+__global__ void __launch_bounds__(BT) jacobi_coop_kernel(const JacProb* probs, int nprob, int total_pairs,
+                                                         int max_rounds, unsigned* bar, int* counters, int* flag) {
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  const int gw = blockIdx.x * BW + warp, TW = gridDim.x * BW;
+  // V = I
+  for (int pi = 0; pi < nprob; ++pi) {
+    const JacProb P = probs[pi];
+    size_t nn = (size_t)P.n * P.n;
+    for (size_t e = blockIdx.x * (size_t)BT + threadIdx.x; e < nn; e += (size_t)gridDim.x * BT)
+      P.V[e] = (e % P.n == e / P.n) ? 1.0 : 0.0;
+  }
+  if (blockIdx.x == 0 && threadIdx.x == 0) {
+    counters[0] = 0;
+    counters[1] = 0;
+    counters[2] = 0;
+  }
+  grid_barrier(bar, flag);
+  const int MAXSWEEP = 80;
+  bool converged = false;
+  for (int sweep = 0; sweep < MAXSWEEP; ++sweep) {
+    int* cnt = counters + (sweep % 3);
+    if (blockIdx.x == 0 && threadIdx.x == 0) counters[(sweep + 1) % 3] = 0;
+    for (int round = 0; round < max_rounds; ++round) {
+      for (int t = gw; t < total_pairs; t += TW) {
+        int pi = 0;
+        while (pi + 1 < nprob && t >= probs[pi + 1].pair_base) ++pi;
+        const JacProb& P = probs[pi];
+        const int np = P.n + (P.n & 1);
+        if (round >= np - 1) continue;
+        int pr = t - P.pair_base;
+        int p = rr_idx(pr, round, np), qd = rr_idx(np - 1 - pr, round, np);
+        if (p >= P.n || qd >= P.n) continue;
+        if (p > qd) { int tt = p; p = qd; qd = tt; }
+        double* up = P.U + (size_t)p * P.m;
+        double* uq = P.U + (size_t)qd * P.m;
+        double al = 0, be = 0, ga = 0;
+        for (int i = lane; i < P.m; i += 32) {
+          double x = up[i], y = uq[i];
+          al += x * x;
+          be += y * y;
+          ga += x * y;
+        }
+        al = wsum(al);
+        be = wsum(be);
+        ga = wsum(ga);
+        const double tol = DBL_EPSILON * (double)max(P.m, 2);
+        if (ga == 0.0 || !(fabs(ga) > tol * sqrt(al * be))) continue;
+        double zeta = (be - al) / (2.0 * ga);
+        double tt = copysign(1.0, zeta) / (fabs(zeta) + sqrt(1.0 + zeta * zeta));
+        double c = 1.0 / sqrt(1.0 + tt * tt), s = c * tt;
+        for (int i = lane; i < P.m; i += 32) {
+          double x = up[i], y = uq[i];
+          up[i] = c * x - s * y;
+          uq[i] = s * x + c * y;
+        }
+        double* vp = P.V + (size_t)p * P.n;
+        double* vq = P.V + (size_t)qd * P.n;
+        for (int i = lane; i < P.n; i += 32) {
+          double x = vp[i], y = vq[i];
+          vp[i] = c * x - s * y;
+          vq[i] = s * x + c * y;
+        }
+        if (lane == 0) atomicAdd(cnt, 1);
+      }
+      grid_barrier(bar, flag);
+    }
+    int rot = *(volatile int*)cnt;
+    if (rot == 0) {
+      converged = true;
+      break;
+    }
+  }
+  if (!converged && blockIdx.x == 0 && threadIdx.x == 0) atomicOr(flag, FLAG_CONV);
+  // singular values
+  for (int pi = 0; pi < nprob; ++pi) {
+    const JacProb P = probs[pi];
+    for (int c = gw; c < P.n; c += TW) {
+      const double* uc = P.U + (size_t)c * P.m;
+      double v = 0;
+      for (int i = lane; i < P.m; i += 32) v += uc[i] * uc[i];
+      v = wsum(v);
+      if (lane == 0) P.sig[c] = sqrt(v);
+    }
+  }
+  grid_barrier(bar, flag);
+  for (int pi = 0; pi < nprob; ++pi) {
+    const JacProb P = probs[pi];
+    for (int c = blockIdx.x * BT + threadIdx.x; c < P.n; c += gridDim.x * BT) {
+      double sc = __ldcg(&P.sig[c]);
+      int rk = 0;
+      for (int j = 0; j < P.n; ++j) {
+        double sj = __ldcg(&P.sig[j]);
+        rk += (sj > sc) || (sj == sc && j < c);
+      }
+      P.rank[c] = rk;
+      P.s[rk] = sc;
+    }
+  }
+  grid_barrier(bar, flag);
+  for (int pi = 0; pi < nprob; ++pi) {
+    const JacProb P = probs[pi];
+    for (int c = gw; c < P.n; c += TW) {
+      int rk = __ldcg(&P.rank[c]);
+      double sc = __ldcg(&P.sig[c]);
+      double inv = sc > 0 ? 1.0 / sc : 0.0;
+      const double* uc = P.U + (size_t)c * P.m;
+      double* qo = P.q + (size_t)rk * P.m;
+      for (int i = lane; i < P.m; i += 32) qo[i] = uc[i] * inv;
+      const double* vc = P.V + (size_t)c * P.n;
+      double* ro = P.r + (size_t)rk * P.n;
+      for (int i = lane; i < P.n; i += 32) ro[i] = vc[i];
+    }
+  }
+}
+
+// problems: (a = U in/out workspace m x n ld m, q out m x n ld m, r out n x n ld n, s out n)
+void svd_big(Engine& E, const std::vector<MatDesc>& d) {
+  if (d.empty()) return;
+  std::vector<JacProb> ps;
+  int pairs = 0, max_rounds = 0;
+  size_t ws = 0;
+  for (auto& x : d) ws += (size_t)x.n * x.n + 2 * (size_t)x.n + 8;
+  Buf wb = E.alloc(sizeof(double) * ws);
+  double* w = (double*)wb->ptr;
+  for (auto& x : d) {
+    if (x.lda != x.m || x.ldq != x.m || x.ldr != x.n) throw Error(SPS_ERR_ARGUMENT, "svd_big: leading dimensions");
+    JacProb P;
+    P.U = x.a;
+    P.q = x.q;
+    P.r = x.r;
+    P.s = x.s;
+    P.m = x.m;
+    P.n = x.n;
+    P.V = w;
+    w += (size_t)x.n * x.n;
+    P.sig = w;
+    w += x.n;
+    P.rank = (int*)w;
+    w += x.n + 8;
+    P.pair_base = pairs;
+    int np = x.n + (x.n & 1);
+    pairs += np / 2;
+    max_rounds = std::max(max_rounds, np - 1);
+    ps.push_back(P);
+  }
+  Buf pb = E.alloc(sizeof(JacProb) * ps.size());
+  E.stage(ps.data(), sizeof(JacProb) * ps.size(), pb->ptr);
+  Buf bb = E.alloc(sizeof(unsigned) * 2 + sizeof(int) * 4);
+  SPS_CUDA(cudaMemsetAsync(bb->ptr, 0, sizeof(unsigned) * 2 + sizeof(int) * 4, E.stream));
+  int maxg = coop_blocks((const void*)jacobi_coop_kernel, BT, 0, E);
+  int G = std::min({E.num_sms, maxg, std::max(1, (pairs + BW - 1) / BW)});
+  const JacProb* dp = (const JacProb*)pb->ptr;
+  int nprob = (int)ps.size();
+  unsigned* bar = (unsigned*)bb->ptr;
+  int* counters = (int*)(bar + 2);
+  void* args[] = {&dp, &nprob, &pairs, &max_rounds, &bar, &counters, &E.dflag};
+  int tk = E.tic("svd_jacobi_coop");
+  SPS_CUDA(cudaLaunchCooperativeKernel((const void*)jacobi_coop_kernel, dim3(G), dim3(BT), args, 0, E.stream));
+  E.toc(tk);
+  E.launches++;
+}
+
+}  // namespace la
+}  // namespace sps

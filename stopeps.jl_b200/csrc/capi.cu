@@ -2,6 +2,7 @@
 // state / cache ids, status codes and the last error message.
 #include "stopeps_gpu.h"
 #include "pipeline.h"
+#include <cstdio>
 #include <cstring>
 #include <memory>
 #include <unordered_map>
@@ -10,6 +11,7 @@ using namespace sps;
 
 struct sps_handle {
   std::unique_ptr<Engine> E;
+  cudaEvent_t t0 = nullptr, t1 = nullptr;
   sps_config cfg;
   std::unordered_map<int, State> states;
   std::unordered_map<int, SamplingCache> caches;
@@ -97,6 +99,8 @@ int sps_create(const sps_config* cfg, sps_handle** out) {
 
 void sps_destroy(sps_handle* h) {
   if (!h) return;
+  if (h->t0) cudaEventDestroy(h->t0);
+  if (h->t1) cudaEventDestroy(h->t1);
   h->caches.clear();
   h->states.clear();
   delete h;
@@ -113,6 +117,52 @@ int sps_counters(sps_handle* h, long long* launches, double* flops) {
   return guarded(h, [&] {
     if (launches) *launches = h->E->launches;
     if (flops) *flops = h->E->flops;
+  });
+}
+
+int sps_set_profile(sps_handle* h, int32_t enable) {
+  return guarded(h, [&] {
+    h->E->reset_stats();
+    h->E->profile = enable != 0;
+  });
+}
+
+int sps_kernel_stats_json(sps_handle* h, char* buf, size_t n) {
+  return guarded(h, [&] {
+    auto st = h->E->kernel_stats();
+    std::string js = "{";
+    bool first = true;
+    char tmp[512];
+    for (auto& kv : st) {
+      std::snprintf(tmp, sizeof(tmp), "%s\"%s\": {\"ms\": %.6f, \"count\": %lld, \"flops\": %.6e, \"bytes\": %.6e}",
+                    first ? "" : ", ", kv.first.c_str(), kv.second.ms, kv.second.count, kv.second.flops,
+                    kv.second.bytes);
+      js += tmp;
+      first = false;
+    }
+    js += "}";
+    if (!buf || js.size() + 1 > n) throw Error(SPS_ERR_ARGUMENT, "buffer too small");
+    std::memcpy(buf, js.c_str(), js.size() + 1);
+  });
+}
+
+int sps_timer_start(sps_handle* h) {
+  return guarded(h, [&] {
+    if (!h->t0) {
+      SPS_CUDA(cudaEventCreate(&h->t0));
+      SPS_CUDA(cudaEventCreate(&h->t1));
+    }
+    SPS_CUDA(cudaEventRecord(h->t0, h->E->stream));
+  });
+}
+
+int sps_timer_stop(sps_handle* h, double* ms) {
+  return guarded(h, [&] {
+    SPS_CUDA(cudaEventRecord(h->t1, h->E->stream));
+    SPS_CUDA(cudaEventSynchronize(h->t1));
+    float f = 0;
+    SPS_CUDA(cudaEventElapsedTime(&f, h->t0, h->t1));
+    if (ms) *ms = f;
   });
 }
 

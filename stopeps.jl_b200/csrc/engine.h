@@ -130,6 +130,21 @@ class Engine {
   // counters
   long long launches = 0;
   double flops = 0;
+
+  // optional per-kernel timing: tic() before a launch, toc() after it; events
+  // are resolved by kernel_stats() after a sync.  Off unless `profile` is set.
+  bool profile = false;
+  int tic(const char* name);
+  void toc(int id, double algorithmic_flops = 0, double algorithmic_bytes = 0);
+  struct KStat { double ms = 0, flops = 0, bytes = 0; long long count = 0; };
+  std::map<std::string, KStat> kernel_stats();
+  void reset_stats();
+ private:
+  struct Pending { std::string name; cudaEvent_t a, b; double flops, bytes; };
+  std::vector<Pending> pending_;
+  std::vector<cudaEvent_t> event_pool_;
+  std::map<std::string, KStat> stats_;
+  cudaEvent_t get_event();
 };
 
 // ---------------------------------------------------------------------------
@@ -207,6 +222,13 @@ void qr_batched(Engine& E, const std::vector<MatDesc>& d);
 void svd_batched(Engine& E, const std::vector<MatDesc>& d);    // m >= n required
 void eigh_batched(Engine& E, const std::vector<MatDesc>& d);   // symmetric n x n
 void inv_batched(Engine& E, const std::vector<MatDesc>& d);    // general square
+// multi-CTA versions for large blocks (bigla.cu)
+void qr_big(Engine& E, double* a, int m, int n, int lda, double* q, int ldq, double* r, int ldr);  // m >= n
+void svd_big(Engine& E, const std::vector<MatDesc>& d);        // m >= n, ld = m / n
+void dgemm_cm(Engine& E, bool ta, int M, int N, int K, double alpha, const double* A, int lda, const double* B,
+              int ldb, double beta, double* C, int ldc);
+bool qr_is_big(int m, int n);
+bool svd_is_big(int m, int n);
 }  // namespace la
 
 // gather/scatter between tensors and dense column-major block matrices

@@ -210,9 +210,11 @@ static Tensor solve_core(Engine& E, const Tensor& normal, const Tensor& rhs, con
   if (M.dims[2] * M.dims[3] != n || b.dims[0] * b.dims[1] != n) throw Error(SPS_ERR_ARGUMENT, "solve_core: shape");
   Tensor x = E.empty(b.legs);
   Buf w = E.alloc(sizeof(double) * (n + 4 * n * P + 8));
+  int tk = E.tic("cg");
   cg_kernel<<<1, CG_T, 0, E.stream>>>(M.ptr(), b.ptr(), x0.ptr(), x.ptr(), (double*)w->ptr, n, P,
                                       o.diagonal_shift, o.linear_max_iterations, o.linear_tolerance,
                                       E.dscal + slot);
+  E.toc(tk);
   SPS_CUDA(cudaGetLastError());
   E.launches++;
   return x;

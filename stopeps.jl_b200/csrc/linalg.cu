@@ -405,13 +405,17 @@ void qr_batched(Engine& E, const std::vector<MatDesc>& d) {
   if (d.empty()) return;
   Buf kd;
   MatDesc* dd = upload_desc(E, d, kd);
-  qr_kernel<<<(int)d.size(), NT, 0, E.stream>>>(dd);
-  SPS_CUDA(cudaGetLastError());
-  E.launches++;
+  double fl = 0;
   for (auto& x : d) {
     double k = std::min(x.m, x.n);
-    E.flops += 4.0 * x.m * x.n * k;
+    fl += 4.0 * x.m * x.n * k;
   }
+  int tk = E.tic("qr_small");
+  qr_kernel<<<(int)d.size(), NT, 0, E.stream>>>(dd);
+  E.toc(tk, fl);
+  SPS_CUDA(cudaGetLastError());
+  E.launches++;
+  E.flops += fl;
 }
 
 void svd_batched(Engine& E, const std::vector<MatDesc>& d) {
@@ -428,8 +432,10 @@ void svd_batched(Engine& E, const std::vector<MatDesc>& d) {
   Buf w = E.alloc(std::max<size_t>(tot, 1) * sizeof(double));
   Buf ko = E.alloc(off.size() * sizeof(size_t));
   E.stage(off.data(), off.size() * sizeof(size_t), ko->ptr);
+  int tk = E.tic("svd_small");
   svd_kernel<<<(int)d.size(), NT, 0, E.stream>>>(dd, (double*)w->ptr, (const size_t*)ko->ptr,
                                                 E.dflag);
+  E.toc(tk);
   SPS_CUDA(cudaGetLastError());
   E.launches++;
 }
@@ -448,8 +454,10 @@ void eigh_batched(Engine& E, const std::vector<MatDesc>& d) {
   Buf w = E.alloc(std::max<size_t>(tot, 1) * sizeof(double));
   Buf ko = E.alloc(off.size() * sizeof(size_t));
   E.stage(off.data(), off.size() * sizeof(size_t), ko->ptr);
+  int tk = E.tic("eigh");
   eigh_kernel<<<(int)d.size(), NT, 0, E.stream>>>(dd, (double*)w->ptr, (const size_t*)ko->ptr,
                                                  E.dflag);
+  E.toc(tk);
   SPS_CUDA(cudaGetLastError());
   E.launches++;
 }

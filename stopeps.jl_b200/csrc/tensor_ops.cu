@@ -192,6 +192,58 @@ int* Engine::upload_i32(const std::vector<int>& v, Buf& keep) {
   return (int*)keep->ptr;
 }
 
+cudaEvent_t Engine::get_event() {
+  if (!event_pool_.empty()) {
+    cudaEvent_t e = event_pool_.back();
+    event_pool_.pop_back();
+    return e;
+  }
+  cudaEvent_t e;
+  SPS_CUDA(cudaEventCreate(&e));
+  return e;
+}
+
+int Engine::tic(const char* name) {
+  if (!profile) return -1;
+  Pending p;
+  p.name = name;
+  p.a = get_event();
+  p.b = get_event();
+  p.flops = p.bytes = 0;
+  SPS_CUDA(cudaEventRecord(p.a, stream));
+  pending_.push_back(p);
+  return (int)pending_.size() - 1;
+}
+
+void Engine::toc(int id, double fl, double by) {
+  if (id < 0 || id >= (int)pending_.size()) return;
+  pending_[id].flops = fl;
+  pending_[id].bytes = by;
+  SPS_CUDA(cudaEventRecord(pending_[id].b, stream));
+}
+
+std::map<std::string, Engine::KStat> Engine::kernel_stats() {
+  SPS_CUDA(cudaStreamSynchronize(stream));
+  for (auto& p : pending_) {
+    float ms = 0;
+    SPS_CUDA(cudaEventElapsedTime(&ms, p.a, p.b));
+    auto& k = stats_[p.name];
+    k.ms += ms;
+    k.flops += p.flops;
+    k.bytes += p.bytes;
+    k.count++;
+    event_pool_.push_back(p.a);
+    event_pool_.push_back(p.b);
+  }
+  pending_.clear();
+  return stats_;
+}
+
+void Engine::reset_stats() {
+  kernel_stats();
+  stats_.clear();
+}
+
 void Engine::sync() {
   SPS_CUDA(cudaStreamSynchronize(stream));
   ring_pos = 0;
@@ -507,7 +559,9 @@ Tensor contiguous(Engine& E, const Tensor& A) {
     d.dims[k] = A.dims[k];
     d.istr[k] = A.strides[k];
   }
+  int tk = E.tic("permute");
   permute_kernel<<<grid_for(n), 256, 0, E.stream>>>(A.ptr(), out.ptr(), d, n);
+  E.toc(tk, 0, 16.0 * n);
   SPS_CUDA(cudaGetLastError());
   E.launches++;
   return out;
@@ -701,7 +755,9 @@ void gather_block(Engine& E, const Tensor& A, const int64_t* rt, const int64_t* 
                   double* dst, int ld, bool transpose) {
   int64_t n = (int64_t)M * N;
   if (!n) return;
+  int tk = E.tic("block_gather");
   gather_kernel<<<grid_for(n), 256, 0, E.stream>>>(A.ptr(), rt, ct, M, N, dst, ld, transpose);
+  E.toc(tk, 0, 16.0 * n);
   SPS_CUDA(cudaGetLastError());
   E.launches++;
 }
@@ -710,7 +766,9 @@ void scatter_block(Engine& E, Tensor& A, const int64_t* rt, const int64_t* ct, i
                    const double* src, int ld, bool transpose) {
   int64_t n = (int64_t)M * N;
   if (!n) return;
+  int tk = E.tic("block_scatter");
   scatter_kernel<<<grid_for(n), 256, 0, E.stream>>>(A.ptr(), rt, ct, M, N, src, ld, transpose);
+  E.toc(tk, 0, 16.0 * n);
   SPS_CUDA(cudaGetLastError());
   E.launches++;
 }
@@ -812,7 +870,14 @@ Tensor ein(Engine& E, const std::string& spec, const Tensor& A, const Tensor& B,
   Buf kp = E.alloc(probs.size() * sizeof(GemmProb));
   E.stage(probs.data(), probs.size() * sizeof(GemmProb), kp->ptr);
   dim3 grid((maxN + TN - 1) / TN, (maxM + TM - 1) / TM, (unsigned)probs.size());
+  double fl = 0, by = 0;
+  for (auto& P : probs) {
+    fl += 2.0 * P.M * P.N * (double)P.K;
+    by += 8.0 * ((double)P.M * P.K + (double)P.K * P.N + (double)P.M * P.N);
+  }
+  int tk = E.tic("gemm_gather");
   gemm_gather_kernel<<<grid, GT, 0, E.stream>>>((const GemmProb*)kp->ptr, alpha);
+  E.toc(tk, fl, by);
   SPS_CUDA(cudaGetLastError());
   E.launches++;
   return C;
@@ -860,6 +925,28 @@ std::vector<int64_t> tensor_rows(const Tensor& T, int first, int count, int c) {
 }
 }  // namespace
 
+namespace la {
+bool qr_is_big(int m, int n) { return m >= n && (double)m * n * n >= 4.0e6; }
+bool svd_is_big(int m, int n) { return m >= n && n >= 160; }
+}  // namespace la
+
+// small blocks share one batched single-CTA launch; large ones use the multi-CTA path
+static void run_qr(Engine& E, const std::vector<la::MatDesc>& ds) {
+  std::vector<la::MatDesc> small;
+  for (auto& d : ds) {
+    if (la::qr_is_big(d.m, d.n)) la::qr_big(E, d.a, d.m, d.n, d.lda, d.q, d.ldq, d.r, d.ldr);
+    else small.push_back(d);
+  }
+  la::qr_batched(E, small);
+}
+
+static void run_svd(Engine& E, const std::vector<la::MatDesc>& ds) {
+  std::vector<la::MatDesc> small, big;
+  for (auto& d : ds) (la::svd_is_big(d.m, d.n) ? big : small).push_back(d);
+  la::svd_batched(E, small);
+  la::svd_big(E, big);
+}
+
 QRres qr(Engine& E, const Tensor& A, const std::vector<int>& rows, const std::vector<int>& cols) {
   BlockTables bt = tables_of(A, rows, cols);
   int m[2], n[2], k[2];
@@ -890,7 +977,7 @@ QRres qr(Engine& E, const Tensor& A, const std::vector<int>& rows, const std::ve
     ds.push_back({a, q, r, s, m[c], n[c], m[c], m[c], k[c]});
     keep.insert(keep.end(), {ba, t1, t2});
   }
-  la::qr_batched(E, ds);
+  run_qr(E, ds);
   int di = 0;
   for (int c = 0; c < 2; ++c) {
     if (k[c] == 0) continue;
@@ -937,7 +1024,7 @@ LQres lq(Engine& E, const Tensor& A, const std::vector<int>& rows, const std::ve
     ds.push_back({a, q, r, s, n[c], m[c], n[c], n[c], k[c]});
     keep.insert(keep.end(), {ba, t1, t2});
   }
-  la::qr_batched(E, ds);
+  run_qr(E, ds);
   int di = 0;
   for (int c = 0; c < 2; ++c) {
     if (k[c] == 0) continue;
@@ -1016,7 +1103,7 @@ SVDres svd(Engine& E, const Tensor& A, const std::vector<int>& rows, const std::
     ds.push_back({a, q, r, s, mm, nn, mm, mm, nn});
     keep.insert(keep.end(), {ba, t1, t2});
   }
-  la::svd_batched(E, ds);
+  run_svd(E, ds);
   SVDres res;
   std::vector<double> sv[2];
   // copy singular values back

@@ -74,6 +74,23 @@ class Engine:
         self.check(self.lib.sps_counters(self.h, C.byref(n), C.byref(f)))
         return n.value, f.value
 
+    def set_profile(self, enable: bool):
+        self.check(self.lib.sps_set_profile(self.h, 1 if enable else 0))
+
+    def kernel_stats(self) -> dict:
+        import json
+        buf = C.create_string_buffer(1 << 16)
+        self.check(self.lib.sps_kernel_stats_json(self.h, buf, 1 << 16))
+        return json.loads(buf.value.decode())
+
+    def timer_start(self):
+        self.check(self.lib.sps_timer_start(self.h))
+
+    def timer_stop(self) -> float:
+        ms = C.c_double()
+        self.check(self.lib.sps_timer_stop(self.h, C.byref(ms)))
+        return ms.value
+
     def close(self):
         if getattr(self, "h", None):
             self.lib.sps_destroy(self.h)

@@ -110,6 +110,13 @@ def pipeline_case(name):
 
 
 if __name__ == "__main__":
+    only = sys.argv[1:]
+    if only:
+        for name in only:
+            {"pepo_4x4_D4.npz": lambda: pepo_case("pepo_4x4_D4.npz", 4, 4, 0.7, 4, (2, 2), 16, (8, 8), 0.5, 0.05,
+                                                  [(16, (8, 8)), (24, (12, 12))], peps_D=4, peps_space=(2, 2),
+                                                  peps_chi=16, peps_env_space=(8, 8), ndraws=4, seed=1)}[name]()
+        sys.exit(0)
     # 3x3, D=4 PEPO; boundary chi 8 truncates, 16 is exact; PEPS step at D=2 exercises the ALS
     pepo_case("pepo_3x3_D4.npz", 3, 3, 0.7, 4, (2, 2), 16, (8, 8), 0.2, 0.05,
               [(8, (4, 4)), (16, (8, 8))], peps_D=2, peps_space=(1, 1), peps_chi=8, peps_env_space=(4, 4))
@@ -118,3 +125,8 @@ if __name__ == "__main__":
               peps_D=2, peps_space=None, peps_chi=4, peps_env_space=None, ndraws=6, seed=5,
               update=fu.FullUpdate(max_iterations=8, linear_max_iterations=40))
     pipeline_case("pipeline_2x2.npz")
+    # the plain-method config (4x4, D=4, chi=16, h=0.7, beta0=0.5, tau=0.05): large enough
+    # for the multi-CTA QR (chi=16) and Jacobi SVD (chi=24) paths of the engine
+    pepo_case("pepo_4x4_D4.npz", 4, 4, 0.7, 4, (2, 2), 16, (8, 8), 0.5, 0.05,
+              [(16, (8, 8)), (24, (12, 12))], peps_D=4, peps_space=(2, 2), peps_chi=16, peps_env_space=(8, 8),
+              ndraws=4, seed=1)

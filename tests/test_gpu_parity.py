@@ -15,7 +15,7 @@ from util import golden, upload_golden, oracle_state, space, rel
 pytestmark = pytest.mark.gpu
 TOL = 1e-10
 
-CASES = ["pepo_3x3_D4.npz", "pepo_2x3_D2.npz"]
+CASES = ["pepo_3x3_D4.npz", "pepo_2x3_D2.npz", "pepo_4x4_D4.npz"]
 
 
 def _engine(sps, g, **kw):
