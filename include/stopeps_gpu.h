@@ -111,6 +111,15 @@ int sps_kernel_stats_json(sps_handle* h, char* buf, size_t n);
 int sps_timer_start(sps_handle* h);
 int sps_timer_stop(sps_handle* h, double* milliseconds);
 
+/* Self-test / timing entry points of the dense factorization kernels (no
+ * reference counterpart; they stand in for LAPACK gesdd / geqrf+orgqr).
+ * Column-major host matrices.  sps_la_svd: a (m x n) = u (m x k) diag(s) vt
+ * (k x n), k = min(m,n), s descending; sweeps = Jacobi sweeps taken.
+ * sps_la_qr: a (m x n) = q (m x k) r (k x n).  ms = device time. */
+int sps_la_svd(sps_handle* h, int32_t m, int32_t n, const double* a, double* u, double* s, double* vt,
+               int32_t* sweeps, double* ms);
+int sps_la_qr(sps_handle* h, int32_t m, int32_t n, const double* a, double* q, double* r, double* ms);
+
 /* --- states: FiniteState (src/states/finite.jl:27-49) ---------------------
  * Site tensors have legs (W,N,Pout,Paux,E,S); each leg is described by its
  * even and odd multiplicities (n0,n1), even states first.  leg_dims holds

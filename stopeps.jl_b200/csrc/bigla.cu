@@ -57,11 +57,10 @@ __device__ void grid_barrier(unsigned* bar, int* flag) {
     } else {
       long long spins = 0;
       while (*gen == g) {
-        if (++spins > (1ll << 26)) {
+        if (++spins > (1ll << 27)) {   // ~seconds: every CTA is co-resident, so only a fault gets here
           atomicOr(flag, FLAG_BARRIER);
           break;
         }
-        __nanosleep(40);
       }
     }
     __threadfence();
@@ -502,8 +501,198 @@ __global__ void __launch_bounds__(BT) jacobi_coop_kernel(const JacProb* probs, i
       break;
     }
   }
-  if (!converged && blockIdx.x == 0 && threadIdx.x == 0) atomicOr(flag, FLAG_CONV);
+  if (blockIdx.x == 0 && threadIdx.x == 0) {
+    if (!converged) atomicOr(flag, FLAG_CONV);
+    atomicMax(flag + 1, 1000 + 0);   // marks the element-pair kernel
+  }
   // singular values
+  for (int pi = 0; pi < nprob; ++pi) {
+    const JacProb P = probs[pi];
+    for (int c = gw; c < P.n; c += TW) {
+      const double* uc = P.U + (size_t)c * P.m;
+      double v = 0;
+      for (int i = lane; i < P.m; i += 32) v += uc[i] * uc[i];
+      v = wsum(v);
+      if (lane == 0) P.sig[c] = sqrt(v);
+    }
+  }
+  grid_barrier(bar, flag);
+  for (int pi = 0; pi < nprob; ++pi) {
+    const JacProb P = probs[pi];
+    for (int c = blockIdx.x * BT + threadIdx.x; c < P.n; c += gridDim.x * BT) {
+      double sc = __ldcg(&P.sig[c]);
+      int rk = 0;
+      for (int j = 0; j < P.n; ++j) {
+        double sj = __ldcg(&P.sig[j]);
+        rk += (sj > sc) || (sj == sc && j < c);
+      }
+      P.rank[c] = rk;
+      P.s[rk] = sc;
+    }
+  }
+  grid_barrier(bar, flag);
+  for (int pi = 0; pi < nprob; ++pi) {
+    const JacProb P = probs[pi];
+    for (int c = gw; c < P.n; c += TW) {
+      int rk = __ldcg(&P.rank[c]);
+      double sc = __ldcg(&P.sig[c]);
+      double inv = sc > 0 ? 1.0 / sc : 0.0;
+      const double* uc = P.U + (size_t)c * P.m;
+      double* qo = P.q + (size_t)rk * P.m;
+      for (int i = lane; i < P.m; i += 32) qo[i] = uc[i] * inv;
+      const double* vc = P.V + (size_t)c * P.n;
+      double* ro = P.r + (size_t)rk * P.n;
+      for (int i = lane; i < P.n; i += 32) ro[i] = vc[i];
+    }
+  }
+}
+
+// ---------------------------------------------------------------------------
+// block one-sided Jacobi: columns in blocks of BJW; each round pairs blocks
+// and one CTA orthogonalizes the 2*BJW columns of its pair in shared memory
+// (inner one-sided Jacobi sweeps), then applies the accumulated 2BJW x 2BJW
+// rotation to V.  A grid barrier separates rounds (nblk-1 per sweep).
+// ---------------------------------------------------------------------------
+static constexpr int BJW = 16;
+static constexpr int BJ2 = 2 * BJW;
+
+__global__ void __launch_bounds__(BT) bjacobi_kernel(const JacProb* probs, int nprob, int total_pairs,
+                                                     int max_rounds, unsigned* bar, int* counters, int* flag,
+                                                     int* sweeps_out) {
+  extern __shared__ double smem[];
+  double* W = smem;                 // BJ2 x BJ2, column-major
+  double* Ub = smem + BJ2 * BJ2;    // m x BJ2, column-major (ld m)
+  __shared__ int inner_rot;
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  for (int pi = 0; pi < nprob; ++pi) {
+    const JacProb P = probs[pi];
+    size_t nn = (size_t)P.n * P.n;
+    for (size_t e = blockIdx.x * (size_t)BT + threadIdx.x; e < nn; e += (size_t)gridDim.x * BT)
+      P.V[e] = (e % P.n == e / P.n) ? 1.0 : 0.0;
+  }
+  if (blockIdx.x == 0 && threadIdx.x == 0) {
+    counters[0] = 0;
+    counters[1] = 0;
+    counters[2] = 0;
+  }
+  grid_barrier(bar, flag);
+  const int MAXSWEEP = 60;
+  bool converged = false;
+  int sweep = 0;
+  for (; sweep < MAXSWEEP; ++sweep) {
+    int* cnt = counters + (sweep % 3);
+    if (blockIdx.x == 0 && threadIdx.x == 0) counters[(sweep + 1) % 3] = 0;
+    for (int round = 0; round < max_rounds; ++round) {
+      for (int t = blockIdx.x; t < total_pairs; t += gridDim.x) {
+        int pi = 0;
+        while (pi + 1 < nprob && t >= probs[pi + 1].pair_base) ++pi;
+        const JacProb& P = probs[pi];
+        const int nb = (P.n + BJW - 1) / BJW;
+        const int nbp = nb + (nb & 1);
+        if (round >= nbp - 1) continue;
+        const int pr = t - P.pair_base;
+        int bi = rr_idx(pr, round, nbp), bj = rr_idx(nbp - 1 - pr, round, nbp);
+        if (bi >= nb || bj >= nb) continue;
+        if (bi > bj) { int tt = bi; bi = bj; bj = tt; }
+        const int c0 = bi * BJW, w1 = min(BJW, P.n - c0);
+        const int c1 = bj * BJW, w2 = min(BJW, P.n - c1);
+        const int wt = w1 + w2, m = P.m;
+        // load the two column blocks and W = I
+        for (int e = threadIdx.x; e < wt * m; e += BT) {
+          int k = e / m, i = e % m;
+          int gc = k < w1 ? c0 + k : c1 + (k - w1);
+          Ub[i + (size_t)k * m] = P.U[i + (size_t)gc * m];
+        }
+        for (int e = threadIdx.x; e < BJ2 * BJ2; e += BT) W[e] = (e % BJ2 == e / BJ2) ? 1.0 : 0.0;
+        __syncthreads();
+        const double tol = DBL_EPSILON * (double)max(m, 2);
+        const int wtp = wt + (wt & 1);
+        bool any = false;
+        for (int inner = 0; inner < 12; ++inner) {
+          if (threadIdx.x == 0) inner_rot = 0;
+          __syncthreads();
+          for (int ir = 0; ir < wtp - 1; ++ir) {
+            for (int q = warp; q < wtp / 2; q += BW) {
+              int a = rr_idx(q, ir, wtp), b = rr_idx(wtp - 1 - q, ir, wtp);
+              if (a >= wt || b >= wt) continue;
+              if (a > b) { int tt = a; a = b; b = tt; }
+              double* ua = Ub + (size_t)a * m;
+              double* ub = Ub + (size_t)b * m;
+              double al = 0, be = 0, ga = 0;
+              for (int i = lane; i < m; i += 32) {
+                double x = ua[i], y = ub[i];
+                al += x * x;
+                be += y * y;
+                ga += x * y;
+              }
+              al = wsum(al);
+              be = wsum(be);
+              ga = wsum(ga);
+              if (ga == 0.0 || !(fabs(ga) > tol * sqrt(al * be))) continue;
+              double zeta = (be - al) / (2.0 * ga);
+              double tt = copysign(1.0, zeta) / (fabs(zeta) + sqrt(1.0 + zeta * zeta));
+              double c = 1.0 / sqrt(1.0 + tt * tt), s = c * tt;
+              for (int i = lane; i < m; i += 32) {
+                double x = ua[i], y = ub[i];
+                ua[i] = c * x - s * y;
+                ub[i] = s * x + c * y;
+              }
+              if (lane < wt) {
+                double x = W[lane + a * BJ2], y = W[lane + b * BJ2];
+                W[lane + a * BJ2] = c * x - s * y;
+                W[lane + b * BJ2] = s * x + c * y;
+              }
+              if (lane == 0) inner_rot = 1;
+            }
+            __syncthreads();
+          }
+          bool rot = inner_rot != 0;
+          __syncthreads();
+          if (!rot) break;
+          any = true;
+        }
+        if (any) {
+          if (threadIdx.x == 0) atomicAdd(cnt, 1);
+          for (int e = threadIdx.x; e < wt * m; e += BT) {
+            int k = e / m, i = e % m;
+            int gc = k < w1 ? c0 + k : c1 + (k - w1);
+            P.U[i + (size_t)gc * m] = Ub[i + (size_t)k * m];
+          }
+          // V[:, cols] <- V[:, cols] W : one warp per row, lane c owns output column c
+          for (int i = warp; i < P.n; i += BW) {
+            double vi = 0;
+            if (lane < wt) {
+              int gc = lane < w1 ? c0 + lane : c1 + (lane - w1);
+              vi = P.V[i + (size_t)gc * P.n];
+            }
+            double out = 0;
+            for (int k = 0; k < wt; ++k) {
+              double vk = __shfl_sync(0xffffffffu, vi, k);
+              if (lane < wt) out += vk * W[k + lane * BJ2];
+            }
+            if (lane < wt) {
+              int gc = lane < w1 ? c0 + lane : c1 + (lane - w1);
+              P.V[i + (size_t)gc * P.n] = out;
+            }
+          }
+        }
+        __syncthreads();
+      }
+      grid_barrier(bar, flag);
+    }
+    int rot = *(volatile int*)cnt;
+    if (rot == 0) {
+      converged = true;
+      break;
+    }
+  }
+  if (blockIdx.x == 0 && threadIdx.x == 0) {
+    if (!converged) atomicOr(flag, FLAG_CONV);
+    atomicMax(sweeps_out, sweep + 1);
+    atomicMax(flag + 1, sweep + 1);
+  }
+  // singular values, order, outputs (as in jacobi_coop_kernel)
+  const int gw = blockIdx.x * BW + warp, TW = gridDim.x * BW;
   for (int pi = 0; pi < nprob; ++pi) {
     const JacProb P = probs[pi];
     for (int c = gw; c < P.n; c += TW) {
@@ -575,10 +764,44 @@ void svd_big(Engine& E, const std::vector<MatDesc>& d) {
     max_rounds = std::max(max_rounds, np - 1);
     ps.push_back(P);
   }
+  int mmax = 0;
+  for (auto& x : d) mmax = std::max(mmax, x.m);
+  size_t bsmem = sizeof(double) * ((size_t)BJ2 * BJ2 + (size_t)mmax * BJ2);
+  const bool blocked = bsmem <= 200 * 1024;
+  if (blocked) {
+    int bpairs = 0, brounds = 0;
+    for (auto& P : ps) {
+      int nb = (P.n + BJW - 1) / BJW;
+      int nbp = nb + (nb & 1);
+      P.pair_base = bpairs;
+      bpairs += nbp / 2;
+      brounds = std::max(brounds, nbp - 1);
+    }
+    pairs = bpairs;
+    max_rounds = brounds;
+  }
   Buf pb = E.alloc(sizeof(JacProb) * ps.size());
   E.stage(ps.data(), sizeof(JacProb) * ps.size(), pb->ptr);
-  Buf bb = E.alloc(sizeof(unsigned) * 2 + sizeof(int) * 4);
-  SPS_CUDA(cudaMemsetAsync(bb->ptr, 0, sizeof(unsigned) * 2 + sizeof(int) * 4, E.stream));
+  Buf bb = E.alloc(sizeof(unsigned) * 2 + sizeof(int) * 6);
+  SPS_CUDA(cudaMemsetAsync(bb->ptr, 0, sizeof(unsigned) * 2 + sizeof(int) * 6, E.stream));
+  if (blocked) {
+    SPS_CUDA(cudaFuncSetAttribute((const void*)bjacobi_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                  (int)bsmem));
+    int per_sm = 0;
+    SPS_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, (const void*)bjacobi_kernel, BT, bsmem));
+    int G = std::min({E.num_sms * std::max(1, per_sm), std::max(1, pairs)});
+    const JacProb* dp = (const JacProb*)pb->ptr;
+    int nprob = (int)ps.size();
+    unsigned* bar = (unsigned*)bb->ptr;
+    int* counters = (int*)(bar + 2);
+    int* sweeps = counters + 4;
+    void* args[] = {&dp, &nprob, &pairs, &max_rounds, &bar, &counters, &E.dflag, &sweeps};
+    int tk = E.tic("svd_block_jacobi");
+    SPS_CUDA(cudaLaunchCooperativeKernel((const void*)bjacobi_kernel, dim3(G), dim3(BT), args, bsmem, E.stream));
+    E.toc(tk);
+    E.launches++;
+    return;
+  }
   int maxg = coop_blocks((const void*)jacobi_coop_kernel, BT, 0, E);
   int G = std::min({E.num_sms, maxg, std::max(1, (pairs + BW - 1) / BW)});
   const JacProb* dp = (const JacProb*)pb->ptr;

@@ -4,6 +4,7 @@
 #include "pipeline.h"
 #include <cstdio>
 #include <cstring>
+#include <algorithm>
 #include <memory>
 #include <unordered_map>
 
@@ -162,6 +163,94 @@ int sps_timer_stop(sps_handle* h, double* ms) {
     SPS_CUDA(cudaEventSynchronize(h->t1));
     float f = 0;
     SPS_CUDA(cudaEventElapsedTime(&f, h->t0, h->t1));
+    if (ms) *ms = f;
+  });
+}
+
+static double* dev_copy(Engine& E, Buf& b, const double* h, size_t n) {
+  b = E.alloc(sizeof(double) * std::max<size_t>(n, 1));
+  SPS_CUDA(cudaMemcpyAsync(b->ptr, h, sizeof(double) * n, cudaMemcpyHostToDevice, E.stream));
+  return (double*)b->ptr;
+}
+
+int sps_la_svd(sps_handle* h, int32_t m, int32_t n, const double* a, double* u, double* s, double* vt,
+               int32_t* sweeps, double* ms) {
+  return guarded(h, [&] {
+    Engine& E = *h->E;
+    if (m < 1 || n < 1) throw Error(SPS_ERR_ARGUMENT, "empty matrix");
+    bool tall = m >= n;
+    int mm = tall ? m : n, nn = tall ? n : m;
+    std::vector<double> at;
+    const double* src = a;
+    if (!tall) {   // work on a^T
+      at.resize((size_t)m * n);
+      for (int i = 0; i < m; ++i)
+        for (int j = 0; j < n; ++j) at[j + (size_t)i * n] = a[i + (size_t)j * m];
+      src = at.data();
+    }
+    Buf ba, bq, br, bs;
+    double* da = dev_copy(E, ba, src, (size_t)mm * nn);
+    bq = E.alloc(sizeof(double) * (size_t)mm * nn);
+    br = E.alloc(sizeof(double) * (size_t)nn * nn);
+    bs = E.alloc(sizeof(double) * nn);
+    la::MatDesc d{da, (double*)bq->ptr, (double*)br->ptr, (double*)bs->ptr, mm, nn, mm, mm, nn};
+    SPS_CUDA(cudaMemsetAsync(E.dflag + 1, 0, sizeof(int), E.stream));
+    if (!h->t0) {
+      SPS_CUDA(cudaEventCreate(&h->t0));
+      SPS_CUDA(cudaEventCreate(&h->t1));
+    }
+    SPS_CUDA(cudaEventRecord(h->t0, E.stream));
+    if (la::svd_is_big(mm, nn)) la::svd_big(E, {d});
+    else la::svd_batched(E, {d});
+    SPS_CUDA(cudaEventRecord(h->t1, E.stream));
+    std::vector<double> U((size_t)mm * nn), V((size_t)nn * nn), S(nn);
+    SPS_CUDA(cudaMemcpyAsync(U.data(), d.q, U.size() * 8, cudaMemcpyDeviceToHost, E.stream));
+    SPS_CUDA(cudaMemcpyAsync(V.data(), d.r, V.size() * 8, cudaMemcpyDeviceToHost, E.stream));
+    SPS_CUDA(cudaMemcpyAsync(S.data(), d.s, S.size() * 8, cudaMemcpyDeviceToHost, E.stream));
+    int sw = 0;
+    SPS_CUDA(cudaMemcpyAsync(&sw, E.dflag + 1, sizeof(int), cudaMemcpyDeviceToHost, E.stream));
+    E.sync();
+    float f = 0;
+    SPS_CUDA(cudaEventElapsedTime(&f, h->t0, h->t1));
+    E.check_flag("sps_la_svd");
+    if (ms) *ms = f;
+    if (sweeps) *sweeps = sw;
+    int k = nn;
+    if (s) std::copy(S.begin(), S.end(), s);
+    // a = U S V^T (tall) ; a^T = U S V^T -> a = V S U^T (wide)
+    for (int l = 0; l < k; ++l) {
+      for (int i = 0; i < m; ++i)
+        if (u) u[i + (size_t)l * m] = tall ? U[i + (size_t)l * mm] : V[i + (size_t)l * nn];
+      for (int j = 0; j < n; ++j)
+        if (vt) vt[l + (size_t)j * k] = tall ? V[j + (size_t)l * nn] : U[j + (size_t)l * mm];
+    }
+  });
+}
+
+int sps_la_qr(sps_handle* h, int32_t m, int32_t n, const double* a, double* q, double* r, double* ms) {
+  return guarded(h, [&] {
+    Engine& E = *h->E;
+    if (m < 1 || n < 1) throw Error(SPS_ERR_ARGUMENT, "empty matrix");
+    int k = std::min(m, n);
+    Buf ba, bq, br, bs;
+    double* da = dev_copy(E, ba, a, (size_t)m * n);
+    bq = E.alloc(sizeof(double) * (size_t)m * k);
+    br = E.alloc(sizeof(double) * (size_t)k * n);
+    bs = E.alloc(sizeof(double) * k);
+    if (!h->t0) {
+      SPS_CUDA(cudaEventCreate(&h->t0));
+      SPS_CUDA(cudaEventCreate(&h->t1));
+    }
+    SPS_CUDA(cudaEventRecord(h->t0, E.stream));
+    if (la::qr_is_big(m, n)) la::qr_big(E, da, m, n, m, (double*)bq->ptr, m, (double*)br->ptr, k);
+    else la::qr_batched(E, {la::MatDesc{da, (double*)bq->ptr, (double*)br->ptr, (double*)bs->ptr, m, n, m, m, k}});
+    SPS_CUDA(cudaEventRecord(h->t1, E.stream));
+    SPS_CUDA(cudaMemcpyAsync(q, bq->ptr, sizeof(double) * (size_t)m * k, cudaMemcpyDeviceToHost, E.stream));
+    SPS_CUDA(cudaMemcpyAsync(r, br->ptr, sizeof(double) * (size_t)k * n, cudaMemcpyDeviceToHost, E.stream));
+    E.sync();
+    float f = 0;
+    SPS_CUDA(cudaEventElapsedTime(&f, h->t0, h->t1));
+    E.check_flag("sps_la_qr");
     if (ms) *ms = f;
   });
 }

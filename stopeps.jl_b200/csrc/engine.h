@@ -120,6 +120,7 @@ class Engine {
   void sync();
   // device-side error flag written by kernels (nonfinite values, iteration caps)
   int* dflag = nullptr;
+  // dflag[1]: largest Jacobi sweep count since the last reset (diagnostic)
   void check_flag(const char* where);
 
   // pinned scalar scratch

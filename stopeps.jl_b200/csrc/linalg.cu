@@ -183,7 +183,9 @@ __global__ void __launch_bounds__(NT) svd_kernel(const MatDesc* ds, double* work
     converged = (rotations == 0);
     __syncthreads();
   }
-  if (!converged && threadIdx.x == 0) atomicOr(flag, FLAG_CONVERGENCE);
+  if (threadIdx.x == 0) {
+    if (!converged) atomicOr(flag, FLAG_CONVERGENCE);
+  }
   // singular values and descending order (stable by index)
   for (int c = warp; c < n; c += NW) {
     const double* uc = U + (size_t)c * lda;

@@ -91,6 +91,32 @@ class Engine:
         self.check(self.lib.sps_timer_stop(self.h, C.byref(ms)))
         return ms.value
 
+    def la_svd(self, a):
+        """Engine SVD of one host matrix: (u, s, vt, sweeps, device_ms)."""
+        a = np.asfortranarray(np.asarray(a, np.float64))
+        m, n = a.shape
+        k = min(m, n)
+        u = np.zeros((m, k), order="F")
+        s = np.zeros(k)
+        vt = np.zeros((k, n), order="F")
+        sw = C.c_int32()
+        ms = C.c_double()
+        self.check(self.lib.sps_la_svd(self.h, m, n, _arr(a, C.c_double), _arr(u, C.c_double), _arr(s, C.c_double),
+                                       _arr(vt, C.c_double), C.byref(sw), C.byref(ms)))
+        return u, s, vt, sw.value, ms.value
+
+    def la_qr(self, a):
+        """Engine Householder QR of one host matrix: (q, r, device_ms)."""
+        a = np.asfortranarray(np.asarray(a, np.float64))
+        m, n = a.shape
+        k = min(m, n)
+        q = np.zeros((m, k), order="F")
+        r = np.zeros((k, n), order="F")
+        ms = C.c_double()
+        self.check(self.lib.sps_la_qr(self.h, m, n, _arr(a, C.c_double), _arr(q, C.c_double), _arr(r, C.c_double),
+                                      C.byref(ms)))
+        return q, r, ms.value
+
     def close(self):
         if getattr(self, "h", None):
             self.lib.sps_destroy(self.h)

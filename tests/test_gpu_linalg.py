@@ -1,0 +1,49 @@
+"""The engine's dense factorization kernels against NumPy/LAPACK (FP64).
+
+Householder QR (single-CTA and blocked multi-CTA) and one-sided Jacobi SVD
+(single-CTA, cooperative element-pair and block variants) must reproduce the
+factorizations to roundoff: A = QR with orthonormal Q, and the singular
+values of LAPACK gesdd with orthonormal singular vectors.
+"""
+import numpy as np
+import pytest
+
+pytestmark = pytest.mark.gpu
+
+
+@pytest.fixture(scope="module")
+def eng(sps):
+    return sps.Engine(2, 2)
+
+
+def graded(m, n, decay, seed):
+    rng = np.random.default_rng(seed)
+    u, _ = np.linalg.qr(rng.standard_normal((m, min(m, n))))
+    v, _ = np.linalg.qr(rng.standard_normal((n, min(m, n))))
+    s = np.exp(-decay * np.arange(min(m, n)))
+    return (u * s) @ v.T
+
+
+@pytest.mark.parametrize("m,n", [(40, 30), (30, 40), (200, 190), (700, 650), (648, 648), (900, 200)])
+@pytest.mark.parametrize("decay", [0.0, 0.05])
+def test_svd_matches_lapack(eng, m, n, decay):
+    a = graded(m, n, decay, m + n) if decay else np.random.default_rng(m * n).standard_normal((m, n))
+    u, s, vt, sweeps, ms = eng.la_svd(a)
+    ref = np.linalg.svd(a, compute_uv=False)
+    np.testing.assert_allclose(s, ref, rtol=1e-12, atol=1e-13 * ref[0])
+    k = min(m, n)
+    np.testing.assert_allclose(u.T @ u, np.eye(k), atol=1e-12)
+    np.testing.assert_allclose(vt @ vt.T, np.eye(k), atol=1e-12)
+    np.testing.assert_allclose((u * s) @ vt, a, atol=1e-12 * ref[0])
+
+
+@pytest.mark.parametrize("m,n", [(50, 20), (20, 50), (2048, 128), (5000, 300), (23328, 96)])
+def test_qr_matches_lapack(eng, m, n):
+    a = np.random.default_rng(m + 7 * n).standard_normal((m, n))
+    q, r, ms = eng.la_qr(a)
+    k = min(m, n)
+    np.testing.assert_allclose(q @ r, a, atol=1e-12 * np.abs(a).max() * np.sqrt(n))
+    np.testing.assert_allclose(q.T @ q, np.eye(k), atol=1e-12)
+    assert np.allclose(np.triu(r), r)
+    rr = np.linalg.qr(a, mode="r")
+    np.testing.assert_allclose(np.abs(np.diag(r)), np.abs(np.diag(rr)), rtol=1e-10)
