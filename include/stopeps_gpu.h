@@ -120,6 +120,21 @@ int sps_la_svd(sps_handle* h, int32_t m, int32_t n, const double* a, double* u, 
                int32_t* sweeps, double* ms);
 int sps_la_qr(sps_handle* h, int32_t m, int32_t n, const double* a, double* q, double* r, double* ms);
 
+/* No counterpart in the reference.  The one-sided Jacobi SVD of one small
+ * matrix for callers that cannot allocate device memory (no cudaMalloc /
+ * cudaFree / allocating library call is made): a (m x n), u (m x k),
+ * s (k) and vt (k x n) are column-major DEVICE buffers of the caller,
+ * k = min(m,n), a = u diag(s) vt with s descending.  All scratch is one
+ * fixed file-scope device array (max(m,n) <= 256, min(m,n) <= 128; larger
+ * sizes return SPS_ERR_ARGUMENT) shared by every call on the device: calls
+ * whose kernels overlap on the GPU race, so serialise them.  The first call
+ * on a device looks up the array's device address; make it before any
+ * stream capture.  Runs on `stream` (a cudaStream_t, NULL = default) and
+ * synchronizes it before returning; SPS_ERR_CONVERGENCE if Jacobi did not
+ * converge. */
+int sps_la_svd_noalloc(int32_t device, void* stream, int32_t m, int32_t n, const double* a, double* u,
+                       double* s, double* vt);
+
 /* --- states: FiniteState (src/states/finite.jl:27-49) ---------------------
  * Site tensors have legs (W,N,Pout,Paux,E,S); each leg is described by its
  * even and odd multiplicities (n0,n1), even states first.  leg_dims holds
