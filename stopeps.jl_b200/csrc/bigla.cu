@@ -42,28 +42,30 @@ __device__ double bsum(double v, double* red) {
   return red[BW];
 }
 
-// bar[0] = arrival count, bar[1] = generation.  Bounded spin (~seconds).
+// bar[0] = arrival count, bar[1] = generation.  Acquire/release ordering at
+// gpu scope; the spin is bounded (a fault is the only way to reach the cap,
+// since every CTA of a cooperative launch is co-resident).
 __device__ void grid_barrier(unsigned* bar, int* flag) {
   __syncthreads();
   if (threadIdx.x == 0) {
-    volatile unsigned* gen = bar + 1;
-    unsigned g = *gen;
-    __threadfence();
-    unsigned arrived = atomicAdd(bar, 1u);
+    unsigned g;
+    asm volatile("ld.acquire.gpu.u32 %0, [%1];" : "=r"(g) : "l"(bar + 1) : "memory");
+    unsigned arrived;
+    asm volatile("atom.add.acq_rel.gpu.u32 %0, [%1], 1;" : "=r"(arrived) : "l"(bar) : "memory");
     if (arrived == gridDim.x - 1) {
-      atomicExch(bar, 0u);
-      __threadfence();
-      atomicAdd(bar + 1, 1u);
+      asm volatile("st.relaxed.gpu.u32 [%0], 0;" ::"l"(bar) : "memory");
+      asm volatile("red.release.gpu.add.u32 [%0], 1;" ::"l"(bar + 1) : "memory");
     } else {
       long long spins = 0;
-      while (*gen == g) {
-        if (++spins > (1ll << 27)) {   // ~seconds: every CTA is co-resident, so only a fault gets here
+      unsigned cur;
+      do {
+        asm volatile("ld.acquire.gpu.u32 %0, [%1];" : "=r"(cur) : "l"(bar + 1) : "memory");
+        if (++spins > (1ll << 27)) {
           atomicOr(flag, FLAG_BARRIER);
           break;
         }
-      }
+      } while (cur == g);
     }
-    __threadfence();
   }
   __syncthreads();
 }
@@ -204,9 +206,10 @@ struct PanelArgs {
 };
 
 __global__ void __launch_bounds__(BT) panel_qr_kernel(PanelArgs p) {
-  extern __shared__ double sm[];   // rpc x jb, row-major in shared memory
+  extern __shared__ double sm[];   // panel rows of this CTA, column-major: sm[c * ld + r]
   __shared__ double red[BW + 1];
   const int jb = p.jb;
+  const int ld = p.rpc;
   const int r0 = p.j0 + blockIdx.x * p.rpc;
   const int r1 = min(p.m, r0 + p.rpc);
   const int nr = max(0, r1 - r0);
@@ -216,23 +219,21 @@ __global__ void __launch_bounds__(BT) panel_qr_kernel(PanelArgs p) {
   double* gram = accw + jb * jb;
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
   for (int e = threadIdx.x; e < nr * jb; e += BT) {
-    int r = e / jb, c = e % jb;
-    sm[e] = p.A[(size_t)(r0 + r) + (size_t)(p.j0 + c) * p.lda];
+    int c = e / nr, r = e % nr;
+    sm[c * ld + r] = p.A[(size_t)(r0 + r) + (size_t)(p.j0 + c) * p.lda];
   }
   __syncthreads();
   for (int jj = 0; jj < jb; ++jj) {
     const int j = p.j0 + jj;
     const bool owner = (j >= r0 && j < r1);
+    const int rs = max(0, j + 1 - r0);   // first local row strictly below the pivot
+    double* cj = sm + jj * ld;
     double part = 0;
-    for (int r = threadIdx.x; r < nr; r += BT)
-      if (r0 + r > j) {
-        double x = sm[r * jb + jj];
-        part += x * x;
-      }
+    for (int r = rs + threadIdx.x; r < nr; r += BT) part += cj[r] * cj[r];
     part = bsum(part, red);
     if (threadIdx.x == 0) {
       if (part != 0.0) atomicAdd(&accn[jj], part);
-      if (owner) alph[jj] = sm[(j - r0) * jb + jj];
+      if (owner) alph[jj] = cj[j - r0];
     }
     grid_barrier(p.bar, p.flag);
     const double sumsq = __ldcg(&accn[jj]);
@@ -245,49 +246,47 @@ __global__ void __launch_bounds__(BT) panel_qr_kernel(PanelArgs p) {
     }
     if (blockIdx.x == 0 && threadIdx.x == 0) p.tau[j] = tau;
     if (tau != 0.0) {
-      for (int r = threadIdx.x; r < nr; r += BT)
-        if (r0 + r > j) sm[r * jb + jj] *= scal;
-      if (owner && threadIdx.x == 0) sm[(j - r0) * jb + jj] = beta;
+      for (int r = rs + threadIdx.x; r < nr; r += BT) cj[r] *= scal;
+      if (owner && threadIdx.x == 0) cj[j - r0] = beta;
       __syncthreads();
       for (int kk = jj + 1 + warp; kk < jb; kk += BW) {
+        const double* ck = sm + kk * ld;
         double w = 0;
-        for (int r = lane; r < nr; r += 32) {
-          int gr = r0 + r;
-          if (gr > j) w += sm[r * jb + jj] * sm[r * jb + kk];
-          else if (gr == j) w += sm[r * jb + kk];
-        }
+        for (int r = rs + lane; r < nr; r += 32) w += cj[r] * ck[r];
+        if (owner && lane == 0) w += ck[j - r0];
         w = wsum(w);
         if (lane == 0 && w != 0.0) atomicAdd(&accw[jj * jb + kk], w);
       }
       grid_barrier(p.bar, p.flag);
       for (int kk = jj + 1 + warp; kk < jb; kk += BW) {
-        double w = __ldcg(&accw[jj * jb + kk]) * tau;
-        for (int r = lane; r < nr; r += 32) {
-          int gr = r0 + r;
-          if (gr > j) sm[r * jb + kk] -= sm[r * jb + jj] * w;
-          else if (gr == j) sm[r * jb + kk] -= w;
-        }
+        double* ck = sm + kk * ld;
+        const double w = __ldcg(&accw[jj * jb + kk]) * tau;
+        for (int r = rs + lane; r < nr; r += 32) ck[r] -= cj[r] * w;
+        if (owner && lane == 0) ck[j - r0] -= w;
       }
     }
     __syncthreads();
   }
-  // write back, explicit V and partial Gram V^T V
+  // write back, explicit V, partial Gram V^T V
   for (int e = threadIdx.x; e < nr * jb; e += BT) {
-    int r = e / jb, c = e % jb;
+    int c = e / nr, r = e % nr;
     int gr = r0 + r, gc = p.j0 + c;
-    double x = sm[e];
+    double x = sm[c * ld + r];
     p.A[(size_t)gr + (size_t)gc * p.lda] = x;
     double v = gr < gc ? 0.0 : (gr == gc ? 1.0 : x);
     p.V[(size_t)gr + (size_t)gc * p.m] = v;
-    sm[e] = v;
+    sm[c * ld + r] = v;
   }
   __syncthreads();
-  for (int e = threadIdx.x; e < jb * jb; e += BT) {
-    int a = e / jb, b = e % jb;
+  for (int pr = warp; pr < jb * jb; pr += BW) {
+    int a = pr / jb, b = pr % jb;
     if (b < a) continue;
+    const double* ca = sm + a * ld;
+    const double* cb = sm + b * ld;
     double s = 0;
-    for (int r = 0; r < nr; ++r) s += sm[r * jb + a] * sm[r * jb + b];
-    if (s != 0.0) atomicAdd(&gram[a * jb + b], s);
+    for (int r = lane; r < nr; r += 32) s += ca[r] * cb[r];
+    s = wsum(s);
+    if (lane == 0 && s != 0.0) atomicAdd(&gram[a * jb + b], s);
   }
   grid_barrier(p.bar, p.flag);
   if (blockIdx.x == 0 && threadIdx.x == 0) {
@@ -316,6 +315,10 @@ static int coop_blocks(const void* kernel, int threads, size_t smem, Engine& E) 
 
 // Householder QR of a (m x n, col-major lda), m >= n: q (m x n, ldq), r (n x n, ldr).
 void qr_big(Engine& E, double* a, int m, int n, int lda, double* q, int ldq, double* r, int ldr) {
+  qr_big_opt(E, a, m, n, lda, q, ldq, r, ldr, true);
+}
+
+void qr_big_opt(Engine& E, double* a, int m, int n, int lda, double* q, int ldq, double* r, int ldr, bool form_q) {
   const int jb_max = 32;
   const int np = (n + jb_max - 1) / jb_max;
   Buf vb = E.alloc(sizeof(double) * (size_t)m * n);
@@ -374,7 +377,8 @@ void qr_big(Engine& E, double* a, int m, int n, int lda, double* q, int ldq, dou
     }
   }
   // R (upper triangle of a) and Q = H_1 ... H_np [I; 0]
-  copy_upper_and_identity(E, a, m, n, lda, r, ldr, q, ldq);
+  copy_upper_and_identity(E, a, m, n, lda, r, ldr, form_q ? q : nullptr, ldq);
+  if (!form_q) return;
   for (int pi = np - 1; pi >= 0; --pi) {
     int j0 = pi * jb_max, jb = std::min(jb_max, n - j0);
     int mrows = m - j0, nc = n - j0;
@@ -393,7 +397,7 @@ __global__ void upper_identity_kernel(const double* a, int m, int n, int lda, do
     if (e < tr) {
       int i = (int)(e % n), j = (int)(e / n);
       r[i + (size_t)j * ldr] = i <= j ? a[i + (size_t)j * lda] : 0.0;
-    } else {
+    } else if (q) {
       size_t f = e - tr;
       int i = (int)(f % m), j = (int)(f / m);
       q[i + (size_t)j * ldq] = i == j ? 1.0 : 0.0;
@@ -403,7 +407,7 @@ __global__ void upper_identity_kernel(const double* a, int m, int n, int lda, do
 
 void copy_upper_and_identity(Engine& E, const double* a, int m, int n, int lda, double* r, int ldr, double* q,
                              int ldq) {
-  size_t total = (size_t)n * n + (size_t)m * n;
+  size_t total = (size_t)n * n + (q ? (size_t)m * n : 0);
   int g = (int)std::min<size_t>((total + 255) / 256, 8192);
   upper_identity_kernel<<<g, 256, 0, E.stream>>>(a, m, n, lda, r, ldr, q, ldq);
   SPS_CUDA(cudaGetLastError());
@@ -732,6 +736,236 @@ __global__ void __launch_bounds__(BT) bjacobi_kernel(const JacProb* probs, int n
       for (int i = lane; i < P.n; i += 32) ro[i] = vc[i];
     }
   }
+}
+
+// ---------------------------------------------------------------------------
+// U-only one-sided Jacobi: rotates the columns of X (m x n, ld m) until they
+// are orthogonal, then writes the normalized columns sorted by descending
+// norm (the left singular vectors of X) and the norms (singular values).
+// No right factor is accumulated: callers recover what they need by one GEMM
+// with the original matrix.  One warp per column pair, the pair's two columns
+// held in registers; a grid barrier between rounds.
+// ---------------------------------------------------------------------------
+static constexpr int JR = 24;   // registers per lane per column: m <= 32*JR
+
+struct JUProb {
+  double* X;      // m x n (ld m), rotated in place
+  double* q;      // output: sorted normalized columns (m x n, ld m)
+  double* s;      // output: sorted norms (n)
+  double* sig;    // scratch n
+  int* rank;      // scratch n
+  int m, n;
+  int pair_base;
+};
+
+template <bool REG>
+__global__ void __launch_bounds__(BT) jacobi_u_kernel(const JUProb* probs, int nprob, int total_pairs,
+                                                      int max_rounds, unsigned* bar, int* counters, int* flag) {
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  const int gw = blockIdx.x * BW + warp, TW = gridDim.x * BW;
+  if (blockIdx.x == 0 && threadIdx.x == 0) {
+    counters[0] = 0;
+    counters[1] = 0;
+    counters[2] = 0;
+  }
+  grid_barrier(bar, flag);
+  const int MAXSWEEP = 80;
+  bool converged = false;
+  int sweep = 0;
+  for (; sweep < MAXSWEEP; ++sweep) {
+    int* cnt = counters + (sweep % 3);
+    if (blockIdx.x == 0 && threadIdx.x == 0) counters[(sweep + 1) % 3] = 0;
+    for (int round = 0; round < max_rounds; ++round) {
+      for (int t = gw; t < total_pairs; t += TW) {
+        int pi = 0;
+        while (pi + 1 < nprob && t >= probs[pi + 1].pair_base) ++pi;
+        const JUProb& P = probs[pi];
+        const int np = P.n + (P.n & 1);
+        if (round >= np - 1) continue;
+        const int pr = t - P.pair_base;
+        int p = rr_idx(pr, round, np), qd = rr_idx(np - 1 - pr, round, np);
+        if (p >= P.n || qd >= P.n) continue;
+        if (p > qd) { int tt = p; p = qd; qd = tt; }
+        double* up = P.X + (size_t)p * P.m;
+        double* uq = P.X + (size_t)qd * P.m;
+        const int m = P.m;
+        const double tol = DBL_EPSILON * (double)max(m, 2);
+        if (REG) {
+          double x[JR], y[JR];
+          double al = 0, be = 0, ga = 0;
+#pragma unroll
+          for (int k = 0; k < JR; ++k) {
+            int i = lane + 32 * k;
+            x[k] = i < m ? up[i] : 0.0;
+            y[k] = i < m ? uq[i] : 0.0;
+            al += x[k] * x[k];
+            be += y[k] * y[k];
+            ga += x[k] * y[k];
+          }
+          al = wsum(al);
+          be = wsum(be);
+          ga = wsum(ga);
+          if (ga == 0.0 || !(fabs(ga) > tol * sqrt(al * be))) continue;
+          double zeta = (be - al) / (2.0 * ga);
+          double tt = copysign(1.0, zeta) / (fabs(zeta) + sqrt(1.0 + zeta * zeta));
+          double c = 1.0 / sqrt(1.0 + tt * tt), sn = c * tt;
+#pragma unroll
+          for (int k = 0; k < JR; ++k) {
+            int i = lane + 32 * k;
+            if (i < m) {
+              up[i] = c * x[k] - sn * y[k];
+              uq[i] = sn * x[k] + c * y[k];
+            }
+          }
+        } else {
+          double al = 0, be = 0, ga = 0;
+          for (int i = lane; i < m; i += 32) {
+            double a = up[i], b = uq[i];
+            al += a * a;
+            be += b * b;
+            ga += a * b;
+          }
+          al = wsum(al);
+          be = wsum(be);
+          ga = wsum(ga);
+          if (ga == 0.0 || !(fabs(ga) > tol * sqrt(al * be))) continue;
+          double zeta = (be - al) / (2.0 * ga);
+          double tt = copysign(1.0, zeta) / (fabs(zeta) + sqrt(1.0 + zeta * zeta));
+          double c = 1.0 / sqrt(1.0 + tt * tt), sn = c * tt;
+          for (int i = lane; i < m; i += 32) {
+            double a = up[i], b = uq[i];
+            up[i] = c * a - sn * b;
+            uq[i] = sn * a + c * b;
+          }
+        }
+        if (lane == 0) atomicAdd(cnt, 1);
+      }
+      grid_barrier(bar, flag);
+    }
+    int rot = *(volatile int*)cnt;
+    if (rot == 0) {
+      converged = true;
+      break;
+    }
+  }
+  if (blockIdx.x == 0 && threadIdx.x == 0) {
+    if (!converged) atomicOr(flag, FLAG_CONV);
+    atomicMax(flag + 1, sweep + 1);
+  }
+  for (int pi = 0; pi < nprob; ++pi) {
+    const JUProb P = probs[pi];
+    for (int c = gw; c < P.n; c += TW) {
+      const double* uc = P.X + (size_t)c * P.m;
+      double v = 0;
+      for (int i = lane; i < P.m; i += 32) v += uc[i] * uc[i];
+      v = wsum(v);
+      if (lane == 0) P.sig[c] = sqrt(v);
+    }
+  }
+  grid_barrier(bar, flag);
+  for (int pi = 0; pi < nprob; ++pi) {
+    const JUProb P = probs[pi];
+    for (int c = blockIdx.x * BT + threadIdx.x; c < P.n; c += gridDim.x * BT) {
+      double sc = __ldcg(&P.sig[c]);
+      int rk = 0;
+      for (int j = 0; j < P.n; ++j) {
+        double sj = __ldcg(&P.sig[j]);
+        rk += (sj > sc) || (sj == sc && j < c);
+      }
+      P.rank[c] = rk;
+      P.s[rk] = sc;
+    }
+  }
+  grid_barrier(bar, flag);
+  for (int pi = 0; pi < nprob; ++pi) {
+    const JUProb P = probs[pi];
+    for (int c = gw; c < P.n; c += TW) {
+      int rk = __ldcg(&P.rank[c]);
+      double sc = __ldcg(&P.sig[c]);
+      double inv = sc > 0 ? 1.0 / sc : 0.0;
+      const double* uc = P.X + (size_t)c * P.m;
+      double* qo = P.q + (size_t)rk * P.m;
+      for (int i = lane; i < P.m; i += 32) qo[i] = uc[i] * inv;
+    }
+  }
+}
+
+// problems: (x = m x n ld m rotated in place, q = sorted left vectors m x n ld m, s = values n)
+void jacobi_left(Engine& E, const std::vector<MatDesc>& d) {
+  if (d.empty()) return;
+  std::vector<JUProb> ps;
+  int pairs = 0, max_rounds = 0, mmax = 0;
+  size_t ws = 0;
+  for (auto& x : d) ws += 2 * (size_t)x.n + 8;
+  Buf wb = E.alloc(sizeof(double) * ws);
+  double* w = (double*)wb->ptr;
+  for (auto& x : d) {
+    JUProb P;
+    P.X = x.a;
+    P.q = x.q;
+    P.s = x.s;
+    P.m = x.m;
+    P.n = x.n;
+    P.sig = w;
+    w += x.n;
+    P.rank = (int*)w;
+    w += x.n + 8;
+    P.pair_base = pairs;
+    int np = x.n + (x.n & 1);
+    pairs += np / 2;
+    max_rounds = std::max(max_rounds, np - 1);
+    mmax = std::max(mmax, x.m);
+    ps.push_back(P);
+  }
+  Buf pb = E.alloc(sizeof(JUProb) * ps.size());
+  E.stage(ps.data(), sizeof(JUProb) * ps.size(), pb->ptr);
+  Buf bb = E.alloc(sizeof(unsigned) * 2 + sizeof(int) * 4);
+  SPS_CUDA(cudaMemsetAsync(bb->ptr, 0, sizeof(unsigned) * 2 + sizeof(int) * 4, E.stream));
+  const bool reg = mmax <= 32 * JR;
+  const void* kfn = reg ? (const void*)jacobi_u_kernel<true> : (const void*)jacobi_u_kernel<false>;
+  int maxg = coop_blocks(kfn, BT, 0, E);
+  int G = std::min({E.num_sms, maxg, std::max(1, (pairs + BW - 1) / BW)});
+  const JUProb* dp = (const JUProb*)pb->ptr;
+  int nprob = (int)ps.size();
+  unsigned* bar = (unsigned*)bb->ptr;
+  int* counters = (int*)(bar + 2);
+  void* args[] = {&dp, &nprob, &pairs, &max_rounds, &bar, &counters, &E.dflag};
+  int tk = E.tic("svd_jacobi_left");
+  SPS_CUDA(cudaLaunchCooperativeKernel(kfn, dim3(G), dim3(BT), args, 0, E.stream));
+  E.toc(tk);
+  E.launches++;
+  if (E.profile) {
+    // algorithmic work: per sweep every column pair costs 3 dot products and a rotation (6m flops)
+    int sweeps = 0;
+    SPS_CUDA(cudaMemcpyAsync(&sweeps, E.dflag + 1, sizeof(int), cudaMemcpyDeviceToHost, E.stream));
+    E.sync();
+    SPS_CUDA(cudaMemsetAsync(E.dflag + 1, 0, sizeof(int), E.stream));
+    double fl = 0, by = 0;
+    for (auto& x : d) {
+      fl += 6.0 * x.m * 0.5 * x.n * (x.n - 1) * sweeps;
+      by += 32.0 * x.m * 0.5 * x.n * (x.n - 1) * sweeps / 2;   // each round reads and writes every column once
+    }
+    E.set_work(tk, fl, by);
+  }
+}
+
+__global__ void transpose_cm_kernel(const double* __restrict__ src, int m, int n, int lds, double* __restrict__ dst,
+                                    int ldd) {
+  size_t total = (size_t)m * n;
+  for (size_t e = blockIdx.x * (size_t)blockDim.x + threadIdx.x; e < total; e += (size_t)gridDim.x * blockDim.x) {
+    int i = (int)(e % m), j = (int)(e / m);
+    dst[j + (size_t)i * ldd] = src[i + (size_t)j * lds];
+  }
+}
+
+// dst (n x m, ld ldd) = src^T, src (m x n, ld lds), both column-major
+void transpose_cm(Engine& E, const double* src, int m, int n, int lds, double* dst, int ldd) {
+  size_t total = (size_t)m * n;
+  if (!total) return;
+  int g = (int)std::min<size_t>((total + 255) / 256, 8192);
+  transpose_cm_kernel<<<g, 256, 0, E.stream>>>(src, m, n, lds, dst, ldd);
+  SPS_CUDA(cudaGetLastError());
+  E.launches++;
 }
 
 // problems: (a = U in/out workspace m x n ld m, q out m x n ld m, r out n x n ld n, s out n)

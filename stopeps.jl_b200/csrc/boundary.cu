@@ -61,13 +61,28 @@ CompressReport compress_boundary(Engine& E, std::vector<Tensor>& B, const BMPS& 
       B[x - 1] = ein(E, "lpk,kr->lpr", B[x - 1], f.L);
     }
     for (int x = 0; x < N - 1; ++x) {
-      SVDres f = svd(E, B[x], {0, 1}, {2}, tr, ent != nullptr);
-      if (ent) ent->record(south_side, row_cut, x + 1, f.entropy);
-      max_error = std::max(max_error, f.norm == 0 ? 0.0 : (f.err / f.norm) * (f.err / f.norm));
-      B[x] = f.U;
-      std::vector<double> s(f.S[0]);
-      s.insert(s.end(), f.S[1].begin(), f.S[1].end());
-      Tensor R = scale_leg(E, f.V, 0, s);
+      Tensor U, R;
+      double err, nrm, entv;
+      if (svd_prefers_kept(B[x], {0, 1}, {2})) {
+        KeptSVD f = svd_kept(E, B[x], {0, 1}, {2}, tr, ent != nullptr, true);
+        U = f.F;
+        R = f.W;   // S V^T = U^T M
+        err = f.err;
+        nrm = f.norm;
+        entv = f.entropy;
+      } else {
+        SVDres f = svd(E, B[x], {0, 1}, {2}, tr, ent != nullptr);
+        std::vector<double> s(f.S[0]);
+        s.insert(s.end(), f.S[1].begin(), f.S[1].end());
+        U = f.U;
+        R = scale_leg(E, f.V, 0, s);
+        err = f.err;
+        nrm = f.norm;
+        entv = f.entropy;
+      }
+      if (ent) ent->record(south_side, row_cut, x + 1, entv);
+      max_error = std::max(max_error, nrm == 0 ? 0.0 : (err / nrm) * (err / nrm));
+      B[x] = U;
       B[x + 1] = ein(E, "lk,kpr->lpr", R, B[x + 1]);
     }
   } else {
@@ -77,13 +92,28 @@ CompressReport compress_boundary(Engine& E, std::vector<Tensor>& B, const BMPS& 
       B[x + 1] = ein(E, "lk,kpr->lpr", f.R, B[x + 1]);
     }
     for (int x = N - 1; x >= 1; --x) {
-      SVDres f = svd(E, B[x], {0}, {1, 2}, tr, ent != nullptr);
-      if (ent) ent->record(south_side, row_cut, x, f.entropy);
-      max_error = std::max(max_error, f.norm == 0 ? 0.0 : (f.err / f.norm) * (f.err / f.norm));
-      B[x] = f.V;
-      std::vector<double> s(f.S[0]);
-      s.insert(s.end(), f.S[1].begin(), f.S[1].end());
-      Tensor L = scale_leg(E, f.U, 1, s);
+      Tensor V, L;
+      double err, nrm, entv;
+      if (svd_prefers_kept(B[x], {0}, {1, 2})) {
+        KeptSVD f = svd_kept(E, B[x], {0}, {1, 2}, tr, ent != nullptr, false);
+        V = f.F;
+        L = f.W;   // U S = M V
+        err = f.err;
+        nrm = f.norm;
+        entv = f.entropy;
+      } else {
+        SVDres f = svd(E, B[x], {0}, {1, 2}, tr, ent != nullptr);
+        std::vector<double> s(f.S[0]);
+        s.insert(s.end(), f.S[1].begin(), f.S[1].end());
+        V = f.V;
+        L = scale_leg(E, f.U, 1, s);
+        err = f.err;
+        nrm = f.norm;
+        entv = f.entropy;
+      }
+      if (ent) ent->record(south_side, row_cut, x, entv);
+      max_error = std::max(max_error, nrm == 0 ? 0.0 : (err / nrm) * (err / nrm));
+      B[x] = V;
       B[x - 1] = ein(E, "lpk,kr->lpr", B[x - 1], L);
     }
   }

@@ -137,6 +137,7 @@ class Engine {
   bool profile = false;
   int tic(const char* name);
   void toc(int id, double algorithmic_flops = 0, double algorithmic_bytes = 0);
+  void set_work(int id, double algorithmic_flops, double algorithmic_bytes = 0);
   struct KStat { double ms = 0, flops = 0, bytes = 0; long long count = 0; };
   std::map<std::string, KStat> kernel_stats();
   void reset_stats();
@@ -194,6 +195,19 @@ struct SVDres {
 };
 SVDres svd(Engine& E, const Tensor& A, const std::vector<int>& rows, const std::vector<int>& cols,
            const Trunc& tr, bool want_entropy = false);
+// Truncated SVD returning one orthonormal factor and the product of the other
+// with the singular values, computed from the original matrix by one GEMM:
+//  left  = true : F = U (rows..., new),  W = S V^T = U^T A  (new, cols...)
+//  left  = false: F = V^T (new, cols...), W = U S = A V     (rows..., new)
+// Large blocks: QR/LQ preconditioning + U-only Jacobi (multi-CTA).
+struct KeptSVD {
+  Tensor F, W;
+  std::vector<double> S[2];
+  double err = 0, entropy = 0, norm = 0;
+};
+KeptSVD svd_kept(Engine& E, const Tensor& A, const std::vector<int>& rows, const std::vector<int>& cols,
+                 const Trunc& tr, bool want_entropy, bool left);
+bool svd_prefers_kept(const Tensor& A, const std::vector<int>& rows, const std::vector<int>& cols);
 // eigendecomposition of a symmetric block matrix (rows | cols must match)
 struct EIGres {
   std::vector<double> w[2];   // eigenvalues (ascending) per block
@@ -225,6 +239,10 @@ void eigh_batched(Engine& E, const std::vector<MatDesc>& d);   // symmetric n x 
 void inv_batched(Engine& E, const std::vector<MatDesc>& d);    // general square
 // multi-CTA versions for large blocks (bigla.cu)
 void qr_big(Engine& E, double* a, int m, int n, int lda, double* q, int ldq, double* r, int ldr);  // m >= n
+void qr_big_opt(Engine& E, double* a, int m, int n, int lda, double* q, int ldq, double* r, int ldr, bool form_q);
+// U-only one-sided Jacobi: q = sorted normalized columns of a (left singular vectors), s = values
+void jacobi_left(Engine& E, const std::vector<MatDesc>& d);
+void transpose_cm(Engine& E, const double* src, int m, int n, int lds, double* dst, int ldd);
 void svd_big(Engine& E, const std::vector<MatDesc>& d);        // m >= n, ld = m / n
 void dgemm_cm(Engine& E, bool ta, int M, int N, int K, double alpha, const double* A, int lda, const double* B,
               int ldb, double beta, double* C, int ldc);

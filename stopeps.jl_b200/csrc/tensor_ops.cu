@@ -222,6 +222,12 @@ void Engine::toc(int id, double fl, double by) {
   SPS_CUDA(cudaEventRecord(pending_[id].b, stream));
 }
 
+void Engine::set_work(int id, double fl, double by) {
+  if (id < 0 || id >= (int)pending_.size()) return;
+  pending_[id].flops = fl;
+  pending_[id].bytes = by;
+}
+
 std::map<std::string, Engine::KStat> Engine::kernel_stats() {
   SPS_CUDA(cudaStreamSynchronize(stream));
   for (auto& p : pending_) {
@@ -1186,6 +1192,174 @@ SVDres svd(Engine& E, const Tensor& A, const std::vector<int>& rows, const std::
       scatter_block(E, res.V, vrd, vcd, kk[c], n[c], d.q, n[c], true);
     }
     keep.insert(keep.end(), {t1, t2, t3, t4});
+  }
+  return res;
+}
+
+bool svd_prefers_kept(const Tensor& A, const std::vector<int>& rows, const std::vector<int>& cols) {
+  BlockTables bt = tables_of(A, rows, cols);
+  for (int c = 0; c < 2; ++c)
+    if (std::min(bt.rt[c].size(), bt.ct[c].size()) >= 160) return true;
+  return false;
+}
+
+KeptSVD svd_kept(Engine& E, const Tensor& A, const std::vector<int>& rows, const std::vector<int>& cols,
+                 const Trunc& tr, bool want_entropy, bool left) {
+  BlockTables bt = tables_of(A, rows, cols);
+  int m[2], n[2], k[2];
+  struct Work { Buf mb, xb, qb, rb, sb, ub; double *M, *X, *U, *s; int mx, nx; bool direct; };
+  Work w[2];
+  std::vector<la::MatDesc> jac;
+  int jmap[2] = {-1, -1};
+  std::vector<Buf> keep;
+  for (int c = 0; c < 2; ++c) {
+    m[c] = (int)bt.rt[c].size();
+    n[c] = (int)bt.ct[c].size();
+    k[c] = std::min(m[c], n[c]);
+    if (k[c] == 0) continue;
+    Work& W = w[c];
+    Buf t1, t2;
+    int64_t* rt = E.upload_i64(bt.rt[c], t1);
+    int64_t* ct = E.upload_i64(bt.ct[c], t2);
+    keep.insert(keep.end(), {t1, t2});
+    W.mb = E.alloc(sizeof(double) * (size_t)m[c] * n[c]);
+    W.M = (double*)W.mb->ptr;
+    gather_block(E, A, rt, ct, m[c], n[c], W.M, m[c], false);
+    // vectors wanted: left -> of M (length m), right -> of M^T (length n)
+    int a = left ? m[c] : n[c];   // length of the wanted vectors
+    int b = left ? n[c] : m[c];   // other dimension
+    if (a <= b) {
+      // X = L from the LQ of the (a x b) matrix: QR of its transpose (b x a), X = R^T (a x a)
+      W.mx = a;
+      W.nx = a;
+      W.direct = false;
+      Buf tb = E.alloc(sizeof(double) * (size_t)b * a);
+      double* T = (double*)tb->ptr;
+      if (left) la::transpose_cm(E, W.M, m[c], n[c], m[c], T, n[c]);                       // M^T (n x m)
+      else SPS_CUDA(cudaMemcpyAsync(T, W.M, sizeof(double) * (size_t)m[c] * n[c], cudaMemcpyDeviceToDevice, E.stream));
+      W.rb = E.alloc(sizeof(double) * (size_t)a * a);
+      double* R = (double*)W.rb->ptr;
+      if (la::qr_is_big(b, a)) {
+        la::qr_big_opt(E, T, b, a, b, nullptr, b, R, a, false);
+      } else {
+        Buf qb = E.alloc(sizeof(double) * (size_t)b * a + a);
+        la::qr_batched(E, {la::MatDesc{T, (double*)qb->ptr, R, (double*)qb->ptr + (size_t)b * a, b, a, b, b, a}});
+        keep.push_back(qb);
+      }
+      keep.push_back(tb);
+      W.xb = E.alloc(sizeof(double) * (size_t)a * a);
+      W.X = (double*)W.xb->ptr;
+      la::transpose_cm(E, R, a, a, a, W.X, a);
+    } else {
+      // a > b: Jacobi directly on the (a x b) matrix whose columns span the wanted space
+      W.mx = a;
+      W.nx = b;
+      W.direct = true;
+      W.xb = E.alloc(sizeof(double) * (size_t)a * b);
+      W.X = (double*)W.xb->ptr;
+      if (left) SPS_CUDA(cudaMemcpyAsync(W.X, W.M, sizeof(double) * (size_t)m[c] * n[c], cudaMemcpyDeviceToDevice, E.stream));
+      else la::transpose_cm(E, W.M, m[c], n[c], m[c], W.X, n[c]);
+    }
+    W.ub = E.alloc(sizeof(double) * (size_t)W.mx * W.nx);
+    W.sb = E.alloc(sizeof(double) * W.nx);
+    W.U = (double*)W.ub->ptr;
+    W.s = (double*)W.sb->ptr;
+    jmap[c] = (int)jac.size();
+    jac.push_back({W.X, W.U, nullptr, W.s, W.mx, W.nx, W.mx, W.mx, 0});
+  }
+  la::jacobi_left(E, jac);
+  // singular values to the host
+  std::vector<double> sv[2];
+  int off = 0;
+  for (int c = 0; c < 2; ++c) {
+    if (jmap[c] < 0) continue;
+    SPS_CUDA(cudaMemcpyAsync(E.hscal + off, w[c].s, sizeof(double) * k[c], cudaMemcpyDeviceToHost, E.stream));
+    off += k[c];
+  }
+  if (off > Engine::NSCAL) throw Error(SPS_ERR_ARGUMENT, "svd_kept: too many singular values");
+  E.sync();
+  E.check_flag("svd_kept");
+  off = 0;
+  for (int c = 0; c < 2; ++c) {
+    if (jmap[c] < 0) continue;
+    sv[c].assign(E.hscal + off, E.hscal + off + k[c]);
+    off += k[c];
+  }
+  KeptSVD res;
+  double tot2 = 0;
+  for (int c = 0; c < 2; ++c)
+    for (double x : sv[c]) tot2 += x * x;
+  res.norm = std::sqrt(tot2);
+  if (want_entropy) {
+    if (res.norm == 0) res.entropy = NAN;
+    else {
+      double ent = 0;
+      for (int c = 0; c < 2; ++c)
+        for (double x : sv[c]) {
+          double p = (x / res.norm) * (x / res.norm);
+          if (p != 0) ent -= p * std::log(p);
+        }
+      res.entropy = std::max(0.0, ent);
+    }
+  }
+  std::vector<char> kp[2];
+  select_truncation(sv, tr, kp);
+  int kk[2] = {0, 0};
+  double disc = 0;
+  for (int c = 0; c < 2; ++c)
+    for (size_t i = 0; i < sv[c].size(); ++i) {
+      if (kp[c][i]) {
+        if ((int)i != kk[c]) throw Error(SPS_ERR_NUMERIC, "svd_kept: non-prefix truncation");
+        kk[c]++;
+        res.S[c].push_back(sv[c][i]);
+      } else {
+        disc += sv[c][i] * sv[c][i];
+      }
+    }
+  res.err = std::sqrt(disc);
+  Par nl = make_par(kk[0], kk[1]);
+  int nr = (int)rows.size(), nc = (int)cols.size();
+  if (left) {
+    std::vector<Par> fl = bt.rp;
+    fl.push_back(nl);
+    std::vector<Par> wl{nl};
+    wl.insert(wl.end(), bt.cp.begin(), bt.cp.end());
+    res.F = E.zeros(fl);
+    res.W = E.zeros(wl);
+  } else {
+    std::vector<Par> fl{nl};
+    fl.insert(fl.end(), bt.cp.begin(), bt.cp.end());
+    std::vector<Par> wl = bt.rp;
+    wl.push_back(nl);
+    res.F = E.zeros(fl);
+    res.W = E.zeros(wl);
+  }
+  for (int c = 0; c < 2; ++c) {
+    if (jmap[c] < 0 || kk[c] == 0) continue;
+    Work& W = w[c];
+    Buf wb = E.alloc(sizeof(double) * (size_t)std::max(m[c], n[c]) * kk[c]);
+    double* Wm = (double*)wb->ptr;
+    Buf t1, t2, t3, t4;
+    if (left) {
+      // U_k = first kk columns (m x kk, ld m); W = U_k^T M (kk x n)
+      la::dgemm_cm(E, true, kk[c], n[c], m[c], 1.0, W.U, m[c], W.M, m[c], 0.0, Wm, kk[c]);
+      auto frow = tensor_rows(res.F, 0, nr, c);
+      auto fcol = leg_offsets(c, kk[0], kk[1], res.F.strides[nr]);
+      scatter_block(E, res.F, E.upload_i64(frow, t1), E.upload_i64(fcol, t2), m[c], kk[c], W.U, m[c], false);
+      auto wrow = leg_offsets(c, kk[0], kk[1], res.W.strides[0]);
+      auto wcol = tensor_rows(res.W, 1, nc, c);
+      scatter_block(E, res.W, E.upload_i64(wrow, t3), E.upload_i64(wcol, t4), kk[c], n[c], Wm, kk[c], false);
+    } else {
+      // V_k = first kk columns (n x kk, ld n); W = M V_k (m x kk)
+      la::dgemm_cm(E, false, m[c], kk[c], n[c], 1.0, W.M, m[c], W.U, n[c], 0.0, Wm, m[c]);
+      auto frow = leg_offsets(c, kk[0], kk[1], res.F.strides[0]);
+      auto fcol = tensor_rows(res.F, 1, nc, c);
+      scatter_block(E, res.F, E.upload_i64(frow, t1), E.upload_i64(fcol, t2), kk[c], n[c], W.U, n[c], true);
+      auto wrow = tensor_rows(res.W, 0, nr, c);
+      auto wcol = leg_offsets(c, kk[0], kk[1], res.W.strides[nr]);
+      scatter_block(E, res.W, E.upload_i64(wrow, t3), E.upload_i64(wcol, t4), m[c], kk[c], Wm, m[c], false);
+    }
+    keep.insert(keep.end(), {wb, t1, t2, t3, t4});
   }
   return res;
 }
