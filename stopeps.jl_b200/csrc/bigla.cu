@@ -289,18 +289,30 @@ __global__ void __launch_bounds__(BT) panel_qr_kernel(PanelArgs p) {
     if (lane == 0 && s != 0.0) atomicAdd(&gram[a * jb + b], s);
   }
   grid_barrier(p.bar, p.flag);
-  if (blockIdx.x == 0 && threadIdx.x == 0) {
-    // T(i,i) = tau_i ; T(0:i, i) = -tau_i T(0:i,0:i) V(:,0:i)^T v_i  (dlarft, forward, columnwise)
-    for (int i = 0; i < jb; ++i) {
-      double ti = p.tau[p.j0 + i];
-      for (int a = 0; a < i; ++a) {
-        double s = 0;
-        for (int b = a; b < i; ++b) s += p.T[a + b * jb] * __ldcg(&gram[b * jb + i]);
-        p.T[a + i * jb] = -ti * s;
-      }
-      p.T[i + i * jb] = ti;
-      for (int a = i + 1; a < jb; ++a) p.T[a + i * jb] = 0.0;
+  if (blockIdx.x == 0) {
+    // T(i,i) = tau_i ; T(0:i, i) = -tau_i T(0:i,0:i) V(:,0:i)^T v_i  (dlarft, forward, columnwise),
+    // built in shared memory: column i is a triangular mat-vec over the already built columns.
+    double* Ts = sm;                  // jb x jb, column-major
+    double* Gs = sm + jb * jb;        // Gram (upper part used)
+    for (int e = threadIdx.x; e < jb * jb; e += BT) {
+      Ts[e] = 0.0;
+      int a = e / jb, b = e % jb;
+      Gs[e] = a <= b ? __ldcg(&gram[a * jb + b]) : 0.0;   // Gs[a*jb + b] = (V^T V)(a,b), a <= b
     }
+    __syncthreads();
+    for (int i = 0; i < jb; ++i) {
+      const double ti = __ldcg(&p.tau[p.j0 + i]);
+      double v = 0;
+      if (threadIdx.x < i) {
+        const int a = threadIdx.x;
+        for (int b = a; b < i; ++b) v += Ts[a + b * jb] * Gs[b * jb + i];
+      }
+      __syncthreads();
+      if (threadIdx.x < i) Ts[threadIdx.x + i * jb] = -ti * v;
+      if (threadIdx.x == 0) Ts[i + i * jb] = ti;
+      __syncthreads();
+    }
+    for (int e = threadIdx.x; e < jb * jb; e += BT) p.T[e] = Ts[e];
   }
 }
 
@@ -340,11 +352,11 @@ void qr_big_opt(Engine& E, double* a, int m, int n, int lda, double* q, int ldq,
     int maxg = coop_blocks((const void*)panel_qr_kernel, BT, 0, E);
     int G = std::min({E.num_sms, maxg, std::max(1, (mrows + 63) / 64)});
     int rpc = (mrows + G - 1) / G;
-    size_t smem = sizeof(double) * (size_t)rpc * jb;
+    size_t smem = sizeof(double) * std::max((size_t)rpc * jb, (size_t)2 * jb * jb);
     if (smem > 200 * 1024) {
       G = std::min(maxg, (int)((mrows * (size_t)jb * 8 + 200 * 1024 - 1) / (200 * 1024)));
       rpc = (mrows + G - 1) / G;
-      smem = sizeof(double) * (size_t)rpc * jb;
+      smem = sizeof(double) * std::max((size_t)rpc * jb, (size_t)2 * jb * jb);
       if (smem > 200 * 1024) throw Error(SPS_ERR_ARGUMENT, "qr_big: panel too tall for shared memory");
     }
     SPS_CUDA(cudaFuncSetAttribute((const void*)panel_qr_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
