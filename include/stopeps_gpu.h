@@ -119,6 +119,10 @@ int sps_timer_stop(sps_handle* h, double* milliseconds);
 int sps_la_svd(sps_handle* h, int32_t m, int32_t n, const double* a, double* u, double* s, double* vt,
                int32_t* sweeps, double* ms);
 int sps_la_qr(sps_handle* h, int32_t m, int32_t n, const double* a, double* q, double* r, double* ms);
+/* Left singular vectors and values only (the U-only Jacobi of the truncated
+ * boundary SVD), m >= n: a = u diag(s) v^T, u (m x n), s (n). */
+int sps_la_svd_left(sps_handle* h, int32_t m, int32_t n, const double* a, double* u, double* s, int32_t* sweeps,
+                    double* ms);
 
 /* No counterpart in the reference.  The one-sided Jacobi SVD of one small
  * matrix for callers that cannot allocate device memory (no cudaMalloc /

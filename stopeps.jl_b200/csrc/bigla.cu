@@ -902,6 +902,147 @@ __global__ void __launch_bounds__(BT) jacobi_u_kernel(const JUProb* probs, int n
   }
 }
 
+// ---------------------------------------------------------------------------
+// U-only block one-sided Jacobi: blocks of UBW columns; each round one CTA
+// takes a block pair (2*UBW columns) into shared memory, runs one inner
+// one-sided Jacobi sweep over its column pairs (shared-memory rounds, no grid
+// barrier) and writes the pair back.  nblk-1 grid barriers per sweep.
+// ---------------------------------------------------------------------------
+static constexpr int UBW = 8;
+static constexpr int UB2 = 2 * UBW;
+
+__global__ void __launch_bounds__(BT) jacobi_ub_kernel(const JUProb* probs, int nprob, int total_pairs,
+                                                       int max_rounds, unsigned* bar, int* counters, int* flag) {
+  extern __shared__ double Ub[];   // m x UB2, column-major (ld m)
+  __shared__ int any_rot;
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  if (blockIdx.x == 0 && threadIdx.x == 0) {
+    counters[0] = 0;
+    counters[1] = 0;
+    counters[2] = 0;
+  }
+  grid_barrier(bar, flag);
+  const int MAXSWEEP = 80;
+  bool converged = false;
+  int sweep = 0;
+  for (; sweep < MAXSWEEP; ++sweep) {
+    int* cnt = counters + (sweep % 3);
+    if (blockIdx.x == 0 && threadIdx.x == 0) counters[(sweep + 1) % 3] = 0;
+    for (int round = 0; round < max_rounds; ++round) {
+      for (int t = blockIdx.x; t < total_pairs; t += gridDim.x) {
+        int pi = 0;
+        while (pi + 1 < nprob && t >= probs[pi + 1].pair_base) ++pi;
+        const JUProb& P = probs[pi];
+        const int nb = (P.n + UBW - 1) / UBW;
+        const int nbp = nb + (nb & 1);
+        if (round >= nbp - 1) continue;
+        const int pr = t - P.pair_base;
+        int bi = rr_idx(pr, round, nbp), bj = rr_idx(nbp - 1 - pr, round, nbp);
+        if (bi >= nb || bj >= nb) continue;
+        if (bi > bj) { int tt = bi; bi = bj; bj = tt; }
+        const int c0 = bi * UBW, w1 = min(UBW, P.n - c0);
+        const int c1 = bj * UBW, w2 = min(UBW, P.n - c1);
+        const int wt = w1 + w2, m = P.m;
+        for (int e = threadIdx.x; e < wt * m; e += BT) {
+          int k = e / m, i = e % m;
+          int gc = k < w1 ? c0 + k : c1 + (k - w1);
+          Ub[i + (size_t)k * m] = P.X[i + (size_t)gc * m];
+        }
+        if (threadIdx.x == 0) any_rot = 0;
+        __syncthreads();
+        const double tol = DBL_EPSILON * (double)max(m, 2);
+        const int wtp = wt + (wt & 1);
+        for (int ir = 0; ir < wtp - 1; ++ir) {
+          for (int q = warp; q < wtp / 2; q += BW) {
+            int a = rr_idx(q, ir, wtp), b = rr_idx(wtp - 1 - q, ir, wtp);
+            if (a >= wt || b >= wt) continue;
+            if (a > b) { int tt = a; a = b; b = tt; }
+            double* ua = Ub + (size_t)a * m;
+            double* ub = Ub + (size_t)b * m;
+            double al = 0, be = 0, ga = 0;
+            for (int i = lane; i < m; i += 32) {
+              double x = ua[i], y = ub[i];
+              al += x * x;
+              be += y * y;
+              ga += x * y;
+            }
+            al = wsum(al);
+            be = wsum(be);
+            ga = wsum(ga);
+            if (ga == 0.0 || !(fabs(ga) > tol * sqrt(al * be))) continue;
+            double zeta = (be - al) / (2.0 * ga);
+            double tt = copysign(1.0, zeta) / (fabs(zeta) + sqrt(1.0 + zeta * zeta));
+            double c = 1.0 / sqrt(1.0 + tt * tt), sn = c * tt;
+            for (int i = lane; i < m; i += 32) {
+              double x = ua[i], y = ub[i];
+              ua[i] = c * x - sn * y;
+              ub[i] = sn * x + c * y;
+            }
+            if (lane == 0) any_rot = 1;
+          }
+          __syncthreads();
+        }
+        if (any_rot) {
+          if (threadIdx.x == 0) atomicAdd(cnt, 1);
+          for (int e = threadIdx.x; e < wt * m; e += BT) {
+            int k = e / m, i = e % m;
+            int gc = k < w1 ? c0 + k : c1 + (k - w1);
+            P.X[i + (size_t)gc * m] = Ub[i + (size_t)k * m];
+          }
+        }
+        __syncthreads();
+      }
+      grid_barrier(bar, flag);
+    }
+    int rot = *(volatile int*)cnt;
+    if (rot == 0) {
+      converged = true;
+      break;
+    }
+  }
+  if (blockIdx.x == 0 && threadIdx.x == 0) {
+    if (!converged) atomicOr(flag, FLAG_CONV);
+    atomicMax(flag + 1, sweep + 1);
+  }
+  const int gw = blockIdx.x * BW + warp, TW = gridDim.x * BW;
+  for (int pi = 0; pi < nprob; ++pi) {
+    const JUProb P = probs[pi];
+    for (int c = gw; c < P.n; c += TW) {
+      const double* uc = P.X + (size_t)c * P.m;
+      double v = 0;
+      for (int i = lane; i < P.m; i += 32) v += uc[i] * uc[i];
+      v = wsum(v);
+      if (lane == 0) P.sig[c] = sqrt(v);
+    }
+  }
+  grid_barrier(bar, flag);
+  for (int pi = 0; pi < nprob; ++pi) {
+    const JUProb P = probs[pi];
+    for (int c = blockIdx.x * BT + threadIdx.x; c < P.n; c += gridDim.x * BT) {
+      double sc = __ldcg(&P.sig[c]);
+      int rk = 0;
+      for (int j = 0; j < P.n; ++j) {
+        double sj = __ldcg(&P.sig[j]);
+        rk += (sj > sc) || (sj == sc && j < c);
+      }
+      P.rank[c] = rk;
+      P.s[rk] = sc;
+    }
+  }
+  grid_barrier(bar, flag);
+  for (int pi = 0; pi < nprob; ++pi) {
+    const JUProb P = probs[pi];
+    for (int c = gw; c < P.n; c += TW) {
+      int rk = __ldcg(&P.rank[c]);
+      double sc = __ldcg(&P.sig[c]);
+      double inv = sc > 0 ? 1.0 / sc : 0.0;
+      const double* uc = P.X + (size_t)c * P.m;
+      double* qo = P.q + (size_t)rk * P.m;
+      for (int i = lane; i < P.m; i += 32) qo[i] = uc[i] * inv;
+    }
+  }
+}
+
 // problems: (x = m x n ld m rotated in place, q = sorted left vectors m x n ld m, s = values n)
 void jacobi_left(Engine& E, const std::vector<MatDesc>& d) {
   if (d.empty()) return;
@@ -933,17 +1074,37 @@ void jacobi_left(Engine& E, const std::vector<MatDesc>& d) {
   E.stage(ps.data(), sizeof(JUProb) * ps.size(), pb->ptr);
   Buf bb = E.alloc(sizeof(unsigned) * 2 + sizeof(int) * 4);
   SPS_CUDA(cudaMemsetAsync(bb->ptr, 0, sizeof(unsigned) * 2 + sizeof(int) * 4, E.stream));
+  size_t ubsmem = sizeof(double) * (size_t)mmax * UB2;
+  const bool blocked = ubsmem <= 200 * 1024;
+  if (blocked) {
+    int bpairs = 0, brounds = 0;
+    for (auto& P : ps) {
+      int nb = (P.n + UBW - 1) / UBW;
+      int nbp = nb + (nb & 1);
+      P.pair_base = bpairs;
+      bpairs += nbp / 2;
+      brounds = std::max(brounds, nbp - 1);
+    }
+    pairs = bpairs;
+    max_rounds = brounds;
+    E.stage(ps.data(), sizeof(JUProb) * ps.size(), pb->ptr);
+  }
   const bool reg = mmax <= 32 * JR;
-  const void* kfn = reg ? (const void*)jacobi_u_kernel<true> : (const void*)jacobi_u_kernel<false>;
-  int maxg = coop_blocks(kfn, BT, 0, E);
-  int G = std::min({E.num_sms, maxg, std::max(1, (pairs + BW - 1) / BW)});
+  const void* kfn = blocked ? (const void*)jacobi_ub_kernel
+                            : (reg ? (const void*)jacobi_u_kernel<true> : (const void*)jacobi_u_kernel<false>);
+  size_t smem = blocked ? ubsmem : 0;
+  if (blocked)
+    SPS_CUDA(cudaFuncSetAttribute(kfn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)std::max<size_t>(smem, 1)));
+  int maxg = coop_blocks(kfn, BT, smem, E);
+  int G = blocked ? std::min(maxg, std::max(1, pairs))
+                  : std::min({E.num_sms, maxg, std::max(1, (pairs + BW - 1) / BW)});
   const JUProb* dp = (const JUProb*)pb->ptr;
   int nprob = (int)ps.size();
   unsigned* bar = (unsigned*)bb->ptr;
   int* counters = (int*)(bar + 2);
   void* args[] = {&dp, &nprob, &pairs, &max_rounds, &bar, &counters, &E.dflag};
   int tk = E.tic("svd_jacobi_left");
-  SPS_CUDA(cudaLaunchCooperativeKernel(kfn, dim3(G), dim3(BT), args, 0, E.stream));
+  SPS_CUDA(cudaLaunchCooperativeKernel(kfn, dim3(G), dim3(BT), args, smem, E.stream));
   E.toc(tk);
   E.launches++;
   if (E.profile) {

@@ -227,6 +227,36 @@ int sps_la_svd(sps_handle* h, int32_t m, int32_t n, const double* a, double* u, 
   });
 }
 
+int sps_la_svd_left(sps_handle* h, int32_t m, int32_t n, const double* a, double* u, double* s, int32_t* sweeps,
+                    double* ms) {
+  return guarded(h, [&] {
+    Engine& E = *h->E;
+    if (m < n || n < 1) throw Error(SPS_ERR_ARGUMENT, "sps_la_svd_left needs m >= n >= 1");
+    Buf ba, bq, bs;
+    double* da = dev_copy(E, ba, a, (size_t)m * n);
+    bq = E.alloc(sizeof(double) * (size_t)m * n);
+    bs = E.alloc(sizeof(double) * n);
+    if (!h->t0) {
+      SPS_CUDA(cudaEventCreate(&h->t0));
+      SPS_CUDA(cudaEventCreate(&h->t1));
+    }
+    SPS_CUDA(cudaMemsetAsync(E.dflag + 1, 0, sizeof(int), E.stream));
+    SPS_CUDA(cudaEventRecord(h->t0, E.stream));
+    la::jacobi_left(E, {la::MatDesc{da, (double*)bq->ptr, nullptr, (double*)bs->ptr, m, n, m, m, 0}});
+    SPS_CUDA(cudaEventRecord(h->t1, E.stream));
+    SPS_CUDA(cudaMemcpyAsync(u, bq->ptr, sizeof(double) * (size_t)m * n, cudaMemcpyDeviceToHost, E.stream));
+    SPS_CUDA(cudaMemcpyAsync(s, bs->ptr, sizeof(double) * n, cudaMemcpyDeviceToHost, E.stream));
+    int sw = 0;
+    SPS_CUDA(cudaMemcpyAsync(&sw, E.dflag + 1, sizeof(int), cudaMemcpyDeviceToHost, E.stream));
+    E.sync();
+    float f = 0;
+    SPS_CUDA(cudaEventElapsedTime(&f, h->t0, h->t1));
+    E.check_flag("sps_la_svd_left");
+    if (ms) *ms = f;
+    if (sweeps) *sweeps = sw;
+  });
+}
+
 int sps_la_qr(sps_handle* h, int32_t m, int32_t n, const double* a, double* q, double* r, double* ms) {
   return guarded(h, [&] {
     Engine& E = *h->E;

@@ -105,6 +105,18 @@ class Engine:
                                        _arr(vt, C.c_double), C.byref(sw), C.byref(ms)))
         return u, s, vt, sw.value, ms.value
 
+    def la_svd_left(self, a):
+        """Left singular vectors and values (m >= n) by the U-only Jacobi: (u, s, sweeps, device_ms)."""
+        a = np.asfortranarray(np.asarray(a, np.float64))
+        m, n = a.shape
+        u = np.zeros((m, n), order="F")
+        s = np.zeros(n)
+        sw = C.c_int32()
+        ms = C.c_double()
+        self.check(self.lib.sps_la_svd_left(self.h, m, n, _arr(a, C.c_double), _arr(u, C.c_double),
+                                            _arr(s, C.c_double), C.byref(sw), C.byref(ms)))
+        return u, s, sw.value, ms.value
+
     def la_qr(self, a):
         """Engine Householder QR of one host matrix: (q, r, device_ms)."""
         a = np.asfortranarray(np.asarray(a, np.float64))

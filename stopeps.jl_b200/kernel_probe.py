@@ -1,0 +1,60 @@
+"""Run one hot operation of the engine on a representative input, for profiling.
+
+  python stopeps.jl_b200/kernel_probe.py svd_left   # U-only Jacobi of a 648x648 LQ-preconditioned block
+  python stopeps.jl_b200/kernel_probe.py qr          # blocked Householder QR of a 23328x648 block
+  python stopeps.jl_b200/kernel_probe.py draw        # one Born draw, 8x8 D=6 chi=36 (synthetic PEPO)
+
+Each operation runs once to warm up and once more; the sizes are those of the
+8x8, D=6, chi=36 boundary compression (parity blocks of 648 and 23328 rows).
+Inputs are seeded synthetic matrices with a graded spectrum like the
+boundary-MPS Schmidt spectra.
+"""
+from __future__ import annotations
+
+import os
+import sys
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, os.path.dirname(HERE))
+
+
+def graded(m, n, decay, seed):
+    rng = np.random.default_rng(seed)
+    u, _ = np.linalg.qr(rng.standard_normal((m, min(m, n))))
+    v, _ = np.linalg.qr(rng.standard_normal((n, min(m, n))))
+    return (u * np.exp(-decay * np.arange(min(m, n)))) @ v.T
+
+
+def main(which):
+    import __graft_entry__ as ge
+    sps = ge.load_package()
+    if which == "svd_left":
+        e = sps.Engine(2, 2)
+        a = graded(648, 648, 0.03, 5)
+        L = np.linalg.qr(a.T)[1].T.copy()
+        for _ in range(2):
+            u, s, sweeps, ms = e.la_svd_left(L)
+        print(f"svd_left 648x648: {ms:.2f} ms, {sweeps} sweeps")
+    elif which == "qr":
+        e = sps.Engine(2, 2)
+        a = np.random.default_rng(3).standard_normal((23328, 648))
+        for _ in range(2):
+            q, r, ms = e.la_qr(a)
+        print(f"qr 23328x648: {ms:.2f} ms")
+    elif which == "draw":
+        e = sps.Engine(8, 8, sps.TFIM(1.0, 3.0))
+        sites, dims = sps.synthetic.synthetic_pepo(8, 8, 6, 0.15, 7)
+        st = e.upload_state(sites, dims, True, beta=0.4)
+        sps.normalize_state(st)
+        cache = sps.SamplingCache(st, sps.BoundaryMPS(36, sps.Z2Space(18, 18)))
+        for i in range(2):
+            d = sps.sample_configuration(cache, uniforms=sps.sample_uniforms(1, i + 1, 64))
+        print("draw log_probability", d["log_probability"])
+    else:
+        raise SystemExit(f"unknown operation {which}")
+
+
+if __name__ == "__main__":
+    main(sys.argv[1] if len(sys.argv) > 1 else "svd_left")

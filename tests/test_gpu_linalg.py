@@ -47,3 +47,15 @@ def test_qr_matches_lapack(eng, m, n):
     assert np.allclose(np.triu(r), r)
     rr = np.linalg.qr(a, mode="r")
     np.testing.assert_allclose(np.abs(np.diag(r)), np.abs(np.diag(rr)), rtol=1e-10)
+
+
+@pytest.mark.parametrize("m,n", [(60, 40), (200, 200), (648, 648), (900, 300), (1300, 180)])
+def test_left_jacobi_matches_lapack(eng, m, n):
+    """The U-only Jacobi of the truncated boundary SVD (block and element-pair variants)."""
+    a = graded(m, n, 0.03, 3 * m + n)
+    u, s, sweeps, ms = eng.la_svd_left(a)
+    ref_u, ref_s, _ = np.linalg.svd(a, full_matrices=False)
+    np.testing.assert_allclose(s, ref_s, rtol=1e-11, atol=1e-13 * ref_s[0])
+    np.testing.assert_allclose(u.T @ u, np.eye(n), atol=1e-10)
+    top = min(n, 36)
+    np.testing.assert_allclose(np.abs(np.sum(u[:, :top] * ref_u[:, :top], axis=0)), 1.0, atol=1e-9)
