@@ -908,7 +908,7 @@ __global__ void __launch_bounds__(BT) jacobi_u_kernel(const JUProb* probs, int n
 // one-sided Jacobi sweep over its column pairs (shared-memory rounds, no grid
 // barrier) and writes the pair back.  nblk-1 grid barriers per sweep.
 // ---------------------------------------------------------------------------
-static constexpr int UBW = 8;
+static constexpr int UBW = 4;
 static constexpr int UB2 = 2 * UBW;
 
 __global__ void __launch_bounds__(BT) jacobi_ub_kernel(const JUProb* probs, int nprob, int total_pairs,
