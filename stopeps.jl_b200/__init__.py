@@ -14,6 +14,7 @@ from .driver import (run_purification, run_stochastic, ensemble_statistics, grou
                      sample_uniforms, step_schedule, ThermalCheckpoint, Particle, RESULT_SCHEMA_VERSION)
 from . import _lib
 from .build import build, LIB as LIBRARY_PATH
+from .parallel import SerialExecution, TorchExecution
 from . import synthetic
 
 __all__ = [

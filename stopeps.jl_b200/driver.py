@@ -129,25 +129,50 @@ class Particle:
     seed: int = 0
 
 
-def _observe(state, c: RunConfig, energy: bool):
+class DeviceOps:
+    """The hot-path operations the drivers call, on the device engine."""
+
+    def sampling_cache(self, state, method):
+        return eng.SamplingCache(state, method)
+
+    def sample(self, cache, uniforms):
+        return eng.sample_configuration(cache, uniforms=uniforms)
+
+    def project(self, state, configuration):
+        return eng.project_configuration(state, configuration)
+
+    def measure_energy(self, state, method):
+        return eng.measure_energy(state, method)
+
+    def lognorm(self, state, method):
+        return eng.lognorm(state, method)
+
+    def evolution_step(self, state, delta, D, method, space):
+        return eng.evolution_step(state, delta, D, method, space)
+
+
+DEVICE_OPS = DeviceOps()
+
+
+def _observe(state, c: RunConfig, energy: bool, ops=DEVICE_OPS):
     """``_observe`` (``particles.jl:35-40``)."""
     t = time.perf_counter()
     if energy:
-        m = eng.measure_energy(state, c.boundary("measurement"))
+        m = ops.measure_energy(state, c.boundary("measurement"))
     else:
-        m = eng.lognorm(state, c.boundary("measurement"))
+        m = ops.lognorm(state, c.boundary("measurement"))
         m.update(energy_total=math.nan, energy_per_site=math.nan, magnetization=math.nan)
     m["measurement_seconds"] = time.perf_counter() - t
     return m
 
 
-def _evolve(state, c: RunConfig, steps, D, space, on_step=None):
+def _evolve(state, c: RunConfig, steps, D, space, on_step=None, ops=DEVICE_OPS):
     """``_evolve!`` (``particles.jl:66-85``)."""
     total = maxstate = maxenv = normalization = 0.0
     maxent = 0.0 if (c.record_boundary_entropy and steps) else math.nan
     for beta in steps:
         t = time.perf_counter()
-        r = eng.evolution_step(state, (beta - state.beta) / 2, D, c.boundary("environment"), space)
+        r = ops.evolution_step(state, (beta - state.beta) / 2, D, c.boundary("environment"), space)
         elapsed = time.perf_counter() - t
         state.beta = beta
         normalization += r["log_normalization_sum"]
@@ -161,18 +186,23 @@ def _evolve(state, c: RunConfig, steps, D, space, on_step=None):
                 max_boundary_entropy=maxent, normalization=normalization)
 
 
-def run_purification(c: RunConfig, engine: eng.Engine | None = None) -> ThermalCheckpoint:
+def run_purification(c: RunConfig, engine: eng.Engine | None = None, ops=None,
+                     identity=None) -> ThermalCheckpoint:
     """Prepare the beta0 thermal PEPO (``run.jl:2-43``)."""
     validate_config(c)
-    e = engine or eng.Engine.from_config(c)
-    state = e.identity_pepo()
-    initial = eng.normalize_state(state)
-    history = [dict(phase="initialization", beta=0.0, normalizations=initial.tolist())]
+    ops = ops or DEVICE_OPS
+    if identity is None:
+        e = engine or eng.Engine.from_config(c)
+        state = e.identity_pepo()
+        initial = eng.normalize_state(state)
+    else:
+        state, initial = identity()
+    history = [dict(phase="initialization", beta=0.0, normalizations=list(initial))]
     rows = []
     for beta in [b for b in temperature_nodes(c) if b <= c.beta0]:
         steps = step_schedule(state.beta, beta, c.delta_tau_pur)
-        rep = _evolve(state, c, steps, c.D_pur, c.bond_space_pur, on_step=history.append)
-        m = _observe(state, c, measure_at(c, beta))
+        rep = _evolve(state, c, steps, c.D_pur, c.bond_space_pur, on_step=history.append, ops=ops)
+        m = _observe(state, c, measure_at(c, beta), ops)
         rows.append(dict(beta=beta, source="purification", energy_total=m["energy_total"],
                          energy_per_site=m["energy_per_site"],
                          energy_per_site_error=0.0 if measure_at(c, beta) else math.nan,
@@ -220,70 +250,104 @@ def _statistics(records, Ns, nsites):
     return s
 
 
-def run_stochastic(c: RunConfig, checkpoint: ThermalCheckpoint, uniforms_fn=None):
+def run_stochastic(c: RunConfig, checkpoint: ThermalCheckpoint, uniforms_fn=None, execution=None, ops=None):
     """Draw Born samples from the beta0 checkpoint and evolve the weighted ensemble (``run.jl:76-134``).
 
-    Returns the result record: ``observables`` (curve, purification, samples),
-    ``diagnostics`` (born draws and grouping), ``metadata`` and ``parameters``.
+    ``execution`` distributes the work like the reference's MPI backend
+    (``ext/StoPEPSMPIExt.jl``): draws round-robin by index, unique
+    configurations by representative position, scalar records gathered at
+    every node; the default runs serially.  Rank 0 returns the result record
+    (``observables``: curve, purification, samples; ``diagnostics``: Born
+    draws and grouping; ``metadata``; ``parameters``); other ranks return None.
     """
-    validate_config(c)
-    if not (same_beta(checkpoint.state.beta, c.beta0)):
-        raise ValueError("checkpoint model, lattice or beta0 mismatch")
+    from .parallel import SerialExecution
+    e = execution or SerialExecution()
+    ops = ops or DEVICE_OPS
+    e.phase(lambda: validate_config(c))
+    e.check_arguments(repr(parameter_dict(c)))
+
+    def check_checkpoint():
+        if not same_beta(checkpoint.state.beta, c.beta0):
+            raise ValueError("checkpoint model, lattice or beta0 mismatch")
+
+    e.phase(check_checkpoint)
     L = c.lattice.Lx * c.lattice.Ly
     if uniforms_fn is None:
         uniforms_fn = lambda i: sample_uniforms(c.seed, i, L)
-    cache = eng.SamplingCache(checkpoint.state, c.boundary("sampling"))
-    draws = []
-    for i in range(1, c.Ns + 1):
-        d = eng.sample_configuration(cache, uniforms=uniforms_fn(i))
-        d["index"] = i
-        draws.append(d)
-    del cache
+    rank, nprocs = e.rank(), e.nprocs()
+
+    def local_draws():
+        cache = ops.sampling_cache(checkpoint.state, c.boundary("sampling"))
+        out = []
+        for i in range(1, c.Ns + 1):
+            if (i - 1) % nprocs != rank:
+                continue
+            d = dict(ops.sample(cache, uniforms_fn(i)))
+            d["index"] = i
+            out.append(d)
+        return out
+
+    draws = sorted([d for part in e.gather(e.phase(local_draws)) for d in part], key=lambda d: d["index"])
     grouping = group_configurations([d["configuration"] for d in draws])
-    particles = []
-    for u, i in enumerate(grouping["first_draw"]):
-        d = draws[i - 1]
-        state, _ = eng.project_configuration(checkpoint.state, d["configuration"])
-        m = _observe(state, c, measure_at(c, c.beta0))
-        particles.append(Particle(id=i, count=grouping["multiplicity"][u], configuration=d["configuration"],
-                                  state=state, log_p0=d["log_probability"], log_q_proposal=d["log_probability"],
-                                  relative_log_weight=m["log_norm"] - d["log_probability"],
-                                  weight_log_scale=0.0, physical_log_norm=m["log_norm"],
-                                  tensor_log_norm=m["tensor_log_norm"], energy_total=m["energy_total"],
-                                  energy_per_site=m["energy_per_site"], magnetization=m["magnetization"],
-                                  max_environment_truncation=max(d["max_environment_truncation"],
-                                                                 m["max_environment_truncation"]),
-                                  measurement_seconds=m["measurement_seconds"], sample_index=i, seed=c.seed))
+
+    def local_particles():
+        out = []
+        for u, i in enumerate(grouping["first_draw"], start=1):
+            if (u - 1) % nprocs != rank:     # _representative_owner (src/driver/execution.jl:34)
+                continue
+            d = draws[i - 1]
+            state, _ = ops.project(checkpoint.state, d["configuration"])
+            m = _observe(state, c, measure_at(c, c.beta0), ops)
+            out.append(Particle(id=i, count=grouping["multiplicity"][u - 1], configuration=d["configuration"],
+                                state=state, log_p0=d["log_probability"], log_q_proposal=d["log_probability"],
+                                relative_log_weight=m["log_norm"] - d["log_probability"],
+                                weight_log_scale=0.0, physical_log_norm=m["log_norm"],
+                                tensor_log_norm=m["tensor_log_norm"], energy_total=m["energy_total"],
+                                energy_per_site=m["energy_per_site"], magnetization=m["magnetization"],
+                                max_environment_truncation=max(d["max_environment_truncation"],
+                                                               m["max_environment_truncation"]),
+                                measurement_seconds=m["measurement_seconds"], sample_index=i, seed=c.seed))
+        return out
+
+    particles = e.phase(local_particles)
     curve = [r for r in checkpoint.purification if r["beta"] < c.beta0 and not same_beta(r["beta"], c.beta0)]
     samples = []
     nodes = [b for b in temperature_nodes(c) if b >= c.beta0]
     for node, beta in enumerate(nodes):
         if node > 0:
             steps = step_schedule(nodes[node - 1], beta, c.delta_tau_peps)
-            for p in particles:
-                old = p.tensor_log_norm
-                rep = _evolve(p.state, c, steps, c.D_peps, c.bond_space_peps)
-                m = _observe(p.state, c, measure_at(c, beta))
-                p.relative_log_weight += 2 * rep["normalization"] + (m["tensor_log_norm"] - old)
-                p.physical_log_norm = m["log_norm"]
-                p.tensor_log_norm = m["tensor_log_norm"]
-                p.energy_total = m["energy_total"]
-                p.energy_per_site = m["energy_per_site"]
-                p.magnetization = m["magnetization"]
-                p.max_state_truncation = rep["max_state_truncation"]
-                p.max_environment_truncation = max(rep["max_environment_truncation"],
-                                                   m["max_environment_truncation"])
-                p.max_boundary_entropy = rep["max_boundary_entropy"]
-                p.time_seconds = rep["time_seconds"]
-                p.measurement_seconds = m["measurement_seconds"]
-        records = [_particle_record(p) for p in particles]
+
+            def advance():
+                for p in particles:
+                    old = p.tensor_log_norm
+                    rep = _evolve(p.state, c, steps, c.D_peps, c.bond_space_peps, ops=ops)
+                    m = _observe(p.state, c, measure_at(c, beta), ops)
+                    p.relative_log_weight += 2 * rep["normalization"] + (m["tensor_log_norm"] - old)
+                    p.physical_log_norm = m["log_norm"]
+                    p.tensor_log_norm = m["tensor_log_norm"]
+                    p.energy_total = m["energy_total"]
+                    p.energy_per_site = m["energy_per_site"]
+                    p.magnetization = m["magnetization"]
+                    p.max_state_truncation = rep["max_state_truncation"]
+                    p.max_environment_truncation = max(rep["max_environment_truncation"],
+                                                       m["max_environment_truncation"])
+                    p.max_boundary_entropy = rep["max_boundary_entropy"]
+                    p.time_seconds = rep["time_seconds"]
+                    p.measurement_seconds = m["measurement_seconds"]
+
+            e.phase(advance)
+        local_records = e.phase(lambda: [dict(_particle_record(p), owner=rank) for p in particles])
+        records = sorted([r for part in e.gather(local_records) for r in part], key=lambda r: r["id"])
         stats = _statistics(records, c.Ns, L)
-        stats.update(source="sampling", time_seconds=sum(p.time_seconds for p in particles))
+        stats.update(source="sampling",
+                     time_seconds=max(e.gather(sum(p.time_seconds for p in particles))))
         if c.resampling.enabled and stats["eta"] < c.resampling.eta_th:
             raise NotImplementedError("annealed Born resampling is not part of this engine; "
                                       "run with resampling=ResamplingOptions(enabled=False)")
         curve.append(stats)
         samples.extend(records)
+    if rank != 0:
+        return None
     return {"schema_version": RESULT_SCHEMA_VERSION, "method": "stoPEPS",
             "parameters": parameter_dict(c), "model": parameter_dict(c)["model"],
             "observables": {"curve": curve, "purification": list(checkpoint.purification),
@@ -291,5 +355,5 @@ def run_stochastic(c: RunConfig, checkpoint: ThermalCheckpoint, uniforms_fn=None
             "diagnostics": {"born_draws": draws, "born_grouping": grouping, "events": [],
                             "history": list(checkpoint.history)},
             "metadata": {"run_id": checkpoint.run_id, "stage": "stochastic", "complete": True,
-                         "mpi_size": 1, "restart_supported": False,
+                         "mpi_size": nprocs, "restart_supported": False,
                          "uncertainty": "conditional_particle_delta_method; shared_history_scale_fixed"}}

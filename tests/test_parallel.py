@@ -1,0 +1,143 @@
+"""The sharded ensemble driver on world-size-2 gloo (CPU), against the serial run.
+
+The numerical operations are supplied by the CPU oracle through the drivers'
+ops interface, so this tests the host-side distribution logic of
+``run_stochastic`` (round-robin draws, representative owners, record
+gathers, collective error propagation) without a GPU.
+"""
+import datetime
+import math
+import multiprocessing as mp
+import os
+import socket
+import sys
+
+import numpy as np
+import pytest
+
+ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+
+
+class OracleOps:
+    """The drivers' ops on the CPU oracle (test-only)."""
+
+    def __init__(self, c):
+        from oracle import boundary as bm, full_update as fu, model as md
+        self.c = c
+        self.bm, self.fu, self.md = bm, fu, md
+
+    def _m(self, m):
+        sp = None if m.sector_space is None else (m.sector_space.n0, m.sector_space.n1)
+        return self.bm.BoundaryMPS(m.chi, sp)
+
+    def identity(self):
+        st = self.md.identity_pepo(self.c.lattice.Lx, self.c.lattice.Ly)
+        rec = self.md.normalize_state(st)
+        return st, [v for _, v in rec]
+
+    def sampling_cache(self, state, method):
+        from oracle import sampling as sp
+        return sp.SamplingCache(state, self._m(method))
+
+    def sample(self, cache, uniforms):
+        from oracle import sampling as sp
+        d = sp.sample_configuration(cache, uniforms=uniforms)
+        return dict(configuration=np.asarray(d["configuration"]), log_probability=d["log_probability"],
+                    max_environment_truncation=d["max_environment_truncation"])
+
+    def project(self, state, configuration):
+        from oracle import sampling as sp
+        st, rec = sp.project_configuration(state, np.asarray(configuration).tolist())
+        return st, [v for _, v in rec]
+
+    def measure_energy(self, state, method):
+        from oracle import sampling as sp
+        m = sp.measure_energy(state, self.md.TFIM(self.c.model.J, self.c.model.h), self._m(method))
+        return dict(m)
+
+    def lognorm(self, state, method):
+        return dict(self.bm.lognorm(state, self._m(method)))
+
+    def evolution_step(self, state, delta, D, method, space):
+        u = self.c.update
+        opts = self.fu.FullUpdate(u.max_iterations, u.error_tolerance, u.diagonal_shift,
+                                  u.linear_max_iterations, u.linear_tolerance)
+        r = self.fu.evolution_step(state, self.md.TFIM(self.c.model.J, self.c.model.h), delta, D, opts,
+                                   self._m(method), order=self.c.trotter_order,
+                                   space=None if space is None else (space.n0, space.n1),
+                                   record_entropy=self.c.record_boundary_entropy)
+        return dict(r, log_normalization_sum=sum(v for _, v in r["normalizations"]))
+
+
+def _config(sps):
+    return sps.RunConfig(lattice=sps.Lattice(2, 2), model=sps.TFIM(1.0, 0.7), beta0=0.1, beta_log=[0.1, 0.2],
+                         beta_measure=[0.1, 0.2], delta_tau_pur=0.05, delta_tau_peps=0.05, D_pur=2, D_peps=2,
+                         chi_environment=4, Ns=5, seed=9, resampling=sps.ResamplingOptions(enabled=False))
+
+
+def _run(sps, execution=None, fail_rank=None):
+    c = _config(sps)
+    ops = OracleOps(c)
+    if fail_rank is not None and execution is not None and execution.rank() == fail_rank:
+        def bad(*a, **k):
+            raise RuntimeError("planted failure")
+        ops.sample = bad
+    cp = sps.run_purification(c, ops=ops, identity=ops.identity)
+    return sps.run_stochastic(c, cp, execution=execution, ops=ops)
+
+
+def _worker(rank, world, port, q, fail_rank):
+    os.environ["MASTER_ADDR"] = "127.0.0.1"
+    os.environ["MASTER_PORT"] = str(port)
+    sys.path.insert(0, ROOT)
+    import torch.distributed as dist
+    dist.init_process_group("gloo", rank=rank, world_size=world, timeout=datetime.timedelta(seconds=120))
+    try:
+        import __graft_entry__ as ge
+        sps = ge.load_package()
+        try:
+            res = _run(sps, sps.TorchExecution(), fail_rank)
+            out = None if res is None else [(r["beta"], r["energy_per_site"], r["lnZ"], r["eta"])
+                                             for r in res["observables"]["curve"]]
+            q.put((rank, "ok", out, None if res is None else res["metadata"]["mpi_size"]))
+        except RuntimeError as ex:
+            q.put((rank, "error", str(ex), None))
+    finally:
+        dist.destroy_process_group()
+
+
+def _free_port():
+    with socket.socket() as s:
+        s.bind(("127.0.0.1", 0))
+        return s.getsockname()[1]
+
+
+def _spawn(world, fail_rank=None):
+    ctx = mp.get_context("spawn")
+    q = ctx.Queue()
+    port = _free_port()
+    procs = [ctx.Process(target=_worker, args=(r, world, port, q, fail_rank)) for r in range(world)]
+    for p in procs:
+        p.start()
+    results = [q.get(timeout=600) for _ in procs]
+    for p in procs:
+        p.join(timeout=120)
+    return sorted(results)
+
+
+def test_two_ranks_match_serial(sps):
+    serial = _run(sps)
+    ref = [(r["beta"], r["energy_per_site"], r["lnZ"], r["eta"]) for r in serial["observables"]["curve"]]
+    results = _spawn(2)
+    assert [r[1] for r in results] == ["ok", "ok"]
+    rank0 = results[0]
+    assert rank0[3] == 2 and results[1][2] is None      # rank 0 returns the record, rank 1 nothing
+    for a, b in zip(rank0[2], ref):
+        for x, y in zip(a, b):
+            assert (math.isnan(x) and math.isnan(y)) or abs(x - y) <= 1e-12 * max(1.0, abs(y))
+
+
+def test_failure_on_one_rank_raises_on_all(sps):
+    results = _spawn(2, fail_rank=1)
+    assert [r[1] for r in results] == ["error", "error"]
+    assert all("planted failure" in r[2] for r in results)
