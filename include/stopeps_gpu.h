@@ -123,6 +123,13 @@ int sps_la_qr(sps_handle* h, int32_t m, int32_t n, const double* a, double* q, d
  * boundary SVD), m >= n: a = u diag(s) v^T, u (m x n), s (n). */
 int sps_la_svd_left(sps_handle* h, int32_t m, int32_t n, const double* a, double* u, double* s, int32_t* sweeps,
                     double* ms);
+/* Leading k singular triplets by block subspace iteration with Rayleigh-Ritz
+ * extraction (the truncated boundary SVD when no entropy is recorded):
+ * u (m x k), s (k, descending), v (n x k), column-major; iterations = the
+ * count used.  SPS_ERR_CONVERGENCE when the residuals did not reach rounding
+ * level within the iteration cap. */
+int sps_la_svd_topk(sps_handle* h, int32_t m, int32_t n, int32_t k, const double* a, double* u, double* s,
+                    double* v, int32_t* iterations, double* ms);
 
 /* No counterpart in the reference.  The one-sided Jacobi SVD of one small
  * matrix for callers that cannot allocate device memory (no cudaMalloc /

@@ -10,6 +10,7 @@
 // Grid barriers are software barriers inside cooperative launches (all CTAs
 // co-resident); every spin is bounded and reports through the device flag.
 #include "engine.h"
+#include "coop.cuh"
 #include <cfloat>
 #include <cstring>
 #include <algorithm>
@@ -20,13 +21,6 @@ namespace la {
 
 static constexpr int BT = 256;
 static constexpr int BW = BT / 32;
-static constexpr int FLAG_BARRIER = 4;
-static constexpr int FLAG_CONV = 2;
-
-__device__ __forceinline__ double wsum(double v) {
-  for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
-  return v;
-}
 
 __device__ double bsum(double v, double* red) {
   v = wsum(v);
@@ -42,33 +36,7 @@ __device__ double bsum(double v, double* red) {
   return red[BW];
 }
 
-// bar[0] = arrival count, bar[1] = generation.  Acquire/release ordering at
-// gpu scope; the spin is bounded (a fault is the only way to reach the cap,
-// since every CTA of a cooperative launch is co-resident).
-__device__ void grid_barrier(unsigned* bar, int* flag) {
-  __syncthreads();
-  if (threadIdx.x == 0) {
-    unsigned g;
-    asm volatile("ld.acquire.gpu.u32 %0, [%1];" : "=r"(g) : "l"(bar + 1) : "memory");
-    unsigned arrived;
-    asm volatile("atom.add.acq_rel.gpu.u32 %0, [%1], 1;" : "=r"(arrived) : "l"(bar) : "memory");
-    if (arrived == gridDim.x - 1) {
-      asm volatile("st.relaxed.gpu.u32 [%0], 0;" ::"l"(bar) : "memory");
-      asm volatile("red.release.gpu.add.u32 [%0], 1;" ::"l"(bar + 1) : "memory");
-    } else {
-      long long spins = 0;
-      unsigned cur;
-      do {
-        asm volatile("ld.acquire.gpu.u32 %0, [%1];" : "=r"(cur) : "l"(bar + 1) : "memory");
-        if (++spins > (1ll << 27)) {
-          atomicOr(flag, FLAG_BARRIER);
-          break;
-        }
-      } while (cur == g);
-    }
-  }
-  __syncthreads();
-}
+__device__ void grid_barrier(unsigned* bar, int* flag) { group_barrier(bar, gridDim.x, flag); }
 
 // ---------------------------------------------------------------------------
 // dense column-major GEMM: C = alpha op(A) B + beta C, split-K into partials

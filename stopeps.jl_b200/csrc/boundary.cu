@@ -63,7 +63,7 @@ CompressReport compress_boundary(Engine& E, std::vector<Tensor>& B, const BMPS& 
     for (int x = 0; x < N - 1; ++x) {
       Tensor U, R;
       double err, nrm, entv;
-      if (svd_prefers_kept(B[x], {0, 1}, {2})) {
+      if (svd_prefers_kept(B[x], {0, 1}, {2}, tr, ent != nullptr)) {
         KeptSVD f = svd_kept(E, B[x], {0, 1}, {2}, tr, ent != nullptr, true);
         U = f.F;
         R = f.W;   // S V^T = U^T M
@@ -94,7 +94,7 @@ CompressReport compress_boundary(Engine& E, std::vector<Tensor>& B, const BMPS& 
     for (int x = N - 1; x >= 1; --x) {
       Tensor V, L;
       double err, nrm, entv;
-      if (svd_prefers_kept(B[x], {0}, {1, 2})) {
+      if (svd_prefers_kept(B[x], {0}, {1, 2}, tr, ent != nullptr)) {
         KeptSVD f = svd_kept(E, B[x], {0}, {1, 2}, tr, ent != nullptr, false);
         V = f.F;
         L = f.W;   // U S = M V

@@ -257,6 +257,44 @@ int sps_la_svd_left(sps_handle* h, int32_t m, int32_t n, const double* a, double
   });
 }
 
+int sps_la_svd_topk(sps_handle* h, int32_t m, int32_t n, int32_t k, const double* a, double* u, double* s,
+                    double* v, int32_t* iterations, double* ms) {
+  return guarded(h, [&] {
+    Engine& E = *h->E;
+    if (k < 1 || la::topk_block_size(k, m, n) == 0)
+      throw Error(SPS_ERR_ARGUMENT, "sps_la_svd_topk needs 1 <= k and a block at least twice the iteration width");
+    if (!la::topk_fits(k, m, n, 1, E)) throw Error(SPS_ERR_ARGUMENT, "sps_la_svd_topk: block too large");
+    Buf ba, bu;
+    double* da = dev_copy(E, ba, a, (size_t)m * n);
+    bu = E.alloc(sizeof(double) * (size_t)(m + n) * k);
+    std::vector<la::TopkDesc> ds(1);
+    ds[0].M = da;
+    ds[0].m = m;
+    ds[0].n = n;
+    ds[0].k = k;
+    ds[0].U = (double*)bu->ptr;
+    ds[0].V = ds[0].U + (size_t)m * k;
+    if (!h->t0) {
+      SPS_CUDA(cudaEventCreate(&h->t0));
+      SPS_CUDA(cudaEventCreate(&h->t1));
+    }
+    SPS_CUDA(cudaEventRecord(h->t0, E.stream));
+    la::svd_topk(E, ds, 5e-14);
+    SPS_CUDA(cudaEventRecord(h->t1, E.stream));
+    SPS_CUDA(cudaMemcpyAsync(u, ds[0].U, sizeof(double) * (size_t)m * k, cudaMemcpyDeviceToHost, E.stream));
+    SPS_CUDA(cudaMemcpyAsync(v, ds[0].V, sizeof(double) * (size_t)n * k, cudaMemcpyDeviceToHost, E.stream));
+    E.sync();
+    float f = 0;
+    SPS_CUDA(cudaEventElapsedTime(&f, h->t0, h->t1));
+    for (int i = 0; i < k; ++i) s[i] = ds[0].s[i];
+    if (ms) *ms = f;
+    if (iterations) *iterations = ds[0].iterations;
+    if (ds[0].status != 0)
+      throw Error(SPS_ERR_CONVERGENCE, "sps_la_svd_topk: subspace iteration did not converge (status " +
+                                           std::to_string(ds[0].status) + ")");
+  });
+}
+
 int sps_la_qr(sps_handle* h, int32_t m, int32_t n, const double* a, double* q, double* r, double* ms) {
   return guarded(h, [&] {
     Engine& E = *h->E;

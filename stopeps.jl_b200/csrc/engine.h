@@ -128,6 +128,10 @@ class Engine {
   double* dscal = nullptr;
   static constexpr int NSCAL = 4096;
 
+  // starting iteration count of the subspace-iteration SVD (adapted per call)
+  int topk_hint = 6;
+  int topk_streak = 0;
+
   // counters
   long long launches = 0;
   double flops = 0;
@@ -207,7 +211,9 @@ struct KeptSVD {
 };
 KeptSVD svd_kept(Engine& E, const Tensor& A, const std::vector<int>& rows, const std::vector<int>& cols,
                  const Trunc& tr, bool want_entropy, bool left);
-bool svd_prefers_kept(const Tensor& A, const std::vector<int>& rows, const std::vector<int>& cols);
+// true when the kept-vector path (svd_kept) beats the full SVD for this view
+bool svd_prefers_kept(const Tensor& A, const std::vector<int>& rows, const std::vector<int>& cols, const Trunc& tr,
+                      bool want_entropy);
 // eigendecomposition of a symmetric block matrix (rows | cols must match)
 struct EIGres {
   std::vector<double> w[2];   // eigenvalues (ascending) per block
@@ -248,6 +254,21 @@ void dgemm_cm(Engine& E, bool ta, int M, int N, int K, double alpha, const doubl
               int ldb, double beta, double* C, int ldc);
 bool qr_is_big(int m, int n);
 bool svd_is_big(int m, int n);
+// leading k singular triplets of an m x n column-major block (ld m) by block
+// subspace iteration with Rayleigh-Ritz extraction (topk.cu)
+struct TopkDesc {
+  const double* M;
+  int m, n, k;
+  double* U;                 // m x k (ld m), left vectors, descending values
+  double* V;                 // n x k (ld n), right vectors
+  // results
+  int b = 0, status = -1, iterations = 0;
+  double fro2 = 0, residual = 0;   // ||M||_F^2; largest residual / acceptance threshold
+  std::vector<double> s;     // b Ritz values, descending (the first k are the wanted values)
+};
+int topk_block_size(int k, int m, int n);   // 0 when the block is too small for the method
+bool topk_fits(int k, int m, int n, int nprob, Engine& E);
+void svd_topk(Engine& E, std::vector<TopkDesc>& ds, double tol);
 }  // namespace la
 
 // gather/scatter between tensors and dense column-major block matrices

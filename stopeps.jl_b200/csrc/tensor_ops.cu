@@ -1196,19 +1196,173 @@ SVDres svd(Engine& E, const Tensor& A, const std::vector<int>& rows, const std::
   return res;
 }
 
-bool svd_prefers_kept(const Tensor& A, const std::vector<int>& rows, const std::vector<int>& cols) {
+bool svd_prefers_kept(const Tensor& A, const std::vector<int>& rows, const std::vector<int>& cols, const Trunc& tr,
+                      bool want_entropy) {
   BlockTables bt = tables_of(A, rows, cols);
   for (int c = 0; c < 2; ++c)
     if (std::min(bt.rt[c].size(), bt.ct[c].size()) >= 160) return true;
-  return false;
+  if (want_entropy) return false;
+  // blocks that suit the subspace iteration (a few kept vectors of a larger block)
+  bool any = false;
+  for (int c = 0; c < 2; ++c) {
+    const int m = (int)bt.rt[c].size(), n = (int)bt.ct[c].size();
+    if (std::min(m, n) == 0) continue;
+    int k = std::min(m, n);
+    if (tr.chi >= 0) k = std::min(k, tr.chi);
+    if (tr.space[0] >= 0) k = std::min(k, tr.space[c]);
+    if (k < 1 || std::max(m, n) < 96 || la::topk_block_size(k, m, n) == 0) return false;
+    any = true;
+  }
+  return any;
+}
+
+// Output tensors of a kept-vector truncated SVD.  Block c has the gathered
+// matrix Mb[c] (m x n, ld m) and its wanted vectors Fv[c] (left: m x kk, ld m;
+// right: n x kk, ld n, as columns); F holds those vectors, W the other factor
+// from one GEMM with the matrix (left: W = U_k^T M; right: W = M V_k).
+static void kept_assemble(Engine& E, const BlockTables& bt, int nr, int nc, bool left, const int m[2],
+                          const int n[2], const int kk[2], double* const Mb[2], double* const Fv[2], KeptSVD& res) {
+  std::vector<Buf> keep;
+  Par nl = make_par(kk[0], kk[1]);
+  if (left) {
+    std::vector<Par> fl = bt.rp;
+    fl.push_back(nl);
+    std::vector<Par> wl{nl};
+    wl.insert(wl.end(), bt.cp.begin(), bt.cp.end());
+    res.F = E.zeros(fl);
+    res.W = E.zeros(wl);
+  } else {
+    std::vector<Par> fl{nl};
+    fl.insert(fl.end(), bt.cp.begin(), bt.cp.end());
+    std::vector<Par> wl = bt.rp;
+    wl.push_back(nl);
+    res.F = E.zeros(fl);
+    res.W = E.zeros(wl);
+  }
+  for (int c = 0; c < 2; ++c) {
+    if (kk[c] == 0) continue;
+    Buf wb = E.alloc(sizeof(double) * (size_t)std::max(m[c], n[c]) * kk[c]);
+    double* Wm = (double*)wb->ptr;
+    Buf t1, t2, t3, t4;
+    if (left) {
+      la::dgemm_cm(E, true, kk[c], n[c], m[c], 1.0, Fv[c], m[c], Mb[c], m[c], 0.0, Wm, kk[c]);
+      auto frow = tensor_rows(res.F, 0, nr, c);
+      auto fcol = leg_offsets(c, kk[0], kk[1], res.F.strides[nr]);
+      scatter_block(E, res.F, E.upload_i64(frow, t1), E.upload_i64(fcol, t2), m[c], kk[c], Fv[c], m[c], false);
+      auto wrow = leg_offsets(c, kk[0], kk[1], res.W.strides[0]);
+      auto wcol = tensor_rows(res.W, 1, nc, c);
+      scatter_block(E, res.W, E.upload_i64(wrow, t3), E.upload_i64(wcol, t4), kk[c], n[c], Wm, kk[c], false);
+    } else {
+      la::dgemm_cm(E, false, m[c], kk[c], n[c], 1.0, Mb[c], m[c], Fv[c], n[c], 0.0, Wm, m[c]);
+      auto frow = leg_offsets(c, kk[0], kk[1], res.F.strides[0]);
+      auto fcol = tensor_rows(res.F, 1, nc, c);
+      scatter_block(E, res.F, E.upload_i64(frow, t1), E.upload_i64(fcol, t2), kk[c], n[c], Fv[c], n[c], true);
+      auto wrow = tensor_rows(res.W, 0, nr, c);
+      auto wcol = leg_offsets(c, kk[0], kk[1], res.W.strides[nr]);
+      scatter_block(E, res.W, E.upload_i64(wrow, t3), E.upload_i64(wcol, t4), m[c], kk[c], Wm, m[c], false);
+    }
+    keep.insert(keep.end(), {wb, t1, t2, t3, t4});
+  }
+}
+
+// Kept sets of a truncation from per-block leading values; every kept set must
+// be a prefix of its block.
+static void kept_counts(const std::vector<double> sv[2], const Trunc& tr, const char* who, int kk[2], KeptSVD& res,
+                        double& kept2, double& disc2) {
+  std::vector<char> kp[2];
+  select_truncation(sv, tr, kp);
+  kk[0] = kk[1] = 0;
+  kept2 = disc2 = 0;
+  for (int c = 0; c < 2; ++c)
+    for (size_t i = 0; i < sv[c].size(); ++i) {
+      if (kp[c][i]) {
+        if ((int)i != kk[c]) throw Error(SPS_ERR_NUMERIC, std::string(who) + ": non-prefix truncation");
+        kk[c]++;
+        res.S[c].push_back(sv[c][i]);
+        kept2 += sv[c][i] * sv[c][i];
+      } else {
+        disc2 += sv[c][i] * sv[c][i];
+      }
+    }
+}
+
+// Leading vectors by subspace iteration (la::svd_topk): only the values that
+// the truncation can keep are computed; the discarded weight is ||M||_F^2 minus
+// the kept weight.  Returns false when a block does not suit the method or the
+// iteration did not converge; the caller then uses the full spectrum.
+static bool svd_kept_topk(Engine& E, const BlockTables& bt, const Tensor& A, int nr, int nc, const Trunc& tr,
+                          bool left, KeptSVD& res) {
+  int m[2], n[2], kmax[2];
+  std::vector<la::TopkDesc> ds;
+  int dmap[2] = {-1, -1};
+  int nprob = 0;
+  for (int c = 0; c < 2; ++c) {
+    m[c] = (int)bt.rt[c].size();
+    n[c] = (int)bt.ct[c].size();
+    kmax[c] = std::min(m[c], n[c]);
+    if (tr.chi >= 0) kmax[c] = std::min(kmax[c], tr.chi);
+    if (tr.space[0] >= 0) kmax[c] = std::min(kmax[c], tr.space[c]);
+    if (std::min(m[c], n[c]) == 0) continue;
+    if (kmax[c] < 1 || la::topk_block_size(kmax[c], m[c], n[c]) == 0) return false;
+    nprob++;
+  }
+  for (int c = 0; c < 2; ++c)
+    if (std::min(m[c], n[c]) > 0 && !la::topk_fits(kmax[c], m[c], n[c], nprob, E)) return false;
+  if (nprob == 0) return false;
+  std::vector<Buf> keep;
+  double* Mb[2] = {nullptr, nullptr};
+  double* Fv[2] = {nullptr, nullptr};
+  for (int c = 0; c < 2; ++c) {
+    if (std::min(m[c], n[c]) == 0) continue;
+    Buf t1, t2;
+    int64_t* rt = E.upload_i64(bt.rt[c], t1);
+    int64_t* ct = E.upload_i64(bt.ct[c], t2);
+    Buf mb = E.alloc(sizeof(double) * ((size_t)m[c] * n[c] + (size_t)(m[c] + n[c]) * kmax[c]));
+    keep.insert(keep.end(), {t1, t2, mb});
+    Mb[c] = (double*)mb->ptr;
+    gather_block(E, A, rt, ct, m[c], n[c], Mb[c], m[c], false);
+    la::TopkDesc d;
+    d.M = Mb[c];
+    d.m = m[c];
+    d.n = n[c];
+    d.k = kmax[c];
+    d.U = Mb[c] + (size_t)m[c] * n[c];
+    d.V = d.U + (size_t)m[c] * kmax[c];
+    Fv[c] = left ? d.U : d.V;
+    dmap[c] = (int)ds.size();
+    ds.push_back(d);
+  }
+  la::svd_topk(E, ds, 5e-14);
+  for (auto& d : ds)
+    if (d.status != 0) return false;
+  std::vector<double> sv[2];
+  double fro2 = 0;
+  for (int c = 0; c < 2; ++c) {
+    if (dmap[c] < 0) continue;
+    const la::TopkDesc& d = ds[dmap[c]];
+    sv[c].assign(d.s.begin(), d.s.begin() + kmax[c]);
+    fro2 += d.fro2;
+  }
+  int kk[2];
+  double kept2, disc2;
+  kept_counts(sv, tr, "svd_kept", kk, res, kept2, disc2);
+  res.norm = std::sqrt(fro2);
+  res.err = std::sqrt(std::max(0.0, fro2 - kept2));
+  kept_assemble(E, bt, nr, nc, left, m, n, kk, Mb, Fv, res);
+  return true;
 }
 
 KeptSVD svd_kept(Engine& E, const Tensor& A, const std::vector<int>& rows, const std::vector<int>& cols,
                  const Trunc& tr, bool want_entropy, bool left) {
   BlockTables bt = tables_of(A, rows, cols);
+  const int nr = (int)rows.size(), nc = (int)cols.size();
+  if (!want_entropy) {
+    KeptSVD res;
+    if (svd_kept_topk(E, bt, A, nr, nc, tr, left, res)) return res;
+  }
   int m[2], n[2], k[2];
   struct Work { Buf mb, xb, qb, rb, sb, ub; double *M, *X, *U, *s; int mx, nx; bool direct; };
-  Work w[2];
+  Work w[2] = {};
   std::vector<la::MatDesc> jac;
   int jmap[2] = {-1, -1};
   std::vector<Buf> keep;
@@ -1302,65 +1456,13 @@ KeptSVD svd_kept(Engine& E, const Tensor& A, const std::vector<int>& rows, const
       res.entropy = std::max(0.0, ent);
     }
   }
-  std::vector<char> kp[2];
-  select_truncation(sv, tr, kp);
-  int kk[2] = {0, 0};
-  double disc = 0;
-  for (int c = 0; c < 2; ++c)
-    for (size_t i = 0; i < sv[c].size(); ++i) {
-      if (kp[c][i]) {
-        if ((int)i != kk[c]) throw Error(SPS_ERR_NUMERIC, "svd_kept: non-prefix truncation");
-        kk[c]++;
-        res.S[c].push_back(sv[c][i]);
-      } else {
-        disc += sv[c][i] * sv[c][i];
-      }
-    }
-  res.err = std::sqrt(disc);
-  Par nl = make_par(kk[0], kk[1]);
-  int nr = (int)rows.size(), nc = (int)cols.size();
-  if (left) {
-    std::vector<Par> fl = bt.rp;
-    fl.push_back(nl);
-    std::vector<Par> wl{nl};
-    wl.insert(wl.end(), bt.cp.begin(), bt.cp.end());
-    res.F = E.zeros(fl);
-    res.W = E.zeros(wl);
-  } else {
-    std::vector<Par> fl{nl};
-    fl.insert(fl.end(), bt.cp.begin(), bt.cp.end());
-    std::vector<Par> wl = bt.rp;
-    wl.push_back(nl);
-    res.F = E.zeros(fl);
-    res.W = E.zeros(wl);
-  }
-  for (int c = 0; c < 2; ++c) {
-    if (jmap[c] < 0 || kk[c] == 0) continue;
-    Work& W = w[c];
-    Buf wb = E.alloc(sizeof(double) * (size_t)std::max(m[c], n[c]) * kk[c]);
-    double* Wm = (double*)wb->ptr;
-    Buf t1, t2, t3, t4;
-    if (left) {
-      // U_k = first kk columns (m x kk, ld m); W = U_k^T M (kk x n)
-      la::dgemm_cm(E, true, kk[c], n[c], m[c], 1.0, W.U, m[c], W.M, m[c], 0.0, Wm, kk[c]);
-      auto frow = tensor_rows(res.F, 0, nr, c);
-      auto fcol = leg_offsets(c, kk[0], kk[1], res.F.strides[nr]);
-      scatter_block(E, res.F, E.upload_i64(frow, t1), E.upload_i64(fcol, t2), m[c], kk[c], W.U, m[c], false);
-      auto wrow = leg_offsets(c, kk[0], kk[1], res.W.strides[0]);
-      auto wcol = tensor_rows(res.W, 1, nc, c);
-      scatter_block(E, res.W, E.upload_i64(wrow, t3), E.upload_i64(wcol, t4), kk[c], n[c], Wm, kk[c], false);
-    } else {
-      // V_k = first kk columns (n x kk, ld n); W = M V_k (m x kk)
-      la::dgemm_cm(E, false, m[c], kk[c], n[c], 1.0, W.M, m[c], W.U, n[c], 0.0, Wm, m[c]);
-      auto frow = leg_offsets(c, kk[0], kk[1], res.F.strides[0]);
-      auto fcol = tensor_rows(res.F, 1, nc, c);
-      scatter_block(E, res.F, E.upload_i64(frow, t1), E.upload_i64(fcol, t2), kk[c], n[c], W.U, n[c], true);
-      auto wrow = tensor_rows(res.W, 0, nr, c);
-      auto wcol = leg_offsets(c, kk[0], kk[1], res.W.strides[nr]);
-      scatter_block(E, res.W, E.upload_i64(wrow, t3), E.upload_i64(wcol, t4), m[c], kk[c], Wm, m[c], false);
-    }
-    keep.insert(keep.end(), {wb, t1, t2, t3, t4});
-  }
+  int kk[2];
+  double kept2, disc2;
+  kept_counts(sv, tr, "svd_kept", kk, res, kept2, disc2);
+  res.err = std::sqrt(disc2);
+  double* Mb[2] = {w[0].M, w[1].M};
+  double* Fv[2] = {w[0].U, w[1].U};
+  kept_assemble(E, bt, nr, nc, left, m, n, kk, Mb, Fv, res);
   return res;
 }
 

@@ -117,6 +117,19 @@ class Engine:
                                             _arr(s, C.c_double), C.byref(sw), C.byref(ms)))
         return u, s, sw.value, ms.value
 
+    def la_svd_topk(self, a, k):
+        """Leading k singular triplets by subspace iteration: (u, s, v, iterations, device_ms)."""
+        a = np.asfortranarray(np.asarray(a, np.float64))
+        m, n = a.shape
+        u = np.zeros((m, k), order="F")
+        v = np.zeros((n, k), order="F")
+        s = np.zeros(k)
+        it = C.c_int32()
+        ms = C.c_double()
+        self.check(self.lib.sps_la_svd_topk(self.h, m, n, k, _arr(a, C.c_double), _arr(u, C.c_double),
+                                            _arr(s, C.c_double), _arr(v, C.c_double), C.byref(it), C.byref(ms)))
+        return u, s, v, it.value, ms.value
+
     def la_qr(self, a):
         """Engine Householder QR of one host matrix: (q, r, device_ms)."""
         a = np.asfortranarray(np.asarray(a, np.float64))

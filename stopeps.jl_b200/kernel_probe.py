@@ -2,6 +2,7 @@
 
   python stopeps.jl_b200/kernel_probe.py svd_left   # U-only Jacobi of a 648x648 LQ-preconditioned block
   python stopeps.jl_b200/kernel_probe.py qr          # blocked Householder QR of a 23328x648 block
+  python stopeps.jl_b200/kernel_probe.py topk        # leading 18 triplets of a 648x648 graded block
   python stopeps.jl_b200/kernel_probe.py draw        # one Born draw, 8x8 D=6 chi=36 (synthetic PEPO)
 
 Each operation runs once to warm up and once more; the sizes are those of the
@@ -37,6 +38,12 @@ def main(which):
         for _ in range(2):
             u, s, sweeps, ms = e.la_svd_left(L)
         print(f"svd_left 648x648: {ms:.2f} ms, {sweeps} sweeps")
+    elif which == "topk":
+        e = sps.Engine(2, 2)
+        a = graded(648, 648, 0.1, 5)
+        for _ in range(2):
+            u, s, v, iters, ms = e.la_svd_topk(a, 18)
+        print(f"topk 648x648 k=18: {ms:.3f} ms, {iters} iterations")
     elif which == "qr":
         e = sps.Engine(2, 2)
         a = np.random.default_rng(3).standard_normal((23328, 648))

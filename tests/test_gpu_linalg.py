@@ -3,7 +3,9 @@
 Householder QR (single-CTA and blocked multi-CTA) and one-sided Jacobi SVD
 (single-CTA, cooperative element-pair and block variants) must reproduce the
 factorizations to roundoff: A = QR with orthonormal Q, and the singular
-values of LAPACK gesdd with orthonormal singular vectors.
+values of LAPACK gesdd with orthonormal singular vectors.  The subspace
+iteration for the leading singular triplets must reproduce LAPACK's leading
+values and its rank-k truncation to roundoff.
 """
 import numpy as np
 import pytest
@@ -59,3 +61,22 @@ def test_left_jacobi_matches_lapack(eng, m, n):
     np.testing.assert_allclose(u.T @ u, np.eye(n), atol=1e-10)
     top = min(n, 36)
     np.testing.assert_allclose(np.abs(np.sum(u[:, :top] * ref_u[:, :top], axis=0)), 1.0, atol=1e-9)
+
+
+@pytest.mark.parametrize("m,n,k,decay", [(648, 648, 18, 0.1), (648, 648, 36, 0.1), (648, 648, 18, 0.03),
+                                         (1296, 648, 18, 0.08), (500, 900, 30, 0.06), (128, 128, 8, 0.2),
+                                         (2048, 2048, 32, 0.05)])
+def test_topk_matches_lapack(eng, m, n, k, decay):
+    """Leading singular triplets by block subspace iteration (truncated boundary SVD)."""
+    a = graded(m, n, decay, 5 * m + n + k)
+    u, s, v, iters, ms = eng.la_svd_topk(a, k)
+    ref_u, ref_s, ref_vt = np.linalg.svd(a, full_matrices=False)
+    np.testing.assert_allclose(s, ref_s[:k], rtol=1e-12, atol=1e-13 * ref_s[0])
+    np.testing.assert_allclose(u.T @ u, np.eye(k), atol=1e-12)
+    np.testing.assert_allclose(v.T @ v, np.eye(k), atol=1e-12)
+    # the rank-k truncation is LAPACK's
+    mine = u @ (u.T @ a)
+    ref = ref_u[:, :k] @ (ref_u[:, :k].T @ a)
+    assert np.linalg.norm(mine - ref) <= 1e-12 * ref_s[0]
+    np.testing.assert_allclose(a @ v, u * s, atol=1e-12 * ref_s[0])
+    assert 1 <= iters <= 48
