@@ -123,6 +123,11 @@ int sps_la_qr(sps_handle* h, int32_t m, int32_t n, const double* a, double* q, d
  * boundary SVD), m >= n: a = u diag(s) v^T, u (m x n), s (n). */
 int sps_la_svd_left(sps_handle* h, int32_t m, int32_t n, const double* a, double* u, double* s, int32_t* sweeps,
                     double* ms);
+/* Dense FP64 GEMM of the factorizations: c = alpha op(a) b + beta c, all
+ * column-major; op(a) = a (m x k, ld m) or a^T (a is k x m, ld k); b k x n
+ * (ld k); c m x n (ld m). */
+int sps_la_gemm(sps_handle* h, int32_t transpose_a, int32_t m, int32_t n, int32_t k, double alpha, const double* a,
+                const double* b, double beta, double* c, double* ms);
 /* Leading k singular triplets by block subspace iteration with Rayleigh-Ritz
  * extraction (the truncated boundary SVD when no entropy is recorded):
  * u (m x k), s (k, descending), v (n x k), column-major; iterations = the

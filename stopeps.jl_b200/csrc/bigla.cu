@@ -3,7 +3,7 @@
 //
 //  * blocked Householder QR: a cooperative panel kernel (one pass over the
 //    panel rows per column, two grid barriers per column) and compact-WY
-//    trailing updates / Q formation as dense FP64 GEMMs with split-K;
+//    trailing updates / Q formation as dense FP64 GEMMs (dgemm.cu);
 //  * one-sided Jacobi SVD with every column pair of a round rotated by its
 //    own warp across the whole GPU and a grid barrier between rounds.
 //
@@ -38,125 +38,6 @@ __device__ double bsum(double v, double* red) {
 
 __device__ void grid_barrier(unsigned* bar, int* flag) { group_barrier(bar, gridDim.x, flag); }
 
-// ---------------------------------------------------------------------------
-// dense column-major GEMM: C = alpha op(A) B + beta C, split-K into partials
-// ---------------------------------------------------------------------------
-static constexpr int GM = 64, GN = 64, GK = 16;
-
-template <bool TA>
-__global__ void __launch_bounds__(BT) dgemm_cm_kernel(int M, int N, int K, const double* __restrict__ A, int lda,
-                                                      const double* __restrict__ B, int ldb, double* __restrict__ C,
-                                                      int ldc, double alpha, double beta, int kchunk,
-                                                      double* __restrict__ partial) {
-  const int i0 = blockIdx.y * GM, j0 = blockIdx.x * GN;
-  const int kbeg = blockIdx.z * kchunk, kend = min(K, kbeg + kchunk);
-  __shared__ double As[GK][GM + 1];
-  __shared__ double Bs[GK][GN + 1];
-  const int t = threadIdx.x, tx = t % 16, ty = t / 16;
-  double acc[4][4] = {};
-  for (int k0 = kbeg; k0 < kend; k0 += GK) {
-    if (TA) {   // op(A)(i,k) = A[k + i*lda]: k contiguous
-      int kk = t % 16;
-#pragma unroll
-      for (int r = 0; r < 4; ++r) {
-        int ii = t / 16 + 16 * r;
-        int i = i0 + ii, k = k0 + kk;
-        As[kk][ii] = (i < M && k < kend) ? A[k + (size_t)i * lda] : 0.0;
-      }
-    } else {    // A[i + k*lda]: i contiguous
-      int ii = t % 64;
-#pragma unroll
-      for (int r = 0; r < 4; ++r) {
-        int kk = t / 64 + 4 * r;
-        int i = i0 + ii, k = k0 + kk;
-        As[kk][ii] = (i < M && k < kend) ? A[i + (size_t)k * lda] : 0.0;
-      }
-    }
-    {
-      int kk = t % 16;
-#pragma unroll
-      for (int r = 0; r < 4; ++r) {
-        int jj = t / 16 + 16 * r;
-        int j = j0 + jj, k = k0 + kk;
-        Bs[kk][jj] = (j < N && k < kend) ? B[k + (size_t)j * ldb] : 0.0;
-      }
-    }
-    __syncthreads();
-#pragma unroll
-    for (int kk = 0; kk < GK; ++kk) {
-      double a[4], b[4];
-#pragma unroll
-      for (int u = 0; u < 4; ++u) a[u] = As[kk][ty + 16 * u];
-#pragma unroll
-      for (int v = 0; v < 4; ++v) b[v] = Bs[kk][tx + 16 * v];
-#pragma unroll
-      for (int u = 0; u < 4; ++u)
-#pragma unroll
-        for (int v = 0; v < 4; ++v) acc[u][v] = fma(a[u], b[v], acc[u][v]);
-    }
-    __syncthreads();
-  }
-#pragma unroll
-  for (int u = 0; u < 4; ++u) {
-    int i = i0 + ty + 16 * u;
-    if (i >= M) continue;
-#pragma unroll
-    for (int v = 0; v < 4; ++v) {
-      int j = j0 + tx + 16 * v;
-      if (j >= N) continue;
-      if (partial) partial[(size_t)blockIdx.z * M * N + i + (size_t)j * M] = acc[u][v];
-      else C[i + (size_t)j * ldc] = alpha * acc[u][v] + (beta == 0.0 ? 0.0 : beta * C[i + (size_t)j * ldc]);
-    }
-  }
-}
-
-__global__ void splitk_reduce_kernel(int M, int N, int splits, const double* __restrict__ partial, double* C, int ldc,
-                                     double alpha, double beta) {
-  size_t total = (size_t)M * N;
-  for (size_t e = blockIdx.x * (size_t)blockDim.x + threadIdx.x; e < total; e += (size_t)gridDim.x * blockDim.x) {
-    double s = 0;
-    for (int z = 0; z < splits; ++z) s += partial[(size_t)z * total + e];
-    int i = (int)(e % M), j = (int)(e / M);
-    double* c = C + i + (size_t)j * ldc;
-    *c = alpha * s + (beta == 0.0 ? 0.0 : beta * *c);
-  }
-}
-
-void dgemm_cm(Engine& E, bool ta, int M, int N, int K, double alpha, const double* A, int lda, const double* B,
-              int ldb, double beta, double* C, int ldc) {
-  if (M <= 0 || N <= 0) return;
-  int tiles = ((M + GM - 1) / GM) * ((N + GN - 1) / GN);
-  int splits = 1, kchunk = std::max(K, 0);
-  if (K > 256 && tiles < 2 * E.num_sms) {
-    splits = std::min((K + 255) / 256, std::max(1, (4 * E.num_sms) / tiles));
-    kchunk = (K + splits - 1) / splits;
-    kchunk = ((kchunk + GK - 1) / GK) * GK;
-    splits = (K + kchunk - 1) / kchunk;
-  }
-  dim3 grid((N + GN - 1) / GN, (M + GM - 1) / GM, splits);
-  Buf part;
-  double* partial = nullptr;
-  if (splits > 1) {
-    part = E.alloc(sizeof(double) * (size_t)splits * M * N);
-    partial = (double*)part->ptr;
-  }
-  int tk = E.tic("dgemm_cm");
-  if (ta)
-    dgemm_cm_kernel<true><<<grid, BT, 0, E.stream>>>(M, N, K, A, lda, B, ldb, C, ldc, alpha, beta, kchunk, partial);
-  else
-    dgemm_cm_kernel<false><<<grid, BT, 0, E.stream>>>(M, N, K, A, lda, B, ldb, C, ldc, alpha, beta, kchunk, partial);
-  E.toc(tk, 2.0 * M * N * (double)K, 8.0 * ((double)M * K + (double)K * N + 2.0 * M * N));
-  SPS_CUDA(cudaGetLastError());
-  E.launches++;
-  if (splits > 1) {
-    size_t total = (size_t)M * N;
-    int g = (int)std::min<size_t>((total + 255) / 256, 4096);
-    splitk_reduce_kernel<<<g, 256, 0, E.stream>>>(M, N, splits, partial, C, ldc, alpha, beta);
-    SPS_CUDA(cudaGetLastError());
-    E.launches++;
-  }
-  E.flops += 2.0 * M * N * (double)K;
-}
 
 // ---------------------------------------------------------------------------
 // cooperative panel factorization

@@ -295,6 +295,31 @@ int sps_la_svd_topk(sps_handle* h, int32_t m, int32_t n, int32_t k, const double
   });
 }
 
+int sps_la_gemm(sps_handle* h, int32_t transpose_a, int32_t m, int32_t n, int32_t k, double alpha, const double* a,
+                const double* b, double beta, double* c, double* ms) {
+  return guarded(h, [&] {
+    Engine& E = *h->E;
+    if (m < 1 || n < 1 || k < 0) throw Error(SPS_ERR_ARGUMENT, "sps_la_gemm: bad sizes");
+    Buf ba, bb, bc;
+    double* da = dev_copy(E, ba, a, (size_t)m * k);
+    double* db = dev_copy(E, bb, b, (size_t)k * n);
+    double* dc = dev_copy(E, bc, c, (size_t)m * n);
+    if (!h->t0) {
+      SPS_CUDA(cudaEventCreate(&h->t0));
+      SPS_CUDA(cudaEventCreate(&h->t1));
+    }
+    SPS_CUDA(cudaEventRecord(h->t0, E.stream));
+    la::dgemm_cm(E, transpose_a != 0, m, n, k, alpha, da, transpose_a ? std::max(k, 1) : m, db, std::max(k, 1), beta,
+                 dc, m);
+    SPS_CUDA(cudaEventRecord(h->t1, E.stream));
+    SPS_CUDA(cudaMemcpyAsync(c, dc, sizeof(double) * (size_t)m * n, cudaMemcpyDeviceToHost, E.stream));
+    E.sync();
+    float f = 0;
+    SPS_CUDA(cudaEventElapsedTime(&f, h->t0, h->t1));
+    if (ms) *ms = f;
+  });
+}
+
 int sps_la_qr(sps_handle* h, int32_t m, int32_t n, const double* a, double* q, double* r, double* ms) {
   return guarded(h, [&] {
     Engine& E = *h->E;

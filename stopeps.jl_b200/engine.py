@@ -117,6 +117,20 @@ class Engine:
                                             _arr(s, C.c_double), C.byref(sw), C.byref(ms)))
         return u, s, sw.value, ms.value
 
+    def la_gemm(self, a, b, c=None, alpha=1.0, beta=0.0, transpose_a=False):
+        """Engine FP64 GEMM alpha op(a) b + beta c: (c, device_ms)."""
+        a = np.asfortranarray(np.asarray(a, np.float64))
+        b = np.asfortranarray(np.asarray(b, np.float64))
+        m = a.shape[1] if transpose_a else a.shape[0]
+        k, n = b.shape
+        if (a.shape[0] if transpose_a else a.shape[1]) != k:
+            raise ValueError("inner dimensions differ")
+        c = np.zeros((m, n), order="F") if c is None else np.asfortranarray(np.array(c, np.float64))
+        ms = C.c_double()
+        self.check(self.lib.sps_la_gemm(self.h, int(transpose_a), m, n, k, float(alpha), _arr(a, C.c_double),
+                                        _arr(b, C.c_double), float(beta), _arr(c, C.c_double), C.byref(ms)))
+        return c, ms.value
+
     def la_svd_topk(self, a, k):
         """Leading k singular triplets by subspace iteration: (u, s, v, iterations, device_ms)."""
         a = np.asfortranarray(np.asarray(a, np.float64))

@@ -3,6 +3,7 @@
   python stopeps.jl_b200/kernel_probe.py svd_left   # U-only Jacobi of a 648x648 LQ-preconditioned block
   python stopeps.jl_b200/kernel_probe.py qr          # blocked Householder QR of a 23328x648 block
   python stopeps.jl_b200/kernel_probe.py topk        # leading 18 triplets of a 648x648 graded block
+  python stopeps.jl_b200/kernel_probe.py gemm        # FP64 GEMM 23328x648x648 and the 648x648x23328 Gram
   python stopeps.jl_b200/kernel_probe.py draw        # one Born draw, 8x8 D=6 chi=36 (synthetic PEPO)
 
 Each operation runs once to warm up and once more; the sizes are those of the
@@ -44,6 +45,17 @@ def main(which):
         for _ in range(2):
             u, s, v, iters, ms = e.la_svd_topk(a, 18)
         print(f"topk 648x648 k=18: {ms:.3f} ms, {iters} iterations")
+    elif which == "gemm":
+        e = sps.Engine(2, 2)
+        rng = np.random.default_rng(1)
+        a = rng.standard_normal((23328, 648))
+        b = rng.standard_normal((648, 648))
+        for _ in range(3):
+            c, ms = e.la_gemm(a, b)
+        print(f"gemm 23328x648x648: {ms:.3f} ms, {2 * 23328 * 648 * 648 / ms / 1e9:.2f} TFLOP/s")
+        for _ in range(3):
+            g, ms = e.la_gemm(a, a, transpose_a=True)
+        print(f"gram 648x648x23328: {ms:.3f} ms, {2 * 23328 * 648 * 648 / ms / 1e9:.2f} TFLOP/s")
     elif which == "qr":
         e = sps.Engine(2, 2)
         a = np.random.default_rng(3).standard_normal((23328, 648))

@@ -80,3 +80,17 @@ def test_topk_matches_lapack(eng, m, n, k, decay):
     assert np.linalg.norm(mine - ref) <= 1e-12 * ref_s[0]
     np.testing.assert_allclose(a @ v, u * s, atol=1e-12 * ref_s[0])
     assert 1 <= iters <= 48
+
+
+@pytest.mark.parametrize("ta", [False, True])
+@pytest.mark.parametrize("m,n,k", [(1, 1, 1), (37, 19, 5), (130, 70, 17), (648, 18, 648), (2000, 648, 648),
+                                   (648, 648, 23328), (300, 200, 0)])
+def test_gemm_matches_numpy(eng, ta, m, n, k):
+    """The FP64 tensor-core GEMM (tiled, split-K, both operand layouts) to roundoff."""
+    rng = np.random.default_rng(m + 3 * n + 7 * k + ta)
+    a = rng.standard_normal((k, m) if ta else (m, k))
+    b = rng.standard_normal((k, n))
+    c0 = rng.standard_normal((m, n))
+    c, ms = eng.la_gemm(a, b, c0, alpha=0.75, beta=-0.5, transpose_a=ta)
+    ref = 0.75 * ((a.T if ta else a) @ b) - 0.5 * c0
+    np.testing.assert_allclose(c, ref, atol=4e-13 * max(1, k) ** 0.5, rtol=1e-13)
