@@ -145,6 +145,7 @@ class Engine {
   struct KStat { double ms = 0, flops = 0, bytes = 0; long long count = 0; };
   std::map<std::string, KStat> kernel_stats();
   void reset_stats();
+  void add_stat(const std::string& name, double ms, long long count = 1);   // host-measured sub-phase
  private:
   struct Pending { std::string name; cudaEvent_t a, b; double flops, bytes; };
   std::vector<Pending> pending_;

@@ -228,6 +228,12 @@ void Engine::set_work(int id, double fl, double by) {
   pending_[id].bytes = by;
 }
 
+void Engine::add_stat(const std::string& name, double ms, long long count) {
+  auto& k = stats_[name];
+  k.ms += ms;
+  k.count += count;
+}
+
 std::map<std::string, Engine::KStat> Engine::kernel_stats() {
   SPS_CUDA(cudaStreamSynchronize(stream));
   for (auto& p : pending_) {
@@ -262,6 +268,7 @@ void Engine::check_flag(const char* where) {
   if (h) {
     SPS_CUDA(cudaMemsetAsync(dflag, 0, sizeof(int), stream));
     if (h & 2) throw Error(SPS_ERR_CONVERGENCE, std::string(where) + ": device iteration cap reached");
+    if (h & 4) throw Error(SPS_ERR_NUMERIC, std::string(where) + ": a grid barrier wait reached its cap");
     throw Error(SPS_ERR_NUMERIC, std::string(where) + ": nonfinite or singular value on device");
   }
 }

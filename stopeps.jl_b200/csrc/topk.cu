@@ -35,13 +35,13 @@ constexpr int TW = TT / 32;       // warps per CTA
 constexpr int KMAXB = 80;         // largest block size b
 constexpr int RMAX = 32;          // largest number of rows owned by one CTA
 constexpr int KC = 32;            // contraction chunk of the row GEMM
-constexpr int XLD = KC + 1;
-constexpr int SLD = KMAXB + 4;
+constexpr int NST = 4;            // pipeline stages of the row GEMM (asynchronous copies)
+constexpr int XLD = KC + 4;       // row stride of the staged operands: a fragment load is 2 wavefronts
+constexpr int STAGE = (RMAX + KMAXB) * XLD;
 constexpr int YLD = KMAXB + 1;
 constexpr int GLD = KMAXB + 1;
 constexpr int OFF_X = 0;
-constexpr int OFF_S = OFF_X + RMAX * XLD;
-constexpr int OFF_Y = OFF_S + KC * SLD;
+constexpr int OFF_Y = OFF_X + NST * STAGE;
 constexpr int OFF_G = OFF_Y + RMAX * YLD;
 constexpr int OFF_V = OFF_G + KMAXB * GLD;
 constexpr int OFF_R = OFF_V + 3 * KMAXB;
@@ -49,25 +49,28 @@ constexpr int SMEM_DOUBLES = OFF_R + 16 + KMAXB;
 constexpr int JLD = KMAXB + 1;    // Jacobi arrays (CTA 0 only, overlays X..V)
 constexpr int MAX_SWEEPS = 40;
 static_assert(2 * KMAXB * JLD <= OFF_R, "Jacobi overlay exceeds the shared arena");
-static_assert((RMAX / 2) * ((KMAXB + 3) / 4) * 8 <= OFF_Y, "GEMM reduction scratch exceeds X+S");
+constexpr int MAXT = (RMAX / 8) * (KMAXB / 8) / TW;   // 8 x 8 output tiles per warp
+static_assert(RMAX % 8 == 0 && KMAXB % 8 == 0 && KC % 4 == 0 && XLD % 2 == 0, "tiling");
+static_assert(TT >= 256, "the 16 x 16 thread grid of the small factorizations needs 256 threads");
 
 enum : int { ST_OK = 0, ST_BREAKDOWN = 1, ST_JACOBI = 2, ST_NOCONV = 3, ST_ZERO = 4 };
 
 }  // namespace
 
 struct TopkProb {
-  const double* M;   // m x n, column-major, ld m (read-only in the kernel)
-  const double* Mt;  // n x m, column-major, ld n (M transposed)
+  const double* M;   // m x n, column-major, ld ldm (read-only in the kernel)
+  const double* Mt;  // n x m, column-major, ld ldn (M transposed)
   int m, n, k, b, P, cta0;
-  double* Q;     // m x b
-  double* Z;     // n x b (Omega, Z iterates, Qb)
+  int ldm, ldn;      // m and n rounded up to even (16-byte aligned columns)
+  double* Q;     // m x b (ld ldm)
+  double* Z;     // n x b (ld ldn): Omega, Z iterates, Qb
+  double* Vi;    // n x k (ld ldn): right vectors
   double* Gp;    // P x KMAXB^2 Gram partials
   double* G;     // b x b
   double* Racc;  // b x b accumulated R of M^T Q (row-major)
   double* Ub;    // b x b left Ritz rotation (column-major)
   double* Jo;    // b x b right Ritz rotation (column-major)
   double* U;     // m x k out (ld m)
-  double* V;     // n x k out (ld n)
   double* s;     // b Ritz values, descending
   double* fpart; // P partial squared Frobenius norms
   double* info;  // [status, iterations, ||M||_F^2, max residual / threshold, done]
@@ -83,85 +86,112 @@ struct Ctx {
   int rn0, rn1;     // rows of n-sized iterates owned here
   double* sm;
   int* flag;
+  unsigned long long* trace;   // profile mode: [count, (phase, clock) ...], CTA 0 only
 };
+
+// phases of the profile-mode trace (interval ending at the record)
+enum : int { PH_START = 0, PH_INIT, PH_GEMM, PH_GRAM, PH_REDUCE, PH_CHOL, PH_APPLY, PH_STORE, PH_JACOBI, PH_ROTATE,
+             PH_RESID, PH_COUNT };
+constexpr int TRACE_CAP = 2048;
+
+__device__ __forceinline__ void trace_mark(const Ctx& x, int phase) {
+  if (x.trace && x.c == 0 && threadIdx.x == 0) {
+    const unsigned long long n = x.trace[0];
+    if (n < TRACE_CAP) {
+      x.trace[1 + 2 * n] = phase;
+      x.trace[2 + 2 * n] = clock64();
+      x.trace[0] = n + 1;
+    }
+  }
+}
 
 __device__ __forceinline__ void sync_group(const Ctx& x) { group_barrier(x.p->bar, (unsigned)x.p->P, x.flag); }
 
+__device__ __forceinline__ void dmma(double& d0, double& d1, double a, double b) {
+  asm volatile("mma.sync.aligned.m8n8k4.row.col.f64.f64.f64.f64 {%0,%1}, {%2}, {%3}, {%0,%1};"
+               : "+d"(d0), "+d"(d1)
+               : "d"(a), "d"(b));
+}
+
+__device__ __forceinline__ void cp_async16(double* dst, const double* src, int bytes) {
+  const unsigned d = (unsigned)__cvta_generic_to_shared(dst);
+  asm volatile("cp.async.cg.shared.global [%0], [%1], 16, %2;" ::"r"(d), "l"(src), "r"(bytes) : "memory");
+}
+__device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;" ::: "memory"); }
+template <int N>
+__device__ __forceinline__ void cp_async_wait() { asm volatile("cp.async.wait_group %0;" ::"n"(N) : "memory"); }
+
 // Ys[r][j] = sum_t X[(r0+r)*ldx + t] * S[j*lds + t]   (r < r1-r0, j < bb, t < K)
-// X is read-only for the whole launch; S is written by other CTAs (L2 loads).
-__device__ void gemm_rows(const Ctx& x, const double* __restrict__ X, int ldx, int K, const double* S, int lds,
-                          int bb, int r0, int r1) {
-  double* Xs = x.sm + OFF_X;
-  double* Ss = x.sm + OFF_S;
+// on the FP64 tensor cores: each warp owns whole 8 x 8 output tiles and runs
+// mma.m8n8k4 over the contraction.  Operands stream through NST stages of
+// shared memory by asynchronous 16-byte copies that bypass L1 (S is written by
+// other CTAs of the launch), contraction index contiguous as in global memory.
+// Requires ldx, lds even and X, S 16-byte aligned.
+__device__ __noinline__ void gemm_rows(const Ctx& x, const double* __restrict__ X, int ldx, int K, const double* S,
+                                       int lds, int bb, int r0, int r1) {
   double* Ys = x.sm + OFF_Y;
   const int R = r1 - r0;
-  const int tr = (R + 1) / 2, tj = (bb + 3) / 4, ntile = tr * tj;
-  int KG = 1;
-  while (KG < 8 && KG * 2 * ntile <= TT) KG *= 2;
-  const int TPG = TT / KG;
-  const int g = threadIdx.x / TPG, lt = threadIdx.x % TPG;
-  double acc[2][2][4];
+  const int mt = (R + 7) / 8, nt = (bb + 7) / 8, ntiles = mt * nt;
+  constexpr int HC = KC / 2;   // 16-byte copies per staged row
+  const int nX = mt * 8 * HC, nS = nt * 8 * HC;
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31, fr = lane >> 2, fc = lane & 3;
+  double acc[MAXT][2];
+  int aoff[MAXT], boff[MAXT];
 #pragma unroll
-  for (int a = 0; a < 2; ++a)
-#pragma unroll
-    for (int r = 0; r < 2; ++r)
-#pragma unroll
-      for (int q = 0; q < 4; ++q) acc[a][r][q] = 0.0;
-  int ri[2], ji[2];
-#pragma unroll
-  for (int a = 0; a < 2; ++a) {
-    const int tl = lt + a * TPG;
-    ri[a] = tl < ntile ? (tl / tj) * 2 : -1;
-    ji[a] = tl < ntile ? (tl % tj) * 4 : 0;
+  for (int q = 0; q < MAXT; ++q) {
+    acc[q][0] = acc[q][1] = 0.0;
+    const int tile = warp + q * TW;
+    aoff[q] = tile < ntiles ? ((tile / nt) * 8 + fr) * XLD + fc : -1;
+    boff[q] = tile < ntiles ? (RMAX + (tile % nt) * 8 + fr) * XLD + fc : 0;
   }
-  for (int t0 = 0; t0 < K; t0 += KC) {
-    const int kc = min(KC, K - t0);
-    __syncthreads();
-    for (int e = threadIdx.x; e < 2 * tr * KC; e += TT) {
-      const int r = e / KC, t = e - r * KC;
-      Xs[r * XLD + t] = (r < R && t < kc) ? X[(size_t)(r0 + r) * ldx + t0 + t] : 0.0;
+  auto issue = [&](int c) {
+    double* st = x.sm + OFF_X + (c % NST) * STAGE;
+    const int t0 = c * KC;
+    for (int e = threadIdx.x; e < nX; e += TT) {
+      const int r = e / HC, t = (e % HC) * 2;
+      const int bytes = (r < R) ? 8 * max(0, min(2, K - t0 - t)) : 0;
+      cp_async16(st + r * XLD + t, bytes ? X + (size_t)(r0 + r) * ldx + t0 + t : X, bytes);
     }
-    for (int e = threadIdx.x; e < 4 * tj * KC; e += TT) {
-      const int j = e / KC, t = e - j * KC;
-      Ss[t * SLD + j] = (j < bb && t < kc) ? __ldcg(&S[(size_t)j * lds + t0 + t]) : 0.0;
+    for (int e = threadIdx.x; e < nS; e += TT) {
+      const int j = e / HC, t = (e % HC) * 2;
+      const int bytes = (j < bb) ? 8 * max(0, min(2, K - t0 - t)) : 0;
+      cp_async16(st + (RMAX + j) * XLD + t, bytes ? S + (size_t)j * lds + t0 + t : S, bytes);
     }
+  };
+  const int nch = (K + KC - 1) / KC;
+  __syncthreads();   // the stages may still be read by the previous phase
+#pragma unroll
+  for (int c = 0; c < NST - 1; ++c) {
+    if (c < nch) issue(c);
+    cp_async_commit();
+  }
+  for (int c = 0; c < nch; ++c) {
+    cp_async_wait<NST - 2>();
     __syncthreads();
-    if (g < KG) {
-      for (int t = g; t < KC; t += KG) {
+    if (c + NST - 1 < nch) issue(c + NST - 1);
+    cp_async_commit();
+    const double* st = x.sm + OFF_X + (c % NST) * STAGE;
+    const int ksteps = (min(KC, K - c * KC) + 3) / 4;
+    for (int ks = 0; ks < ksteps; ++ks) {
 #pragma unroll
-        for (int a = 0; a < 2; ++a) {
-          if (ri[a] < 0) continue;
-          const double x0 = Xs[ri[a] * XLD + t], x1 = Xs[(ri[a] + 1) * XLD + t];
-          const double* sr = Ss + t * SLD + ji[a];
-#pragma unroll
-          for (int q = 0; q < 4; ++q) {
-            const double sv = sr[q];
-            acc[a][0][q] = fma(x0, sv, acc[a][0][q]);
-            acc[a][1][q] = fma(x1, sv, acc[a][1][q]);
-          }
-        }
+      for (int q = 0; q < MAXT; ++q) {
+        if (aoff[q] < 0) continue;
+        dmma(acc[q][0], acc[q][1], st[aoff[q] + 4 * ks], st[boff[q] + 4 * ks]);
       }
     }
   }
+  cp_async_wait<0>();
   __syncthreads();
-  double* part = x.sm + OFF_X;   // KG x (2 tr) x (4 tj)
-  const int pr = 2 * tr, pc = 4 * tj;
-  if (g < KG) {
+  // accumulator fragment: row fr, columns 2 fc + {0, 1} of the tile
 #pragma unroll
-    for (int a = 0; a < 2; ++a) {
-      if (ri[a] < 0) continue;
-#pragma unroll
-      for (int r = 0; r < 2; ++r)
-#pragma unroll
-        for (int q = 0; q < 4; ++q) part[(g * pr + ri[a] + r) * pc + ji[a] + q] = acc[a][r][q];
+  for (int q = 0; q < MAXT; ++q) {
+    const int tile = warp + q * TW;
+    if (tile >= ntiles) continue;
+    const int r = (tile / nt) * 8 + fr, j = (tile % nt) * 8 + 2 * fc;
+    if (r < R) {
+      if (j < bb) Ys[r * YLD + j] = acc[q][0];
+      if (j + 1 < bb) Ys[r * YLD + j + 1] = acc[q][1];
     }
-  }
-  __syncthreads();
-  for (int e = threadIdx.x; e < R * bb; e += TT) {
-    const int r = e / bb, j = e - r * bb;
-    double v = 0.0;
-    for (int q = 0; q < KG; ++q) v += part[(q * pr + r) * pc + j];
-    Ys[r * YLD + j] = v;
   }
   __syncthreads();
 }
@@ -190,7 +220,7 @@ __device__ void store_rows(const Ctx& x, double* A, int ld, int bb, int r0, int 
 // Cholesky QR pass on the distributed rows held in Ys (rows [r0, r1) of an
 // nrows x bb matrix).  racc: 0 none, 1 Racc = R, 2 Racc = R Racc (CTA 0).
 // Returns false (uniformly over the group) on breakdown.
-__device__ bool orth_pass(const Ctx& x, int bb, int r0, int r1, int nrows, bool shifted, int racc) {
+__device__ __noinline__ bool orth_pass(const Ctx& x, int bb, int r0, int r1, int nrows, bool shifted, int racc) {
   const TopkProb& p = *x.p;
   double* Ys = x.sm + OFF_Y;
   double* Gs = x.sm + OFF_G;
@@ -199,34 +229,46 @@ __device__ bool orth_pass(const Ctx& x, int bb, int r0, int r1, int nrows, bool 
   const int R = r1 - r0;
   // partial Gram of the owned rows (upper triangle)
   double* gp = p.Gp + (size_t)x.c * KMAXB * KMAXB;
-  for (int e = threadIdx.x; e < bb * bb; e += TT) {
-    const int i = e / bb, j = e - i * bb;
-    if (j < i) continue;
-    double v = 0.0;
-    for (int r = 0; r < R; ++r) v = fma(Ys[r * YLD + i], Ys[r * YLD + j], v);
-    gp[e] = v;
-  }
+  const int ty = threadIdx.x >> 4, tx = threadIdx.x & 15;   // 16 x 16 thread grid
+  for (int i = ty; i < bb; i += 16)
+    for (int j = i + tx; j < bb; j += 16) {
+      double v = 0.0;
+      for (int r = 0; r < R; ++r) v = fma(Ys[r * YLD + i], Ys[r * YLD + j], v);
+      gp[i * bb + j] = v;
+    }
   sync_group(x);
-  // reduce this CTA's slice of entries over the partials, in partial order
+  trace_mark(x, PH_GRAM);
+  // reduce this CTA's slice of entries over the partials: thread groups take
+  // interleaved partials, then the groups are summed in order (deterministic)
   {
     const int total = bb * bb;
     const int slice = (total + p.P - 1) / p.P;
-    const int e0 = x.c * slice, e1 = min(total, e0 + slice);
-    for (int e = e0 + threadIdx.x; e < e1; e += TT) {
-      const int i = e / bb, j = e - i * bb;
-      if (j < i) continue;
-      double v = 0.0;
-      for (int q = 0; q < p.P; ++q) v += __ldcg(&p.Gp[(size_t)q * KMAXB * KMAXB + e]);
-      p.G[e] = v;
+    const int e0 = min(total, x.c * slice), e1 = min(total, e0 + slice);
+    double* red2 = x.sm + OFF_X;   // TT doubles (the GEMM staging area is free here)
+    for (int base = e0; base < e1; base += TT) {
+      const int ns = min(TT, e1 - base), ng = TT / ns;
+      const int el = threadIdx.x % ns, q0 = threadIdx.x / ns;
+      if (q0 < ng) {
+        double v = 0.0;
+        for (int q = q0; q < p.P; q += ng) v += __ldcg(&p.Gp[(size_t)q * KMAXB * KMAXB + base + el]);
+        red2[q0 * ns + el] = v;
+      }
+      __syncthreads();
+      if (threadIdx.x < ns) {
+        double v = 0.0;
+        for (int q = 0; q < ng; ++q) v += red2[q * ns + threadIdx.x];
+        const int e = base + threadIdx.x, i = e / bb, j = e - i * bb;
+        if (j >= i) p.G[e] = v;
+      }
+      __syncthreads();
     }
   }
   sync_group(x);
+  trace_mark(x, PH_REDUCE);
   // factor G (+ shift) redundantly: G = U^T D U with U unit upper, kept as the
   // unscaled upper rows D U in Gs
-  for (int e = threadIdx.x; e < bb * bb; e += TT) {
-    const int i = e / bb, j = e - i * bb;
-    if (j >= i) Gs[i * GLD + j] = __ldcg(&p.G[e]);
-  }
+  for (int i = ty; i < bb; i += 16)
+    for (int j = i + tx; j < bb; j += 16) Gs[i * GLD + j] = __ldcg(&p.G[i * bb + j]);
   __syncthreads();
   if (shifted) {
     if (threadIdx.x == 0) {
@@ -244,10 +286,10 @@ __device__ bool orth_pass(const Ctx& x, int bb, int r0, int r1, int nrows, bool 
       return false;
     }
     const double inv = 1.0 / d;
-    const int nt = bb - 1 - j;
-    for (int e = threadIdx.x; e < nt * nt; e += TT) {
-      const int i = j + 1 + e / nt, l = j + 1 + e % nt;
-      if (l >= i) Gs[i * GLD + l] -= Gs[j * GLD + i] * Gs[j * GLD + l] * inv;
+    const double* gj = Gs + j * GLD;
+    for (int i = j + 1 + ty; i < bb; i += 16) {
+      const double gji = gj[i] * inv;
+      for (int l = i + tx; l < bb; l += 16) Gs[i * GLD + l] -= gji * gj[l];
     }
   }
   __syncthreads();
@@ -257,10 +299,8 @@ __device__ bool orth_pass(const Ctx& x, int bb, int r0, int r1, int nrows, bool 
   }
   __syncthreads();
   // unit upper U in place (diagonal kept as the pivot)
-  for (int e = threadIdx.x; e < bb * bb; e += TT) {
-    const int i = e / bb, j = e - i * bb;
-    if (j > i) Gs[i * GLD + j] *= invd[i];
-  }
+  for (int i = ty; i < bb; i += 16)
+    for (int j = i + 1 + tx; j < bb; j += 16) Gs[i * GLD + j] *= invd[i];
   __syncthreads();
   if (racc && x.c == 0) {
     // R = diag(sq) U;  Racc <- R (racc 1) or R Racc (racc 2), via CTA 0's partial slot
@@ -283,27 +323,26 @@ __device__ bool orth_pass(const Ctx& x, int bb, int r0, int r1, int nrows, bool 
     __syncthreads();
     for (int e = threadIdx.x; e < bb * bb; e += TT) p.Racc[e] = tmp[e];
   }
+  trace_mark(x, PH_CHOL);
   // rows: y <- y R^{-1}, R = diag(sq) U: forward substitution on the unit
   // upper factor, one column per step, then the diagonal scaling
   for (int j = 0; j < bb - 1; ++j) {
-    const int nt = bb - 1 - j;
-    for (int e = threadIdx.x; e < R * nt; e += TT) {
-      const int r = e / nt, l = j + 1 + e % nt;
-      Ys[r * YLD + l] -= Ys[r * YLD + j] * Gs[j * GLD + l];
+    for (int r = ty; r < R; r += 16) {
+      const double yj = Ys[r * YLD + j];
+      for (int l = j + 1 + tx; l < bb; l += 16) Ys[r * YLD + l] -= yj * Gs[j * GLD + l];
     }
     __syncthreads();
   }
-  for (int e = threadIdx.x; e < R * bb; e += TT) {
-    const int r = e / bb, j = e - r * bb;
-    Ys[r * YLD + j] /= sq[j];
-  }
+  for (int r = ty; r < R; r += 16)
+    for (int j = tx; j < bb; j += 16) Ys[r * YLD + j] /= sq[j];
   __syncthreads();
+  trace_mark(x, PH_APPLY);
   return true;
 }
 
 // One-sided Jacobi SVD of A = Racc^T (bb x bb) in CTA 0; sorted outputs to
 // p.s, p.Ub (left vectors), p.Jo (right vectors).
-__device__ void ritz_small(const Ctx& x, int bb) {
+__device__ __noinline__ void ritz_small(const Ctx& x, int bb) {
   const TopkProb& p = *x.p;
   double* A = x.sm;                 // column-major, JLD
   double* J = x.sm + KMAXB * JLD;   // column-major, JLD
@@ -316,14 +355,21 @@ __device__ void ritz_small(const Ctx& x, int bb) {
     J[col * JLD + row] = (row == col) ? 1.0 : 0.0;
   }
   __syncthreads();
+  const double tol_rot = DBL_EPSILON * bb;   // stop rotating pairs orthogonal to rounding level
   int sweep = 0;
   for (; sweep < MAX_SWEEPS; ++sweep) {
     if (threadIdx.x == 0) *cnt = 0;
     for (int round = 0; round < bb - 1; ++round) {
       __syncthreads();
-      for (int pi = warp; pi < bb / 2; pi += TW) {
-        int pp, qq;
-        if (pi == 0) {
+      // 8 threads per column pair: 32 pairs at a time
+      const int grp = threadIdx.x >> 3, sub = threadIdx.x & 7;
+      // every lane runs the same number of passes so that the shuffles are convergent
+      for (int base = 0; base < bb / 2; base += TT / 8) {
+        const int pi = base + grp;
+        const bool active = pi < bb / 2;
+        int pp = 0, qq = 1;
+        if (!active) {
+        } else if (pi == 0) {
           pp = round;
           qq = bb - 1;
         } else {
@@ -333,22 +379,25 @@ __device__ void ritz_small(const Ctx& x, int bb) {
         double* ap = A + pp * JLD;
         double* aq = A + qq * JLD;
         double al = 0.0, be = 0.0, ga = 0.0;
-        for (int r = lane; r < bb; r += 32) {
+        for (int r = sub; active && r < bb; r += 8) {
           const double u = ap[r], v = aq[r];
           al = fma(u, u, al);
           be = fma(v, v, be);
           ga = fma(u, v, ga);
         }
-        al = wsum(al);
-        be = wsum(be);
-        ga = wsum(ga);
-        if (ga != 0.0 && fabs(ga) > DBL_EPSILON * sqrt(al) * sqrt(be)) {
+#pragma unroll
+        for (int o = 4; o > 0; o >>= 1) {
+          al += __shfl_xor_sync(0xffffffffu, al, o);
+          be += __shfl_xor_sync(0xffffffffu, be, o);
+          ga += __shfl_xor_sync(0xffffffffu, ga, o);
+        }
+        if (active && ga != 0.0 && fabs(ga) > tol_rot * sqrt(al) * sqrt(be)) {
           const double zeta = (be - al) / (2.0 * ga);
           const double t = copysign(1.0, zeta) / (fabs(zeta) + sqrt(1.0 + zeta * zeta));
           const double cs = 1.0 / sqrt(1.0 + t * t), sn = cs * t;
           double* jp = J + pp * JLD;
           double* jq = J + qq * JLD;
-          for (int r = lane; r < bb; r += 32) {
+          for (int r = sub; r < bb; r += 8) {
             const double u = ap[r], v = aq[r];
             ap[r] = cs * u - sn * v;
             aq[r] = sn * u + cs * v;
@@ -356,7 +405,7 @@ __device__ void ritz_small(const Ctx& x, int bb) {
             jp[r] = cs * ju - sn * jv;
             jq[r] = sn * ju + cs * jv;
           }
-          if (lane == 0) atomicAdd(cnt, 1);
+          if (sub == 0) atomicAdd(cnt, 1);
         }
       }
     }
@@ -416,8 +465,8 @@ __device__ __forceinline__ double omega(unsigned long long i) {
 
 }  // namespace
 
-__global__ void __launch_bounds__(TT) topk_kernel(const TopkProb* __restrict__ probs, int nprob, int q0, int qstep,
-                                                  int qmax, double tol, int* flag) {
+__global__ void __launch_bounds__(TT, 1) topk_kernel(const TopkProb* __restrict__ probs, int nprob, int q0, int qstep,
+                                                  int qmax, double tol, int* flag, unsigned long long* trace) {
   extern __shared__ double sm[];
   int pi = -1;
   for (int q = 0; q < nprob; ++q)
@@ -429,6 +478,8 @@ __global__ void __launch_bounds__(TT) topk_kernel(const TopkProb* __restrict__ p
   x.c = blockIdx.x - p.cta0;
   x.sm = sm;
   x.flag = flag;
+  x.trace = (pi == 0) ? trace : nullptr;
+  trace_mark(x, PH_START);
   const int Rm = (p.m + p.P - 1) / p.P, Rn = (p.n + p.P - 1) / p.P;
   x.rm0 = min(p.m, x.c * Rm);
   x.rm1 = min(p.m, x.rm0 + Rm);
@@ -442,11 +493,11 @@ __global__ void __launch_bounds__(TT) topk_kernel(const TopkProb* __restrict__ p
     double f = 0.0;
     for (int e = threadIdx.x; e < (x.rn1 - x.rn0) * b; e += TT) {
       const int j = e / (x.rn1 - x.rn0), r = e - j * (x.rn1 - x.rn0);
-      p.Z[(size_t)j * p.n + x.rn0 + r] = omega((unsigned long long)j * p.n + x.rn0 + r);
+      p.Z[(size_t)j * p.ldn + x.rn0 + r] = omega((unsigned long long)j * p.n + x.rn0 + r);
     }
     for (int col = x.rn0; col < x.rn1; ++col)
       for (int r = threadIdx.x; r < p.m; r += TT) {
-        const double v = p.M[(size_t)col * p.m + r];
+        const double v = p.M[(size_t)col * p.ldm + r];
         f = fma(v, v, f);
       }
     f = wsum(f);
@@ -460,47 +511,60 @@ __global__ void __launch_bounds__(TT) topk_kernel(const TopkProb* __restrict__ p
     }
   }
   sync_group(x);
+  trace_mark(x, PH_INIT);
   if (x.c == 0 && threadIdx.x == 0) {
     double s = 0.0;
     for (int q = 0; q < p.P; ++q) s += __ldcg(&p.fpart[q]);
     p.info[2] = s;
   }
-  gemm_rows(x, p.Mt, p.n, p.n, p.Z, p.n, b, x.rm0, x.rm1);
+  gemm_rows(x, p.Mt, p.ldn, p.n, p.Z, p.ldn, b, x.rm0, x.rm1);
+  trace_mark(x, PH_GEMM);
   if (!orth_pass(x, b, x.rm0, x.rm1, p.m, true, 0)) return;
-  store_rows(x, p.Q, p.m, b, x.rm0, x.rm1);
+  store_rows(x, p.Q, p.ldm, b, x.rm0, x.rm1);
   sync_group(x);
+  trace_mark(x, PH_STORE);
 
   int it = 0, target = q0;
   for (;;) {
     for (; it < target; ++it) {
-      gemm_rows(x, p.M, p.m, p.m, p.Q, p.m, b, x.rn0, x.rn1);
+      gemm_rows(x, p.M, p.ldm, p.m, p.Q, p.ldm, b, x.rn0, x.rn1);
+      trace_mark(x, PH_GEMM);
       if (!orth_pass(x, b, x.rn0, x.rn1, p.n, true, 0)) return;
-      store_rows(x, p.Z, p.n, b, x.rn0, x.rn1);
+      store_rows(x, p.Z, p.ldn, b, x.rn0, x.rn1);
       sync_group(x);
-      gemm_rows(x, p.Mt, p.n, p.n, p.Z, p.n, b, x.rm0, x.rm1);
+      trace_mark(x, PH_STORE);
+      gemm_rows(x, p.Mt, p.ldn, p.n, p.Z, p.ldn, b, x.rm0, x.rm1);
+      trace_mark(x, PH_GEMM);
       if (!orth_pass(x, b, x.rm0, x.rm1, p.m, true, 0)) return;
-      store_rows(x, p.Q, p.m, b, x.rm0, x.rm1);
+      store_rows(x, p.Q, p.ldm, b, x.rm0, x.rm1);
       sync_group(x);
+      trace_mark(x, PH_STORE);
     }
     // Rayleigh-Ritz: Q <- orth(Q); M^T Q = Qb Rb; Rb^T = Ub S J^T
-    load_rows(x, p.Q, p.m, b, x.rm0, x.rm1);
+    load_rows(x, p.Q, p.ldm, b, x.rm0, x.rm1);
     if (!orth_pass(x, b, x.rm0, x.rm1, p.m, false, 0)) return;
-    store_rows(x, p.Q, p.m, b, x.rm0, x.rm1);
+    store_rows(x, p.Q, p.ldm, b, x.rm0, x.rm1);
     sync_group(x);
-    gemm_rows(x, p.M, p.m, p.m, p.Q, p.m, b, x.rn0, x.rn1);
+    trace_mark(x, PH_STORE);
+    gemm_rows(x, p.M, p.ldm, p.m, p.Q, p.ldm, b, x.rn0, x.rn1);
+    trace_mark(x, PH_GEMM);
     if (!orth_pass(x, b, x.rn0, x.rn1, p.n, true, 1)) return;
     if (!orth_pass(x, b, x.rn0, x.rn1, p.n, false, 2)) return;
     if (!orth_pass(x, b, x.rn0, x.rn1, p.n, false, 2)) return;
-    store_rows(x, p.Z, p.n, b, x.rn0, x.rn1);
+    store_rows(x, p.Z, p.ldn, b, x.rn0, x.rn1);
     sync_group(x);
+    trace_mark(x, PH_STORE);
     if (x.c == 0) ritz_small(x, b);
     sync_group(x);
+    trace_mark(x, PH_JACOBI);
     if (__ldcg(&p.info[0]) != ST_OK) return;
-    rotate_rows(x, p.Q, p.m, p.Ub, b, k, p.U, p.m, x.rm0, x.rm1);
-    rotate_rows(x, p.Z, p.n, p.Jo, b, k, p.V, p.n, x.rn0, x.rn1);
+    rotate_rows(x, p.Q, p.ldm, p.Ub, b, k, p.U, p.m, x.rm0, x.rm1);
+    rotate_rows(x, p.Z, p.ldn, p.Jo, b, k, p.Vi, p.ldn, x.rn0, x.rn1);
     sync_group(x);
+    trace_mark(x, PH_ROTATE);
     // residuals ||M v_i - s_i u_i||^2, partial over the owned m-rows
-    gemm_rows(x, p.Mt, p.n, p.n, p.V, p.n, k, x.rm0, x.rm1);
+    gemm_rows(x, p.Mt, p.ldn, p.n, p.Vi, p.ldn, k, x.rm0, x.rm1);
+    trace_mark(x, PH_GEMM);
     {
       const double* Ys = sm + OFF_Y;
       double* gp = p.Gp + (size_t)x.c * KMAXB * KMAXB;
@@ -543,6 +607,7 @@ __global__ void __launch_bounds__(TT) topk_kernel(const TopkProb* __restrict__ p
       p.info[4] = done;
     }
     sync_group(x);
+    trace_mark(x, PH_RESID);
     if (__ldcg(&p.info[4]) != 0.0) return;
     target = it + qstep;
   }
@@ -593,27 +658,42 @@ void svd_topk(Engine& E, std::vector<TopkDesc>& ds, double tol) {
     P = std::min(P, capacity / nprob);
     if ((mx + P - 1) / P > RMAX) throw Error(SPS_ERR_ARGUMENT, "svd_topk: block too large for the grid");
     const int b = d.b;
-    const size_t nd = (size_t)n * m + (size_t)m * b + (size_t)n * b + (size_t)P * KMAXB * KMAXB + 4 * (size_t)b * b +
-                      b + P + 8;
+    const int ldm = m + (m & 1), ldn = n + (n & 1);
+    // every buffer read by the asynchronous copies has an even length, so all
+    // of them start 16-byte aligned
+    const size_t nd = (size_t)ldn * m + (size_t)ldm * b + (size_t)ldn * b + (size_t)ldn * d.k +
+                      ((m & 1) ? (size_t)ldm * n : 0) + (size_t)P * KMAXB * KMAXB + 4 * (size_t)b * b + b + P + 8;
     Buf w = E.alloc(sizeof(double) * nd + 64);
     keep.push_back(w);
     double* base = (double*)w->ptr;
     TopkProb& p = hp[i];
-    p.M = d.M;
     double* mt = base;
     p.Mt = mt;
-    base += (size_t)n * m;
+    base += (size_t)ldn * m;
     p.m = m;
     p.n = n;
+    p.ldm = ldm;
+    p.ldn = ldn;
     p.k = d.k;
     p.b = b;
     p.P = P;
     p.cta0 = cta;
     cta += P;
     p.Q = base;
-    base += (size_t)m * b;
+    base += (size_t)ldm * b;
     p.Z = base;
-    base += (size_t)n * b;
+    base += (size_t)ldn * b;
+    p.Vi = base;
+    base += (size_t)ldn * d.k;
+    if (m & 1) {   // odd leading dimension: an even-ld copy of M
+      SPS_CUDA(cudaMemcpy2DAsync(base, sizeof(double) * ldm, d.M, sizeof(double) * m, sizeof(double) * m, n,
+                                 cudaMemcpyDeviceToDevice, E.stream));
+      p.M = base;
+      base += (size_t)ldm * n;
+    } else {
+      if (reinterpret_cast<uintptr_t>(d.M) % 16) throw Error(SPS_ERR_ARGUMENT, "svd_topk: matrix not 16-byte aligned");
+      p.M = d.M;
+    }
     p.Gp = base;
     base += (size_t)P * KMAXB * KMAXB;
     p.G = base;
@@ -632,9 +712,8 @@ void svd_topk(Engine& E, std::vector<TopkDesc>& ds, double tol) {
     base += 6;
     p.bar = (unsigned*)(base);
     p.U = d.U;
-    p.V = d.V;
     SPS_CUDA(cudaMemsetAsync(p.info, 0, sizeof(double) * 6 + 8, E.stream));
-    transpose_cm(E, d.M, m, n, m, mt, n);
+    transpose_cm(E, d.M, m, n, m, mt, ldn);
   }
   Buf pb = E.alloc(sizeof(TopkProb) * nprob);
   keep.push_back(pb);
@@ -642,11 +721,23 @@ void svd_topk(Engine& E, std::vector<TopkDesc>& ds, double tol) {
   const TopkProb* dp = (const TopkProb*)pb->ptr;
   int q0 = std::max(2, E.topk_hint), qstep = 2, qmax = 48;
   int* flag = E.dflag;
-  void* args[] = {(void*)&dp, (void*)&nprob, (void*)&q0, (void*)&qstep, (void*)&qmax, (void*)&tol, (void*)&flag};
+  // profile mode: phase trace of the first problem's CTA 0
+  Buf tb;
+  unsigned long long* trace = nullptr;
+  if (E.profile) {
+    tb = E.alloc(sizeof(unsigned long long) * (1 + 2 * TRACE_CAP));
+    trace = (unsigned long long*)tb->ptr;
+    SPS_CUDA(cudaMemsetAsync(trace, 0, sizeof(unsigned long long), E.stream));
+  }
+  void* args[] = {(void*)&dp,   (void*)&nprob, (void*)&q0,   (void*)&qstep,
+                  (void*)&qmax, (void*)&tol,   (void*)&flag, (void*)&trace};
   const int tid = E.tic("svd_topk");
   SPS_CUDA(cudaLaunchCooperativeKernel((const void*)topk_kernel, dim3(cta), dim3(TT), args, smem, E.stream));
   E.launches++;
-  // info and Ritz values to the host
+  // right vectors into the caller's layout, info and Ritz values to the host
+  for (int i = 0; i < nprob; ++i)
+    SPS_CUDA(cudaMemcpy2DAsync(ds[i].V, sizeof(double) * hp[i].n, hp[i].Vi, sizeof(double) * hp[i].ldn,
+                               sizeof(double) * hp[i].n, hp[i].k, cudaMemcpyDeviceToDevice, E.stream));
   int off = 0;
   for (int i = 0; i < nprob; ++i) {
     SPS_CUDA(cudaMemcpyAsync(E.hscal + off, hp[i].info, sizeof(double) * 6, cudaMemcpyDeviceToHost, E.stream));
@@ -668,6 +759,20 @@ void svd_topk(Engine& E, std::vector<TopkDesc>& ds, double tol) {
     d.s.assign(E.hscal + off + 6, E.hscal + off + 6 + d.b);
     qused = std::max(qused, d.iterations);
     off += 6 + d.b;
+  }
+  if (trace) {
+    std::vector<unsigned long long> h(1 + 2 * TRACE_CAP);
+    SPS_CUDA(cudaMemcpy(h.data(), trace, sizeof(unsigned long long) * h.size(), cudaMemcpyDeviceToHost));
+    int khz = 0;
+    SPS_CUDA(cudaDeviceGetAttribute(&khz, cudaDevAttrClockRate, E.device));
+    static const char* names[PH_COUNT] = {"start", "init", "gemm", "gram", "reduce", "cholesky",
+                                          "apply", "store", "jacobi", "rotate", "residual"};
+    const unsigned long long n = std::min<unsigned long long>(h[0], TRACE_CAP);
+    for (unsigned long long i = 1; i < n; ++i) {
+      const int ph = (int)h[1 + 2 * i];
+      const double cyc = (double)(h[2 + 2 * i] - h[2 + 2 * (i - 1)]);
+      if (ph > 0 && ph < PH_COUNT && khz > 0) E.add_stat(std::string("svd_topk.") + names[ph], cyc / khz);
+    }
   }
   // work of the launch: 2 m n b flops per half-iteration, plus the extraction
   double fl = 0;

@@ -42,9 +42,12 @@ def main(which):
     elif which == "topk":
         e = sps.Engine(2, 2)
         a = graded(648, 648, 0.1, 5)
-        for _ in range(2):
-            u, s, v, iters, ms = e.la_svd_topk(a, 18)
+        u, s, v, iters, ms = e.la_svd_topk(a, 18)
+        e.set_profile(True)
+        u, s, v, iters, ms = e.la_svd_topk(a, 18)
         print(f"topk 648x648 k=18: {ms:.3f} ms, {iters} iterations")
+        for name, st in sorted(e.kernel_stats().items()):
+            print(f"  {name:24s} {st['ms']:9.3f} ms  x{st['count']}")
     elif which == "gemm":
         e = sps.Engine(2, 2)
         rng = np.random.default_rng(1)
