@@ -2,11 +2,13 @@
 """Born samples/s on the 8x8 open TFIM (J=1, h=3.0), D=6 (3+3), chi=36 (18+18).
 
 One step = one perfect Born draw (``sample_configuration``, src/sampling/born.jl:86-163):
-eight row absorptions with the reference's exact LQ + truncated-SVD boundary
-compression and 64 conditionals, from a device-resident SamplingCache of a
-seeded synthetic beta0 PEPO with the workload's shapes.  The plain FP64 path
-is the one timed.  Every rank draws its own samples (weak scaling: samples
-shard with no data-path collective); rank 0 prints one JSON line.
+eight row absorptions and 64 conditionals from a device-resident SamplingCache
+of a seeded synthetic beta0 PEPO with the workload's shapes.  The headline
+`value` is the zip-up absorption path (FP64); the plain FP64 path with the
+reference's exact LQ + truncated-SVD compression is timed beside it on the same
+draw indices (`plain_fp64`, `agreement_vs_plain`).  Every rank draws its own
+samples (weak scaling: samples shard with no data-path collective); rank 0
+prints one JSON line.
 
   python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
 """
@@ -198,18 +200,10 @@ def ours_arm(args, rank, world, local_rank):
     sites, dims = sps.synthetic.synthetic_pepo(LX, LY, D, PEPO_EPS, 7)
     st = e.upload_state(sites, dims, True, beta=0.4)
     sps.normalize_state(st)
-    method = sps.BoundaryMPS(CHI, sps.Z2Space(CHI // 2, CHI // 2))
-    cache = sps.SamplingCache(st, method)
+    space = sps.Z2Space(CHI // 2, CHI // 2)
 
     def index(step):
         return 1 + rank + world * step
-
-    def draw(i):
-        u = sps.sample_uniforms(SEED, i, LX * LY)
-        return sps.sample_configuration(cache, uniforms=u)
-
-    for s in range(args.warmup):
-        draw(index(s))
 
     def barrier():
         torch.cuda.synchronize()
@@ -217,38 +211,64 @@ def ours_arm(args, rank, world, local_rank):
             dist.barrier()
         torch.cuda.synchronize()
 
-    # device-timed region (events on the engine's stream)
-    barrier()
-    n0, _ = e.counters()
-    with Clocks(local_rank) as clk:
-        e.timer_start()
-        for s in range(args.steps):
-            draw(index(args.warmup + s))
-        ms = e.timer_stop()
-    n1, _ = e.counters()
-    barrier()
-    # end-to-end through the public API, host wall clock, fresh host uniforms in / configuration out
-    t0 = time.perf_counter()
-    for s in range(args.steps):
-        d = draw(index(args.warmup + args.steps + s))
-    barrier()
-    wall = time.perf_counter() - t0
-    t = torch.tensor([ms, wall], dtype=torch.float64, device=f"cuda:{local_rank}")
-    if dist is not None:
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-    ms_max, wall_max = float(t[0]), float(t[1])
-    value = world * args.steps / (ms_max * 1e-3)
-    e2e = world * args.steps / wall_max
-    # per-kernel profile of one draw (separate pass; not part of the timed number)
-    e.set_profile(True)
-    draw(index(2 * args.steps + args.warmup))
-    stats = e.kernel_stats()
-    e.set_profile(False)
+    def measure(method, steps, warmup, profile):
+        """Device-timed and end-to-end Born draws from a cache built with `method`."""
+        cache = sps.SamplingCache(st, method)
+
+        def draw(i):
+            u = sps.sample_uniforms(SEED, i, LX * LY)
+            return sps.sample_configuration(cache, uniforms=u)
+
+        for s in range(warmup):
+            draw(index(s))
+        barrier()
+        n0, _ = e.counters()
+        draws = []
+        with Clocks(local_rank) as clk:
+            e.timer_start()
+            for s in range(steps):
+                draws.append(draw(index(warmup + s)))
+            ms = e.timer_stop()
+        n1, _ = e.counters()
+        barrier()
+        # end to end through the public API: host uniforms in, configuration out, wall clock
+        t0 = time.perf_counter()
+        for s in range(steps):
+            draw(index(warmup + steps + s))
+        barrier()
+        wall = time.perf_counter() - t0
+        t = torch.tensor([ms, wall], dtype=torch.float64, device=f"cuda:{local_rank}")
+        if dist is not None:
+            dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        stats = None
+        if profile:   # per-kernel profile of one draw (separate pass; not part of the timed number)
+            e.set_profile(True)
+            draw(index(2 * steps + warmup))
+            stats = e.kernel_stats()
+            e.set_profile(False)
+        del cache
+        return {"ms": float(t[0]), "wall": float(t[1]), "launches": int(n1 - n0), "clocks": clk.summary(),
+                "draws": draws, "stats": stats}
+
+    zip_run = measure(sps.BoundaryMPSZipUp(CHI, space), args.steps, args.warmup, True)
+    plain_steps = max(1, min(args.steps, 2))
+    plain_run = measure(sps.BoundaryMPS(CHI, space), plain_steps, min(args.warmup, 3), False)
+    value = world * args.steps / (zip_run["ms"] * 1e-3)
+    e2e = world * args.steps / zip_run["wall"]
+    plain_value = world * plain_steps / (plain_run["ms"] * 1e-3)
+    plain_e2e = world * plain_steps / plain_run["wall"]
+    # the two paths on the same draw indices
+    import numpy as np
+    same, dlp = 0, 0.0
+    for dz, dp in zip(zip_run["draws"], plain_run["draws"]):
+        same += int(np.array_equal(dz["configuration"], dp["configuration"]))
+        dlp = max(dlp, abs(dz["log_probability"] - dp["log_probability"]))
     result = None
     if rank == 0:
+        stats = zip_run["stats"]
         peak = measure_fp64_peak(torch, f"cuda:{local_rank}")
-        tot = sum(v["ms"] for v in stats.values())
-        dom = max(((k, v) for k, v in stats.items() if v["flops"] > 0), key=lambda kv: kv[1]["ms"])
+        tot = sum(v["ms"] for k, v in stats.items() if "." not in k)
+        dom = max(((k, v) for k, v in stats.items() if v["flops"] > 0 and "." not in k), key=lambda kv: kv[1]["ms"])
         name, v = dom
         per_launch_flops = v["flops"] / v["count"]
         avg_ms = v["ms"] / v["count"]
@@ -259,26 +279,34 @@ def ours_arm(args, rank, world, local_rank):
                                    "MEASURED_PEAKS.json); tensor-core FP64 and DFMA share the FP64 rate on B200",
                     "share_of_profiled_time": v["ms"] / tot if tot else None,
                     "kernels": {k: {"ms": round(s["ms"], 3), "count": s["count"],
-                                    "share": round(s["ms"] / tot, 4) if tot else None}
+                                    "share": round(s["ms"] / tot, 4) if tot and "." not in k else None}
                                 for k, s in sorted(stats.items(), key=lambda kv: -kv[1]["ms"])}}
         cpu = None
         if world == 1:
             per_draw, measured = cpu_row_sample()
             cpu = {"value": 1.0 / per_draw, "unit": "samples/s", "cores": os.cpu_count(), "kind": "port",
                    "sample": f"one interior row of a draw (absorption + {LX} conditionals) timed "
-                             f"({measured:.1f} s) and scaled x{LY}; CPU oracle (NumPy/OpenBLAS FP64)"}
+                             f"({measured:.1f} s) and scaled x{LY}; CPU oracle (NumPy/OpenBLAS FP64), "
+                             "reference algorithm"}
         L = LX * LY
         result = {"metric": METRIC, "value": value, "unit": "samples/s", "n_gpus": world, "steps": args.steps,
-                  "warmup": args.warmup, "ms_per_step": ms_max / args.steps, "higher_is_better": True,
+                  "warmup": args.warmup, "ms_per_step": zip_run["ms"] / args.steps, "higher_is_better": True,
                   "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
                   "config": workload_config({"parallelism": f"samples sharded over {world} GPU(s)",
-                                             "path": "plain FP64 (reference algorithm)"}),
+                                             "path": "zip-up boundary absorption, FP64, one sample per launch"}),
                   "e2e": {"value": e2e, "unit": "samples/s", "h2d_bytes_per_step": 8 * L,
                           "d2h_bytes_per_step": 4 * L + 8 + 8},
-                  "gpu_launches": int(n1 - n0), "clocks": clk.summary(), "roofline": roofline,
-                  "cpu_baseline": cpu}
+                  "gpu_launches": zip_run["launches"], "clocks": zip_run["clocks"], "roofline": roofline,
+                  "cpu_baseline": cpu,
+                  "plain_fp64": {"value": plain_value, "e2e": plain_e2e, "unit": "samples/s",
+                                 "steps": plain_steps, "ms_per_step": plain_run["ms"] / plain_steps,
+                                 "gpu_launches": plain_run["launches"], "clocks": plain_run["clocks"],
+                                 "path": "reference algorithm: exact LQ sweep + truncated SVD sweep, FP64"},
+                  "speedup_vs_plain_fp64": value / plain_value,
+                  "agreement_vs_plain": {"draws": min(len(zip_run["draws"]), len(plain_run["draws"])),
+                                         "identical_configurations": same, "max_abs_dlogp": dlp}}
         print(json.dumps(result), flush=True)
-    del cache, st
+    del st
     e.close()
     if dist is not None:
         dist.barrier()

@@ -53,10 +53,15 @@ typedef struct sps_config {
 } sps_config;
 
 /* BoundaryMPS(chi, sector_space) (src/contraction/boundary_mps.jl:11-18);
- * space0/space1 < 0 means sector_space = nothing. */
+ * space0/space1 < 0 means sector_space = nothing.  absorption 0 is the
+ * reference's row absorption (exact LQ sweep + truncated SVD sweep,
+ * compress_boundary!, boundary_mps.jl:94-134); 1 is this library's zip-up
+ * absorption (one sweep of truncated SVDs without a canonical form), which
+ * has no counterpart in the reference. */
 typedef struct sps_boundary {
   int32_t chi;
   int32_t space0, space1;
+  int32_t absorption;
 } sps_boundary;
 
 /* Report of evolution_step! (src/evolution/full_update.jl:580-596). */

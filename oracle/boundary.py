@@ -19,9 +19,15 @@ from .z2 import T, einsum, fuse, norm, unit
 
 @dataclass
 class BoundaryMPS:
-    """``BoundaryMPS(chi, sector_space)`` (``boundary_mps.jl:11-18``)."""
+    """``BoundaryMPS(chi, sector_space)`` (``boundary_mps.jl:11-18``).
+
+    ``zipup`` selects the zip-up row absorption of ``absorb_zipup`` (the
+    GPU engine's batched variant, which has no counterpart in the reference)
+    in place of the reference's exact-LQ-plus-SVD compression.
+    """
     chi: int
     space: tuple | None = None
+    zipup: bool = False
 
 
 @dataclass
@@ -137,8 +143,75 @@ def compress_boundary(B, chi, reverse=False, space=None, observer=None):
     return max_error, (-math.inf if scale == 0.0 else math.log(scale))
 
 
+def absorb_zipup(env: Env, row, method: BoundaryMPS, side="north") -> Env:
+    """Zip-up row absorption, the GPU engine's variant (no counterpart in the reference).
+
+    The boundary is first brought into the canonical form opposite to the
+    sweep (an LQ sweep north, a QR sweep south, on the small chi-bond tensors).
+    Then one sweep over the row: the carried factor times the boundary tensor times
+    the row tensor is split by a truncated SVD (``truncrank(chi) &
+    truncspace(space)``, as in ``_boundary_svd``, ``boundary_mps.jl:33-42``);
+    the isometry becomes the new boundary tensor and the rest (S V^T north,
+    U S south) is carried to the next site.  No canonical form is built, so
+    each truncation is local; the centre (last site north, first site south)
+    is normalised as in ``compress_boundary!`` (``boundary_mps.jl:129-133``).
+    """
+    N = len(row)
+    maxe = 0.0
+    out = [None] * N
+    E = list(env.tensors)
+    if side == "north":
+        # right-canonical boundary (LQ sweep), so that everything right of the
+        # zip front except the row is an isometry
+        for x in range(N - 1, 0, -1):
+            L, Q = z2.lq(E[x], [0], [1, 2])
+            E[x] = Q
+            E[x - 1] = einsum("lnk,kr->lnr", E[x - 1], L)
+        C = unit([z2.leg(1, 0), E[0].p[0], row[0].p[0]])      # (a, l, w)
+        for x in range(N):
+            T1 = einsum("alw,lnr->awnr", C, E[x])
+            Tt = einsum("awnr,wnes->asre", T1, row[x])
+            if x == N - 1:
+                out[x] = fuse(Tt, 2, 2)
+                continue
+            nM = norm(Tt)
+            U, S, V, err, _ = z2.svd_trunc(Tt, [0, 1], [2, 3], chi=method.chi, space=method.space)
+            maxe = max(maxe, 0.0 if nM == 0 else (err / nM) ** 2)
+            out[x] = U
+            C = einsum("k,kre->kre", T(np.concatenate(S), [V.p[0]]), V)
+        center = N - 1
+    else:
+        # left-canonical boundary (QR sweep)
+        for x in range(N - 1):
+            Q, R = z2.qr(E[x], [0, 1], [2])
+            E[x] = Q
+            E[x + 1] = einsum("lk,knr->lnr", R, E[x + 1])
+        C = unit([E[N - 1].p[2], row[N - 1].p[2], z2.leg(1, 0)])   # (r, e, a)
+        for x in range(N - 1, -1, -1):
+            T1 = einsum("lsr,rea->lsea", E[x], C)
+            Tt = einsum("lsea,wnes->lwna", T1, row[x])
+            if x == 0:
+                out[x] = fuse(Tt, 0, 2)
+                continue
+            nM = norm(Tt)
+            U, S, V, err, _ = z2.svd_trunc(Tt, [0, 1], [2, 3], chi=method.chi, space=method.space)
+            maxe = max(maxe, 0.0 if nM == 0 else (err / nM) ** 2)
+            out[x] = V
+            C = einsum("lwk,k->lwk", U, T(np.concatenate(S), [U.p[2]]))
+        center = 0
+    scale = norm(out[center])
+    if not math.isfinite(scale):
+        raise RuntimeError("nonfinite boundary norm")
+    if scale != 0.0:
+        out[center] = out[center] / scale
+    ls = -math.inf if scale == 0.0 else math.log(scale)
+    return Env(out, env.log_scale + ls, max(env.max_truncation, maxe))
+
+
 def absorb(env: Env, row, method: BoundaryMPS, side="north", entropy=None, row_cut=0) -> Env:
     """``_absorb`` for the row method (``boundary_mps.jl:136-151``)."""
+    if method.zipup:
+        return absorb_zipup(env, row, method, side)
     B = []
     for A, E in zip(env.tensors, row):
         if side == "north":

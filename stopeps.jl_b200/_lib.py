@@ -35,7 +35,7 @@ class sps_config(C.Structure):
 
 
 class sps_boundary(C.Structure):
-    _fields_ = [("chi", C.c_int32), ("space0", C.c_int32), ("space1", C.c_int32)]
+    _fields_ = [("chi", C.c_int32), ("space0", C.c_int32), ("space1", C.c_int32), ("absorption", C.c_int32)]
 
 
 class sps_step_report(C.Structure):

@@ -74,6 +74,14 @@ BoundaryMPSRow = BoundaryMPS
 
 
 @dataclass(frozen=True)
+class BoundaryMPSZipUp(BoundaryMPS):
+    """Row boundary MPS whose rows are absorbed by one zip-up sweep of
+    truncated SVDs (no canonical form), this library's variant of
+    ``BoundaryMPS``; same ``chi`` and ``sector_space`` truncation
+    (``boundary_mps.jl:18``)."""
+
+
+@dataclass(frozen=True)
 class ResamplingOptions:
     enabled: bool = True
     eta_th: float = 0.7

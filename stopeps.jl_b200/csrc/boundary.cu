@@ -124,9 +124,108 @@ CompressReport compress_boundary(Engine& E, std::vector<Tensor>& B, const BMPS& 
   return {max_error, scale == 0 ? -INFINITY : std::log(scale)};
 }
 
+// Truncated split of T (rows | cols) for the zip-up: `left` keeps the left
+// vectors as F (rows..., k) and returns W = S V^T (k, cols...); otherwise F =
+// V^T (k, cols...) and W = U S (rows..., k).
+static void zipup_split(Engine& E, const Tensor& T, const Trunc& tr, bool left, Tensor& F, Tensor& W,
+                        double& max_err) {
+  const std::vector<int> rows{0, 1}, cols{2, 3};
+  double err, nrm;
+  if (svd_prefers_kept(T, rows, cols, tr, false)) {
+    KeptSVD f = svd_kept(E, T, rows, cols, tr, false, left);
+    F = f.F;
+    W = f.W;
+    err = f.err;
+    nrm = f.norm;
+  } else {
+    SVDres f = svd(E, T, rows, cols, tr, false);
+    std::vector<double> sv(f.S[0]);
+    sv.insert(sv.end(), f.S[1].begin(), f.S[1].end());
+    if (left) {
+      F = f.U;
+      W = scale_leg(E, f.V, 0, sv);
+    } else {
+      F = f.V;
+      W = scale_leg(E, f.U, 2, sv);
+    }
+    err = f.err;
+    nrm = f.norm;
+  }
+  max_err = std::max(max_err, nrm == 0 ? 0.0 : (err / nrm) * (err / nrm));
+}
+
+// Zip-up row absorption, this engine's variant (no counterpart in the
+// reference): the boundary is brought into the canonical form opposite to the
+// sweep (LQ sweep north, QR sweep south, on the small chi-bond tensors), then
+// one sweep in which the carried factor times the boundary tensor times the
+// row tensor is split by a truncated SVD with the truncation of
+// _boundary_svd (boundary_mps.jl:33-42); the isometry becomes the new boundary
+// tensor, the rest is carried on.  No canonical form is built, so no LQ/QR of
+// the (chi d) x (d chi d) absorbed tensors is needed.  The centre is
+// normalised as in compress_boundary! (boundary_mps.jl:129-133).
+static Env absorb_zipup(Engine& E, const Env& env, const std::vector<Tensor>& row, const BMPS& m, bool north) {
+  const int N = (int)row.size();
+  Trunc tr;
+  tr.chi = m.chi;
+  tr.space[0] = m.space[0];
+  tr.space[1] = m.space[1];
+  std::vector<Tensor> out(N);
+  double max_err = 0;
+  Par triv = make_par(1, 0);
+  int center;
+  std::vector<Tensor> B = env.t;
+  if (north) {
+    // right-canonical boundary (LQ sweep on the chi-bond tensors), so that
+    // everything right of the zip front except the row is an isometry
+    for (int x = N - 1; x >= 1; --x) {
+      LQres f = lq(E, B[x], {0}, {1, 2});
+      B[x] = f.Q;
+      B[x - 1] = ein(E, "lnk,kr->lnr", B[x - 1], f.L);
+    }
+    Tensor C = unit_tensor(E, {triv, B[0].legs[0], row[0].legs[0]});   // (a, l, w)
+    for (int x = 0; x < N; ++x) {
+      Tensor T1 = ein(E, "alw,lnr->awnr", C, B[x]);
+      Tensor T = ein(E, "awnr,wnes->asre", T1, row[x]);
+      if (x == N - 1) {
+        out[x] = fuse(E, T, 2, 2);
+        break;
+      }
+      zipup_split(E, T, tr, true, out[x], C, max_err);
+    }
+    center = N - 1;
+  } else {
+    // left-canonical boundary (QR sweep)
+    for (int x = 0; x < N - 1; ++x) {
+      QRres f = qr(E, B[x], {0, 1}, {2});
+      B[x] = f.Q;
+      B[x + 1] = ein(E, "lk,knr->lnr", f.R, B[x + 1]);
+    }
+    Tensor C = unit_tensor(E, {B[N - 1].legs[2], row[N - 1].legs[2], triv});   // (r, e, a)
+    for (int x = N - 1; x >= 0; --x) {
+      Tensor T1 = ein(E, "lsr,rea->lsea", B[x], C);
+      Tensor T = ein(E, "lsea,wnes->lwna", T1, row[x]);
+      if (x == 0) {
+        out[x] = fuse(E, T, 0, 2);
+        break;
+      }
+      zipup_split(E, T, tr, false, out[x], C, max_err);
+    }
+    center = 0;
+  }
+  double scale = norm(E, out[center]);
+  if (!std::isfinite(scale)) throw Error(SPS_ERR_NUMERIC, "nonfinite boundary norm");
+  if (scale != 0) scale_inplace(E, out[center], 1.0 / scale);
+  Env res;
+  res.t = std::move(out);
+  res.log_scale = env.log_scale + (scale == 0 ? -INFINITY : std::log(scale));
+  res.max_trunc = std::max(env.max_trunc, max_err);
+  return res;
+}
+
 // _absorb for the row method (boundary_mps.jl:136-151)
 Env absorb(Engine& E, const Env& env, const std::vector<Tensor>& row, const BMPS& m, bool north,
            Entropy* ent, int row_cut) {
+  if (m.zipup) return absorb_zipup(E, env, row, m, north);
   std::vector<Tensor> B;
   B.reserve(row.size());
   for (size_t x = 0; x < row.size(); ++x) {

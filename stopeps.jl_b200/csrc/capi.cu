@@ -51,6 +51,8 @@ BMPS to_bmps(const sps_boundary* b) {
   m.chi = b->chi;
   m.space[0] = b->space0 >= 0 && b->space1 >= 0 ? b->space0 : -1;
   m.space[1] = b->space0 >= 0 && b->space1 >= 0 ? b->space1 : -1;
+  if (b->absorption != 0 && b->absorption != 1) throw Error(SPS_ERR_ARGUMENT, "unknown boundary absorption");
+  m.zipup = b->absorption == 1;
   return m;
 }
 

@@ -23,6 +23,7 @@ struct FUOptions {   // FullUpdate (src/evolution/full_update.jl:11-17)
 struct BMPS {        // BoundaryMPS (src/contraction/boundary_mps.jl:11-18)
   int chi = 32;
   int space[2] = {-1, -1};
+  bool zipup = false;   // zip-up row absorption (this engine's variant) instead of the exact compression
 };
 
 struct State {       // FiniteState (src/states/finite.jl:27-49)

@@ -14,7 +14,7 @@ import math
 import numpy as np
 
 from . import _lib
-from .config import BoundaryMPS, RunConfig, TFIM, FullUpdate, Z2Space
+from .config import BoundaryMPS, BoundaryMPSZipUp, RunConfig, TFIM, FullUpdate, Z2Space
 
 
 def _arr(a, ctype):
@@ -28,6 +28,7 @@ def _boundary(m: BoundaryMPS):
         b.space0 = b.space1 = -1
     else:
         b.space0, b.space1 = int(m.sector_space.n0), int(m.sector_space.n1)
+    b.absorption = 1 if isinstance(m, BoundaryMPSZipUp) else 0
     return b
 
 

@@ -146,3 +146,31 @@ def test_error_status_is_raised(sps):
         sps.sample_configuration(sps.SamplingCache(st, sps.BoundaryMPS(4)))
     with pytest.raises(sps._lib.EngineError):
         sps.lognorm(st, sps.BoundaryMPS(0))
+
+
+@pytest.mark.parametrize("case", CASES)
+def test_zipup_draws_and_energy(sps, case):
+    """The zip-up absorption against its oracle restatement (gauge-invariant
+    outputs to 1e-10), and against the reference's exact compression within
+    the precision target of the batched path (energy per site within 1e-4)."""
+    from oracle import boundary as bm, model as md, sampling as osp
+    g = golden(case)
+    e = _engine(sps, g)
+    st = upload_golden(sps, g, e)
+    chi, a, b = (int(v) for v in g["chi0"])
+    osp_space = None if a < 0 else (a, b)
+    zm = sps.BoundaryMPSZipUp(chi, None if a < 0 else sps.Z2Space(a, b))
+    ost = oracle_state(g)
+    ocache = osp.SamplingCache(ost, bm.BoundaryMPS(chi, osp_space, zipup=True))
+    cache = sps.SamplingCache(st, zm)
+    for u, cfg in zip(g["uniforms"], g["configs"]):
+        d = sps.sample_configuration(cache, uniforms=u)
+        od = osp.sample_configuration(ocache, uniforms=u)
+        np.testing.assert_array_equal(d["configuration"], np.asarray(od["configuration"]))
+        assert rel(d["log_probability"], od["log_probability"]) < TOL
+    model = md.TFIM(float(g["J"]), float(g["h"]))
+    oe = osp.measure_energy(ost, model, bm.BoundaryMPS(chi, osp_space, zipup=True))
+    en = sps.measure_energy(st, zm)
+    assert rel(en["energy_per_site"], oe["energy_per_site"]) < TOL
+    assert rel(en["log_norm"], oe["log_norm"]) < TOL
+    assert abs(en["energy_per_site"] - g["energy0"][1]) < 1e-4
