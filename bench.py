@@ -41,6 +41,8 @@ def parse():
     p.add_argument("--steps", type=int, default=4)
     p.add_argument("--warmup", type=int, default=3)
     p.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    p.add_argument("--concurrency", type=int, default=4,
+                   help="samples drawn at the same time on one GPU (own stream and workspace each)")
     return p.parse_args()
 
 
@@ -211,13 +213,21 @@ def ours_arm(args, rank, world, local_rank):
             dist.barrier()
         torch.cuda.synchronize()
 
-    def measure(method, steps, warmup, profile):
-        """Device-timed and end-to-end Born draws from a cache built with `method`."""
+    def measure(method, steps, warmup, profile, batch=1):
+        """Device-timed and end-to-end Born draws from a cache built with `method`;
+        a step is `batch` draws (concurrent when batch > 1)."""
         cache = sps.SamplingCache(st, method)
+        e.set_concurrency(batch)
 
         def draw(i):
-            u = sps.sample_uniforms(SEED, i, LX * LY)
-            return sps.sample_configuration(cache, uniforms=u)
+            # draw j of step index i uses the uniforms of sample id i * W + j (W: the zip-up batch)
+            ids = [i * W + j for j in range(batch)]
+            if batch == 1:
+                d = sps.sample_configuration(cache, uniforms=sps.sample_uniforms(SEED, ids[0], LX * LY))
+                return [dict(d, uid=ids[0])]
+            u = np.stack([sps.sample_uniforms(SEED, k, LX * LY) for k in ids])
+            cfg, lp = sps.sample_batch(cache, u)
+            return [{"configuration": c, "log_probability": l, "uid": k} for c, l, k in zip(cfg, lp, ids)]
 
         for s in range(warmup):
             draw(index(s))
@@ -227,7 +237,7 @@ def ours_arm(args, rank, world, local_rank):
         with Clocks(local_rank) as clk:
             e.timer_start()
             for s in range(steps):
-                draws.append(draw(index(warmup + s)))
+                draws.extend(draw(index(warmup + s)))
             ms = e.timer_stop()
         n1, _ = e.counters()
         barrier()
@@ -241,26 +251,37 @@ def ours_arm(args, rank, world, local_rank):
         if dist is not None:
             dist.all_reduce(t, op=dist.ReduceOp.MAX)
         stats = None
-        if profile:   # per-kernel profile of one draw (separate pass; not part of the timed number)
+        if profile:   # per-kernel profile of one serial draw (separate pass; not part of the timed number)
+            e.set_concurrency(1)
             e.set_profile(True)
-            draw(index(2 * steps + warmup))
+            u = sps.sample_uniforms(SEED, index(2 * steps + warmup) * W, LX * LY)
+            sps.sample_configuration(cache, uniforms=u)
             stats = e.kernel_stats()
             e.set_profile(False)
+        e.set_concurrency(1)
         del cache
         return {"ms": float(t[0]), "wall": float(t[1]), "launches": int(n1 - n0), "clocks": clk.summary(),
                 "draws": draws, "stats": stats}
 
-    zip_run = measure(sps.BoundaryMPSZipUp(CHI, space), args.steps, args.warmup, True)
+    W = max(1, args.concurrency)
+    zip_run = measure(sps.BoundaryMPSZipUp(CHI, space), args.steps, args.warmup, True, W)
     plain_steps = max(1, min(args.steps, 2))
     plain_run = measure(sps.BoundaryMPS(CHI, space), plain_steps, min(args.warmup, 3), False)
-    value = world * args.steps / (zip_run["ms"] * 1e-3)
-    e2e = world * args.steps / zip_run["wall"]
+    value = world * args.steps * W / (zip_run["ms"] * 1e-3)
+    e2e = world * args.steps * W / zip_run["wall"]
     plain_value = world * plain_steps / (plain_run["ms"] * 1e-3)
     plain_e2e = world * plain_steps / plain_run["wall"]
     # the two paths on the same draw indices
     import numpy as np
     same, dlp = 0, 0.0
-    for dz, dp in zip(zip_run["draws"], plain_run["draws"]):
+    # the two paths on the same uniforms (same sample ids)
+    zmap = {d["uid"]: d for d in zip_run["draws"]}
+    same, dlp, ncmp = 0, 0.0, 0
+    for dp in plain_run["draws"]:
+        dz = zmap.get(dp["uid"])
+        if dz is None:
+            continue
+        ncmp += 1
         same += int(np.array_equal(dz["configuration"], dp["configuration"]))
         dlp = max(dlp, abs(dz["log_probability"] - dp["log_probability"]))
     result = None
@@ -293,9 +314,11 @@ def ours_arm(args, rank, world, local_rank):
                   "warmup": args.warmup, "ms_per_step": zip_run["ms"] / args.steps, "higher_is_better": True,
                   "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
                   "config": workload_config({"parallelism": f"samples sharded over {world} GPU(s)",
-                                             "path": "zip-up boundary absorption, FP64, one sample per launch"}),
-                  "e2e": {"value": e2e, "unit": "samples/s", "h2d_bytes_per_step": 8 * L,
-                          "d2h_bytes_per_step": 4 * L + 8 + 8},
+                                             "path": f"zip-up boundary absorption, FP64, {W} samples "
+                                                     "concurrently (own stream and workspace each)",
+                                             "samples_per_step": W}),
+                  "e2e": {"value": e2e, "unit": "samples/s", "h2d_bytes_per_step": 8 * L * W,
+                          "d2h_bytes_per_step": (4 * L + 8) * W},
                   "gpu_launches": zip_run["launches"], "clocks": zip_run["clocks"], "roofline": roofline,
                   "cpu_baseline": cpu,
                   "plain_fp64": {"value": plain_value, "e2e": plain_e2e, "unit": "samples/s",
@@ -303,8 +326,8 @@ def ours_arm(args, rank, world, local_rank):
                                  "gpu_launches": plain_run["launches"], "clocks": plain_run["clocks"],
                                  "path": "reference algorithm: exact LQ sweep + truncated SVD sweep, FP64"},
                   "speedup_vs_plain_fp64": value / plain_value,
-                  "agreement_vs_plain": {"draws": min(len(zip_run["draws"]), len(plain_run["draws"])),
-                                         "identical_configurations": same, "max_abs_dlogp": dlp}}
+                  "agreement_vs_plain": {"draws": ncmp, "identical_configurations": same,
+                                         "max_abs_dlogp": dlp}}
         print(json.dumps(result), flush=True)
     del st
     e.close()

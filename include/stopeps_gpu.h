@@ -196,6 +196,12 @@ int sps_sample(sps_handle* h, int32_t cache_id, const double* uniforms, int32_t*
 /* sample_configuration(cache; configuration) : probability of a given draw */
 int sps_sample_probability(sps_handle* h, int32_t cache_id, const int32_t* configuration,
                            sps_sample_report* report);
+/* No counterpart in the reference (its ensemble is spread over MPI ranks):
+ * the number of samples sps_sample_batch draws at the same time, each on its
+ * own CUDA stream and device workspace, sharing the read-only SamplingCache
+ * (1..16, default 1).  Each concurrent sample's cooperative launches use at
+ * most 1/samples of the SMs. */
+int sps_set_concurrency(sps_handle* h, int32_t samples);
 /* n draws in one call (the MPI sample loop of src/driver/run.jl:45-49 on one device) */
 int sps_sample_batch(sps_handle* h, int32_t cache_id, int32_t n, const double* uniforms,
                      int32_t* configurations, double* log_probabilities);

@@ -171,7 +171,7 @@ void copy_upper_and_identity(Engine& E, const double* a, int m, int n, int lda, 
 static int coop_blocks(const void* kernel, int threads, size_t smem, Engine& E) {
   int per_sm = 0;
   SPS_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kernel, threads, smem));
-  return std::max(1, per_sm) * E.num_sms;
+  return E.coop_capacity(per_sm);
 }
 
 // Householder QR of a (m x n, col-major lda), m >= n: q (m x n, ldq), r (n x n, ldr).
@@ -1045,7 +1045,7 @@ void svd_big(Engine& E, const std::vector<MatDesc>& d) {
                                   (int)bsmem));
     int per_sm = 0;
     SPS_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, (const void*)bjacobi_kernel, BT, bsmem));
-    int G = std::min({E.num_sms * std::max(1, per_sm), std::max(1, pairs)});
+    int G = std::min({E.coop_capacity(per_sm), std::max(1, pairs)});
     const JacProb* dp = (const JacProb*)pb->ptr;
     int nprob = (int)ps.size();
     unsigned* bar = (unsigned*)bb->ptr;

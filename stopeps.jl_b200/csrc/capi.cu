@@ -2,6 +2,7 @@
 // state / cache ids, status codes and the last error message.
 #include "stopeps_gpu.h"
 #include "pipeline.h"
+#include <thread>
 #include <cstdio>
 #include <cstring>
 #include <algorithm>
@@ -12,6 +13,9 @@ using namespace sps;
 
 struct sps_handle {
   std::unique_ptr<Engine> E;
+  // batch workers: one engine (stream, pool, staging) per concurrent sample
+  std::vector<std::unique_ptr<Engine>> workers;
+  int concurrency = 1;
   cudaEvent_t t0 = nullptr, t1 = nullptr;
   sps_config cfg;
   std::unordered_map<int, State> states;
@@ -118,8 +122,22 @@ int sps_last_error(const sps_handle* h, char* buf, size_t n) {
 
 int sps_counters(sps_handle* h, long long* launches, double* flops) {
   return guarded(h, [&] {
-    if (launches) *launches = h->E->launches;
-    if (flops) *flops = h->E->flops;
+    long long n = h->E->launches;
+    double f = h->E->flops;
+    for (auto& w : h->workers) {
+      n += w->launches;
+      f += w->flops;
+    }
+    if (launches) *launches = n;
+    if (flops) *flops = f;
+  });
+}
+
+int sps_set_concurrency(sps_handle* h, int32_t samples) {
+  return guarded(h, [&] {
+    if (samples < 1 || samples > 16) throw Error(SPS_ERR_ARGUMENT, "concurrency must be in 1..16");
+    h->concurrency = samples;
+    for (auto& w : h->workers) w->ctas_cap = h->E->num_sms / samples;
   });
 }
 
@@ -587,12 +605,60 @@ int sps_sample_batch(sps_handle* h, int32_t cache_id, int32_t n, const double* u
                      double* log_probabilities) {
   return guarded(h, [&] {
     SamplingCache& c = get_cache(h, cache_id);
-    int L = c.Lx * c.Ly;
-    for (int i = 0; i < n; ++i) {
-      SampleResult r = sample_configuration(*h->E, c, uniforms + (size_t)i * L, nullptr);
-      for (int k = 0; k < L; ++k) configurations[(size_t)i * L + k] = r.config[k];
-      log_probabilities[i] = r.log_probability;
+    const int L = c.Lx * c.Ly;
+    const int W = std::min<int>(h->concurrency, std::max(n, 1));
+    if (W <= 1) {
+      for (int i = 0; i < n; ++i) {
+        SampleResult r = sample_configuration(*h->E, c, uniforms + (size_t)i * L, nullptr);
+        for (int k = 0; k < L; ++k) configurations[(size_t)i * L + k] = r.config[k];
+        log_probabilities[i] = r.log_probability;
+      }
+      return;
     }
+    // W samples at a time, each on its own engine and stream; the shared
+    // cache is read-only.  The handle's stream waits for the workers, so
+    // events recorded on it bracket the whole batch.
+    Engine& M = *h->E;
+    while ((int)h->workers.size() < W) {
+      h->workers.push_back(std::make_unique<Engine>(M.device));
+      h->workers.back()->ctas_cap = M.num_sms / h->concurrency;
+    }
+    cudaEvent_t start;
+    SPS_CUDA(cudaEventCreateWithFlags(&start, cudaEventDisableTiming));
+    SPS_CUDA(cudaEventRecord(start, M.stream));
+    for (int w = 0; w < W; ++w) SPS_CUDA(cudaStreamWaitEvent(h->workers[w]->stream, start, 0));
+    std::vector<int> codes(W, SPS_OK);
+    std::vector<std::string> msgs(W);
+    std::vector<std::thread> threads;
+    for (int w = 0; w < W; ++w)
+      threads.emplace_back([&, w] {
+        try {
+          SPS_CUDA(cudaSetDevice(M.device));
+          Engine& E = *h->workers[w];
+          for (int i = w; i < n; i += W) {
+            SampleResult r = sample_configuration(E, c, uniforms + (size_t)i * L, nullptr);
+            for (int k = 0; k < L; ++k) configurations[(size_t)i * L + k] = r.config[k];
+            log_probabilities[i] = r.log_probability;
+          }
+        } catch (const Error& e) {
+          codes[w] = e.code;
+          msgs[w] = e.what();
+        } catch (const std::exception& e) {
+          codes[w] = SPS_ERR_ARGUMENT;
+          msgs[w] = e.what();
+        }
+      });
+    for (auto& t : threads) t.join();
+    for (int w = 0; w < W; ++w) {
+      cudaEvent_t done;
+      SPS_CUDA(cudaEventCreateWithFlags(&done, cudaEventDisableTiming));
+      SPS_CUDA(cudaEventRecord(done, h->workers[w]->stream));
+      SPS_CUDA(cudaStreamWaitEvent(M.stream, done, 0));
+      SPS_CUDA(cudaEventDestroy(done));
+    }
+    SPS_CUDA(cudaEventDestroy(start));
+    for (int w = 0; w < W; ++w)
+      if (codes[w] != SPS_OK) throw Error(codes[w], msgs[w]);
   });
 }
 

@@ -12,6 +12,7 @@
 // Split-K writes FP64 partials that a second kernel reduces in a fixed order.
 #include "engine.h"
 #include <algorithm>
+#include <mutex>
 
 namespace sps {
 namespace la {
@@ -182,12 +183,11 @@ void dgemm_cm(Engine& E, bool ta, int M, int N, int K, double alpha, const doubl
     part = E.alloc(sizeof(double) * (size_t)splits * M * N);
     partial = (double*)part->ptr;
   }
-  static bool attr = false;
-  if (!attr) {
+  static std::once_flag attr;
+  std::call_once(attr, [] {
     SPS_CUDA(cudaFuncSetAttribute(dgemm_tc_kernel<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)SMEM));
     SPS_CUDA(cudaFuncSetAttribute(dgemm_tc_kernel<false>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)SMEM));
-    attr = true;
-  }
+  });
   const int tk = E.tic("dgemm_cm");
   if (ta)
     dgemm_tc_kernel<true><<<grid, NT, SMEM, E.stream>>>(M, N, K, A, lda, B, ldb, C, ldc, alpha, beta, kchunk, partial);

@@ -11,6 +11,7 @@
 // alike).  Every GEMM, QR, LQ, SVD and eigendecomposition works on those
 // blocks, which is what TensorKit does per coupled sector of a Z2 TensorMap.
 #pragma once
+#include <algorithm>
 #include <cuda_runtime.h>
 #include <cstdint>
 #include <cstdio>
@@ -127,6 +128,14 @@ class Engine {
   double* hscal = nullptr;
   double* dscal = nullptr;
   static constexpr int NSCAL = 4096;
+
+  // largest grid of a cooperative launch (0: the whole GPU); engines that run
+  // concurrently on one GPU share its SMs
+  int ctas_cap = 0;
+  int coop_capacity(int per_sm) const {
+    const int c = std::max(1, per_sm) * num_sms;
+    return ctas_cap > 0 ? std::min(c, ctas_cap) : c;
+  }
 
   // starting iteration count of the subspace-iteration SVD (adapted per call)
   int topk_hint = 6;

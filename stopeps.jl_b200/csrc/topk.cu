@@ -24,6 +24,7 @@
 #include "coop.cuh"
 #include <cfloat>
 #include <algorithm>
+#include <mutex>
 
 namespace sps {
 namespace la {
@@ -33,9 +34,9 @@ namespace {
 constexpr int TT = 256;           // threads per CTA
 constexpr int TW = TT / 32;       // warps per CTA
 constexpr int KMAXB = 80;         // largest block size b
-constexpr int RMAX = 32;          // largest number of rows owned by one CTA
+constexpr int RMAX = 48;          // largest number of rows owned by one CTA
 constexpr int KC = 32;            // contraction chunk of the row GEMM
-constexpr int NST = 4;            // pipeline stages of the row GEMM (asynchronous copies)
+constexpr int NST = 3;            // pipeline stages of the row GEMM (asynchronous copies)
 constexpr int XLD = KC + 4;       // row stride of the staged operands: a fragment load is 2 wavefronts
 constexpr int STAGE = (RMAX + KMAXB) * XLD;
 constexpr int YLD = KMAXB + 1;
@@ -49,7 +50,7 @@ constexpr int SMEM_DOUBLES = OFF_R + 16 + KMAXB;
 constexpr int JLD = KMAXB + 1;    // Jacobi arrays (CTA 0 only, overlays X..V)
 constexpr int MAX_SWEEPS = 40;
 static_assert(2 * KMAXB * JLD <= OFF_R, "Jacobi overlay exceeds the shared arena");
-constexpr int MAXT = (RMAX / 8) * (KMAXB / 8) / TW;   // 8 x 8 output tiles per warp
+constexpr int MAXT = ((RMAX / 8) * (KMAXB / 8) + TW - 1) / TW;   // 8 x 8 output tiles per warp
 static_assert(RMAX % 8 == 0 && KMAXB % 8 == 0 && KC % 4 == 0 && XLD % 2 == 0, "tiling");
 static_assert(TT >= 256, "the 16 x 16 thread grid of the small factorizations needs 256 threads");
 
@@ -629,20 +630,19 @@ bool topk_fits(int k, int m, int n, int nprob, Engine& E) {
   const int b = topk_block_size(k, m, n);
   if (b == 0) return false;
   const int P = (std::max(m, n) + RMAX - 1) / RMAX;
-  return P * nprob <= E.num_sms;
+  return P * nprob <= E.coop_capacity(1);
 }
 
 void svd_topk(Engine& E, std::vector<TopkDesc>& ds, double tol) {
   if (ds.empty()) return;
-  static bool attr = false;
+  static std::once_flag attr;
   const size_t smem = sizeof(double) * SMEM_DOUBLES;
-  if (!attr) {
+  std::call_once(attr, [smem] {
     SPS_CUDA(cudaFuncSetAttribute(topk_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
-    attr = true;
-  }
+  });
   int per_sm = 0;
   SPS_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, topk_kernel, TT, smem));
-  const int capacity = std::max(1, per_sm) * E.num_sms;
+  const int capacity = E.coop_capacity(per_sm);
   const int nprob = (int)ds.size();
   std::vector<TopkProb> hp(nprob);
   std::vector<Buf> keep;

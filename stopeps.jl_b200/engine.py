@@ -75,6 +75,10 @@ class Engine:
         self.check(self.lib.sps_counters(self.h, C.byref(n), C.byref(f)))
         return n.value, f.value
 
+    def set_concurrency(self, samples: int):
+        """How many samples ``sample_batch`` draws at the same time (own stream and workspace each)."""
+        self.check(self.lib.sps_set_concurrency(self.h, int(samples)))
+
     def set_profile(self, enable: bool):
         self.check(self.lib.sps_set_profile(self.h, 1 if enable else 0))
 

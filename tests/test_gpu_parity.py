@@ -174,3 +174,23 @@ def test_zipup_draws_and_energy(sps, case):
     assert rel(en["energy_per_site"], oe["energy_per_site"]) < TOL
     assert rel(en["log_norm"], oe["log_norm"]) < TOL
     assert abs(en["energy_per_site"] - g["energy0"][1]) < 1e-4
+
+
+@pytest.mark.parametrize("case", ["pepo_4x4_D4.npz"])
+def test_concurrent_batch_matches_serial(sps, case):
+    """Samples drawn concurrently (own stream and workspace each, shared cache)
+    are the serial draws: same configurations, log-probabilities to rounding."""
+    g = golden(case)
+    e = _engine(sps, g)
+    st = upload_golden(sps, g, e)
+    for m in (_bmps(sps, *g["chi0"]),
+              sps.BoundaryMPSZipUp(int(g["chi0"][0]), _bmps(sps, *g["chi0"]).sector_space)):
+        cache = sps.SamplingCache(st, m)
+        u = np.stack([sps.sample_uniforms(3, i, int(g["Lx"]) * int(g["Ly"])) for i in range(1, 8)])
+        e.set_concurrency(1)
+        c1, l1 = sps.sample_batch(cache, u)
+        e.set_concurrency(3)
+        c3, l3 = sps.sample_batch(cache, u)
+        e.set_concurrency(1)
+        np.testing.assert_array_equal(c1, c3)
+        np.testing.assert_allclose(l1, l3, rtol=1e-12)
