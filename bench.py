@@ -41,7 +41,7 @@ def parse():
     p.add_argument("--steps", type=int, default=4)
     p.add_argument("--warmup", type=int, default=3)
     p.add_argument("--impl", default="ours", choices=["ours", "reference"])
-    p.add_argument("--concurrency", type=int, default=4,
+    p.add_argument("--concurrency", type=int, default=5,
                    help="samples drawn at the same time on one GPU (own stream and workspace each)")
     return p.parse_args()
 
@@ -274,6 +274,10 @@ def ours_arm(args, rank, world, local_rank):
     # the two paths on the same draw indices
     import numpy as np
     same, dlp = 0, 0.0
+    # precision of the zip-up path: energy per site of the beta0 state with both
+    # absorptions (outside the timed regions)
+    en_plain = sps.measure_energy(st, sps.BoundaryMPS(CHI, space))
+    en_zip = sps.measure_energy(st, sps.BoundaryMPSZipUp(CHI, space))
     # the two paths on the same uniforms (same sample ids)
     zmap = {d["uid"]: d for d in zip_run["draws"]}
     same, dlp, ncmp = 0, 0.0, 0
@@ -327,7 +331,12 @@ def ours_arm(args, rank, world, local_rank):
                                  "path": "reference algorithm: exact LQ sweep + truncated SVD sweep, FP64"},
                   "speedup_vs_plain_fp64": value / plain_value,
                   "agreement_vs_plain": {"draws": ncmp, "identical_configurations": same,
-                                         "max_abs_dlogp": dlp}}
+                                         "max_abs_dlogp": dlp},
+                  "precision": {"energy_per_site_plain_fp64": en_plain["energy_per_site"],
+                                "energy_per_site_zipup": en_zip["energy_per_site"],
+                                "abs_delta_e": abs(en_zip["energy_per_site"] - en_plain["energy_per_site"]),
+                                "tolerance": 1e-4,
+                                "state": "the synthetic beta0 PEPO of the workload, chi=36 (18+18)"}}
         print(json.dumps(result), flush=True)
     del st
     e.close()
