@@ -304,7 +304,9 @@ def ours_arm(args, rank, world, local_rank):
                                    "MEASURED_PEAKS.json); tensor-core FP64 and DFMA share the FP64 rate on B200",
                     "share_of_profiled_time": v["ms"] / tot if tot else None,
                     "kernels": {k: {"ms": round(s["ms"], 3), "count": s["count"],
-                                    "share": round(s["ms"] / tot, 4) if tot and "." not in k else None}
+                                    "share": round(s["ms"] / tot, 4) if tot and "." not in k else None,
+                                    "tflops": round(s["flops"] / (s["ms"] * 1e-3) / 1e12, 3)
+                                    if s["ms"] > 0 and s["flops"] > 0 else None}
                                 for k, s in sorted(stats.items(), key=lambda kv: -kv[1]["ms"])}}
         cpu = None
         if world == 1:

@@ -327,79 +327,133 @@ struct GemmProb {
 };
 
 static constexpr int TM = 64, TN = 64, TK = 16, GT = 256;
+static constexpr int GALD = TM + 8, GBLD = TN + 8;   // k-major tiles: a fragment load is 2 wavefronts
 
+__device__ __forceinline__ void dmma_f64(double& d0, double& d1, double a, double b) {
+  asm volatile("mma.sync.aligned.m8n8k4.row.col.f64.f64.f64.f64 {%0,%1}, {%2}, {%3}, {%0,%1};"
+               : "+d"(d0), "+d"(d1)
+               : "d"(a), "d"(b));
+}
+
+// C_c[i, j] = alpha sum_k A[ra[i] + ca[k]] B[rb[k] + cb[j]] for the parity
+// block c = blockIdx.z, written through C's tables.  The gathered operands
+// are staged global -> registers -> shared memory (double-buffered, so the
+// indirect loads of the next k tile overlap the products of this one) and
+// multiplied on the FP64 tensor cores (mma.m8n8k4.f64): 8 warps as 2 (M) x
+// 4 (N), warp tile 32 x 16.
 __global__ void __launch_bounds__(GT) gemm_gather_kernel(const GemmProb* probs, double alpha) {
   const GemmProb P = probs[blockIdx.z];
   const int i0 = blockIdx.y * TM, j0 = blockIdx.x * TN;
   if (i0 >= P.M || j0 >= P.N) return;
-  __shared__ double As[TK][TM + 1];
-  __shared__ double Bs[TK][TN + 1];
+  __shared__ __align__(16) double As[2][TK * GALD];
+  __shared__ __align__(16) double Bs[2][TK * GBLD];
   __shared__ int64_t rA[TM], cB[TN];
   const int t = threadIdx.x;
   if (t < TM) rA[t] = (i0 + t < P.M) ? P.ra[i0 + t] : 0;
   else if (t < TM + TN) cB[t - TM] = (j0 + t - TM < P.N) ? P.cb[j0 + t - TM] : 0;
-  const int tx = t % 16, ty = t / 16;
-  double acc[4][4] = {};
-  for (int k0 = 0; k0 < P.K; k0 += TK) {
-    __syncthreads();
-    // A tile: 64 x 16
+  __syncthreads();
+  double ra[4], rb[4];
+  auto load = [&](int k0) {
     if (P.a_kfast) {
-      int kk = t % 16;
-      int64_t ck = (k0 + kk < P.K) ? P.ca[k0 + kk] : -1;
+      const int kk = t % 16;
+      const int64_t ck = (k0 + kk < P.K) ? P.ca[k0 + kk] : -1;
 #pragma unroll
       for (int r = 0; r < 4; ++r) {
-        int ii = t / 16 + 16 * r;
-        As[kk][ii] = (ck >= 0 && i0 + ii < P.M) ? P.A[rA[ii] + ck] : 0.0;
+        const int ii = t / 16 + 16 * r;
+        ra[r] = (ck >= 0 && i0 + ii < P.M) ? P.A[rA[ii] + ck] : 0.0;
       }
     } else {
-      int ii = t % 64;
+      const int ii = t % 64;
 #pragma unroll
       for (int r = 0; r < 4; ++r) {
-        int kk = t / 64 + 4 * r;
-        As[kk][ii] = (k0 + kk < P.K && i0 + ii < P.M) ? P.A[rA[ii] + P.ca[k0 + kk]] : 0.0;
+        const int kk = t / 64 + 4 * r;
+        ra[r] = (k0 + kk < P.K && i0 + ii < P.M) ? P.A[rA[ii] + P.ca[k0 + kk]] : 0.0;
       }
     }
-    // B tile: 16 x 64
     if (P.b_jfast) {
-      int jj = t % 64;
+      const int jj = t % 64;
 #pragma unroll
       for (int r = 0; r < 4; ++r) {
-        int kk = t / 64 + 4 * r;
-        Bs[kk][jj] = (k0 + kk < P.K && j0 + jj < P.N) ? P.B[P.rb[k0 + kk] + cB[jj]] : 0.0;
+        const int kk = t / 64 + 4 * r;
+        rb[r] = (k0 + kk < P.K && j0 + jj < P.N) ? P.B[P.rb[k0 + kk] + cB[jj]] : 0.0;
       }
     } else {
-      int kk = t % 16;
-      int64_t rk = (k0 + kk < P.K) ? P.rb[k0 + kk] : -1;
+      const int kk = t % 16;
+      const int64_t rk = (k0 + kk < P.K) ? P.rb[k0 + kk] : -1;
 #pragma unroll
       for (int r = 0; r < 4; ++r) {
-        int jj = t / 16 + 16 * r;
-        Bs[kk][jj] = (rk >= 0 && j0 + jj < P.N) ? P.B[rk + cB[jj]] : 0.0;
+        const int jj = t / 16 + 16 * r;
+        rb[r] = (rk >= 0 && j0 + jj < P.N) ? P.B[rk + cB[jj]] : 0.0;
       }
+    }
+  };
+  auto store = [&](double* as, double* bs) {
+    if (P.a_kfast) {
+      const int kk = t % 16;
+#pragma unroll
+      for (int r = 0; r < 4; ++r) as[kk * GALD + t / 16 + 16 * r] = ra[r];
+    } else {
+      const int ii = t % 64;
+#pragma unroll
+      for (int r = 0; r < 4; ++r) as[(t / 64 + 4 * r) * GALD + ii] = ra[r];
+    }
+    if (P.b_jfast) {
+      const int jj = t % 64;
+#pragma unroll
+      for (int r = 0; r < 4; ++r) bs[(t / 64 + 4 * r) * GBLD + jj] = rb[r];
+    } else {
+      const int kk = t % 16;
+#pragma unroll
+      for (int r = 0; r < 4; ++r) bs[kk * GBLD + t / 16 + 16 * r] = rb[r];
+    }
+  };
+  const int warp = t >> 5, lane = t & 31, fr = lane >> 2, fc = lane & 3;
+  const int wm = (warp & 1) * 32, wn = (warp >> 1) * 16;
+  double acc[4][2][2];
+#pragma unroll
+  for (int a = 0; a < 4; ++a)
+#pragma unroll
+    for (int b = 0; b < 2; ++b) acc[a][b][0] = acc[a][b][1] = 0.0;
+  int buf = 0;
+  load(0);
+  store(As[0], Bs[0]);
+  __syncthreads();
+  for (int k0 = 0; k0 < P.K; k0 += TK) {
+    const bool more = k0 + TK < P.K;
+    if (more) load(k0 + TK);
+    const double* as = As[buf];
+    const double* bs = Bs[buf];
+#pragma unroll
+    for (int ks = 0; ks < TK; ks += 4) {
+      double fa[4], fb[2];
+#pragma unroll
+      for (int a = 0; a < 4; ++a) fa[a] = as[(ks + fc) * GALD + wm + a * 8 + fr];
+#pragma unroll
+      for (int b = 0; b < 2; ++b) fb[b] = bs[(ks + fc) * GBLD + wn + b * 8 + fr];
+#pragma unroll
+      for (int a = 0; a < 4; ++a)
+#pragma unroll
+        for (int b = 0; b < 2; ++b) dmma_f64(acc[a][b][0], acc[a][b][1], fa[a], fb[b]);
+    }
+    if (more) {
+      store(As[buf ^ 1], Bs[buf ^ 1]);
+      buf ^= 1;
     }
     __syncthreads();
-#pragma unroll
-    for (int kk = 0; kk < TK; ++kk) {
-      double a[4], b[4];
-#pragma unroll
-      for (int u = 0; u < 4; ++u) a[u] = As[kk][ty + 16 * u];
-#pragma unroll
-      for (int v = 0; v < 4; ++v) b[v] = Bs[kk][tx + 16 * v];
-#pragma unroll
-      for (int u = 0; u < 4; ++u)
-#pragma unroll
-        for (int v = 0; v < 4; ++v) acc[u][v] = fma(a[u], b[v], acc[u][v]);
-    }
   }
+  // accumulator fragment: row fr, columns 2 fc + {0, 1} of each 8 x 8 tile
 #pragma unroll
-  for (int u = 0; u < 4; ++u) {
-    int i = i0 + ty + 16 * u;
+  for (int a = 0; a < 4; ++a) {
+    const int i = i0 + wm + a * 8 + fr;
     if (i >= P.M) continue;
-    int64_t ro = P.rc[i];
+    const int64_t ro = P.rc[i];
 #pragma unroll
-    for (int v = 0; v < 4; ++v) {
-      int j = j0 + tx + 16 * v;
-      if (j < P.N) P.C[ro + P.cc[j]] = alpha * acc[u][v];
-    }
+    for (int b = 0; b < 2; ++b)
+#pragma unroll
+      for (int e = 0; e < 2; ++e) {
+        const int j = j0 + wn + b * 8 + 2 * fc + e;
+        if (j < P.N) P.C[ro + P.cc[j]] = alpha * acc[a][b][e];
+      }
   }
 }
 

@@ -121,12 +121,26 @@ __device__ __forceinline__ void cp_async16(double* dst, const double* src, int b
 __device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;" ::: "memory"); }
 template <int N>
 __device__ __forceinline__ void cp_async_wait() { asm volatile("cp.async.wait_group %0;" ::"n"(N) : "memory"); }
+// wait until at most n (0..MAXST-2) copy groups of this thread are pending
+constexpr int MAXST = 8;
+__device__ __forceinline__ void cp_async_wait_n(int n) {
+  switch (n) {
+    case 0: cp_async_wait<0>(); break;
+    case 1: cp_async_wait<1>(); break;
+    case 2: cp_async_wait<2>(); break;
+    case 3: cp_async_wait<3>(); break;
+    case 4: cp_async_wait<4>(); break;
+    case 5: cp_async_wait<5>(); break;
+    default: cp_async_wait<6>(); break;
+  }
+}
 
 // Ys[r][j] = sum_t X[(r0+r)*ldx + t] * S[j*lds + t]   (r < r1-r0, j < bb, t < K)
 // on the FP64 tensor cores: each warp owns whole 8 x 8 output tiles and runs
-// mma.m8n8k4 over the contraction.  Operands stream through NST stages of
-// shared memory by asynchronous 16-byte copies that bypass L1 (S is written by
-// other CTAs of the launch), contraction index contiguous as in global memory.
+// mma.m8n8k4 over the contraction.  Operands stream through shared-memory
+// stages sized to the tile (as many as fit, up to MAXST) by asynchronous
+// 16-byte copies that bypass L1 (S is written by other CTAs of the launch),
+// contraction index contiguous as in global memory.
 // Requires ldx, lds even and X, S 16-byte aligned.
 __device__ __noinline__ void gemm_rows(const Ctx& x, const double* __restrict__ X, int ldx, int K, const double* S,
                                        int lds, int bb, int r0, int r1) {
@@ -143,10 +157,12 @@ __device__ __noinline__ void gemm_rows(const Ctx& x, const double* __restrict__ 
     acc[q][0] = acc[q][1] = 0.0;
     const int tile = warp + q * TW;
     aoff[q] = tile < ntiles ? ((tile / nt) * 8 + fr) * XLD + fc : -1;
-    boff[q] = tile < ntiles ? (RMAX + (tile % nt) * 8 + fr) * XLD + fc : 0;
+    boff[q] = tile < ntiles ? (mt * 8 + (tile % nt) * 8 + fr) * XLD + fc : 0;
   }
+  const int stage = (mt + nt) * 8 * XLD;
+  const int nst = max(2, min(MAXST, (NST * STAGE) / stage));
   auto issue = [&](int c) {
-    double* st = x.sm + OFF_X + (c % NST) * STAGE;
+    double* st = x.sm + OFF_X + (c % nst) * stage;
     const int t0 = c * KC;
     for (int e = threadIdx.x; e < nX; e += TT) {
       const int r = e / HC, t = (e % HC) * 2;
@@ -156,22 +172,21 @@ __device__ __noinline__ void gemm_rows(const Ctx& x, const double* __restrict__ 
     for (int e = threadIdx.x; e < nS; e += TT) {
       const int j = e / HC, t = (e % HC) * 2;
       const int bytes = (j < bb) ? 8 * max(0, min(2, K - t0 - t)) : 0;
-      cp_async16(st + (RMAX + j) * XLD + t, bytes ? S + (size_t)j * lds + t0 + t : S, bytes);
+      cp_async16(st + (mt * 8 + j) * XLD + t, bytes ? S + (size_t)j * lds + t0 + t : S, bytes);
     }
   };
   const int nch = (K + KC - 1) / KC;
   __syncthreads();   // the stages may still be read by the previous phase
-#pragma unroll
-  for (int c = 0; c < NST - 1; ++c) {
+  for (int c = 0; c < nst - 1; ++c) {
     if (c < nch) issue(c);
     cp_async_commit();
   }
   for (int c = 0; c < nch; ++c) {
-    cp_async_wait<NST - 2>();
+    cp_async_wait_n(nst - 2);
     __syncthreads();
-    if (c + NST - 1 < nch) issue(c + NST - 1);
+    if (c + nst - 1 < nch) issue(c + nst - 1);
     cp_async_commit();
-    const double* st = x.sm + OFF_X + (c % NST) * STAGE;
+    const double* st = x.sm + OFF_X + (c % nst) * stage;
     const int ksteps = (min(KC, K - c * KC) + 3) / 4;
     for (int ks = 0; ks < ksteps; ++ks) {
 #pragma unroll
@@ -272,11 +287,13 @@ __device__ __noinline__ bool orth_pass(const Ctx& x, int bb, int r0, int r1, int
     for (int j = i + tx; j < bb; j += 16) Gs[i * GLD + j] = __ldcg(&p.G[i * bb + j]);
   __syncthreads();
   if (shifted) {
-    if (threadIdx.x == 0) {
+    if (threadIdx.x < 32) {   // trace by one warp, then the shift of shifted Cholesky QR on the diagonal
       double tr = 0.0;
-      for (int i = 0; i < bb; ++i) tr += Gs[i * GLD + i];
+      for (int i = threadIdx.x; i < bb; i += 32) tr += Gs[i * GLD + i];
+      tr = wsum(tr);
       const double sh = 11.0 * ((double)nrows * bb + (double)bb * (bb + 1)) * DBL_EPSILON * tr;
-      for (int i = 0; i < bb; ++i) Gs[i * GLD + i] += sh;
+      __syncwarp();
+      for (int i = threadIdx.x; i < bb; i += 32) Gs[i * GLD + i] += sh;
     }
   }
   for (int j = 0; j < bb; ++j) {
@@ -304,8 +321,14 @@ __device__ __noinline__ bool orth_pass(const Ctx& x, int bb, int r0, int r1, int
     for (int j = i + 1 + tx; j < bb; j += 16) Gs[i * GLD + j] *= invd[i];
   __syncthreads();
   if (racc && x.c == 0) {
-    // R = diag(sq) U;  Racc <- R (racc 1) or R Racc (racc 2), via CTA 0's partial slot
+    // R = diag(sq) U;  Racc <- R (racc 1) or R Racc (racc 2), via CTA 0's partial slot;
+    // the previous Racc is staged in shared memory (the GEMM stages are free here)
     double* tmp = gp;
+    double* old = x.sm + OFF_X;
+    if (racc == 2) {
+      for (int e = threadIdx.x; e < bb * bb; e += TT) old[e] = __ldcg(&p.Racc[e]);
+      __syncthreads();
+    }
     for (int e = threadIdx.x; e < bb * bb; e += TT) {
       const int i = e / bb, j = e - i * bb;
       double v = 0.0;
@@ -315,7 +338,7 @@ __device__ __noinline__ bool orth_pass(const Ctx& x, int bb, int r0, int r1, int
         } else {
           for (int l = i; l <= j; ++l) {
             const double ril = (l == i) ? sq[i] : sq[i] * Gs[i * GLD + l];
-            v = fma(ril, __ldcg(&p.Racc[l * bb + j]), v);
+            v = fma(ril, old[l * bb + j], v);
           }
         }
       }
@@ -581,16 +604,25 @@ __global__ void __launch_bounds__(TT, 1) topk_kernel(const TopkProb* __restrict_
       }
     }
     sync_group(x);
+    if (x.c == 0) {
+      // squared residual of vector i summed over the partials, one thread per i
+      double* res2 = sm + OFF_R + 16;
+      for (int i = threadIdx.x; i < k; i += TT) {
+        double v = 0.0;
+        for (int q = 0; q < p.P; ++q) v += __ldcg(&p.Gp[(size_t)q * KMAXB * KMAXB + i]);
+        res2[i] = v;
+      }
+      __syncthreads();
+    }
     if (x.c == 0 && threadIdx.x == 0) {
       const double s0 = __ldcg(&p.s[0]);
       const double fro = sqrt(__ldcg(&p.info[2]));
       const double thr = fmax(tol * s0, 8.0 * DBL_EPSILON * sqrt((double)max(p.m, p.n)) * fro);
+      const double* res2 = sm + OFF_R + 16;
       double worst = 0.0;
       bool zero = false;
       for (int i = 0; i < k; ++i) {
-        double v = 0.0;
-        for (int q = 0; q < p.P; ++q) v += __ldcg(&p.Gp[(size_t)q * KMAXB * KMAXB + i]);
-        worst = fmax(worst, thr > 0.0 ? sqrt(v) / thr : 0.0);
+        worst = fmax(worst, thr > 0.0 ? sqrt(res2[i]) / thr : 0.0);
         zero |= !(__ldcg(&p.s[i]) > 0.0);
       }
       p.info[1] = it;
@@ -733,6 +765,7 @@ void svd_topk(Engine& E, std::vector<TopkDesc>& ds, double tol) {
                   (void*)&qmax, (void*)&tol,   (void*)&flag, (void*)&trace};
   const int tid = E.tic("svd_topk");
   SPS_CUDA(cudaLaunchCooperativeKernel((const void*)topk_kernel, dim3(cta), dim3(TT), args, smem, E.stream));
+  E.toc(tid);
   E.launches++;
   // right vectors into the caller's layout, info and Ritz values to the host
   for (int i = 0; i < nprob; ++i)
@@ -777,7 +810,7 @@ void svd_topk(Engine& E, std::vector<TopkDesc>& ds, double tol) {
   // work of the launch: 2 m n b flops per half-iteration, plus the extraction
   double fl = 0;
   for (auto& d : ds) fl += (4.0 * d.iterations + 6.0) * d.m * d.n * d.b;
-  E.toc(tid, fl);
+  E.set_work(tid, fl);
   // next starting count: the count that converged; after four first-check
   // successes in a row, one less
   if (qused > q0) {

@@ -5,6 +5,7 @@
   python stopeps.jl_b200/kernel_probe.py topk        # leading 18 triplets of a 648x648 graded block
   python stopeps.jl_b200/kernel_probe.py gemm        # FP64 GEMM 23328x648x648 and the 648x648x23328 Gram
   python stopeps.jl_b200/kernel_probe.py draw        # one Born draw, 8x8 D=6 chi=36 (synthetic PEPO)
+  python stopeps.jl_b200/kernel_probe.py zipdraw     # the same draw with the zip-up absorption
 
 Each operation runs once to warm up and once more; the sizes are those of the
 8x8, D=6, chi=36 boundary compression (parity blocks of 648 and 23328 rows).
@@ -65,12 +66,13 @@ def main(which):
         for _ in range(2):
             q, r, ms = e.la_qr(a)
         print(f"qr 23328x648: {ms:.2f} ms")
-    elif which == "draw":
+    elif which in ("draw", "zipdraw"):
         e = sps.Engine(8, 8, sps.TFIM(1.0, 3.0))
         sites, dims = sps.synthetic.synthetic_pepo(8, 8, 6, 0.15, 7)
         st = e.upload_state(sites, dims, True, beta=0.4)
         sps.normalize_state(st)
-        cache = sps.SamplingCache(st, sps.BoundaryMPS(36, sps.Z2Space(18, 18)))
+        kind = sps.BoundaryMPS if which == "draw" else sps.BoundaryMPSZipUp
+        cache = sps.SamplingCache(st, kind(36, sps.Z2Space(18, 18)))
         for i in range(2):
             d = sps.sample_configuration(cache, uniforms=sps.sample_uniforms(1, i + 1, 64))
         print("draw log_probability", d["log_probability"])
