@@ -199,6 +199,9 @@ struct Trunc {
   int chi = -1;             // truncrank (-1: none)
   int space[2] = {-1, -1};  // truncspace per sector (-1: none)
   double atol = -1;         // trunctol (<0: none)
+  // acceptance of iteratively computed singular triplets: residual
+  // ||M v - s u|| relative to the largest singular value (rounding level by default)
+  double rtol = 5e-14;
 };
 struct SVDres {
   Tensor U, V;                    // U (rows..., new), V (new, cols...)

@@ -1393,7 +1393,7 @@ static bool svd_kept_topk(Engine& E, const BlockTables& bt, const Tensor& A, int
     dmap[c] = (int)ds.size();
     ds.push_back(d);
   }
-  la::svd_topk(E, ds, 5e-14);
+  la::svd_topk(E, ds, tr.rtol);
   for (auto& d : ds)
     if (d.status != 0) return false;
   std::vector<double> sv[2];

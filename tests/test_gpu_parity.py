@@ -194,3 +194,27 @@ def test_concurrent_batch_matches_serial(sps, case):
         e.set_concurrency(1)
         np.testing.assert_array_equal(c1, c3)
         np.testing.assert_allclose(l1, l3, rtol=1e-12)
+
+
+def test_rank_deficient_boundary(sps):
+    """A PEPO whose boundary blocks have rank 1 (the identity thermal factor in
+    D = 4 bonds): the subspace-iteration SVD meets zero Ritz values and hands
+    the blocks to the full Jacobi SVD; both absorptions agree with the oracle."""
+    from oracle import boundary as bm
+    from oracle.model import State
+    from oracle.z2 import T, leg
+    L = 4
+    sites, dims = sps.synthetic.synthetic_pepo(L, L, 4, 0.0, 7)
+    e = sps.Engine(L, L, sps.TFIM(1.0, 0.7))
+    st = e.upload_state(sites, dims, True, beta=0.0)
+    grid = [[None] * L for _ in range(L)]
+    for i, (a, d) in enumerate(zip(sites, dims)):
+        grid[i % L][i // L] = T(np.asarray(a, float), [leg(int(p), int(q)) for p, q in d])
+    ost = State(L, L, grid, 0.0, 0.0, "pepo")
+    for zip_up in (False, True):
+        kind = sps.BoundaryMPSZipUp if zip_up else sps.BoundaryMPS
+        ln = sps.lognorm(st, kind(16, sps.Z2Space(8, 8)))
+        ref = bm.lognorm(ost, bm.BoundaryMPS(16, (8, 8), zipup=zip_up))
+        # the normalised product state: log norm 0 (absolute comparison)
+        assert abs(ln["log_norm"] - ref["log_norm"]) < 1e-10
+        assert abs(ln["tensor_log_norm"] - ref["tensor_log_norm"]) < 1e-10
