@@ -172,6 +172,7 @@ static Env absorb_zipup(Engine& E, const Env& env, const std::vector<Tensor>& ro
   // the zip-up's own truncation error is far above rounding: its splits
   // accept singular triplets at a relative residual of 1e-10
   tr.rtol = 1e-10;
+  tr.gram = true;
   std::vector<Tensor> out(N);
   double max_err = 0;
   Par triv = make_par(1, 0);

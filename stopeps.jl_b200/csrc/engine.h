@@ -202,6 +202,9 @@ struct Trunc {
   // acceptance of iteratively computed singular triplets: residual
   // ||M v - s u|| relative to the largest singular value (rounding level by default)
   double rtol = 5e-14;
+  // iterate on M M^T (one product per step; the condition number is squared,
+  // so only for an rtol far above rounding)
+  bool gram = false;
 };
 struct SVDres {
   Tensor U, V;                    // U (rows..., new), V (new, cols...)
@@ -274,6 +277,7 @@ struct TopkDesc {
   int m, n, k;
   double* U;                 // m x k (ld m), left vectors, descending values
   double* V;                 // n x k (ld n), right vectors
+  bool gram = false;         // iterate on the Gram matrix M M^T (extraction still from M)
   // results
   int b = 0, status = -1, iterations = 0;
   double fro2 = 0, residual = 0;   // ||M||_F^2; largest residual / acceptance threshold

@@ -1389,6 +1389,7 @@ static bool svd_kept_topk(Engine& E, const BlockTables& bt, const Tensor& A, int
     d.k = kmax[c];
     d.U = Mb[c] + (size_t)m[c] * n[c];
     d.V = d.U + (size_t)m[c] * kmax[c];
+    d.gram = tr.gram;
     Fv[c] = left ? d.U : d.V;
     dmap[c] = (int)ds.size();
     ds.push_back(d);

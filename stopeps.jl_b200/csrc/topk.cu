@@ -66,6 +66,7 @@ struct TopkProb {
   double* Q;     // m x b (ld ldm)
   double* Z;     // n x b (ld ldn): Omega, Z iterates, Qb
   double* Vi;    // n x k (ld ldn): right vectors
+  const double* Gm;  // m x m (ld ldm): M M^T when iterating on the Gram matrix, else null
   double* Gp;    // P x KMAXB^2 Gram partials
   double* G;     // b x b
   double* Racc;  // b x b accumulated R of M^T Q (row-major)
@@ -550,6 +551,14 @@ __global__ void __launch_bounds__(TT, 1) topk_kernel(const TopkProb* __restrict_
 
   int it = 0, target = q0;
   for (;;) {
+    for (; it < target && p.Gm; ++it) {   // Gram iteration: Q = orth(M M^T Q)
+      gemm_rows(x, p.Gm, p.ldm, p.m, p.Q, p.ldm, b, x.rm0, x.rm1);
+      trace_mark(x, PH_GEMM);
+      if (!orth_pass(x, b, x.rm0, x.rm1, p.m, true, 0)) return;
+      store_rows(x, p.Q, p.ldm, b, x.rm0, x.rm1);
+      sync_group(x);
+      trace_mark(x, PH_STORE);
+    }
     for (; it < target; ++it) {
       gemm_rows(x, p.M, p.ldm, p.m, p.Q, p.ldm, b, x.rn0, x.rn1);
       trace_mark(x, PH_GEMM);
@@ -694,6 +703,7 @@ void svd_topk(Engine& E, std::vector<TopkDesc>& ds, double tol) {
     // every buffer read by the asynchronous copies has an even length, so all
     // of them start 16-byte aligned
     const size_t nd = (size_t)ldn * m + (size_t)ldm * b + (size_t)ldn * b + (size_t)ldn * d.k +
+                      (d.gram ? (size_t)ldm * m : 0) +
                       ((m & 1) ? (size_t)ldm * n : 0) + (size_t)P * KMAXB * KMAXB + 4 * (size_t)b * b + b + P + 8;
     Buf w = E.alloc(sizeof(double) * nd + 64);
     keep.push_back(w);
@@ -717,6 +727,12 @@ void svd_topk(Engine& E, std::vector<TopkDesc>& ds, double tol) {
     base += (size_t)ldn * b;
     p.Vi = base;
     base += (size_t)ldn * d.k;
+    double* g = nullptr;
+    if (d.gram) {
+      g = base;
+      base += (size_t)ldm * m;
+    }
+    p.Gm = g;
     if (m & 1) {   // odd leading dimension: an even-ld copy of M
       SPS_CUDA(cudaMemcpy2DAsync(base, sizeof(double) * ldm, d.M, sizeof(double) * m, sizeof(double) * m, n,
                                  cudaMemcpyDeviceToDevice, E.stream));
@@ -746,6 +762,7 @@ void svd_topk(Engine& E, std::vector<TopkDesc>& ds, double tol) {
     p.U = d.U;
     SPS_CUDA(cudaMemsetAsync(p.info, 0, sizeof(double) * 6 + 8, E.stream));
     transpose_cm(E, d.M, m, n, m, mt, ldn);
+    if (g) dgemm_cm(E, false, m, m, n, 1.0, p.M, ldm, mt, ldn, 0.0, g, ldm);   // G = M M^T
   }
   Buf pb = E.alloc(sizeof(TopkProb) * nprob);
   keep.push_back(pb);
@@ -809,7 +826,9 @@ void svd_topk(Engine& E, std::vector<TopkDesc>& ds, double tol) {
   }
   // work of the launch: 2 m n b flops per half-iteration, plus the extraction
   double fl = 0;
-  for (auto& d : ds) fl += (4.0 * d.iterations + 6.0) * d.m * d.n * d.b;
+  for (auto& d : ds)
+    fl += d.gram ? 2.0 * d.m * d.m * (d.n + d.iterations * d.b) + 6.0 * d.m * d.n * d.b
+                 : (4.0 * d.iterations + 6.0) * d.m * d.n * d.b;
   E.set_work(tid, fl);
   // next starting count: the count that converged; after four first-check
   // successes in a row, one less
