@@ -12,6 +12,7 @@
 // blocks, which is what TensorKit does per coupled sector of a Z2 TensorMap.
 #pragma once
 #include <algorithm>
+#include <unordered_map>
 #include <cuda_runtime.h>
 #include <cstdint>
 #include <cstdio>
@@ -128,6 +129,15 @@ class Engine {
   double* hscal = nullptr;
   double* dscal = nullptr;
   static constexpr int NSCAL = 4096;
+
+  // contraction plans: device-resident index tables of ein, keyed by the
+  // spec and the operands' layouts (the same layouts recur in every draw)
+  struct EinBlock {
+    Buf ra, ca, rb, cb, rc, cc;
+    int M = 0, N = 0, K = 0, a_kfast = 0, b_jfast = 0;
+  };
+  std::unordered_map<std::string, std::vector<EinBlock>> ein_plans;
+  size_t ein_plan_bytes = 0;
 
   // largest grid of a cooperative launch (0: the whole GPU); engines that run
   // concurrently on one GPU share its SMs

@@ -54,6 +54,10 @@ struct Entropy {     // BoundaryEntropy (boundary_mps.jl:44-57)
 struct Layer {       // a row entry: plain double layer or SlabColumn (boundary_mps.jl:212-215)
   Tensor a, b;
   bool slab = false;
+  // when set, `a` is double_layer(ket, ket) of the single-layer `ket` (legs
+  // W,N,P,Aux,E,S) and the row steps contract ket and bra one after the other
+  Tensor ket;
+  bool layered = false;
 };
 
 // contraction
@@ -64,14 +68,18 @@ Env trivial_boundary(Engine& E, const std::vector<Tensor>& row, bool north);
 struct CompressReport { double max_trunc, log_scale; };
 CompressReport compress_boundary(Engine& E, std::vector<Tensor>& B, const BMPS& m, bool reverse,
                                  Entropy* ent, bool south_side, int row_cut);
+// kets: optional single layers of the row (row[x] = double_layer(kets[x], kets[x])),
+// used by the zip-up absorption to contract ket and bra one after the other
 Env absorb(Engine& E, const Env& env, const std::vector<Tensor>& row, const BMPS& m, bool north,
-           Entropy* ent = nullptr, int row_cut = 0);
+           Entropy* ent = nullptr, int row_cut = 0, const std::vector<Tensor>* kets = nullptr);
 double close_boundary(Engine& E, const std::vector<Tensor>& B);
 struct LogNorm { double log_norm, tensor_log_norm, max_env_trunc; };
 LogNorm lognorm(Engine& E, const State& s, const BMPS& m);
 struct Envs { std::vector<Env> north, south; double max_trunc = 0; };
 Envs boundary_environments(Engine& E, const std::vector<Tensor>& layers, int Lx, int Ly, const BMPS& m,
                            int side /*0 both,1 north,2 south*/, Entropy* ent);
+// X (w, b, n, c) times double_layer(ket, ket) over (w, n) -> (b, c, e, s), ket then bra
+Tensor layer_apply_wn(Engine& E, const Tensor& X, const Tensor& ket);
 Tensor left_step(Engine& E, const Tensor& L, const Tensor& T, const Layer& row, const Tensor& B);
 Tensor right_step(Engine& E, const Tensor& T, const Layer& row, const Tensor& B, const Tensor& R);
 Tensor row_edge(Engine& E, const std::vector<Tensor>& top, const std::vector<Layer>& row,
@@ -113,6 +121,7 @@ struct SamplingCache {
   int Lx, Ly;
   std::vector<Tensor> layers;
   std::vector<std::array<Tensor, 2>> candidates;
+  std::vector<std::array<Tensor, 2>> candidate_kets;   // the projected single layers of the candidates
   std::vector<Env> south;
   BMPS method;
   const State* state_ref = nullptr;

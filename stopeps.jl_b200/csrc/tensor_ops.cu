@@ -903,31 +903,68 @@ Tensor ein(Engine& E, const std::string& spec, const Tensor& A, const Tensor& B,
   }
   for (int k : fa) ScA.push_back(C.strides[lo.find(la[k])]);
   for (int k : fb) ScB.push_back(C.strides[lo.find(lb[k])]);
+  // plan: the index tables of both parity blocks, cached per layout
+  std::string key = spec;
+  auto add_layout = [&key](const Tensor& T) {
+    key += '|';
+    for (int k = 0; k < T.rank(); ++k) {
+      key += std::to_string(T.dims[k]) + ':' + std::to_string(T.strides[k]) + ':';
+      uint64_t h = 1469598103934665603ull;   // FNV-1a of the leg's parities
+      for (uint8_t v : *T.legs[k]) h = (h ^ v) * 1099511628211ull;
+      key += std::to_string(h) + ',';
+    }
+  };
+  add_layout(A);
+  add_layout(B);
+  auto it = E.ein_plans.find(key);
+  if (it == E.ein_plans.end()) {
+    std::vector<Engine::EinBlock> blocks;
+    size_t bytes = 0;
+    for (int c = 0; c < 2; ++c) {
+      auto ra = block_index(LfA, SfA, c), rc = block_index(LfA, ScA, c);
+      auto ca = block_index(Lk, SkA, c), rb = block_index(Lk, SkB, c);
+      auto cb = block_index(LfB, SfB, c), cc = block_index(LfB, ScB, c);
+      if (ra.empty() || cb.empty() || ca.empty()) continue;
+      Engine::EinBlock bl;
+      E.upload_i64(ra, bl.ra);
+      E.upload_i64(ca, bl.ca);
+      E.upload_i64(rb, bl.rb);
+      E.upload_i64(cb, bl.cb);
+      E.upload_i64(rc, bl.rc);
+      E.upload_i64(cc, bl.cc);
+      bl.M = (int)ra.size();
+      bl.N = (int)cb.size();
+      bl.K = (int)ca.size();
+      bl.a_kfast = (ca.size() > 1 && ca[1] - ca[0] == 1) ? 1 : 0;
+      bl.b_jfast = (cb.size() > 1 && cb[1] - cb[0] == 1) ? 1 : (rb.size() > 1 && rb[1] - rb[0] == 1 ? 0 : 1);
+      bytes += 8 * (ra.size() + ca.size() + rb.size() + cb.size() + rc.size() + cc.size());
+      blocks.push_back(std::move(bl));
+    }
+    if (E.ein_plan_bytes + bytes > ((size_t)256 << 20)) {   // bounded: start over when full
+      E.ein_plans.clear();
+      E.ein_plan_bytes = 0;
+    }
+    E.ein_plan_bytes += bytes;
+    it = E.ein_plans.emplace(key, std::move(blocks)).first;
+  }
   std::vector<GemmProb> probs;
-  std::vector<Buf> keep;
   int maxM = 0, maxN = 0;
-  for (int c = 0; c < 2; ++c) {
-    auto ra = block_index(LfA, SfA, c), rc = block_index(LfA, ScA, c);
-    auto ca = block_index(Lk, SkA, c), rb = block_index(Lk, SkB, c);
-    auto cb = block_index(LfB, SfB, c), cc = block_index(LfB, ScB, c);
-    if (ra.empty() || cb.empty() || ca.empty()) continue;
+  for (const auto& bl : it->second) {
     GemmProb P;
     P.A = A.ptr();
     P.B = B.ptr();
     P.C = C.ptr();
-    Buf b1, b2, b3, b4, b5, b6;
-    P.ra = E.upload_i64(ra, b1);
-    P.ca = E.upload_i64(ca, b2);
-    P.rb = E.upload_i64(rb, b3);
-    P.cb = E.upload_i64(cb, b4);
-    P.rc = E.upload_i64(rc, b5);
-    P.cc = E.upload_i64(cc, b6);
-    keep.insert(keep.end(), {b1, b2, b3, b4, b5, b6});
-    P.M = (int)ra.size();
-    P.N = (int)cb.size();
-    P.K = (int)ca.size();
-    P.a_kfast = (ca.size() > 1 && ca[1] - ca[0] == 1) ? 1 : 0;
-    P.b_jfast = (cb.size() > 1 && cb[1] - cb[0] == 1) ? 1 : (rb.size() > 1 && rb[1] - rb[0] == 1 ? 0 : 1);
+    P.ra = (const int64_t*)bl.ra->ptr;
+    P.ca = (const int64_t*)bl.ca->ptr;
+    P.rb = (const int64_t*)bl.rb->ptr;
+    P.cb = (const int64_t*)bl.cb->ptr;
+    P.rc = (const int64_t*)bl.rc->ptr;
+    P.cc = (const int64_t*)bl.cc->ptr;
+    P.M = bl.M;
+    P.N = bl.N;
+    P.K = bl.K;
+    P.a_kfast = bl.a_kfast;
+    P.b_jfast = bl.b_jfast;
     maxM = std::max(maxM, P.M);
     maxN = std::max(maxN, P.N);
     E.flops += 2.0 * P.M * P.N * P.K;
