@@ -41,7 +41,7 @@ def parse():
     p.add_argument("--steps", type=int, default=4)
     p.add_argument("--warmup", type=int, default=3)
     p.add_argument("--impl", default="ours", choices=["ours", "reference"])
-    p.add_argument("--concurrency", type=int, default=5,
+    p.add_argument("--concurrency", type=int, default=8,
                    help="samples drawn at the same time on one GPU (own stream and workspace each)")
     return p.parse_args()
 

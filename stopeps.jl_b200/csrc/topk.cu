@@ -34,9 +34,9 @@ namespace {
 constexpr int TT = 256;           // threads per CTA
 constexpr int TW = TT / 32;       // warps per CTA
 constexpr int KMAXB = 80;         // largest block size b
-constexpr int RMAX = 48;          // largest number of rows owned by one CTA
+constexpr int RMAX = 96;          // largest number of rows owned by one CTA
 constexpr int KC = 32;            // contraction chunk of the row GEMM
-constexpr int NST = 3;            // pipeline stages of the row GEMM (asynchronous copies)
+constexpr int NST = 2;            // stage budget of the row GEMM, in stages of the largest tile
 constexpr int XLD = KC + 4;       // row stride of the staged operands: a fragment load is 2 wavefronts
 constexpr int STAGE = (RMAX + KMAXB) * XLD;
 constexpr int YLD = KMAXB + 1;
