@@ -15,6 +15,8 @@
 #include <cstring>
 #include <algorithm>
 #include <initializer_list>
+#include <mutex>
+#include <set>
 
 namespace sps {
 namespace la {
@@ -168,6 +170,24 @@ __global__ void __launch_bounds__(BT) panel_qr_kernel(PanelArgs p) {
 void copy_upper_and_identity(Engine& E, const double* a, int m, int n, int lda, double* r, int ldr, double* q,
                              int ldq);
 
+// Allow a kernel the device's full opt-in shared memory once per process: a
+// per-call attribute with the call's own size would race between host
+// threads that launch the same kernel with different sizes.
+static void allow_max_smem(const void* kernel) {
+  static std::mutex mu;
+  static std::set<const void*> done;
+  std::lock_guard<std::mutex> g(mu);
+  if (done.count(kernel)) return;
+  int dev = 0, maxopt = 0;
+  SPS_CUDA(cudaGetDevice(&dev));
+  SPS_CUDA(cudaDeviceGetAttribute(&maxopt, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev));
+  cudaFuncAttributes fa;
+  SPS_CUDA(cudaFuncGetAttributes(&fa, kernel));   // static shared memory counts against the limit
+  SPS_CUDA(cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                maxopt - (int)fa.sharedSizeBytes));
+  done.insert(kernel);
+}
+
 static int coop_blocks(const void* kernel, int threads, size_t smem, Engine& E) {
   int per_sm = 0;
   SPS_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kernel, threads, smem));
@@ -208,8 +228,7 @@ void qr_big_opt(Engine& E, double* a, int m, int n, int lda, double* q, int ldq,
       smem = sizeof(double) * std::max((size_t)rpc * jb, (size_t)2 * jb * jb);
       if (smem > 200 * 1024) throw Error(SPS_ERR_ARGUMENT, "qr_big: panel too tall for shared memory");
     }
-    SPS_CUDA(cudaFuncSetAttribute((const void*)panel_qr_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                  (int)std::max<size_t>(smem, 1)));
+    allow_max_smem((const void*)panel_qr_kernel);
     PanelArgs pa;
     pa.A = a;
     pa.lda = lda;
@@ -943,7 +962,7 @@ void jacobi_left(Engine& E, const std::vector<MatDesc>& d) {
                             : (reg ? (const void*)jacobi_u_kernel<true> : (const void*)jacobi_u_kernel<false>);
   size_t smem = blocked ? ubsmem : 0;
   if (blocked)
-    SPS_CUDA(cudaFuncSetAttribute(kfn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)std::max<size_t>(smem, 1)));
+    allow_max_smem(kfn);
   int maxg = coop_blocks(kfn, BT, smem, E);
   int G = blocked ? std::min(maxg, std::max(1, pairs))
                   : std::min({E.num_sms, maxg, std::max(1, (pairs + BW - 1) / BW)});
@@ -1041,8 +1060,7 @@ void svd_big(Engine& E, const std::vector<MatDesc>& d) {
   Buf bb = E.alloc(sizeof(unsigned) * 2 + sizeof(int) * 6);
   SPS_CUDA(cudaMemsetAsync(bb->ptr, 0, sizeof(unsigned) * 2 + sizeof(int) * 6, E.stream));
   if (blocked) {
-    SPS_CUDA(cudaFuncSetAttribute((const void*)bjacobi_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                  (int)bsmem));
+    allow_max_smem((const void*)bjacobi_kernel);
     int per_sm = 0;
     SPS_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, (const void*)bjacobi_kernel, BT, bsmem));
     int G = std::min({E.coop_capacity(per_sm), std::max(1, pairs)});

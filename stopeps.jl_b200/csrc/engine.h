@@ -12,6 +12,7 @@
 // blocks, which is what TensorKit does per coupled sector of a Z2 TensorMap.
 #pragma once
 #include <algorithm>
+#include <chrono>
 #include <unordered_map>
 #include <cuda_runtime.h>
 #include <cstdint>
@@ -124,6 +125,8 @@ class Engine {
   int* dflag = nullptr;
   // dflag[1]: largest Jacobi sweep count since the last reset (diagnostic)
   void check_flag(const char* where);
+  // throw for a flag value already copied to the host (after a sync)
+  void raise_flag(int value, const char* where);
 
   // pinned scalar scratch
   double* hscal = nullptr;
@@ -297,6 +300,15 @@ int topk_block_size(int k, int m, int n);   // 0 when the block is too small for
 bool topk_fits(int k, int m, int n, int nprob, Engine& E);
 void svd_topk(Engine& E, std::vector<TopkDesc>& ds, double tol);
 }  // namespace la
+
+// host time of a scope, recorded as a statistic in profile mode
+struct HostTimer {
+  Engine& E;
+  const char* name;
+  std::chrono::steady_clock::time_point t0;
+  HostTimer(Engine& e, const char* n);
+  ~HostTimer();
+};
 
 // gather/scatter between tensors and dense column-major block matrices
 void gather_block(Engine& E, const Tensor& A, const int64_t* rt, const int64_t* ct, int M, int N,

@@ -228,6 +228,14 @@ void Engine::set_work(int id, double fl, double by) {
   pending_[id].bytes = by;
 }
 
+HostTimer::HostTimer(Engine& e, const char* n) : E(e), name(n) {
+  if (E.profile) t0 = std::chrono::steady_clock::now();
+}
+HostTimer::~HostTimer() {
+  if (E.profile)
+    E.add_stat(name, std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - t0).count());
+}
+
 void Engine::add_stat(const std::string& name, double ms, long long count) {
   auto& k = stats_[name];
   k.ms += ms;
@@ -265,6 +273,10 @@ void Engine::check_flag(const char* where) {
   int h = 0;
   SPS_CUDA(cudaMemcpyAsync(&h, dflag, sizeof(int), cudaMemcpyDeviceToHost, stream));
   sync();
+  raise_flag(h, where);
+}
+
+void Engine::raise_flag(int h, const char* where) {
   if (h) {
     SPS_CUDA(cudaMemsetAsync(dflag, 0, sizeof(int), stream));
     if (h & 2) throw Error(SPS_ERR_CONVERGENCE, std::string(where) + ": device iteration cap reached");
@@ -846,6 +858,7 @@ void scatter_block(Engine& E, Tensor& A, const int64_t* rt, const int64_t* ct, i
 static bool same_par(const Par& a, const Par& b) { return a == b || *a == *b; }
 
 Tensor ein(Engine& E, const std::string& spec, const Tensor& A, const Tensor& B, double alpha) {
+  HostTimer ht(E, "host.ein");
   auto arrow = spec.find("->");
   auto comma = spec.find(',');
   if (arrow == std::string::npos || comma == std::string::npos || comma > arrow)
@@ -905,13 +918,15 @@ Tensor ein(Engine& E, const std::string& spec, const Tensor& A, const Tensor& B,
   for (int k : fb) ScB.push_back(C.strides[lo.find(lb[k])]);
   // plan: the index tables of both parity blocks, cached per layout
   std::string key = spec;
-  auto add_layout = [&key](const Tensor& T) {
-    key += '|';
+  auto add_layout = [&key](const Tensor& T) {   // binary: rank, then (dim, stride, parity hash) per leg
+    auto put = [&key](uint64_t v) { key.append(reinterpret_cast<const char*>(&v), sizeof v); };
+    put((uint64_t)T.rank());
     for (int k = 0; k < T.rank(); ++k) {
-      key += std::to_string(T.dims[k]) + ':' + std::to_string(T.strides[k]) + ':';
+      put((uint64_t)T.dims[k]);
+      put((uint64_t)T.strides[k]);
       uint64_t h = 1469598103934665603ull;   // FNV-1a of the leg's parities
       for (uint8_t v : *T.legs[k]) h = (h ^ v) * 1099511628211ull;
-      key += std::to_string(h) + ',';
+      put(h);
     }
   };
   add_layout(A);
@@ -1390,6 +1405,7 @@ static void kept_counts(const std::vector<double> sv[2], const Trunc& tr, const 
 // iteration did not converge; the caller then uses the full spectrum.
 static bool svd_kept_topk(Engine& E, const BlockTables& bt, const Tensor& A, int nr, int nc, const Trunc& tr,
                           bool left, KeptSVD& res) {
+  HostTimer ht(E, "host.svd_kept");
   int m[2], n[2], kmax[2];
   std::vector<la::TopkDesc> ds;
   int dmap[2] = {-1, -1};

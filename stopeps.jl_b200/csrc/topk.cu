@@ -671,19 +671,23 @@ bool topk_fits(int k, int m, int n, int nprob, Engine& E) {
   const int b = topk_block_size(k, m, n);
   if (b == 0) return false;
   const int P = (std::max(m, n) + RMAX - 1) / RMAX;
-  return P * nprob <= E.coop_capacity(1);
+  return P * nprob <= E.num_sms;   // one CTA per SM; the whole GPU (see svd_topk)
 }
 
 void svd_topk(Engine& E, std::vector<TopkDesc>& ds, double tol) {
   if (ds.empty()) return;
   static std::once_flag attr;
+  static int per_sm = 0;
   const size_t smem = sizeof(double) * SMEM_DOUBLES;
   std::call_once(attr, [smem] {
     SPS_CUDA(cudaFuncSetAttribute(topk_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+    SPS_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, topk_kernel, TT, smem));
   });
-  int per_sm = 0;
-  SPS_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, topk_kernel, TT, smem));
+  // the engine's share of the GPU is a target: a problem that needs more CTAs
+  // than its share gets the minimum it needs (the cooperative launch then
+  // waits for free SMs), up to the whole GPU
   const int capacity = E.coop_capacity(per_sm);
+  const int capacity_full = std::max(1, per_sm) * E.num_sms;
   const int nprob = (int)ds.size();
   std::vector<TopkProb> hp(nprob);
   std::vector<Buf> keep;
@@ -695,9 +699,10 @@ void svd_topk(Engine& E, std::vector<TopkDesc>& ds, double tol) {
     if (d.b == 0) throw Error(SPS_ERR_ARGUMENT, "svd_topk: block too small for subspace iteration");
     const int mx = std::max(m, n);
     int P = (mx + 11) / 12;                       // about 12 owned rows per CTA
+    P = std::min(P, std::max(1, capacity / nprob));
     P = std::max(P, (mx + RMAX - 1) / RMAX);
-    P = std::min(P, capacity / nprob);
-    if ((mx + P - 1) / P > RMAX) throw Error(SPS_ERR_ARGUMENT, "svd_topk: block too large for the grid");
+    if (P * nprob > capacity_full || (mx + P - 1) / P > RMAX)
+      throw Error(SPS_ERR_ARGUMENT, "svd_topk: block too large for the grid");
     const int b = d.b;
     const int ldm = m + (m & 1), ldn = n + (n & 1);
     // every buffer read by the asynchronous copies has an even length, so all
@@ -764,6 +769,7 @@ void svd_topk(Engine& E, std::vector<TopkDesc>& ds, double tol) {
     transpose_cm(E, d.M, m, n, m, mt, ldn);
     if (g) dgemm_cm(E, false, m, m, n, 1.0, p.M, ldm, mt, ldn, 0.0, g, ldm);   // G = M M^T
   }
+  if (cta > capacity_full) throw Error(SPS_ERR_ARGUMENT, "svd_topk: blocks too large for one cooperative grid");
   Buf pb = E.alloc(sizeof(TopkProb) * nprob);
   keep.push_back(pb);
   E.stage(hp.data(), sizeof(TopkProb) * nprob, pb->ptr);
@@ -795,9 +801,12 @@ void svd_topk(Engine& E, std::vector<TopkDesc>& ds, double tol) {
                              E.stream));
     off += 6 + hp[i].b;
   }
-  if (off > Engine::NSCAL) throw Error(SPS_ERR_ARGUMENT, "svd_topk: too many values");
+  if (off + 1 > Engine::NSCAL) throw Error(SPS_ERR_ARGUMENT, "svd_topk: too many values");
+  // the device flag travels with the values: one synchronisation
+  int* hflag = reinterpret_cast<int*>(E.hscal + off);
+  SPS_CUDA(cudaMemcpyAsync(hflag, E.dflag, sizeof(int), cudaMemcpyDeviceToHost, E.stream));
   E.sync();
-  E.check_flag("svd_topk");
+  E.raise_flag(*hflag, "svd_topk");
   off = 0;
   int qused = 0;
   for (int i = 0; i < nprob; ++i) {
