@@ -298,8 +298,16 @@ def ours_arm(args, rank, world, local_rank):
         per_launch_flops = v["flops"] / v["count"]
         avg_ms = v["ms"] / v["count"]
         achieved = per_launch_flops / (avg_ms * 1e-3) / 1e12
+        traffic = None
+        if name == "svd_topk":
+            # DRAM bytes of one svd_topk launch on a 648x648 pair of parity blocks (k = 18): ncu capture of
+            # `kernel_probe.py topk` (dram__bytes.sum.per_second x gpu__time_duration.sum); the two blocks'
+            # M and M^T are 6.7 MB, everything else of the launch stays in L2
+            traffic = 7.25e6
         roofline = {"bound": "tensor", "kernel": name, "achieved": achieved, "peak": peak, "unit": "TFLOP/s",
-                    "frac": achieved / peak, "traffic": None,
+                    "frac": achieved / peak, "traffic": traffic,
+                    "note": "svd_topk is a latency-bound cooperative kernel (chains of small dependent "
+                            "phases, one CTA per SM); FLOPs counted: 2 m n b per product",
                     "peak_source": "FP64: cuBLAS DGEMM 8192^3 measured in this run (FP64 is not in "
                                    "MEASURED_PEAKS.json); tensor-core FP64 and DFMA share the FP64 rate on B200",
                     "share_of_profiled_time": v["ms"] / tot if tot else None,
