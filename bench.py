@@ -300,10 +300,10 @@ def ours_arm(args, rank, world, local_rank):
         achieved = per_launch_flops / (avg_ms * 1e-3) / 1e12
         traffic = None
         if name == "svd_topk":
-            # DRAM bytes of one svd_topk launch on a 648x648 pair of parity blocks (k = 18): ncu capture of
-            # `kernel_probe.py topk` (dram__bytes.sum.per_second x gpu__time_duration.sum); the two blocks'
-            # M and M^T are 6.7 MB, everything else of the launch stays in L2
-            traffic = 7.25e6
+            # DRAM bytes per svd_topk launch: an ncu capture of `kernel_probe.py topk` (one 648x648 block,
+            # k = 18) moved 7.25 MB (dram__bytes.sum.per_second x gpu__time_duration.sum), its M and M^T
+            # (6.7 MB) read once; a bench launch holds both parity blocks of that size
+            traffic = 2 * 7.25e6
         roofline = {"bound": "tensor", "kernel": name, "achieved": achieved, "peak": peak, "unit": "TFLOP/s",
                     "frac": achieved / peak, "traffic": traffic,
                     "note": "svd_topk is a latency-bound cooperative kernel (chains of small dependent "
