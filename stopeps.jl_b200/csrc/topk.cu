@@ -730,7 +730,13 @@ void svd_topk(Engine& E, std::vector<TopkDesc>& ds, double tol) {
     base += (size_t)ldm * b;
     p.Z = base;
     base += (size_t)ldn * b;
-    p.Vi = base;
+    // right vectors straight into the caller's buffer when its layout suits
+    // the asynchronous copies (even n, 16-byte aligned), else via Vi
+    if (ldn == n && reinterpret_cast<uintptr_t>(d.V) % 16 == 0) {
+      p.Vi = d.V;
+    } else {
+      p.Vi = base;
+    }
     base += (size_t)ldn * d.k;
     double* g = nullptr;
     if (d.gram) {
@@ -792,8 +798,9 @@ void svd_topk(Engine& E, std::vector<TopkDesc>& ds, double tol) {
   E.launches++;
   // right vectors into the caller's layout, info and Ritz values to the host
   for (int i = 0; i < nprob; ++i)
-    SPS_CUDA(cudaMemcpy2DAsync(ds[i].V, sizeof(double) * hp[i].n, hp[i].Vi, sizeof(double) * hp[i].ldn,
-                               sizeof(double) * hp[i].n, hp[i].k, cudaMemcpyDeviceToDevice, E.stream));
+    if (hp[i].Vi != ds[i].V)
+      SPS_CUDA(cudaMemcpy2DAsync(ds[i].V, sizeof(double) * hp[i].n, hp[i].Vi, sizeof(double) * hp[i].ldn,
+                                 sizeof(double) * hp[i].n, hp[i].k, cudaMemcpyDeviceToDevice, E.stream));
   int off = 0;
   for (int i = 0; i < nprob; ++i) {
     SPS_CUDA(cudaMemcpyAsync(E.hscal + off, hp[i].info, sizeof(double) * 6, cudaMemcpyDeviceToHost, E.stream));

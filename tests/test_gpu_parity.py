@@ -218,3 +218,23 @@ def test_rank_deficient_boundary(sps):
         # the normalised product state: log norm 0 (absolute comparison)
         assert abs(ln["log_norm"] - ref["log_norm"]) < 1e-10
         assert abs(ln["tensor_log_norm"] - ref["tensor_log_norm"]) < 1e-10
+
+
+@pytest.mark.parametrize("zip_up", [False, True])
+def test_truncrank_without_sector_budget(sps, zip_up):
+    """truncrank(chi) with sector_space = nothing: the kept values are chosen
+    across both parity blocks (the subspace-iteration SVD computes chi per
+    block), against the oracle run live on the 4x4 D=4 fixture."""
+    from oracle import boundary as bm, model as md, sampling as osp
+    g = golden("pepo_4x4_D4.npz")
+    e = _engine(sps, g)
+    st = upload_golden(sps, g, e)
+    ost = oracle_state(g)
+    kind = sps.BoundaryMPSZipUp if zip_up else sps.BoundaryMPS
+    ln = sps.lognorm(st, kind(16, None))
+    ref = bm.lognorm(ost, bm.BoundaryMPS(16, None, zipup=zip_up))
+    assert rel(ln["log_norm"], ref["log_norm"]) < TOL
+    assert abs(ln["max_environment_truncation"] - ref["max_environment_truncation"]) < 1e-9
+    en = sps.measure_energy(st, kind(16, None))
+    oen = osp.measure_energy(ost, md.TFIM(float(g["J"]), float(g["h"])), bm.BoundaryMPS(16, None, zipup=zip_up))
+    assert rel(en["energy_per_site"], oen["energy_per_site"]) < TOL
