@@ -6,6 +6,7 @@
   python stopeps.jl_b200/kernel_probe.py gemm        # FP64 GEMM 23328x648x648 and the 648x648x23328 Gram
   python stopeps.jl_b200/kernel_probe.py draw        # one Born draw, 8x8 D=6 chi=36 (synthetic PEPO)
   python stopeps.jl_b200/kernel_probe.py zipdraw     # the same draw with the zip-up absorption
+  python stopeps.jl_b200/kernel_probe.py scale       # zip-up draws at 12x12 D=8 chi=64 (32+32): 1 and 4 at a time
 
 Each operation runs once to warm up and once more; the sizes are those of the
 8x8, D=6, chi=36 boundary compression (parity blocks of 648 and 23328 rows).
@@ -76,6 +77,29 @@ def main(which):
         for i in range(2):
             d = sps.sample_configuration(cache, uniforms=sps.sample_uniforms(1, i + 1, 64))
         print("draw log_probability", d["log_probability"])
+    elif which == "scale":
+        import time
+        L, Dd, chi = 12, 8, 64
+        e = sps.Engine(L, L, sps.TFIM(1.0, 3.0))
+        sites, dims = sps.synthetic.synthetic_pepo(L, L, Dd, 0.15, 11)
+        st = e.upload_state(sites, dims, True, beta=0.5)
+        sps.normalize_state(st)
+        t = time.perf_counter()
+        cache = sps.SamplingCache(st, sps.BoundaryMPSZipUp(chi, sps.Z2Space(chi // 2, chi // 2)))
+        print(f"cache {time.perf_counter() - t:.2f} s")
+        d = sps.sample_configuration(cache, uniforms=sps.sample_uniforms(1, 1, L * L))
+        t = time.perf_counter()
+        d = sps.sample_configuration(cache, uniforms=sps.sample_uniforms(1, 2, L * L))
+        print(f"one draw {time.perf_counter() - t:.3f} s, log_probability {d['log_probability']:.6f}")
+        for w in (4,):
+            e.set_concurrency(w)
+            u = np.stack([sps.sample_uniforms(1, 10 + j, L * L) for j in range(2 * w)])
+            sps.sample_batch(cache, u[:w])
+            t = time.perf_counter()
+            sps.sample_batch(cache, u)
+            dt = time.perf_counter() - t
+            print(f"{2 * w} draws {w} at a time: {dt:.3f} s, {2 * w / dt:.2f} samples/s")
+        e.set_concurrency(1)
     else:
         raise SystemExit(f"unknown operation {which}")
 
