@@ -75,7 +75,7 @@ struct TopkProb {
   double* U;     // m x k out (ld m)
   double* s;     // b Ritz values, descending
   double* fpart; // P partial squared Frobenius norms
-  double* info;  // [status, iterations, ||M||_F^2, max residual / threshold, done]
+  double* info;  // [status, iterations, ||M||_F^2, max residual / threshold, done, Ritz Jacobi sweeps]
   unsigned* bar; // 2 words
 };
 
@@ -439,6 +439,7 @@ __device__ __noinline__ void ritz_small(const Ctx& x, int bb) {
     __syncthreads();
     if (rotations == 0) break;
   }
+  if (threadIdx.x == 0) p.info[5] += sweep + 1;
   if (sweep == MAX_SWEEPS) {
     if (threadIdx.x == 0) p.info[0] = ST_JACOBI;
     return;
@@ -822,6 +823,7 @@ void svd_topk(Engine& E, std::vector<TopkDesc>& ds, double tol) {
     d.iterations = (int)E.hscal[off + 1];
     d.fro2 = E.hscal[off + 2];
     d.residual = E.hscal[off + 3];
+    if (E.profile) E.add_stat("svd_topk.sweeps", 0.0, (long long)E.hscal[off + 5]);
     d.s.assign(E.hscal + off + 6, E.hscal + off + 6 + d.b);
     qused = std::max(qused, d.iterations);
     off += 6 + d.b;
