@@ -359,9 +359,9 @@ __global__ void __launch_bounds__(BT) jacobi_coop_kernel(const JacProb* probs, i
         be = wsum(be);
         ga = wsum(ga);
         const double tol = DBL_EPSILON * (double)max(P.m, 2);
-        if (ga == 0.0 || !(fabs(ga) > tol * sqrt(al * be))) continue;
+        if (!(al >= DBL_MIN && be >= DBL_MIN) || ga == 0.0 || !(fabs(ga) > tol * sqrt(al) * sqrt(be))) continue;
         double zeta = (be - al) / (2.0 * ga);
-        double tt = copysign(1.0, zeta) / (fabs(zeta) + sqrt(1.0 + zeta * zeta));
+        double tt = copysign(1.0, zeta) / (fabs(zeta) + hypot(1.0, zeta));
         double c = 1.0 / sqrt(1.0 + tt * tt), s = c * tt;
         for (int i = lane; i < P.m; i += 32) {
           double x = up[i], y = uq[i];
@@ -512,9 +512,9 @@ __global__ void __launch_bounds__(BT) bjacobi_kernel(const JacProb* probs, int n
               al = wsum(al);
               be = wsum(be);
               ga = wsum(ga);
-              if (ga == 0.0 || !(fabs(ga) > tol * sqrt(al * be))) continue;
+              if (!(al >= DBL_MIN && be >= DBL_MIN) || ga == 0.0 || !(fabs(ga) > tol * sqrt(al) * sqrt(be))) continue;
               double zeta = (be - al) / (2.0 * ga);
-              double tt = copysign(1.0, zeta) / (fabs(zeta) + sqrt(1.0 + zeta * zeta));
+              double tt = copysign(1.0, zeta) / (fabs(zeta) + hypot(1.0, zeta));
               double c = 1.0 / sqrt(1.0 + tt * tt), s = c * tt;
               for (int i = lane; i < m; i += 32) {
                 double x = ua[i], y = ub[i];
@@ -685,9 +685,9 @@ __global__ void __launch_bounds__(BT) jacobi_u_kernel(const JUProb* probs, int n
           al = wsum(al);
           be = wsum(be);
           ga = wsum(ga);
-          if (ga == 0.0 || !(fabs(ga) > tol * sqrt(al * be))) continue;
+          if (!(al >= DBL_MIN && be >= DBL_MIN) || ga == 0.0 || !(fabs(ga) > tol * sqrt(al) * sqrt(be))) continue;
           double zeta = (be - al) / (2.0 * ga);
-          double tt = copysign(1.0, zeta) / (fabs(zeta) + sqrt(1.0 + zeta * zeta));
+          double tt = copysign(1.0, zeta) / (fabs(zeta) + hypot(1.0, zeta));
           double c = 1.0 / sqrt(1.0 + tt * tt), sn = c * tt;
 #pragma unroll
           for (int k = 0; k < JR; ++k) {
@@ -708,9 +708,9 @@ __global__ void __launch_bounds__(BT) jacobi_u_kernel(const JUProb* probs, int n
           al = wsum(al);
           be = wsum(be);
           ga = wsum(ga);
-          if (ga == 0.0 || !(fabs(ga) > tol * sqrt(al * be))) continue;
+          if (!(al >= DBL_MIN && be >= DBL_MIN) || ga == 0.0 || !(fabs(ga) > tol * sqrt(al) * sqrt(be))) continue;
           double zeta = (be - al) / (2.0 * ga);
-          double tt = copysign(1.0, zeta) / (fabs(zeta) + sqrt(1.0 + zeta * zeta));
+          double tt = copysign(1.0, zeta) / (fabs(zeta) + hypot(1.0, zeta));
           double c = 1.0 / sqrt(1.0 + tt * tt), sn = c * tt;
           for (int i = lane; i < m; i += 32) {
             double a = up[i], b = uq[i];
@@ -837,9 +837,9 @@ __global__ void __launch_bounds__(BT) jacobi_ub_kernel(const JUProb* probs, int 
             al = wsum(al);
             be = wsum(be);
             ga = wsum(ga);
-            if (ga == 0.0 || !(fabs(ga) > tol * sqrt(al * be))) continue;
+            if (!(al >= DBL_MIN && be >= DBL_MIN) || ga == 0.0 || !(fabs(ga) > tol * sqrt(al) * sqrt(be))) continue;
             double zeta = (be - al) / (2.0 * ga);
-            double tt = copysign(1.0, zeta) / (fabs(zeta) + sqrt(1.0 + zeta * zeta));
+            double tt = copysign(1.0, zeta) / (fabs(zeta) + hypot(1.0, zeta));
             double c = 1.0 / sqrt(1.0 + tt * tt), sn = c * tt;
             for (int i = lane; i < m; i += 32) {
               double x = ua[i], y = ub[i];

@@ -27,7 +27,7 @@ static void jacobi_sym(int n, double* a, double* v, double* w) {
         double apq = a[p * n + q];
         if (apq == 0) continue;
         double zeta = (a[q * n + q] - a[p * n + p]) / (2 * apq);
-        double t = std::copysign(1.0, zeta) / (std::fabs(zeta) + std::sqrt(1 + zeta * zeta));
+        double t = std::copysign(1.0, zeta) / (std::fabs(zeta) + std::hypot(1.0, zeta));
         double c = 1 / std::sqrt(1 + t * t), s = c * t;
         for (int k = 0; k < n; ++k) {  // A <- A J
           double x = a[k * n + p], y = a[k * n + q];
@@ -342,11 +342,46 @@ static void restore_pair(Engine& E, const Pair& p, const Tensor& A, const Tensor
   sb = perm(E, second, invperm(p.pb));
 }
 
-// _reduced_layer (full_update.jl:143-149): legs (w,n,e,rb,rk)
-static Tensor reduced_layer(Engine& E, const Tensor& Q) {
-  Tensor A = ein(E, "wneuk,WNEub->wWnNeEbk", Q, Q);
-  for (int k : {4, 2, 0}) A = fuse(E, A, k, 2);
-  return A;
+// X contracted over its legs x1, x2 with the reduced layer of Q
+// (_reduced_layer, full_update.jl:143-149: Q (x) Q over the auxiliary leg, the
+// outer legs' (ket, bra) pairs fused) on Q's outer legs q1, q2: the ket Q, then
+// the bra Q, never forming the d^3 r^2 layer.  Returns X's other legs in order,
+// then the fused pair of Q's remaining outer leg, then (bra bond, ket bond).
+// Q legs: three outer legs, auxiliary, reduced bond.
+static Tensor reduced_apply(Engine& E, const Tensor& X, int x1, int x2, const Tensor& Q, int q1, int q2) {
+  const int q3 = 3 - q1 - q2;
+  const int hi = std::max(x1, x2), lo = std::min(x1, x2);
+  const Par phi = Q.legs[hi == x1 ? q1 : q2], plo = Q.legs[lo == x1 ? q1 : q2];
+  Tensor S = split(E, split(E, X, hi, {phi, phi}), lo, {plo, plo});
+  auto ket_pos = [&](int x) { return x == lo ? lo : hi + 1; };   // bra half right after it
+  const int k1 = ket_pos(x1), k2 = ket_pos(x2);
+  std::string sx(S.rank(), '?'), fr;
+  char c = 'a';
+  for (int i = 0; i < S.rank(); ++i)
+    if (i != k1 && i != k1 + 1 && i != k2 && i != k2 + 1) {
+      sx[i] = c;
+      fr += c;
+      ++c;
+    }
+  sx[k1] = 'P';
+  sx[k1 + 1] = 'Q';
+  sx[k2] = 'R';
+  sx[k2 + 1] = 'S';
+  std::string qk(5, '?'), qb(5, '?');
+  qk[q1] = 'P';
+  qk[q2] = 'R';
+  qk[q3] = 'T';
+  qk[3] = 'U';
+  qk[4] = 'K';
+  qb[q1] = 'Q';
+  qb[q2] = 'S';
+  qb[q3] = 'V';
+  qb[3] = 'U';
+  qb[4] = 'B';
+  const std::string y1 = fr + "QSTUK", y2 = fr + "TVBK";
+  Tensor Y1 = ein(E, sx + "," + qk + "->" + y1, S, Q);
+  Tensor Y2 = ein(E, y1 + "," + qb + "->" + y2, Y1, Q);
+  return fuse(E, Y2, (int)fr.size(), 2);
 }
 
 struct BondEnv {
@@ -356,23 +391,26 @@ struct BondEnv {
   bool horizontal;
 };
 
-// _reduced_metric(::BondEnvironment) (full_update.jl:151-172)
+// _reduced_metric(::BondEnvironment) (full_update.jl:151-172), N[B,S,K,P]
+// (bra bonds of a and b, ket bonds of a and b).  The reduced layers enter
+// through reduced_apply; the vertical bond joins the right and bottom
+// environments first (Rh) and contracts the upper and lower halves once,
+// which is the same sum as the reference's order with far smaller GEMMs.
 static Tensor reduced_metric(Engine& E, const BondEnv& env, const Tensor& Qa, const Tensor& Qb) {
-  Tensor A = reduced_layer(E, Qa), B = reduced_layer(E, Qb);
   if (env.horizontal) {
     Tensor X = ein(E, "awb,anc->bncw", env.left, env.top[0]);
-    Tensor Y = ein(E, "bncw,wnsBK->bcsBK", X, A);
+    Tensor Y = reduced_apply(E, X, 3, 1, Qa, 0, 1);                 // (b c s B K)
     Tensor L = ein(E, "bcsBK,bsf->cfBK", Y, env.bottom[0]);
     Tensor U = ein(E, "deg,cvd->cveg", env.right, env.top[1]);
-    Tensor V = ein(E, "cveg,vetSP->cgtSP", U, B);
+    Tensor V = reduced_apply(E, U, 1, 2, Qb, 0, 1);                 // (c g t S P)
     Tensor R = ein(E, "cgtSP,ftg->cfSP", V, env.bottom[1]);
     return ein(E, "cfBK,cfSP->BSKP", L, R);
   }
   Tensor X = ein(E, "awvb,anc->wvbnc", env.left, env.top[0]);
-  Tensor Y = ein(E, "wvbnc,wneBK->vbceBK", X, A);
-  Tensor L = ein(E, "vbceBK,cefd->vbfdBK", Y, env.right);
-  Tensor R = ein(E, "vfsSP,bsd->vfSPbd", B, env.bottom[0]);
-  return ein(E, "vbfdBK,vfSPbd->BSKP", L, R);
+  Tensor Y = reduced_apply(E, X, 0, 3, Qa, 0, 1);                   // (v b c e B K)
+  Tensor RB = ein(E, "cefd,bsd->cefbs", env.right, env.bottom[0]);
+  Tensor Rh = reduced_apply(E, RB, 2, 4, Qb, 1, 2);                 // (c e b v S P)
+  return ein(E, "vbceBK,cebvSP->BSKP", Y, Rh);
 }
 
 // bond_hole (boundary_mps.jl:331-350): 12 legs (ket,bra) x 6

@@ -160,9 +160,11 @@ __global__ void __launch_bounds__(NT) svd_kernel(const MatDesc* ds, double* work
           al += x * x; be += y * y; ga += x * y;
         }
         al = warp_sum(al); be = warp_sum(be); ga = warp_sum(ga);
-        if (ga == 0.0 || !(fabs(ga) > tol * sqrt(al * be))) continue;
+        // a column whose squared norm underflows counts as zero: rotating it
+        // against a normal one is a no-op that would repeat every sweep
+        if (!(al >= DBL_MIN && be >= DBL_MIN) || ga == 0.0 || !(fabs(ga) > tol * sqrt(al) * sqrt(be))) continue;
         double zeta = (be - al) / (2.0 * ga);
-        double t = copysign(1.0, zeta) / (fabs(zeta) + sqrt(1.0 + zeta * zeta));
+        double t = copysign(1.0, zeta) / (fabs(zeta) + hypot(1.0, zeta));
         double c = 1.0 / sqrt(1.0 + t * t), s = c * t;
         for (int i = lane; i < m; i += 32) {
           double x = up[i], y = uq[i];
@@ -246,7 +248,10 @@ __global__ void __launch_bounds__(NT) eigh_kernel(const MatDesc* ds, double* wor
     part += x * x;
   }
   const double fro = sqrt(block_sum(part, red));
-  const double abs_floor = DBL_EPSILON * 1e-3 * fro;
+  // off-diagonals below eps ||A||_F are rounding noise (the backward error of
+  // any symmetric eigensolver); rotating them would not end for nearly
+  // rank-deficient matrices, whose diagonal is itself at noise level
+  const double abs_floor = DBL_EPSILON * fro;
   const int np = n + (n & 1);
   const int npair = np / 2;
   bool converged = (n == 1) || fro == 0.0;
@@ -265,7 +270,7 @@ __global__ void __launch_bounds__(NT) eigh_kernel(const MatDesc* ds, double* wor
           double app = A[p + (size_t)p * lda], aqq = A[q + (size_t)q * lda];
           if (apq != 0.0 && fabs(apq) > DBL_EPSILON * sqrt(fabs(app * aqq)) && fabs(apq) > abs_floor) {
             double zeta = (aqq - app) / (2.0 * apq);
-            double t = copysign(1.0, zeta) / (fabs(zeta) + sqrt(1.0 + zeta * zeta));
+            double t = copysign(1.0, zeta) / (fabs(zeta) + hypot(1.0, zeta));
             c = 1.0 / sqrt(1.0 + t * t);
             s = c * t;
             atomicAdd(&rotations, 1);

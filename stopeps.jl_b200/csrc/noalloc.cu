@@ -90,9 +90,9 @@ __global__ void __launch_bounds__(NT) svd_noalloc_kernel(const double* __restric
           al += x * x; be += y * y; ga += x * y;
         }
         al = warp_sum(al); be = warp_sum(be); ga = warp_sum(ga);
-        if (ga == 0.0 || !(fabs(ga) > tol * sqrt(al * be))) continue;
+        if (!(al >= DBL_MIN && be >= DBL_MIN) || ga == 0.0 || !(fabs(ga) > tol * sqrt(al) * sqrt(be))) continue;
         double zeta = (be - al) / (2.0 * ga);
-        double t = copysign(1.0, zeta) / (fabs(zeta) + sqrt(1.0 + zeta * zeta));
+        double t = copysign(1.0, zeta) / (fabs(zeta) + hypot(1.0, zeta));
         double c = 1.0 / sqrt(1.0 + t * t), sn = c * t;
         for (int i = lane; i < mm; i += 32) {
           double x = up[i], y = uq[i];

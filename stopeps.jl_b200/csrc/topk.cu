@@ -416,9 +416,9 @@ __device__ __noinline__ void ritz_small(const Ctx& x, int bb) {
           be += __shfl_xor_sync(0xffffffffu, be, o);
           ga += __shfl_xor_sync(0xffffffffu, ga, o);
         }
-        if (active && ga != 0.0 && fabs(ga) > tol_rot * sqrt(al) * sqrt(be)) {
+        if (active && al >= DBL_MIN && be >= DBL_MIN && ga != 0.0 && fabs(ga) > tol_rot * sqrt(al) * sqrt(be)) {
           const double zeta = (be - al) / (2.0 * ga);
-          const double t = copysign(1.0, zeta) / (fabs(zeta) + sqrt(1.0 + zeta * zeta));
+          const double t = copysign(1.0, zeta) / (fabs(zeta) + hypot(1.0, zeta));
           const double cs = 1.0 / sqrt(1.0 + t * t), sn = cs * t;
           double* jp = J + pp * JLD;
           double* jq = J + qq * JLD;

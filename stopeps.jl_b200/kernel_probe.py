@@ -7,6 +7,7 @@
   python stopeps.jl_b200/kernel_probe.py draw        # one Born draw, 8x8 D=6 chi=36 (synthetic PEPO)
   python stopeps.jl_b200/kernel_probe.py zipdraw     # the same draw with the zip-up absorption
   python stopeps.jl_b200/kernel_probe.py scale       # zip-up draws at 12x12 D=8 chi=64 (32+32): 1 and 4 at a time
+  python stopeps.jl_b200/kernel_probe.py fustep [L]  # one full-update Trotter step, L x L D=6 chi=36 (default 8)
 
 Each operation runs once to warm up and once more; the sizes are those of the
 8x8, D=6, chi=36 boundary compression (parity blocks of 648 and 23328 rows).
@@ -100,6 +101,23 @@ def main(which):
             dt = time.perf_counter() - t
             print(f"{2 * w} draws {w} at a time: {dt:.3f} s, {2 * w / dt:.2f} samples/s")
         e.set_concurrency(1)
+    elif which == "fustep":
+        import time
+        L = int(sys.argv[2]) if len(sys.argv) > 2 else 8
+        for zipup in (True, False):
+            e = sps.Engine(L, L, sps.TFIM(1.0, 3.0))
+            sites, dims = sps.synthetic.synthetic_pepo(L, L, 6, 0.15, 7)
+            st = e.upload_state(sites, dims, True, beta=0.4)
+            sps.normalize_state(st)
+            kind = sps.BoundaryMPSZipUp if zipup else sps.BoundaryMPS
+            e.set_profile(True)
+            t = time.perf_counter()
+            r = sps.evolution_step(st, 0.02, 6, kind(36, sps.Z2Space(18, 18)), sps.Z2Space(3, 3))
+            dt = time.perf_counter() - t
+            top = sorted(e.kernel_stats().items(), key=lambda kv: -kv[1]["ms"])[:6]
+            print(f"{L}x{L} {'zip-up' if zipup else 'exact'} environments: {dt:.2f} s, bond updates "
+                  f"{r['bond_updates']}, " + ", ".join(f"{k} {v['ms']:.0f} ms" for k, v in top))
+            e.close()
     else:
         raise SystemExit(f"unknown operation {which}")
 
