@@ -133,13 +133,20 @@ int sps_la_svd_left(sps_handle* h, int32_t m, int32_t n, const double* a, double
  * (ld k); c m x n (ld m). */
 int sps_la_gemm(sps_handle* h, int32_t transpose_a, int32_t m, int32_t n, int32_t k, double alpha, const double* a,
                 const double* b, double beta, double* c, double* ms);
+/* No counterpart in the reference.  Caps the cooperative launches of the
+ * handle's own (serial) path at `ctas` CTAs each, 0 = the whole GPU: for a
+ * handle that shares its GPU with other work.  sps_set_concurrency sets the
+ * caps of the concurrent samples' engines. */
+int sps_set_sm_share(sps_handle* h, int32_t ctas);
 /* Leading k singular triplets by block subspace iteration with Rayleigh-Ritz
  * extraction (the truncated boundary SVD when no entropy is recorded):
  * u (m x k), s (k, descending), v (n x k), column-major; iterations = the
- * count used.  SPS_ERR_CONVERGENCE when the residuals did not reach rounding
- * level within the iteration cap. */
-int sps_la_svd_topk(sps_handle* h, int32_t m, int32_t n, int32_t k, const double* a, double* u, double* s,
-                    double* v, int32_t* iterations, double* ms);
+ * count used.  gram != 0 iterates on a a^T (the zip-up splits' mode; the
+ * extraction and the residual test still use a).  rtol: the residual bound
+ * relative to s[0] (0 selects 5e-14).  SPS_ERR_CONVERGENCE when the residuals
+ * did not reach it within the iteration cap. */
+int sps_la_svd_topk(sps_handle* h, int32_t m, int32_t n, int32_t k, const double* a, int32_t gram, double rtol,
+                    double* u, double* s, double* v, int32_t* iterations, double* ms);
 
 /* No counterpart in the reference.  The one-sided Jacobi SVD of one small
  * matrix for callers that cannot allocate device memory (no cudaMalloc /

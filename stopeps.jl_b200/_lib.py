@@ -20,6 +20,7 @@ EXPORTS = [
     "sps_sampling_cache", "sps_sampling_cache_free", "sps_sample", "sps_sample_probability",
     "sps_sample_batch", "sps_project", "sps_set_profile", "sps_kernel_stats_json", "sps_timer_start",
     "sps_timer_stop", "sps_la_svd", "sps_la_qr", "sps_la_svd_noalloc", "sps_la_svd_left", "sps_la_svd_topk", "sps_la_gemm", "sps_set_concurrency",
+    "sps_set_sm_share",
 ]
 
 STATUS = {0: "SPS_OK", 1: "SPS_ERR_ARGUMENT", 2: "SPS_ERR_CUDA", 3: "SPS_ERR_NUMERIC",
@@ -110,8 +111,10 @@ def load():
         "sps_la_svd_noalloc": ([i32, vp, i32, i32, vp, vp, vp, vp], C.c_int),
         "sps_la_svd_left": ([vp, i32, i32, P(dbl), P(dbl), P(dbl), P(i32), P(dbl)], C.c_int),
         "sps_set_concurrency": ([vp, i32], C.c_int),
+        "sps_set_sm_share": ([vp, i32], C.c_int),
         "sps_la_gemm": ([vp, i32, i32, i32, i32, dbl, P(dbl), P(dbl), dbl, P(dbl), P(dbl)], C.c_int),
-        "sps_la_svd_topk": ([vp, i32, i32, i32, P(dbl), P(dbl), P(dbl), P(dbl), P(i32), P(dbl)], C.c_int),
+        "sps_la_svd_topk": ([vp, i32, i32, i32, P(dbl), i32, C.c_double, P(dbl), P(dbl), P(dbl), P(i32), P(dbl)],
+                            C.c_int),
     }
     for name, (args, res) in sig.items():
         f = getattr(lib, name)

@@ -141,10 +141,17 @@ int sps_set_concurrency(sps_handle* h, int32_t samples) {
   });
 }
 
+int sps_set_sm_share(sps_handle* h, int32_t ctas) {
+  return guarded(h, [&] {
+    if (ctas < 0 || ctas > h->E->num_sms) throw Error(SPS_ERR_ARGUMENT, "sps_set_sm_share: ctas must be in 0..SMs");
+    h->E->ctas_cap = ctas;
+  });
+}
+
 int sps_set_profile(sps_handle* h, int32_t enable) {
   return guarded(h, [&] {
     h->E->reset_stats();
-    h->E->profile = enable != 0;
+    h->E->profile = enable < 0 ? 0 : (enable > 2 ? 2 : enable);
   });
 }
 
@@ -277,8 +284,8 @@ int sps_la_svd_left(sps_handle* h, int32_t m, int32_t n, const double* a, double
   });
 }
 
-int sps_la_svd_topk(sps_handle* h, int32_t m, int32_t n, int32_t k, const double* a, double* u, double* s,
-                    double* v, int32_t* iterations, double* ms) {
+int sps_la_svd_topk(sps_handle* h, int32_t m, int32_t n, int32_t k, const double* a, int32_t gram, double rtol,
+                    double* u, double* s, double* v, int32_t* iterations, double* ms) {
   return guarded(h, [&] {
     Engine& E = *h->E;
     if (k < 1 || la::topk_block_size(k, m, n) == 0)
@@ -294,12 +301,14 @@ int sps_la_svd_topk(sps_handle* h, int32_t m, int32_t n, int32_t k, const double
     ds[0].k = k;
     ds[0].U = (double*)bu->ptr;
     ds[0].V = ds[0].U + (size_t)m * k;
+    ds[0].gram = gram != 0;
+    if (!(rtol >= 0.0)) throw Error(SPS_ERR_ARGUMENT, "sps_la_svd_topk: rtol must be >= 0");
     if (!h->t0) {
       SPS_CUDA(cudaEventCreate(&h->t0));
       SPS_CUDA(cudaEventCreate(&h->t1));
     }
     SPS_CUDA(cudaEventRecord(h->t0, E.stream));
-    la::svd_topk(E, ds, 5e-14);
+    la::svd_topk(E, ds, rtol > 0.0 ? rtol : 5e-14);
     SPS_CUDA(cudaEventRecord(h->t1, E.stream));
     SPS_CUDA(cudaMemcpyAsync(u, ds[0].U, sizeof(double) * (size_t)m * k, cudaMemcpyDeviceToHost, E.stream));
     SPS_CUDA(cudaMemcpyAsync(v, ds[0].V, sizeof(double) * (size_t)n * k, cudaMemcpyDeviceToHost, E.stream));

@@ -7,6 +7,7 @@ namespace la {
 
 static constexpr int FLAG_CONV = 2;
 static constexpr int FLAG_BARRIER = 4;
+static constexpr int FLAG_COPY = 8;   // a bulk-copy completion wait reached its cap
 
 __device__ __forceinline__ double wsum(double v) {
   for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);

@@ -141,6 +141,10 @@ class Engine {
   };
   std::unordered_map<std::string, std::vector<EinBlock>> ein_plans;
   size_t ein_plan_bytes = 0;
+  // arrival counters of the split-K contractions: zero between launches (the
+  // last CTA of an output tile resets its counter)
+  Buf gg_counters;
+  size_t gg_counter_slots = 0;
 
   // largest grid of a cooperative launch (0: the whole GPU); engines that run
   // concurrently on one GPU share its SMs
@@ -160,7 +164,7 @@ class Engine {
 
   // optional per-kernel timing: tic() before a launch, toc() after it; events
   // are resolved by kernel_stats() after a sync.  Off unless `profile` is set.
-  bool profile = false;
+  int profile = 0;   // 0 off, 1 per-kernel stats, 2 also per-shape contraction stats
   int tic(const char* name);
   void toc(int id, double algorithmic_flops = 0, double algorithmic_bytes = 0);
   void set_work(int id, double algorithmic_flops, double algorithmic_bytes = 0);

@@ -265,6 +265,7 @@ void Engine::reset_stats() {
 }
 
 void Engine::sync() {
+  HostTimer ht(*this, "host.sync");
   SPS_CUDA(cudaStreamSynchronize(stream));
   ring_pos = 0;
 }
@@ -281,6 +282,7 @@ void Engine::raise_flag(int h, const char* where) {
     SPS_CUDA(cudaMemsetAsync(dflag, 0, sizeof(int), stream));
     if (h & 2) throw Error(SPS_ERR_CONVERGENCE, std::string(where) + ": device iteration cap reached");
     if (h & 4) throw Error(SPS_ERR_NUMERIC, std::string(where) + ": a grid barrier wait reached its cap");
+    if (h & 8) throw Error(SPS_ERR_NUMERIC, std::string(where) + ": a bulk-copy wait reached its cap");
     throw Error(SPS_ERR_NUMERIC, std::string(where) + ": nonfinite or singular value on device");
   }
 }
@@ -336,6 +338,8 @@ struct GemmProb {
   const int64_t *ra, *ca, *rb, *cb, *rc, *cc;
   int M, N, K;
   int a_kfast, b_jfast;
+  double* ws;   // split-K partial sums, S x M x N (row-major M x N per slice)
+  int* cnt;     // split-K arrival counters, one per output tile
 };
 
 static constexpr int TM = 64, TN = 64, TK = 16, GT = 256;
@@ -348,15 +352,21 @@ __device__ __forceinline__ void dmma_f64(double& d0, double& d1, double a, doubl
 }
 
 // C_c[i, j] = alpha sum_k A[ra[i] + ca[k]] B[rb[k] + cb[j]] for the parity
-// block c = blockIdx.z, written through C's tables.  The gathered operands
+// block c = blockIdx.z / S, written through C's tables.  The gathered operands
 // are staged global -> registers -> shared memory (double-buffered, so the
 // indirect loads of the next k tile overlap the products of this one) and
 // multiplied on the FP64 tensor cores (mma.m8n8k4.f64): 8 warps as 2 (M) x
-// 4 (N), warp tile 32 x 16.
-__global__ void __launch_bounds__(GT) gemm_gather_kernel(const GemmProb* probs, double alpha) {
-  const GemmProb P = probs[blockIdx.z];
+// 4 (N), warp tile 32 x 16.  With S > 1 the contraction is split into S
+// slices (blockIdx.z % S): every slice stores its partial tile, and the last
+// CTA of a tile to arrive adds the S partials in slice order (deterministic)
+// and resets the tile's counter.
+__global__ void __launch_bounds__(GT) gemm_gather_kernel(const GemmProb* probs, double alpha, int S) {
+  const GemmProb P = probs[blockIdx.z / S];
+  const int kz = blockIdx.z % S;
   const int i0 = blockIdx.y * TM, j0 = blockIdx.x * TN;
   if (i0 >= P.M || j0 >= P.N) return;
+  const int kchunk = (((P.K + S - 1) / S + TK - 1) / TK) * TK;
+  const int kb = min(P.K, kz * kchunk), ke = min(P.K, kb + kchunk);
   __shared__ __align__(16) double As[2][TK * GALD];
   __shared__ __align__(16) double Bs[2][TK * GBLD];
   __shared__ int64_t rA[TM], cB[TN];
@@ -368,7 +378,7 @@ __global__ void __launch_bounds__(GT) gemm_gather_kernel(const GemmProb* probs, 
   auto load = [&](int k0) {
     if (P.a_kfast) {
       const int kk = t % 16;
-      const int64_t ck = (k0 + kk < P.K) ? P.ca[k0 + kk] : -1;
+      const int64_t ck = (k0 + kk < ke) ? P.ca[k0 + kk] : -1;
 #pragma unroll
       for (int r = 0; r < 4; ++r) {
         const int ii = t / 16 + 16 * r;
@@ -379,7 +389,7 @@ __global__ void __launch_bounds__(GT) gemm_gather_kernel(const GemmProb* probs, 
 #pragma unroll
       for (int r = 0; r < 4; ++r) {
         const int kk = t / 64 + 4 * r;
-        ra[r] = (k0 + kk < P.K && i0 + ii < P.M) ? P.A[rA[ii] + P.ca[k0 + kk]] : 0.0;
+        ra[r] = (k0 + kk < ke && i0 + ii < P.M) ? P.A[rA[ii] + P.ca[k0 + kk]] : 0.0;
       }
     }
     if (P.b_jfast) {
@@ -387,11 +397,11 @@ __global__ void __launch_bounds__(GT) gemm_gather_kernel(const GemmProb* probs, 
 #pragma unroll
       for (int r = 0; r < 4; ++r) {
         const int kk = t / 64 + 4 * r;
-        rb[r] = (k0 + kk < P.K && j0 + jj < P.N) ? P.B[P.rb[k0 + kk] + cB[jj]] : 0.0;
+        rb[r] = (k0 + kk < ke && j0 + jj < P.N) ? P.B[P.rb[k0 + kk] + cB[jj]] : 0.0;
       }
     } else {
       const int kk = t % 16;
-      const int64_t rk = (k0 + kk < P.K) ? P.rb[k0 + kk] : -1;
+      const int64_t rk = (k0 + kk < ke) ? P.rb[k0 + kk] : -1;
 #pragma unroll
       for (int r = 0; r < 4; ++r) {
         const int jj = t / 16 + 16 * r;
@@ -427,11 +437,11 @@ __global__ void __launch_bounds__(GT) gemm_gather_kernel(const GemmProb* probs, 
 #pragma unroll
     for (int b = 0; b < 2; ++b) acc[a][b][0] = acc[a][b][1] = 0.0;
   int buf = 0;
-  load(0);
+  load(kb);
   store(As[0], Bs[0]);
   __syncthreads();
-  for (int k0 = 0; k0 < P.K; k0 += TK) {
-    const bool more = k0 + TK < P.K;
+  for (int k0 = kb; k0 < ke; k0 += TK) {
+    const bool more = k0 + TK < ke;
     if (more) load(k0 + TK);
     const double* as = As[buf];
     const double* bs = Bs[buf];
@@ -454,19 +464,51 @@ __global__ void __launch_bounds__(GT) gemm_gather_kernel(const GemmProb* probs, 
     __syncthreads();
   }
   // accumulator fragment: row fr, columns 2 fc + {0, 1} of each 8 x 8 tile
+  if (S == 1) {
+#pragma unroll
+    for (int a = 0; a < 4; ++a) {
+      const int i = i0 + wm + a * 8 + fr;
+      if (i >= P.M) continue;
+      const int64_t ro = P.rc[i];
+#pragma unroll
+      for (int b = 0; b < 2; ++b)
+#pragma unroll
+        for (int e = 0; e < 2; ++e) {
+          const int j = j0 + wn + b * 8 + 2 * fc + e;
+          if (j < P.N) P.C[ro + P.cc[j]] = alpha * acc[a][b][e];
+        }
+    }
+    return;
+  }
+  double* part = P.ws + (size_t)kz * P.M * P.N;
 #pragma unroll
   for (int a = 0; a < 4; ++a) {
     const int i = i0 + wm + a * 8 + fr;
     if (i >= P.M) continue;
-    const int64_t ro = P.rc[i];
 #pragma unroll
     for (int b = 0; b < 2; ++b)
 #pragma unroll
       for (int e = 0; e < 2; ++e) {
         const int j = j0 + wn + b * 8 + 2 * fc + e;
-        if (j < P.N) P.C[ro + P.cc[j]] = alpha * acc[a][b][e];
+        if (j < P.N) part[(size_t)i * P.N + j] = acc[a][b][e];
       }
   }
+  __threadfence();
+  __syncthreads();
+  __shared__ int last;
+  int* cnt = P.cnt + blockIdx.y * gridDim.x + blockIdx.x;
+  if (t == 0) last = (atomicAdd(cnt, 1) == S - 1);
+  __syncthreads();
+  if (!last) return;
+  __threadfence();
+  const int mi = min(TM, P.M - i0), nj = min(TN, P.N - j0);
+  for (int e = t; e < mi * nj; e += GT) {
+    const int i = i0 + e / nj, j = j0 + e % nj;
+    double v = 0.0;
+    for (int z = 0; z < S; ++z) v += __ldcg(&P.ws[(size_t)z * P.M * P.N + (size_t)i * P.N + j]);
+    P.C[P.rc[i] + P.cc[j]] = alpha * v;
+  }
+  if (t == 0) *cnt = 0;
 }
 
 struct PermDesc {
@@ -966,6 +1008,8 @@ Tensor ein(Engine& E, const std::string& spec, const Tensor& A, const Tensor& B,
   int maxM = 0, maxN = 0;
   for (const auto& bl : it->second) {
     GemmProb P;
+    P.ws = nullptr;
+    P.cnt = nullptr;
     P.A = A.ptr();
     P.B = B.ptr();
     P.C = C.ptr();
@@ -986,17 +1030,52 @@ Tensor ein(Engine& E, const std::string& spec, const Tensor& A, const Tensor& B,
     probs.push_back(P);
   }
   if (probs.empty()) return C;
+  // split the contraction when the output tiles alone leave most SMs idle
+  // and every slice keeps at least 4 k-steps
+  const int tiles = ((maxN + TN - 1) / TN) * ((maxM + TM - 1) / TM);
+  const int nprob = (int)probs.size();
+  int maxK = 0;
+  for (auto& P : probs) maxK = std::max(maxK, P.K);
+  int S = 1;
+  if (maxK >= 8 * TK && tiles * nprob < E.num_sms)
+    S = std::min((maxK + 4 * TK - 1) / (4 * TK), (E.num_sms + tiles * nprob - 1) / (tiles * nprob));
+  Buf ws;
+  if (S > 1) {
+    size_t wsz = 0;
+    for (auto& P : probs) wsz += (size_t)S * P.M * P.N;
+    ws = E.alloc(wsz * sizeof(double));
+    const size_t slots = (size_t)tiles * nprob;
+    if (slots > E.gg_counter_slots) {   // zeroed once; the kernels leave them zero
+      E.gg_counter_slots = std::max<size_t>(slots, 4096);
+      E.gg_counters = E.alloc(E.gg_counter_slots * sizeof(int));
+      SPS_CUDA(cudaMemsetAsync(E.gg_counters->ptr, 0, E.gg_counter_slots * sizeof(int), E.stream));
+    }
+    size_t off = 0;
+    for (int p = 0; p < nprob; ++p) {
+      probs[p].ws = (double*)ws->ptr + off;
+      off += (size_t)S * probs[p].M * probs[p].N;
+      probs[p].cnt = (int*)E.gg_counters->ptr + (size_t)p * tiles;
+    }
+  }
   Buf kp = E.alloc(probs.size() * sizeof(GemmProb));
   E.stage(probs.data(), probs.size() * sizeof(GemmProb), kp->ptr);
-  dim3 grid((maxN + TN - 1) / TN, (maxM + TM - 1) / TM, (unsigned)probs.size());
+  dim3 grid((maxN + TN - 1) / TN, (maxM + TM - 1) / TM, (unsigned)(probs.size() * S));
   double fl = 0, by = 0;
   for (auto& P : probs) {
     fl += 2.0 * P.M * P.N * (double)P.K;
     by += 8.0 * ((double)P.M * P.K + (double)P.K * P.N + (double)P.M * P.N);
   }
   int tk = E.tic("gemm_gather");
-  gemm_gather_kernel<<<grid, GT, 0, E.stream>>>((const GemmProb*)kp->ptr, alpha);
+  int tshape = -1;
+  if (E.profile > 1) {
+    std::string nm = "gemm_gather " + std::to_string(maxM) + "x" + std::to_string(maxN) + "x" +
+                     std::to_string(probs[0].K) + " p" + std::to_string(nprob) + " s" + std::to_string(S) + " g" +
+                     std::to_string(grid.x * grid.y * grid.z);
+    tshape = E.tic(nm.c_str());
+  }
+  gemm_gather_kernel<<<grid, GT, 0, E.stream>>>((const GemmProb*)kp->ptr, alpha, S);
   E.toc(tk, fl, by);
+  E.toc(tshape, fl, by);
   SPS_CUDA(cudaGetLastError());
   E.launches++;
   return C;

@@ -22,6 +22,8 @@
 // uses the full SVD.  Everything is FP64.
 #include "engine.h"
 #include "coop.cuh"
+#include <cuda.h>
+#include <cudaTypedefs.h>
 #include <cfloat>
 #include <algorithm>
 #include <mutex>
@@ -37,12 +39,14 @@ constexpr int KMAXB = 80;         // largest block size b
 constexpr int RMAX = 96;          // largest number of rows owned by one CTA
 constexpr int KC = 32;            // contraction chunk of the row GEMM
 constexpr int NST = 2;            // stage budget of the row GEMM, in stages of the largest tile
+constexpr int MAXST = 8;          // most stages (and stage barriers) of the row GEMM
 constexpr int XLD = KC + 4;       // row stride of the staged operands: a fragment load is 2 wavefronts
 constexpr int STAGE = (RMAX + KMAXB) * XLD;
 constexpr int YLD = KMAXB + 1;
 constexpr int GLD = KMAXB + 1;
 constexpr int OFF_X = 0;
-constexpr int OFF_Y = OFF_X + NST * STAGE;
+constexpr int STG_PAD = 128;      // the stages start at the first 1024-byte boundary of the arena
+constexpr int OFF_Y = OFF_X + NST * STAGE + STG_PAD;
 constexpr int OFF_G = OFF_Y + RMAX * YLD;
 constexpr int OFF_V = OFF_G + KMAXB * GLD;
 constexpr int OFF_R = OFF_V + 3 * KMAXB;
@@ -53,16 +57,24 @@ static_assert(2 * KMAXB * JLD <= OFF_R, "Jacobi overlay exceeds the shared arena
 constexpr int MAXT = ((RMAX / 8) * (KMAXB / 8) + TW - 1) / TW;   // 8 x 8 output tiles per warp
 static_assert(RMAX % 8 == 0 && KMAXB % 8 == 0 && KC % 4 == 0 && XLD % 2 == 0, "tiling");
 static_assert(TT >= 256, "the 16 x 16 thread grid of the small factorizations needs 256 threads");
+static_assert(KC == 32 && MAXT <= 15, "the row GEMM's chunk is 8 k-steps; its tile dispatch covers 15 tiles per warp");
+static_assert(MAXT * TW * 64 <= NST * STAGE, "k-part partial sums exceed the staging area");
+static_assert(2 * (RMAX / 8 + KMAXB / 8) * 128 <= STAGE, "a stage of the largest tile exceeds the budget");
+static_assert(2 * (RMAX / 8 + KMAXB / 8) * 128 < 65536, "packed fragment offsets are 16-bit");
 
 enum : int { ST_OK = 0, ST_BREAKDOWN = 1, ST_JACOBI = 2, ST_NOCONV = 3, ST_ZERO = 4 };
 
 }  // namespace
 
 struct TopkProb {
+  // TMA maps of the row-GEMM operands (16 x rows boxes, 128-byte swizzle):
+  // M (box Rn rows), M^T and M M^T (box Rm rows), Q and Z (box b), Vi (box k)
+  CUtensorMap tM, tMt, tGm, tQ, tZ, tVi;
   const double* M;   // m x n, column-major, ld ldm (read-only in the kernel)
   const double* Mt;  // n x m, column-major, ld ldn (M transposed)
   int m, n, k, b, P, cta0;
-  int ldm, ldn;      // m and n rounded up to even (16-byte aligned columns)
+  int ldm, ldn;      // m and n rounded up to even (16-byte row strides)
+  int Rm, Rn;        // rows of the m- and n-sized iterates owned by one CTA (the last may own fewer)
   double* Q;     // m x b (ld ldm)
   double* Z;     // n x b (ld ldn): Omega, Z iterates, Qb
   double* Vi;    // n x k (ld ldn): right vectors
@@ -87,127 +99,224 @@ struct Ctx {
   int rm0, rm1;     // rows of m-sized iterates owned here
   int rn0, rn1;     // rows of n-sized iterates owned here
   double* sm;
+  double* stg;                 // the row GEMM's stages: 1024-byte aligned, NST * STAGE doubles
   int* flag;
   unsigned long long* trace;   // profile mode: [count, (phase, clock) ...], CTA 0 only
+  unsigned* trace_n;           // its count (shared memory)
+  unsigned long long* mbar;    // MAXST stage barriers (shared memory)
+  unsigned phase;              // bit s: parity of stage barrier s's next completion
 };
 
 // phases of the profile-mode trace (interval ending at the record)
 enum : int { PH_START = 0, PH_INIT, PH_GEMM, PH_GRAM, PH_REDUCE, PH_CHOL, PH_APPLY, PH_STORE, PH_JACOBI, PH_ROTATE,
-             PH_RESID, PH_COUNT };
+             PH_RESID, PH_GISSUE, PH_GWAIT, PH_GMMA, PH_COUNT };
 constexpr int TRACE_CAP = 2048;
 
 __device__ __forceinline__ void trace_mark(const Ctx& x, int phase) {
   if (x.trace && x.c == 0 && threadIdx.x == 0) {
-    const unsigned long long n = x.trace[0];
+    const unsigned n = *x.trace_n;
     if (n < TRACE_CAP) {
       x.trace[1 + 2 * n] = phase;
       x.trace[2 + 2 * n] = clock64();
       x.trace[0] = n + 1;
+      *x.trace_n = n + 1;
     }
   }
 }
 
-__device__ __forceinline__ void sync_group(const Ctx& x) { group_barrier(x.p->bar, (unsigned)x.p->P, x.flag); }
+// every global write before a group barrier may be read by a bulk copy after it
+__device__ __forceinline__ void sync_group(const Ctx& x) {
+  asm volatile("fence.proxy.async.global;" ::: "memory");
+  group_barrier(x.p->bar, (unsigned)x.p->P, x.flag);
+}
 
 __device__ __forceinline__ void dmma(double& d0, double& d1, double a, double b) {
-  asm volatile("mma.sync.aligned.m8n8k4.row.col.f64.f64.f64.f64 {%0,%1}, {%2}, {%3}, {%0,%1};"
+  asm("mma.sync.aligned.m8n8k4.row.col.f64.f64.f64.f64 {%0,%1}, {%2}, {%3}, {%0,%1};"
                : "+d"(d0), "+d"(d1)
                : "d"(a), "d"(b));
 }
 
-__device__ __forceinline__ void cp_async16(double* dst, const double* src, int bytes) {
-  const unsigned d = (unsigned)__cvta_generic_to_shared(dst);
-  asm volatile("cp.async.cg.shared.global [%0], [%1], 16, %2;" ::"r"(d), "l"(src), "r"(bytes) : "memory");
+__device__ __forceinline__ unsigned smem_addr(const void* p) { return (unsigned)__cvta_generic_to_shared(p); }
+
+// Stage barriers: one mbarrier per shared-memory stage, armed with the bytes
+// its bulk copies deliver, completed by the copies themselves.
+__device__ __forceinline__ void stage_expect(unsigned long long* bar, unsigned bytes) {
+  asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(smem_addr(bar)), "r"(bytes) : "memory");
 }
-__device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;" ::: "memory"); }
-template <int N>
-__device__ __forceinline__ void cp_async_wait() { asm volatile("cp.async.wait_group %0;" ::"n"(N) : "memory"); }
-// wait until at most n (0..MAXST-2) copy groups of this thread are pending
-constexpr int MAXST = 8;
-__device__ __forceinline__ void cp_async_wait_n(int n) {
-  switch (n) {
-    case 0: cp_async_wait<0>(); break;
-    case 1: cp_async_wait<1>(); break;
-    case 2: cp_async_wait<2>(); break;
-    case 3: cp_async_wait<3>(); break;
-    case 4: cp_async_wait<4>(); break;
-    case 5: cp_async_wait<5>(); break;
-    default: cp_async_wait<6>(); break;
+// one 16 x rows box of a row-major view (x0: first element of the row, even;
+// y0: first row); elements outside the matrix arrive as zeros
+__device__ __forceinline__ void tma_load(double* dst, const CUtensorMap* map, int x0, int y0, unsigned long long* bar) {
+  asm volatile(
+      "cp.async.bulk.tensor.2d.shared::cluster.global.tile.mbarrier::complete_tx::bytes [%0], [%1, {%2, %3}], [%4];" ::"r"(
+          smem_addr(dst)),
+      "l"(reinterpret_cast<unsigned long long>(map)), "r"(x0), "r"(y0), "r"(smem_addr(bar))
+      : "memory");
+}
+__device__ __forceinline__ bool stage_try(unsigned long long* bar, unsigned parity) {
+  unsigned ok;
+  asm volatile(
+      "{\n .reg .pred p;\n mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n selp.u32 %0, 1, 0, p;\n}"
+      : "=r"(ok)
+      : "r"(smem_addr(bar)), "r"(parity)
+      : "memory");
+  return ok != 0;
+}
+// bounded: after the cap the copy flag is raised and the data is not trusted
+__device__ __forceinline__ void stage_wait(const Ctx& x, unsigned long long* bar, unsigned parity) {
+  long long spins = 0;
+  while (!stage_try(bar, parity))
+    if (++spins > (1ll << 24)) {
+      if (threadIdx.x == 0) atomicOr(x.flag, FLAG_COPY);
+      break;
+    }
+}
+// orders this thread's generic-proxy shared-memory accesses before later TMA
+// writes to the same bytes (async proxy)
+__device__ __forceinline__ void proxy_fence() { asm volatile("fence.proxy.async.shared::cta;" ::: "memory"); }
+
+// NQ output tiles of this warp over KSN k-steps of one staged chunk.  A
+// staged operand row is 16 doubles (128 bytes) per half-chunk, its 16-byte
+// pieces permuted by the 128-byte swizzle: piece u of row r sits at u ^ (r % 8).
+// off[q] packs the fragment offsets of item q: X row in the low 16 bits, S
+// row in the high 16 bits (doubles from the stage start).
+template <int NQ, int KSN>
+__device__ __forceinline__ void mma_chunk(double (&acc)[MAXT][2], const double* st, const unsigned (&off)[MAXT],
+                                          const int (&cx)[4], int hx, int hs) {
+#pragma unroll
+  for (int ks = 0; ks < KSN; ++ks) {
+    const int h = ks >> 2;
+#pragma unroll
+    for (int q = 0; q < NQ; ++q)
+      dmma(acc[q][0], acc[q][1], st[(off[q] & 0xffffu) + h * hx + cx[ks & 3]],
+           st[(off[q] >> 16) + h * hs + cx[ks & 3]]);
   }
 }
 
-// Ys[r][j] = sum_t X[(r0+r)*ldx + t] * S[j*lds + t]   (r < r1-r0, j < bb, t < K)
-// on the FP64 tensor cores: each warp owns whole 8 x 8 output tiles and runs
-// mma.m8n8k4 over the contraction.  Operands stream through shared-memory
-// stages sized to the tile (as many as fit, up to MAXST) by asynchronous
-// 16-byte copies that bypass L1 (S is written by other CTAs of the launch),
-// contraction index contiguous as in global memory.
-// Requires ldx, lds even and X, S 16-byte aligned.
-__device__ __noinline__ void gemm_rows(const Ctx& x, const double* __restrict__ X, int ldx, int K, const double* S,
-                                       int lds, int bb, int r0, int r1) {
+// Ys[r][j] = sum_t X[r0 + r][t] * S[j][t]   (r < r1 - r0, j < bb, t < K), X
+// and S row-major views given by their TMA maps (boxes of 16 x rbox and
+// 16 x bb), on the FP64 tensor cores.  Chunks of 32 along t stream through as
+// many shared-memory stages as fit (up to MAXST): lane 0 of warps 4-7 issues
+// one box load each per chunk (two halves of X and of S), completing on the
+// stage's mbarrier (warp 4 arms it with the chunk's byte count; a load that
+// lands first leaves the count negative, and the phase cannot complete before
+// that single arrival); rows and columns past the matrices arrive as zeros.  Work items
+// are (8 x 8 output tile, half of the chunk's k-steps) when splitting the
+// k-steps evens out the warps' tile counts; the halves are then added in a
+// fixed order at the end.
+__device__ __noinline__ void gemm_rows(Ctx& x, const CUtensorMap* tX, int rbox, const CUtensorMap* tS, int bb, int K,
+                                       int r0, int r1) {
   double* Ys = x.sm + OFF_Y;
   const int R = r1 - r0;
-  const int mt = (R + 7) / 8, nt = (bb + 7) / 8, ntiles = mt * nt;
-  constexpr int HC = KC / 2;   // 16-byte copies per staged row
-  const int nX = mt * 8 * HC, nS = nt * 8 * HC;
+  const int mt = (rbox + 7) / 8, nt = (bb + 7) / 8, ntiles = mt * nt;
+  const int per1 = (ntiles + TW - 1) / TW, per2 = (2 * ntiles + TW - 1) / TW;
+  const int parts = (per2 <= MAXT && per2 * 4 < per1 * 8) ? 2 : 1;
+  const int items = ntiles * parts;
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31, fr = lane >> 2, fc = lane & 3;
+  const int nq = warp < items ? (items - warp + TW - 1) / TW : 0;
+  const int hx = mt * 128, hs = nt * 128;   // doubles of one half-chunk region of X and of S
+  const int stage = 2 * (hx + hs);
+  int cx[4];
+#pragma unroll
+  for (int u = 0; u < 4; ++u) cx[u] = ((((u << 1) | (fc >> 1)) ^ fr) << 1) | (fc & 1);
   double acc[MAXT][2];
-  int aoff[MAXT], boff[MAXT];
+  unsigned off[MAXT];
 #pragma unroll
   for (int q = 0; q < MAXT; ++q) {
     acc[q][0] = acc[q][1] = 0.0;
-    const int tile = warp + q * TW;
-    aoff[q] = tile < ntiles ? ((tile / nt) * 8 + fr) * XLD + fc : -1;
-    boff[q] = tile < ntiles ? (mt * 8 + (tile % nt) * 8 + fr) * XLD + fc : 0;
+    const int item = warp + q * TW;
+    const int tile = item % ntiles, part = item / ntiles;
+    const unsigned ao = q < nq ? part * hx + ((tile / nt) * 8 + fr) * 16 : 0;
+    const unsigned bo = q < nq ? 2 * hx + part * hs + ((tile % nt) * 8 + fr) * 16 : 0;
+    off[q] = ao | (bo << 16);
   }
-  const int stage = (mt + nt) * 8 * XLD;
   const int nst = max(2, min(MAXST, (NST * STAGE) / stage));
+  const int nch = (K + KC - 1) / KC;
+  const unsigned bytes = 2u * 128u * (unsigned)(rbox + bb);
+  const int role = (lane == 0 && warp >= TW - 4) ? warp - (TW - 4) : -1;   // which of the four boxes
   auto issue = [&](int c) {
-    double* st = x.sm + OFF_X + (c % nst) * stage;
+    double* st = x.stg + (c % nst) * stage;
+    unsigned long long* bar = x.mbar + (c % nst);
     const int t0 = c * KC;
-    for (int e = threadIdx.x; e < nX; e += TT) {
-      const int r = e / HC, t = (e % HC) * 2;
-      const int bytes = (r < R) ? 8 * max(0, min(2, K - t0 - t)) : 0;
-      cp_async16(st + r * XLD + t, bytes ? X + (size_t)(r0 + r) * ldx + t0 + t : X, bytes);
-    }
-    for (int e = threadIdx.x; e < nS; e += TT) {
-      const int j = e / HC, t = (e % HC) * 2;
-      const int bytes = (j < bb) ? 8 * max(0, min(2, K - t0 - t)) : 0;
-      cp_async16(st + (mt * 8 + j) * XLD + t, bytes ? S + (size_t)j * lds + t0 + t : S, bytes);
+    if (role == 0) {
+      stage_expect(bar, bytes);
+      tma_load(st, tX, t0, r0, bar);
+    } else if (role == 1) {
+      tma_load(st + hx, tX, t0 + 16, r0, bar);
+    } else if (role == 2) {
+      tma_load(st + 2 * hx, tS, t0, 0, bar);
+    } else {
+      tma_load(st + 2 * hx + hs, tS, t0 + 16, 0, bar);
     }
   };
-  const int nch = (K + KC - 1) / KC;
+  proxy_fence();
   __syncthreads();   // the stages may still be read by the previous phase
-  for (int c = 0; c < nst - 1; ++c) {
-    if (c < nch) issue(c);
-    cp_async_commit();
-  }
+  if (role >= 0)
+    for (int c = 0; c < nst - 1 && c < nch; ++c) issue(c);
+  trace_mark(x, PH_GISSUE);
   for (int c = 0; c < nch; ++c) {
-    cp_async_wait_n(nst - 2);
-    __syncthreads();
-    if (c + nst - 1 < nch) issue(c + nst - 1);
-    cp_async_commit();
-    const double* st = x.sm + OFF_X + (c % nst) * stage;
-    const int ksteps = (min(KC, K - c * KC) + 3) / 4;
-    for (int ks = 0; ks < ksteps; ++ks) {
-#pragma unroll
-      for (int q = 0; q < MAXT; ++q) {
-        if (aoff[q] < 0) continue;
-        dmma(acc[q][0], acc[q][1], st[aoff[q] + 4 * ks], st[boff[q] + 4 * ks]);
+    stage_wait(x, x.mbar + (c % nst), (x.phase >> (c % nst)) & 1u);
+    x.phase ^= 1u << (c % nst);
+    __syncthreads();   // every warp is done with chunk c - 1: its stage is free
+    trace_mark(x, PH_GWAIT);
+    if (role >= 0 && c + nst - 1 < nch) issue(c + nst - 1);
+    const double* st = x.stg + (c % nst) * stage;
+    if (parts == 1) {
+      switch (nq) {
+#define SPS_TOPK_MMA(N) \
+  case N:               \
+    mma_chunk<N, 8>(acc, st, off, cx, hx, hs); \
+    break;
+        SPS_TOPK_MMA(1) SPS_TOPK_MMA(2) SPS_TOPK_MMA(3) SPS_TOPK_MMA(4) SPS_TOPK_MMA(5)
+        SPS_TOPK_MMA(6) SPS_TOPK_MMA(7) SPS_TOPK_MMA(8) SPS_TOPK_MMA(9) SPS_TOPK_MMA(10)
+        SPS_TOPK_MMA(11) SPS_TOPK_MMA(12) SPS_TOPK_MMA(13) SPS_TOPK_MMA(14) SPS_TOPK_MMA(15)
+#undef SPS_TOPK_MMA
+        default:
+          break;
+      }
+    } else {
+      switch (nq) {
+#define SPS_TOPK_MMA(N) \
+  case N:               \
+    mma_chunk<N, 4>(acc, st, off, cx, hx, hs); \
+    break;
+        SPS_TOPK_MMA(1) SPS_TOPK_MMA(2) SPS_TOPK_MMA(3) SPS_TOPK_MMA(4) SPS_TOPK_MMA(5)
+        SPS_TOPK_MMA(6) SPS_TOPK_MMA(7) SPS_TOPK_MMA(8) SPS_TOPK_MMA(9) SPS_TOPK_MMA(10)
+        SPS_TOPK_MMA(11) SPS_TOPK_MMA(12) SPS_TOPK_MMA(13) SPS_TOPK_MMA(14) SPS_TOPK_MMA(15)
+#undef SPS_TOPK_MMA
+        default:
+          break;
       }
     }
+    trace_mark(x, PH_GMMA);
   }
-  cp_async_wait<0>();
-  __syncthreads();
+  __syncthreads();   // the stages are free: partial sums of the halves go there
   // accumulator fragment: row fr, columns 2 fc + {0, 1} of the tile
+  if (parts == 1) {
 #pragma unroll
-  for (int q = 0; q < MAXT; ++q) {
-    const int tile = warp + q * TW;
-    if (tile >= ntiles) continue;
-    const int r = (tile / nt) * 8 + fr, j = (tile % nt) * 8 + 2 * fc;
-    if (r < R) {
-      if (j < bb) Ys[r * YLD + j] = acc[q][0];
-      if (j + 1 < bb) Ys[r * YLD + j + 1] = acc[q][1];
+    for (int q = 0; q < MAXT; ++q) {
+      if (q >= nq) break;
+      const int tile = warp + q * TW;
+      const int r = (tile / nt) * 8 + fr, j = (tile % nt) * 8 + 2 * fc;
+      if (r < R) {
+        if (j < bb) Ys[r * YLD + j] = acc[q][0];
+        if (j + 1 < bb) Ys[r * YLD + j + 1] = acc[q][1];
+      }
+    }
+  } else {
+    double* part = x.stg;   // [item][64]
+#pragma unroll
+    for (int q = 0; q < MAXT; ++q) {
+      if (q >= nq) break;
+      const int item = warp + q * TW;
+      part[item * 64 + fr * 8 + 2 * fc] = acc[q][0];
+      part[item * 64 + fr * 8 + 2 * fc + 1] = acc[q][1];
+    }
+    __syncthreads();
+    for (int e = threadIdx.x; e < ntiles * 64; e += TT) {
+      const int tile = e >> 6, w = e & 63;
+      const int r = (tile / nt) * 8 + (w >> 3), j = (tile % nt) * 8 + (w & 7);
+      const double v = part[tile * 64 + w] + part[(ntiles + tile) * 64 + w];
+      if (r < R && j < bb) Ys[r * YLD + j] = v;
     }
   }
   __syncthreads();
@@ -493,7 +602,9 @@ __device__ __forceinline__ double omega(unsigned long long i) {
 
 __global__ void __launch_bounds__(TT, 1) topk_kernel(const TopkProb* __restrict__ probs, int nprob, int q0, int qstep,
                                                   int qmax, double tol, int* flag, unsigned long long* trace) {
-  extern __shared__ double sm[];
+  extern __shared__ __align__(128) double sm[];
+  __shared__ unsigned long long stage_bar[MAXST];
+  __shared__ unsigned trace_count;
   int pi = -1;
   for (int q = 0; q < nprob; ++q)
     if ((int)blockIdx.x >= probs[q].cta0 && (int)blockIdx.x < probs[q].cta0 + probs[q].P) pi = q;
@@ -505,12 +616,29 @@ __global__ void __launch_bounds__(TT, 1) topk_kernel(const TopkProb* __restrict_
   x.sm = sm;
   x.flag = flag;
   x.trace = (pi == 0) ? trace : nullptr;
+  x.mbar = stage_bar;
+  x.phase = 0;
+  x.trace_n = &trace_count;
+  x.stg = sm + ((1024u - (smem_addr(sm) & 1023u)) & 1023u) / sizeof(double);
+  if (threadIdx.x == 0) {
+    // the maps were written through the generic proxy (a host copy into
+    // pooled memory that earlier launches may have used for other maps)
+    const CUtensorMap* maps[6] = {&p.tM, &p.tMt, &p.tGm, &p.tQ, &p.tZ, &p.tVi};
+    for (int i = 0; i < 6; ++i) {
+      asm volatile("fence.proxy.tensormap::generic.acquire.gpu [%0], 128;" ::"l"(maps[i]) : "memory");
+      asm volatile("prefetch.tensormap [%0];" ::"l"(maps[i]) : "memory");
+    }
+    trace_count = 0;
+    for (int st = 0; st < MAXST; ++st)
+      asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(smem_addr(stage_bar + st)) : "memory");
+    asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+  }
+  __syncthreads();
   trace_mark(x, PH_START);
-  const int Rm = (p.m + p.P - 1) / p.P, Rn = (p.n + p.P - 1) / p.P;
-  x.rm0 = min(p.m, x.c * Rm);
-  x.rm1 = min(p.m, x.rm0 + Rm);
-  x.rn0 = min(p.n, x.c * Rn);
-  x.rn1 = min(p.n, x.rn0 + Rn);
+  x.rm0 = min(p.m, x.c * p.Rm);
+  x.rm1 = min(p.m, x.rm0 + p.Rm);
+  x.rn0 = min(p.n, x.c * p.Rn);
+  x.rn1 = min(p.n, x.rn0 + p.Rn);
   const int b = p.b, k = p.k;
   double* red = sm + OFF_R;
 
@@ -543,7 +671,7 @@ __global__ void __launch_bounds__(TT, 1) topk_kernel(const TopkProb* __restrict_
     for (int q = 0; q < p.P; ++q) s += __ldcg(&p.fpart[q]);
     p.info[2] = s;
   }
-  gemm_rows(x, p.Mt, p.ldn, p.n, p.Z, p.ldn, b, x.rm0, x.rm1);
+  gemm_rows(x, &p.tMt, p.Rm, &p.tZ, b, p.n, x.rm0, x.rm1);
   trace_mark(x, PH_GEMM);
   if (!orth_pass(x, b, x.rm0, x.rm1, p.m, true, 0)) return;
   store_rows(x, p.Q, p.ldm, b, x.rm0, x.rm1);
@@ -553,7 +681,7 @@ __global__ void __launch_bounds__(TT, 1) topk_kernel(const TopkProb* __restrict_
   int it = 0, target = q0;
   for (;;) {
     for (; it < target && p.Gm; ++it) {   // Gram iteration: Q = orth(M M^T Q)
-      gemm_rows(x, p.Gm, p.ldm, p.m, p.Q, p.ldm, b, x.rm0, x.rm1);
+      gemm_rows(x, &p.tGm, p.Rm, &p.tQ, b, p.m, x.rm0, x.rm1);
       trace_mark(x, PH_GEMM);
       if (!orth_pass(x, b, x.rm0, x.rm1, p.m, true, 0)) return;
       store_rows(x, p.Q, p.ldm, b, x.rm0, x.rm1);
@@ -561,13 +689,13 @@ __global__ void __launch_bounds__(TT, 1) topk_kernel(const TopkProb* __restrict_
       trace_mark(x, PH_STORE);
     }
     for (; it < target; ++it) {
-      gemm_rows(x, p.M, p.ldm, p.m, p.Q, p.ldm, b, x.rn0, x.rn1);
+      gemm_rows(x, &p.tM, p.Rn, &p.tQ, b, p.m, x.rn0, x.rn1);
       trace_mark(x, PH_GEMM);
       if (!orth_pass(x, b, x.rn0, x.rn1, p.n, true, 0)) return;
       store_rows(x, p.Z, p.ldn, b, x.rn0, x.rn1);
       sync_group(x);
       trace_mark(x, PH_STORE);
-      gemm_rows(x, p.Mt, p.ldn, p.n, p.Z, p.ldn, b, x.rm0, x.rm1);
+      gemm_rows(x, &p.tMt, p.Rm, &p.tZ, b, p.n, x.rm0, x.rm1);
       trace_mark(x, PH_GEMM);
       if (!orth_pass(x, b, x.rm0, x.rm1, p.m, true, 0)) return;
       store_rows(x, p.Q, p.ldm, b, x.rm0, x.rm1);
@@ -580,7 +708,7 @@ __global__ void __launch_bounds__(TT, 1) topk_kernel(const TopkProb* __restrict_
     store_rows(x, p.Q, p.ldm, b, x.rm0, x.rm1);
     sync_group(x);
     trace_mark(x, PH_STORE);
-    gemm_rows(x, p.M, p.ldm, p.m, p.Q, p.ldm, b, x.rn0, x.rn1);
+    gemm_rows(x, &p.tM, p.Rn, &p.tQ, b, p.m, x.rn0, x.rn1);
     trace_mark(x, PH_GEMM);
     if (!orth_pass(x, b, x.rn0, x.rn1, p.n, true, 1)) return;
     if (!orth_pass(x, b, x.rn0, x.rn1, p.n, false, 2)) return;
@@ -597,7 +725,7 @@ __global__ void __launch_bounds__(TT, 1) topk_kernel(const TopkProb* __restrict_
     sync_group(x);
     trace_mark(x, PH_ROTATE);
     // residuals ||M v_i - s_i u_i||^2, partial over the owned m-rows
-    gemm_rows(x, p.Mt, p.ldn, p.n, p.Vi, p.ldn, k, x.rm0, x.rm1);
+    gemm_rows(x, &p.tMt, p.Rm, &p.tVi, k, p.n, x.rm0, x.rm1);
     trace_mark(x, PH_GEMM);
     {
       const double* Ys = sm + OFF_Y;
@@ -660,6 +788,36 @@ __global__ void __launch_bounds__(TT, 1) topk_kernel(const TopkProb* __restrict_
 // host driver
 // ---------------------------------------------------------------------------
 
+namespace {
+
+PFN_cuTensorMapEncodeTiled_v12000 encode_fn() {
+  static PFN_cuTensorMapEncodeTiled_v12000 fn = nullptr;
+  static std::once_flag once;
+  std::call_once(once, [] {
+    void* f = nullptr;
+    cudaDriverEntryPointQueryResult q = cudaDriverEntryPointSymbolNotFound;
+    SPS_CUDA(cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &f, cudaEnableDefault, &q));
+    if (q != cudaDriverEntryPointSuccess || !f) throw Error(SPS_ERR_CUDA, "cuTensorMapEncodeTiled is not available");
+    fn = reinterpret_cast<PFN_cuTensorMapEncodeTiled_v12000>(f);
+  });
+  return fn;
+}
+
+// TMA map of a matrix seen as `rows` rows of `len` contiguous doubles, row
+// stride ld (even); boxes of 16 x box_rows, 128-byte swizzle, zero fill
+void encode_rows(CUtensorMap* map, const double* base, int len, int rows, int ld, int box_rows) {
+  const cuuint64_t dims[2] = {(cuuint64_t)len, (cuuint64_t)rows};
+  const cuuint64_t strides[1] = {(cuuint64_t)ld * sizeof(double)};
+  const cuuint32_t box[2] = {16u, (cuuint32_t)box_rows};
+  const cuuint32_t es[2] = {1u, 1u};
+  const CUresult r = encode_fn()(map, CU_TENSOR_MAP_DATA_TYPE_FLOAT64, 2, const_cast<double*>(base), dims, strides, box,
+                                 es, CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_128B,
+                                 CU_TENSOR_MAP_L2_PROMOTION_L2_256B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
+  if (r != CUDA_SUCCESS) throw Error(SPS_ERR_CUDA, "cuTensorMapEncodeTiled failed (" + std::to_string((int)r) + ")");
+}
+
+}  // namespace
+
 int topk_block_size(int k, int m, int n) {
   int b = k + std::max(16, std::min(k, 32));
   b = std::min(b, KMAXB);
@@ -706,8 +864,8 @@ void svd_topk(Engine& E, std::vector<TopkDesc>& ds, double tol) {
       throw Error(SPS_ERR_ARGUMENT, "svd_topk: block too large for the grid");
     const int b = d.b;
     const int ldm = m + (m & 1), ldn = n + (n & 1);
-    // every buffer read by the asynchronous copies has an even length, so all
-    // of them start 16-byte aligned
+    // even leading dimensions: the TMA maps' row strides are multiples of 16
+    // bytes and every buffer starts 16-byte aligned
     const size_t nd = (size_t)ldn * m + (size_t)ldm * b + (size_t)ldn * b + (size_t)ldn * d.k +
                       (d.gram ? (size_t)ldm * m : 0) +
                       ((m & 1) ? (size_t)ldm * n : 0) + (size_t)P * KMAXB * KMAXB + 4 * (size_t)b * b + b + P + 8;
@@ -732,7 +890,7 @@ void svd_topk(Engine& E, std::vector<TopkDesc>& ds, double tol) {
     p.Z = base;
     base += (size_t)ldn * b;
     // right vectors straight into the caller's buffer when its layout suits
-    // the asynchronous copies (even n, 16-byte aligned), else via Vi
+    // the TMA maps (even n, 16-byte aligned), else via Vi
     if (ldn == n && reinterpret_cast<uintptr_t>(d.V) % 16 == 0) {
       p.Vi = d.V;
     } else {
@@ -772,6 +930,14 @@ void svd_topk(Engine& E, std::vector<TopkDesc>& ds, double tol) {
     base += 6;
     p.bar = (unsigned*)(base);
     p.U = d.U;
+    p.Rm = (m + P - 1) / P;
+    p.Rn = (n + P - 1) / P;
+    encode_rows(&p.tM, p.M, m, n, ldm, p.Rn);
+    encode_rows(&p.tMt, p.Mt, n, m, ldn, p.Rm);
+    if (g) encode_rows(&p.tGm, g, m, m, ldm, p.Rm);
+    encode_rows(&p.tQ, p.Q, m, b, ldm, b);
+    encode_rows(&p.tZ, p.Z, n, b, ldn, b);
+    encode_rows(&p.tVi, p.Vi, n, d.k, ldn, d.k);
     SPS_CUDA(cudaMemsetAsync(p.info, 0, sizeof(double) * 6 + 8, E.stream));
     transpose_cm(E, d.M, m, n, m, mt, ldn);
     if (g) dgemm_cm(E, false, m, m, n, 1.0, p.M, ldm, mt, ldn, 0.0, g, ldm);   // G = M M^T
@@ -833,8 +999,9 @@ void svd_topk(Engine& E, std::vector<TopkDesc>& ds, double tol) {
     SPS_CUDA(cudaMemcpy(h.data(), trace, sizeof(unsigned long long) * h.size(), cudaMemcpyDeviceToHost));
     int khz = 0;
     SPS_CUDA(cudaDeviceGetAttribute(&khz, cudaDevAttrClockRate, E.device));
-    static const char* names[PH_COUNT] = {"start", "init", "gemm", "gram", "reduce", "cholesky",
-                                          "apply", "store", "jacobi", "rotate", "residual"};
+    static const char* names[PH_COUNT] = {"start",  "init",   "gemm",     "gram",       "reduce",
+                                          "cholesky", "apply", "store",   "jacobi",     "rotate",
+                                          "residual", "gemm_issue", "gemm_wait", "gemm_mma"};
     const unsigned long long n = std::min<unsigned long long>(h[0], TRACE_CAP);
     for (unsigned long long i = 1; i < n; ++i) {
       const int ph = (int)h[1 + 2 * i];

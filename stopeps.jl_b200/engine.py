@@ -79,8 +79,13 @@ class Engine:
         """How many samples ``sample_batch`` draws at the same time (own stream and workspace each)."""
         self.check(self.lib.sps_set_concurrency(self.h, int(samples)))
 
-    def set_profile(self, enable: bool):
-        self.check(self.lib.sps_set_profile(self.h, 1 if enable else 0))
+    def set_sm_share(self, ctas: int):
+        """Cap this handle's own cooperative launches at ``ctas`` CTAs each (0: the whole GPU)."""
+        self.check(self.lib.sps_set_sm_share(self.h, int(ctas)))
+
+    def set_profile(self, enable):
+        """0/False off, 1/True per-kernel stats, 2 also per-shape contraction stats (resets the stats)."""
+        self.check(self.lib.sps_set_profile(self.h, int(enable)))
 
     def kernel_stats(self) -> dict:
         import json
@@ -136,8 +141,11 @@ class Engine:
                                         _arr(b, C.c_double), float(beta), _arr(c, C.c_double), C.byref(ms)))
         return c, ms.value
 
-    def la_svd_topk(self, a, k):
-        """Leading k singular triplets by subspace iteration: (u, s, v, iterations, device_ms)."""
+    def la_svd_topk(self, a, k, gram=False, rtol=0.0):
+        """Leading k singular triplets by subspace iteration: (u, s, v, iterations, device_ms).
+
+        ``gram`` iterates on a a^T; ``rtol`` is the residual bound relative to
+        the largest singular value (0: rounding level, 5e-14)."""
         a = np.asfortranarray(np.asarray(a, np.float64))
         m, n = a.shape
         u = np.zeros((m, k), order="F")
@@ -145,8 +153,9 @@ class Engine:
         s = np.zeros(k)
         it = C.c_int32()
         ms = C.c_double()
-        self.check(self.lib.sps_la_svd_topk(self.h, m, n, k, _arr(a, C.c_double), _arr(u, C.c_double),
-                                            _arr(s, C.c_double), _arr(v, C.c_double), C.byref(it), C.byref(ms)))
+        self.check(self.lib.sps_la_svd_topk(self.h, m, n, k, _arr(a, C.c_double), int(bool(gram)), float(rtol),
+                                            _arr(u, C.c_double), _arr(s, C.c_double), _arr(v, C.c_double),
+                                            C.byref(it), C.byref(ms)))
         return u, s, v, it.value, ms.value
 
     def la_qr(self, a):

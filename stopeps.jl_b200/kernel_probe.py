@@ -2,7 +2,7 @@
 
   python stopeps.jl_b200/kernel_probe.py svd_left   # U-only Jacobi of a 648x648 LQ-preconditioned block
   python stopeps.jl_b200/kernel_probe.py qr          # blocked Householder QR of a 23328x648 block
-  python stopeps.jl_b200/kernel_probe.py topk        # leading 18 triplets of a 648x648 graded block
+  python stopeps.jl_b200/kernel_probe.py topk [W] [gram]  # leading 18 triplets of a 648x648 graded block (1/W of the SMs)
   python stopeps.jl_b200/kernel_probe.py gemm        # FP64 GEMM 23328x648x648 and the 648x648x23328 Gram
   python stopeps.jl_b200/kernel_probe.py draw        # one Born draw, 8x8 D=6 chi=36 (synthetic PEPO)
   python stopeps.jl_b200/kernel_probe.py zipdraw     # the same draw with the zip-up absorption
@@ -44,11 +44,16 @@ def main(which):
         print(f"svd_left 648x648: {ms:.2f} ms, {sweeps} sweeps")
     elif which == "topk":
         e = sps.Engine(2, 2)
+        w = int(sys.argv[2]) if len(sys.argv) > 2 else 1
+        gram = len(sys.argv) > 3 and sys.argv[3] == "gram"
+        import torch
+        sms = torch.cuda.get_device_properties(0).multi_processor_count
+        e.set_sm_share(sms // w if w > 1 else 0)   # the launch's share of the SMs: 1/w
         a = graded(648, 648, 0.1, 5)
-        u, s, v, iters, ms = e.la_svd_topk(a, 18)
+        u, s, v, iters, ms = e.la_svd_topk(a, 18, gram=gram, rtol=1e-10 if gram else 0.0)
         e.set_profile(True)
-        u, s, v, iters, ms = e.la_svd_topk(a, 18)
-        print(f"topk 648x648 k=18: {ms:.3f} ms, {iters} iterations")
+        u, s, v, iters, ms = e.la_svd_topk(a, 18, gram=gram, rtol=1e-10 if gram else 0.0)
+        print(f"topk 648x648 k=18 (SM share 1/{w}{', gram' if gram else ''}): {ms:.3f} ms, {iters} iterations")
         for name, st in sorted(e.kernel_stats().items()):
             print(f"  {name:24s} {st['ms']:9.3f} ms  x{st['count']}")
     elif which == "gemm":
@@ -75,9 +80,20 @@ def main(which):
         sps.normalize_state(st)
         kind = sps.BoundaryMPS if which == "draw" else sps.BoundaryMPSZipUp
         cache = sps.SamplingCache(st, kind(36, sps.Z2Space(18, 18)))
+        import time
         for i in range(2):
+            if i == 1:
+                e.set_profile(2)
+                t0 = time.perf_counter()
             d = sps.sample_configuration(cache, uniforms=sps.sample_uniforms(1, i + 1, 64))
-        print("draw log_probability", d["log_probability"])
+        wall = (time.perf_counter() - t0) * 1e3
+        stats = e.kernel_stats()
+        e.set_profile(False)
+        dev = sum(v["ms"] for k, v in stats.items() if not k.startswith(("host.", "svd_topk.", "gemm_gather ")))
+        print(f"draw log_probability {d['log_probability']}: wall {wall:.1f} ms (profiled), kernels {dev:.1f} ms")
+        for name, v in sorted(stats.items(), key=lambda kv: -kv[1]["ms"])[:60]:
+            tf = v["flops"] / v["ms"] / 1e9 if v["ms"] > 0 else 0.0
+            print(f"  {name:40s} {v['ms']:9.3f} ms  x{v['count']:<5d} {tf:6.2f} TF/s")
     elif which == "scale":
         import time
         L, Dd, chi = 12, 8, 64

@@ -65,7 +65,8 @@ def test_left_jacobi_matches_lapack(eng, m, n):
 
 @pytest.mark.parametrize("m,n,k,decay", [(648, 648, 18, 0.1), (648, 648, 36, 0.1), (648, 648, 18, 0.03),
                                          (1296, 648, 18, 0.08), (500, 900, 30, 0.06), (128, 128, 8, 0.2),
-                                         (2048, 2048, 32, 0.05)])
+                                         (2048, 2048, 32, 0.05), (333, 517, 12, 0.08), (646, 650, 18, 0.1),
+                                         (101, 97, 4, 0.3)])
 def test_topk_matches_lapack(eng, m, n, k, decay):
     """Leading singular triplets by block subspace iteration (truncated boundary SVD)."""
     a = graded(m, n, decay, 5 * m + n + k)
@@ -80,6 +81,22 @@ def test_topk_matches_lapack(eng, m, n, k, decay):
     assert np.linalg.norm(mine - ref) <= 1e-12 * ref_s[0]
     np.testing.assert_allclose(a @ v, u * s, atol=1e-12 * ref_s[0])
     assert 1 <= iters <= 48
+
+
+@pytest.mark.parametrize("m,n,k,decay", [(648, 648, 18, 0.1), (1296, 1296, 36, 0.06), (646, 650, 18, 0.1),
+                                         (333, 517, 12, 0.08), (518, 341, 20, 0.05)])
+def test_topk_gram_mode_matches_lapack(eng, m, n, k, decay):
+    """The zip-up splits' mode: iterate on a a^T, extract and test residuals on a (1e-10 relative)."""
+    a = graded(m, n, decay, 11 * m + n + k)
+    u, s, v, iters, ms = eng.la_svd_topk(a, k, gram=True, rtol=1e-10)
+    ref_u, ref_s, _ = np.linalg.svd(a, full_matrices=False)
+    np.testing.assert_allclose(s, ref_s[:k], rtol=1e-10, atol=2e-10 * ref_s[0])
+    np.testing.assert_allclose(u.T @ u, np.eye(k), atol=1e-10)
+    np.testing.assert_allclose(v.T @ v, np.eye(k), atol=1e-10)
+    assert np.linalg.norm(a @ v - u * s, axis=0).max() <= 1e-10 * ref_s[0] * (1 + 1e-6)
+    mine = u @ (u.T @ a)
+    ref = ref_u[:, :k] @ (ref_u[:, :k].T @ a)
+    assert np.linalg.norm(mine - ref) <= 5e-8 * ref_s[0]
 
 
 @pytest.mark.parametrize("ta", [False, True])
