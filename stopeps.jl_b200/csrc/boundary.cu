@@ -297,11 +297,15 @@ Envs boundary_environments(Engine& E, const std::vector<Tensor>& layers, int Lx,
 // _left_step / _right_step, plain and slab (boundary_mps.jl:216-246)
 // X (w, b, n, c) contracted over (w, n) with double_layer(ket, ket): the
 // (b, c, e, s) of ein("wbnc,wnes->bces", X, E) in two single-layer steps,
-// ket then bra (2 chi^2 D^6 P A flops each instead of 2 chi^2 D^8).
+// ket then bra (2 chi^2 D^6 P A flops each instead of 2 chi^2 D^8): one fused
+// kernel when its shared-memory tiles fit, else two table-driven contractions.
 Tensor layer_apply_wn(Engine& E, const Tensor& X, const Tensor& ket) {
   Tensor X5 = split(E, split(E, X, 2, {ket.legs[1], ket.legs[1]}), 0, {ket.legs[0], ket.legs[0]});   // w1 w2 b n1 n2 c
-  Tensor Y = ein(E, "xybuvc,xupaef->ybvcpaef", X5, ket);
-  Tensor Z = ein(E, "ybvcpaef,yvpagh->bcegfh", Y, ket);
+  Tensor Z;
+  if (!layer_wn_fused(E, X5, ket, Z)) {
+    Tensor Y = ein(E, "xybuvc,xupaef->ybvcpaef", X5, ket);
+    Z = ein(E, "ybvcpaef,yvpagh->bcegfh", Y, ket);
+  }
   return fuse(E, fuse(E, Z, 4, 2), 2, 2);
 }
 

@@ -80,6 +80,10 @@ Envs boundary_environments(Engine& E, const std::vector<Tensor>& layers, int Lx,
                            int side /*0 both,1 north,2 south*/, Entropy* ent);
 // X (w, b, n, c) times double_layer(ket, ket) over (w, n) -> (b, c, e, s), ket then bra
 Tensor layer_apply_wn(Engine& E, const Tensor& X, const Tensor& ket);
+// the two steps of layer_apply_wn in one kernel (layered.cu): X5 (x, y, b, u, v, c)
+// and ket (x, u, p, a, e, f) to Z (b, c, e, g, f, h); false when its tiles do not
+// fit in shared memory (Z untouched)
+bool layer_wn_fused(Engine& E, const Tensor& X5, const Tensor& ket, Tensor& Z);
 Tensor left_step(Engine& E, const Tensor& L, const Tensor& T, const Layer& row, const Tensor& B);
 Tensor right_step(Engine& E, const Tensor& T, const Layer& row, const Tensor& B, const Tensor& R);
 Tensor row_edge(Engine& E, const std::vector<Tensor>& top, const std::vector<Layer>& row,
