@@ -300,10 +300,11 @@ def ours_arm(args, rank, world, local_rank):
         achieved = per_launch_flops / (avg_ms * 1e-3) / 1e12
         traffic = None
         if name == "svd_topk":
-            # DRAM bytes per svd_topk launch: an ncu capture of `kernel_probe.py topk` (one 648x648 block,
-            # k = 18) moved 7.25 MB (dram__bytes.sum.per_second x gpu__time_duration.sum), its M and M^T
-            # (6.7 MB) read once; a bench launch holds both parity blocks of that size
-            traffic = 2 * 7.25e6
+            # DRAM bytes per svd_topk launch: an ncu capture of `kernel_probe.py topk 1 gram` (one 648x648
+            # block, k = 18, Gram mode as in the zip-up splits) moved 10.57 MB (dram__bytes.sum.per_second
+            # 11.35 GB/s x gpu__time_duration.sum 931 us): M, M^T and M M^T (10.1 MB) read about once; a
+            # bench launch holds both parity blocks of that size
+            traffic = 2 * 10.57e6
         roofline = {"bound": "tensor", "kernel": name, "achieved": achieved, "peak": peak, "unit": "TFLOP/s",
                     "frac": achieved / peak, "traffic": traffic,
                     "note": "svd_topk is a latency-bound cooperative kernel (chains of small dependent "

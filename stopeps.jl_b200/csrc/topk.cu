@@ -1009,11 +1009,17 @@ void svd_topk(Engine& E, std::vector<TopkDesc>& ds, double tol) {
       if (ph > 0 && ph < PH_COUNT && khz > 0) E.add_stat(std::string("svd_topk.") + names[ph], cyc / khz);
     }
   }
-  // work of the launch: 2 m n b flops per half-iteration, plus the extraction
+  // work of the launch: the start M Omega, 2 m n b flops per half-iteration
+  // (2 m^2 b per Gram iteration; M M^T itself is dgemm_cm's), and per
+  // extraction M^T Q and the residual products M V
   double fl = 0;
-  for (auto& d : ds)
-    fl += d.gram ? 2.0 * d.m * d.m * (d.n + d.iterations * d.b) + 6.0 * d.m * d.n * d.b
-                 : (4.0 * d.iterations + 6.0) * d.m * d.n * d.b;
+  for (auto& d : ds) {
+    const double ext = 1.0 + std::max(0, d.iterations - q0) / qstep;
+    fl += d.gram ? 2.0 * d.m * d.m * d.iterations * d.b + 2.0 * d.m * d.n * d.b +
+                       ext * (2.0 * d.m * d.n * d.b + 2.0 * d.m * d.n * d.k)
+                 : 4.0 * d.iterations * d.m * d.n * d.b + 2.0 * d.m * d.n * d.b +
+                       ext * (2.0 * d.m * d.n * d.b + 2.0 * d.m * d.n * d.k);
+  }
   E.set_work(tid, fl);
   // next starting count: the count that converged; after four first-check
   // successes in a row, one less
