@@ -156,6 +156,10 @@ bool layer_wn_fused(Engine& E, const Tensor& X5, const Tensor& ket0, Tensor& Z) 
   if (X5.dims[0] != Dw || X5.dims[1] != Dw || X5.dims[3] != Dn || X5.dims[4] != Dn) return false;
   const int B = (int)X5.dims[2], C = (int)X5.dims[5];
   const int K1 = Dw * Dn, N2 = De * Ds, N1 = PA * N2;
+  // measured to beat the two table-driven contractions up to D = 6 (D^2 <= 36 on
+  // each side); at D = 8 the tiles need one SM each and the dense products
+  // (twice the block-sparse flops) no longer pay
+  if (K1 > 36 || N2 > 36) return false;
   // the largest chunk of c that keeps two CTAs per SM (else one), shrunk
   // while the grid is under four CTAs per SM (small CTAs cut the last wave)
   int CC = 8;
