@@ -17,7 +17,8 @@
 // break down.  Rayleigh-Ritz extraction: Q <- orth(Q) (plain pass),
 // M^T Q = Qb Rb (shifted Cholesky QR3), Rb^T = Ub S J^T by one-sided Jacobi in
 // one CTA, U = Q Ub, V = Qb J.  The extraction is accepted when
-// ||M v_i - s_i u_i|| is at rounding level for every wanted i; otherwise two
+// ||M v_i - s_i u_i|| is within the requested relative residual (rounding
+// level unless the caller asks for less) for every wanted i; otherwise two
 // more iterations and a new extraction, up to a cap, after which the caller
 // uses the full SVD.  Everything is FP64.
 #include "engine.h"
