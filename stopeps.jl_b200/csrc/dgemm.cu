@@ -81,15 +81,20 @@ __device__ __forceinline__ void store_tile(double* As, double* Bs, const double 
   for (int u = 0; u < B_PER; ++u) Bs[(kb + u) * BLD + j] = rb[u];
 }
 
+// symmetric results (sym): a tile wholly below the diagonal is not computed;
+// its elements come from the mirrored elements of computed tiles
+__host__ __device__ __forceinline__ bool tile_skipped(int i, int j) { return (i / TM) * TM >= (j / TN) * TN + TN; }
+
 template <bool TA>
 __global__ void __launch_bounds__(NT, 2) dgemm_tc_kernel(int M, int N, int K, const double* __restrict__ A, int lda,
                                                          const double* __restrict__ B, int ldb,
                                                          double* __restrict__ C, int ldc, double alpha, double beta,
-                                                         int kchunk, double* __restrict__ partial) {
+                                                         int kchunk, double* __restrict__ partial, int sym) {
   extern __shared__ __align__(16) double gsm[];
   double* const As = gsm;                  // two buffers of TK x ALD
   double* const Bs = gsm + 2 * TK * ALD;   // two buffers of TK x BLD
   const int i0 = blockIdx.y * TM, j0 = blockIdx.x * TN;
+  if (sym && tile_skipped(i0, j0)) return;
   const int kbeg = blockIdx.z * kchunk, kend = min(K, kbeg + kchunk);
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
   const int wm = (warp & 3) * 32, wn = (warp >> 2) * 32;
@@ -145,18 +150,24 @@ __global__ void __launch_bounds__(NT, 2) dgemm_tc_kernel(int M, int N, int K, co
         } else {
           double* c = C + i + (size_t)j * ldc;
           *c = alpha * acc[a][b][e] + (beta == 0.0 ? 0.0 : beta * *c);
+          if (sym && tile_skipped(j, i)) {   // the mirror's own tile is not computed
+            double* cm = C + j + (size_t)i * ldc;
+            *cm = alpha * acc[a][b][e] + (beta == 0.0 ? 0.0 : beta * *cm);
+          }
         }
       }
   }
 }
 
 __global__ void splitk_reduce_kernel(int M, int N, int splits, const double* __restrict__ partial, double* C, int ldc,
-                                     double alpha, double beta) {
+                                     double alpha, double beta, int sym) {
   const size_t total = (size_t)M * N;
   for (size_t e = blockIdx.x * (size_t)blockDim.x + threadIdx.x; e < total; e += (size_t)gridDim.x * blockDim.x) {
-    double s = 0;
-    for (int z = 0; z < splits; ++z) s += partial[(size_t)z * total + e];
     const int i = (int)(e % M), j = (int)(e / M);
+    // a skipped tile's element sums the partials of its mirror (whose tile is computed)
+    const size_t src = (sym && tile_skipped(i, j)) ? (size_t)j + (size_t)i * M : e;
+    double s = 0;
+    for (int z = 0; z < splits; ++z) s += partial[(size_t)z * total + src];
     double* c = C + i + (size_t)j * ldc;
     *c = alpha * s + (beta == 0.0 ? 0.0 : beta * *c);
   }
@@ -165,8 +176,10 @@ __global__ void splitk_reduce_kernel(int M, int N, int splits, const double* __r
 }  // namespace
 
 void dgemm_cm(Engine& E, bool ta, int M, int N, int K, double alpha, const double* A, int lda, const double* B,
-              int ldb, double beta, double* C, int ldc) {
+              int ldb, double beta, double* C, int ldc, bool symmetric) {
   if (M <= 0 || N <= 0) return;
+  if (symmetric && M != N) throw Error(SPS_ERR_ARGUMENT, "dgemm_cm: a symmetric product must be square");
+  const int sym = symmetric ? 1 : 0;
   const int tiles = ((M + TM - 1) / TM) * ((N + TN - 1) / TN);
   int splits = 1, kchunk = std::max(K, 0);
   // split K when the output tiles alone cannot fill two CTAs per SM
@@ -190,20 +203,23 @@ void dgemm_cm(Engine& E, bool ta, int M, int N, int K, double alpha, const doubl
   });
   const int tk = E.tic("dgemm_cm");
   if (ta)
-    dgemm_tc_kernel<true><<<grid, NT, SMEM, E.stream>>>(M, N, K, A, lda, B, ldb, C, ldc, alpha, beta, kchunk, partial);
+    dgemm_tc_kernel<true><<<grid, NT, SMEM, E.stream>>>(M, N, K, A, lda, B, ldb, C, ldc, alpha, beta, kchunk, partial,
+                                                         sym);
   else
-    dgemm_tc_kernel<false><<<grid, NT, SMEM, E.stream>>>(M, N, K, A, lda, B, ldb, C, ldc, alpha, beta, kchunk, partial);
-  E.toc(tk, 2.0 * M * N * (double)K, 8.0 * ((double)M * K + (double)K * N + 2.0 * M * N));
+    dgemm_tc_kernel<false><<<grid, NT, SMEM, E.stream>>>(M, N, K, A, lda, B, ldb, C, ldc, alpha, beta, kchunk, partial,
+                                                          sym);
+  const double fl = sym ? (double)M * (M + 1) * (double)K : 2.0 * M * N * (double)K;
+  E.toc(tk, fl, 8.0 * ((double)M * K + (double)K * N + 2.0 * M * N));
   SPS_CUDA(cudaGetLastError());
   E.launches++;
   if (splits > 1) {
     const size_t total = (size_t)M * N;
     const int g = (int)std::min<size_t>((total + 255) / 256, 4096);
-    splitk_reduce_kernel<<<g, 256, 0, E.stream>>>(M, N, splits, partial, C, ldc, alpha, beta);
+    splitk_reduce_kernel<<<g, 256, 0, E.stream>>>(M, N, splits, partial, C, ldc, alpha, beta, sym);
     SPS_CUDA(cudaGetLastError());
     E.launches++;
   }
-  E.flops += 2.0 * M * N * (double)K;
+  E.flops += fl;
 }
 
 }  // namespace la

@@ -283,8 +283,10 @@ void qr_big_opt(Engine& E, double* a, int m, int n, int lda, double* q, int ldq,
 void jacobi_left(Engine& E, const std::vector<MatDesc>& d);
 void transpose_cm(Engine& E, const double* src, int m, int n, int lds, double* dst, int ldd);
 void svd_big(Engine& E, const std::vector<MatDesc>& d);        // m >= n, ld = m / n
+// symmetric: the product is known to be symmetric (M == N, e.g. A A^T); only
+// tiles on or above the diagonal are computed and the rest mirrored
 void dgemm_cm(Engine& E, bool ta, int M, int N, int K, double alpha, const double* A, int lda, const double* B,
-              int ldb, double beta, double* C, int ldc);
+              int ldb, double beta, double* C, int ldc, bool symmetric = false);
 bool qr_is_big(int m, int n);
 bool svd_is_big(int m, int n);
 // leading k singular triplets of an m x n column-major block (ld m) by block

@@ -941,7 +941,7 @@ void svd_topk(Engine& E, std::vector<TopkDesc>& ds, double tol) {
     encode_rows(&p.tVi, p.Vi, n, d.k, ldn, d.k);
     SPS_CUDA(cudaMemsetAsync(p.info, 0, sizeof(double) * 6 + 8, E.stream));
     transpose_cm(E, d.M, m, n, m, mt, ldn);
-    if (g) dgemm_cm(E, false, m, m, n, 1.0, p.M, ldm, mt, ldn, 0.0, g, ldm);   // G = M M^T
+    if (g) dgemm_cm(E, false, m, m, n, 1.0, p.M, ldm, mt, ldn, 0.0, g, ldm, true);   // G = M M^T
   }
   if (cta > capacity_full) throw Error(SPS_ERR_ARGUMENT, "svd_topk: blocks too large for one cooperative grid");
   Buf pb = E.alloc(sizeof(TopkProb) * nprob);

@@ -84,9 +84,10 @@ def test_topk_matches_lapack(eng, m, n, k, decay):
 
 
 @pytest.mark.parametrize("m,n,k,decay", [(648, 648, 18, 0.1), (1296, 1296, 36, 0.06), (646, 650, 18, 0.1),
-                                         (333, 517, 12, 0.08), (518, 341, 20, 0.05)])
+                                         (333, 517, 12, 0.08), (518, 341, 20, 0.05), (2048, 2048, 32, 0.05)])
 def test_topk_gram_mode_matches_lapack(eng, m, n, k, decay):
-    """The zip-up splits' mode: iterate on a a^T, extract and test residuals on a (1e-10 relative)."""
+    """The zip-up splits' mode: iterate on a a^T (formed by the symmetric GEMM, split-K below about 1800
+    rows, mirrored in the epilogue above), extract and test residuals on a (1e-10 relative)."""
     a = graded(m, n, decay, 11 * m + n + k)
     u, s, v, iters, ms = eng.la_svd_topk(a, k, gram=True, rtol=1e-10)
     ref_u, ref_s, _ = np.linalg.svd(a, full_matrices=False)
