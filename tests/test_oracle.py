@@ -115,3 +115,21 @@ def test_golden_fixture_is_reproducible(name):
     cache = sp.SamplingCache(st, bm.BoundaryMPS(int(a), space(b, cc)))
     d = sp.sample_configuration(cache, uniforms=g["uniforms"][0])
     assert np.array_equal(np.asarray(d["configuration"]), g["configs"][0])
+
+
+@pytest.mark.parametrize("name", ["pepo_2x3_D2.npz"])
+def test_zipup_equals_exact_compression_without_truncation(name):
+    """With chi above the exact boundary bond (d = D^2 = 4 for a 2-wide D=2 lattice) neither absorption
+    truncates, so the zip-up restatement must give the plain compression's norm and the same Born draws."""
+    from util import oracle_state
+    g = golden(name)
+    st = oracle_state(g)
+    plain, zip_ = bm.BoundaryMPS(16), bm.BoundaryMPS(16, None, zipup=True)
+    a, b = bm.lognorm(st, plain), bm.lognorm(st, zip_)
+    assert abs(a["log_norm"] - b["log_norm"]) < 1e-12 * max(1.0, abs(a["log_norm"]))
+    cp, cz = sp.SamplingCache(st, plain), sp.SamplingCache(st, zip_)
+    for u in g["uniforms"][:2]:
+        dp = sp.sample_configuration(cp, uniforms=u)
+        dz = sp.sample_configuration(cz, uniforms=u)
+        assert np.array_equal(np.asarray(dp["configuration"]), np.asarray(dz["configuration"]))
+        assert abs(dp["log_probability"] - dz["log_probability"]) < 1e-11 * max(1.0, abs(dp["log_probability"]))
