@@ -161,10 +161,11 @@ bool layer_wn_fused(Engine& E, const Tensor& X5, const Tensor& ket0, Tensor& Z) 
   // (twice the block-sparse flops) no longer pay
   if (K1 > 36 || N2 > 36) return false;
   // the largest chunk of c that keeps two CTAs per SM (else one), shrunk
-  // while the grid is under four CTAs per SM (small CTAs cut the last wave)
+  // while the grid is under eight CTAs per SM (small CTAs cut the last wave
+  // and, at 52 KB, four of them share an SM)
   int CC = 8;
   while (CC > 1 && (CC > C || layer_wn_smem(CC, K1, N1, N2, PA) > LW_SMEM_TWO)) CC >>= 1;
-  while (CC > 1 && (long long)((C + CC - 1) / CC) * B < 4LL * E.num_sms) CC >>= 1;
+  while (CC > 1 && (long long)((C + CC - 1) / CC) * B < 8LL * E.num_sms) CC >>= 1;
   int lgc = 0;
   while ((1 << lgc) < CC) ++lgc;
   const size_t smem = layer_wn_smem(CC, K1, N1, N2, PA);
