@@ -624,8 +624,9 @@ __global__ void __launch_bounds__(TT, 1) topk_kernel(const TopkProb* __restrict_
   if (threadIdx.x == 0) {
     // the maps were written through the generic proxy (a host copy into
     // pooled memory that earlier launches may have used for other maps)
-    const CUtensorMap* maps[6] = {&p.tM, &p.tMt, &p.tGm, &p.tQ, &p.tZ, &p.tVi};
-    for (int i = 0; i < 6; ++i) {
+    // (the Gram map exists only when iterating on M M^T)
+    const CUtensorMap* maps[6] = {&p.tM, &p.tMt, &p.tQ, &p.tZ, &p.tVi, &p.tGm};
+    for (int i = 0; i < (p.Gm ? 6 : 5); ++i) {
       asm volatile("fence.proxy.tensormap::generic.acquire.gpu [%0], 128;" ::"l"(maps[i]) : "memory");
       asm volatile("prefetch.tensormap [%0];" ::"l"(maps[i]) : "memory");
     }
