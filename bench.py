@@ -1,16 +1,22 @@
 #!/usr/bin/env python
 """Born samples/s on the 8x8 open TFIM (J=1, h=3.0), D=6 (3+3), chi=36 (18+18).
 
-One step = one perfect Born draw (``sample_configuration``, src/sampling/born.jl:86-163):
-eight row absorptions and 64 conditionals from a device-resident SamplingCache
-of a seeded synthetic beta0 PEPO with the workload's shapes.  The headline
-`value` is the zip-up absorption path (FP64); the plain FP64 path with the
-reference's exact LQ + truncated-SVD compression is timed beside it on the same
-draw indices (`plain_fp64`, `agreement_vs_plain`).  Every rank draws its own
-samples (weak scaling: samples shard with no data-path collective); rank 0
-prints one JSON line.
+One step = W perfect Born draws (``sample_configuration``, src/sampling/born.jl:86-163)
+drawn at the same time from a device-resident SamplingCache of a seeded
+synthetic beta0 PEPO with the workload's shapes: per draw eight row absorptions
+and 64 conditionals.  The headline `value` is the zip-up absorption path
+(FP64); the plain FP64 path (the reference's exact LQ + truncated-SVD
+compression, one sample per launch sequence) draws the same sample ids beside
+it (`plain_fp64`, `agreement_vs_plain`).  `pipeline` times the rest of the
+per-sample unit on the same state: projection, one full-update Trotter step
+(src/evolution/full_update.jl:559-597) and one energy measurement
+(src/measurement/energy.jl:31-78), and composes the per-sample rate for
+beta 0.4 -> 2.0 at tau = 0.02.  Every rank draws its own samples (weak
+scaling: samples shard with no data-path collective); rank 0 prints one JSON
+line.
 
-  python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
+  python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference] [--concurrency C]
+  python bench.py --probe NAME [ARGS]   # one hot operation, for profiling (see PROBES)
 """
 from __future__ import annotations
 
@@ -32,27 +38,45 @@ CHI = 36
 H_FIELD = 3.0
 SEED = 1
 PEPO_EPS = 0.15
+PEPO_SEED = 7
+BETA0, BETA_MAX, DTAU = 0.4, 2.0, 0.02
+MEASURE_BETAS = [0.5 + 0.25 * k for k in range(7)]   # 0.5, 0.75, ..., 2.0
 METRIC = "Born samples/s at 8x8 D6 χ36: batched mixed-prec vs plain FP64 GPU, ΔE≤1e-4"
+ORACLE_ENERGY = os.path.join(ROOT, "tests", "golden", "bench_8x8_D6_chi36_energy.npz")
+
+PROBES = """probes (one hot operation on a representative input, run once to warm up and once more):
+  svd_left          U-only Jacobi of a 648x648 LQ-preconditioned block
+  qr                blocked Householder QR of a 23328x648 block
+  topk [W] [gram]   leading 18 triplets of a 648x648 graded block (1/W of the SMs)
+  gemm              FP64 GEMM 23328x648x648 and the 648x648x23328 Gram
+  draw              one Born draw, 8x8 D=6 chi=36, exact compression (synthetic PEPO)
+  zipdraw           the same draw with the zip-up absorption
+  scale             zip-up draws at 12x12 D=8 chi=64 (32+32): 1 and 4 at a time
+  fustep [L]        one full-update Trotter step, L x L D=6 chi=36 (default 8), both absorptions"""
 
 
 def parse():
-    p = argparse.ArgumentParser()
+    p = argparse.ArgumentParser(epilog=PROBES, formatter_class=argparse.RawDescriptionHelpFormatter)
     p.add_argument("--gpus", type=int, default=1)
     p.add_argument("--steps", type=int, default=4)
     p.add_argument("--warmup", type=int, default=3)
     p.add_argument("--impl", default="ours", choices=["ours", "reference"])
     p.add_argument("--concurrency", type=int, default=8,
                    help="samples drawn at the same time on one GPU (own stream and workspace each)")
+    p.add_argument("--no-pipeline", action="store_true", help="skip the full-update / measurement sub-lines")
+    p.add_argument("--no-cpu", action="store_true", help="skip the CPU baseline sample")
+    p.add_argument("--probe", nargs="+", metavar="NAME", help="run one probe instead of the benchmark")
     return p.parse_args()
 
 
 def workload_config(extra=None):
     c = {"workload": "tfim_8x8_D6_chi36_born_draw", "Lx": LX, "Ly": LY, "J": 1.0, "h": H_FIELD, "D": D,
          "bond_space": [D // 2, D // 2], "chi_sampling": CHI, "sampling_space": [CHI // 2, CHI // 2],
-         "pepo": f"synthetic seeded beta0 stand-in (identity + {PEPO_EPS} Gaussian Z2 noise, seed 7)",
-         "step": "one Born draw from a device-resident SamplingCache",
-         "uniforms": "numpy default_rng([seed, sample_index])", "seed": SEED,
-         "l2": "inputs larger than L2 (absorbed boundary tensors ~480 MB each)"}
+         "pepo": f"synthetic seeded beta0 stand-in (identity + {PEPO_EPS} Gaussian Z2 noise, seed {PEPO_SEED}); "
+                 "purifying the 8x8 D=6 PEPO is outside the benchmark's time budget",
+         "step": "W Born draws from a device-resident SamplingCache",
+         "uniforms": "numpy default_rng([seed, sample_id])", "seed": SEED,
+         "l2": "inputs larger than L2 (the south boundaries and candidate double layers of the cache, ~0.6 GB)"}
     if extra:
         c.update(extra)
     return c
@@ -112,62 +136,98 @@ class Clocks:
                 "samples": len(sm)}
 
 
-def cpu_row_sample():
-    """Time the CPU oracle on one interior row of a Born draw: its absorption
-    (absorb + exact LQ sweep + truncated SVD sweep) and its Lx conditionals.
-    Returns (seconds per draw extrapolated as Ly rows, seconds measured)."""
-    import numpy as np
-    from oracle import boundary as bm, model as omd, sampling as osp
-    from oracle.z2 import T, leg
-    import __graft_entry__ as ge
-    syn = ge.load_package().synthetic
-    sites, dims = syn.synthetic_pepo(LX, LY, D, PEPO_EPS, 7)
-    grid = [[None] * LY for _ in range(LX)]
-    for i, (a, ld) in enumerate(zip(sites, dims)):
-        grid[i % LX][i // LX] = T(a, [leg(int(p), int(q)) for p, q in ld])
-    st = omd.State(LX, LY, grid, 0.4, 0.0, "pepo")
-    m = bm.BoundaryMPS(CHI, (CHI // 2, CHI // 2))
-    layers = bm.row_layers(st)
-    env = bm.trivial_boundary(bm.col(layers, 0), "north")
-    env = bm.absorb(env, bm.col(layers, 0), m)           # row 0 (untimed setup)
-    bottom = env.tensors   # stand-in south boundary with the legs a row-1 conditional contracts
-    t0 = time.perf_counter()
-    row = bm.col(layers, 1)
-    le, ri = bm.row_environments(env.tensors, row, bottom, side="right")
-    left = le[0]
-    for x in range(LX):
-        cand = [bm.double_layer(osp.project(st[x, 1], k)) for k in (0, 1)]
-        raw = [bm.row_scalar(left, env.tensors[x], E, bottom[x], ri[x + 1]) for E in cand]
-        if x < LX - 1:
-            left = bm.safe_scale(bm.left_step(left, env.tensors[x], cand[0], bottom[x]))
-    env = bm.absorb(env, row, m)
-    dt = time.perf_counter() - t0
-    return dt * LY, dt
+# ---------------------------------------------------------------------------
+# CPU reference algorithm (the oracle restatement), drawn row by row
+# ---------------------------------------------------------------------------
+class OracleRowDraws:
+    """Reference-algorithm Born draws on the CPU oracle with real boundaries.
+
+    The SamplingCache (PEPO double layers, candidates, the Ly south boundaries
+    by the exact compression) is built once, untimed, as the reference builds
+    it once per checkpoint (born.jl:56-73).  ``step()`` then advances the
+    current draw by one row (its Lx conditionals and the north absorption);
+    after Ly rows the next sample id starts, so consecutive steps are whole
+    draws of sample ids 1, 2, ..."""
+
+    def __init__(self):
+        import numpy as np
+        from oracle import boundary as bm, model as omd, sampling as osp
+        from oracle.z2 import T, leg
+        import __graft_entry__ as ge
+        syn = ge.load_package().synthetic
+        sites, dims = syn.synthetic_pepo(LX, LY, D, PEPO_EPS, PEPO_SEED)
+        grid = [[None] * LY for _ in range(LX)]
+        for i, (a, ld) in enumerate(zip(sites, dims)):
+            grid[i % LX][i // LX] = T(np.asarray(a, float), [leg(int(p), int(q)) for p, q in ld])
+        st = omd.State(LX, LY, grid, BETA0, 0.0, "pepo")
+        omd.normalize_state(st)
+        self.osp = osp
+        self.ge = ge
+        t = time.perf_counter()
+        self.cache = osp.SamplingCache(st, bm.BoundaryMPS(CHI, (CHI // 2, CHI // 2)))
+        self.setup_s = time.perf_counter() - t
+        self.sample_id = 0
+        self.rows = None
+        self.draws = []
+
+    def step(self):
+        if self.rows is None:
+            self.sample_id += 1
+            u = self.ge.load_package().sample_uniforms(SEED, self.sample_id, LX * LY)
+            self.rows = self.osp.sample_rows(self.cache, uniforms=u)
+        try:
+            next(self.rows)
+        except StopIteration as done:
+            self.draws.append((self.sample_id, done.value))
+            self.rows = None
+            self.step()
 
 
 def reference_arm(args, rank, world):
+    """The reference algorithm on the host cores (the Julia reference itself cannot
+    run here: no Julia).  A step is one row of a real draw (see OracleRowDraws);
+    value = (rows timed / Ly) draws over the timed seconds."""
     if rank != 0:
         return
-    import numpy as np
     cores = os.cpu_count()
-    times = []
-    for s in range(args.warmup + args.steps):
-        per_draw, measured = cpu_row_sample()
-        if s >= args.warmup:
-            times.append(per_draw)
-    value = 1.0 / (sum(times) / len(times))
+    rd = OracleRowDraws()
+    for _ in range(args.warmup):
+        rd.step()
+    t0 = time.perf_counter()
+    for _ in range(args.steps):
+        rd.step()
+    dt = time.perf_counter() - t0
+    value = (args.steps / LY) / dt
+    sample = (f"{args.steps} consecutive rows of real draws (sample ids from 1; {args.steps / LY:.2f} draws; a row is "
+              f"{LX} conditionals + the north absorption), after {args.warmup} warm-up rows; the SamplingCache "
+              f"(7 south absorptions) built untimed in {rd.setup_s:.1f} s; CPU oracle (NumPy/OpenBLAS FP64, "
+              f"{cores} threads) restating the reference algorithm (exact LQ + truncated SVD), which cannot run "
+              "here as Julia is not installed")
     line = {"impl": "reference", "metric": METRIC, "value": value, "unit": "samples/s", "n_gpus": args.gpus,
-            "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1e3 / value,
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": dt * 1e3 / args.steps,
             "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
-            "data": "synthetic", "config": workload_config(),
-            "cpu_baseline": {"value": value, "unit": "samples/s", "cores": cores, "kind": "port",
-                             "sample": "one interior row of a draw (absorption + 8 conditionals) per step, "
-                                       "x8 rows; CPU oracle (NumPy/OpenBLAS FP64) restating the Julia "
-                                       "reference, which cannot run here (no Julia)"},
+            "data": "synthetic", "config": workload_config({"step": "one row of a Born draw (reference arm)"}),
+            "cpu_baseline": {"value": value, "unit": "samples/s", "cores": cores, "kind": "port", "sample": sample},
             "e2e": {"value": value, "unit": "samples/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
     print(json.dumps(line), flush=True)
 
 
+def cpu_baseline_sample(rows=2):
+    """The oracle's reference algorithm on `rows` rows of a real draw (cache built untimed)."""
+    rd = OracleRowDraws()
+    t0 = time.perf_counter()
+    for _ in range(rows):
+        rd.step()
+    dt = time.perf_counter() - t0
+    return {"value": (rows / LY) / dt, "unit": "samples/s", "cores": os.cpu_count(), "kind": "port",
+            "sample": f"the first {rows} rows of real draw 1 ({dt:.1f} s; {LX} conditionals + north absorption "
+                      f"each; SamplingCache built untimed in {rd.setup_s:.1f} s), scaled to a draw of {LY} rows; "
+                      "CPU oracle (NumPy/OpenBLAS FP64), reference algorithm"}
+
+
+# ---------------------------------------------------------------------------
+# GPU
+# ---------------------------------------------------------------------------
 def measure_fp64_peak(torch, device):
     """cuBLAS DGEMM 8192^3 through torch (the FP64 denominator of the roofline)."""
     n = 8192
@@ -187,6 +247,27 @@ def measure_fp64_peak(torch, device):
     return best
 
 
+def roofline_of(stats, peak, note):
+    """The dominant FLOP-counted kernel of a per-kernel profile against the FP64 peak."""
+    tot = sum(v["ms"] for k, v in stats.items() if "." not in k and not k.startswith("gemm_gather "))
+    cands = [(k, v) for k, v in stats.items() if v["flops"] > 0 and "." not in k and not k.startswith("gemm_gather ")]
+    name, v = max(cands, key=lambda kv: kv[1]["ms"])
+    per_launch_flops = v["flops"] / v["count"]
+    avg_ms = v["ms"] / v["count"]
+    achieved = per_launch_flops / (avg_ms * 1e-3) / 1e12
+    return {"bound": "tensor", "kernel": name, "achieved": achieved, "peak": peak, "unit": "TFLOP/s",
+            "frac": achieved / peak, "traffic": None, "note": note,
+            "peak_source": "FP64: cuBLAS DGEMM 8192^3 measured in this run (FP64 is not in MEASURED_PEAKS.json); "
+                           "tensor-core FP64 and DFMA share the FP64 rate on B200",
+            "share_of_profiled_time": v["ms"] / tot if tot else None,
+            "kernels": {k: {"ms": round(s["ms"], 3), "count": s["count"],
+                            "share": round(s["ms"] / tot, 4) if tot and "." not in k else None,
+                            "tflops": round(s["flops"] / (s["ms"] * 1e-3) / 1e12, 3)
+                            if s["ms"] > 0 and s["flops"] > 0 else None}
+                        for k, s in sorted(stats.items(), key=lambda kv: -kv[1]["ms"])
+                        if not k.startswith("gemm_gather ")}}
+
+
 def ours_arm(args, rank, world, local_rank):
     import numpy as np
     import torch
@@ -199,13 +280,23 @@ def ours_arm(args, rank, world, local_rank):
         dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=600))
     torch.cuda.set_device(local_rank)
     e = sps.Engine(LX, LY, sps.TFIM(1.0, H_FIELD), device=local_rank)
-    sites, dims = sps.synthetic.synthetic_pepo(LX, LY, D, PEPO_EPS, 7)
-    st = e.upload_state(sites, dims, True, beta=0.4)
+    sites, dims = sps.synthetic.synthetic_pepo(LX, LY, D, PEPO_EPS, PEPO_SEED)
+    st = e.upload_state(sites, dims, True, beta=BETA0)
     sps.normalize_state(st)
     space = sps.Z2Space(CHI // 2, CHI // 2)
+    W = max(1, args.concurrency)
+    L = LX * LY
 
-    def index(step):
-        return 1 + rank + world * step
+    # sample ids: rank r of N draws ids r+1, r+1+N, ...; warm-up, timed and end-to-end draws use disjoint ids
+    def ids_of(first_step, nsteps):
+        out = []
+        for s in range(first_step, first_step + nsteps):
+            out.append([1 + rank + world * (s * W + j) for j in range(W)])
+        return out
+
+    warm_ids = ids_of(0, args.warmup)
+    timed_ids = ids_of(args.warmup, args.steps)
+    e2e_ids = ids_of(args.warmup + args.steps, args.steps)
 
     def barrier():
         torch.cuda.synchronize()
@@ -213,72 +304,69 @@ def ours_arm(args, rank, world, local_rank):
             dist.barrier()
         torch.cuda.synchronize()
 
-    def measure(method, steps, warmup, profile, batch=1):
-        """Device-timed and end-to-end Born draws from a cache built with `method`;
-        a step is `batch` draws (concurrent when batch > 1)."""
-        cache = sps.SamplingCache(st, method)
-        e.set_concurrency(batch)
+    def draw(cache, ids):
+        if len(ids) == 1:
+            d = sps.sample_configuration(cache, uniforms=sps.sample_uniforms(SEED, ids[0], L))
+            return [dict(d, uid=ids[0])]
+        u = np.stack([sps.sample_uniforms(SEED, k, L) for k in ids])
+        cfg, lp = sps.sample_batch(cache, u)
+        return [{"configuration": c, "log_probability": l, "uid": k} for c, l, k in zip(cfg, lp, ids)]
 
-        def draw(i):
-            # draw j of step index i uses the uniforms of sample id i * W + j (W: the zip-up batch)
-            ids = [i * W + j for j in range(batch)]
-            if batch == 1:
-                d = sps.sample_configuration(cache, uniforms=sps.sample_uniforms(SEED, ids[0], LX * LY))
-                return [dict(d, uid=ids[0])]
-            u = np.stack([sps.sample_uniforms(SEED, k, LX * LY) for k in ids])
-            cfg, lp = sps.sample_batch(cache, u)
-            return [{"configuration": c, "log_probability": l, "uid": k} for c, l, k in zip(cfg, lp, ids)]
-
-        for s in range(warmup):
-            draw(index(s))
+    def measure(cache, batch_ids, warm, e2e=None, concurrency=1):
+        """Device-timed draws of the id batches in `batch_ids` (one step each); `e2e`
+        batches are drawn again through the public API and timed by the wall clock."""
+        e.set_concurrency(concurrency)
+        for ids in warm:
+            draw(cache, ids)
         barrier()
         n0, _ = e.counters()
         draws = []
         with Clocks(local_rank) as clk:
             e.timer_start()
-            for s in range(steps):
-                draws.extend(draw(index(warmup + s)))
+            for ids in batch_ids:
+                draws.extend(draw(cache, ids))
             ms = e.timer_stop()
         n1, _ = e.counters()
         barrier()
-        # end to end through the public API: host uniforms in, configuration out, wall clock
-        t0 = time.perf_counter()
-        for s in range(steps):
-            draw(index(warmup + steps + s))
-        barrier()
-        wall = time.perf_counter() - t0
-        t = torch.tensor([ms, wall], dtype=torch.float64, device=f"cuda:{local_rank}")
+        wall = None
+        if e2e:
+            t0 = time.perf_counter()
+            for ids in e2e:
+                draw(cache, ids)
+            barrier()
+            wall = time.perf_counter() - t0
+        t = torch.tensor([ms, wall or 0.0], dtype=torch.float64, device=f"cuda:{local_rank}")
         if dist is not None:
             dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        stats = None
-        if profile:   # per-kernel profile of one serial draw (separate pass; not part of the timed number)
-            e.set_concurrency(1)
-            e.set_profile(True)
-            u = sps.sample_uniforms(SEED, index(2 * steps + warmup) * W, LX * LY)
-            sps.sample_configuration(cache, uniforms=u)
-            stats = e.kernel_stats()
-            e.set_profile(False)
-        e.set_concurrency(1)
-        del cache
         return {"ms": float(t[0]), "wall": float(t[1]), "launches": int(n1 - n0), "clocks": clk.summary(),
-                "draws": draws, "stats": stats}
+                "draws": draws}
 
-    W = max(1, args.concurrency)
-    zip_run = measure(sps.BoundaryMPSZipUp(CHI, space), args.steps, args.warmup, True, W)
-    plain_steps = max(1, min(args.steps, 2))
-    plain_run = measure(sps.BoundaryMPS(CHI, space), plain_steps, min(args.warmup, 3), False)
+    zcache = sps.SamplingCache(st, sps.BoundaryMPSZipUp(CHI, space))
+    zip_run = measure(zcache, timed_ids, warm_ids, e2e_ids, concurrency=W)
+    # per-kernel profile of one more batch at the same concurrency (the timed configuration; untimed)
+    e.set_concurrency(W)
+    e.set_profile(True)
+    draw(zcache, ids_of(args.warmup + 2 * args.steps, 1)[0])
+    conc_stats = e.kernel_stats()
+    e.set_profile(False)
+    # ... and of one serial draw (the per-kernel shares the ncu launch list is compared with)
+    e.set_concurrency(1)
+    e.set_profile(True)
+    draw(zcache, [ids_of(args.warmup + 2 * args.steps + 1, 1)[0][0]])
+    serial_stats = e.kernel_stats()
+    e.set_profile(False)
+
+    # the plain FP64 path, one sample at a time, on the first timed zip-up sample ids
+    plain_steps = max(1, min(args.steps * W, 2))
+    pcache = sps.SamplingCache(st, sps.BoundaryMPS(CHI, space))
+    flat_timed = [k for ids in timed_ids for k in ids]
+    plain_run = measure(pcache, [[k] for k in flat_timed[:plain_steps]], [[1 + rank + world * 10 ** 6]],
+                        e2e=[[k] for k in flat_timed[:plain_steps]])
+    del pcache
     value = world * args.steps * W / (zip_run["ms"] * 1e-3)
     e2e = world * args.steps * W / zip_run["wall"]
     plain_value = world * plain_steps / (plain_run["ms"] * 1e-3)
     plain_e2e = world * plain_steps / plain_run["wall"]
-    # the two paths on the same draw indices
-    import numpy as np
-    same, dlp = 0, 0.0
-    # precision of the zip-up path: energy per site of the beta0 state with both
-    # absorptions (outside the timed regions)
-    en_plain = sps.measure_energy(st, sps.BoundaryMPS(CHI, space))
-    en_zip = sps.measure_energy(st, sps.BoundaryMPSZipUp(CHI, space))
-    # the two paths on the same uniforms (same sample ids)
     zmap = {d["uid"]: d for d in zip_run["draws"]}
     same, dlp, ncmp = 0, 0.0, 0
     for dp in plain_run["draws"]:
@@ -288,43 +376,40 @@ def ours_arm(args, rank, world, local_rank):
         ncmp += 1
         same += int(np.array_equal(dz["configuration"], dp["configuration"]))
         dlp = max(dlp, abs(dz["log_probability"] - dp["log_probability"]))
+
+    # precision: the beta0 state's energy per site under both absorptions against the oracle's FP64
+    # value (exact compression; fixture made by tests/golden/make_golden.py)
+    en_plain = sps.measure_energy(st, sps.BoundaryMPS(CHI, space))
+    en_zip = sps.measure_energy(st, sps.BoundaryMPSZipUp(CHI, space))
+    oracle_e = None
+    if os.path.exists(ORACLE_ENERGY):
+        oracle_e = float(np.load(ORACLE_ENERGY)["energy"][1])
+    ref_e = oracle_e if oracle_e is not None else en_plain["energy_per_site"]
+    precision = {"energy_per_site_oracle_fp64": oracle_e,
+                 "energy_per_site_plain_fp64": en_plain["energy_per_site"],
+                 "energy_per_site_zipup": en_zip["energy_per_site"],
+                 "abs_delta_e_zipup_vs_oracle": abs(en_zip["energy_per_site"] - ref_e),
+                 "abs_delta_e_plain_vs_oracle": abs(en_plain["energy_per_site"] - ref_e),
+                 "reference": "oracle" if oracle_e is not None else "plain FP64 GPU (oracle fixture missing)",
+                 "tolerance": 1e-4,
+                 "state": "the synthetic beta0 PEPO of the workload, chi=36 (18+18)"}
+
+    pipeline = None
+    if not args.no_pipeline:
+        pipeline = pipeline_timing(sps, e, st, zip_run["draws"], W, space, np, torch, local_rank, dist)
+
     result = None
     if rank == 0:
-        stats = zip_run["stats"]
         peak = measure_fp64_peak(torch, f"cuda:{local_rank}")
-        tot = sum(v["ms"] for k, v in stats.items() if "." not in k)
-        dom = max(((k, v) for k, v in stats.items() if v["flops"] > 0 and "." not in k), key=lambda kv: kv[1]["ms"])
-        name, v = dom
-        per_launch_flops = v["flops"] / v["count"]
-        avg_ms = v["ms"] / v["count"]
-        achieved = per_launch_flops / (avg_ms * 1e-3) / 1e12
-        traffic = None
-        if name == "svd_topk":
-            # DRAM bytes per svd_topk launch: an ncu capture of `kernel_probe.py topk 1 gram` (one 648x648
-            # block, k = 18, Gram mode as in the zip-up splits) moved 10.57 MB (dram__bytes.sum.per_second
-            # 11.35 GB/s x gpu__time_duration.sum 931 us): M, M^T and M M^T (10.1 MB) read about once; a
-            # bench launch holds both parity blocks of that size
-            traffic = 2 * 10.57e6
-        roofline = {"bound": "tensor", "kernel": name, "achieved": achieved, "peak": peak, "unit": "TFLOP/s",
-                    "frac": achieved / peak, "traffic": traffic,
-                    "note": "svd_topk is a latency-bound cooperative kernel (chains of small dependent "
-                            "phases, one CTA per SM); FLOPs counted: 2 m n b per product",
-                    "peak_source": "FP64: cuBLAS DGEMM 8192^3 measured in this run (FP64 is not in "
-                                   "MEASURED_PEAKS.json); tensor-core FP64 and DFMA share the FP64 rate on B200",
-                    "share_of_profiled_time": v["ms"] / tot if tot else None,
-                    "kernels": {k: {"ms": round(s["ms"], 3), "count": s["count"],
-                                    "share": round(s["ms"] / tot, 4) if tot and "." not in k else None,
-                                    "tflops": round(s["flops"] / (s["ms"] * 1e-3) / 1e12, 3)
-                                    if s["ms"] > 0 and s["flops"] > 0 else None}
-                                for k, s in sorted(stats.items(), key=lambda kv: -kv[1]["ms"])}}
+        roofline = roofline_of(conc_stats, peak,
+                               f"per-kernel CUDA events of one batch of {W} concurrent draws (the timed "
+                               "configuration: each launch's duration on its stream while the other samples' "
+                               "kernels share the GPU); FLOPs counted over the nonzero Z2 blocks")
+        roofline_serial = roofline_of(serial_stats, peak, "one draw alone (the ncu launch list's configuration)")
         cpu = None
-        if world == 1:
-            per_draw, measured = cpu_row_sample()
-            cpu = {"value": 1.0 / per_draw, "unit": "samples/s", "cores": os.cpu_count(), "kind": "port",
-                   "sample": f"one interior row of a draw (absorption + {LX} conditionals) timed "
-                             f"({measured:.1f} s) and scaled x{LY}; CPU oracle (NumPy/OpenBLAS FP64), "
-                             "reference algorithm"}
-        L = LX * LY
+        if world == 1 and not args.no_cpu:
+            cpu = cpu_baseline_sample()
+        n_h2d = 8 * L * W
         result = {"metric": METRIC, "value": value, "unit": "samples/s", "n_gpus": world, "steps": args.steps,
                   "warmup": args.warmup, "ms_per_step": zip_run["ms"] / args.steps, "higher_is_better": True,
                   "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
@@ -332,22 +417,21 @@ def ours_arm(args, rank, world, local_rank):
                                              "path": f"zip-up boundary absorption, FP64, {W} samples "
                                                      "concurrently (own stream and workspace each)",
                                              "samples_per_step": W}),
-                  "e2e": {"value": e2e, "unit": "samples/s", "h2d_bytes_per_step": 8 * L * W,
+                  "e2e": {"value": e2e, "unit": "samples/s", "h2d_bytes_per_step": n_h2d,
                           "d2h_bytes_per_step": (4 * L + 8) * W},
                   "gpu_launches": zip_run["launches"], "clocks": zip_run["clocks"], "roofline": roofline,
+                  "roofline_serial_draw": roofline_serial,
                   "cpu_baseline": cpu,
                   "plain_fp64": {"value": plain_value, "e2e": plain_e2e, "unit": "samples/s",
                                  "steps": plain_steps, "ms_per_step": plain_run["ms"] / plain_steps,
                                  "gpu_launches": plain_run["launches"], "clocks": plain_run["clocks"],
+                                 "sample_ids": flat_timed[:plain_steps],
                                  "path": "reference algorithm: exact LQ sweep + truncated SVD sweep, FP64"},
                   "speedup_vs_plain_fp64": value / plain_value,
                   "agreement_vs_plain": {"draws": ncmp, "identical_configurations": same,
                                          "max_abs_dlogp": dlp},
-                  "precision": {"energy_per_site_plain_fp64": en_plain["energy_per_site"],
-                                "energy_per_site_zipup": en_zip["energy_per_site"],
-                                "abs_delta_e": abs(en_zip["energy_per_site"] - en_plain["energy_per_site"]),
-                                "tolerance": 1e-4,
-                                "state": "the synthetic beta0 PEPO of the workload, chi=36 (18+18)"}}
+                  "precision": precision,
+                  "pipeline": pipeline}
         print(json.dumps(result), flush=True)
     del st
     e.close()
@@ -356,8 +440,166 @@ def ours_arm(args, rank, world, local_rank):
         dist.destroy_process_group()
 
 
+def pipeline_timing(sps, e, st, draws, W, space, np, torch, local_rank, dist):
+    """The rest of the per-sample unit: projection, one full-update Trotter step and one
+    energy measurement of projected samples (zip-up environments, concurrency W), device-timed;
+    composed with the draw rate into samples/s for beta 0.4 -> 2.0 at tau = 0.02."""
+    n_steps = len(sps.step_schedule(BETA0, BETA_MAX, DTAU))
+    zm = sps.BoundaryMPSZipUp(CHI, space)
+    cfgs = np.stack([d["configuration"] for d in draws[:W]])
+    e.set_concurrency(W)
+    e.timer_start()
+    states, _ = sps.project_batch(st, cfgs)
+    proj_ms = e.timer_stop()
+    e.timer_start()
+    reps = sps.evolution_step_batch(states, [DTAU] * len(states), D, zm, sps.Z2Space(D // 2, D // 2))
+    fu_ms = e.timer_stop()
+    e.timer_start()
+    ens = sps.measure_energy_batch(states, zm)
+    meas_ms = e.timer_stop()
+    e.set_concurrency(1)
+    n = len(states)
+    per_sample_s = (fu_ms * n_steps + meas_ms * len(MEASURE_BETAS) + proj_ms) / n * 1e-3
+    return {"samples": n, "concurrency": W, "environment": "zip-up boundary absorption, FP64",
+            "project_ms_per_batch": proj_ms, "fu_step_ms_per_batch": fu_ms, "measure_ms_per_batch": meas_ms,
+            "fu_step_ms_per_sample": fu_ms / n, "measure_ms_per_sample": meas_ms / n,
+            "fu_bond_updates": reps[0]["bond_updates"], "fu_stop_reasons": {
+                k: sum(r[f"stop_{k}"] for r in reps) for k in ("error_tolerance", "iteration_limit",
+                                                               "residual_fallback", "disabled")},
+            "energy_per_site_after_step": [r["energy_per_site"] for r in ens],
+            "schedule": f"beta {BETA0} -> {BETA_MAX}, tau {DTAU}: {n_steps} steps, {len(MEASURE_BETAS)} measurements",
+            "composed_seconds_per_sample": per_sample_s,
+            "composed_samples_per_s_excluding_draw": 1.0 / per_sample_s if per_sample_s > 0 else None}
+
+
+# ---------------------------------------------------------------------------
+# probes
+# ---------------------------------------------------------------------------
+def graded(m, n, decay, seed):
+    import numpy as np
+    rng = np.random.default_rng(seed)
+    u, _ = np.linalg.qr(rng.standard_normal((m, min(m, n))))
+    v, _ = np.linalg.qr(rng.standard_normal((n, min(m, n))))
+    return (u * np.exp(-decay * np.arange(min(m, n)))) @ v.T
+
+
+def probe(argv):
+    import numpy as np
+    import __graft_entry__ as ge
+    sps = ge.load_package()
+    which = argv[0]
+    if which == "svd_left":
+        e = sps.Engine(2, 2)
+        a = graded(648, 648, 0.03, 5)
+        Lm = np.linalg.qr(a.T)[1].T.copy()
+        for _ in range(2):
+            u, s, sweeps, ms = e.la_svd_left(Lm)
+        print(f"svd_left 648x648: {ms:.2f} ms, {sweeps} sweeps")
+    elif which == "topk":
+        e = sps.Engine(2, 2)
+        w = int(argv[1]) if len(argv) > 1 else 1
+        gram = len(argv) > 2 and argv[2] == "gram"
+        import torch
+        sms = torch.cuda.get_device_properties(0).multi_processor_count
+        e.set_sm_share(sms // w if w > 1 else 0)
+        a = graded(648, 648, 0.1, 5)
+        e.la_svd_topk(a, 18, gram=gram, rtol=1e-10 if gram else 0.0)
+        e.set_profile(True)
+        u, s, v, iters, ms = e.la_svd_topk(a, 18, gram=gram, rtol=1e-10 if gram else 0.0)
+        print(f"topk 648x648 k=18 (SM share 1/{w}{', gram' if gram else ''}): {ms:.3f} ms, {iters} iterations")
+        for name, st in sorted(e.kernel_stats().items()):
+            print(f"  {name:24s} {st['ms']:9.3f} ms  x{st['count']}")
+    elif which == "gemm":
+        e = sps.Engine(2, 2)
+        rng = np.random.default_rng(1)
+        a = rng.standard_normal((23328, 648))
+        b = rng.standard_normal((648, 648))
+        for _ in range(3):
+            c, ms = e.la_gemm(a, b)
+        print(f"gemm 23328x648x648: {ms:.3f} ms, {2 * 23328 * 648 * 648 / ms / 1e9:.2f} TFLOP/s")
+        for _ in range(3):
+            g, ms = e.la_gemm(a, a, transpose_a=True)
+        print(f"gram 648x648x23328: {ms:.3f} ms, {2 * 23328 * 648 * 648 / ms / 1e9:.2f} TFLOP/s")
+    elif which == "qr":
+        e = sps.Engine(2, 2)
+        a = np.random.default_rng(3).standard_normal((23328, 648))
+        for _ in range(2):
+            q, r, ms = e.la_qr(a)
+        print(f"qr 23328x648: {ms:.2f} ms")
+    elif which in ("draw", "zipdraw"):
+        e = sps.Engine(LX, LY, sps.TFIM(1.0, H_FIELD))
+        sites, dims = sps.synthetic.synthetic_pepo(LX, LY, D, PEPO_EPS, PEPO_SEED)
+        st = e.upload_state(sites, dims, True, beta=BETA0)
+        sps.normalize_state(st)
+        kind = sps.BoundaryMPS if which == "draw" else sps.BoundaryMPSZipUp
+        cache = sps.SamplingCache(st, kind(CHI, sps.Z2Space(CHI // 2, CHI // 2)))
+        for i in range(2):
+            if i == 1:
+                e.set_profile(2)
+                t0 = time.perf_counter()
+            d = sps.sample_configuration(cache, uniforms=sps.sample_uniforms(SEED, i + 1, LX * LY))
+        wall = (time.perf_counter() - t0) * 1e3
+        stats = e.kernel_stats()
+        e.set_profile(False)
+        dev = sum(v["ms"] for k, v in stats.items() if not k.startswith(("host.", "svd_topk.", "gemm_gather ")))
+        print(f"draw log_probability {d['log_probability']}: wall {wall:.1f} ms (profiled), kernels {dev:.1f} ms")
+        for name, v in sorted(stats.items(), key=lambda kv: -kv[1]["ms"])[:60]:
+            tf = v["flops"] / v["ms"] / 1e9 if v["ms"] > 0 else 0.0
+            print(f"  {name:40s} {v['ms']:9.3f} ms  x{v['count']:<5d} {tf:6.2f} TF/s")
+    elif which == "scale":
+        Ls, Dd, chi = 12, 8, 64
+        e = sps.Engine(Ls, Ls, sps.TFIM(1.0, H_FIELD))
+        sites, dims = sps.synthetic.synthetic_pepo(Ls, Ls, Dd, PEPO_EPS, 11)
+        st = e.upload_state(sites, dims, True, beta=0.5)
+        sps.normalize_state(st)
+        t = time.perf_counter()
+        cache = sps.SamplingCache(st, sps.BoundaryMPSZipUp(chi, sps.Z2Space(chi // 2, chi // 2)))
+        print(f"cache {time.perf_counter() - t:.2f} s")
+        sps.sample_configuration(cache, uniforms=sps.sample_uniforms(SEED, 1, Ls * Ls))
+        t = time.perf_counter()
+        d = sps.sample_configuration(cache, uniforms=sps.sample_uniforms(SEED, 2, Ls * Ls))
+        print(f"one draw {time.perf_counter() - t:.3f} s, log_probability {d['log_probability']:.6f}")
+        w = 4
+        e.set_concurrency(w)
+        u = np.stack([sps.sample_uniforms(SEED, 10 + j, Ls * Ls) for j in range(2 * w)])
+        sps.sample_batch(cache, u[:w])
+        t = time.perf_counter()
+        sps.sample_batch(cache, u)
+        dt = time.perf_counter() - t
+        print(f"{2 * w} draws {w} at a time: {dt:.3f} s, {2 * w / dt:.2f} samples/s")
+        e.set_concurrency(1)
+    elif which == "fustep":
+        Ls = int(argv[1]) if len(argv) > 1 else LX
+        for zipup in (True, False):
+            e = sps.Engine(Ls, Ls, sps.TFIM(1.0, H_FIELD))
+            sites, dims = sps.synthetic.synthetic_pepo(Ls, Ls, D, PEPO_EPS, PEPO_SEED)
+            st = e.upload_state(sites, dims, True, beta=BETA0)
+            sps.normalize_state(st)
+            ps, _ = sps.project_configuration(st, np.ones((Ls, Ls), np.int32))
+            kind = sps.BoundaryMPSZipUp if zipup else sps.BoundaryMPS
+            m = kind(CHI, sps.Z2Space(CHI // 2, CHI // 2))
+            e.set_profile(True)
+            t = time.perf_counter()
+            r = sps.evolution_step(ps, DTAU, D, m, sps.Z2Space(D // 2, D // 2))
+            dt = time.perf_counter() - t
+            top = sorted(e.kernel_stats().items(), key=lambda kv: -kv[1]["ms"])[:8]
+            e.set_profile(False)
+            t = time.perf_counter()
+            en = sps.measure_energy(ps, m)
+            dm = time.perf_counter() - t
+            print(f"{Ls}x{Ls} {'zip-up' if zipup else 'exact'} environments: FU step {dt:.2f} s, bond updates "
+                  f"{r['bond_updates']}, measure_energy {dm:.2f} s (E {en['energy_per_site']:.8f}); "
+                  + ", ".join(f"{k} {v['ms']:.0f} ms" for k, v in top), flush=True)
+            e.close()
+    else:
+        raise SystemExit(f"unknown probe {which}\n{PROBES}")
+
+
 def main():
     args = parse()
+    if args.probe:
+        probe(args.probe)
+        return
     rank = int(os.environ.get("RANK", 0))
     world = int(os.environ.get("WORLD_SIZE", 1))
     local_rank = int(os.environ.get("LOCAL_RANK", 0))

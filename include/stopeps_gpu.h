@@ -152,7 +152,9 @@ int sps_la_svd_topk(sps_handle* h, int32_t m, int32_t n, int32_t k, const double
  * matrix for callers that cannot allocate device memory (no cudaMalloc /
  * cudaFree / allocating library call is made): a (m x n), u (m x k),
  * s (k) and vt (k x n) are column-major DEVICE buffers of the caller,
- * k = min(m,n), a = u diag(s) vt with s descending.  All scratch is one
+ * k = min(m,n), a = u diag(s) vt with s descending; u and vt stay
+ * orthonormal where singular values are zero (completed to an orthonormal
+ * set).  NaN or Inf input returns SPS_ERR_NUMERIC.  All scratch is one
  * fixed file-scope device array (max(m,n) <= 256, min(m,n) <= 128; larger
  * sizes return SPS_ERR_ARGUMENT) shared by every call on the device: calls
  * whose kernels overlap on the GPU race, so serialise them.  The first call
@@ -209,12 +211,45 @@ int sps_sample_probability(sps_handle* h, int32_t cache_id, const int32_t* confi
  * (1..16, default 1).  Each concurrent sample's cooperative launches use at
  * most 1/samples of the SMs. */
 int sps_set_concurrency(sps_handle* h, int32_t samples);
-/* n draws in one call (the MPI sample loop of src/driver/run.jl:45-49 on one device) */
+/* No counterpart in the reference: host-side failure injection for tests
+ * (nothing faults on the device; the library takes its ordinary error
+ * paths).  force_repair != 0 treats every full-update bond fit as triggered,
+ * so update_bond! takes its PSD-repair branch (src/evolution/full_update.jl:
+ * 490-501) on well-conditioned input; svd_sweep_cap > 0 caps the sweeps of
+ * the single-CTA Jacobi SVD and eigh kernels, which then report
+ * SPS_ERR_CONVERGENCE (the non-convergence status of _retry_svd,
+ * src/states/svd.jl:2-33); 0 restores the default cap of 80. */
+int sps_set_injection(sps_handle* h, int32_t force_repair, int32_t svd_sweep_cap);
+/* n draws in one call (the MPI sample loop of src/driver/run.jl:45-49 on one device);
+ * reports (n) may be NULL. */
 int sps_sample_batch(sps_handle* h, int32_t cache_id, int32_t n, const double* uniforms,
-                     int32_t* configurations, double* log_probabilities);
+                     int32_t* configurations, double* log_probabilities, sps_sample_report* reports);
 /* project_configuration(checkpoint, configuration) (src/sampling/born.jl:27-36) */
 int sps_project(sps_handle* h, int32_t pepo_id, const int32_t* configuration, int32_t* state_id,
                 double* log_normalizations);
+
+/* --- batched variants -------------------------------------------------------
+ * One call over n samples, in place of the reference's per-particle loops
+ * (src/driver/run.jl:52-57 projection + observation of the unique
+ * configurations, :104-108 _advance_particle! per node).  Up to the
+ * sps_set_concurrency count run at the same time, each on its own CUDA
+ * stream and workspace; results are those of the single-sample calls.  Each
+ * state id may appear once per call.  On error the first failing sample's
+ * status is returned (the others have completed). */
+/* n x project_configuration: configurations (n x Lx*Ly labels), state_ids (n)
+ * receive new PEPS states, log_normalizations (n x Lx*Ly) may be NULL. */
+int sps_project_batch(sps_handle* h, int32_t pepo_id, int32_t n, const int32_t* configurations,
+                      int32_t* state_ids, double* log_normalizations);
+/* n x evolution_step! (full_update.jl:559-597) with per-state delta; reports (n) may be NULL. */
+int sps_evolution_step_batch(sps_handle* h, int32_t n, const int32_t* state_ids, const double* deltas, int32_t D,
+                             const int32_t* space, const sps_boundary* environment, sps_step_report* reports);
+/* n x measure_energy (energy.jl:31-78): out (n), site_x (n x Lx*Ly, may be NULL). */
+int sps_measure_energy_batch(sps_handle* h, int32_t n, const int32_t* state_ids, const sps_boundary* method,
+                             sps_energy* out, double* site_x);
+/* n x lognorm (boundary_mps.jl:180-186), the observation at nodes without an energy measurement
+ * (src/driver/particles.jl:35-40). */
+int sps_lognorm_batch(sps_handle* h, int32_t n, const int32_t* state_ids, const sps_boundary* method,
+                      sps_lognorm_result* out);
 
 #ifdef __cplusplus
 }

@@ -92,6 +92,19 @@ def sample_configuration(cache: SamplingCache, uniforms=None, configuration=None
     ``uniforms`` (length Lx*Ly, row-major) replaces ``rand(rng)``;
     ``configuration`` (labels 1/2, indexed [x][y]) evaluates a given draw.
     """
+    rows = sample_rows(cache, uniforms, configuration)
+    while True:
+        try:
+            next(rows)
+        except StopIteration as done:
+            return done.value
+
+
+def sample_rows(cache: SamplingCache, uniforms=None, configuration=None):
+    """``sample_configuration`` as a generator that yields after every row (its
+    Lx conditionals and the absorption of the chosen row into the north
+    boundary); the draw's result is the generator's return value.  Lets a
+    caller time a draw row by row."""
     Lx, Ly = cache.state.Lx, cache.state.Ly
     if uniforms is None and configuration is None:
         raise ValueError("an explicit RNG is required")
@@ -129,6 +142,7 @@ def sample_configuration(cache: SamplingCache, uniforms=None, configuration=None
                 left = bm.safe_scale(bm.left_step(left, top[x], row[x], bottom[x]))
         north = bm.absorb(north, row, cache.method, row_cut=y + 1)
         maxtr = max(maxtr, north.max_truncation)
+        yield y
     return dict(configuration=selected, log_probability=logp, conditionals=conditionals,
                 max_environment_truncation=maxtr, raw=raws)
 

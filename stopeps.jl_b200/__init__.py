@@ -9,7 +9,8 @@ The numerical work runs in ``libstopeps_gpu.so`` (C ABI in
 from .config import (Z2Space, Lattice, TFIM, FullUpdate, BoundaryMPS, BoundaryMPSRow, BoundaryMPSZipUp, ResamplingOptions,
                      SymmetryBasis, RunConfig, validate_config, temperature_nodes, parameter_dict)
 from .engine import (Engine, DeviceState, SamplingCache, normalize_state, evolution_step, lognorm,
-                     measure_energy, sample_configuration, sample_batch, project_configuration)
+                     measure_energy, sample_configuration, sample_batch, project_configuration,
+                     project_batch, evolution_step_batch, measure_energy_batch, lognorm_batch)
 from .driver import (run_purification, run_stochastic, ensemble_statistics, group_configurations,
                      sample_uniforms, step_schedule, ThermalCheckpoint, Particle, RESULT_SCHEMA_VERSION)
 from . import _lib
@@ -21,7 +22,8 @@ __all__ = [
     "Z2Space", "Lattice", "TFIM", "FullUpdate", "BoundaryMPS", "BoundaryMPSRow", "ResamplingOptions",
     "SymmetryBasis", "RunConfig", "validate_config", "temperature_nodes", "parameter_dict", "Engine",
     "DeviceState", "SamplingCache", "normalize_state", "evolution_step", "lognorm", "measure_energy",
-    "sample_configuration", "sample_batch", "project_configuration", "run_purification", "run_stochastic",
+    "sample_configuration", "sample_batch", "project_configuration", "project_batch", "evolution_step_batch",
+    "measure_energy_batch", "lognorm_batch", "run_purification", "run_stochastic",
     "ensemble_statistics", "group_configurations", "sample_uniforms", "step_schedule", "ThermalCheckpoint",
     "Particle", "RESULT_SCHEMA_VERSION", "build", "LIBRARY_PATH",
 ]

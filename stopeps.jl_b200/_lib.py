@@ -20,7 +20,8 @@ EXPORTS = [
     "sps_sampling_cache", "sps_sampling_cache_free", "sps_sample", "sps_sample_probability",
     "sps_sample_batch", "sps_project", "sps_set_profile", "sps_kernel_stats_json", "sps_timer_start",
     "sps_timer_stop", "sps_la_svd", "sps_la_qr", "sps_la_svd_noalloc", "sps_la_svd_left", "sps_la_svd_topk", "sps_la_gemm", "sps_set_concurrency",
-    "sps_set_sm_share",
+    "sps_set_sm_share", "sps_project_batch", "sps_evolution_step_batch", "sps_measure_energy_batch",
+    "sps_lognorm_batch", "sps_set_injection",
 ]
 
 STATUS = {0: "SPS_OK", 1: "SPS_ERR_ARGUMENT", 2: "SPS_ERR_CUDA", 3: "SPS_ERR_NUMERIC",
@@ -100,9 +101,15 @@ def load():
         "sps_sampling_cache_free": ([vp, i32], C.c_int),
         "sps_sample": ([vp, i32, P(dbl), P(i32), P(sps_sample_report)], C.c_int),
         "sps_sample_probability": ([vp, i32, P(i32), P(sps_sample_report)], C.c_int),
-        "sps_sample_batch": ([vp, i32, i32, P(dbl), P(i32), P(dbl)], C.c_int),
+        "sps_sample_batch": ([vp, i32, i32, P(dbl), P(i32), P(dbl), P(sps_sample_report)], C.c_int),
         "sps_project": ([vp, i32, P(i32), P(i32), P(dbl)], C.c_int),
+        "sps_project_batch": ([vp, i32, i32, P(i32), P(i32), P(dbl)], C.c_int),
+        "sps_evolution_step_batch": ([vp, i32, P(i32), P(dbl), i32, P(i32), P(sps_boundary), P(sps_step_report)],
+                                     C.c_int),
+        "sps_measure_energy_batch": ([vp, i32, P(i32), P(sps_boundary), P(sps_energy), P(dbl)], C.c_int),
+        "sps_lognorm_batch": ([vp, i32, P(i32), P(sps_boundary), P(sps_lognorm_result)], C.c_int),
         "sps_set_profile": ([vp, i32], C.c_int),
+        "sps_set_injection": ([vp, i32, i32], C.c_int),
         "sps_kernel_stats_json": ([vp, C.c_char_p, C.c_size_t], C.c_int),
         "sps_timer_start": ([vp], C.c_int),
         "sps_timer_stop": ([vp, P(dbl)], C.c_int),

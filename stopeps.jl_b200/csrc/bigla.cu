@@ -170,28 +170,20 @@ __global__ void __launch_bounds__(BT) panel_qr_kernel(PanelArgs p) {
 void copy_upper_and_identity(Engine& E, const double* a, int m, int n, int lda, double* r, int ldr, double* q,
                              int ldq);
 
-// Allow a kernel the device's full opt-in shared memory once per process: a
-// per-call attribute with the call's own size would race between host
-// threads that launch the same kernel with different sizes.
+// Allow a kernel the current device's full opt-in shared memory (once per
+// device and kernel): a per-call attribute with the call's own size would race
+// between host threads that launch the same kernel with different sizes.
 static void allow_max_smem(const void* kernel) {
-  static std::mutex mu;
-  static std::set<const void*> done;
-  std::lock_guard<std::mutex> g(mu);
-  if (done.count(kernel)) return;
   int dev = 0, maxopt = 0;
   SPS_CUDA(cudaGetDevice(&dev));
   SPS_CUDA(cudaDeviceGetAttribute(&maxopt, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev));
   cudaFuncAttributes fa;
   SPS_CUDA(cudaFuncGetAttributes(&fa, kernel));   // static shared memory counts against the limit
-  SPS_CUDA(cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                maxopt - (int)fa.sharedSizeBytes));
-  done.insert(kernel);
+  set_max_dynamic_smem(kernel, maxopt - (int)fa.sharedSizeBytes);
 }
 
 static int coop_blocks(const void* kernel, int threads, size_t smem, Engine& E) {
-  int per_sm = 0;
-  SPS_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kernel, threads, smem));
-  return E.coop_capacity(per_sm);
+  return E.coop_capacity(occupancy_per_sm(kernel, threads, smem));
 }
 
 // Householder QR of a (m x n, col-major lda), m >= n: q (m x n, ldq), r (n x n, ldr).
@@ -1061,8 +1053,7 @@ void svd_big(Engine& E, const std::vector<MatDesc>& d) {
   SPS_CUDA(cudaMemsetAsync(bb->ptr, 0, sizeof(unsigned) * 2 + sizeof(int) * 6, E.stream));
   if (blocked) {
     allow_max_smem((const void*)bjacobi_kernel);
-    int per_sm = 0;
-    SPS_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, (const void*)bjacobi_kernel, BT, bsmem));
+    const int per_sm = occupancy_per_sm((const void*)bjacobi_kernel, BT, bsmem);
     int G = std::min({E.coop_capacity(per_sm), std::max(1, pairs)});
     const JacProb* dp = (const JacProb*)pb->ptr;
     int nprob = (int)ps.size();

@@ -74,6 +74,107 @@ FUOptions fu_of(const sps_handle* h) {
 
 int leg_sector(const Par& p, int c) { return par_count(p, c); }
 
+void fill_report(const StepReport& r, sps_step_report& o) {
+  o.beta = r.beta;
+  o.max_state_truncation = r.max_state_truncation;
+  o.max_environment_truncation = r.max_environment_truncation;
+  o.max_boundary_entropy = r.max_boundary_entropy;
+  o.max_solver_residual = r.max_solver_residual;
+  o.max_iteration_limit_error = r.max_iteration_limit_error;
+  o.bond_updates = r.bond_updates;
+  o.iteration_limit_hits = r.iteration_limit_hits;
+  o.stop_error_tolerance = r.stop_reasons[0];
+  o.stop_iteration_limit = r.stop_reasons[1];
+  o.stop_residual_fallback = r.stop_reasons[2];
+  o.stop_disabled = r.stop_reasons[3];
+  o.linear_unconverged_updates = r.linear_unconverged;
+  o.repairs = r.repairs;
+  o.fallbacks = r.fallbacks;
+  double sum = 0;
+  for (double v : r.log_normalizations) sum += v;
+  o.log_normalization_sum = sum;
+}
+
+void fill_energy(const EnergyResult& r, sps_energy& o) {
+  o.energy_total = r.energy_total;
+  o.energy_per_site = r.energy_per_site;
+  o.log_norm = r.log_norm;
+  o.tensor_log_norm = r.tensor_log_norm;
+  o.max_environment_truncation = r.max_env_trunc;
+  o.x_sum = r.x_sum;
+  o.zz_sum = r.zz_sum;
+}
+
+// Run fn(engine, i) for i in [0, n): serially on the handle's engine when the
+// concurrency is 1, else on min(concurrency, n) worker engines (own CUDA
+// stream, memory pool and staging ring each), worker w taking i = w, w + W,
+// ...  The workers' streams wait for the handle's stream at the start and the
+// handle's stream waits for them at the end, so events recorded on the
+// handle's stream bracket the whole batch and every buffer that changes
+// hands between engines is used in stream order.  The first error (lowest
+// worker) is rethrown after all workers have finished.
+template <class F>
+void run_batch(sps_handle* h, int n, F&& fn) {
+  if (n < 0) throw Error(SPS_ERR_ARGUMENT, "negative batch size");
+  const int W = std::min<int>(h->concurrency, std::max(n, 1));
+  Engine& M = *h->E;
+  if (W <= 1) {
+    for (int i = 0; i < n; ++i) fn(M, i);
+    return;
+  }
+  while ((int)h->workers.size() < W) {
+    h->workers.push_back(std::make_unique<Engine>(M.device));
+    h->workers.back()->ctas_cap = M.num_sms / h->concurrency;
+    h->workers.back()->force_repair = M.force_repair;
+    h->workers.back()->sweep_cap = M.sweep_cap;
+    h->workers.back()->profile = M.profile;
+  }
+  cudaEvent_t start;
+  SPS_CUDA(cudaEventCreateWithFlags(&start, cudaEventDisableTiming));
+  SPS_CUDA(cudaEventRecord(start, M.stream));
+  for (int w = 0; w < W; ++w) SPS_CUDA(cudaStreamWaitEvent(h->workers[w]->stream, start, 0));
+  std::vector<int> codes(W, SPS_OK);
+  std::vector<std::string> msgs(W);
+  std::vector<std::thread> threads;
+  for (int w = 0; w < W; ++w)
+    threads.emplace_back([&, w] {
+      try {
+        SPS_CUDA(cudaSetDevice(M.device));
+        Engine& E = *h->workers[w];
+        for (int i = w; i < n; i += W) fn(E, i);
+      } catch (const Error& e) {
+        codes[w] = e.code;
+        msgs[w] = e.what();
+      } catch (const std::exception& e) {
+        codes[w] = SPS_ERR_ARGUMENT;
+        msgs[w] = e.what();
+      }
+    });
+  for (auto& t : threads) t.join();
+  for (int w = 0; w < W; ++w) {
+    cudaEvent_t done;
+    SPS_CUDA(cudaEventCreateWithFlags(&done, cudaEventDisableTiming));
+    SPS_CUDA(cudaEventRecord(done, h->workers[w]->stream));
+    SPS_CUDA(cudaStreamWaitEvent(M.stream, done, 0));
+    SPS_CUDA(cudaEventDestroy(done));
+  }
+  SPS_CUDA(cudaEventDestroy(start));
+  for (int w = 0; w < W; ++w)
+    if (codes[w] != SPS_OK) throw Error(codes[w], msgs[w]);
+}
+
+// distinct states of a batch call (a state updated in place appears once)
+std::vector<State*> batch_states(sps_handle* h, int n, const int32_t* ids) {
+  if (n > 0 && !ids) throw Error(SPS_ERR_ARGUMENT, "missing state ids");
+  std::vector<State*> out(n);
+  for (int i = 0; i < n; ++i) {
+    out[i] = &get_state(h, ids[i]);
+    for (int j = 0; j < i; ++j)
+      if (ids[j] == ids[i]) throw Error(SPS_ERR_ARGUMENT, "a state id appears twice in one batch");
+  }
+  return out;
+}
+
 bool sorted_leg(const Par& p) {
   for (size_t i = 1; i < p->size(); ++i)
     if ((*p)[i] < (*p)[i - 1]) return false;
@@ -148,16 +249,44 @@ int sps_set_sm_share(sps_handle* h, int32_t ctas) {
   });
 }
 
+int sps_set_injection(sps_handle* h, int32_t force_repair, int32_t svd_sweep_cap) {
+  return guarded(h, [&] {
+    if (svd_sweep_cap < 0) throw Error(SPS_ERR_ARGUMENT, "sps_set_injection: negative sweep cap");
+    h->E->force_repair = force_repair != 0;
+    h->E->sweep_cap = svd_sweep_cap;
+    for (auto& w : h->workers) {
+      w->force_repair = force_repair != 0;
+      w->sweep_cap = svd_sweep_cap;
+    }
+  });
+}
+
 int sps_set_profile(sps_handle* h, int32_t enable) {
   return guarded(h, [&] {
+    const int level = enable < 0 ? 0 : (enable > 2 ? 2 : enable);
     h->E->reset_stats();
-    h->E->profile = enable < 0 ? 0 : (enable > 2 ? 2 : enable);
+    h->E->profile = level;
+    for (auto& w : h->workers) {
+      w->reset_stats();
+      w->profile = level;
+    }
   });
 }
 
 int sps_kernel_stats_json(sps_handle* h, char* buf, size_t n) {
   return guarded(h, [&] {
+    // the handle's engine and every batch worker (per-kernel times add up
+    // over the engines; under concurrency each is the kernel's own duration
+    // on its stream while the others run beside it)
     auto st = h->E->kernel_stats();
+    for (auto& w : h->workers)
+      for (auto& kv : w->kernel_stats()) {
+        auto& k = st[kv.first];
+        k.ms += kv.second.ms;
+        k.flops += kv.second.flops;
+        k.bytes += kv.second.bytes;
+        k.count += kv.second.count;
+      }
     std::string js = "{";
     bool first = true;
     char tmp[512];
@@ -492,27 +621,28 @@ int sps_evolution_step(sps_handle* h, int32_t state_id, double delta, int32_t D,
     }
     StepReport r = evolution_step(*h->E, s, model_of(h), delta, D, fu_of(h), to_bmps(environment),
                                   h->cfg.trotter_order, sp, h->cfg.record_boundary_entropy != 0);
-    if (report) {
-      sps_step_report& o = *report;
-      o.beta = r.beta;
-      o.max_state_truncation = r.max_state_truncation;
-      o.max_environment_truncation = r.max_environment_truncation;
-      o.max_boundary_entropy = r.max_boundary_entropy;
-      o.max_solver_residual = r.max_solver_residual;
-      o.max_iteration_limit_error = r.max_iteration_limit_error;
-      o.bond_updates = r.bond_updates;
-      o.iteration_limit_hits = r.iteration_limit_hits;
-      o.stop_error_tolerance = r.stop_reasons[0];
-      o.stop_iteration_limit = r.stop_reasons[1];
-      o.stop_residual_fallback = r.stop_reasons[2];
-      o.stop_disabled = r.stop_reasons[3];
-      o.linear_unconverged_updates = r.linear_unconverged;
-      o.repairs = r.repairs;
-      o.fallbacks = r.fallbacks;
-      double sum = 0;
-      for (double v : r.log_normalizations) sum += v;
-      o.log_normalization_sum = sum;
+    if (report) fill_report(r, *report);
+  });
+}
+
+int sps_evolution_step_batch(sps_handle* h, int32_t n, const int32_t* state_ids, const double* deltas, int32_t D,
+                             const int32_t* space, const sps_boundary* environment, sps_step_report* reports) {
+  return guarded(h, [&] {
+    if (n > 0 && !deltas) throw Error(SPS_ERR_ARGUMENT, "missing deltas");
+    std::vector<State*> st = batch_states(h, n, state_ids);
+    int sp[2] = {-1, -1};
+    if (space) {
+      sp[0] = space[0];
+      sp[1] = space[1];
     }
+    const BMPS m = to_bmps(environment);
+    const Model md = model_of(h);
+    const FUOptions o = fu_of(h);
+    run_batch(h, n, [&](Engine& E, int i) {
+      StepReport r = evolution_step(E, *st[i], md, deltas[i], D, o, m, h->cfg.trotter_order, sp,
+                                    h->cfg.record_boundary_entropy != 0);
+      if (reports) fill_report(r, reports[i]);
+    });
   });
 }
 
@@ -532,20 +662,43 @@ int sps_measure_energy(sps_handle* h, int32_t state_id, const sps_boundary* meth
   return guarded(h, [&] {
     State& s = get_state(h, state_id);
     EnergyResult r = measure_energy(*h->E, s, model_of(h), to_bmps(method), h->cfg.record_boundary_entropy != 0);
-    if (out) {
-      out->energy_total = r.energy_total;
-      out->energy_per_site = r.energy_per_site;
-      out->log_norm = r.log_norm;
-      out->tensor_log_norm = r.tensor_log_norm;
-      out->max_environment_truncation = r.max_env_trunc;
-      out->x_sum = r.x_sum;
-      out->zz_sum = r.zz_sum;
-    }
+    if (out) fill_energy(r, *out);
     if (site_x) std::memcpy(site_x, r.site_x.data(), r.site_x.size() * sizeof(double));
     if (se_north && r.entropy.profile)
       std::memcpy(se_north, r.entropy.north.data(), r.entropy.north.size() * sizeof(double));
     if (se_south && r.entropy.profile)
       std::memcpy(se_south, r.entropy.south.data(), r.entropy.south.size() * sizeof(double));
+  });
+}
+
+int sps_measure_energy_batch(sps_handle* h, int32_t n, const int32_t* state_ids, const sps_boundary* method,
+                             sps_energy* out, double* site_x) {
+  return guarded(h, [&] {
+    std::vector<State*> st = batch_states(h, n, state_ids);
+    const BMPS m = to_bmps(method);
+    const Model md = model_of(h);
+    const size_t L = (size_t)h->cfg.Lx * h->cfg.Ly;
+    run_batch(h, n, [&](Engine& E, int i) {
+      EnergyResult r = measure_energy(E, *st[i], md, m, h->cfg.record_boundary_entropy != 0);
+      if (out) fill_energy(r, out[i]);
+      if (site_x) std::memcpy(site_x + i * L, r.site_x.data(), std::min(L, r.site_x.size()) * sizeof(double));
+    });
+  });
+}
+
+int sps_lognorm_batch(sps_handle* h, int32_t n, const int32_t* state_ids, const sps_boundary* method,
+                      sps_lognorm_result* out) {
+  return guarded(h, [&] {
+    std::vector<State*> st = batch_states(h, n, state_ids);
+    const BMPS m = to_bmps(method);
+    run_batch(h, n, [&](Engine& E, int i) {
+      LogNorm r = lognorm(E, *st[i], m);
+      if (out) {
+        out[i].log_norm = r.log_norm;
+        out[i].tensor_log_norm = r.tensor_log_norm;
+        out[i].max_environment_truncation = r.max_env_trunc;
+      }
+    });
   });
 }
 
@@ -611,63 +764,23 @@ int sps_sample_probability(sps_handle* h, int32_t cache_id, const int32_t* confi
 }
 
 int sps_sample_batch(sps_handle* h, int32_t cache_id, int32_t n, const double* uniforms, int32_t* configurations,
-                     double* log_probabilities) {
+                     double* log_probabilities, sps_sample_report* reports) {
   return guarded(h, [&] {
+    if (n > 0 && (!uniforms || !configurations || !log_probabilities))
+      throw Error(SPS_ERR_ARGUMENT, "missing batch buffers");
     SamplingCache& c = get_cache(h, cache_id);
     const int L = c.Lx * c.Ly;
-    const int W = std::min<int>(h->concurrency, std::max(n, 1));
-    if (W <= 1) {
-      for (int i = 0; i < n; ++i) {
-        SampleResult r = sample_configuration(*h->E, c, uniforms + (size_t)i * L, nullptr);
-        for (int k = 0; k < L; ++k) configurations[(size_t)i * L + k] = r.config[k];
-        log_probabilities[i] = r.log_probability;
+    // the shared cache is read-only
+    run_batch(h, n, [&](Engine& E, int i) {
+      SampleResult r = sample_configuration(E, c, uniforms + (size_t)i * L, nullptr);
+      for (int k = 0; k < L; ++k) configurations[(size_t)i * L + k] = r.config[k];
+      log_probabilities[i] = r.log_probability;
+      if (reports) {
+        reports[i].log_probability = r.log_probability;
+        reports[i].max_environment_truncation = r.max_env_trunc;
+        reports[i].near_boundary = r.near_boundary;
       }
-      return;
-    }
-    // W samples at a time, each on its own engine and stream; the shared
-    // cache is read-only.  The handle's stream waits for the workers, so
-    // events recorded on it bracket the whole batch.
-    Engine& M = *h->E;
-    while ((int)h->workers.size() < W) {
-      h->workers.push_back(std::make_unique<Engine>(M.device));
-      h->workers.back()->ctas_cap = M.num_sms / h->concurrency;
-    }
-    cudaEvent_t start;
-    SPS_CUDA(cudaEventCreateWithFlags(&start, cudaEventDisableTiming));
-    SPS_CUDA(cudaEventRecord(start, M.stream));
-    for (int w = 0; w < W; ++w) SPS_CUDA(cudaStreamWaitEvent(h->workers[w]->stream, start, 0));
-    std::vector<int> codes(W, SPS_OK);
-    std::vector<std::string> msgs(W);
-    std::vector<std::thread> threads;
-    for (int w = 0; w < W; ++w)
-      threads.emplace_back([&, w] {
-        try {
-          SPS_CUDA(cudaSetDevice(M.device));
-          Engine& E = *h->workers[w];
-          for (int i = w; i < n; i += W) {
-            SampleResult r = sample_configuration(E, c, uniforms + (size_t)i * L, nullptr);
-            for (int k = 0; k < L; ++k) configurations[(size_t)i * L + k] = r.config[k];
-            log_probabilities[i] = r.log_probability;
-          }
-        } catch (const Error& e) {
-          codes[w] = e.code;
-          msgs[w] = e.what();
-        } catch (const std::exception& e) {
-          codes[w] = SPS_ERR_ARGUMENT;
-          msgs[w] = e.what();
-        }
-      });
-    for (auto& t : threads) t.join();
-    for (int w = 0; w < W; ++w) {
-      cudaEvent_t done;
-      SPS_CUDA(cudaEventCreateWithFlags(&done, cudaEventDisableTiming));
-      SPS_CUDA(cudaEventRecord(done, h->workers[w]->stream));
-      SPS_CUDA(cudaStreamWaitEvent(M.stream, done, 0));
-      SPS_CUDA(cudaEventDestroy(done));
-    }
-    SPS_CUDA(cudaEventDestroy(start));
-    for (int w = 0; w < W; ++w)
-      if (codes[w] != SPS_OK) throw Error(codes[w], msgs[w]);
+    });
   });
 }
 
@@ -682,6 +795,27 @@ int sps_project(sps_handle* h, int32_t pepo_id, const int32_t* configuration, in
     h->states[id] = std::move(s);
     *state_id = id;
     if (log_normalizations) std::memcpy(log_normalizations, ln.data(), ln.size() * sizeof(double));
+  });
+}
+
+int sps_project_batch(sps_handle* h, int32_t pepo_id, int32_t n, const int32_t* configurations, int32_t* state_ids,
+                      double* log_normalizations) {
+  return guarded(h, [&] {
+    State& p = get_state(h, pepo_id);
+    if (n > 0 && (!configurations || !state_ids)) throw Error(SPS_ERR_ARGUMENT, "missing batch buffers");
+    const size_t L = (size_t)p.Lx * p.Ly;
+    std::vector<State> out(std::max(n, 0));
+    run_batch(h, n, [&](Engine& E, int i) {
+      std::vector<int> cfg(configurations + i * L, configurations + (i + 1) * L);
+      std::vector<double> ln;
+      out[i] = project_configuration(E, p, cfg.data(), &ln);
+      if (log_normalizations) std::memcpy(log_normalizations + i * L, ln.data(), ln.size() * sizeof(double));
+    });
+    for (int i = 0; i < n; ++i) {
+      int id = h->next_id++;
+      h->states[id] = std::move(out[i]);
+      state_ids[i] = id;
+    }
   });
 }
 

@@ -196,11 +196,8 @@ void dgemm_cm(Engine& E, bool ta, int M, int N, int K, double alpha, const doubl
     part = E.alloc(sizeof(double) * (size_t)splits * M * N);
     partial = (double*)part->ptr;
   }
-  static std::once_flag attr;
-  std::call_once(attr, [] {
-    SPS_CUDA(cudaFuncSetAttribute(dgemm_tc_kernel<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)SMEM));
-    SPS_CUDA(cudaFuncSetAttribute(dgemm_tc_kernel<false>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)SMEM));
-  });
+  set_max_dynamic_smem((const void*)dgemm_tc_kernel<true>, (int)SMEM);
+  set_max_dynamic_smem((const void*)dgemm_tc_kernel<false>, (int)SMEM);
   const int tk = E.tic("dgemm_cm");
   if (ta)
     dgemm_tc_kernel<true><<<grid, NT, SMEM, E.stream>>>(M, N, K, A, lda, B, ldb, C, ldc, alpha, beta, kchunk, partial,

@@ -19,6 +19,7 @@
 #include <cstdio>
 #include <map>
 #include <memory>
+#include <mutex>
 #include <stdexcept>
 #include <string>
 #include <vector>
@@ -43,6 +44,10 @@ struct Error : std::runtime_error {
 // ---------------------------------------------------------------------------
 // device memory pool (stream-ordered reuse on the engine's single stream)
 // ---------------------------------------------------------------------------
+// Thread-safe: a buffer allocated by one engine may be released by another
+// host thread (batch workers hand states back to the handle).  Reuse stays
+// stream-ordered because every batch call orders the handle's stream and the
+// workers' streams by events at its start and end.
 class Pool {
  public:
   void* get(size_t bytes);
@@ -51,6 +56,8 @@ class Pool {
   ~Pool();
   size_t held() const { return held_; }
  private:
+  void trim_locked();
+  std::mutex mu_;
   std::multimap<size_t, void*> free_;
   size_t held_ = 0;
 };
@@ -153,6 +160,12 @@ class Engine {
     const int c = std::max(1, per_sm) * num_sms;
     return ctas_cap > 0 ? std::min(c, ctas_cap) : c;
   }
+
+  // host-side failure injection (tests): sweep cap of the single-CTA Jacobi
+  // SVD / eigh kernels (0: their default of 80) and a forced PSD repair of
+  // every full-update bond
+  int sweep_cap = 0;
+  bool force_repair = false;
 
   // starting iteration count of the subspace-iteration SVD (adapted per call)
   int topk_hint = 6;
@@ -315,6 +328,12 @@ struct HostTimer {
   HostTimer(Engine& e, const char* n);
   ~HostTimer();
 };
+
+// Per-device kernel attributes.  The opt-in dynamic shared-memory limit is a
+// property of the (device, kernel) pair, so it is set once per pair for the
+// current device; occupancy (CTAs per SM) is cached per (device, kernel, smem).
+void set_max_dynamic_smem(const void* kernel, int bytes);
+int occupancy_per_sm(const void* kernel, int threads, size_t smem);
 
 // gather/scatter between tensors and dense column-major block matrices
 void gather_block(Engine& E, const Tensor& A, const int64_t* rt, const int64_t* ct, int M, int N,

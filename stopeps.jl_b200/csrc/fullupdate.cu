@@ -720,7 +720,7 @@ StepReport evolution_step(Engine& E, State& s, const Model& m, double delta, int
       if (sw.h && s.Lx < 2) continue;
       if (!sw.h && s.Ly < 2) continue;
       sweep(E, s, m, gd, D, o, env_method, sw.h, sw.r, space, record_entropy ? &ent : nullptr, rep, env_err,
-            force_repair);
+            force_repair || E.force_repair);
     }
   }
   s.beta += 2 * delta;

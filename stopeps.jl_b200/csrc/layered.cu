@@ -172,13 +172,8 @@ bool layer_wn_fused(Engine& E, const Tensor& X5, const Tensor& ket0, Tensor& Z) 
   if (smem > LW_SMEM_ONE || B == 0 || C == 0) return false;
   Tensor ket = contiguous(E, ket0);
   Z = E.empty({X5.legs[2], X5.legs[5], ket.legs[4], ket.legs[4], ket.legs[5], ket.legs[5]});
-  static std::once_flag attr;
-  std::call_once(attr, [] {
-    SPS_CUDA(cudaFuncSetAttribute(layer_wn_kernel<6, 6, 6, 6>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                  (int)LW_SMEM_ONE));
-    SPS_CUDA(cudaFuncSetAttribute(layer_wn_kernel<0, 0, 0, 0>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                  (int)LW_SMEM_ONE));
-  });
+  set_max_dynamic_smem((const void*)layer_wn_kernel<6, 6, 6, 6>, (int)LW_SMEM_ONE);
+  set_max_dynamic_smem((const void*)layer_wn_kernel<0, 0, 0, 0>, (int)LW_SMEM_ONE);
   LayerWN d;
   d.X = X5.ptr();
   d.sx = X5.strides[0];

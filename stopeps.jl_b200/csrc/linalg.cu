@@ -128,7 +128,7 @@ __device__ __forceinline__ int rr_index(int i, int round, int np) {
 }
 
 __global__ void __launch_bounds__(NT) svd_kernel(const MatDesc* ds, double* work_base,
-                                                 const size_t* work_off, int* flag) {
+                                                 const size_t* work_off, int* flag, int max_sweeps) {
   const MatDesc d = ds[blockIdx.x];
   const int m = d.m, n = d.n, lda = d.lda;
   if (n == 0) return;
@@ -142,7 +142,7 @@ __global__ void __launch_bounds__(NT) svd_kernel(const MatDesc* ds, double* work
   __syncthreads();
   const double tol = DBL_EPSILON * (double)max(m, 2);
   const int np = n + (n & 1);
-  const int MAXSWEEP = 80;
+  const int MAXSWEEP = max_sweeps;
   bool converged = (n == 1);
   for (int sweep = 0; sweep < MAXSWEEP && !converged; ++sweep) {
     if (threadIdx.x == 0) rotations = 0;
@@ -226,7 +226,7 @@ __global__ void __launch_bounds__(NT) svd_kernel(const MatDesc* ds, double* work
 // ascending in s, eigenvectors in q (n x n, ldq).  `work` holds V and flags.
 // ---------------------------------------------------------------------------
 __global__ void __launch_bounds__(NT) eigh_kernel(const MatDesc* ds, double* work_base,
-                                                  const size_t* work_off, int* flag) {
+                                                  const size_t* work_off, int* flag, int max_sweeps) {
   const MatDesc d = ds[blockIdx.x];
   const int n = d.n, lda = d.lda;
   if (n == 0) return;
@@ -255,7 +255,7 @@ __global__ void __launch_bounds__(NT) eigh_kernel(const MatDesc* ds, double* wor
   const int np = n + (n & 1);
   const int npair = np / 2;
   bool converged = (n == 1) || fro == 0.0;
-  const int MAXSWEEP = 80;
+  const int MAXSWEEP = max_sweeps;
   for (int sweep = 0; sweep < MAXSWEEP && !converged; ++sweep) {
     if (threadIdx.x == 0) rotations = 0;
     __syncthreads();
@@ -441,7 +441,7 @@ void svd_batched(Engine& E, const std::vector<MatDesc>& d) {
   E.stage(off.data(), off.size() * sizeof(size_t), ko->ptr);
   int tk = E.tic("svd_small");
   svd_kernel<<<(int)d.size(), NT, 0, E.stream>>>(dd, (double*)w->ptr, (const size_t*)ko->ptr,
-                                                E.dflag);
+                                                E.dflag, E.sweep_cap > 0 ? E.sweep_cap : 80);
   E.toc(tk);
   SPS_CUDA(cudaGetLastError());
   E.launches++;
@@ -463,7 +463,7 @@ void eigh_batched(Engine& E, const std::vector<MatDesc>& d) {
   E.stage(off.data(), off.size() * sizeof(size_t), ko->ptr);
   int tk = E.tic("eigh");
   eigh_kernel<<<(int)d.size(), NT, 0, E.stream>>>(dd, (double*)w->ptr, (const size_t*)ko->ptr,
-                                                 E.dflag);
+                                                 E.dflag, E.sweep_cap > 0 ? E.sweep_cap : 80);
   E.toc(tk);
   SPS_CUDA(cudaGetLastError());
   E.launches++;

@@ -9,6 +9,11 @@
 // lives in one file-scope __device__ array of fixed size below, so the call
 // allocates nothing (no cudaMalloc, no cudaFree, no allocating library call).
 //
+// Results: a = u diag(s) vt with s descending; u and vt have orthonormal
+// columns / rows even where singular values are zero (the factor is completed
+// to an orthonormal set there).  NaN or Inf in a, or overflow in the column
+// norms, returns SPS_ERR_NUMERIC with the outputs unspecified.
+//
 // Limits and sharing: max(m, n) <= SPS_NOALLOC_MAX_DIM and
 // min(m, n) <= SPS_NOALLOC_MAX_RANK; larger problems are rejected with
 // SPS_ERR_ARGUMENT.  The array is shared by every call on a device and keeps
@@ -63,14 +68,24 @@ __global__ void __launch_bounds__(NT) svd_noalloc_kernel(const double* __restric
   int* rank = (int*)(sig + SPS_NOALLOC_MAX_RANK);
   int* flag = (int*)(sig + 2 * SPS_NOALLOC_MAX_RANK);
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-  if (threadIdx.x == 0) *flag = 0;
+  __shared__ int rotations, nonfinite;
+  if (threadIdx.x == 0) {
+    *flag = 0;
+    nonfinite = 0;
+  }
+  __syncthreads();
   for (int e = threadIdx.x; e < mm * nn; e += NT) {
     int i = e % mm, j = e / mm;
-    U[e] = tall ? a[i + (size_t)j * m] : a[j + (size_t)i * m];
+    const double x = tall ? a[i + (size_t)j * m] : a[j + (size_t)i * m];
+    if (!isfinite(x)) nonfinite = 1;
+    U[e] = x;
   }
   for (int e = threadIdx.x; e < nn * nn; e += NT) V[e] = (e % nn == e / nn) ? 1.0 : 0.0;
-  __shared__ int rotations;
   __syncthreads();
+  if (nonfinite) {   // a NaN or Inf entry: no rotation test is meaningful, write nothing
+    if (threadIdx.x == 0) *flag = 2;
+    return;
+  }
   const double tol = DBL_EPSILON * (double)max(mm, 2);
   const int np = nn + (nn & 1);
   bool converged = (nn == 1);
@@ -114,14 +129,100 @@ __global__ void __launch_bounds__(NT) svd_noalloc_kernel(const double* __restric
     __syncthreads();
   }
   if (!converged && threadIdx.x == 0) *flag = 1;
+  __shared__ int deficient[SPS_NOALLOC_MAX_RANK];
+  __shared__ int bad;
+  if (threadIdx.x == 0) bad = 0;
+  __syncthreads();
   for (int c = warp; c < nn; c += NW) {
-    const double* uc = U + (size_t)c * mm;
+    double* uc = U + (size_t)c * mm;
     double v = 0;
     for (int i = lane; i < mm; i += 32) v += uc[i] * uc[i];
     v = warp_sum(v);
-    if (lane == 0) sig[c] = sqrt(v);
+    const double sc = sqrt(v);
+    // a column whose squared norm is below DBL_MIN took part in no rotation
+    // test: its direction carries no information and is replaced below
+    const bool zero = !(v >= DBL_MIN);
+    if (lane == 0) {
+      sig[c] = zero ? 0.0 : sc;
+      deficient[c] = zero ? 1 : 0;
+      if (!isfinite(sc)) bad = 1;
+    }
+    const double inv = zero ? 0.0 : 1.0 / sc;
+    for (int i = lane; i < mm; i += 32) uc[i] *= inv;   // normalised Jacobi columns
   }
   __syncthreads();
+  if (bad) {   // overflow in the column norms
+    if (threadIdx.x == 0) *flag = 2;
+    return;
+  }
+  // Complete the normalised columns to an orthonormal set where a column is
+  // zero: take the unit vector e_j least covered by the columns already
+  // orthonormal (sum_c U[j,c]^2 smallest, so its residual has squared norm at
+  // least 1/mm), subtract its projection twice (classical Gram-Schmidt with
+  // one reorthogonalisation) and normalise.
+  __shared__ double red_v[NT];
+  __shared__ int red_i[NT];
+  __shared__ double coef[SPS_NOALLOC_MAX_RANK];
+  for (int c = 0; c < nn; ++c) {
+    if (!deficient[c]) continue;
+    double best = 2.0;
+    int bj = 0;
+    for (int j = threadIdx.x; j < mm; j += NT) {
+      double cov = 0;
+      for (int q = 0; q < nn; ++q)
+        if (!deficient[q]) cov += U[j + (size_t)q * mm] * U[j + (size_t)q * mm];
+      if (cov < best) { best = cov; bj = j; }
+    }
+    red_v[threadIdx.x] = best;
+    red_i[threadIdx.x] = bj;
+    __syncthreads();
+    for (int o = NT / 2; o > 0; o >>= 1) {
+      if (threadIdx.x < o) {
+        const double v2 = red_v[threadIdx.x + o];
+        const int i2 = red_i[threadIdx.x + o];
+        if (v2 < red_v[threadIdx.x] || (v2 == red_v[threadIdx.x] && i2 < red_i[threadIdx.x])) {
+          red_v[threadIdx.x] = v2;
+          red_i[threadIdx.x] = i2;
+        }
+      }
+      __syncthreads();
+    }
+    const int jstar = red_i[0];
+    double* x = U + (size_t)c * mm;
+    for (int i = threadIdx.x; i < mm; i += NT) x[i] = (i == jstar) ? 1.0 : 0.0;
+    __syncthreads();
+    for (int pass = 0; pass < 2; ++pass) {
+      for (int q = warp; q < nn; q += NW) {
+        double d = 0;
+        if (!deficient[q]) {
+          const double* uq = U + (size_t)q * mm;
+          for (int i = lane; i < mm; i += 32) d += uq[i] * x[i];
+          d = warp_sum(d);
+        }
+        if (lane == 0) coef[q] = d;
+      }
+      __syncthreads();
+      for (int i = threadIdx.x; i < mm; i += NT) {
+        double v = x[i];
+        for (int q = 0; q < nn; ++q)
+          if (!deficient[q]) v -= coef[q] * U[i + (size_t)q * mm];
+        x[i] = v;
+      }
+      __syncthreads();
+    }
+    if (warp == 0) {
+      double v = 0;
+      for (int i = lane; i < mm; i += 32) v += x[i] * x[i];
+      v = warp_sum(v);
+      if (lane == 0) coef[0] = v > 0 ? 1.0 / sqrt(v) : 0.0;
+    }
+    __syncthreads();
+    const double inv = coef[0];
+    for (int i = threadIdx.x; i < mm; i += NT) x[i] *= inv;
+    __syncthreads();
+    if (threadIdx.x == 0) deficient[c] = 0;   // now part of the orthonormal set
+    __syncthreads();
+  }
   for (int c = threadIdx.x; c < nn; c += NT) {
     double sc = sig[c];
     int r = 0;
@@ -133,15 +234,14 @@ __global__ void __launch_bounds__(NT) svd_noalloc_kernel(const double* __restric
   // X = Ux S V^T; for a^T the roles of the two factors swap.
   for (int c = warp; c < nn; c += NW) {
     int r = rank[c];
-    double inv = sig[c] > 0 ? 1.0 / sig[c] : 0.0;
     const double* uc = U + (size_t)c * mm;
     const double* vc = V + (size_t)c * nn;
     if (tall) {
-      for (int i = lane; i < m; i += 32) u[i + (size_t)r * m] = uc[i] * inv;
+      for (int i = lane; i < m; i += 32) u[i + (size_t)r * m] = uc[i];
       for (int j = lane; j < n; j += 32) vt[r + (size_t)j * nn] = vc[j];
     } else {
       for (int i = lane; i < m; i += 32) u[i + (size_t)r * m] = vc[i];
-      for (int j = lane; j < n; j += 32) vt[r + (size_t)j * nn] = uc[j] * inv;
+      for (int j = lane; j < n; j += 32) vt[r + (size_t)j * nn] = uc[j];
     }
   }
 }
@@ -188,5 +288,6 @@ extern "C" int sps_la_svd_noalloc(int32_t device, void* stream, int32_t m, int32
   }
   if (prev != device) cudaSetDevice(prev);
   if (e != cudaSuccess) return SPS_ERR_CUDA;
+  if (flag == 2) return SPS_ERR_NUMERIC;
   return flag ? SPS_ERR_CONVERGENCE : SPS_OK;
 }

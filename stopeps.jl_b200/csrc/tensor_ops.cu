@@ -6,7 +6,9 @@
 #include <algorithm>
 #include <cmath>
 #include <cstring>
+#include <mutex>
 #include <numeric>
+#include <tuple>
 
 namespace sps {
 
@@ -25,6 +27,7 @@ static size_t round_bytes(size_t b) {
 }
 
 void* Pool::get(size_t bytes) {
+  std::lock_guard<std::mutex> g(mu_);
   auto it = free_.lower_bound(bytes);
   if (it != free_.end() && it->first <= bytes + bytes / 4 + 4096) {
     void* p = it->second;
@@ -36,18 +39,24 @@ void* Pool::get(size_t bytes) {
   cudaError_t e = cudaMalloc(&p, bytes);
   if (e != cudaSuccess) {
     (void)cudaGetLastError();
-    trim();
+    trim_locked();
     SPS_CUDA(cudaMalloc(&p, bytes));
   }
   return p;
 }
 
 void Pool::put(void* p, size_t bytes) {
+  std::lock_guard<std::mutex> g(mu_);
   free_.emplace(bytes, p);
   held_ += bytes;
 }
 
 void Pool::trim() {
+  std::lock_guard<std::mutex> g(mu_);
+  trim_locked();
+}
+
+void Pool::trim_locked() {
   cudaDeviceSynchronize();
   for (auto& kv : free_) cudaFree(kv.second);
   free_.clear();
@@ -285,6 +294,37 @@ void Engine::raise_flag(int h, const char* where) {
     if (h & 8) throw Error(SPS_ERR_NUMERIC, std::string(where) + ": a bulk-copy wait reached its cap");
     throw Error(SPS_ERR_NUMERIC, std::string(where) + ": nonfinite or singular value on device");
   }
+}
+
+// ---------------------------------------------------------------------------
+// per-device kernel attributes
+// ---------------------------------------------------------------------------
+void set_max_dynamic_smem(const void* kernel, int bytes) {
+  static std::mutex mu;
+  static std::map<std::pair<int, const void*>, int> done;
+  int dev = 0;
+  SPS_CUDA(cudaGetDevice(&dev));
+  std::lock_guard<std::mutex> g(mu);
+  auto key = std::make_pair(dev, kernel);
+  auto it = done.find(key);
+  if (it != done.end() && it->second >= bytes) return;
+  SPS_CUDA(cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, bytes));
+  done[key] = bytes;
+}
+
+int occupancy_per_sm(const void* kernel, int threads, size_t smem) {
+  static std::mutex mu;
+  static std::map<std::tuple<int, const void*, int, size_t>, int> cache;
+  int dev = 0;
+  SPS_CUDA(cudaGetDevice(&dev));
+  std::lock_guard<std::mutex> g(mu);
+  auto key = std::make_tuple(dev, kernel, threads, smem);
+  auto it = cache.find(key);
+  if (it != cache.end()) return it->second;
+  int per_sm = 0;
+  SPS_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kernel, threads, smem));
+  cache[key] = per_sm;
+  return per_sm;
 }
 
 // ---------------------------------------------------------------------------

@@ -837,13 +837,9 @@ bool topk_fits(int k, int m, int n, int nprob, Engine& E) {
 
 void svd_topk(Engine& E, std::vector<TopkDesc>& ds, double tol) {
   if (ds.empty()) return;
-  static std::once_flag attr;
-  static int per_sm = 0;
   const size_t smem = sizeof(double) * SMEM_DOUBLES;
-  std::call_once(attr, [smem] {
-    SPS_CUDA(cudaFuncSetAttribute(topk_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
-    SPS_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, topk_kernel, TT, smem));
-  });
+  set_max_dynamic_smem((const void*)topk_kernel, (int)smem);
+  const int per_sm = occupancy_per_sm((const void*)topk_kernel, TT, smem);
   // the engine's share of the GPU is a target: a problem that needs more CTAs
   // than its share gets the minimum it needs (the cooperative launch then
   // waits for free SMs), up to the whole GPU

@@ -150,8 +150,78 @@ class DeviceOps:
     def evolution_step(self, state, delta, D, method, space):
         return eng.evolution_step(state, delta, D, method, space)
 
+    # batched forms: one library call over many samples (sps_*_batch)
+    def sample_batch(self, cache, uniforms):
+        cfgs, lps, reps = eng.sample_batch(cache, uniforms, reports=True)
+        return [dict(configuration=c, log_probability=float(lp), **r) for c, lp, r in zip(cfgs, lps, reps)]
+
+    def project_batch(self, state, configurations):
+        states, ln = eng.project_batch(state, configurations)
+        return list(zip(states, ln))
+
+    def measure_energy_batch(self, states, method):
+        return eng.measure_energy_batch(states, method)
+
+    def lognorm_batch(self, states, method):
+        return eng.lognorm_batch(states, method)
+
+    def evolution_step_batch(self, states, deltas, D, method, space):
+        return eng.evolution_step_batch(states, deltas, D, method, space)
+
 
 DEVICE_OPS = DeviceOps()
+
+
+def _batched(ops, name, single, items, *args):
+    """ops.<name>_batch(items, *args) when the ops provide it, else the single
+    operation item by item (the ops of a test double may define only those)."""
+    f = getattr(ops, name + "_batch", None)
+    if f is not None:
+        return list(f(items, *args))
+    return [single(x, *args) for x in items]
+
+
+def _observe_batch(states, c: RunConfig, energy: bool, ops=DEVICE_OPS):
+    """``_observe`` of many states in one call; the elapsed time is shared equally."""
+    t = time.perf_counter()
+    method = c.boundary("measurement")
+    if energy:
+        ms = _batched(ops, "measure_energy", ops.measure_energy, states, method)
+    else:
+        ms = _batched(ops, "lognorm", ops.lognorm, states, method)
+        for m in ms:
+            m.update(energy_total=math.nan, energy_per_site=math.nan, magnetization=math.nan)
+    dt = (time.perf_counter() - t) / max(1, len(states))
+    for m in ms:
+        m["measurement_seconds"] = dt
+    return ms
+
+
+def _evolve_batch(states, c: RunConfig, steps, D, space, ops=DEVICE_OPS):
+    """``_evolve!`` (``particles.jl:66-85``) of many states over the same beta
+    schedule: one batched evolution step per beta; the elapsed time is shared
+    equally."""
+    n = len(states)
+    out = [dict(time_seconds=0.0, max_state_truncation=0.0, max_environment_truncation=0.0,
+                max_boundary_entropy=0.0 if (c.record_boundary_entropy and steps) else math.nan,
+                normalization=0.0) for _ in range(n)]
+    single = getattr(ops, "evolution_step_batch", None)
+    for beta in steps:
+        t = time.perf_counter()
+        deltas = [(beta - s.beta) / 2 for s in states]
+        if single is not None:
+            reps = single(states, deltas, D, c.boundary("environment"), space)
+        else:
+            reps = [ops.evolution_step(s, d, D, c.boundary("environment"), space) for s, d in zip(states, deltas)]
+        elapsed = (time.perf_counter() - t) / max(1, n)
+        for s, r, o in zip(states, reps, out):
+            s.beta = beta
+            o["normalization"] += r["log_normalization_sum"]
+            o["time_seconds"] += elapsed
+            o["max_state_truncation"] = max(o["max_state_truncation"], r["max_state_truncation"])
+            o["max_environment_truncation"] = max(o["max_environment_truncation"], r["max_environment_truncation"])
+            o["max_boundary_entropy"] = max(o["max_boundary_entropy"], r["max_boundary_entropy"])
+    return out
 
 
 def _observe(state, c: RunConfig, energy: bool, ops=DEVICE_OPS):
@@ -278,26 +348,35 @@ def run_stochastic(c: RunConfig, checkpoint: ThermalCheckpoint, uniforms_fn=None
 
     def local_draws():
         cache = ops.sampling_cache(checkpoint.state, c.boundary("sampling"))
-        out = []
-        for i in range(1, c.Ns + 1):
-            if (i - 1) % nprocs != rank:
-                continue
-            d = dict(ops.sample(cache, uniforms_fn(i)))
+        idx = [i for i in range(1, c.Ns + 1) if (i - 1) % nprocs == rank]
+        if not idx:
+            return []
+        if hasattr(ops, "sample_batch"):   # every local draw in one call
+            out = [dict(d) for d in ops.sample_batch(cache, np.stack([uniforms_fn(i) for i in idx]))]
+        else:
+            out = [dict(ops.sample(cache, uniforms_fn(i))) for i in idx]
+        for d, i in zip(out, idx):
             d["index"] = i
-            out.append(d)
         return out
 
     draws = sorted([d for part in e.gather(e.phase(local_draws)) for d in part], key=lambda d: d["index"])
     grouping = group_configurations([d["configuration"] for d in draws])
 
     def local_particles():
+        # _representative_owner (src/driver/execution.jl:34): unique configuration u on rank (u-1) % nprocs
+        mine = [(u, i) for u, i in enumerate(grouping["first_draw"], start=1) if (u - 1) % nprocs == rank]
+        if not mine:
+            return []
+        cfgs = [draws[i - 1]["configuration"] for _, i in mine]
+        if hasattr(ops, "project_batch"):
+            projected = ops.project_batch(checkpoint.state, np.stack([np.asarray(x) for x in cfgs]))
+        else:
+            projected = [ops.project(checkpoint.state, x) for x in cfgs]
+        states = [p[0] for p in projected]
+        obs = _observe_batch(states, c, measure_at(c, c.beta0), ops)
         out = []
-        for u, i in enumerate(grouping["first_draw"], start=1):
-            if (u - 1) % nprocs != rank:     # _representative_owner (src/driver/execution.jl:34)
-                continue
+        for (u, i), state, m in zip(mine, states, obs):
             d = draws[i - 1]
-            state, _ = ops.project(checkpoint.state, d["configuration"])
-            m = _observe(state, c, measure_at(c, c.beta0), ops)
             out.append(Particle(id=i, count=grouping["multiplicity"][u - 1], configuration=d["configuration"],
                                 state=state, log_p0=d["log_probability"], log_q_proposal=d["log_probability"],
                                 relative_log_weight=m["log_norm"] - d["log_probability"],
@@ -318,10 +397,12 @@ def run_stochastic(c: RunConfig, checkpoint: ThermalCheckpoint, uniforms_fn=None
             steps = step_schedule(nodes[node - 1], beta, c.delta_tau_peps)
 
             def advance():
-                for p in particles:
+                # _advance_particle! (particles.jl:86-102) for every local particle, batched per step
+                states = [p.state for p in particles]
+                reps = _evolve_batch(states, c, steps, c.D_peps, c.bond_space_peps, ops=ops)
+                obs = _observe_batch(states, c, measure_at(c, beta), ops)
+                for p, rep, m in zip(particles, reps, obs):
                     old = p.tensor_log_norm
-                    rep = _evolve(p.state, c, steps, c.D_peps, c.bond_space_peps, ops=ops)
-                    m = _observe(p.state, c, measure_at(c, beta), ops)
                     p.relative_log_weight += 2 * rep["normalization"] + (m["tensor_log_norm"] - old)
                     p.physical_log_norm = m["log_norm"]
                     p.tensor_log_norm = m["tensor_log_norm"]

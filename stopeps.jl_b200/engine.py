@@ -83,6 +83,11 @@ class Engine:
         """Cap this handle's own cooperative launches at ``ctas`` CTAs each (0: the whole GPU)."""
         self.check(self.lib.sps_set_sm_share(self.h, int(ctas)))
 
+    def set_injection(self, force_repair=False, svd_sweep_cap=0):
+        """Host-side failure injection for tests: force the PSD-repair branch of
+        every bond update; cap the small-block Jacobi sweeps (0 = default)."""
+        self.check(self.lib.sps_set_injection(self.h, 1 if force_repair else 0, int(svd_sweep_cap)))
+
     def set_profile(self, enable):
         """0/False off, 1/True per-kernel stats, 2 also per-shape contraction stats (resets the stats)."""
         self.check(self.lib.sps_set_profile(self.h, int(enable)))
@@ -357,17 +362,92 @@ def sample_configuration(cache: SamplingCache, uniforms=None, configuration=None
                 max_environment_truncation=rep.max_environment_truncation, near_boundary=rep.near_boundary)
 
 
-def sample_batch(cache: SamplingCache, uniforms):
-    """Many draws in one call: uniforms (n, Lx*Ly) -> configurations (n, Lx, Ly), log_p (n,)."""
+def sample_batch(cache: SamplingCache, uniforms, reports=False):
+    """Many draws in one call: uniforms (n, Lx*Ly) -> configurations (n, Lx, Ly), log_p (n,)
+    (and, with ``reports``, each draw's max_environment_truncation and near_boundary count)."""
     e = cache.engine
     L = e.Lx * e.Ly
     u = np.ascontiguousarray(np.asarray(uniforms, np.float64).reshape(-1, L))
     n = u.shape[0]
     cfg = np.zeros((n, L), np.int32)
     lp = np.zeros(n)
+    rep = (_lib.sps_sample_report * max(n, 1))()
     e.check(e.lib.sps_sample_batch(e.h, cache.id, n, _arr(u, C.c_double), _arr(cfg, C.c_int32),
-                                   _arr(lp, C.c_double)))
-    return cfg.reshape(n, e.Ly, e.Lx).transpose(0, 2, 1).copy(), lp
+                                   _arr(lp, C.c_double), rep))
+    cfgs = cfg.reshape(n, e.Ly, e.Lx).transpose(0, 2, 1).copy()
+    if reports:
+        return cfgs, lp, [dict(max_environment_truncation=rep[i].max_environment_truncation,
+                               near_boundary=rep[i].near_boundary) for i in range(n)]
+    return cfgs, lp
+
+
+def _ids(states):
+    e = states[0].engine if states else None
+    if any(s.engine is not e for s in states):
+        raise ValueError("a batch must hold states of one engine")
+    return e, np.ascontiguousarray([s.id for s in states], np.int32)
+
+
+def evolution_step_batch(states, deltas, D, contraction: BoundaryMPS, sector_space: Z2Space | None = None):
+    """``evolution_step!`` on every state of ``states`` in one call (per-state ``deltas``)."""
+    if not states:
+        return []
+    e, ids = _ids(states)
+    n = len(states)
+    d = np.ascontiguousarray(np.broadcast_to(np.asarray(deltas, np.float64), (n,)))
+    reps = (_lib.sps_step_report * n)()
+    b = _boundary(contraction)
+    sp = None if sector_space is None else (C.c_int32 * 2)(sector_space.n0, sector_space.n1)
+    e.check(e.lib.sps_evolution_step_batch(e.h, n, _arr(ids, C.c_int32), _arr(d, C.c_double), int(D), sp,
+                                           C.byref(b), reps))
+    return [{f: getattr(r, f) for f, _ in r._fields_} for r in reps]
+
+
+def measure_energy_batch(states, contraction: BoundaryMPS):
+    """``measure_energy`` of every state in one call."""
+    if not states:
+        return []
+    e, ids = _ids(states)
+    n, L = len(states), e.Lx * e.Ly
+    out = (_lib.sps_energy * n)()
+    sx = np.zeros(n * L)
+    b = _boundary(contraction)
+    e.check(e.lib.sps_measure_energy_batch(e.h, n, _arr(ids, C.c_int32), C.byref(b), out, _arr(sx, C.c_double)))
+    res = []
+    for i, r in enumerate(out):
+        res.append(dict(energy_total=r.energy_total, energy_per_site=r.energy_per_site, log_norm=r.log_norm,
+                        tensor_log_norm=r.tensor_log_norm, max_environment_truncation=r.max_environment_truncation,
+                        x_sum=r.x_sum, zz_sum=r.zz_sum, magnetization=r.x_sum / L,
+                        site_x=sx[i * L:(i + 1) * L].reshape(e.Ly, e.Lx).T.copy()))
+    return res
+
+
+def lognorm_batch(states, contraction: BoundaryMPS):
+    """``lognorm`` of every state in one call."""
+    if not states:
+        return []
+    e, ids = _ids(states)
+    n = len(states)
+    out = (_lib.sps_lognorm_result * n)()
+    b = _boundary(contraction)
+    e.check(e.lib.sps_lognorm_batch(e.h, n, _arr(ids, C.c_int32), C.byref(b), out))
+    return [dict(log_norm=r.log_norm, tensor_log_norm=r.tensor_log_norm,
+                 max_environment_truncation=r.max_environment_truncation) for r in out]
+
+
+def project_batch(pepo: DeviceState, configurations):
+    """``project_configuration`` of every configuration ((n, Lx, Ly) labels) in one call."""
+    e = pepo.engine
+    cfgs = np.asarray(configurations, np.int32)
+    n = cfgs.shape[0]
+    if n == 0:
+        return [], np.zeros((0, e.Lx * e.Ly))
+    flat = np.ascontiguousarray(cfgs.transpose(0, 2, 1).reshape(n, -1))
+    sids = np.zeros(n, np.int32)
+    ln = np.zeros((n, e.Lx * e.Ly))
+    e.check(e.lib.sps_project_batch(e.h, pepo.id, n, _arr(flat, C.c_int32), _arr(sids, C.c_int32),
+                                    _arr(ln, C.c_double)))
+    return [DeviceState(e, int(i)) for i in sids], ln
 
 
 def project_configuration(pepo: DeviceState, configuration):

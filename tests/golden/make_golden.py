@@ -89,6 +89,90 @@ def pepo_case(name, Lx, Ly, h, D, space, chi_env, env_space, beta0, dtau, chis, 
           "step", out["step_stops"], out["step_report"])
 
 
+def synthetic_state(Lx, Ly, D, eps, seed):
+    """The seeded synthetic PEPO of ``stopeps.jl_b200/synthetic.py`` (pure NumPy)
+    as an oracle state; loaded from the file so that no device code is imported."""
+    import importlib.util
+    spec = importlib.util.spec_from_file_location("_synthetic", os.path.join(ROOT, "stopeps.jl_b200", "synthetic.py"))
+    syn = importlib.util.module_from_spec(spec)
+    spec.loader.exec_module(syn)
+    from oracle.model import State
+    from oracle.z2 import leg
+    sites, dims = syn.synthetic_pepo(Lx, Ly, D, eps, seed)
+    grid = [[None] * Ly for _ in range(Lx)]
+    for i, (a, d) in enumerate(zip(sites, dims)):
+        grid[i % Lx][i // Lx] = T(np.asarray(a, float), [leg(int(p), int(q)) for p, q in d])
+    return State(Lx, Ly, grid, 0.4, 0.0, "pepo")
+
+
+def headline_case(name, Lx=4, Ly=4, D=6, chi=36, h=3.0, dtau=0.02, ndraws=3, seed=1):
+    """The headline shapes (D=6 = 3+3, chi=36 = 18+18, h=3.0, tau=0.02) on a
+    small lattice: the seeded synthetic beta0 PEPO of the benchmark workload.
+    Both absorptions (exact compression and zip-up): lognorm, energy with the
+    site <X> profile and the Schmidt entropies, Born draws; the projection of
+    the first draw and one full-update step of that D=6 PEPS."""
+    st = synthetic_state(Lx, Ly, D, 0.15, 7)
+    data, dims = state_arrays(st)
+    model = md.TFIM(1.0, h)
+    sec = (chi // 2, chi // 2)
+    out = dict(Lx=Lx, Ly=Ly, J=1.0, h=h, beta=st.beta, log_amplitude=st.log_amplitude, data=data, dims=dims,
+               chi=np.array([chi, sec[0], sec[1]]), dtau=dtau, D=D)
+    U = np.stack([dr.sample_uniforms(seed, i, Lx * Ly) for i in range(1, ndraws + 1)])
+    out["uniforms"] = U
+    for tag, zipup in (("plain", False), ("zip", True)):
+        m = bm.BoundaryMPS(chi, sec, zipup=zipup)
+        ln = bm.lognorm(st, m)
+        en = sp.measure_energy(st, model, m, record_entropy=not zipup)
+        out[f"{tag}_lognorm"] = np.array([ln["log_norm"], ln["tensor_log_norm"], ln["max_environment_truncation"]])
+        out[f"{tag}_energy"] = np.array([en["energy_total"], en["energy_per_site"], en["log_norm"], en["x_sum"],
+                                         en["max_environment_truncation"], en["zz_sum"]])
+        out[f"{tag}_site_x"] = en["site_x"]
+        if not zipup:
+            out["plain_Se_north"] = en["Se"]["north"]
+            out["plain_Se_south"] = en["Se"]["south"]
+        cache = sp.SamplingCache(st, m)
+        cfgs, lps = [], []
+        for u in U:
+            d = sp.sample_configuration(cache, uniforms=u)
+            cfgs.append(np.asarray(d["configuration"]))
+            lps.append(d["log_probability"])
+        out[f"{tag}_configs"] = np.stack(cfgs)
+        out[f"{tag}_log_probs"] = np.asarray(lps)
+        print(name, tag, "lognorm", ln["log_norm"], "E", en["energy_per_site"], "logp", lps, flush=True)
+    cfg0 = out["plain_configs"][0]
+    ps, norms = sp.project_configuration(st, cfg0.tolist())
+    pm = bm.BoundaryMPS(chi, sec)
+    e0 = sp.measure_energy(ps, model, pm)
+    r = fu.evolution_step(ps, model, dtau, D, fu.FullUpdate(), pm, space=(D // 2, D // 2), record_entropy=True)
+    e1 = sp.measure_energy(ps, model, pm)
+    out.update(proj_norms=np.asarray([v for _, v in norms]),
+               proj_energy=np.array([e0["energy_per_site"], e0["log_norm"], e0["x_sum"]]),
+               step_norm_sum=sum(v for _, v in r["normalizations"]),
+               step_norms=np.asarray([v for _, v in r["normalizations"]]),
+               step_report=np.array([r["max_state_truncation"], r["max_environment_truncation"],
+                                     r["max_boundary_entropy"], r["bond_updates"]]),
+               step_stops=np.array([r["stop_reasons"][k] for k in
+                                    ("error_tolerance", "iteration_limit", "residual_fallback", "disabled")]),
+               step_energy=np.array([e1["energy_per_site"], e1["log_norm"], e1["tensor_log_norm"], e1["x_sum"]]),
+               step_site_x=e1["site_x"])
+    np.savez_compressed(os.path.join(HERE, name), **out)
+    print(name, "step", out["step_stops"], out["step_report"], "E1", e1["energy_per_site"], flush=True)
+
+
+def bench_energy_case(name, L=8, D=6, chi=36, h=3.0):
+    """The FP64 oracle energy of the benchmark's beta0 state (8x8 synthetic PEPO,
+    D=6, chi=36 = 18+18, exact compression): the reference value of the
+    benchmark's precision check."""
+    st = synthetic_state(L, L, D, 0.15, 7)
+    md.normalize_state(st)
+    m = bm.BoundaryMPS(chi, (chi // 2, chi // 2))
+    en = sp.measure_energy(st, md.TFIM(1.0, h), m)
+    out = dict(energy=np.array([en["energy_total"], en["energy_per_site"], en["log_norm"], en["x_sum"],
+                                en["max_environment_truncation"]]), site_x=en["site_x"])
+    np.savez_compressed(os.path.join(HERE, name), **out)
+    print(name, "E", en["energy_per_site"], flush=True)
+
+
 def pipeline_case(name):
     c = dr.RunConfig(Lx=2, Ly=2, J=1.0, h=0.7, beta0=0.2, beta_log=[0.1, 0.2, 0.3], beta_measure=[0.2, 0.3],
                      delta_tau_pur=0.05, delta_tau_peps=0.05, D_pur=2, D_peps=2, bond_space_pur=(1, 1),
@@ -115,7 +199,9 @@ if __name__ == "__main__":
         for name in only:
             {"pepo_4x4_D4.npz": lambda: pepo_case("pepo_4x4_D4.npz", 4, 4, 0.7, 4, (2, 2), 16, (8, 8), 0.5, 0.05,
                                                   [(16, (8, 8)), (24, (12, 12))], peps_D=4, peps_space=(2, 2),
-                                                  peps_chi=16, peps_env_space=(8, 8), ndraws=4, seed=1)}[name]()
+                                                  peps_chi=16, peps_env_space=(8, 8), ndraws=4, seed=1),
+             "headline_4x4_D6_chi36.npz": lambda: headline_case("headline_4x4_D6_chi36.npz"),
+             "bench_8x8_D6_chi36_energy.npz": lambda: bench_energy_case("bench_8x8_D6_chi36_energy.npz")}[name]()
         sys.exit(0)
     # 3x3, D=4 PEPO; boundary chi 8 truncates, 16 is exact; PEPS step at D=2 exercises the ALS
     pepo_case("pepo_3x3_D4.npz", 3, 3, 0.7, 4, (2, 2), 16, (8, 8), 0.2, 0.05,
@@ -130,3 +216,7 @@ if __name__ == "__main__":
     pepo_case("pepo_4x4_D4.npz", 4, 4, 0.7, 4, (2, 2), 16, (8, 8), 0.5, 0.05,
               [(16, (8, 8)), (24, (12, 12))], peps_D=4, peps_space=(2, 2), peps_chi=16, peps_env_space=(8, 8),
               ndraws=4, seed=1)
+    # the headline shapes (D=6, chi=36 = 18+18, h=3.0, tau=0.02) on 4x4, synthetic seeded PEPO
+    headline_case("headline_4x4_D6_chi36.npz")
+    # the benchmark's precision reference: the 8x8 beta0 state's FP64 energy
+    bench_energy_case("bench_8x8_D6_chi36_energy.npz")

@@ -51,6 +51,46 @@ def test_noalloc_svd_matches_allocating_entry_point(sps, m, n):
         np.testing.assert_allclose(u.T @ u, np.eye(k), atol=TOL)
 
 
+@pytest.mark.parametrize("m,n,r", [(100, 60, 20), (40, 90, 7), (50, 50, 0)])
+def test_noalloc_svd_rank_deficient(sps, m, n, r):
+    """Rank r < min(m, n) (r = 0: the zero matrix): the singular values match
+    numpy.linalg.svd, zero values stay zero, and both factors are still
+    orthonormal (the columns of the zero values are completed), on two calls
+    in a row."""
+    import torch
+    lib = sps._lib.load()
+    rng = np.random.default_rng(7 * m + n + r)
+    k = min(m, n)
+    for call in range(2):
+        a = rng.standard_normal((m, r)) @ rng.standard_normal((r, n)) if r else np.zeros((m, n))
+        u, s, vt = _call(lib, torch, a)
+        s_np = np.linalg.svd(a, compute_uv=False)
+        scale = max(1.0, s_np[0])
+        np.testing.assert_allclose(s, s_np, atol=1e-12 * scale)
+        np.testing.assert_allclose((u * s) @ vt, a, atol=1e-12 * scale)
+        np.testing.assert_allclose(u.T @ u, np.eye(k), atol=1e-12)
+        np.testing.assert_allclose(vt @ vt.T, np.eye(k), atol=1e-12)
+
+
+def test_noalloc_rejects_nonfinite_input(sps):
+    """NaN or Inf in the input returns SPS_ERR_NUMERIC (3), and the next call
+    on a finite matrix is unaffected."""
+    import torch
+    lib = sps._lib.load()
+    a = np.random.default_rng(3).standard_normal((30, 20))
+    for bad in (np.nan, np.inf):
+        b = a.copy()
+        b[4, 7] = bad
+        dev = torch.device("cuda:0")
+        t = torch.from_numpy(np.asfortranarray(b).T.copy()).to(dev)
+        out = [torch.zeros(n, dtype=torch.float64, device=dev) for n in (30 * 20, 20, 20 * 20)]
+        rc = lib.sps_la_svd_noalloc(0, None, 30, 20, C.c_void_p(t.data_ptr()), C.c_void_p(out[0].data_ptr()),
+                                    C.c_void_p(out[1].data_ptr()), C.c_void_p(out[2].data_ptr()))
+        assert rc == 3, rc
+    u, s, vt = _call(lib, torch, a)
+    np.testing.assert_allclose(s, np.linalg.svd(a, compute_uv=False), rtol=1e-12)
+
+
 def test_noalloc_rejects_sizes_beyond_the_array(sps):
     lib = sps._lib.load()
     assert lib.sps_la_svd_noalloc(0, None, 300, 10, C.c_void_p(1), C.c_void_p(1), C.c_void_p(1),
