@@ -141,3 +141,57 @@ def test_failure_on_one_rank_raises_on_all(sps):
     results = _spawn(2, fail_rank=1)
     assert [r[1] for r in results] == ["error", "error"]
     assert all("planted failure" in r[2] for r in results)
+
+
+class BatchedOracleOps(OracleOps):
+    """The drivers' batched ops (sample/project/measure/lognorm/evolution
+    batches), each a loop over the single oracle operation: exercises the
+    batched code path of run_stochastic on the CPU."""
+
+    def __init__(self, c):
+        super().__init__(c)
+        self.calls = {}
+
+    def _count(self, name, n):
+        self.calls[name] = self.calls.get(name, 0) + 1
+        assert n >= 1
+
+    def sample_batch(self, cache, uniforms):
+        self._count("sample_batch", len(uniforms))
+        return [self.sample(cache, u) for u in uniforms]
+
+    def project_batch(self, state, configurations):
+        self._count("project_batch", len(configurations))
+        return [self.project(state, c) for c in configurations]
+
+    def measure_energy_batch(self, states, method):
+        self._count("measure_energy_batch", len(states))
+        return [self.measure_energy(s, method) for s in states]
+
+    def lognorm_batch(self, states, method):
+        self._count("lognorm_batch", len(states))
+        return [self.lognorm(s, method) for s in states]
+
+    def evolution_step_batch(self, states, deltas, D, method, space):
+        self._count("evolution_step_batch", len(states))
+        return [self.evolution_step(s, d, D, method, space) for s, d in zip(states, deltas)]
+
+
+def test_batched_ops_match_single_ops(sps):
+    """run_stochastic through the batched ops: one call per phase (draws,
+    projections, observations, each evolution step), same result as the
+    single-operation path."""
+    serial = _run(sps)
+    c = _config(sps)
+    ops = BatchedOracleOps(c)
+    cp = sps.run_purification(c, ops=ops, identity=ops.identity)
+    res = sps.run_stochastic(c, cp, ops=ops)
+    assert ops.calls["sample_batch"] == 1
+    assert ops.calls["project_batch"] == 1
+    assert ops.calls["evolution_step_batch"] >= 1
+    for a, b in zip(res["observables"]["curve"], serial["observables"]["curve"]):
+        for k in ("beta", "energy_per_site", "lnZ", "eta"):
+            x, y = a[k], b[k]
+            assert (math.isnan(x) and math.isnan(y)) or abs(x - y) <= 1e-12 * max(1.0, abs(y))
+    assert [d["configuration"].tolist() for d in res["diagnostics"]["born_draws"]] == \
+        [d["configuration"].tolist() for d in serial["diagnostics"]["born_draws"]]
