@@ -133,6 +133,13 @@ int sps_la_svd_left(sps_handle* h, int32_t m, int32_t n, const double* a, double
  * (ld k); c m x n (ld m). */
 int sps_la_gemm(sps_handle* h, int32_t transpose_a, int32_t m, int32_t n, int32_t k, double alpha, const double* a,
                 const double* b, double beta, double* c, double* ms);
+/* No counterpart in the reference.  The low-precision contraction GEMM on
+ * the tcgen05 tensor cores (the kernel behind sps_set_precision), on dense
+ * row-major host matrices: c (m x n) = a (m x k) b (k x n) with operands
+ * rounded to TF32 (mode 1) or split into two TF32 (2) or two BF16 (3) parts,
+ * FP32 accumulation, FP64 result; ms = device time of pack + GEMM. */
+int sps_la_gemm_mixed(sps_handle* h, int32_t mode, int32_t m, int32_t n, int32_t k, const double* a,
+                      const double* b, double* c, double* ms);
 /* No counterpart in the reference.  Caps the cooperative launches of the
  * handle's own (serial) path at `ctas` CTAs each, 0 = the whole GPU: for a
  * handle that shares its GPU with other work.  sps_set_concurrency sets the
@@ -211,6 +218,26 @@ int sps_sample_probability(sps_handle* h, int32_t cache_id, const int32_t* confi
  * (1..16, default 1).  Each concurrent sample's cooperative launches use at
  * most 1/samples of the SMs. */
 int sps_set_concurrency(sps_handle* h, int32_t samples);
+/* No counterpart in the reference (it computes in Float64 throughout,
+ * src/states/finite.jl:80): the arithmetic of the large contraction GEMMs --
+ * row absorptions, row and slab steps, reduced metrics
+ * (boundary_mps.jl:136-151, :216-246; full_update.jl:151-172).
+ * mode 0 = FP64 (default); 1 = TF32, 2 = 3xTF32 (split operands, three
+ * products), 3 = 3xBF16 (split operands, three products), all three on the
+ * tcgen05 tensor cores with FP32 accumulation.  QR/SVD truncations, gauge
+ * and normalisation scales, log-weights and Born probability
+ * normalisations stay FP64 in every mode. */
+int sps_set_precision(sps_handle* h, int32_t mode);
+/* No counterpart in the reference.  enable != 0: launch shapes (the split-K
+ * slice count of the table-driven contraction, the tile width of the tcgen05
+ * GEMM) are picked by timing the candidates on the first call with a new
+ * shape; the choice is kept for the process and shared by every handle on the
+ * device.  Off by default (a choice changes the order of floating-point sums,
+ * so a tuned run can differ from an untuned one at rounding level).
+ * sps_autotune_report writes the table as JSON (key -> choice and the
+ * candidates' milliseconds). */
+int sps_set_autotune(sps_handle* h, int32_t enable);
+int sps_autotune_report(sps_handle* h, char* buf, size_t n);
 /* No counterpart in the reference: host-side failure injection for tests
  * (nothing faults on the device; the library takes its ordinary error
  * paths).  force_repair != 0 treats every full-update bond fit as triggered,

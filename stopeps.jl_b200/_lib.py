@@ -21,7 +21,8 @@ EXPORTS = [
     "sps_sample_batch", "sps_project", "sps_set_profile", "sps_kernel_stats_json", "sps_timer_start",
     "sps_timer_stop", "sps_la_svd", "sps_la_qr", "sps_la_svd_noalloc", "sps_la_svd_left", "sps_la_svd_topk", "sps_la_gemm", "sps_set_concurrency",
     "sps_set_sm_share", "sps_project_batch", "sps_evolution_step_batch", "sps_measure_energy_batch",
-    "sps_lognorm_batch", "sps_set_injection",
+    "sps_lognorm_batch", "sps_set_injection", "sps_set_precision", "sps_la_gemm_mixed",
+    "sps_set_autotune", "sps_autotune_report",
 ]
 
 STATUS = {0: "SPS_OK", 1: "SPS_ERR_ARGUMENT", 2: "SPS_ERR_CUDA", 3: "SPS_ERR_NUMERIC",
@@ -110,6 +111,10 @@ def load():
         "sps_lognorm_batch": ([vp, i32, P(i32), P(sps_boundary), P(sps_lognorm_result)], C.c_int),
         "sps_set_profile": ([vp, i32], C.c_int),
         "sps_set_injection": ([vp, i32, i32], C.c_int),
+        "sps_set_precision": ([vp, i32], C.c_int),
+        "sps_set_autotune": ([vp, i32], C.c_int),
+        "sps_autotune_report": ([vp, C.c_char_p, C.c_size_t], C.c_int),
+        "sps_la_gemm_mixed": ([vp, i32, i32, i32, i32, P(dbl), P(dbl), P(dbl), P(dbl)], C.c_int),
         "sps_kernel_stats_json": ([vp, C.c_char_p, C.c_size_t], C.c_int),
         "sps_timer_start": ([vp], C.c_int),
         "sps_timer_stop": ([vp, P(dbl)], C.c_int),

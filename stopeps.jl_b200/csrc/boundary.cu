@@ -302,7 +302,8 @@ Envs boundary_environments(Engine& E, const std::vector<Tensor>& layers, int Lx,
 Tensor layer_apply_wn(Engine& E, const Tensor& X, const Tensor& ket) {
   Tensor X5 = split(E, split(E, X, 2, {ket.legs[1], ket.legs[1]}), 0, {ket.legs[0], ket.legs[0]});   // w1 w2 b n1 n2 c
   Tensor Z;
-  if (!layer_wn_fused(E, X5, ket, Z)) {
+  // the fused kernel is FP64; a low-precision mode takes the two contractions
+  if (E.precision > 0 || !layer_wn_fused(E, X5, ket, Z)) {
     Tensor Y = ein(E, "xybuvc,xupaef->ybvcpaef", X5, ket);
     Z = ein(E, "ybvcpaef,yvpagh->bcegfh", Y, ket);
   }

@@ -127,6 +127,8 @@ void run_batch(sps_handle* h, int n, F&& fn) {
     h->workers.back()->ctas_cap = M.num_sms / h->concurrency;
     h->workers.back()->force_repair = M.force_repair;
     h->workers.back()->sweep_cap = M.sweep_cap;
+    h->workers.back()->precision = M.precision;
+    h->workers.back()->autotune = M.autotune;
     h->workers.back()->profile = M.profile;
   }
   cudaEvent_t start;
@@ -246,6 +248,29 @@ int sps_set_sm_share(sps_handle* h, int32_t ctas) {
   return guarded(h, [&] {
     if (ctas < 0 || ctas > h->E->num_sms) throw Error(SPS_ERR_ARGUMENT, "sps_set_sm_share: ctas must be in 0..SMs");
     h->E->ctas_cap = ctas;
+  });
+}
+
+int sps_set_precision(sps_handle* h, int32_t mode) {
+  return guarded(h, [&] {
+    if (mode < 0 || mode > 3) throw Error(SPS_ERR_ARGUMENT, "sps_set_precision: mode must be 0..3");
+    h->E->precision = mode;
+    for (auto& w : h->workers) w->precision = mode;
+  });
+}
+
+int sps_set_autotune(sps_handle* h, int32_t enable) {
+  return guarded(h, [&] {
+    h->E->autotune = enable != 0;
+    for (auto& w : h->workers) w->autotune = enable != 0;
+  });
+}
+
+int sps_autotune_report(sps_handle* h, char* buf, size_t n) {
+  return guarded(h, [&] {
+    const std::string js = tune::report_json();
+    if (!buf || js.size() + 1 > n) throw Error(SPS_ERR_ARGUMENT, "buffer too small");
+    std::memcpy(buf, js.c_str(), js.size() + 1);
   });
 }
 
@@ -472,6 +497,44 @@ int sps_la_gemm(sps_handle* h, int32_t transpose_a, int32_t m, int32_t n, int32_
     SPS_CUDA(cudaEventRecord(h->t1, E.stream));
     SPS_CUDA(cudaMemcpyAsync(c, dc, sizeof(double) * (size_t)m * n, cudaMemcpyDeviceToHost, E.stream));
     E.sync();
+    float f = 0;
+    SPS_CUDA(cudaEventElapsedTime(&f, h->t0, h->t1));
+    if (ms) *ms = f;
+  });
+}
+
+int sps_la_gemm_mixed(sps_handle* h, int32_t mode, int32_t m, int32_t n, int32_t k, const double* a,
+                      const double* b, double* c, double* ms) {
+  return guarded(h, [&] {
+    Engine& E = *h->E;
+    if (m < 1 || n < 1 || k < 1) throw Error(SPS_ERR_ARGUMENT, "sps_la_gemm_mixed: bad sizes");
+    if (mode < 1 || mode > 3) throw Error(SPS_ERR_ARGUMENT, "sps_la_gemm_mixed: mode must be 1..3");
+    Buf ba, bb, bc, t[6];
+    double* da = dev_copy(E, ba, a, (size_t)m * k);
+    double* db = dev_copy(E, bb, b, (size_t)k * n);
+    bc = E.alloc(sizeof(double) * (size_t)m * n);
+    double* dc = (double*)bc->ptr;
+    // row-major a (m x k), b (k x n), c (m x n) as offset tables
+    std::vector<int64_t> ra(m), ca(k), rb(k), cb(n), rc(m), cc(n);
+    for (int i = 0; i < m; ++i) ra[i] = (int64_t)i * k, rc[i] = (int64_t)i * n;
+    for (int i = 0; i < k; ++i) ca[i] = i, rb[i] = (int64_t)i * n;
+    for (int i = 0; i < n; ++i) cb[i] = i, cc[i] = i;
+    const int64_t* dra = E.upload_i64(ra, t[0]);
+    const int64_t* dca = E.upload_i64(ca, t[1]);
+    const int64_t* drb = E.upload_i64(rb, t[2]);
+    const int64_t* dcb = E.upload_i64(cb, t[3]);
+    const int64_t* drc = E.upload_i64(rc, t[4]);
+    const int64_t* dcc = E.upload_i64(cc, t[5]);
+    if (!h->t0) {
+      SPS_CUDA(cudaEventCreate(&h->t0));
+      SPS_CUDA(cudaEventCreate(&h->t1));
+    }
+    SPS_CUDA(cudaEventRecord(h->t0, E.stream));
+    tc::gemm_block(E, mode, da, dra, dca, 1, db, drb, dcb, 1, dc, drc, dcc, m, n, k, 1.0);
+    SPS_CUDA(cudaEventRecord(h->t1, E.stream));
+    SPS_CUDA(cudaMemcpyAsync(c, dc, sizeof(double) * (size_t)m * n, cudaMemcpyDeviceToHost, E.stream));
+    E.sync();
+    E.check_flag("sps_la_gemm_mixed");
     float f = 0;
     SPS_CUDA(cudaEventElapsedTime(&f, h->t0, h->t1));
     if (ms) *ms = f;

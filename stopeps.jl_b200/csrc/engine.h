@@ -13,6 +13,7 @@
 #pragma once
 #include <algorithm>
 #include <chrono>
+#include <functional>
 #include <unordered_map>
 #include <cuda_runtime.h>
 #include <cstdint>
@@ -160,6 +161,16 @@ class Engine {
     const int c = std::max(1, per_sm) * num_sms;
     return ctas_cap > 0 ? std::min(c, ctas_cap) : c;
   }
+
+  // pick launch shapes (split-K slices of the table-driven contraction, tile
+  // width of the tcgen05 GEMM) by timing the candidates on first use (tune::)
+  bool autotune = false;
+
+  // arithmetic of the large contraction GEMMs: 0 FP64 (tensor-core DMMA and
+  // table-driven kernels), 1 TF32, 2 3xTF32 (split), 3 3xBF16 (split), the last
+  // three on tcgen05 with FP32 accumulation (tcgemm.cu); factorizations,
+  // normalisations and log weights are FP64 in every mode
+  int precision = 0;
 
   // host-side failure injection (tests): sweep cap of the single-CTA Jacobi
   // SVD / eigh kernels (0: their default of 80) and a forced PSD repair of
@@ -334,6 +345,30 @@ struct HostTimer {
 // current device; occupancy (CTAs per SM) is cached per (device, kernel, smem).
 void set_max_dynamic_smem(const void* kernel, int bytes);
 int occupancy_per_sm(const void* kernel, int threads, size_t smem);
+
+// autotuner (autotune.cu): a process-wide table of launch-shape choices
+namespace tune {
+std::string key(Engine& E, const char* op, std::initializer_list<long long> shape);
+bool lookup(const std::string& key, int* choice);
+// the tuned choice for `key`: on a miss, times run(candidate) for each
+// candidate on the engine's stream (synchronising) and stores the fastest
+int pick(Engine& E, const std::string& key, const std::vector<int>& candidates, const std::function<void(int)>& run);
+std::string report_json();
+void clear();
+}  // namespace tune
+
+// tcgen05 contraction GEMM of one parity block (tcgemm.cu):
+// C[rc[i] + cc[j]] = alpha sum_k A[ra[i] + ca[k]] B[rb[k] + cb[j]] in the
+// low-precision mode `mode` (1 TF32, 2 3xTF32, 3 3xBF16) with FP32 accumulation
+namespace tc {
+void gemm_block(Engine& E, int mode, const double* A, const int64_t* ra, const int64_t* ca, int a_kfast,
+                const double* B, const int64_t* rb, const int64_t* cb, int b_jfast, double* C, const int64_t* rc,
+                const int64_t* cc, int M, int N, int K, double alpha);
+// a block worth the pack + tensor-core route
+inline bool worth(int M, int N, int K) {
+  return M >= 64 && N >= 32 && K >= 32 && 2.0 * M * N * (double)K >= 3.2e7;
+}
+}  // namespace tc
 
 // gather/scatter between tensors and dense column-major block matrices
 void gather_block(Engine& E, const Tensor& A, const int64_t* rt, const int64_t* ct, int M, int N,

@@ -1070,6 +1070,28 @@ Tensor ein(Engine& E, const std::string& spec, const Tensor& A, const Tensor& B,
     probs.push_back(P);
   }
   if (probs.empty()) return C;
+  if (E.precision > 0) {
+    // low-precision mode: large blocks on the tcgen05 GEMM, the rest stays FP64
+    std::vector<GemmProb> small;
+    for (auto& P : probs) {
+      if (tc::worth(P.M, P.N, P.K)) {
+        tc::gemm_block(E, E.precision, P.A, P.ra, P.ca, P.a_kfast, P.B, P.rb, P.cb, P.b_jfast, P.C, P.rc, P.cc, P.M,
+                       P.N, P.K, alpha);
+        E.flops -= 2.0 * P.M * P.N * P.K;   // counted once, by gemm_block
+      } else {
+        small.push_back(P);
+      }
+    }
+    if (small.empty()) return C;
+    if (small.size() != probs.size()) {
+      probs = small;
+      maxM = maxN = 0;
+      for (auto& P : probs) {
+        maxM = std::max(maxM, P.M);
+        maxN = std::max(maxN, P.N);
+      }
+    }
+  }
   // split the contraction when the output tiles alone leave most SMs idle
   // and every slice keeps at least 4 k-steps
   const int tiles = ((maxN + TN - 1) / TN) * ((maxM + TM - 1) / TM);
@@ -1079,10 +1101,20 @@ Tensor ein(Engine& E, const std::string& spec, const Tensor& A, const Tensor& B,
   int S = 1;
   if (maxK >= 8 * TK && tiles * nprob < E.num_sms)
     S = std::min((maxK + 4 * TK - 1) / (4 * TK), (E.num_sms + tiles * nprob - 1) / (tiles * nprob));
+  // candidate slice counts for the autotuner: the heuristic's, half and double
+  // it, and no split; every slice keeps at least two k-steps
+  std::vector<int> cands;
+  int Smax = S;
+  if (E.autotune && maxK >= 4 * TK) {
+    const int cap = std::max(1, maxK / (2 * TK));
+    for (int c : {1, std::max(1, S / 2), S, 2 * S})
+      if (c <= cap && std::find(cands.begin(), cands.end(), c) == cands.end()) cands.push_back(c);
+    for (int c : cands) Smax = std::max(Smax, c);
+  }
   Buf ws;
-  if (S > 1) {
+  if (Smax > 1) {
     size_t wsz = 0;
-    for (auto& P : probs) wsz += (size_t)S * P.M * P.N;
+    for (auto& P : probs) wsz += (size_t)Smax * P.M * P.N;
     ws = E.alloc(wsz * sizeof(double));
     const size_t slots = (size_t)tiles * nprob;
     if (slots > E.gg_counter_slots) {   // zeroed once; the kernels leave them zero
@@ -1093,12 +1125,20 @@ Tensor ein(Engine& E, const std::string& spec, const Tensor& A, const Tensor& B,
     size_t off = 0;
     for (int p = 0; p < nprob; ++p) {
       probs[p].ws = (double*)ws->ptr + off;
-      off += (size_t)S * probs[p].M * probs[p].N;
+      off += (size_t)Smax * probs[p].M * probs[p].N;
       probs[p].cnt = (int*)E.gg_counters->ptr + (size_t)p * tiles;
     }
   }
   Buf kp = E.alloc(probs.size() * sizeof(GemmProb));
   E.stage(probs.data(), probs.size() * sizeof(GemmProb), kp->ptr);
+  if (cands.size() > 1) {
+    const std::string key = tune::key(E, "gemm_gather.split", {maxM, maxN, maxK, nprob});
+    S = tune::pick(E, key, cands, [&](int c) {
+      dim3 g((maxN + TN - 1) / TN, (maxM + TM - 1) / TM, (unsigned)(probs.size() * c));
+      gemm_gather_kernel<<<g, GT, 0, E.stream>>>((const GemmProb*)kp->ptr, alpha, c);
+      SPS_CUDA(cudaGetLastError());
+    });
+  }
   dim3 grid((maxN + TN - 1) / TN, (maxM + TM - 1) / TM, (unsigned)(probs.size() * S));
   double fl = 0, by = 0;
   for (auto& P : probs) {

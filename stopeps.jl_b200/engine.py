@@ -9,6 +9,7 @@ work runs in ``libstopeps_gpu.so``; there is no host fallback.
 from __future__ import annotations
 
 import ctypes as C
+import json
 import math
 
 import numpy as np
@@ -83,6 +84,27 @@ class Engine:
         """Cap this handle's own cooperative launches at ``ctas`` CTAs each (0: the whole GPU)."""
         self.check(self.lib.sps_set_sm_share(self.h, int(ctas)))
 
+    PRECISIONS = {"fp64": 0, "tf32": 1, "3xtf32": 2, "3xbf16": 3}
+
+    def set_precision(self, mode="fp64"):
+        """Arithmetic of the large contraction GEMMs: "fp64" (default), or on the
+        tcgen05 tensor cores with FP32 accumulation "tf32", "3xtf32" (split
+        operands) or "3xbf16" (split operands); factorizations, normalisations
+        and log-weights stay FP64."""
+        if mode not in self.PRECISIONS:
+            raise ValueError(f"unknown precision {mode!r}; one of {sorted(self.PRECISIONS)}")
+        self.check(self.lib.sps_set_precision(self.h, self.PRECISIONS[mode]))
+
+    def set_autotune(self, enable=True):
+        """Pick launch shapes (split-K slices, tcgen05 tile width) by timing the
+        candidates on first use; the choices are shared process-wide."""
+        self.check(self.lib.sps_set_autotune(self.h, 1 if enable else 0))
+
+    def autotune_report(self) -> dict:
+        buf = C.create_string_buffer(1 << 20)
+        self.check(self.lib.sps_autotune_report(self.h, buf, 1 << 20))
+        return json.loads(buf.value.decode())
+
     def set_injection(self, force_repair=False, svd_sweep_cap=0):
         """Host-side failure injection for tests: force the PSD-repair branch of
         every bond update; cap the small-block Jacobi sweeps (0 = default)."""
@@ -144,6 +166,20 @@ class Engine:
         ms = C.c_double()
         self.check(self.lib.sps_la_gemm(self.h, int(transpose_a), m, n, k, float(alpha), _arr(a, C.c_double),
                                         _arr(b, C.c_double), float(beta), _arr(c, C.c_double), C.byref(ms)))
+        return c, ms.value
+
+    def la_gemm_mixed(self, a, b, mode="3xtf32"):
+        """tcgen05 GEMM a @ b in a low-precision mode ("tf32", "3xtf32", "3xbf16"): (c, device_ms)."""
+        a = np.ascontiguousarray(np.asarray(a, np.float64))
+        b = np.ascontiguousarray(np.asarray(b, np.float64))
+        m, k = a.shape
+        k2, n = b.shape
+        if k != k2:
+            raise ValueError("inner dimensions differ")
+        c = np.zeros((m, n))
+        ms = C.c_double()
+        self.check(self.lib.sps_la_gemm_mixed(self.h, self.PRECISIONS[mode], m, n, k, _arr(a, C.c_double),
+                                              _arr(b, C.c_double), _arr(c, C.c_double), C.byref(ms)))
         return c, ms.value
 
     def la_svd_topk(self, a, k, gram=False, rtol=0.0):
