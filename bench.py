@@ -52,7 +52,10 @@ PROBES = """probes (one hot operation on a representative input, run once to war
   draw              one Born draw, 8x8 D=6 chi=36, exact compression (synthetic PEPO)
   zipdraw           the same draw with the zip-up absorption
   scale             zip-up draws at 12x12 D=8 chi=64 (32+32): 1 and 4 at a time
-  fustep [L]        one full-update Trotter step, L x L D=6 chi=36 (default 8), both absorptions"""
+  fustep [L]        one full-update Trotter step + energy, L x L D=6 chi=36 (default 8): both absorptions,
+                    FP64 and 3xTF32 contractions
+  purify [L] [s] [p] purification of the L x L TFIM to beta0 = 0.4 at D=6 chi=36 within s seconds
+                    (precision p), the state saved under gpurun_out/"""
 
 
 def parse():
@@ -396,7 +399,11 @@ def ours_arm(args, rank, world, local_rank):
 
     pipeline = None
     if not args.no_pipeline:
-        pipeline = pipeline_timing(sps, e, st, zip_run["draws"], W, space, np, torch, local_rank, dist)
+        try:
+            pipeline = pipeline_timing(sps, e, st, zip_run["draws"], W, space, np, torch, local_rank, dist)
+        except Exception as ex:   # reported in the line; the draw measurement stands on its own
+            e.set_concurrency(1)
+            pipeline = {"error": f"{type(ex).__name__}: {ex}"}
 
     result = None
     if rank == 0:
@@ -569,28 +576,75 @@ def probe(argv):
         print(f"{2 * w} draws {w} at a time: {dt:.3f} s, {2 * w / dt:.2f} samples/s")
         e.set_concurrency(1)
     elif which == "fustep":
+        # one full-update Trotter step of a projected sample and one energy measurement,
+        # L x L D=6 chi=36: both absorptions, FP64 and the split-TF32 contractions
         Ls = int(argv[1]) if len(argv) > 1 else LX
+        e = sps.Engine(Ls, Ls, sps.TFIM(1.0, H_FIELD))
+        sites, dims = sps.synthetic.synthetic_pepo(Ls, Ls, D, PEPO_EPS, PEPO_SEED)
+        st = e.upload_state(sites, dims, True, beta=BETA0)
+        sps.normalize_state(st)
+        cfg = sps.sample_configuration(sps.SamplingCache(st, sps.BoundaryMPSZipUp(CHI, sps.Z2Space(CHI // 2, CHI // 2))),
+                                       uniforms=sps.sample_uniforms(SEED, 1, Ls * Ls))["configuration"]
         for zipup in (True, False):
-            e = sps.Engine(Ls, Ls, sps.TFIM(1.0, H_FIELD))
-            sites, dims = sps.synthetic.synthetic_pepo(Ls, Ls, D, PEPO_EPS, PEPO_SEED)
-            st = e.upload_state(sites, dims, True, beta=BETA0)
-            sps.normalize_state(st)
-            ps, _ = sps.project_configuration(st, np.ones((Ls, Ls), np.int32))
-            kind = sps.BoundaryMPSZipUp if zipup else sps.BoundaryMPS
-            m = kind(CHI, sps.Z2Space(CHI // 2, CHI // 2))
-            e.set_profile(True)
+            for prec in ("fp64", "3xtf32"):
+                kind = sps.BoundaryMPSZipUp if zipup else sps.BoundaryMPS
+                m = kind(CHI, sps.Z2Space(CHI // 2, CHI // 2))
+                ps, _ = sps.project_configuration(st, cfg)
+                e.set_precision(prec)
+                tag = f"{Ls}x{Ls} {'zip-up' if zipup else 'exact'} {prec}"
+                try:
+                    e.set_profile(True)
+                    t = time.perf_counter()
+                    r = sps.evolution_step(ps, DTAU, D, m, sps.Z2Space(D // 2, D // 2))
+                    dt = time.perf_counter() - t
+                    top = sorted(e.kernel_stats().items(), key=lambda kv: -kv[1]["ms"])[:8]
+                    e.set_profile(False)
+                    t = time.perf_counter()
+                    en = sps.measure_energy(ps, m)
+                    dm = time.perf_counter() - t
+                    print(f"{tag}: FU step {dt:.2f} s, bond updates {r['bond_updates']}, repairs {r['repairs']}, "
+                          f"stops {[r['stop_' + k] for k in ('error_tolerance', 'iteration_limit', 'residual_fallback', 'disabled')]}, "
+                          f"measure_energy {dm:.2f} s (E {en['energy_per_site']:.10f}); "
+                          + ", ".join(f"{k} {v['ms']:.0f} ms" for k, v in top), flush=True)
+                except Exception as ex:
+                    e.set_profile(False)
+                    print(f"{tag}: {type(ex).__name__}: {ex}", flush=True)
+                e.set_precision("fp64")
+                del ps
+        e.close()
+    elif which == "purify":
+        # run_purification of the L x L TFIM (h = 3.0) at D=6 chi=36 to beta0 = 0.4 (tau = 0.02), one
+        # evolution step at a time within a wall-clock budget; the state reached is saved
+        Ls = int(argv[1]) if len(argv) > 1 else LX
+        budget = float(argv[2]) if len(argv) > 2 else 600.0
+        prec = argv[3] if len(argv) > 3 else "fp64"
+        e = sps.Engine(Ls, Ls, sps.TFIM(1.0, H_FIELD))
+        e.set_precision(prec)
+        st = e.identity_pepo()
+        sps.normalize_state(st)
+        m = sps.BoundaryMPS(CHI, sps.Z2Space(CHI // 2, CHI // 2))
+        t0 = time.perf_counter()
+        for beta in sps.step_schedule(0.0, BETA0, DTAU):
             t = time.perf_counter()
-            r = sps.evolution_step(ps, DTAU, D, m, sps.Z2Space(D // 2, D // 2))
-            dt = time.perf_counter() - t
-            top = sorted(e.kernel_stats().items(), key=lambda kv: -kv[1]["ms"])[:8]
-            e.set_profile(False)
-            t = time.perf_counter()
-            en = sps.measure_energy(ps, m)
-            dm = time.perf_counter() - t
-            print(f"{Ls}x{Ls} {'zip-up' if zipup else 'exact'} environments: FU step {dt:.2f} s, bond updates "
-                  f"{r['bond_updates']}, measure_energy {dm:.2f} s (E {en['energy_per_site']:.8f}); "
-                  + ", ".join(f"{k} {v['ms']:.0f} ms" for k, v in top), flush=True)
-            e.close()
+            try:
+                r = sps.evolution_step(st, (beta - st.beta) / 2, D, m, sps.Z2Space(D // 2, D // 2))
+            except Exception as ex:
+                print(f"beta {beta}: {type(ex).__name__}: {ex}", flush=True)
+                break
+            st.beta = beta
+            print(f"beta {beta:.2f}: {time.perf_counter() - t:.2f} s, repairs {r['repairs']}, "
+                  f"max state truncation {r['max_state_truncation']:.3e}, env truncation "
+                  f"{r['max_environment_truncation']:.3e}", flush=True)
+            if time.perf_counter() - t0 > budget:
+                break
+        sites, dims = st.download()
+        os.makedirs(os.path.join(ROOT, "gpurun_out"), exist_ok=True)
+        np.savez_compressed(os.path.join(ROOT, "gpurun_out", f"purified_{Ls}x{Ls}_D{D}_{prec}.npz"),
+                            data=np.concatenate([np.asarray(a).reshape(-1) for a in sites]), dims=np.asarray(dims),
+                            beta=st.beta, log_amplitude=st.log_amplitude)
+        en = sps.measure_energy(st, m)
+        print(f"beta {st.beta}: E per site {en['energy_per_site']:.12f}, lnZ {en['log_norm']:.12f}, "
+              f"total {time.perf_counter() - t0:.1f} s", flush=True)
     else:
         raise SystemExit(f"unknown probe {which}\n{PROBES}")
 

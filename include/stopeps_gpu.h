@@ -245,8 +245,11 @@ int sps_autotune_report(sps_handle* h, char* buf, size_t n);
  * 490-501) on well-conditioned input; svd_sweep_cap > 0 caps the sweeps of
  * the single-CTA Jacobi SVD and eigh kernels, which then report
  * SPS_ERR_CONVERGENCE (the non-convergence status of _retry_svd,
- * src/states/svd.jl:2-33); 0 restores the default cap of 80. */
-int sps_set_injection(sps_handle* h, int32_t force_repair, int32_t svd_sweep_cap);
+ * src/states/svd.jl:2-33); 0 restores the default cap of 80.
+ * multi_cta_eigh_min > 0: parity blocks of the PSD repair's eigendecomposition
+ * with at least that many rows take the multi-CTA route (one-sided Jacobi of
+ * the shifted hole); 0 restores the default of 1024. */
+int sps_set_injection(sps_handle* h, int32_t force_repair, int32_t svd_sweep_cap, int32_t multi_cta_eigh_min);
 /* n draws in one call (the MPI sample loop of src/driver/run.jl:45-49 on one device);
  * reports (n) may be NULL. */
 int sps_sample_batch(sps_handle* h, int32_t cache_id, int32_t n, const double* uniforms,

@@ -110,7 +110,7 @@ def load():
         "sps_measure_energy_batch": ([vp, i32, P(i32), P(sps_boundary), P(sps_energy), P(dbl)], C.c_int),
         "sps_lognorm_batch": ([vp, i32, P(i32), P(sps_boundary), P(sps_lognorm_result)], C.c_int),
         "sps_set_profile": ([vp, i32], C.c_int),
-        "sps_set_injection": ([vp, i32, i32], C.c_int),
+        "sps_set_injection": ([vp, i32, i32, i32], C.c_int),
         "sps_set_precision": ([vp, i32], C.c_int),
         "sps_set_autotune": ([vp, i32], C.c_int),
         "sps_autotune_report": ([vp, C.c_char_p, C.c_size_t], C.c_int),

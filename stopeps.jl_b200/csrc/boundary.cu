@@ -475,8 +475,167 @@ static int categorical(const std::vector<double>& lm, double u, int* near) {
   return last;
 }
 
+// One Born conditional on the device (born.jl:130-151 with _categorical,
+// selection.jl:68-80): raw[0..1] are the two candidates' scalars.  Validity
+// checks, normalisation, the categorical choice with the site's uniform, the
+// log-probability and the conditional are computed by one thread; the choice
+// goes to cfg[site] (label 1/2) and *sel (0/1).  err[0] records the first
+// failure (1 invalid conditional, 2 zero total mass) and err[1] its site;
+// once set, later sites only copy their choice so that the draw stays
+// well-defined until the host reads the flag at the end of the row.
+__global__ void born_step_kernel(const double* raw, const double* u, int site, int* cfg, int* sel, double* logp,
+                                 double* cond, int* err, int* near) {
+  if (threadIdx.x != 0) return;
+  const double r0 = raw[0], r1 = raw[1];
+  const double scale = fmax(fabs(r0), fabs(r1));
+  int k = 0;
+  if (err[0] == 0) {
+    const bool bad = !(isfinite(r0) && r0 >= -64 * DBL_EPSILON * scale) ||
+                     !(isfinite(r1) && r1 >= -64 * DBL_EPSILON * scale);
+    const double v0 = fmax(r0, 0.0), v1 = fmax(r1, 0.0), total = v0 + v1;
+    if (bad || !(total > 0)) {
+      err[0] = bad ? 1 : 2;
+      err[1] = site;
+    } else {
+      const double p[2] = {v0 / total, v1 / total};
+      const double lm[2] = {p[0] > 0 ? log(p[0]) : -INFINITY, p[1] > 0 ? log(p[1]) : -INFINITY};
+      const double pivot = fmax(lm[0], lm[1]);
+      double ssum = 0;
+      for (int j = 0; j < 2; ++j) ssum += exp(lm[j] - pivot);
+      const double z = pivot + log(ssum);
+      double cum = 0;
+      int last = -1;
+      k = -1;
+      for (int j = 0; j < 2; ++j) {
+        if (lm[j] == -INFINITY) continue;
+        last = j;
+        cum += exp(lm[j] - z);
+        if (fabs(u[site] - cum) < 1e-12) ++*near;
+        if (u[site] < cum) {
+          k = j;
+          break;
+        }
+      }
+      if (k < 0) k = last;
+      cond[site] = p[k];
+      *logp += log(p[k]);
+    }
+  }
+  cfg[site] = k + 1;
+  *sel = k;
+}
+
+// out = sel ? b : a, elementwise (a and b share one layout)
+__global__ void select2_kernel(const double* __restrict__ a, const double* __restrict__ b, const int* sel,
+                               double* __restrict__ out, int64_t n) {
+  const double* src = *sel ? b : a;
+  for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x)
+    out[i] = src[i];
+}
+
+// A draw from uniforms with the conditionals decided on the device: the
+// contractions of a row are queued without a host round trip per site (the
+// chosen candidate's step becomes the next left environment by a device-side
+// select), and the host synchronises once per row to learn the row's
+// choices, which fix the tensors of the row's absorption.  Same arithmetic
+// and order as the host path below.
+static SampleResult sample_device(Engine& E, const SamplingCache& c, const double* uniforms) {
+  const int Lx = c.Lx, Ly = c.Ly, L = Lx * Ly;
+  SampleResult res;
+  res.config.assign(L, 0);
+  Buf ib = E.alloc(sizeof(int) * (L + 8));
+  Buf db = E.alloc(sizeof(double) * (2 * (size_t)L + 8));
+  int* dcfg = (int*)ib->ptr;
+  int* derr = dcfg + L;      // 2 ints
+  int* dnear = derr + 2;
+  int* dsel = derr + 3;
+  double* dlogp = (double*)db->ptr;
+  double* dcond = dlogp + 1;
+  double* du = dcond + L;
+  SPS_CUDA(cudaMemsetAsync(ib->ptr, 0, sizeof(int) * (L + 8), E.stream));
+  SPS_CUDA(cudaMemsetAsync(db->ptr, 0, sizeof(double) * (L + 1), E.stream));
+  E.stage(uniforms, sizeof(double) * L, du);
+  Env north = trivial_boundary(E, column(c.layers, Lx, 0), true);
+  double maxtr = 0;
+  for (auto& e : c.south) maxtr = std::max(maxtr, e.max_trunc);
+  // row choices + err[2] + near, clear of the log-probability and conditionals at the front
+  int* hrow = reinterpret_cast<int*>(E.hscal + Engine::NSCAL - 64);
+  for (int y = 0; y < Ly; ++y) {
+    std::vector<Layer> row(Lx);
+    std::vector<Tensor> rowt = column(c.layers, Lx, y);
+    for (int x = 0; x < Lx; ++x) {
+      row[x].a = rowt[x];
+      row[x].ket = c.state_ref->sites[x + y * Lx];
+      row[x].layered = true;
+    }
+    const auto& top = north.t;
+    const auto& bottom = c.south[y + 1].t;
+    RowEnvs e = row_environments(E, top, row, bottom, 2);
+    Tensor left = e.left[0];
+    for (int x = 0; x < Lx; ++x) {
+      const int site = x + y * Lx;
+      Tensor LT = ein(E, "awb,anc->wbnc", left, top[x]);
+      Tensor step[2];
+      for (int k = 0; k < 2; ++k) {
+        Tensor Y = layer_apply_wn(E, LT, c.candidate_kets[site][k]);
+        step[k] = ein(E, "bces,bsd->ced", Y, bottom[x]);
+        dot_to(E, step[k], e.right[x + 1], 10 + k);
+      }
+      born_step_kernel<<<1, 32, 0, E.stream>>>(E.dscal + 10, du, site, dcfg, dsel, dlogp, dcond, derr, dnear);
+      SPS_CUDA(cudaGetLastError());
+      E.launches++;
+      if (x < Lx - 1) {
+        if (!step[0].contiguous() || !step[1].contiguous() || step[0].dims != step[1].dims)
+          throw Error(SPS_ERR_ARGUMENT, "sample_configuration: candidate steps differ in layout");
+        Tensor nl = E.empty(step[0].legs);
+        const int64_t n = nl.size();
+        select2_kernel<<<(int)std::min<int64_t>((n + 255) / 256, 1024), 256, 0, E.stream>>>(
+            step[0].ptr(), step[1].ptr(), dsel, nl.ptr(), n);
+        SPS_CUDA(cudaGetLastError());
+        E.launches++;
+        left = nl;
+        safe_scale_inplace(E, left);
+      }
+    }
+    // the row's choices (and the first failure) to the host: one synchronisation per row
+    SPS_CUDA(cudaMemcpyAsync(hrow, dcfg + y * Lx, sizeof(int) * Lx, cudaMemcpyDeviceToHost, E.stream));
+    SPS_CUDA(cudaMemcpyAsync(hrow + Lx, derr, sizeof(int) * 3, cudaMemcpyDeviceToHost, E.stream));
+    E.sync();
+    if (hrow[Lx] != 0) {
+      SPS_CUDA(cudaMemsetAsync(E.dflag, 0, sizeof(int), E.stream));   // flags raised by the draw after the failure
+      const int s = hrow[Lx + 1];
+      const std::string where = "(" + std::to_string(s % Lx + 1) + "," + std::to_string(s / Lx + 1) + ")";
+      if (hrow[Lx] == 1)
+        throw Error(SPS_ERR_BORN, "invalid Born conditional at " + where + "; increase chi_sampling");
+      throw Error(SPS_ERR_BORN, "Born conditional has zero total mass at " + where);
+    }
+    E.check_flag("sample_configuration");
+    std::vector<Tensor> rt(Lx), rk(Lx);
+    for (int x = 0; x < Lx; ++x) {
+      const int k = hrow[x] - 1;
+      if (k < 0 || k > 1) throw Error(SPS_ERR_NUMERIC, "sample_configuration: no candidate chosen");
+      res.config[x + y * Lx] = k + 1;
+      rt[x] = c.candidates[x + y * Lx][k];
+      rk[x] = c.candidate_kets[x + y * Lx][k];
+    }
+    if (y == Ly - 1) {   // log-probability, conditionals and near-boundary count with the last row
+      SPS_CUDA(cudaMemcpyAsync(E.hscal, dlogp, sizeof(double) * (L + 1), cudaMemcpyDeviceToHost, E.stream));
+      E.sync();
+      res.log_probability = E.hscal[0];
+      res.conditionals.assign(E.hscal + 1, E.hscal + 1 + L);
+      res.near_boundary = hrow[Lx + 2];
+    }
+    north = absorb(E, north, rt, c.method, true, nullptr, y + 1, &rk);
+    maxtr = std::max(maxtr, north.max_trunc);
+  }
+  res.max_env_trunc = maxtr;
+  return res;
+}
+
 SampleResult sample_configuration(Engine& E, const SamplingCache& c, const double* uniforms,
                                   const int* configuration) {
+  if (uniforms && !configuration && c.Lx * c.Ly + 1 <= Engine::NSCAL - 64 && c.Lx + 3 <= 128)
+    return sample_device(E, c, uniforms);
   const int Lx = c.Lx, Ly = c.Ly;
   SampleResult res;
   res.config.assign(Lx * Ly, 0);

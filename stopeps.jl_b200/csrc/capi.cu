@@ -127,6 +127,7 @@ void run_batch(sps_handle* h, int n, F&& fn) {
     h->workers.back()->ctas_cap = M.num_sms / h->concurrency;
     h->workers.back()->force_repair = M.force_repair;
     h->workers.back()->sweep_cap = M.sweep_cap;
+    h->workers.back()->eigh_multi_min = M.eigh_multi_min;
     h->workers.back()->precision = M.precision;
     h->workers.back()->autotune = M.autotune;
     h->workers.back()->profile = M.profile;
@@ -274,14 +275,17 @@ int sps_autotune_report(sps_handle* h, char* buf, size_t n) {
   });
 }
 
-int sps_set_injection(sps_handle* h, int32_t force_repair, int32_t svd_sweep_cap) {
+int sps_set_injection(sps_handle* h, int32_t force_repair, int32_t svd_sweep_cap, int32_t multi_cta_eigh_min) {
   return guarded(h, [&] {
-    if (svd_sweep_cap < 0) throw Error(SPS_ERR_ARGUMENT, "sps_set_injection: negative sweep cap");
+    if (svd_sweep_cap < 0 || multi_cta_eigh_min < 0) throw Error(SPS_ERR_ARGUMENT, "sps_set_injection: negative value");
+    const int em = multi_cta_eigh_min > 0 ? multi_cta_eigh_min : 1024;
     h->E->force_repair = force_repair != 0;
     h->E->sweep_cap = svd_sweep_cap;
+    h->E->eigh_multi_min = em;
     for (auto& w : h->workers) {
       w->force_repair = force_repair != 0;
       w->sweep_cap = svd_sweep_cap;
+      w->eigh_multi_min = em;
     }
   });
 }

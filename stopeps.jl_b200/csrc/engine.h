@@ -177,6 +177,10 @@ class Engine {
   // every full-update bond
   int sweep_cap = 0;
   bool force_repair = false;
+  // eigendecompositions of blocks with at least this many rows in the PSD
+  // repair take the multi-CTA route (eigh_unit_shifted); smaller ones the
+  // single-CTA Jacobi eigh
+  int eigh_multi_min = 1024;
 
   // starting iteration count of the subspace-iteration SVD (adapted per call)
   int topk_hint = 6;
@@ -277,6 +281,12 @@ struct EIGres {
   Tensor V;                   // (rows..., new)
 };
 EIGres eigh(Engine& E, const Tensor& A, const std::vector<int>& rows, const std::vector<int>& cols);
+// eigendecomposition of a symmetric block matrix whose spectral norm is at
+// most 1 (e.g. Frobenius-normalised), for blocks too large for the single-CTA
+// eigh: the one-sided Jacobi SVD (multi-CTA) of A + I, which is positive
+// semidefinite, so its singular pairs are its eigenpairs; w = sigma - 1
+// (descending per block), V the singular vectors
+EIGres eigh_unit_shifted(Engine& E, const Tensor& A, const std::vector<int>& rows, const std::vector<int>& cols);
 // block inverse of a square 2-leg tensor (out,in) -> (in,out)
 Tensor block_inverse(Engine& E, const Tensor& R);
 // multiply a leg by a per-state diagonal (values in leg order) : A[..k..] *= d[k]

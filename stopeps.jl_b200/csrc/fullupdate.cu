@@ -442,8 +442,12 @@ static Tensor positive_reduced_metric(Engine& E, const BondEnv& env, const Tenso
   Tensor Hm = contiguous(E, perm_view(H, bk));                     // (bras..., kets...)
   Tensor HmT = perm_view(Hm, {6, 7, 8, 9, 10, 11, 0, 1, 2, 3, 4, 5});
   double f = scale != 0 ? 0.5 / scale : 0.5;
-  Tensor Hs = axpby(E, f, Hm, f, HmT);
-  EIGres eg = eigh(E, Hs, {0, 1, 2, 3, 4, 5}, {6, 7, 8, 9, 10, 11});
+  Tensor Hs = axpby(E, f, Hm, f, HmT);   // symmetric, Frobenius norm <= 1
+  const std::vector<int> bras{0, 1, 2, 3, 4, 5}, kets{6, 7, 8, 9, 10, 11};
+  int64_t half = 1;
+  for (int k = 0; k < 6; ++k) half *= Hs.dims[k];
+  // the parity blocks hold about half the fused states each
+  EIGres eg = (half / 2 >= E.eigh_multi_min) ? eigh_unit_shifted(E, Hs, bras, kets) : eigh(E, Hs, bras, kets);
   std::vector<double> wpos;
   for (int c = 0; c < 2; ++c)
     for (double v : eg.w[c]) wpos.push_back(v > 0 ? v : 0.0);

@@ -1352,6 +1352,41 @@ static std::vector<char> select_truncation(const std::vector<double> s[2], const
   return {};
 }
 
+// Device value arrays to the host after one synchronisation: through the
+// pinned scalar scratch when they fit, else by plain copies after the sync.
+// The device flag is checked (and raised as an error) on the way.
+static std::vector<std::vector<double>> read_values(Engine& E, const std::vector<std::pair<const double*, int>>& src,
+                                                    const char* where) {
+  size_t total = 0;
+  for (auto& x : src) total += (size_t)x.second;
+  std::vector<std::vector<double>> out(src.size());
+  if (total <= (size_t)Engine::NSCAL) {
+    size_t off = 0;
+    for (auto& x : src) {
+      if (x.second > 0)
+        SPS_CUDA(cudaMemcpyAsync(E.hscal + off, x.first, sizeof(double) * x.second, cudaMemcpyDeviceToHost,
+                                 E.stream));
+      off += x.second;
+    }
+    E.sync();
+    E.check_flag(where);
+    off = 0;
+    for (size_t i = 0; i < src.size(); ++i) {
+      out[i].assign(E.hscal + off, E.hscal + off + src[i].second);
+      off += src[i].second;
+    }
+  } else {
+    E.sync();
+    E.check_flag(where);
+    for (size_t i = 0; i < src.size(); ++i) {
+      out[i].resize(src[i].second);
+      if (src[i].second > 0)
+        SPS_CUDA(cudaMemcpy(out[i].data(), src[i].first, sizeof(double) * src[i].second, cudaMemcpyDeviceToHost));
+    }
+  }
+  return out;
+}
+
 SVDres svd(Engine& E, const Tensor& A, const std::vector<int>& rows, const std::vector<int>& cols,
            const Trunc& tr, bool want_entropy) {
   BlockTables bt = tables_of(A, rows, cols);
@@ -1385,21 +1420,11 @@ SVDres svd(Engine& E, const Tensor& A, const std::vector<int>& rows, const std::
   SVDres res;
   std::vector<double> sv[2];
   // copy singular values back
-  int off = 0;
-  for (int c = 0; c < 2; ++c) {
-    if (dmap[c] < 0) continue;
-    SPS_CUDA(cudaMemcpyAsync(E.hscal + off, ds[dmap[c]].s, sizeof(double) * k[c], cudaMemcpyDeviceToHost,
-                             E.stream));
-    off += k[c];
-  }
-  if (off > Engine::NSCAL) throw Error(SPS_ERR_ARGUMENT, "svd: too many singular values");
-  E.sync();
-  E.check_flag("svd");
-  off = 0;
-  for (int c = 0; c < 2; ++c) {
-    if (dmap[c] < 0) continue;
-    sv[c].assign(E.hscal + off, E.hscal + off + k[c]);
-    off += k[c];
+  {
+    std::vector<std::pair<const double*, int>> src;
+    for (int c = 0; c < 2; ++c) src.push_back({dmap[c] < 0 ? nullptr : ds[dmap[c]].s, dmap[c] < 0 ? 0 : k[c]});
+    auto v = read_values(E, src, "svd");
+    for (int c = 0; c < 2; ++c) sv[c] = std::move(v[c]);
   }
   double tot2 = 0;
   for (int c = 0; c < 2; ++c)
@@ -1698,20 +1723,11 @@ KeptSVD svd_kept(Engine& E, const Tensor& A, const std::vector<int>& rows, const
   la::jacobi_left(E, jac);
   // singular values to the host
   std::vector<double> sv[2];
-  int off = 0;
-  for (int c = 0; c < 2; ++c) {
-    if (jmap[c] < 0) continue;
-    SPS_CUDA(cudaMemcpyAsync(E.hscal + off, w[c].s, sizeof(double) * k[c], cudaMemcpyDeviceToHost, E.stream));
-    off += k[c];
-  }
-  if (off > Engine::NSCAL) throw Error(SPS_ERR_ARGUMENT, "svd_kept: too many singular values");
-  E.sync();
-  E.check_flag("svd_kept");
-  off = 0;
-  for (int c = 0; c < 2; ++c) {
-    if (jmap[c] < 0) continue;
-    sv[c].assign(E.hscal + off, E.hscal + off + k[c]);
-    off += k[c];
+  {
+    std::vector<std::pair<const double*, int>> src;
+    for (int c = 0; c < 2; ++c) src.push_back({jmap[c] < 0 ? nullptr : w[c].s, jmap[c] < 0 ? 0 : k[c]});
+    auto v = read_values(E, src, "svd_kept");
+    for (int c = 0; c < 2; ++c) sv[c] = std::move(v[c]);
   }
   KeptSVD res;
   double tot2 = 0;
@@ -1764,21 +1780,11 @@ EIGres eigh(Engine& E, const Tensor& A, const std::vector<int>& rows, const std:
   }
   la::eigh_batched(E, ds);
   EIGres res;
-  int off = 0;
-  for (int c = 0; c < 2; ++c) {
-    if (dmap[c] < 0) continue;
-    SPS_CUDA(cudaMemcpyAsync(E.hscal + off, ds[dmap[c]].s, sizeof(double) * n[c], cudaMemcpyDeviceToHost,
-                             E.stream));
-    off += n[c];
-  }
-  if (off > Engine::NSCAL) throw Error(SPS_ERR_ARGUMENT, "eigh: too large");
-  E.sync();
-  E.check_flag("eigh");
-  off = 0;
-  for (int c = 0; c < 2; ++c) {
-    if (dmap[c] < 0) continue;
-    res.w[c].assign(E.hscal + off, E.hscal + off + n[c]);
-    off += n[c];
+  {
+    std::vector<std::pair<const double*, int>> src;
+    for (int c = 0; c < 2; ++c) src.push_back({dmap[c] < 0 ? nullptr : ds[dmap[c]].s, dmap[c] < 0 ? 0 : n[c]});
+    auto v = read_values(E, src, "eigh");
+    for (int c = 0; c < 2; ++c) res.w[c] = std::move(v[c]);
   }
   Par nl = make_par(n[0], n[1]);
   std::vector<Par> vl = bt.rp;
@@ -1792,6 +1798,61 @@ EIGres eigh(Engine& E, const Tensor& A, const std::vector<int>& rows, const std:
     auto vc = leg_offsets(c, n[0], n[1], res.V.strides[nr]);
     scatter_block(E, res.V, E.upload_i64(vr, t1), E.upload_i64(vc, t2), n[c], n[c], ds[dmap[c]].q, n[c],
                   false);
+    keep.insert(keep.end(), {t1, t2});
+  }
+  return res;
+}
+
+__global__ void add_diag_kernel(double* a, int n, int lda, double v) {
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) a[i + (size_t)i * lda] += v;
+}
+
+EIGres eigh_unit_shifted(Engine& E, const Tensor& A, const std::vector<int>& rows, const std::vector<int>& cols) {
+  BlockTables bt = tables_of(A, rows, cols);
+  int n[2];
+  for (int c = 0; c < 2; ++c) {
+    n[c] = (int)bt.rt[c].size();
+    if ((int)bt.ct[c].size() != n[c]) throw Error(SPS_ERR_ARGUMENT, "eigh_unit_shifted: non-square block");
+  }
+  std::vector<la::MatDesc> ds;
+  std::vector<Buf> keep;
+  int dmap[2] = {-1, -1};
+  for (int c = 0; c < 2; ++c) {
+    if (n[c] == 0) continue;
+    Buf ba = E.alloc(sizeof(double) * ((size_t)n[c] * n[c] * 2 + n[c]));
+    double* a = (double*)ba->ptr;
+    double* q = a + (size_t)n[c] * n[c];
+    double* s = q + (size_t)n[c] * n[c];
+    Buf t1, t2;
+    gather_block(E, A, E.upload_i64(bt.rt[c], t1), E.upload_i64(bt.ct[c], t2), n[c], n[c], a, n[c], false);
+    add_diag_kernel<<<std::min(1024, (n[c] + 255) / 256), 256, 0, E.stream>>>(a, n[c], n[c], 1.0);
+    SPS_CUDA(cudaGetLastError());
+    dmap[c] = (int)ds.size();
+    ds.push_back({a, q, nullptr, s, n[c], n[c], n[c], n[c], 0});
+    keep.insert(keep.end(), {ba, t1, t2});
+  }
+  la::jacobi_left(E, ds);
+  EIGres res;
+  {
+    std::vector<std::pair<const double*, int>> src;
+    for (int c = 0; c < 2; ++c) src.push_back({dmap[c] < 0 ? nullptr : ds[dmap[c]].s, dmap[c] < 0 ? 0 : n[c]});
+    auto v = read_values(E, src, "eigh_unit_shifted");
+    for (int c = 0; c < 2; ++c) {
+      res.w[c] = std::move(v[c]);
+      for (double& x : res.w[c]) x -= 1.0;
+    }
+  }
+  Par nl = make_par(n[0], n[1]);
+  std::vector<Par> vl = bt.rp;
+  vl.push_back(nl);
+  res.V = E.zeros(vl);
+  int nr = (int)rows.size();
+  for (int c = 0; c < 2; ++c) {
+    if (dmap[c] < 0) continue;
+    Buf t1, t2;
+    auto vr = tensor_rows(res.V, 0, nr, c);
+    auto vc = leg_offsets(c, n[0], n[1], res.V.strides[nr]);
+    scatter_block(E, res.V, E.upload_i64(vr, t1), E.upload_i64(vc, t2), n[c], n[c], ds[dmap[c]].q, n[c], false);
     keep.insert(keep.end(), {t1, t2});
   }
   return res;

@@ -105,10 +105,13 @@ class Engine:
         self.check(self.lib.sps_autotune_report(self.h, buf, 1 << 20))
         return json.loads(buf.value.decode())
 
-    def set_injection(self, force_repair=False, svd_sweep_cap=0):
+    def set_injection(self, force_repair=False, svd_sweep_cap=0, multi_cta_eigh_min=0):
         """Host-side failure injection for tests: force the PSD-repair branch of
-        every bond update; cap the small-block Jacobi sweeps (0 = default)."""
-        self.check(self.lib.sps_set_injection(self.h, 1 if force_repair else 0, int(svd_sweep_cap)))
+        every bond update; cap the small-block Jacobi sweeps (0 = default);
+        route repair eigendecompositions of blocks with at least
+        ``multi_cta_eigh_min`` rows to the multi-CTA solver (0 = default 1024)."""
+        self.check(self.lib.sps_set_injection(self.h, 1 if force_repair else 0, int(svd_sweep_cap),
+                                              int(multi_cta_eigh_min)))
 
     def set_profile(self, enable):
         """0/False off, 1/True per-kernel stats, 2 also per-shape contraction stats (resets the stats)."""

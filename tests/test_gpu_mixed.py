@@ -17,10 +17,15 @@ from util import golden, rel
 
 pytestmark = pytest.mark.gpu
 
-# relative Frobenius error of one GEMM, per mode
-GEMM_TOL = {"tf32": 3e-3, "3xtf32": 2e-6, "3xbf16": 1e-4}
-# absolute error of the energy / magnetisation per site at the headline shapes
-OBS_TOL = {"tf32": 2e-3, "3xtf32": 1e-6, "3xbf16": 5e-5}
+# relative Frobenius error of one GEMM, per mode: the operand rounding (TF32
+# 2^-11; split TF32 ~2^-21; split BF16 ~2^-16 per product) plus the FP32
+# accumulation over K, which dominates the split TF32 mode (~2^-24 sqrt(K) to
+# 2^-24 K: 4e-6 at K = 700, 3e-5 at K = 4096 measured on the B200)
+GEMM_TOL = {"tf32": 3e-3, "3xtf32": 1e-4, "3xbf16": 2e-4}
+# absolute error of the energy / magnetisation per site at the headline shapes:
+# the split modes within the 1e-4 energy target with a factor-two margin, the
+# single-pass TF32 mode (2^-11 per operand) an order of magnitude looser
+OBS_TOL = {"tf32": 2e-3, "3xtf32": 5e-5, "3xbf16": 5e-5}
 CASE = "headline_4x4_D6_chi36.npz"
 
 
