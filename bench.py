@@ -2,8 +2,8 @@
 """Born samples/s on the 8x8 open TFIM (J=1, h=3.0), D=6 (3+3), chi=36 (18+18).
 
 One step = W perfect Born draws (``sample_configuration``, src/sampling/born.jl:86-163)
-drawn at the same time from a device-resident SamplingCache of a seeded
-synthetic beta0 PEPO with the workload's shapes: per draw eight row absorptions
+drawn at the same time from a device-resident SamplingCache of the purified
+beta0 = 0.4 PEPO of the workload (stored, bench_states.py): per draw eight row absorptions
 and 64 conditionals.  The headline `value` is the zip-up absorption path
 (FP64); the plain FP64 path (the reference's exact LQ + truncated-SVD
 compression, one sample per launch sequence) draws the same sample ids beside
@@ -49,7 +49,7 @@ PROBES = """probes (one hot operation on a representative input, run once to war
   qr                blocked Householder QR of a 23328x648 block
   topk [W] [gram]   leading 18 triplets of a 648x648 graded block (1/W of the SMs)
   gemm              FP64 GEMM 23328x648x648 and the 648x648x23328 Gram
-  draw              one Born draw, 8x8 D=6 chi=36, exact compression (synthetic PEPO)
+  draw              one Born draw, 8x8 D=6 chi=36, exact compression (purified beta0 PEPO)
   zipdraw           the same draw with the zip-up absorption
   scale             zip-up draws at 12x12 D=8 chi=64 (32+32): 1 and 4 at a time
   fustep [L]        one full-update Trotter step + energy, L x L D=6 chi=36 (default 8): both absorptions,
@@ -75,8 +75,8 @@ def parse():
 def workload_config(extra=None):
     c = {"workload": "tfim_8x8_D6_chi36_born_draw", "Lx": LX, "Ly": LY, "J": 1.0, "h": H_FIELD, "D": D,
          "bond_space": [D // 2, D // 2], "chi_sampling": CHI, "sampling_space": [CHI // 2, CHI // 2],
-         "pepo": f"synthetic seeded beta0 stand-in (identity + {PEPO_EPS} Gaussian Z2 noise, seed {PEPO_SEED}); "
-                 "purifying the 8x8 D=6 PEPO is outside the benchmark's time budget",
+         "pepo": "purified beta0 = 0.4 PEPO (run_purification on this engine: identity PEPO, 10 full-update "
+                 "steps tau = 0.02, D=6, chi=36, FP64; stored in stopeps.jl_b200/states/)",
          "step": "W Born draws from a device-resident SamplingCache",
          "uniforms": "numpy default_rng([seed, sample_id])", "seed": SEED,
          "l2": "inputs larger than L2 (the south boundaries and candidate double layers of the cache, ~0.6 GB)"}
@@ -157,13 +157,11 @@ class OracleRowDraws:
         from oracle import boundary as bm, model as omd, sampling as osp
         from oracle.z2 import T, leg
         import __graft_entry__ as ge
-        syn = ge.load_package().synthetic
-        sites, dims = syn.synthetic_pepo(LX, LY, D, PEPO_EPS, PEPO_SEED)
+        sites, dims, beta, log_amplitude = ge.load_package().bench_states.load()
         grid = [[None] * LY for _ in range(LX)]
         for i, (a, ld) in enumerate(zip(sites, dims)):
             grid[i % LX][i // LX] = T(np.asarray(a, float), [leg(int(p), int(q)) for p, q in ld])
-        st = omd.State(LX, LY, grid, BETA0, 0.0, "pepo")
-        omd.normalize_state(st)
+        st = omd.State(LX, LY, grid, beta, log_amplitude, "pepo")
         self.osp = osp
         self.ge = ge
         t = time.perf_counter()
@@ -209,7 +207,7 @@ def reference_arm(args, rank, world):
     line = {"impl": "reference", "metric": METRIC, "value": value, "unit": "samples/s", "n_gpus": args.gpus,
             "steps": args.steps, "warmup": args.warmup, "ms_per_step": dt * 1e3 / args.steps,
             "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
-            "data": "synthetic", "config": workload_config({"step": "one row of a Born draw (reference arm)"}),
+            "data": "synthetic (a TFIM state prepared by this engine; no dataset)", "config": workload_config({"step": "one row of a Born draw (reference arm)"}),
             "cpu_baseline": {"value": value, "unit": "samples/s", "cores": cores, "kind": "port", "sample": sample},
             "e2e": {"value": value, "unit": "samples/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
     print(json.dumps(line), flush=True)
@@ -231,6 +229,12 @@ def cpu_baseline_sample(rows=2):
 # ---------------------------------------------------------------------------
 # GPU
 # ---------------------------------------------------------------------------
+def purified_state(sps, e):
+    """The stored beta0 = 0.4 PEPO of the 8x8 TFIM (bench_states.py) on the engine."""
+    sites, dims, beta, log_amplitude = sps.bench_states.load()
+    return e.upload_state(sites, dims, True, beta=beta, log_amplitude=log_amplitude)
+
+
 def measure_fp64_peak(torch, device):
     """cuBLAS DGEMM 8192^3 through torch (the FP64 denominator of the roofline)."""
     n = 8192
@@ -283,9 +287,7 @@ def ours_arm(args, rank, world, local_rank):
         dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=600))
     torch.cuda.set_device(local_rank)
     e = sps.Engine(LX, LY, sps.TFIM(1.0, H_FIELD), device=local_rank)
-    sites, dims = sps.synthetic.synthetic_pepo(LX, LY, D, PEPO_EPS, PEPO_SEED)
-    st = e.upload_state(sites, dims, True, beta=BETA0)
-    sps.normalize_state(st)
+    st = purified_state(sps, e)
     space = sps.Z2Space(CHI // 2, CHI // 2)
     W = max(1, args.concurrency)
     L = LX * LY
@@ -346,6 +348,11 @@ def ours_arm(args, rank, world, local_rank):
 
     zcache = sps.SamplingCache(st, sps.BoundaryMPSZipUp(CHI, space))
     zip_run = measure(zcache, timed_ids, warm_ids, e2e_ids, concurrency=W)
+    # the same draws with the contraction GEMMs in split TF32 on the tensor cores
+    # (truncations, normalisations and log-probabilities FP64; same cache)
+    e.set_precision("3xtf32")
+    mixed_run = measure(zcache, timed_ids, warm_ids, e2e_ids, concurrency=W)
+    e.set_precision("fp64")
     # per-kernel profile of one more batch at the same concurrency (the timed configuration; untimed)
     e.set_concurrency(W)
     e.set_profile(True)
@@ -368,6 +375,10 @@ def ours_arm(args, rank, world, local_rank):
     del pcache
     value = world * args.steps * W / (zip_run["ms"] * 1e-3)
     e2e = world * args.steps * W / zip_run["wall"]
+    mixed_value = world * args.steps * W / (mixed_run["ms"] * 1e-3)
+    mmap = {d["uid"]: d for d in mixed_run["draws"]}
+    msame = sum(int(np.array_equal(d["configuration"], mmap[d["uid"]]["configuration"])) for d in zip_run["draws"])
+    mdlp = max(abs(d["log_probability"] - mmap[d["uid"]]["log_probability"]) for d in zip_run["draws"])
     plain_value = world * plain_steps / (plain_run["ms"] * 1e-3)
     plain_e2e = world * plain_steps / plain_run["wall"]
     zmap = {d["uid"]: d for d in zip_run["draws"]}
@@ -384,18 +395,25 @@ def ours_arm(args, rank, world, local_rank):
     # value (exact compression; fixture made by tests/golden/make_golden.py)
     en_plain = sps.measure_energy(st, sps.BoundaryMPS(CHI, space))
     en_zip = sps.measure_energy(st, sps.BoundaryMPSZipUp(CHI, space))
+    e.set_precision("3xtf32")
+    en_mixed = sps.measure_energy(st, sps.BoundaryMPSZipUp(CHI, space))
+    e.set_precision("fp64")
     oracle_e = None
     if os.path.exists(ORACLE_ENERGY):
-        oracle_e = float(np.load(ORACLE_ENERGY)["energy"][1])
+        fx = np.load(ORACLE_ENERGY)
+        if "state" in fx and str(fx["state"]) == sps.bench_states.PURIFIED_8X8:   # made for this very state
+            oracle_e = float(fx["energy"][1])
     ref_e = oracle_e if oracle_e is not None else en_plain["energy_per_site"]
     precision = {"energy_per_site_oracle_fp64": oracle_e,
                  "energy_per_site_plain_fp64": en_plain["energy_per_site"],
                  "energy_per_site_zipup": en_zip["energy_per_site"],
                  "abs_delta_e_zipup_vs_oracle": abs(en_zip["energy_per_site"] - ref_e),
+                 "energy_per_site_zipup_3xtf32": en_mixed["energy_per_site"],
+                 "abs_delta_e_zipup_3xtf32_vs_oracle": abs(en_mixed["energy_per_site"] - ref_e),
                  "abs_delta_e_plain_vs_oracle": abs(en_plain["energy_per_site"] - ref_e),
                  "reference": "oracle" if oracle_e is not None else "plain FP64 GPU (oracle fixture missing)",
                  "tolerance": 1e-4,
-                 "state": "the synthetic beta0 PEPO of the workload, chi=36 (18+18)"}
+                 "state": "the purified beta0 PEPO of the workload, chi=36 (18+18)"}
 
     pipeline = None
     if not args.no_pipeline:
@@ -419,7 +437,7 @@ def ours_arm(args, rank, world, local_rank):
         n_h2d = 8 * L * W
         result = {"metric": METRIC, "value": value, "unit": "samples/s", "n_gpus": world, "steps": args.steps,
                   "warmup": args.warmup, "ms_per_step": zip_run["ms"] / args.steps, "higher_is_better": True,
-                  "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+                  "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic (a TFIM state prepared by this engine; no dataset)",
                   "config": workload_config({"parallelism": f"samples sharded over {world} GPU(s)",
                                              "path": f"zip-up boundary absorption, FP64, {W} samples "
                                                      "concurrently (own stream and workspace each)",
@@ -435,6 +453,15 @@ def ours_arm(args, rank, world, local_rank):
                                  "sample_ids": flat_timed[:plain_steps],
                                  "path": "reference algorithm: exact LQ sweep + truncated SVD sweep, FP64"},
                   "speedup_vs_plain_fp64": value / plain_value,
+                  "mixed_3xtf32": {"value": mixed_value, "e2e": world * args.steps * W / mixed_run["wall"],
+                                   "unit": "samples/s", "ms_per_step": mixed_run["ms"] / args.steps,
+                                   "gpu_launches": mixed_run["launches"], "clocks": mixed_run["clocks"],
+                                   "speedup_vs_plain_fp64": mixed_value / plain_value,
+                                   "agreement_vs_fp64_zipup": {"draws": len(zip_run["draws"]),
+                                                               "identical_configurations": msame,
+                                                               "max_abs_dlogp": mdlp},
+                                   "path": "zip-up absorption, contraction GEMMs 3xTF32 on tcgen05 (FP32 "
+                                           "accumulation), truncations and log-weights FP64, same sample ids"},
                   "agreement_vs_plain": {"draws": ncmp, "identical_configurations": same,
                                          "max_abs_dlogp": dlp},
                   "precision": precision,
@@ -453,6 +480,7 @@ def pipeline_timing(sps, e, st, draws, W, space, np, torch, local_rank, dist):
     composed with the draw rate into samples/s for beta 0.4 -> 2.0 at tau = 0.02."""
     n_steps = len(sps.step_schedule(BETA0, BETA_MAX, DTAU))
     zm = sps.BoundaryMPSZipUp(CHI, space)
+    W = min(W, 4)
     cfgs = np.stack([d["configuration"] for d in draws[:W]])
     e.set_concurrency(W)
     e.timer_start()
@@ -535,9 +563,7 @@ def probe(argv):
         print(f"qr 23328x648: {ms:.2f} ms")
     elif which in ("draw", "zipdraw"):
         e = sps.Engine(LX, LY, sps.TFIM(1.0, H_FIELD))
-        sites, dims = sps.synthetic.synthetic_pepo(LX, LY, D, PEPO_EPS, PEPO_SEED)
-        st = e.upload_state(sites, dims, True, beta=BETA0)
-        sps.normalize_state(st)
+        st = purified_state(sps, e)
         kind = sps.BoundaryMPS if which == "draw" else sps.BoundaryMPSZipUp
         cache = sps.SamplingCache(st, kind(CHI, sps.Z2Space(CHI // 2, CHI // 2)))
         for i in range(2):
@@ -580,9 +606,12 @@ def probe(argv):
         # L x L D=6 chi=36: both absorptions, FP64 and the split-TF32 contractions
         Ls = int(argv[1]) if len(argv) > 1 else LX
         e = sps.Engine(Ls, Ls, sps.TFIM(1.0, H_FIELD))
-        sites, dims = sps.synthetic.synthetic_pepo(Ls, Ls, D, PEPO_EPS, PEPO_SEED)
-        st = e.upload_state(sites, dims, True, beta=BETA0)
-        sps.normalize_state(st)
+        if Ls == LX:
+            st = purified_state(sps, e)
+        else:
+            sites, dims = sps.synthetic.synthetic_pepo(Ls, Ls, D, PEPO_EPS, PEPO_SEED)
+            st = e.upload_state(sites, dims, True, beta=BETA0)
+            sps.normalize_state(st)
         cfg = sps.sample_configuration(sps.SamplingCache(st, sps.BoundaryMPSZipUp(CHI, sps.Z2Space(CHI // 2, CHI // 2))),
                                        uniforms=sps.sample_uniforms(SEED, 1, Ls * Ls))["configuration"]
         for zipup in (True, False):

@@ -209,6 +209,12 @@ int sps_sampling_cache_free(sps_handle* h, int32_t cache_id);
  * receives SymmetryBasis labels 1 (even) / 2 (odd), index x + y*Lx. */
 int sps_sample(sps_handle* h, int32_t cache_id, const double* uniforms, int32_t* configuration,
                sps_sample_report* report);
+/* sample_configuration with the `conditionals` of its result (born.jl:95,
+ * :146): the Lx*Ly conditional probabilities of the chosen labels in row-major
+ * site order (0 past a zero-probability stop).  Draws from `uniforms`, or
+ * evaluates `given` (labels) when it is not NULL. */
+int sps_sample_conditionals(sps_handle* h, int32_t cache_id, const double* uniforms, const int32_t* given,
+                            int32_t* configuration, double* conditionals, sps_sample_report* report);
 /* sample_configuration(cache; configuration) : probability of a given draw */
 int sps_sample_probability(sps_handle* h, int32_t cache_id, const int32_t* configuration,
                            sps_sample_report* report);

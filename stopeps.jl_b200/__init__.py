@@ -10,20 +10,22 @@ from .config import (Z2Space, Lattice, TFIM, FullUpdate, BoundaryMPS, BoundaryMP
                      SymmetryBasis, RunConfig, validate_config, temperature_nodes, parameter_dict)
 from .engine import (Engine, DeviceState, SamplingCache, normalize_state, evolution_step, lognorm,
                      measure_energy, sample_configuration, sample_batch, project_configuration,
-                     project_batch, evolution_step_batch, measure_energy_batch, lognorm_batch)
+                     project_batch, evolution_step_batch, measure_energy_batch, lognorm_batch,
+                     sample_conditionals)
 from .driver import (run_purification, run_stochastic, ensemble_statistics, group_configurations,
                      sample_uniforms, step_schedule, ThermalCheckpoint, Particle, RESULT_SCHEMA_VERSION)
 from . import _lib
 from .build import build, LIB as LIBRARY_PATH
 from .parallel import SerialExecution, TorchExecution
 from . import synthetic
+from . import bench_states
 
 __all__ = [
     "Z2Space", "Lattice", "TFIM", "FullUpdate", "BoundaryMPS", "BoundaryMPSRow", "ResamplingOptions",
     "SymmetryBasis", "RunConfig", "validate_config", "temperature_nodes", "parameter_dict", "Engine",
     "DeviceState", "SamplingCache", "normalize_state", "evolution_step", "lognorm", "measure_energy",
     "sample_configuration", "sample_batch", "project_configuration", "project_batch", "evolution_step_batch",
-    "measure_energy_batch", "lognorm_batch", "run_purification", "run_stochastic",
+    "measure_energy_batch", "lognorm_batch", "sample_conditionals", "run_purification", "run_stochastic",
     "ensemble_statistics", "group_configurations", "sample_uniforms", "step_schedule", "ThermalCheckpoint",
     "Particle", "RESULT_SCHEMA_VERSION", "build", "LIBRARY_PATH",
 ]

@@ -23,6 +23,7 @@ EXPORTS = [
     "sps_set_sm_share", "sps_project_batch", "sps_evolution_step_batch", "sps_measure_energy_batch",
     "sps_lognorm_batch", "sps_set_injection", "sps_set_precision", "sps_la_gemm_mixed",
     "sps_set_autotune", "sps_autotune_report",
+    "sps_sample_conditionals",
 ]
 
 STATUS = {0: "SPS_OK", 1: "SPS_ERR_ARGUMENT", 2: "SPS_ERR_CUDA", 3: "SPS_ERR_NUMERIC",
@@ -102,6 +103,7 @@ def load():
         "sps_sampling_cache_free": ([vp, i32], C.c_int),
         "sps_sample": ([vp, i32, P(dbl), P(i32), P(sps_sample_report)], C.c_int),
         "sps_sample_probability": ([vp, i32, P(i32), P(sps_sample_report)], C.c_int),
+        "sps_sample_conditionals": ([vp, i32, P(dbl), P(i32), P(i32), P(dbl), P(sps_sample_report)], C.c_int),
         "sps_sample_batch": ([vp, i32, i32, P(dbl), P(i32), P(dbl), P(sps_sample_report)], C.c_int),
         "sps_project": ([vp, i32, P(i32), P(i32), P(dbl)], C.c_int),
         "sps_project_batch": ([vp, i32, i32, P(i32), P(i32), P(dbl)], C.c_int),

@@ -815,6 +815,26 @@ int sps_sample(sps_handle* h, int32_t cache_id, const double* uniforms, int32_t*
   });
 }
 
+int sps_sample_conditionals(sps_handle* h, int32_t cache_id, const double* uniforms, const int32_t* given,
+                            int32_t* configuration, double* conditionals, sps_sample_report* report) {
+  return guarded(h, [&] {
+    if (!uniforms && !given) throw Error(SPS_ERR_ARGUMENT, "an explicit RNG is required");
+    SamplingCache& c = get_cache(h, cache_id);
+    std::vector<int> cfg;
+    if (given) cfg.assign(given, given + c.Lx * c.Ly);
+    SampleResult r = sample_configuration(*h->E, c, given ? nullptr : uniforms, given ? cfg.data() : nullptr);
+    if (configuration)
+      for (size_t i = 0; i < r.config.size(); ++i) configuration[i] = r.config[i];
+    if (conditionals)
+      for (size_t i = 0; i < r.config.size(); ++i) conditionals[i] = i < r.conditionals.size() ? r.conditionals[i] : 0.0;
+    if (report) {
+      report->log_probability = r.log_probability;
+      report->max_environment_truncation = r.max_env_trunc;
+      report->near_boundary = r.near_boundary;
+    }
+  });
+}
+
 int sps_sample_probability(sps_handle* h, int32_t cache_id, const int32_t* configuration,
                            sps_sample_report* report) {
   return guarded(h, [&] {

@@ -1814,9 +1814,13 @@ EIGres eigh_unit_shifted(Engine& E, const Tensor& A, const std::vector<int>& row
     n[c] = (int)bt.rt[c].size();
     if ((int)bt.ct[c].size() != n[c]) throw Error(SPS_ERR_ARGUMENT, "eigh_unit_shifted: non-square block");
   }
-  std::vector<la::MatDesc> ds;
+  // blocks below SMALL rows go to the single-CTA two-sided Jacobi (the block
+  // one-sided Jacobi pairs column blocks of four and needs several of them)
+  constexpr int SMALL = 32;
+  std::vector<la::MatDesc> big, small;
   std::vector<Buf> keep;
-  int dmap[2] = {-1, -1};
+  la::MatDesc dd[2];
+  bool shifted[2] = {false, false};
   for (int c = 0; c < 2; ++c) {
     if (n[c] == 0) continue;
     Buf ba = E.alloc(sizeof(double) * ((size_t)n[c] * n[c] * 2 + n[c]));
@@ -1825,21 +1829,28 @@ EIGres eigh_unit_shifted(Engine& E, const Tensor& A, const std::vector<int>& row
     double* s = q + (size_t)n[c] * n[c];
     Buf t1, t2;
     gather_block(E, A, E.upload_i64(bt.rt[c], t1), E.upload_i64(bt.ct[c], t2), n[c], n[c], a, n[c], false);
-    add_diag_kernel<<<std::min(1024, (n[c] + 255) / 256), 256, 0, E.stream>>>(a, n[c], n[c], 1.0);
-    SPS_CUDA(cudaGetLastError());
-    dmap[c] = (int)ds.size();
-    ds.push_back({a, q, nullptr, s, n[c], n[c], n[c], n[c], 0});
+    dd[c] = {a, q, nullptr, s, n[c], n[c], n[c], n[c], 0};
+    if (n[c] >= SMALL) {
+      add_diag_kernel<<<std::min(1024, (n[c] + 255) / 256), 256, 0, E.stream>>>(a, n[c], n[c], 1.0);
+      SPS_CUDA(cudaGetLastError());
+      shifted[c] = true;
+      big.push_back(dd[c]);
+    } else {
+      small.push_back(dd[c]);
+    }
     keep.insert(keep.end(), {ba, t1, t2});
   }
-  la::jacobi_left(E, ds);
+  if (!big.empty()) la::jacobi_left(E, big);
+  if (!small.empty()) la::eigh_batched(E, small);
   EIGres res;
   {
     std::vector<std::pair<const double*, int>> src;
-    for (int c = 0; c < 2; ++c) src.push_back({dmap[c] < 0 ? nullptr : ds[dmap[c]].s, dmap[c] < 0 ? 0 : n[c]});
+    for (int c = 0; c < 2; ++c) src.push_back({n[c] == 0 ? nullptr : dd[c].s, n[c]});
     auto v = read_values(E, src, "eigh_unit_shifted");
     for (int c = 0; c < 2; ++c) {
       res.w[c] = std::move(v[c]);
-      for (double& x : res.w[c]) x -= 1.0;
+      if (shifted[c])
+        for (double& x : res.w[c]) x -= 1.0;
     }
   }
   Par nl = make_par(n[0], n[1]);
@@ -1848,11 +1859,11 @@ EIGres eigh_unit_shifted(Engine& E, const Tensor& A, const std::vector<int>& row
   res.V = E.zeros(vl);
   int nr = (int)rows.size();
   for (int c = 0; c < 2; ++c) {
-    if (dmap[c] < 0) continue;
+    if (n[c] == 0) continue;
     Buf t1, t2;
     auto vr = tensor_rows(res.V, 0, nr, c);
     auto vc = leg_offsets(c, n[0], n[1], res.V.strides[nr]);
-    scatter_block(E, res.V, E.upload_i64(vr, t1), E.upload_i64(vc, t2), n[c], n[c], ds[dmap[c]].q, n[c], false);
+    scatter_block(E, res.V, E.upload_i64(vr, t1), E.upload_i64(vc, t2), n[c], n[c], dd[c].q, n[c], false);
     keep.insert(keep.end(), {t1, t2});
   }
   return res;

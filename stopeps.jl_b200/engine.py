@@ -401,6 +401,27 @@ def sample_configuration(cache: SamplingCache, uniforms=None, configuration=None
                 max_environment_truncation=rep.max_environment_truncation, near_boundary=rep.near_boundary)
 
 
+def sample_conditionals(cache: SamplingCache, uniforms=None, configuration=None):
+    """``sample_configuration`` with its ``conditionals`` (the probability of each
+    chosen label, (Lx, Ly) array) from uniforms, or for a given configuration."""
+    e = cache.engine
+    L = e.Lx * e.Ly
+    rep = _lib.sps_sample_report()
+    out = np.zeros(L, np.int32)
+    cond = np.zeros(L)
+    u = None if uniforms is None else np.ascontiguousarray(np.asarray(uniforms, np.float64).reshape(-1))
+    g = None if configuration is None else np.ascontiguousarray(np.asarray(configuration, np.int32).T.reshape(-1))
+    if u is None and g is None:
+        raise ValueError("an explicit RNG is required")
+    if u is not None and u.size != L:
+        raise ValueError("one uniform per site is required")
+    e.check(e.lib.sps_sample_conditionals(e.h, cache.id, None if u is None else _arr(u, C.c_double),
+                                          None if g is None else _arr(g, C.c_int32), _arr(out, C.c_int32),
+                                          _arr(cond, C.c_double), C.byref(rep)))
+    return dict(configuration=out.reshape(e.Ly, e.Lx).T.copy(), conditionals=cond.reshape(e.Ly, e.Lx).T.copy(),
+                log_probability=rep.log_probability, max_environment_truncation=rep.max_environment_truncation)
+
+
 def sample_batch(cache: SamplingCache, uniforms, reports=False):
     """Many draws in one call: uniforms (n, Lx*Ly) -> configurations (n, Lx, Ly), log_p (n,)
     (and, with ``reports``, each draw's max_environment_truncation and near_boundary count)."""

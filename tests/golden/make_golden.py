@@ -159,16 +159,33 @@ def headline_case(name, Lx=4, Ly=4, D=6, chi=36, h=3.0, dtau=0.02, ndraws=3, see
     print(name, "step", out["step_stops"], out["step_report"], "E1", e1["energy_per_site"], flush=True)
 
 
-def bench_energy_case(name, L=8, D=6, chi=36, h=3.0):
-    """The FP64 oracle energy of the benchmark's beta0 state (8x8 synthetic PEPO,
-    D=6, chi=36 = 18+18, exact compression): the reference value of the
-    benchmark's precision check."""
-    st = synthetic_state(L, L, D, 0.15, 7)
-    md.normalize_state(st)
+def stored_state(name):
+    """A stored PEPO of ``stopeps.jl_b200/bench_states.py`` as an oracle state."""
+    import importlib.util
+    spec = importlib.util.spec_from_file_location("_bench_states",
+                                                  os.path.join(ROOT, "stopeps.jl_b200", "bench_states.py"))
+    bs = importlib.util.module_from_spec(spec)
+    spec.loader.exec_module(bs)
+    from oracle.model import State
+    from oracle.z2 import leg
+    sites, dims, beta, log_amplitude = bs.load(name)
+    L = int(round(len(sites) ** 0.5))
+    grid = [[None] * L for _ in range(L)]
+    for i, (a, d) in enumerate(zip(sites, dims)):
+        grid[i % L][i // L] = T(np.asarray(a, float), [leg(int(p), int(q)) for p, q in d])
+    return State(L, L, grid, beta, log_amplitude, "pepo")
+
+
+def bench_energy_case(name, D=6, chi=36, h=3.0):
+    """The FP64 oracle energy of the benchmark's beta0 state (the stored purified
+    8x8 PEPO, D=6, chi=36 = 18+18, exact compression): the reference value of
+    the benchmark's precision check."""
+    st = stored_state("tfim_8x8_h3_D6_chi36_beta0.4.npz")
     m = bm.BoundaryMPS(chi, (chi // 2, chi // 2))
     en = sp.measure_energy(st, md.TFIM(1.0, h), m)
     out = dict(energy=np.array([en["energy_total"], en["energy_per_site"], en["log_norm"], en["x_sum"],
-                                en["max_environment_truncation"]]), site_x=en["site_x"])
+                                en["max_environment_truncation"]]), site_x=en["site_x"],
+               state="tfim_8x8_h3_D6_chi36_beta0.4.npz")
     np.savez_compressed(os.path.join(HERE, name), **out)
     print(name, "E", en["energy_per_site"], flush=True)
 

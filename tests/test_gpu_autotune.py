@@ -41,4 +41,4 @@ def test_autotuned_tensor_core_tile(sps):
     keys = [k for k in report if ":tc_gemm.bn:" in k]
     assert keys, report
     assert report[keys[0]]["choice"] in (64, 128, 256)
-    assert np.linalg.norm(c - a @ b) / np.linalg.norm(a @ b) < 2e-6
+    assert np.linalg.norm(c - a @ b) / np.linalg.norm(a @ b) < 1e-4   # split TF32, FP32 accumulation

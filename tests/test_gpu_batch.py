@@ -102,8 +102,8 @@ def test_forced_psd_repair_matches_oracle(sps, multi_cta):
     every bond of one step: the repaired metric (hole in the (bras | kets)
     grouping, per-sector eigendecomposition, negative eigenvalues clipped) and
     the refit, against the oracle with the same bonds forced.  multi_cta: the
-    eigendecomposition takes the multi-CTA route of large holes (one-sided
-    Jacobi of the shifted hole) at this small size."""
+    parity blocks of 32 rows and more take the multi-CTA route of large holes
+    (one-sided Jacobi of the shifted hole) at this small size."""
     from oracle import full_update as fu, model as md, boundary as bm, sampling as osp
     g = golden("pepo_2x3_D2.npz")
     upd = sps.FullUpdate(max_iterations=8, linear_max_iterations=40)
@@ -112,7 +112,7 @@ def test_forced_psd_repair_matches_oracle(sps, multi_cta):
     D, m, sp = _env(sps, g)
     cfg = g["configs"][0]
     ps, _ = sps.project_configuration(st, cfg)
-    e.set_injection(force_repair=True, multi_cta_eigh_min=1 if multi_cta else 0)
+    e.set_injection(force_repair=True, multi_cta_eigh_min=32 if multi_cta else 0)
     try:
         r = sps.evolution_step(ps, float(g["dtau"]), D, m, sp)
     finally:
