@@ -480,7 +480,7 @@ def pipeline_timing(sps, e, st, draws, W, space, np, torch, local_rank, dist):
     composed with the draw rate into samples/s for beta 0.4 -> 2.0 at tau = 0.02."""
     n_steps = len(sps.step_schedule(BETA0, BETA_MAX, DTAU))
     zm = sps.BoundaryMPSZipUp(CHI, space)
-    W = min(W, 4)
+    W = 1   # one sample: a full-update step at 8x8 D=6 takes tens of seconds
     cfgs = np.stack([d["configuration"] for d in draws[:W]])
     e.set_concurrency(W)
     e.timer_start()
