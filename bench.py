@@ -46,6 +46,7 @@ ORACLE_ENERGY = os.path.join(ROOT, "tests", "golden", "bench_8x8_D6_chi36_energy
 
 PROBES = """probes (one hot operation on a representative input, run once to warm up and once more):
   svd_left          U-only Jacobi of a 648x648 LQ-preconditioned block
+  tcgemm [mode m n k] the tcgen05 contraction GEMM (tf32 | 3xtf32 | 3xbf16), default 3xtf32 8192^3
   qr                blocked Householder QR of a 23328x648 block
   topk [W] [gram]   leading 18 triplets of a 648x648 graded block (1/W of the SMs)
   gemm              FP64 GEMM 23328x648x648 and the 648x648x23328 Gram
@@ -555,6 +556,25 @@ def probe(argv):
         for _ in range(3):
             g, ms = e.la_gemm(a, a, transpose_a=True)
         print(f"gram 648x648x23328: {ms:.3f} ms, {2 * 23328 * 648 * 648 / ms / 1e9:.2f} TFLOP/s")
+    elif which == "tcgemm":
+        # the tcgen05 contraction GEMM on dense operands: (m x k) (k x n) in a low-precision mode
+        mode = argv[1] if len(argv) > 1 else "3xtf32"
+        m, n, k = (int(v) for v in argv[2:5]) if len(argv) > 4 else (8192, 8192, 8192)
+        e = sps.Engine(2, 2)
+        rng = np.random.default_rng(1)
+        a = rng.standard_normal((m, k))
+        b = rng.standard_normal((k, n))
+        for _ in range(3):
+            c, ms = e.la_gemm_mixed(a, b, mode)
+        e.set_profile(True)
+        c, ms = e.la_gemm_mixed(a, b, mode)
+        st = e.kernel_stats()
+        e.set_profile(False)
+        g = [v for kk, v in st.items() if kk.startswith("tc_gemm")][0]
+        passes = 1 if mode == "tf32" else 3
+        print(f"tcgemm {mode} {m}x{n}x{k}: pack+gemm {ms:.3f} ms, gemm {g['ms']:.3f} ms, "
+              f"{2 * m * n * k / g['ms'] / 1e9:.1f} TFLOP/s effective, {passes * 2 * m * n * k / g['ms'] / 1e9:.1f} "
+              f"TFLOP/s on the tensor cores; rel err {np.linalg.norm(c - a @ b) / np.linalg.norm(a @ b):.2e}")
     elif which == "qr":
         e = sps.Engine(2, 2)
         a = np.random.default_rng(3).standard_normal((23328, 648))
