@@ -50,8 +50,9 @@ PROBES = """probes (one hot operation on a representative input, run once to war
   qr                blocked Householder QR of a 23328x648 block
   topk [W] [gram]   leading 18 triplets of a 648x648 graded block (1/W of the SMs)
   gemm              FP64 GEMM 23328x648x648 and the 648x648x23328 Gram
-  draw              one Born draw, 8x8 D=6 chi=36, exact compression (purified beta0 PEPO)
-  zipdraw           the same draw with the zip-up absorption
+  draw [synthetic]  one Born draw, 8x8 D=6 chi=36, exact compression (purified beta0 PEPO, or the
+                    seeded synthetic stand-in of the same shapes)
+  zipdraw [synthetic] the same draw with the zip-up absorption
   scale             zip-up draws at 12x12 D=8 chi=64 (32+32): 1 and 4 at a time
   fustep [L]        one full-update Trotter step + energy, L x L D=6 chi=36 (default 8): both absorptions,
                     FP64 and 3xTF32 contractions
@@ -583,7 +584,12 @@ def probe(argv):
         print(f"qr 23328x648: {ms:.2f} ms")
     elif which in ("draw", "zipdraw"):
         e = sps.Engine(LX, LY, sps.TFIM(1.0, H_FIELD))
-        st = purified_state(sps, e)
+        if len(argv) > 1 and argv[1] == "synthetic":   # the seeded synthetic beta0 stand-in of the same shapes
+            sites, dims = sps.synthetic.synthetic_pepo(LX, LY, D, PEPO_EPS, PEPO_SEED)
+            st = e.upload_state(sites, dims, True, beta=BETA0)
+            sps.normalize_state(st)
+        else:
+            st = purified_state(sps, e)
         kind = sps.BoundaryMPS if which == "draw" else sps.BoundaryMPSZipUp
         cache = sps.SamplingCache(st, kind(CHI, sps.Z2Space(CHI // 2, CHI // 2)))
         for i in range(2):
