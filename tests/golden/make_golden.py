@@ -190,6 +190,28 @@ def bench_energy_case(name, D=6, chi=36, h=3.0):
     print(name, "E", en["energy_per_site"], flush=True)
 
 
+def config1_case(name, Ns=4):
+    """The plain-method configuration end to end (4x4, D=4 = 2+2, chi=16 = 8+8,
+    h=0.7, tau=0.05, beta0=0.5, seed 1) with Ns draws evolved to beta=1 and
+    measured at 0.5 and 1: purification, draws, grouping, full-update evolution,
+    weights and the ensemble curve."""
+    c = dr.RunConfig(Lx=4, Ly=4, J=1.0, h=0.7, beta0=0.5, beta_log=[1.0], beta_measure=[0.5, 1.0],
+                     delta_tau_pur=0.05, delta_tau_peps=0.05, D_pur=4, D_peps=4, bond_space_pur=(2, 2),
+                     bond_space_peps=(2, 2), chi_environment=16, environment_space=(8, 8), Ns=Ns, seed=1)
+    st, rows = dr.run_purification(c)
+    res = dr.run_stochastic(c, st)
+    curve = res["curve"]
+    out = dict(pur_lnZ=np.array([r["lnZ"] for r in rows]), pur_energy=np.array([r["energy_per_site"] for r in rows]),
+               beta=np.array([r["beta"] for r in curve]), energy=np.array([r["energy_per_site"] for r in curve]),
+               lnZ=np.array([r["lnZ"] for r in curve]), eta=np.array([r["eta"] for r in curve]),
+               magnetization=np.array([r.get("magnetization", np.nan) for r in curve]),
+               draw_logp=np.array([d["log_probability"] for d in res["draws"]]),
+               draw_cfg=np.stack([np.asarray(d["configuration"]) for d in res["draws"]]),
+               multiplicity=np.asarray(res["grouping"]["multiplicity"]))
+    np.savez_compressed(os.path.join(HERE, name), **out)
+    print(name, out["energy"], out["lnZ"], out["eta"], flush=True)
+
+
 def pipeline_case(name):
     c = dr.RunConfig(Lx=2, Ly=2, J=1.0, h=0.7, beta0=0.2, beta_log=[0.1, 0.2, 0.3], beta_measure=[0.2, 0.3],
                      delta_tau_pur=0.05, delta_tau_peps=0.05, D_pur=2, D_peps=2, bond_space_pur=(1, 1),
@@ -218,7 +240,8 @@ if __name__ == "__main__":
                                                   [(16, (8, 8)), (24, (12, 12))], peps_D=4, peps_space=(2, 2),
                                                   peps_chi=16, peps_env_space=(8, 8), ndraws=4, seed=1),
              "headline_4x4_D6_chi36.npz": lambda: headline_case("headline_4x4_D6_chi36.npz"),
-             "bench_8x8_D6_chi36_energy.npz": lambda: bench_energy_case("bench_8x8_D6_chi36_energy.npz")}[name]()
+             "bench_8x8_D6_chi36_energy.npz": lambda: bench_energy_case("bench_8x8_D6_chi36_energy.npz"),
+             "config1_4x4_D4_run.npz": lambda: config1_case("config1_4x4_D4_run.npz")}[name]()
         sys.exit(0)
     # 3x3, D=4 PEPO; boundary chi 8 truncates, 16 is exact; PEPS step at D=2 exercises the ALS
     pepo_case("pepo_3x3_D4.npz", 3, 3, 0.7, 4, (2, 2), 16, (8, 8), 0.2, 0.05,
@@ -237,3 +260,5 @@ if __name__ == "__main__":
     headline_case("headline_4x4_D6_chi36.npz")
     # the benchmark's precision reference: the 8x8 beta0 state's FP64 energy
     bench_energy_case("bench_8x8_D6_chi36_energy.npz")
+    # the plain-method configuration end to end with four draws evolved to beta = 1
+    config1_case("config1_4x4_D4_run.npz")

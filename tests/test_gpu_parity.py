@@ -238,3 +238,31 @@ def test_truncrank_without_sector_budget(sps, zip_up):
     en = sps.measure_energy(st, kind(16, None))
     oen = osp.measure_energy(ost, md.TFIM(float(g["J"]), float(g["h"])), bm.BoundaryMPS(16, None, zipup=zip_up))
     assert rel(en["energy_per_site"], oen["energy_per_site"]) < TOL
+
+
+def test_config1_end_to_end(sps):
+    """The plain-method configuration (4x4 TFIM h=0.7, D=4 = 2+2, chi=16 = 8+8,
+    tau=0.05, beta0=0.5, seed 1) end to end: purification, four Born draws,
+    full-update evolution of the unique configurations to beta=1 and the
+    ensemble curve, against the oracle's run (fixture config1_4x4_D4_run.npz)."""
+    import os
+    from util import GOLDEN
+    if not os.path.exists(os.path.join(GOLDEN, "config1_4x4_D4_run.npz")):
+        pytest.skip("fixture not generated")
+    g = golden("config1_4x4_D4_run.npz")
+    c = sps.RunConfig(lattice=sps.Lattice(4, 4), model=sps.TFIM(1.0, 0.7), beta0=0.5, beta_log=[1.0],
+                      beta_measure=[0.5, 1.0], delta_tau_pur=0.05, delta_tau_peps=0.05, D_pur=4, D_peps=4,
+                      bond_space_pur=sps.Z2Space(2, 2), bond_space_peps=sps.Z2Space(2, 2), chi_environment=16,
+                      environment_space=sps.Z2Space(8, 8), Ns=4, seed=1,
+                      resampling=sps.ResamplingOptions(enabled=False))
+    cp = sps.run_purification(c)
+    np.testing.assert_allclose([r["lnZ"] for r in cp.purification], g["pur_lnZ"], rtol=1e-9)
+    res = sps.run_stochastic(c, cp)
+    draws = res["diagnostics"]["born_draws"]
+    np.testing.assert_array_equal(np.stack([d["configuration"] for d in draws]), g["draw_cfg"])
+    np.testing.assert_allclose([d["log_probability"] for d in draws], g["draw_logp"], rtol=1e-9)
+    curve = [r for r in res["observables"]["curve"] if r.get("source") == "sampling"]
+    np.testing.assert_allclose([r["beta"] for r in curve], g["beta"], rtol=1e-14)
+    np.testing.assert_allclose([r["energy_per_site"] for r in curve], g["energy"], rtol=1e-8)
+    np.testing.assert_allclose([r["lnZ"] for r in curve], g["lnZ"], rtol=1e-8)
+    np.testing.assert_allclose([r["eta"] for r in curve], g["eta"], rtol=1e-8)
