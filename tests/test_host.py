@@ -84,3 +84,26 @@ def test_create_without_device_fails_loudly(sps):
         pytest.skip("a CUDA device is present")
     with pytest.raises(sps._lib.EngineError):
         sps.Engine(2, 2)
+
+
+def test_stored_benchmark_state_layout(sps):
+    """The stored purified 8x8 PEPO: 64 sites, legs (W,N,Pout,Paux,E,S) with the
+    D = 6 (3+3) bulk bonds, trivial outer legs, sector-sorted blocks whose
+    parity-odd entries are zero."""
+    import numpy as np
+    sites, dims, beta, log_amplitude = sps.bench_states.load()
+    assert len(sites) == 64 and dims.shape == (64, 6, 2)
+    assert abs(beta - 0.4) < 1e-14 and np.isfinite(log_amplitude)
+    for i, (a, d) in enumerate(zip(sites, dims)):
+        x, y = i % 8, i // 8
+        assert tuple(d[2]) == (1, 1) and tuple(d[3]) == (1, 1)
+        assert tuple(d[0]) == ((1, 0) if x == 0 else (3, 3))
+        assert tuple(d[5]) == ((1, 0) if y == 7 else (3, 3))
+        par = np.zeros(a.shape, np.int64)
+        for k, (n0, n1) in enumerate(d):
+            p = np.concatenate([np.zeros(n0, np.int64), np.ones(n1, np.int64)])
+            sh = [1] * 6
+            sh[k] = n0 + n1
+            par = par + p.reshape(sh)
+        assert np.all(a[par % 2 == 1] == 0.0)
+        assert np.linalg.norm(a) > 0
