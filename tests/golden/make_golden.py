@@ -176,16 +176,21 @@ def stored_state(name):
     return State(L, L, grid, beta, log_amplitude, "pepo")
 
 
-def bench_energy_case(name, D=6, chi=36, h=3.0):
-    """The FP64 oracle energy of the benchmark's beta0 state (the stored purified
-    8x8 PEPO, D=6, chi=36 = 18+18, exact compression): the reference value of
-    the benchmark's precision check."""
-    st = stored_state("tfim_8x8_h3_D6_chi36_beta0.4.npz")
+def bench_energy_case(name, D=6, chi=36, h=3.0, state="tfim_8x8_h3_D6_chi36_beta0.4.npz"):
+    """The FP64 oracle energy of a benchmark state (the stored purified 8x8
+    PEPO, or state="synthetic": the seeded synthetic stand-in of the same
+    shapes; D=6, chi=36 = 18+18, exact compression): the reference value of the
+    benchmark's precision check."""
+    if state == "synthetic":
+        st = synthetic_state(8, 8, D, 0.15, 7)
+        md.normalize_state(st)
+    else:
+        st = stored_state(state)
     m = bm.BoundaryMPS(chi, (chi // 2, chi // 2))
     en = sp.measure_energy(st, md.TFIM(1.0, h), m)
     out = dict(energy=np.array([en["energy_total"], en["energy_per_site"], en["log_norm"], en["x_sum"],
                                 en["max_environment_truncation"]]), site_x=en["site_x"],
-               state="tfim_8x8_h3_D6_chi36_beta0.4.npz")
+               state=state)
     np.savez_compressed(os.path.join(HERE, name), **out)
     print(name, "E", en["energy_per_site"], flush=True)
 
@@ -241,7 +246,9 @@ if __name__ == "__main__":
                                                   peps_chi=16, peps_env_space=(8, 8), ndraws=4, seed=1),
              "headline_4x4_D6_chi36.npz": lambda: headline_case("headline_4x4_D6_chi36.npz"),
              "bench_8x8_D6_chi36_energy.npz": lambda: bench_energy_case("bench_8x8_D6_chi36_energy.npz"),
-             "config1_4x4_D4_run.npz": lambda: config1_case("config1_4x4_D4_run.npz")}[name]()
+             "config1_4x4_D4_run.npz": lambda: config1_case("config1_4x4_D4_run.npz"),
+             "bench_8x8_D6_chi36_synthetic_energy.npz":
+                 lambda: bench_energy_case("bench_8x8_D6_chi36_synthetic_energy.npz", state="synthetic")}[name]()
         sys.exit(0)
     # 3x3, D=4 PEPO; boundary chi 8 truncates, 16 is exact; PEPS step at D=2 exercises the ALS
     pepo_case("pepo_3x3_D4.npz", 3, 3, 0.7, 4, (2, 2), 16, (8, 8), 0.2, 0.05,
@@ -260,5 +267,6 @@ if __name__ == "__main__":
     headline_case("headline_4x4_D6_chi36.npz")
     # the benchmark's precision reference: the 8x8 beta0 state's FP64 energy
     bench_energy_case("bench_8x8_D6_chi36_energy.npz")
+    bench_energy_case("bench_8x8_D6_chi36_synthetic_energy.npz", state="synthetic")
     # the plain-method configuration end to end with four draws evolved to beta = 1
     config1_case("config1_4x4_D4_run.npz")
