@@ -149,9 +149,12 @@ int sps_set_sm_share(sps_handle* h, int32_t ctas);
  * extraction (the truncated boundary SVD when no entropy is recorded):
  * u (m x k), s (k, descending), v (n x k), column-major; iterations = the
  * count used.  gram != 0 iterates on a a^T (the zip-up splits' mode; the
- * extraction and the residual test still use a).  rtol: the residual bound
- * relative to s[0] (0 selects 5e-14).  SPS_ERR_CONVERGENCE when the residuals
- * did not reach it within the iteration cap. */
+ * extraction and the residual test still use a); when the spectrum decays
+ * too fast for a a^T to keep the wanted directions above its rounding level,
+ * the call iterates on a instead.  rtol: the residual bound relative to s[0]
+ * (0 selects 5e-14).  SPS_ERR_CONVERGENCE when the residuals did not reach it
+ * within the iteration cap, or when a has fewer than k singular values above
+ * its rounding level. */
 int sps_la_svd_topk(sps_handle* h, int32_t m, int32_t n, int32_t k, const double* a, int32_t gram, double rtol,
                     double* u, double* s, double* v, int32_t* iterations, double* ms);
 

@@ -467,6 +467,10 @@ int sps_la_svd_topk(sps_handle* h, int32_t m, int32_t n, int32_t k, const double
     }
     SPS_CUDA(cudaEventRecord(h->t0, E.stream));
     la::svd_topk(E, ds, rtol > 0.0 ? rtol : 5e-14);
+    if (ds[0].status == 4 && ds[0].gram) {   // wanted directions lost on M M^T: again on M, as the engine does
+      ds[0].gram = false;
+      la::svd_topk(E, ds, rtol > 0.0 ? rtol : 5e-14);
+    }
     SPS_CUDA(cudaEventRecord(h->t1, E.stream));
     SPS_CUDA(cudaMemcpyAsync(u, ds[0].U, sizeof(double) * (size_t)m * k, cudaMemcpyDeviceToHost, E.stream));
     SPS_CUDA(cudaMemcpyAsync(v, ds[0].V, sizeof(double) * (size_t)n * k, cudaMemcpyDeviceToHost, E.stream));

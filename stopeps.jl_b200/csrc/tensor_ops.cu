@@ -1633,65 +1633,68 @@ static bool svd_kept_topk(Engine& E, const BlockTables& bt, const Tensor& A, int
     ds.push_back(d);
   }
   la::svd_topk(E, ds, tr.rtol);
-  constexpr int TOPK_ZERO = 4;   // zero Ritz values among the wanted ones
+  // A Gram-mode problem whose iterate lost wanted directions (a spectrum that
+  // decays faster than the rounding level of M M^T resolves: status 4) runs
+  // again on M itself.
+  constexpr int TOPK_ZERO = 4;
+  std::vector<la::TopkDesc> again;
+  std::vector<int> where;
+  for (size_t i = 0; i < ds.size(); ++i)
+    if (ds[i].status == TOPK_ZERO && ds[i].gram) {
+      again.push_back(ds[i]);
+      again.back().gram = false;
+      where.push_back((int)i);
+    }
+  if (!again.empty()) {
+    if (E.profile) E.add_stat("svd_topk.gram_retry", 0.0, (long long)again.size());
+    la::svd_topk(E, again, tr.rtol);
+    for (size_t i = 0; i < again.size(); ++i) ds[where[i]] = again[i];
+  }
   for (auto& d : ds)
-    if (d.status != 0 && d.status != TOPK_ZERO) return false;
+    if (d.status != 0 && !(d.status == TOPK_ZERO && !d.gram)) return false;
   std::vector<double> sv[2];
   double fro2 = 0;
   for (int c = 0; c < 2; ++c) {
     if (dmap[c] < 0) continue;
     la::TopkDesc& d = ds[dmap[c]];
     fro2 += d.fro2;
-    if (d.status == 0) {
-      sv[c].assign(d.s.begin(), d.s.begin() + kmax[c]);
-      continue;
-    }
-    // Rank-deficient block (rank r < k): the r nonzero triplets by a second
-    // subspace iteration with k = r, the other k - r wanted vectors an
-    // orthonormal completion (they carry zero singular values, so any
-    // completion gives the same contractions); no full-spectrum SVD.
-    const double zthr = 8.0 * DBL_EPSILON * std::sqrt((double)std::max(d.m, d.n)) * std::sqrt(d.fro2);
+    sv[c].assign(d.s.begin(), d.s.begin() + kmax[c]);
+    if (d.status == 0) continue;
+    // Converged on M with r < k nonzero values (fewer than k singular values
+    // above the rounding level): the wanted vectors r..k-1 carry zero values,
+    // so any orthonormal completion gives the same contractions.  Seeded
+    // Gaussian columns after the first r, a Householder QR of the len x k set,
+    // and Q's columns r..k-1 (orthogonal to the first r) into place; the first
+    // r columns are kept as they are.
     int r = 0;
-    while (r < kmax[c] && d.s[r] > zthr) ++r;
-    std::vector<double> vals(kmax[c], 0.0);
-    if (r > 0) {
-      if (la::topk_block_size(r, d.m, d.n) == 0) return false;
-      la::TopkDesc d2 = d;
-      d2.k = r;
-      std::vector<la::TopkDesc> one{d2};
-      la::svd_topk(E, one, tr.rtol);
-      if (one[0].status != 0) return false;
-      for (int i = 0; i < r; ++i) vals[i] = one[0].s[i];
-    }
+    while (r < kmax[c] && sv[c][r] > 0.0) ++r;
+    for (int i = r; i < kmax[c]; ++i) sv[c][i] = 0.0;
     const int len = left ? d.m : d.n, kk = kmax[c];
-    if (r < kk) {
-      // columns r..k-1 of the wanted vectors: seeded Gaussian columns, then a
-      // Householder QR of the whole len x k set (its first r columns are
-      // orthonormal already, so Q keeps them up to sign)
-      std::vector<double> rnd((size_t)len * (kk - r));
-      uint64_t st = 0x9E3779B97F4A7C15ull ^ ((uint64_t)len << 20) ^ (uint64_t)kk;
-      for (auto& v : rnd) {   // splitmix64 -> two uniforms -> Box-Muller
-        auto next = [&st]() {
-          uint64_t z = (st += 0x9E3779B97F4A7C15ull);
-          z = (z ^ (z >> 30)) * 0xBF58476D1CE4E5B9ull;
-          z = (z ^ (z >> 27)) * 0x94D049BB133111EBull;
-          return (double)((z ^ (z >> 31)) >> 11) * (1.0 / 9007199254740992.0);
-        };
-        const double u1 = std::max(next(), 1e-300), u2 = next();
-        v = std::sqrt(-2.0 * std::log(u1)) * std::cos(6.283185307179586 * u2);
-      }
-      double* F = Fv[c];
-      E.stage(rnd.data(), sizeof(double) * rnd.size(), F + (size_t)len * r);
-      Buf qb = E.alloc(sizeof(double) * ((size_t)len * kk * 2 + (size_t)kk * kk + kk));
-      double* T = (double*)qb->ptr;
-      double* Q = T + (size_t)len * kk;
-      double* R = Q + (size_t)len * kk;
-      SPS_CUDA(cudaMemcpyAsync(T, F, sizeof(double) * (size_t)len * kk, cudaMemcpyDeviceToDevice, E.stream));
-      la::qr_batched(E, {la::MatDesc{T, Q, R, R + (size_t)kk * kk, len, kk, len, len, kk}});
-      SPS_CUDA(cudaMemcpyAsync(F, Q, sizeof(double) * (size_t)len * kk, cudaMemcpyDeviceToDevice, E.stream));
-      keep.push_back(qb);
+    if (r == kk) continue;
+    std::vector<double> rnd((size_t)len * (kk - r));
+    uint64_t st = 0x9E3779B97F4A7C15ull ^ ((uint64_t)len << 20) ^ (uint64_t)kk;
+    auto next = [&st]() {   // splitmix64
+      uint64_t z = (st += 0x9E3779B97F4A7C15ull);
+      z = (z ^ (z >> 30)) * 0xBF58476D1CE4E5B9ull;
+      z = (z ^ (z >> 27)) * 0x94D049BB133111EBull;
+      return (double)((z ^ (z >> 31)) >> 11) * (1.0 / 9007199254740992.0);
+    };
+    for (auto& v : rnd) {   // two uniforms -> Box-Muller
+      const double u1 = std::max(next(), 1e-300), u2 = next();
+      v = std::sqrt(-2.0 * std::log(u1)) * std::cos(6.283185307179586 * u2);
     }
-    sv[c] = vals;
+    double* F = Fv[c];
+    Buf qb = E.alloc(sizeof(double) * ((size_t)len * kk * 2 + (size_t)kk * kk + kk));
+    double* T = (double*)qb->ptr;
+    double* Q = T + (size_t)len * kk;
+    double* R = Q + (size_t)len * kk;
+    SPS_CUDA(cudaMemcpyAsync(T, F, sizeof(double) * (size_t)len * r, cudaMemcpyDeviceToDevice, E.stream));
+    E.stage(rnd.data(), sizeof(double) * rnd.size(), T + (size_t)len * r);
+    la::qr_batched(E, {la::MatDesc{T, Q, R, R + (size_t)kk * kk, len, kk, len, len, kk}});
+    SPS_CUDA(cudaMemcpyAsync(F + (size_t)len * r, Q + (size_t)len * r, sizeof(double) * (size_t)len * (kk - r),
+                             cudaMemcpyDeviceToDevice, E.stream));
+    keep.push_back(qb);
+    if (E.profile) E.add_stat("svd_topk.completed", 0.0, (long long)(kk - r));
   }
   int kk[2];
   double kept2, disc2;

@@ -16,7 +16,14 @@
 // Yamamoto, Yanagisawa, SIAM J. Sci. Comput. 42 (2020)) so that they cannot
 // break down.  Rayleigh-Ritz extraction: Q <- orth(Q) (plain pass),
 // M^T Q = Qb Rb (shifted Cholesky QR3), Rb^T = Ub S J^T by one-sided Jacobi in
-// one CTA, U = Q Ub, V = Qb J.  The extraction is accepted when
+// one CTA, U = Q Ub, V = Qb J.  When a plain pass meets a non-positive pivot
+// (trailing columns of the iterate at the rounding level, as a fast-decaying
+// spectrum leaves them, most of all on M M^T) it is redone with the shift and
+// followed by two deflating passes that zero those columns.  If fewer than k
+// columns survive on M M^T, the launch stops with status 4 (the caller then
+// iterates on M); on M the extraction goes on, and a converged extraction with
+// zero values among the wanted ones reports status 4 (the caller completes
+// their vectors).  The extraction is accepted when
 // ||M v_i - s_i u_i|| is within the requested relative residual (rounding
 // level unless the caller asks for less) for every wanted i; otherwise two
 // more iterations and a new extraction, up to a cap, after which the caller
@@ -346,13 +353,23 @@ __device__ void store_rows(const Ctx& x, double* A, int ld, int bb, int r0, int 
 
 // Cholesky QR pass on the distributed rows held in Ys (rows [r0, r1) of an
 // nrows x bb matrix).  racc: 0 none, 1 Racc = R, 2 Racc = R Racc (CTA 0).
-// Returns false (uniformly over the group) on breakdown.
-__device__ __noinline__ bool orth_pass(const Ctx& x, int bb, int r0, int r1, int nrows, bool shifted, int racc) {
+// mode OP_SHIFT: shifted Cholesky QR (never meets a non-positive pivot);
+// OP_PLAIN: plain Cholesky QR, redone with the shift when a pivot is not
+// positive (the iterate's trailing columns fell to the rounding level of G);
+// OP_DEFLATE: plain, dropping every column whose pivot is at the rounding
+// level of G (a zero column of the result, a zero row of R).
+// Returns -1 on breakdown, else bit 0 = redone with the shift (plain) or a
+// column left short of unit norm (shifted), bits 1.. = the number of dropped
+// columns; the value is the same in every CTA of the group (each factors the
+// same reduced G).
+enum : int { OP_SHIFT = 0, OP_PLAIN = 1, OP_DEFLATE = 2 };
+__device__ __noinline__ int orth_pass(const Ctx& x, int bb, int r0, int r1, int nrows, int mode, int racc) {
   const TopkProb& p = *x.p;
   double* Ys = x.sm + OFF_Y;
   double* Gs = x.sm + OFF_G;
   double* sq = x.sm + OFF_V;              // sqrt of the pivots
   double* invd = sq + KMAXB;              // 1 / pivots
+  double* defl = sq + 2 * KMAXB;          // 1: column dropped
   const int R = r1 - r0;
   // partial Gram of the owned rows (upper triangle)
   double* gp = p.Gp + (size_t)x.c * KMAXB * KMAXB;
@@ -394,37 +411,73 @@ __device__ __noinline__ bool orth_pass(const Ctx& x, int bb, int r0, int r1, int
   trace_mark(x, PH_REDUCE);
   // factor G (+ shift) redundantly: G = U^T D U with U unit upper, kept as the
   // unscaled upper rows D U in Gs
-  for (int i = ty; i < bb; i += 16)
-    for (int j = i + tx; j < bb; j += 16) Gs[i * GLD + j] = __ldcg(&p.G[i * bb + j]);
-  __syncthreads();
-  if (shifted) {
-    if (threadIdx.x < 32) {   // trace by one warp, then the shift of shifted Cholesky QR on the diagonal
-      double tr = 0.0;
-      for (int i = threadIdx.x; i < bb; i += 32) tr += Gs[i * GLD + i];
-      tr = wsum(tr);
-      const double sh = 11.0 * ((double)nrows * bb + (double)bb * (bb + 1)) * DBL_EPSILON * tr;
-      __syncwarp();
-      for (int i = threadIdx.x; i < bb; i += 32) Gs[i * GLD + i] += sh;
-    }
-  }
-  for (int j = 0; j < bb; ++j) {
+  int retried = 0;
+  for (int attempt = 0; attempt < 2; ++attempt) {
     __syncthreads();
-    const double d = Gs[j * GLD + j];
-    if (!(d > 0.0) || !isfinite(d)) {
+    for (int i = ty; i < bb; i += 16)
+      for (int j = i + tx; j < bb; j += 16) Gs[i * GLD + j] = __ldcg(&p.G[i * bb + j]);
+    for (int j = threadIdx.x; j < bb; j += TT) defl[j] = 0.0;
+    __syncthreads();
+    // the rounding level of G's pivots: a deflating pass drops the columns at
+    // or below it, a plain pass is redone with the shift when it meets one
+    const bool deflating = mode == OP_DEFLATE, plain = mode == OP_PLAIN && attempt == 0;
+    double delta = 0.0;
+    if (deflating || plain) {
+      double mx = 0.0;
+      for (int i = 0; i < bb; ++i) mx = fmax(mx, Gs[i * GLD + i]);
+      delta = 32.0 * bb * DBL_EPSILON * mx;
+    } else {
+      if (threadIdx.x < 32) {   // trace by one warp, then the shift of shifted Cholesky QR on the diagonal
+        double tr = 0.0;
+        for (int i = threadIdx.x; i < bb; i += 32) tr += Gs[i * GLD + i];
+        tr = wsum(tr);
+        const double sh = 11.0 * ((double)nrows * bb + (double)bb * (bb + 1)) * DBL_EPSILON * tr;
+        __syncwarp();
+        for (int i = threadIdx.x; i < bb; i += 32) Gs[i * GLD + i] += sh;
+      }
+    }
+    bool ok = true;
+    for (int j = 0; j < bb; ++j) {
+      __syncthreads();
+      const double d = Gs[j * GLD + j];
+      if (deflating && d <= delta) {   // dropped: no elimination by row j
+        if (threadIdx.x == 0) defl[j] = 1.0;
+        continue;
+      }
+      if (!(d > (plain ? delta : 0.0)) || !isfinite(d)) {
+        ok = false;
+        break;
+      }
+      const double inv = 1.0 / d;
+      const double* gj = Gs + j * GLD;
+      for (int i = j + 1 + ty; i < bb; i += 16) {
+        const double gji = gj[i] * inv;
+        for (int l = i + tx; l < bb; l += 16) Gs[i * GLD + l] -= gji * gj[l];
+      }
+    }
+    if (ok) break;
+    if (mode != OP_PLAIN || attempt == 1) {
       if (x.c == 0 && threadIdx.x == 0) p.info[0] = ST_BREAKDOWN;
-      return false;
+      return -1;
     }
-    const double inv = 1.0 / d;
-    const double* gj = Gs + j * GLD;
-    for (int i = j + 1 + ty; i < bb; i += 16) {
-      const double gji = gj[i] * inv;
-      for (int l = i + tx; l < bb; l += 16) Gs[i * GLD + l] -= gji * gj[l];
-    }
+    retried = 1;
   }
   __syncthreads();
+  int dropped = 0;
+  for (int j = 0; j < bb; ++j) dropped += defl[j] != 0.0;
+  // a shifted pass whose pivot stayed below twice the shift left that column
+  // short of unit norm (its part of the iterate was below the shift's scale)
+  int under = 0;
+  if (mode == OP_SHIFT) {
+    double tr = 0.0;
+    for (int i = 0; i < bb; ++i) tr += __ldcg(&p.G[i * bb + i]);
+    const double sh2 = 22.0 * ((double)nrows * bb + (double)bb * (bb + 1)) * DBL_EPSILON * tr;
+    for (int j = 0; j < bb; ++j) under |= Gs[j * GLD + j] < sh2;
+  }
   for (int j = threadIdx.x; j < bb; j += TT) {
-    sq[j] = sqrt(Gs[j * GLD + j]);
-    invd[j] = 1.0 / Gs[j * GLD + j];
+    const bool dj = defl[j] != 0.0;
+    sq[j] = dj ? 0.0 : sqrt(Gs[j * GLD + j]);
+    invd[j] = dj ? 0.0 : 1.0 / Gs[j * GLD + j];
   }
   __syncthreads();
   // unit upper U in place (diagonal kept as the pivot)
@@ -469,10 +522,20 @@ __device__ __noinline__ bool orth_pass(const Ctx& x, int bb, int r0, int r1, int
     __syncthreads();
   }
   for (int r = ty; r < R; r += 16)
-    for (int j = tx; j < bb; j += 16) Ys[r * YLD + j] /= sq[j];
+    for (int j = tx; j < bb; j += 16) Ys[r * YLD + j] = sq[j] > 0.0 ? Ys[r * YLD + j] / sq[j] : 0.0;
   __syncthreads();
   trace_mark(x, PH_APPLY);
-  return true;
+  return retried | under | (dropped << 1);
+}
+
+// The orthonormalisation of an iteration step: a shifted pass, repeated once
+// when it left a column short of unit norm (without the repeat, a column whose
+// singular value is below the shift's scale, about 5e-5 of the largest, shrinks
+// by that factor at every step until it reaches the rounding level).
+__device__ __forceinline__ int orth_iter(const Ctx& x, int bb, int r0, int r1, int nrows) {
+  const int f = orth_pass(x, bb, r0, r1, nrows, OP_SHIFT, 0);
+  if (f < 0 || !(f & 1)) return f;
+  return orth_pass(x, bb, r0, r1, nrows, OP_SHIFT, 0);
 }
 
 // One-sided Jacobi SVD of A = Racc^T (bb x bb) in CTA 0; sorted outputs to
@@ -675,7 +738,7 @@ __global__ void __launch_bounds__(TT, 1) topk_kernel(const TopkProb* __restrict_
   }
   gemm_rows(x, &p.tMt, p.Rm, &p.tZ, b, p.n, x.rm0, x.rm1);
   trace_mark(x, PH_GEMM);
-  if (!orth_pass(x, b, x.rm0, x.rm1, p.m, true, 0)) return;
+  if (orth_iter(x, b, x.rm0, x.rm1, p.m) < 0) return;
   store_rows(x, p.Q, p.ldm, b, x.rm0, x.rm1);
   sync_group(x);
   trace_mark(x, PH_STORE);
@@ -685,7 +748,7 @@ __global__ void __launch_bounds__(TT, 1) topk_kernel(const TopkProb* __restrict_
     for (; it < target && p.Gm; ++it) {   // Gram iteration: Q = orth(M M^T Q)
       gemm_rows(x, &p.tGm, p.Rm, &p.tQ, b, p.m, x.rm0, x.rm1);
       trace_mark(x, PH_GEMM);
-      if (!orth_pass(x, b, x.rm0, x.rm1, p.m, true, 0)) return;
+      if (orth_iter(x, b, x.rm0, x.rm1, p.m) < 0) return;
       store_rows(x, p.Q, p.ldm, b, x.rm0, x.rm1);
       sync_group(x);
       trace_mark(x, PH_STORE);
@@ -693,28 +756,53 @@ __global__ void __launch_bounds__(TT, 1) topk_kernel(const TopkProb* __restrict_
     for (; it < target; ++it) {
       gemm_rows(x, &p.tM, p.Rn, &p.tQ, b, p.m, x.rn0, x.rn1);
       trace_mark(x, PH_GEMM);
-      if (!orth_pass(x, b, x.rn0, x.rn1, p.n, true, 0)) return;
+      if (orth_iter(x, b, x.rn0, x.rn1, p.n) < 0) return;
       store_rows(x, p.Z, p.ldn, b, x.rn0, x.rn1);
       sync_group(x);
       trace_mark(x, PH_STORE);
       gemm_rows(x, &p.tMt, p.Rm, &p.tZ, b, p.n, x.rm0, x.rm1);
       trace_mark(x, PH_GEMM);
-      if (!orth_pass(x, b, x.rm0, x.rm1, p.m, true, 0)) return;
+      if (orth_iter(x, b, x.rm0, x.rm1, p.m) < 0) return;
       store_rows(x, p.Q, p.ldm, b, x.rm0, x.rm1);
       sync_group(x);
       trace_mark(x, PH_STORE);
     }
     // Rayleigh-Ritz: Q <- orth(Q); M^T Q = Qb Rb; Rb^T = Ub S J^T
+    // (a plain pass that had to be redone with the shift means columns at the
+    // rounding level: two deflating passes then make Q orthonormal with those
+    // columns zero; fewer than k columns left means the iteration lost wanted
+    // directions, ST_ZERO)
     load_rows(x, p.Q, p.ldm, b, x.rm0, x.rm1);
-    if (!orth_pass(x, b, x.rm0, x.rm1, p.m, false, 0)) return;
+    int fq = orth_pass(x, b, x.rm0, x.rm1, p.m, OP_PLAIN, 0);
+    if (fq < 0) return;
+    if (fq & 1)
+      for (int pass = 0; pass < 2; ++pass)
+        if ((fq = orth_pass(x, b, x.rm0, x.rm1, p.m, OP_DEFLATE, 0)) < 0) return;
     store_rows(x, p.Q, p.ldm, b, x.rm0, x.rm1);
     sync_group(x);
     trace_mark(x, PH_STORE);
     gemm_rows(x, &p.tM, p.Rn, &p.tQ, b, p.m, x.rn0, x.rn1);
     trace_mark(x, PH_GEMM);
-    if (!orth_pass(x, b, x.rn0, x.rn1, p.n, true, 1)) return;
-    if (!orth_pass(x, b, x.rn0, x.rn1, p.n, false, 2)) return;
-    if (!orth_pass(x, b, x.rn0, x.rn1, p.n, false, 2)) return;
+    if (orth_pass(x, b, x.rn0, x.rn1, p.n, OP_SHIFT, 1) < 0) return;
+    int fz = 0, redone = 0;
+    for (int pass = 0; pass < 2; ++pass) {
+      if ((fz = orth_pass(x, b, x.rn0, x.rn1, p.n, OP_PLAIN, 2)) < 0) return;
+      redone |= fz & 1;
+    }
+    if (redone)
+      for (int pass = 0; pass < 2; ++pass)
+        if ((fz = orth_pass(x, b, x.rn0, x.rn1, p.n, OP_DEFLATE, 2)) < 0) return;
+    if (p.Gm && (b - (fq >> 1) < k || b - (fz >> 1) < k)) {
+      // on M M^T: wanted directions below its rounding level; the caller
+      // iterates on M.  (On M, fewer than k surviving columns means fewer than
+      // k singular values above the rounding level: the extraction goes on and
+      // reports the missing ones as zero, status 4.)
+      if (x.c == 0 && threadIdx.x == 0) {
+        p.info[0] = ST_ZERO;
+        p.info[1] = it;
+      }
+      return;
+    }
     store_rows(x, p.Z, p.ldn, b, x.rn0, x.rn1);
     sync_group(x);
     trace_mark(x, PH_STORE);
@@ -768,11 +856,9 @@ __global__ void __launch_bounds__(TT, 1) topk_kernel(const TopkProb* __restrict_
       p.info[1] = it;
       p.info[3] = worst;
       int done = 0;
-      if (zero) {
-        p.info[0] = ST_ZERO;
+      if (worst <= 1.0) {
         done = 1;
-      } else if (worst <= 1.0) {
-        done = 1;
+        if (zero) p.info[0] = ST_ZERO;   // converged, with zero values among the wanted ones
       } else if (it + qstep > qmax) {
         p.info[0] = ST_NOCONV;
         done = 1;

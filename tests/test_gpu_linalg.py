@@ -100,6 +100,41 @@ def test_topk_gram_mode_matches_lapack(eng, m, n, k, decay):
     assert np.linalg.norm(mine - ref) <= 5e-8 * ref_s[0]
 
 
+@pytest.mark.parametrize("m,n,k,decay", [(648, 648, 18, 0.55), (630, 648, 18, 0.6), (1296, 1296, 36, 0.3),
+                                         (648, 648, 18, 0.8)])
+@pytest.mark.parametrize("gram", [True, False])
+def test_topk_fast_decay_matches_lapack(eng, m, n, k, decay, gram):
+    """Spectra that fall by 1e-5 to 1e-6 over the kept k values, as the boundary blocks of a purified
+    state do: the oversampling columns of the iterate reach the rounding level (on a a^T already
+    after two iterations), the plain Cholesky QR of the extraction meets non-positive pivots and is
+    redone with the shift plus two deflating passes.  The iteration steps repeat their shifted pass
+    when it leaves a column short of unit norm, so that wanted directions down to about 1e-9 of the
+    largest stay in the iterate.  The kept triplets still match LAPACK."""
+    a = graded(m, n, decay, 3 * m + n + k)
+    u, s, v, iters, ms = eng.la_svd_topk(a, k, gram=gram, rtol=1e-10)
+    ref_u, ref_s, _ = np.linalg.svd(a, full_matrices=False)
+    np.testing.assert_allclose(s, ref_s[:k], rtol=1e-9, atol=1e-12 * ref_s[0])
+    np.testing.assert_allclose(u.T @ u, np.eye(k), atol=1e-10)
+    np.testing.assert_allclose(v.T @ v, np.eye(k), atol=1e-10)
+    assert np.linalg.norm(a @ v - u * s, axis=0).max() <= 1e-10 * ref_s[0] * (1 + 1e-6)
+    mine = u @ (u.T @ a)
+    ref = ref_u[:, :k] @ (ref_u[:, :k].T @ a)
+    assert np.linalg.norm(mine - ref) <= 1e-9 * ref_s[0]
+
+
+def test_topk_rank_below_k_is_reported(eng):
+    """A block of rank 10 asked for 18 triplets: the plain Cholesky QR of the extraction meets pivots
+    at the rounding level and the deflating passes leave 10 columns.  On a a^T the call stops and
+    runs again on a, where the extraction converges with eight zero values: status 4, which this
+    entry point reports as non-convergence (the engine instead completes the eight vectors)."""
+    rng = np.random.default_rng(4)
+    a = rng.standard_normal((648, 10)) @ rng.standard_normal((10, 648))
+    for gram in (True, False):
+        with pytest.raises(Exception) as ei:
+            eng.la_svd_topk(a, 18, gram=gram, rtol=1e-10)
+        assert getattr(ei.value, "code", None) == 5
+
+
 @pytest.mark.parametrize("ta", [False, True])
 @pytest.mark.parametrize("m,n,k", [(1, 1, 1), (37, 19, 5), (130, 70, 17), (648, 18, 648), (2000, 648, 648),
                                    (648, 648, 23328), (300, 200, 0)])
