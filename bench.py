@@ -2,13 +2,13 @@
 """Born samples/s on the 8x8 open TFIM (J=1, h=3.0), D=6 (3+3), chi=36 (18+18).
 
 One step = W perfect Born draws (``sample_configuration``, src/sampling/born.jl:86-163)
-drawn at the same time from a device-resident SamplingCache of a seeded
-synthetic beta0 PEPO with the workload's shapes: per draw eight row absorptions
-and 64 conditionals.  The headline `value` is the zip-up absorption path
+drawn at the same time from a device-resident SamplingCache of the purified
+beta0 = 0.4 PEPO (stored, bench_states.py): per draw eight row absorptions and
+64 conditionals.  The headline `value` is the zip-up absorption path
 (FP64); the plain FP64 path (the reference's exact LQ + truncated-SVD
 compression, one sample per launch sequence) draws the same sample ids beside
 it (`plain_fp64`, `agreement_vs_plain`).  `pipeline` times the rest of the
-per-sample unit on the purified beta0 PEPO (stored, bench_states.py): projection, one full-update Trotter step
+per-sample unit on the same PEPO: projection, one full-update Trotter step
 (src/evolution/full_update.jl:559-597) and one energy measurement
 (src/measurement/energy.jl:31-78), and composes the per-sample rate for
 beta 0.4 -> 2.0 at tau = 0.02.  Every rank draws its own samples (weak
@@ -42,7 +42,7 @@ PEPO_SEED = 7
 BETA0, BETA_MAX, DTAU = 0.4, 2.0, 0.02
 MEASURE_BETAS = [0.5 + 0.25 * k for k in range(7)]   # 0.5, 0.75, ..., 2.0
 METRIC = "Born samples/s at 8x8 D6 χ36: batched mixed-prec vs plain FP64 GPU, ΔE≤1e-4"
-ORACLE_ENERGY = os.path.join(ROOT, "tests", "golden", "bench_8x8_D6_chi36_synthetic_energy.npz")
+ORACLE_ENERGY = os.path.join(ROOT, "tests", "golden", "bench_8x8_D6_chi36_energy.npz")
 
 PROBES = """probes (one hot operation on a representative input, run once to warm up and once more):
   svd_left          U-only Jacobi of a 648x648 LQ-preconditioned block
@@ -77,10 +77,8 @@ def parse():
 def workload_config(extra=None):
     c = {"workload": "tfim_8x8_D6_chi36_born_draw", "Lx": LX, "Ly": LY, "J": 1.0, "h": H_FIELD, "D": D,
          "bond_space": [D // 2, D // 2], "chi_sampling": CHI, "sampling_space": [CHI // 2, CHI // 2],
-         "pepo": f"draws: seeded synthetic beta0 stand-in (identity + {PEPO_EPS} Gaussian Z2 noise, seed "
-                 f"{PEPO_SEED}); the purified beta0 = 0.4 PEPO (stopeps.jl_b200/states/) has rank-deficient "
-                 "boundaries that send every truncated SVD of a draw to the full Jacobi SVD (~5 s per draw); "
-                 "pipeline: the purified PEPO",
+         "pepo": "the purified beta0 = 0.4 PEPO of the 8x8 TFIM (10 full-update steps at tau = 0.02 from the "
+                 "identity, D=6, chi=36; stored in stopeps.jl_b200/states/)",
          "step": "W Born draws from a device-resident SamplingCache",
          "uniforms": "numpy default_rng([seed, sample_id])", "seed": SEED,
          "l2": "inputs larger than L2 (the south boundaries and candidate double layers of the cache, ~0.6 GB)"}
@@ -161,12 +159,11 @@ class OracleRowDraws:
         from oracle import boundary as bm, model as omd, sampling as osp
         from oracle.z2 import T, leg
         import __graft_entry__ as ge
-        sites, dims = ge.load_package().synthetic.synthetic_pepo(LX, LY, D, PEPO_EPS, PEPO_SEED)
+        sites, dims, beta, log_amplitude = ge.load_package().bench_states.load()
         grid = [[None] * LY for _ in range(LX)]
         for i, (a, ld) in enumerate(zip(sites, dims)):
             grid[i % LX][i // LX] = T(np.asarray(a, float), [leg(int(p), int(q)) for p, q in ld])
-        st = omd.State(LX, LY, grid, BETA0, 0.0, "pepo")
-        omd.normalize_state(st)
+        st = omd.State(LX, LY, grid, beta, log_amplitude, "pepo")
         self.osp = osp
         self.ge = ge
         t = time.perf_counter()
@@ -212,7 +209,7 @@ def reference_arm(args, rank, world):
     line = {"impl": "reference", "metric": METRIC, "value": value, "unit": "samples/s", "n_gpus": args.gpus,
             "steps": args.steps, "warmup": args.warmup, "ms_per_step": dt * 1e3 / args.steps,
             "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
-            "data": "synthetic (a TFIM state prepared by this engine; no dataset)", "config": workload_config({"step": "one row of a Born draw (reference arm)"}),
+            "data": "synthetic (a TFIM state prepared by this engine, stored; no dataset)", "config": workload_config({"step": "one row of a Born draw (reference arm)"}),
             "cpu_baseline": {"value": value, "unit": "samples/s", "cores": cores, "kind": "port", "sample": sample},
             "e2e": {"value": value, "unit": "samples/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
     print(json.dumps(line), flush=True)
@@ -234,14 +231,6 @@ def cpu_baseline_sample(rows=2):
 # ---------------------------------------------------------------------------
 # GPU
 # ---------------------------------------------------------------------------
-def synthetic_state(sps, e):
-    """The seeded synthetic beta0 stand-in with the workload's shapes on the engine."""
-    sites, dims = sps.synthetic.synthetic_pepo(LX, LY, D, PEPO_EPS, PEPO_SEED)
-    st = e.upload_state(sites, dims, True, beta=BETA0)
-    sps.normalize_state(st)
-    return st
-
-
 def purified_state(sps, e):
     """The stored beta0 = 0.4 PEPO of the 8x8 TFIM (bench_states.py) on the engine."""
     sites, dims, beta, log_amplitude = sps.bench_states.load()
@@ -300,7 +289,7 @@ def ours_arm(args, rank, world, local_rank):
         dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=600))
     torch.cuda.set_device(local_rank)
     e = sps.Engine(LX, LY, sps.TFIM(1.0, H_FIELD), device=local_rank)
-    st = synthetic_state(sps, e)
+    st = purified_state(sps, e)
     space = sps.Z2Space(CHI // 2, CHI // 2)
     W = max(1, args.concurrency)
     L = LX * LY
@@ -414,7 +403,7 @@ def ours_arm(args, rank, world, local_rank):
     oracle_e = None
     if os.path.exists(ORACLE_ENERGY):
         fx = np.load(ORACLE_ENERGY)
-        if "state" in fx and str(fx["state"]) == "synthetic":   # made for this very state
+        if "state" in fx and str(fx["state"]) == sps.bench_states.PURIFIED_8X8:   # made for this very state
             oracle_e = float(fx["energy"][1])
     ref_e = oracle_e if oracle_e is not None else en_plain["energy_per_site"]
     precision = {"energy_per_site_oracle_fp64": oracle_e,
@@ -426,14 +415,12 @@ def ours_arm(args, rank, world, local_rank):
                  "abs_delta_e_plain_vs_oracle": abs(en_plain["energy_per_site"] - ref_e),
                  "reference": "oracle" if oracle_e is not None else "plain FP64 GPU (oracle fixture missing)",
                  "tolerance": 1e-4,
-                 "state": "the synthetic beta0 stand-in of the draws, chi=36 (18+18)"}
+                 "state": "the purified beta0 = 0.4 PEPO of the draws, chi=36 (18+18)"}
 
     pipeline = None
     if not args.no_pipeline:
         try:
-            pst = purified_state(sps, e)
-            pipeline = pipeline_timing(sps, e, pst, zip_run["draws"], W, space, np, torch, local_rank, dist)
-            del pst
+            pipeline = pipeline_timing(sps, e, st, zip_run["draws"], W, space, np, torch, local_rank, dist)
         except Exception as ex:   # reported in the line; the draw measurement stands on its own
             e.set_concurrency(1)
             pipeline = {"error": f"{type(ex).__name__}: {ex}"}
@@ -452,7 +439,7 @@ def ours_arm(args, rank, world, local_rank):
         n_h2d = 8 * L * W
         result = {"metric": METRIC, "value": value, "unit": "samples/s", "n_gpus": world, "steps": args.steps,
                   "warmup": args.warmup, "ms_per_step": zip_run["ms"] / args.steps, "higher_is_better": True,
-                  "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic (a TFIM state prepared by this engine; no dataset)",
+                  "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic (a TFIM state prepared by this engine, stored; no dataset)",
                   "config": workload_config({"parallelism": f"samples sharded over {world} GPU(s)",
                                              "path": f"zip-up boundary absorption, FP64, {W} samples "
                                                      "concurrently (own stream and workspace each)",
