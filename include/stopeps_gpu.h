@@ -100,6 +100,11 @@ typedef struct sps_sample_report {
   double log_probability;
   double max_environment_truncation;
   int32_t near_boundary; /* draws whose uniform lay within 1e-12 of a cumulative probability */
+  /* kind = physical (the resampling proposal): the `repairs` records of the
+   * draw (born.jl:119-131) as counts, 0 for the auxiliary kind */
+  int32_t metric_repairs;          /* site metrics whose negative eigenvalues were clipped */
+  int32_t zero_proposals;          /* sites whose allowed outcomes all had zero weight */
+  double min_relative_eigenvalue;  /* smallest site-metric eigenvalue / its spectral scale (<= 0) */
 } sps_sample_report;
 
 /* --- lifetime ------------------------------------------------------------ */
@@ -206,6 +211,14 @@ int sps_measure_energy(sps_handle* h, int32_t state_id, const sps_boundary* meth
                        double* site_x, double* se_north, double* se_south);
 /* SamplingCache(state, BoundaryMPS; kind=:auxiliary) (src/sampling/born.jl:56-73) */
 int sps_sampling_cache(sps_handle* h, int32_t pepo_id, const sps_boundary* method, int32_t* cache_id);
+/* SamplingCache(state, BoundaryMPS; kind) (src/sampling/born.jl:56-73):
+ * kind 0 = :auxiliary (state a PEPO; the same as sps_sampling_cache), 1 =
+ * :physical (state a PEPS, e.g. a projected and evolved sample: the Born
+ * proposal of annealed resampling over physical labels 1 (even) / 2 (odd),
+ * conditionals from the PSD-projected site holes, born.jl:117-134, and
+ * configurations restricted to the PEPS's total parity). */
+int sps_sampling_cache_kind(sps_handle* h, int32_t state_id, const sps_boundary* method, int32_t kind,
+                            int32_t* cache_id);
 int sps_sampling_cache_free(sps_handle* h, int32_t cache_id);
 /* sample_configuration(cache; rng) with the Lx*Ly uniforms (row-major site
  * order) in place of rand(rng) (src/sampling/born.jl:86-163).  configuration
@@ -221,6 +234,12 @@ int sps_sample_conditionals(sps_handle* h, int32_t cache_id, const double* unifo
 /* sample_configuration(cache; configuration) : probability of a given draw */
 int sps_sample_probability(sps_handle* h, int32_t cache_id, const int32_t* configuration,
                            sps_sample_report* report);
+/* sample_configuration(cache; configuration) for n configurations (n x
+ * Lx*Ly labels): the scores of a resampling event (_score_configurations!,
+ * src/resample/scores.jl:38-71) in one call, spread over the concurrent
+ * samples like sps_sample_batch; reports may be NULL. */
+int sps_sample_probability_batch(sps_handle* h, int32_t cache_id, int32_t n, const int32_t* configurations,
+                                 double* log_probabilities, sps_sample_report* reports);
 /* No counterpart in the reference (its ensemble is spread over MPI ranks):
  * the number of samples sps_sample_batch draws at the same time, each on its
  * own CUDA stream and device workspace, sharing the read-only SamplingCache

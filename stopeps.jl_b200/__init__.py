@@ -11,7 +11,7 @@ from .config import (Z2Space, Lattice, TFIM, FullUpdate, BoundaryMPS, BoundaryMP
 from .engine import (Engine, DeviceState, SamplingCache, normalize_state, evolution_step, lognorm,
                      measure_energy, sample_configuration, sample_batch, project_configuration,
                      project_batch, evolution_step_batch, measure_energy_batch, lognorm_batch,
-                     sample_conditionals)
+                     sample_conditionals, sample_probability_batch)
 from .driver import (run_purification, run_stochastic, ensemble_statistics, group_configurations,
                      sample_uniforms, step_schedule, ThermalCheckpoint, Particle, RESULT_SCHEMA_VERSION)
 from . import _lib
@@ -25,7 +25,8 @@ __all__ = [
     "SymmetryBasis", "RunConfig", "validate_config", "temperature_nodes", "parameter_dict", "Engine",
     "DeviceState", "SamplingCache", "normalize_state", "evolution_step", "lognorm", "measure_energy",
     "sample_configuration", "sample_batch", "project_configuration", "project_batch", "evolution_step_batch",
-    "measure_energy_batch", "lognorm_batch", "sample_conditionals", "run_purification", "run_stochastic",
+    "measure_energy_batch", "lognorm_batch", "sample_conditionals", "sample_probability_batch",
+    "run_purification", "run_stochastic",
     "ensemble_statistics", "group_configurations", "sample_uniforms", "step_schedule", "ThermalCheckpoint",
     "Particle", "RESULT_SCHEMA_VERSION", "build", "LIBRARY_PATH",
 ]

@@ -420,23 +420,43 @@ std::vector<double> normalize_state(Engine& E, State& s) {
 }
 
 // ---------------------------------------------------------------------------
-// Born sampling (src/sampling/born.jl:56-163), kind = :auxiliary
+// Born sampling (src/sampling/born.jl:56-163), kind = :auxiliary and :physical
 // ---------------------------------------------------------------------------
 static Tensor project_aux(Engine& E, const Tensor& A, int k) {
   return slice_leg(E, A, 3, k, k == 0 ? make_par(1, 0) : make_par(0, 1));
 }
 
-SamplingCache make_sampling_cache(Engine& E, const State& s, const BMPS& m) {
+// _project(A, B, k, :physical) for SymmetryBasis (basis.jl:87): the physical
+// leg restricted to its basis state k, a one-dimensional leg of that state's parity
+static Tensor project_physical(Engine& E, const Tensor& A, int k) {
+  const int c = (*A.legs[2])[k];
+  return slice_leg(E, A, 2, k, c == 0 ? make_par(1, 0) : make_par(0, 1));
+}
+
+SamplingCache make_sampling_cache(Engine& E, const State& s, const BMPS& m, int kind) {
+  if (kind != KIND_AUXILIARY && kind != KIND_PHYSICAL) throw Error(SPS_ERR_ARGUMENT, "unknown sampling kind");
   SamplingCache c;
   c.Lx = s.Lx;
   c.Ly = s.Ly;
+  c.kind = kind;
   c.method = m;
   c.state_ref = &s;
+  if (kind == KIND_PHYSICAL) {
+    // a PEPS (one-dimensional auxiliary legs); its total charge is the fusion
+    // of the auxiliary charges (_state_charge, basis.jl:89-92), which every
+    // physical configuration of nonzero amplitude fuses to
+    c.target = 0;
+    for (auto& A : s.sites) {
+      if (A.dims[3] != 1) throw Error(SPS_ERR_ARGUMENT, "proposal requires PEPS");
+      if (A.dims[2] != 2) throw Error(SPS_ERR_ARGUMENT, "proposal sampling needs a two-state physical leg");
+      c.target ^= (*A.legs[3])[0];
+    }
+  }
   c.layers = row_layers(E, s);
   for (auto& A : s.sites) {
     std::array<Tensor, 2> cand, kets;
     for (int k = 0; k < 2; ++k) {
-      kets[k] = project_aux(E, A, k);
+      kets[k] = kind == KIND_PHYSICAL ? project_physical(E, A, k) : project_aux(E, A, k);
       cand[k] = double_layer(E, kets[k], kets[k]);
     }
     c.candidates.push_back(cand);
@@ -632,8 +652,152 @@ static SampleResult sample_device(Engine& E, const SamplingCache& c, const doubl
   return res;
 }
 
+// The site hole of a row (born.jl:75-84): left, top, bottom and right
+// environments joined around site x, each fused double-layer leg split into
+// (ket, bra), as a symmetric matrix on the ket virtual legs: scaled by its
+// Frobenius norm and symmetrised, then projected on its nonnegative spectrum
+// (_positive_metric with square_root, tensors.jl:65-94).  Returns the
+// eigenvectors scaled by the square roots of the clipped eigenvalues (legs
+// w, n, e, s, z), so that a candidate's weight is |v . root|^2.
+static Tensor site_metric_root(Engine& E, const Tensor& left, const Tensor& top, const Tensor& bottom,
+                               const Tensor& right, const Tensor& A, SampleResult& res) {
+  Tensor X = ein(E, "awb,anc->wbnc", left, top);
+  Tensor Y = ein(E, "bsd,ced->bsce", bottom, right);
+  Tensor H = contiguous(E, ein(E, "wbnc,bsce->wnes", X, Y));
+  const int vl[4] = {0, 1, 4, 5};   // the site's virtual legs w, n, e, s
+  for (int k = 3; k >= 0; --k) H = split(E, H, k, {A.legs[vl[k]], A.legs[vl[k]]});   // (wk wb nk nb ek eb sk sb)
+  if (!all_finite(E, H)) throw Error(SPS_ERR_NUMERIC, "nonfinite norm metric");
+  const double scale = norm(E, H);
+  Tensor Hm = contiguous(E, perm_view(H, {1, 3, 5, 7, 0, 2, 4, 6}));   // (bras, kets)
+  Tensor HmT = perm_view(Hm, {4, 5, 6, 7, 0, 1, 2, 3});
+  const double f = scale != 0 ? 0.5 / scale : 0.5;
+  Tensor Hs = axpby(E, f, Hm, f, HmT);
+  int64_t half = 1;
+  for (int k = 0; k < 4; ++k) half *= Hs.dims[k];
+  EIGres eg = (half / 2 >= E.eigh_multi_min) ? eigh_unit_shifted(E, Hs, {0, 1, 2, 3}, {4, 5, 6, 7})
+                                             : eigh(E, Hs, {0, 1, 2, 3}, {4, 5, 6, 7});
+  std::vector<double> root;
+  double lo = 0.0, hi = 0.0;
+  int negative = 0;
+  for (int c = 0; c < 2; ++c)
+    for (double v : eg.w[c]) {
+      lo = std::min(lo, v);
+      hi = std::max(hi, std::fabs(v));
+      negative += v < 0;
+      root.push_back(v > 0 ? std::sqrt(v) : 0.0);
+    }
+  res.metric_repairs += negative > 0;
+  res.min_relative_eigenvalue = std::min(res.min_relative_eigenvalue, lo / std::max(hi, DBL_MIN));
+  return scale_leg(E, eg.V, 4, root);
+}
+
+// sample_configuration for kind = :physical (born.jl:86-163): the Born
+// proposal of a PEPS over its physical labels.  Each conditional weighs the
+// site's two physically projected kets with the PSD-projected site hole;
+// outcomes that cannot reach the PEPS's total parity get no weight (the
+// charge rule of born.jl:114-116, which binds at the last site), all-zero
+// weights fall back to the uniform choice among the allowed outcomes
+// (born.jl:127-131), and the last row is not absorbed.
+static SampleResult sample_physical(Engine& E, const SamplingCache& c, const double* uniforms,
+                                    const int* configuration) {
+  const int Lx = c.Lx, Ly = c.Ly, L = Lx * Ly;
+  SampleResult res;
+  res.config.assign(L, 0);
+  double maxtr = 0;
+  for (auto& e : c.south) maxtr = std::max(maxtr, e.max_trunc);
+  res.max_env_trunc = maxtr;
+  if (configuration) {
+    int charge = 0;
+    for (int i = 0; i < L; ++i) {
+      if (configuration[i] != 1 && configuration[i] != 2)
+        throw Error(SPS_ERR_ARGUMENT, "configuration contains an unknown basis label");
+      charge ^= configuration[i] - 1;
+    }
+    if (charge != c.target) {
+      for (int i = 0; i < L; ++i) res.config[i] = configuration[i];
+      res.log_probability = -INFINITY;
+      return res;
+    }
+  }
+  Env north = trivial_boundary(E, column(c.layers, Lx, 0), true);
+  int prefix = 0;
+  double logp = 0;
+  for (int y = 0; y < Ly; ++y) {
+    std::vector<Layer> row(Lx);
+    std::vector<Tensor> rowt = column(c.layers, Lx, y);
+    for (int x = 0; x < Lx; ++x) {
+      row[x].a = rowt[x];
+      row[x].ket = c.state_ref->sites[x + y * Lx];
+      row[x].layered = true;
+    }
+    const auto& top = north.t;
+    const auto& bottom = c.south[y + 1].t;
+    RowEnvs e = row_environments(E, top, row, bottom, 2);
+    Tensor left = e.left[0];
+    std::vector<Tensor> rt(Lx), rk(Lx);
+    for (int x = 0; x < Lx; ++x) {
+      const int site = x + y * Lx;
+      const Tensor& A = c.state_ref->sites[site];
+      Tensor root = site_metric_root(E, left, top[x], bottom[x], e.right[x + 1], A, res);
+      bool allowed[2];
+      double values[2];
+      for (int k = 0; k < 2; ++k) {
+        // every later site offers both parities, so only the last site is bound
+        allowed[k] = site < L - 1 || (prefix ^ (*A.legs[2])[k]) == c.target;
+        values[k] = 0.0;
+        if (!allowed[k]) continue;
+        Tensor u = ein(E, "wnpaes,wnesz->paz", c.candidate_kets[site][k], root);
+        values[k] = dot(E, u, u);
+      }
+      if (!allowed[0] && !allowed[1]) throw Error(SPS_ERR_BORN, "sampling prefix violates the total symmetry sector");
+      const double total = values[0] + values[1];
+      if (!std::isfinite(total)) throw Error(SPS_ERR_NUMERIC, "nonfinite proposal weight");
+      double p[2];
+      if (total == 0) {
+        const int n = (int)allowed[0] + (int)allowed[1];
+        for (int k = 0; k < 2; ++k) p[k] = allowed[k] ? 1.0 / n : 0.0;
+        res.zero_proposals++;
+      } else {
+        for (int k = 0; k < 2; ++k) p[k] = values[k] / total;
+      }
+      int k;
+      if (configuration) {
+        k = configuration[site] - 1;
+      } else {
+        std::vector<double> lm{p[0] > 0 ? std::log(p[0]) : -INFINITY, p[1] > 0 ? std::log(p[1]) : -INFINITY};
+        k = categorical(lm, uniforms[site], &res.near_boundary);
+      }
+      res.config[site] = k + 1;
+      res.conditionals.push_back(p[k]);
+      if (p[k] == 0.0) {
+        res.log_probability = -INFINITY;
+        res.max_env_trunc = maxtr;
+        return res;
+      }
+      logp += std::log(p[k]);
+      prefix ^= (*A.legs[2])[k];
+      rt[x] = c.candidates[site][k];
+      rk[x] = c.candidate_kets[site][k];
+      if (x < Lx - 1) {
+        Tensor LT = ein(E, "awb,anc->wbnc", left, top[x]);
+        Tensor Yk = layer_apply_wn(E, LT, rk[x]);
+        left = ein(E, "bces,bsd->ced", Yk, bottom[x]);
+        safe_scale_inplace(E, left);
+      }
+    }
+    if (y < Ly - 1) {
+      north = absorb(E, north, rt, c.method, true, nullptr, y + 1, &rk);
+      maxtr = std::max(maxtr, north.max_trunc);
+    }
+  }
+  res.log_probability = logp;
+  res.max_env_trunc = maxtr;
+  return res;
+}
+
 SampleResult sample_configuration(Engine& E, const SamplingCache& c, const double* uniforms,
                                   const int* configuration) {
+  if (c.kind == KIND_PHYSICAL) return sample_physical(E, c, uniforms, configuration);
   if (uniforms && !configuration && c.Lx * c.Ly + 1 <= Engine::NSCAL - 64 && c.Lx + 3 <= 128)
     return sample_device(E, c, uniforms);
   const int Lx = c.Lx, Ly = c.Ly;

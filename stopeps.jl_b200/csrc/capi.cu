@@ -773,6 +773,15 @@ int sps_lognorm_batch(sps_handle* h, int32_t n, const int32_t* state_ids, const 
   });
 }
 
+static void fill_sample(const SampleResult& r, sps_sample_report& o) {
+  o.log_probability = r.log_probability;
+  o.max_environment_truncation = r.max_env_trunc;
+  o.near_boundary = r.near_boundary;
+  o.metric_repairs = r.metric_repairs;
+  o.zero_proposals = r.zero_proposals;
+  o.min_relative_eigenvalue = r.min_relative_eigenvalue;
+}
+
 int sps_sampling_cache(sps_handle* h, int32_t pepo_id, const sps_boundary* method, int32_t* cache_id) {
   return guarded(h, [&] {
     State& s = get_state(h, pepo_id);
@@ -782,6 +791,21 @@ int sps_sampling_cache(sps_handle* h, int32_t pepo_id, const sps_boundary* metho
     h->states[sid] = s;
     int id = h->next_id++;
     h->caches[id] = make_sampling_cache(*h->E, h->states[sid], to_bmps(method));
+    h->cache_state[id] = sid;
+    *cache_id = id;
+  });
+}
+
+int sps_sampling_cache_kind(sps_handle* h, int32_t state_id, const sps_boundary* method, int32_t kind,
+                            int32_t* cache_id) {
+  return guarded(h, [&] {
+    State& s = get_state(h, state_id);
+    if (kind == KIND_AUXILIARY && !s.pepo) throw Error(SPS_ERR_ARGUMENT, "auxiliary sampling requires a PEPO");
+    if (kind == KIND_PHYSICAL && s.pepo) throw Error(SPS_ERR_ARGUMENT, "proposal requires PEPS");
+    int sid = h->next_id++;
+    h->states[sid] = s;
+    int id = h->next_id++;
+    h->caches[id] = make_sampling_cache(*h->E, h->states[sid], to_bmps(method), kind);
     h->cache_state[id] = sid;
     *cache_id = id;
   });
@@ -811,11 +835,7 @@ int sps_sample(sps_handle* h, int32_t cache_id, const double* uniforms, int32_t*
     SampleResult r = sample_configuration(*h->E, c, uniforms, nullptr);
     if (configuration)
       for (size_t i = 0; i < r.config.size(); ++i) configuration[i] = r.config[i];
-    if (report) {
-      report->log_probability = r.log_probability;
-      report->max_environment_truncation = r.max_env_trunc;
-      report->near_boundary = r.near_boundary;
-    }
+    if (report) fill_sample(r, *report);
   });
 }
 
@@ -831,11 +851,7 @@ int sps_sample_conditionals(sps_handle* h, int32_t cache_id, const double* unifo
       for (size_t i = 0; i < r.config.size(); ++i) configuration[i] = r.config[i];
     if (conditionals)
       for (size_t i = 0; i < r.config.size(); ++i) conditionals[i] = i < r.conditionals.size() ? r.conditionals[i] : 0.0;
-    if (report) {
-      report->log_probability = r.log_probability;
-      report->max_environment_truncation = r.max_env_trunc;
-      report->near_boundary = r.near_boundary;
-    }
+    if (report) fill_sample(r, *report);
   });
 }
 
@@ -846,11 +862,7 @@ int sps_sample_probability(sps_handle* h, int32_t cache_id, const int32_t* confi
     SamplingCache& c = get_cache(h, cache_id);
     std::vector<int> cfg(configuration, configuration + c.Lx * c.Ly);
     SampleResult r = sample_configuration(*h->E, c, nullptr, cfg.data());
-    if (report) {
-      report->log_probability = r.log_probability;
-      report->max_environment_truncation = r.max_env_trunc;
-      report->near_boundary = 0;
-    }
+    if (report) fill_sample(r, *report);
   });
 }
 
@@ -866,11 +878,22 @@ int sps_sample_batch(sps_handle* h, int32_t cache_id, int32_t n, const double* u
       SampleResult r = sample_configuration(E, c, uniforms + (size_t)i * L, nullptr);
       for (int k = 0; k < L; ++k) configurations[(size_t)i * L + k] = r.config[k];
       log_probabilities[i] = r.log_probability;
-      if (reports) {
-        reports[i].log_probability = r.log_probability;
-        reports[i].max_environment_truncation = r.max_env_trunc;
-        reports[i].near_boundary = r.near_boundary;
-      }
+      if (reports) fill_sample(r, reports[i]);
+    });
+  });
+}
+
+int sps_sample_probability_batch(sps_handle* h, int32_t cache_id, int32_t n, const int32_t* configurations,
+                                 double* log_probabilities, sps_sample_report* reports) {
+  return guarded(h, [&] {
+    if (n > 0 && (!configurations || !log_probabilities)) throw Error(SPS_ERR_ARGUMENT, "missing batch buffers");
+    SamplingCache& c = get_cache(h, cache_id);
+    const int L = c.Lx * c.Ly;
+    run_batch(h, n, [&](Engine& E, int i) {
+      std::vector<int> cfg(configurations + (size_t)i * L, configurations + (size_t)(i + 1) * L);
+      SampleResult r = sample_configuration(E, c, nullptr, cfg.data());
+      log_probabilities[i] = r.log_probability;
+      if (reports) fill_sample(r, reports[i]);
     });
   });
 }

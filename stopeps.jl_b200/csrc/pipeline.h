@@ -121,8 +121,11 @@ StepReport evolution_step(Engine& E, State& s, const Model& m, double delta, int
 std::vector<double> normalize_state(Engine& E, State& s);
 
 // sampling
+enum SamplingKind : int { KIND_AUXILIARY = 0, KIND_PHYSICAL = 1 };
 struct SamplingCache {
   int Lx, Ly;
+  int kind = KIND_AUXILIARY;   // the leg the draw labels: auxiliary (PEPO) or physical (PEPS proposal)
+  int target = -1;             // physical kind: the PEPS's total parity, which a configuration must fuse to
   std::vector<Tensor> layers;
   std::vector<std::array<Tensor, 2>> candidates;
   std::vector<std::array<Tensor, 2>> candidate_kets;   // the projected single layers of the candidates
@@ -130,13 +133,17 @@ struct SamplingCache {
   BMPS method;
   const State* state_ref = nullptr;
 };
-SamplingCache make_sampling_cache(Engine& E, const State& s, const BMPS& m);
+SamplingCache make_sampling_cache(Engine& E, const State& s, const BMPS& m, int kind = KIND_AUXILIARY);
 struct SampleResult {
   std::vector<int> config;   // labels 1/2, index x + y*Lx
   double log_probability = 0;
   double max_env_trunc = 0;
   std::vector<double> conditionals;
   int near_boundary = 0;     // draws within 1e-12 of a cumulative boundary
+  // physical kind: the PSD projections of the site metrics (born.jl:119-121)
+  int metric_repairs = 0;              // site metrics with negative eigenvalues clipped
+  double min_relative_eigenvalue = 0;  // the smallest eigenvalue / spectral scale over the sites
+  int zero_proposals = 0;              // sites whose allowed outcomes all had zero weight
 };
 SampleResult sample_configuration(Engine& E, const SamplingCache& c, const double* uniforms,
                                   const int* configuration);

@@ -358,14 +358,24 @@ def measure_energy(state: DeviceState, contraction: BoundaryMPS, site_profile=Fa
     return out
 
 
-class SamplingCache:
-    """``SamplingCache(state, contraction; kind=:auxiliary)`` on the device."""
+SAMPLING_KINDS = {"auxiliary": 0, "physical": 1}
 
-    def __init__(self, state: DeviceState, contraction: BoundaryMPS):
+
+class SamplingCache:
+    """``SamplingCache(state, contraction; kind)`` on the device: ``kind="auxiliary"``
+    draws the auxiliary labels of a thermal PEPO, ``kind="physical"`` the
+    physical labels of a PEPS (the Born proposal of annealed resampling,
+    ``born.jl:117-134``)."""
+
+    def __init__(self, state: DeviceState, contraction: BoundaryMPS, kind="auxiliary"):
+        if kind not in SAMPLING_KINDS:
+            raise ValueError("unknown sampling kind")
         self.engine = state.engine
+        self.kind = kind
         cid = C.c_int32()
         b = _boundary(contraction)
-        self.engine.check(self.engine.lib.sps_sampling_cache(self.engine.h, state.id, C.byref(b), C.byref(cid)))
+        self.engine.check(self.engine.lib.sps_sampling_cache_kind(self.engine.h, state.id, C.byref(b),
+                                                                  SAMPLING_KINDS[kind], C.byref(cid)))
         self.id = cid.value
 
     def __del__(self):
@@ -389,7 +399,7 @@ def sample_configuration(cache: SamplingCache, uniforms=None, configuration=None
         cfg = np.ascontiguousarray(np.asarray(configuration, np.int32).T.reshape(-1))
         e.check(e.lib.sps_sample_probability(e.h, cache.id, _arr(cfg, C.c_int32), C.byref(rep)))
         return dict(configuration=np.asarray(configuration), log_probability=rep.log_probability,
-                    max_environment_truncation=rep.max_environment_truncation)
+                    max_environment_truncation=rep.max_environment_truncation, **_repairs(rep))
     if uniforms is None:
         raise ValueError("an explicit RNG is required")
     u = np.ascontiguousarray(np.asarray(uniforms, np.float64).reshape(-1))
@@ -398,7 +408,30 @@ def sample_configuration(cache: SamplingCache, uniforms=None, configuration=None
     out = np.zeros(L, np.int32)
     e.check(e.lib.sps_sample(e.h, cache.id, _arr(u, C.c_double), _arr(out, C.c_int32), C.byref(rep)))
     return dict(configuration=out.reshape(e.Ly, e.Lx).T.copy(), log_probability=rep.log_probability,
-                max_environment_truncation=rep.max_environment_truncation, near_boundary=rep.near_boundary)
+                max_environment_truncation=rep.max_environment_truncation, near_boundary=rep.near_boundary,
+                **_repairs(rep))
+
+
+def _repairs(rep):
+    """The physical kind's PSD-repair counts of a draw (zero for the auxiliary kind)."""
+    return dict(metric_repairs=rep.metric_repairs, zero_proposals=rep.zero_proposals,
+                min_relative_eigenvalue=rep.min_relative_eigenvalue)
+
+
+def sample_probability_batch(cache: SamplingCache, configurations):
+    """``sample_configuration(cache; configuration)`` for each of n configurations
+    ((n, Lx, Ly) labels) in one call: (log_probabilities, reports)."""
+    e = cache.engine
+    L = e.Lx * e.Ly
+    cfgs = np.asarray(configurations, np.int32)
+    n = cfgs.shape[0]
+    flat = np.ascontiguousarray(np.transpose(cfgs, (0, 2, 1)).reshape(n, L))
+    lps = np.zeros(n)
+    reps = (_lib.sps_sample_report * max(n, 1))()
+    e.check(e.lib.sps_sample_probability_batch(e.h, cache.id, n, _arr(flat, C.c_int32), _arr(lps, C.c_double),
+                                               reps))
+    return lps, [dict(max_environment_truncation=reps[i].max_environment_truncation, **_repairs(reps[i]))
+                 for i in range(n)]
 
 
 def sample_conditionals(cache: SamplingCache, uniforms=None, configuration=None):
