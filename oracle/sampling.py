@@ -27,14 +27,41 @@ def project(A: T, k: int) -> T:
                                           A.p[4], A.p[5]])
 
 
-class SamplingCache:
-    """``SamplingCache(state, method; kind=:auxiliary)`` (``born.jl:56-73``)."""
+def project_physical(A: T, k: int) -> T:
+    """``_project(A,B,k,:physical)`` for ``SymmetryBasis`` (``basis.jl:64-68,87``):
+    the physical leg restricted to its basis state k, a one-dimensional leg of
+    that state's parity."""
+    c = int(A.p[2][k])
+    return T(A.a[:, :, k:k + 1, :, :, :], [A.p[0], A.p[1], z2.leg(1, 0) if c == 0 else z2.leg(0, 1),
+                                          A.p[3], A.p[4], A.p[5]])
 
-    def __init__(self, state: State, method: bm.BoundaryMPS):
+
+class SamplingCache:
+    """``SamplingCache(state, method; kind)`` (``born.jl:56-73``).
+
+    ``kind="auxiliary"`` labels the auxiliary leg of a PEPO; ``kind="physical"``
+    the physical leg of a PEPS (the resampling proposal), whose configurations
+    must fuse to the PEPS's total charge: the fusion of its one-dimensional
+    auxiliary legs (``_state_charge``, ``basis.jl:89-92``)."""
+
+    def __init__(self, state: State, method: bm.BoundaryMPS, kind="auxiliary"):
+        if kind not in ("auxiliary", "physical"):
+            raise ValueError("unknown sampling kind")
         self.state = state
         self.method = method
+        self.kind = kind
+        self.target = None
+        if kind == "physical":
+            self.target = 0
+            for y in range(state.Ly):
+                for x in range(state.Lx):
+                    A = state[x, y]
+                    if A.shape[3] != 1:
+                        raise ValueError("proposal requires PEPS")
+                    self.target ^= int(A.p[3][0])
+        proj = project_physical if kind == "physical" else project
         self.layers = bm.row_layers(state)
-        self.candidates = [[[bm.double_layer(project(state[x, y], k)) for k in (0, 1)]
+        self.candidates = [[[bm.double_layer(proj(state[x, y], k)) for k in (0, 1)]
                             for y in range(state.Ly)] for x in range(state.Lx)]
         Ly = state.Ly
         self.south = [None] * (Ly + 1)
@@ -92,6 +119,8 @@ def sample_configuration(cache: SamplingCache, uniforms=None, configuration=None
     ``uniforms`` (length Lx*Ly, row-major) replaces ``rand(rng)``;
     ``configuration`` (labels 1/2, indexed [x][y]) evaluates a given draw.
     """
+    if cache.kind == "physical":
+        return sample_physical(cache, uniforms, configuration)
     rows = sample_rows(cache, uniforms, configuration)
     while True:
         try:
@@ -145,6 +174,139 @@ def sample_rows(cache: SamplingCache, uniforms=None, configuration=None):
         yield y
     return dict(configuration=selected, log_probability=logp, conditionals=conditionals,
                 max_environment_truncation=maxtr, raw=raws)
+
+
+def site_hole(L: T, Tt: T, B: T, R: T, A: T) -> T:
+    """``_site_hole`` (``born.jl:75-84``): the row environments around one site,
+    each fused double-layer leg split into (ket, bra); legs (wk,wb,nk,nb,ek,eb,sk,sb)."""
+    X = einsum("awb,anc->wbnc", L, Tt)
+    Y = einsum("bsd,ced->bsce", B, R)
+    H = einsum("wbnc,bsce->wnes", X, Y)
+    for k, axis in reversed(list(enumerate((0, 1, 4, 5)))):
+        H = z2.split(H, k, [A.p[axis], A.p[axis]])
+    return H
+
+
+def positive_metric_root(H: T):
+    """``_positive_metric(N; square_root=true)`` (``tensors.jl:65-94``) of a site
+    hole: scaled by its Frobenius norm, symmetrised, eigendecomposed per parity
+    block, negative eigenvalues clipped.  Returns per block the eigenvectors
+    times the square roots of the clipped eigenvalues (rows in the bra-leg
+    order of the (bras | kets) view, which is also the ket-leg order), and the
+    diagnostic record."""
+    if not np.all(np.isfinite(H.a)):
+        raise RuntimeError("nonfinite norm metric")
+    scale = z2.norm(H)
+    v = z2.MatView(H, [1, 3, 5, 7], [0, 2, 4, 6])
+    roots, vals = [], []
+    defect_num = defect_den = 0.0
+    for b in v.blocks:
+        M = b / scale if scale != 0 else b.copy()
+        defect_num += float(np.sum((M - M.T) ** 2))
+        defect_den += float(np.sum(M * M))
+        M = 0.5 * (M + M.T)
+        if M.size == 0:
+            roots.append(np.zeros((M.shape[0], 0)))
+            continue
+        w, V = np.linalg.eigh(M)
+        vals.extend(w.tolist())
+        roots.append(V * np.sqrt(np.maximum(w, 0.0)))
+    vals = np.asarray(vals)
+    lo = min(float(vals.min()) if vals.size else 0.0, 0.0)
+    hi = max(float(np.abs(vals).max()) if vals.size else 0.0, FLOATMIN)
+    neg = vals[vals < 0]
+    report = dict(minimum_relative_eigenvalue=lo / hi, negative_eigenvalues=int(neg.size),
+                  negative_multiplets=int(neg.size),
+                  negative_spectral_fraction=float(np.sqrt(np.sum(neg * neg)) / max(np.sqrt(np.sum(vals * vals)),
+                                                                                    FLOATMIN)),
+                  hermiticity_defect=math.sqrt(defect_num) / max(math.sqrt(defect_den), FLOATMIN))
+    return roots, report
+
+
+def sample_physical(cache: SamplingCache, uniforms=None, configuration=None):
+    """``sample_configuration`` for ``kind=:physical`` (``born.jl:86-163``).
+
+    Each conditional weighs the site's two physically projected kets with the
+    PSD-projected site hole (``born.jl:117-126``); outcomes that cannot reach
+    the total charge get no weight (``born.jl:110-116``: with both parities
+    available at every site only the last site is bound); all-zero weights
+    fall back to the uniform choice among the allowed outcomes
+    (``born.jl:127-131``); the last row is not absorbed (``born.jl:155-158``).
+    ``repairs`` holds one diagnostic record per site plus the zero-weight ones.
+    """
+    st = cache.state
+    Lx, Ly = st.Lx, st.Ly
+    N = Lx * Ly
+    if uniforms is None and configuration is None:
+        raise ValueError("an explicit RNG is required")
+    selected = [[0] * Ly for _ in range(Lx)] if configuration is None else [list(c) for c in configuration]
+    north = bm.trivial_boundary(bm.col(cache.layers, 0), "north")
+    maxtr = max(e.max_truncation for e in cache.south)
+    logp = 0.0
+    conditionals, repairs = [], []
+
+    def result(lp):
+        return dict(configuration=selected, log_probability=lp, conditionals=conditionals,
+                    max_environment_truncation=maxtr, repairs=repairs)
+
+    if configuration is not None:
+        charge = 0
+        for x in range(Lx):
+            for y in range(Ly):
+                lab = selected[x][y]
+                if lab not in (1, 2):
+                    raise ValueError("configuration contains an unknown basis label")
+                charge ^= int(st[x, y].p[2][lab - 1])
+        if charge != cache.target:
+            return result(-math.inf)
+    prefix = 0
+    for y in range(Ly):
+        row = bm.col(cache.layers, y)
+        top = north.tensors
+        bottom = cache.south[y + 1].tensors
+        _, ri = bm.row_environments(top, row, bottom, side="right")
+        left = bm.row_edge(top, row, bottom, "left")
+        for x in range(Lx):
+            position = x + y * Lx
+            A = st[x, y]
+            allowed = [position < N - 1 or (prefix ^ int(A.p[2][k])) == cache.target for k in (0, 1)]
+            if not any(allowed):
+                raise RuntimeError("sampling prefix violates the total symmetry sector")
+            roots, diag = positive_metric_root(site_hole(left, top[x], bottom[x], ri[x + 1], A))
+            repairs.append(dict(diag, site=(x + 1, y + 1)))
+            values = []
+            for k in (0, 1):
+                if not allowed[k]:
+                    values.append(0.0)
+                    continue
+                vb = z2.MatView(project_physical(A, k), [0, 1, 4, 5], [2, 3]).blocks
+                values.append(sum(float(np.sum((r.T @ b) ** 2)) for r, b in zip(roots, vb) if r.size and b.size))
+            total = sum(values)
+            if total == 0:
+                n = sum(allowed)
+                probs = [1.0 / n if a else 0.0 for a in allowed]
+                repairs.append(dict(site=(x + 1, y + 1), reason="zero_proposal_weights", allowed_outcomes=n))
+            else:
+                probs = [v / total for v in values]
+            if configuration is None:
+                lm = [math.log(p) if p > 0 else -math.inf for p in probs]
+                k = categorical(lm, uniforms[position])
+            else:
+                k = selected[x][y] - 1
+            selected[x][y] = k + 1
+            p = probs[k]
+            conditionals.append(p)
+            if p == 0.0:
+                return result(-math.inf)
+            logp += math.log(p)
+            row[x] = cache.candidates[x][y][k]
+            prefix ^= int(A.p[2][k])
+            if x < Lx - 1:
+                left = bm.safe_scale(bm.left_step(left, top[x], row[x], bottom[x]))
+        if y < Ly - 1:
+            north = bm.absorb(north, row, cache.method, row_cut=y + 1)
+            maxtr = max(maxtr, north.max_truncation)
+    return result(logp)
 
 
 def project_configuration(checkpoint: State, configuration):

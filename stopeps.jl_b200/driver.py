@@ -5,9 +5,11 @@ Restates the control flow of ``src/driver/run.jl:2-66,76-134``,
 same temperature grid, step schedule, particle weights, ensemble statistics
 and result record (schema 2.7.0 field names).  Born draws take their
 uniforms from ``sample_uniforms(seed, index, n)``, the explicit replacement
-of the reference's ``sample_rng(seed, index)`` stream.  File output (JLD2,
-run.log) and annealed resampling are not part of this engine: a run whose
-ensemble would trigger resampling stops with an error.
+of the reference's ``sample_rng(seed, index)`` stream.  Annealed Born
+resampling (``src/resample/event.jl``) runs when the ensemble's efficiency
+falls below ``eta_th``, on one process (its scores are not distributed over
+ranks); its math is in ``resample.py``.  File output (JLD2, run.log) is not
+part of this engine.
 """
 from __future__ import annotations
 
@@ -132,11 +134,18 @@ class Particle:
 class DeviceOps:
     """The hot-path operations the drivers call, on the device engine."""
 
-    def sampling_cache(self, state, method):
-        return eng.SamplingCache(state, method)
+    def sampling_cache(self, state, method, kind="auxiliary"):
+        return eng.SamplingCache(state, method, kind)
 
     def sample(self, cache, uniforms):
         return eng.sample_configuration(cache, uniforms=uniforms)
+
+    def probability(self, cache, configuration):
+        return eng.sample_configuration(cache, configuration=configuration)
+
+    def probability_batch(self, cache, configurations):
+        lps, reps = eng.sample_probability_batch(cache, np.stack([np.asarray(x) for x in configurations]))
+        return [dict(r, log_probability=float(lp)) for lp, r in zip(lps, reps)]
 
     def project(self, state, configuration):
         return eng.project_configuration(state, configuration)
@@ -320,6 +329,56 @@ def _statistics(records, Ns, nsites):
     return s
 
 
+def _new_particles(checkpoint, c: RunConfig, items, energy: bool, ops=DEVICE_OPS):
+    """``_new_particle`` (``particles.jl:42-52``) for many configurations at once:
+    projection of the beta0 PEPO, one observation, estimator weight
+    log_norm - log_q.  ``items``: dicts with id, count, configuration, log_p0,
+    log_q, sampling_error and generation."""
+    if not items:
+        return []
+    cfgs = [np.asarray(it["configuration"]) for it in items]
+    if hasattr(ops, "project_batch"):
+        projected = ops.project_batch(checkpoint.state, np.stack(cfgs))
+    else:
+        projected = [ops.project(checkpoint.state, x) for x in cfgs]
+    states = [p[0] for p in projected]
+    obs = _observe_batch(states, c, energy, ops)
+    out = []
+    for it, state, m in zip(items, states, obs):
+        out.append(Particle(id=it["id"], count=it["count"], configuration=np.asarray(it["configuration"]),
+                            state=state, log_p0=it["log_p0"], log_q_proposal=it["log_q"],
+                            relative_log_weight=m["log_norm"] - it["log_q"], weight_log_scale=0.0,
+                            physical_log_norm=m["log_norm"], tensor_log_norm=m["tensor_log_norm"],
+                            energy_total=m["energy_total"], energy_per_site=m["energy_per_site"],
+                            magnetization=m["magnetization"],
+                            max_environment_truncation=max(it["sampling_error"], m["max_environment_truncation"]),
+                            measurement_seconds=m["measurement_seconds"], generation=it.get("generation", 0),
+                            sample_index=it["id"], seed=c.seed))
+    return out
+
+
+def _advance_particles(particles, c: RunConfig, steps, energy: bool, ops=DEVICE_OPS):
+    """``_advance_particle!`` (``particles.jl:86-102``) for every particle, batched per step."""
+    if not particles:
+        return
+    states = [p.state for p in particles]
+    reps = _evolve_batch(states, c, steps, c.D_peps, c.bond_space_peps, ops=ops)
+    obs = _observe_batch(states, c, energy, ops)
+    for p, rep, m in zip(particles, reps, obs):
+        old = p.tensor_log_norm
+        p.relative_log_weight += 2 * rep["normalization"] + (m["tensor_log_norm"] - old)
+        p.physical_log_norm = m["log_norm"]
+        p.tensor_log_norm = m["tensor_log_norm"]
+        p.energy_total = m["energy_total"]
+        p.energy_per_site = m["energy_per_site"]
+        p.magnetization = m["magnetization"]
+        p.max_state_truncation = rep["max_state_truncation"]
+        p.max_environment_truncation = max(rep["max_environment_truncation"], m["max_environment_truncation"])
+        p.max_boundary_entropy = rep["max_boundary_entropy"]
+        p.time_seconds = rep["time_seconds"]
+        p.measurement_seconds = m["measurement_seconds"]
+
+
 def run_stochastic(c: RunConfig, checkpoint: ThermalCheckpoint, uniforms_fn=None, execution=None, ops=None):
     """Draw Born samples from the beta0 checkpoint and evolve the weighted ensemble (``run.jl:76-134``).
 
@@ -346,8 +405,9 @@ def run_stochastic(c: RunConfig, checkpoint: ThermalCheckpoint, uniforms_fn=None
         uniforms_fn = lambda i: sample_uniforms(c.seed, i, L)
     rank, nprocs = e.rank(), e.nprocs()
 
+    cache = e.phase(lambda: ops.sampling_cache(checkpoint.state, c.boundary("sampling")))
+
     def local_draws():
-        cache = ops.sampling_cache(checkpoint.state, c.boundary("sampling"))
         idx = [i for i in range(1, c.Ns + 1) if (i - 1) % nprocs == rank]
         if not idx:
             return []
@@ -364,67 +424,36 @@ def run_stochastic(c: RunConfig, checkpoint: ThermalCheckpoint, uniforms_fn=None
 
     def local_particles():
         # _representative_owner (src/driver/execution.jl:34): unique configuration u on rank (u-1) % nprocs
-        mine = [(u, i) for u, i in enumerate(grouping["first_draw"], start=1) if (u - 1) % nprocs == rank]
-        if not mine:
-            return []
-        cfgs = [draws[i - 1]["configuration"] for _, i in mine]
-        if hasattr(ops, "project_batch"):
-            projected = ops.project_batch(checkpoint.state, np.stack([np.asarray(x) for x in cfgs]))
-        else:
-            projected = [ops.project(checkpoint.state, x) for x in cfgs]
-        states = [p[0] for p in projected]
-        obs = _observe_batch(states, c, measure_at(c, c.beta0), ops)
-        out = []
-        for (u, i), state, m in zip(mine, states, obs):
-            d = draws[i - 1]
-            out.append(Particle(id=i, count=grouping["multiplicity"][u - 1], configuration=d["configuration"],
-                                state=state, log_p0=d["log_probability"], log_q_proposal=d["log_probability"],
-                                relative_log_weight=m["log_norm"] - d["log_probability"],
-                                weight_log_scale=0.0, physical_log_norm=m["log_norm"],
-                                tensor_log_norm=m["tensor_log_norm"], energy_total=m["energy_total"],
-                                energy_per_site=m["energy_per_site"], magnetization=m["magnetization"],
-                                max_environment_truncation=max(d["max_environment_truncation"],
-                                                               m["max_environment_truncation"]),
-                                measurement_seconds=m["measurement_seconds"], sample_index=i, seed=c.seed))
-        return out
+        items = [dict(id=i, count=grouping["multiplicity"][u - 1], configuration=draws[i - 1]["configuration"],
+                      log_p0=draws[i - 1]["log_probability"], log_q=draws[i - 1]["log_probability"],
+                      sampling_error=draws[i - 1]["max_environment_truncation"])
+                 for u, i in enumerate(grouping["first_draw"], start=1) if (u - 1) % nprocs == rank]
+        return _new_particles(checkpoint, c, items, measure_at(c, c.beta0), ops)
 
     particles = e.phase(local_particles)
     curve = [r for r in checkpoint.purification if r["beta"] < c.beta0 and not same_beta(r["beta"], c.beta0)]
-    samples = []
+    samples, events, replay_rows = [], [], []
+    replay = []   # the evolution history: (beta, steps) per output node, replayed by fresh samples
+    event, next_sample_id = 0, c.Ns + 1
     nodes = [b for b in temperature_nodes(c) if b >= c.beta0]
     for node, beta in enumerate(nodes):
+        steps = [] if node == 0 else step_schedule(nodes[node - 1], beta, c.delta_tau_peps)
+        replay.append(dict(beta=beta, steps=list(steps)))
         if node > 0:
-            steps = step_schedule(nodes[node - 1], beta, c.delta_tau_peps)
-
-            def advance():
-                # _advance_particle! (particles.jl:86-102) for every local particle, batched per step
-                states = [p.state for p in particles]
-                reps = _evolve_batch(states, c, steps, c.D_peps, c.bond_space_peps, ops=ops)
-                obs = _observe_batch(states, c, measure_at(c, beta), ops)
-                for p, rep, m in zip(particles, reps, obs):
-                    old = p.tensor_log_norm
-                    p.relative_log_weight += 2 * rep["normalization"] + (m["tensor_log_norm"] - old)
-                    p.physical_log_norm = m["log_norm"]
-                    p.tensor_log_norm = m["tensor_log_norm"]
-                    p.energy_total = m["energy_total"]
-                    p.energy_per_site = m["energy_per_site"]
-                    p.magnetization = m["magnetization"]
-                    p.max_state_truncation = rep["max_state_truncation"]
-                    p.max_environment_truncation = max(rep["max_environment_truncation"],
-                                                       m["max_environment_truncation"])
-                    p.max_boundary_entropy = rep["max_boundary_entropy"]
-                    p.time_seconds = rep["time_seconds"]
-                    p.measurement_seconds = m["measurement_seconds"]
-
-            e.phase(advance)
+            e.phase(lambda: _advance_particles(particles, c, steps, measure_at(c, beta), ops))
         local_records = e.phase(lambda: [dict(_particle_record(p), owner=rank) for p in particles])
         records = sorted([r for part in e.gather(local_records) for r in part], key=lambda r: r["id"])
         stats = _statistics(records, c.Ns, L)
         stats.update(source="sampling",
                      time_seconds=max(e.gather(sum(p.time_seconds for p in particles))))
         if c.resampling.enabled and stats["eta"] < c.resampling.eta_th:
-            raise NotImplementedError("annealed Born resampling is not part of this engine; "
-                                      "run with resampling=ResamplingOptions(enabled=False)")
+            if nprocs > 1:
+                raise NotImplementedError("annealed Born resampling runs on one process")
+            event += 1
+            particles, records, stats, next_sample_id, audit = _resample(
+                particles, records, checkpoint, c, cache, replay, event, next_sample_id, ops)
+            events.append(audit)
+            replay_rows.extend(audit.pop("replay_rows"))
         curve.append(stats)
         samples.extend(records)
     if rank != 0:
@@ -432,9 +461,224 @@ def run_stochastic(c: RunConfig, checkpoint: ThermalCheckpoint, uniforms_fn=None
     return {"schema_version": RESULT_SCHEMA_VERSION, "method": "stoPEPS",
             "parameters": parameter_dict(c), "model": parameter_dict(c)["model"],
             "observables": {"curve": curve, "purification": list(checkpoint.purification),
-                            "samples": samples, "replay": []},
-            "diagnostics": {"born_draws": draws, "born_grouping": grouping, "events": [],
+                            "samples": samples, "replay": replay_rows},
+            "diagnostics": {"born_draws": draws, "born_grouping": grouping, "events": events,
                             "history": list(checkpoint.history)},
             "metadata": {"run_id": checkpoint.run_id, "stage": "stochastic", "complete": True,
                          "mpi_size": nprocs, "restart_supported": False,
                          "uncertainty": "conditional_particle_delta_method; shared_history_scale_fixed"}}
+
+
+# ---------------------------------------------------------------------------
+# annealed Born resampling (src/resample/event.jl, scores.jl)
+# ---------------------------------------------------------------------------
+def _score(memo, caches, member_ids, configurations, ops):
+    """``_score_configurations!`` (``scores.jl:38-71``): the probabilities of
+    ``configurations`` under each member's cache that the table does not hold
+    yet, one batched call per member.  Returns the member ids and the
+    configurations' columns."""
+    columns = memo.columns_of(configurations)
+    unique = list(dict.fromkeys(columns))
+    for mid in member_ids:
+        todo = [j for j in unique if (mid, j) not in memo.index]
+        if not todo:
+            continue
+        cfgs = [memo.configurations[j - 1] for j in todo]
+        if hasattr(ops, "probability_batch"):
+            res = ops.probability_batch(caches[mid], cfgs)
+        else:
+            res = [ops.probability(caches[mid], x) for x in cfgs]
+        for j, r in zip(todo, res):
+            memo.record(mid, j, float(r["log_probability"]), r.get("max_environment_truncation", 0.0),
+                        {k: r[k] for k in ("metric_repairs", "zero_proposals", "min_relative_eigenvalue") if k in r})
+    for mid in member_ids:
+        for j in unique:
+            if (mid, j) not in memo.index:
+                raise RuntimeError("missing proposal scores")
+    return dict(member_ids=list(member_ids), configuration_indices=columns)
+
+
+def _evaluate_resampling(memo, caches, particles, records, c: RunConfig, ops, after_sweep):
+    """``_evaluate_resampling!`` (``event.jl:27-43``): a physical-kind proposal
+    cache per particle, the leave-one-out score matrix and the plan."""
+    from . import resample as rs
+    t = time.perf_counter()
+    for p in particles:
+        if p.id not in caches:
+            caches[p.id] = ops.sampling_cache(p.state, c.boundary("proposal"), "physical")
+    ref = _score(memo, caches, [r["id"] for r in records], [r["configuration"] for r in records], ops)
+    stats = _statistics(records, c.Ns, c.lattice.Lx * c.lattice.Ly)
+    plan = rs.resampling_plan(records, memo.matrix(ref["member_ids"], ref["configuration_indices"]), c.resampling,
+                              stats)
+    return dict(after_sweep=after_sweep, plan=plan, score_reference=ref, loo_seconds=time.perf_counter() - t)
+
+
+def _draw_resampling_batch(memo, caches, records, plan, M, c: RunConfig, event, sweep, ops):
+    """``_draw_resampling_batch!`` (``event.jl:114-174``): M fresh draws from the
+    mixture proposal (member 0, the beta0 Born distribution, with probability
+    1 - lambda, else a pool member by its parent mass), their grouping, the
+    baseline and mixture scores of the distinct configurations and their
+    proposal log-probabilities log q."""
+    from . import resample as rs
+    lam = plan["selection"]["lam"]
+    L = c.lattice.Lx * c.lattice.Ly
+    slots = [(sweep - 1) * c.Ns + d for d in range(1, M + 1)]
+    members = []
+    for slot in slots:
+        u = rs.event_uniforms(c.seed, rs.DOMAIN_MIXTURE, event, slot, 2)
+        members.append(rs.categorical(list(plan["parent_log_mass"]), u[1]) + 1 if u[0] < lam else 0)
+    draws = []
+    for d, (slot, member) in enumerate(zip(slots, members), start=1):
+        mid = 0 if member == 0 else records[member - 1]["id"]
+        r = ops.sample(caches[mid], rs.event_uniforms(c.seed, rs.DOMAIN_FRESH, event, slot, L))
+        draws.append(dict(index=d, slot=slot, member=member, member_id=mid,
+                          configuration=np.asarray(r["configuration"]),
+                          selected_log_probability=float(r["log_probability"]),
+                          max_environment_truncation=r.get("max_environment_truncation", 0.0),
+                          repairs={k: r[k] for k in ("metric_repairs", "zero_proposals", "min_relative_eigenvalue")
+                                   if k in r}))
+    # _seed_draw_scores! (scores.jl:73-87): a draw has evaluated its own component
+    for d, col in zip(draws, memo.columns_of([d["configuration"] for d in draws])):
+        memo.record(d["member_id"], col, d["selected_log_probability"], d["max_environment_truncation"],
+                    d["repairs"], source="draw")
+    grouping = group_configurations([d["configuration"] for d in draws])
+    configurations = [draws[i - 1]["configuration"] for i in grouping["first_draw"]]
+    baseline = _score(memo, caches, [0], configurations, ops)
+    scored_ref = None if lam == 0 else _score(memo, caches, [r["id"] for r in records], configurations, ops)
+    norm = rs.logsumexp(plan["parent_log_mass"])
+    proposals = []
+    for col in baseline["configuration_indices"]:
+        p0 = memo.get(0, col)
+        scored = [] if scored_ref is None else [memo.get(i, col) for i in scored_ref["member_ids"]]
+        pr = None if scored_ref is None else rs.logsumexp(
+            [m + s["log_probability"] for m, s in zip(plan["parent_log_mass"], scored)]) - norm
+        q = rs.mixture_log_probability(p0["log_probability"], pr, lam)
+        err = max([p0["max_environment_truncation"]] + [s["max_environment_truncation"] for s in scored])
+        proposals.append(dict(log_p0=p0["log_probability"], log_pr=pr, log_q=q, max_environment_truncation=err))
+    for i, d in enumerate(draws):
+        g = proposals[grouping["draw_to_group"][i] - 1]
+        d["log_probability"] = g["log_q"]
+        d["max_environment_truncation"] = max(d["max_environment_truncation"], g["max_environment_truncation"])
+    return dict(members=members, draws=draws, grouping=grouping, configurations=configurations, proposals=proposals,
+                baseline_reference=baseline, score_reference=scored_ref)
+
+
+def _replay_fresh(fresh, replay, c: RunConfig, event, sweep, ops):
+    """``_replay_fresh!`` (``event.jl:79-112``): fresh samples re-evolved through
+    the saved step endpoints, observed at every output node (energy where the
+    node is measured); one statistics row per node."""
+    rows = []
+    for node, segment in enumerate(replay):
+        if node > 0:
+            _advance_particles(fresh, c, segment["steps"],
+                               node == len(replay) - 1 and measure_at(c, segment["beta"]), ops)
+        records = [_particle_record(p) for p in fresh]
+        if records:
+            stats = _statistics(records, sum(r["count"] for r in records), c.lattice.Lx * c.lattice.Ly)
+            stats.update(event=event, sweep=sweep, time_seconds=sum(p.time_seconds for p in fresh),
+                         source="fresh_replay")
+            rows.append(dict(event=event, sweep=sweep, statistics=stats, samples=records))
+    return [_particle_record(p) for p in fresh], rows
+
+
+def _resample(particles, records, checkpoint, c: RunConfig, baseline_cache, replay, event, next_sample_id, ops):
+    """``_resample!`` (``event.jl:176-253``): one annealed Born resampling event.
+
+    Leave-one-out plan, then up to ``max_resample_sweep`` sweeps of fresh draws
+    from the mixture proposal, each sweep's distinct configurations projected
+    from the beta0 PEPO and replayed to the current beta and added to the
+    pool, with a new plan after every sweep that does not stop; finally SIR
+    selection of Ns distinct representatives from the pool with equal
+    weights.  Returns the new particles, their records and statistics, the
+    next free sample id and the event's audit record."""
+    from . import resample as rs
+    started = time.perf_counter()
+    beta = replay[-1]["beta"]
+    interval_seconds = sum(p.time_seconds for p in particles)
+    memo = rs.ScoreTable()
+    caches = {0: baseline_cache}
+    evaluations, sweeps, replay_rows = [], [], []
+    evaluation = _evaluate_resampling(memo, caches, particles, records, c, ops, 0)
+    evaluations.append(evaluation)
+    plan = evaluation["plan"]
+    M = rs.resample_fresh_count(plan, c.resampling)
+    pool_particles = list(particles)
+    pool_records = list(records)
+    all_fresh = []
+    stop_reason = "continue"
+    proposal_seconds = replay_seconds = 0.0
+    for sweep in range(1, c.resampling.max_resample_sweep + 1):
+        t = time.perf_counter()
+        batch = _draw_resampling_batch(memo, caches, pool_records, plan, M, c, event, sweep, ops)
+        proposal_time = time.perf_counter() - t
+        proposal_seconds += proposal_time
+        lam = plan["selection"]["lam"]
+        stop_reason = "no_fresh_draws" if M == 0 else rs.resample_stop(lam, sweep, c.resampling)
+        if stop_reason != "continue":
+            caches.clear()   # proposal environments are released before the last replay
+        first_id = next_sample_id
+        next_sample_id += c.Ns
+        t = time.perf_counter()
+        items = [dict(id=first_id + d - 1, count=batch["grouping"]["multiplicity"][u], generation=event,
+                      configuration=batch["configurations"][u], log_p0=batch["proposals"][u]["log_p0"],
+                      log_q=batch["proposals"][u]["log_q"],
+                      sampling_error=batch["proposals"][u]["max_environment_truncation"])
+                 for u, d in enumerate(batch["grouping"]["first_draw"])]
+        fresh = _new_particles(checkpoint, c, items, len(replay) == 1 and measure_at(c, beta), ops)
+        fresh_records, rows = ([], []) if M == 0 else _replay_fresh(fresh, replay, c, event, sweep, ops)
+        replay_rows.extend(rows)
+        replay_time = time.perf_counter() - t
+        replay_seconds += replay_time
+        pool_particles.extend(fresh)
+        all_fresh.extend(fresh_records)
+        pool_records = list(records) + all_fresh
+        sweeps.append(dict(sweep=sweep, evaluation=len(evaluations), lam=lam, M=M, members=batch["members"],
+                           draws=batch["draws"], grouping=batch["grouping"], proposals=batch["proposals"],
+                           fresh_ids=[r["id"] for r in fresh_records], pool_representatives=len(pool_records),
+                           pool_virtual_samples=sum(r["count"] for r in pool_records),
+                           timing=dict(proposal_seconds=proposal_time, replay_seconds=replay_time)))
+        if stop_reason != "continue":
+            break
+        evaluation = _evaluate_resampling(memo, caches, pool_particles, pool_records, c, ops, sweep)
+        evaluations.append(evaluation)
+        plan = evaluation["plan"]
+        if plan["selection"]["lam"] >= c.resampling.lambda_threshold:
+            stop_reason = "lambda_threshold"
+            break
+    caches.clear()
+    # _pool_selection (event.jl:69-77) and _redistribute (execution.jl:28-31)
+    pool = list(records) + all_fresh
+    relative, scale = rs.aligned_weights(pool)
+    pivot = max(relative)
+    selection = rs.sir_select_until_unique([v - pivot for v in relative], [r["count"] for r in pool], c.Ns,
+                                           c.seed, event)
+    selection.update(common_log_weight=scale + pivot + selection["common_log_weight"],
+                     pool_statistics=_statistics(pool, c.Ns, c.lattice.Lx * c.lattice.Ly))
+    by_id = {p.id: p for p in pool_particles}
+    nxt = []
+    for i in selection["active"]:
+        p = by_id[pool[i]["id"]]
+        p.count = selection["multiplicity"][i]
+        p.relative_log_weight = selection["output_relative_log_weight"][i]
+        p.weight_log_scale = selection["common_log_weight"]
+        nxt.append(p)
+    post = sorted([_particle_record(p) for p in nxt], key=lambda r: r["id"])
+    stats = _statistics(post, c.Ns, c.lattice.Lx * c.lattice.Ly)
+    stats.update(source="sampling", time_seconds=interval_seconds)
+    audit = dict(event=event, beta=beta, M=M,
+                 lambda_evaluations=[dict(after_sweep=v["after_sweep"], lam=v["plan"]["selection"]["lam"],
+                                          selection=v["plan"]["selection"], M=v["plan"]["M"],
+                                          loo_log_probability=v["plan"]["loo_log_probability"].tolist(),
+                                          parent_log_mass=v["plan"]["parent_log_mass"].tolist(),
+                                          loo_seconds=v["loo_seconds"]) for v in evaluations],
+                 sweeps=sweeps, stop_reason=stop_reason,
+                 score_table=dict(configurations=memo.configurations,
+                                  entries=sorted(memo.entries, key=lambda r: (r["member_id"],
+                                                                              r["configuration_index"]))),
+                 pre=list(records), fresh=all_fresh, selection=selection, post=post, post_statistics=stats,
+                 accepted=True, proposal="finite_chi_psd_sequential_basis",
+                 timing=dict(loo_seconds=sum(v["loo_seconds"] for v in evaluations),
+                             proposal_seconds=proposal_seconds, replay_seconds=replay_seconds,
+                             total_seconds=time.perf_counter() - started),
+                 replay_rows=replay_rows)
+    return nxt, post, stats, next_sample_id, audit

@@ -133,3 +133,37 @@ def test_zipup_equals_exact_compression_without_truncation(name):
         dz = sp.sample_configuration(cz, uniforms=u)
         assert np.array_equal(np.asarray(dp["configuration"]), np.asarray(dz["configuration"]))
         assert abs(dp["log_probability"] - dz["log_probability"]) < 1e-11 * max(1.0, abs(dp["log_probability"]))
+
+
+def test_physical_proposal_is_the_born_distribution_of_the_peps():
+    """The physical-kind proposal (``born.jl:117-134``) on a projected 2x3 D=2
+    PEPS contracted exactly (chi=64): every configuration's probability is
+    |psi(s)|^2 / <psi|psi> (the PEPS with its physical legs fixed, contracted
+    on its own), the parity-forbidden half has probability zero, and the
+    probabilities sum to one."""
+    from oracle.model import State
+    from util import oracle_state
+    g = golden("pepo_2x3_D2.npz")
+    ps, _ = sp.project_configuration(oracle_state(g), np.asarray(g["configs"][0]).tolist())
+    m = bm.BoundaryMPS(64, None)
+    cache = sp.SamplingCache(ps, m, kind="physical")
+    ln0 = bm.lognorm(ps, m)["tensor_log_norm"]
+    Lx, Ly = ps.Lx, ps.Ly
+    total, nonzero = 0.0, 0
+    for labs in itertools.product((1, 2), repeat=Lx * Ly):
+        conf = [[labs[x + y * Lx] for y in range(Ly)] for x in range(Lx)]
+        lp = sp.sample_configuration(cache, configuration=conf)["log_probability"]
+        if lp == -math.inf:
+            continue
+        nonzero += 1
+        total += math.exp(lp)
+        sites = [[sp.project_physical(ps[x, y], conf[x][y] - 1) for y in range(Ly)] for x in range(Lx)]
+        exact = bm.lognorm(State(Lx, Ly, sites, ps.beta, 0.0, "peps"), m)["tensor_log_norm"] - ln0
+        assert abs(math.exp(lp) - math.exp(exact)) <= 1e-12 * math.exp(exact)
+    assert nonzero == 2 ** (Lx * Ly - 1)
+    assert abs(total - 1.0) < 1e-12
+    # a draw from uniforms has the probability of its configuration
+    d = sp.sample_configuration(cache, uniforms=np.random.default_rng(3).random(Lx * Ly))
+    again = sp.sample_configuration(cache, configuration=d["configuration"])
+    assert abs(d["log_probability"] - again["log_probability"]) < 1e-13
+    assert len([r for r in d["repairs"] if "minimum_relative_eigenvalue" in r]) == Lx * Ly

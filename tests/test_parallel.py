@@ -35,15 +35,29 @@ class OracleOps:
         rec = self.md.normalize_state(st)
         return st, [v for _, v in rec]
 
-    def sampling_cache(self, state, method):
+    def sampling_cache(self, state, method, kind="auxiliary"):
         from oracle import sampling as sp
-        return sp.SamplingCache(state, self._m(method))
+        return sp.SamplingCache(state, self._m(method), kind=kind)
+
+    @staticmethod
+    def _repairs(d):
+        reps = d.get("repairs", [])
+        neg = [r for r in reps if "minimum_relative_eigenvalue" in r]
+        return dict(metric_repairs=sum(1 for r in neg if r["negative_eigenvalues"] > 0),
+                    zero_proposals=sum(1 for r in reps if r.get("reason") == "zero_proposal_weights"),
+                    min_relative_eigenvalue=min([0.0] + [r["minimum_relative_eigenvalue"] for r in neg]))
 
     def sample(self, cache, uniforms):
         from oracle import sampling as sp
         d = sp.sample_configuration(cache, uniforms=uniforms)
         return dict(configuration=np.asarray(d["configuration"]), log_probability=d["log_probability"],
-                    max_environment_truncation=d["max_environment_truncation"])
+                    max_environment_truncation=d["max_environment_truncation"], **self._repairs(d))
+
+    def probability(self, cache, configuration):
+        from oracle import sampling as sp
+        d = sp.sample_configuration(cache, configuration=np.asarray(configuration).tolist())
+        return dict(log_probability=d["log_probability"],
+                    max_environment_truncation=d["max_environment_truncation"], **self._repairs(d))
 
     def project(self, state, configuration):
         from oracle import sampling as sp
