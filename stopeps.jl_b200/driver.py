@@ -7,9 +7,9 @@ and result record (schema 2.7.0 field names).  Born draws take their
 uniforms from ``sample_uniforms(seed, index, n)``, the explicit replacement
 of the reference's ``sample_rng(seed, index)`` stream.  Annealed Born
 resampling (``src/resample/event.jl``) runs when the ensemble's efficiency
-falls below ``eta_th``, on one process (its scores are not distributed over
-ranks); its math is in ``resample.py``.  File output (JLD2, run.log) is not
-part of this engine.
+falls below ``eta_th``, over the same ranks (scores, draws and fresh samples
+on their owners, selected particles moved to their new owners); its math is
+in ``resample.py``.  File output (JLD2, run.log) is not part of this engine.
 """
 from __future__ import annotations
 
@@ -146,6 +146,16 @@ class DeviceOps:
     def probability_batch(self, cache, configurations):
         lps, reps = eng.sample_probability_batch(cache, np.stack([np.asarray(x) for x in configurations]))
         return [dict(r, log_probability=float(lp)) for lp, r in zip(lps, reps)]
+
+    # a particle's state between ranks (a resampling event moves selected particles)
+    def export_state(self, state):
+        sites, dims = state.download()
+        return dict(sites=sites, dims=np.asarray(dims), is_pepo=state.is_pepo, beta=state.beta,
+                    log_amplitude=state.log_amplitude)
+
+    def import_state(self, blob, like):
+        return like.engine.upload_state(blob["sites"], blob["dims"], blob["is_pepo"], beta=blob["beta"],
+                                        log_amplitude=blob["log_amplitude"])
 
     def project(self, state, configuration):
         return eng.project_configuration(state, configuration)
@@ -447,11 +457,9 @@ def run_stochastic(c: RunConfig, checkpoint: ThermalCheckpoint, uniforms_fn=None
         stats.update(source="sampling",
                      time_seconds=max(e.gather(sum(p.time_seconds for p in particles))))
         if c.resampling.enabled and stats["eta"] < c.resampling.eta_th:
-            if nprocs > 1:
-                raise NotImplementedError("annealed Born resampling runs on one process")
             event += 1
             particles, records, stats, next_sample_id, audit = _resample(
-                particles, records, checkpoint, c, cache, replay, event, next_sample_id, ops)
+                particles, records, checkpoint, c, cache, replay, event, next_sample_id, ops, e)
             events.append(audit)
             replay_rows.extend(audit.pop("replay_rows"))
         curve.append(stats)
@@ -472,89 +480,135 @@ def run_stochastic(c: RunConfig, checkpoint: ThermalCheckpoint, uniforms_fn=None
 # ---------------------------------------------------------------------------
 # annealed Born resampling (src/resample/event.jl, scores.jl)
 # ---------------------------------------------------------------------------
-def _score(memo, caches, member_ids, configurations, ops):
+_REPAIR_KEYS = ("metric_repairs", "zero_proposals", "min_relative_eigenvalue")
+
+
+def _score(memo, caches, member_ids, configurations, ops, e):
     """``_score_configurations!`` (``scores.jl:38-71``): the probabilities of
     ``configurations`` under each member's cache that the table does not hold
-    yet, one batched call per member.  Returns the member ids and the
-    configurations' columns."""
+    yet.  The beta0 column j is scored on rank (j-1) % nprocs, a member's on
+    the rank holding its cache; one batched call per member, then every rank
+    records every entry (ordered by member and column).  Returns the member
+    ids and the configurations' columns."""
     columns = memo.columns_of(configurations)
     unique = list(dict.fromkeys(columns))
-    for mid in member_ids:
-        todo = [j for j in unique if (mid, j) not in memo.index]
-        if not todo:
-            continue
-        cfgs = [memo.configurations[j - 1] for j in todo]
-        if hasattr(ops, "probability_batch"):
-            res = ops.probability_batch(caches[mid], cfgs)
-        else:
-            res = [ops.probability(caches[mid], x) for x in cfgs]
-        for j, r in zip(todo, res):
-            memo.record(mid, j, float(r["log_probability"]), r.get("max_environment_truncation", 0.0),
-                        {k: r[k] for k in ("metric_repairs", "zero_proposals", "min_relative_eigenvalue") if k in r})
-    for mid in member_ids:
-        for j in unique:
-            if (mid, j) not in memo.index:
-                raise RuntimeError("missing proposal scores")
+    rank, nprocs = e.rank(), e.nprocs()
+
+    def local():
+        out = []
+        for mid in member_ids:
+            if mid == 0:
+                todo = [j for j in unique if (j - 1) % nprocs == rank]
+            elif mid in caches:
+                todo = list(unique)
+            else:
+                continue
+            todo = [j for j in todo if (mid, j) not in memo.index]
+            if not todo:
+                continue
+            cfgs = [memo.configurations[j - 1] for j in todo]
+            if hasattr(ops, "probability_batch"):
+                res = ops.probability_batch(caches[mid], cfgs)
+            else:
+                res = [ops.probability(caches[mid], x) for x in cfgs]
+            for j, r in zip(todo, res):
+                out.append(dict(member_id=mid, column=j, log_probability=float(r["log_probability"]),
+                                max_environment_truncation=r.get("max_environment_truncation", 0.0),
+                                repairs={k: r[k] for k in _REPAIR_KEYS if k in r}))
+        return out
+
+    parts = e.gather(e.phase(local))
+    for r in sorted([r for p in parts for r in p], key=lambda r: (r["member_id"], r["column"])):
+        memo.record(r["member_id"], r["column"], r["log_probability"], r["max_environment_truncation"],
+                    r["repairs"])
+
+    def check():
+        for mid in member_ids:
+            for j in unique:
+                if (mid, j) not in memo.index:
+                    raise RuntimeError("missing proposal scores")
+    e.phase(check)
     return dict(member_ids=list(member_ids), configuration_indices=columns)
 
 
-def _evaluate_resampling(memo, caches, particles, records, c: RunConfig, ops, after_sweep):
+def _evaluate_resampling(memo, caches, particles, records, c: RunConfig, ops, e, after_sweep):
     """``_evaluate_resampling!`` (``event.jl:27-43``): a physical-kind proposal
-    cache per particle, the leave-one-out score matrix and the plan."""
+    cache per local particle, the leave-one-out score matrix, and the plan
+    (made on rank 0, broadcast)."""
     from . import resample as rs
     t = time.perf_counter()
-    for p in particles:
-        if p.id not in caches:
-            caches[p.id] = ops.sampling_cache(p.state, c.boundary("proposal"), "physical")
-    ref = _score(memo, caches, [r["id"] for r in records], [r["configuration"] for r in records], ops)
-    stats = _statistics(records, c.Ns, c.lattice.Lx * c.lattice.Ly)
-    plan = rs.resampling_plan(records, memo.matrix(ref["member_ids"], ref["configuration_indices"]), c.resampling,
-                              stats)
-    return dict(after_sweep=after_sweep, plan=plan, score_reference=ref, loo_seconds=time.perf_counter() - t)
+
+    def build():
+        for p in particles:
+            if p.id not in caches:
+                caches[p.id] = ops.sampling_cache(p.state, c.boundary("proposal"), "physical")
+    e.phase(build)
+    ref = _score(memo, caches, [r["id"] for r in records], [r["configuration"] for r in records], ops, e)
+    plan = e.broadcast(lambda: rs.resampling_plan(
+        records, memo.matrix(ref["member_ids"], ref["configuration_indices"]), c.resampling,
+        _statistics(records, c.Ns, c.lattice.Lx * c.lattice.Ly)))
+    seconds = max(e.gather(time.perf_counter() - t))
+    return dict(after_sweep=after_sweep, plan=plan, score_reference=ref, loo_seconds=seconds)
 
 
-def _draw_resampling_batch(memo, caches, records, plan, M, c: RunConfig, event, sweep, ops):
+def _draw_resampling_batch(memo, caches, records, plan, M, c: RunConfig, event, sweep, ops, e):
     """``_draw_resampling_batch!`` (``event.jl:114-174``): M fresh draws from the
     mixture proposal (member 0, the beta0 Born distribution, with probability
-    1 - lambda, else a pool member by its parent mass), their grouping, the
-    baseline and mixture scores of the distinct configurations and their
-    proposal log-probabilities log q."""
+    1 - lambda, else a pool member by its parent mass), each on the rank that
+    owns its component (member 0: draw d on rank (d-1) % nprocs); their
+    grouping, the baseline and mixture scores of the distinct configurations
+    and their proposal log-probabilities log q (made on rank 0, broadcast)."""
     from . import resample as rs
     lam = plan["selection"]["lam"]
     L = c.lattice.Lx * c.lattice.Ly
+    rank, nprocs = e.rank(), e.nprocs()
     slots = [(sweep - 1) * c.Ns + d for d in range(1, M + 1)]
-    members = []
-    for slot in slots:
-        u = rs.event_uniforms(c.seed, rs.DOMAIN_MIXTURE, event, slot, 2)
-        members.append(rs.categorical(list(plan["parent_log_mass"]), u[1]) + 1 if u[0] < lam else 0)
-    draws = []
-    for d, (slot, member) in enumerate(zip(slots, members), start=1):
-        mid = 0 if member == 0 else records[member - 1]["id"]
-        r = ops.sample(caches[mid], rs.event_uniforms(c.seed, rs.DOMAIN_FRESH, event, slot, L))
-        draws.append(dict(index=d, slot=slot, member=member, member_id=mid,
-                          configuration=np.asarray(r["configuration"]),
-                          selected_log_probability=float(r["log_probability"]),
-                          max_environment_truncation=r.get("max_environment_truncation", 0.0),
-                          repairs={k: r[k] for k in ("metric_repairs", "zero_proposals", "min_relative_eigenvalue")
-                                   if k in r}))
+
+    def choose():
+        out = []
+        for slot in slots:
+            u = rs.event_uniforms(c.seed, rs.DOMAIN_MIXTURE, event, slot, 2)
+            out.append(rs.categorical(list(plan["parent_log_mass"]), u[1]) + 1 if u[0] < lam else 0)
+        return out
+    members = e.broadcast(choose)
+
+    def local_draws():
+        out = []
+        for d, (slot, member) in enumerate(zip(slots, members), start=1):
+            owner = (d - 1) % nprocs if member == 0 else records[member - 1]["owner"]
+            if owner != rank:
+                continue
+            mid = 0 if member == 0 else records[member - 1]["id"]
+            r = ops.sample(caches[mid], rs.event_uniforms(c.seed, rs.DOMAIN_FRESH, event, slot, L))
+            out.append(dict(index=d, slot=slot, member=member, member_id=mid,
+                            configuration=np.asarray(r["configuration"]),
+                            selected_log_probability=float(r["log_probability"]),
+                            max_environment_truncation=r.get("max_environment_truncation", 0.0),
+                            repairs={k: r[k] for k in _REPAIR_KEYS if k in r}))
+        return out
+    draws = sorted([d for p in e.gather(e.phase(local_draws)) for d in p], key=lambda d: d["index"])
     # _seed_draw_scores! (scores.jl:73-87): a draw has evaluated its own component
     for d, col in zip(draws, memo.columns_of([d["configuration"] for d in draws])):
         memo.record(d["member_id"], col, d["selected_log_probability"], d["max_environment_truncation"],
                     d["repairs"], source="draw")
     grouping = group_configurations([d["configuration"] for d in draws])
     configurations = [draws[i - 1]["configuration"] for i in grouping["first_draw"]]
-    baseline = _score(memo, caches, [0], configurations, ops)
-    scored_ref = None if lam == 0 else _score(memo, caches, [r["id"] for r in records], configurations, ops)
-    norm = rs.logsumexp(plan["parent_log_mass"])
-    proposals = []
-    for col in baseline["configuration_indices"]:
-        p0 = memo.get(0, col)
-        scored = [] if scored_ref is None else [memo.get(i, col) for i in scored_ref["member_ids"]]
-        pr = None if scored_ref is None else rs.logsumexp(
-            [m + s["log_probability"] for m, s in zip(plan["parent_log_mass"], scored)]) - norm
-        q = rs.mixture_log_probability(p0["log_probability"], pr, lam)
-        err = max([p0["max_environment_truncation"]] + [s["max_environment_truncation"] for s in scored])
-        proposals.append(dict(log_p0=p0["log_probability"], log_pr=pr, log_q=q, max_environment_truncation=err))
+    baseline = _score(memo, caches, [0], configurations, ops, e)
+    scored_ref = None if lam == 0 else _score(memo, caches, [r["id"] for r in records], configurations, ops, e)
+
+    def make_proposals():
+        norm = rs.logsumexp(plan["parent_log_mass"])
+        out = []
+        for col in baseline["configuration_indices"]:
+            p0 = memo.get(0, col)
+            scored = [] if scored_ref is None else [memo.get(i, col) for i in scored_ref["member_ids"]]
+            pr = None if scored_ref is None else rs.logsumexp(
+                [m + s["log_probability"] for m, s in zip(plan["parent_log_mass"], scored)]) - norm
+            q = rs.mixture_log_probability(p0["log_probability"], pr, lam)
+            err = max([p0["max_environment_truncation"]] + [s["max_environment_truncation"] for s in scored])
+            out.append(dict(log_p0=p0["log_probability"], log_pr=pr, log_q=q, max_environment_truncation=err))
+        return out
+    proposals = e.broadcast(make_proposals)
     for i, d in enumerate(draws):
         g = proposals[grouping["draw_to_group"][i] - 1]
         d["log_probability"] = g["log_q"]
@@ -563,42 +617,91 @@ def _draw_resampling_batch(memo, caches, records, plan, M, c: RunConfig, event, 
                 baseline_reference=baseline, score_reference=scored_ref)
 
 
-def _replay_fresh(fresh, replay, c: RunConfig, event, sweep, ops):
-    """``_replay_fresh!`` (``event.jl:79-112``): fresh samples re-evolved through
-    the saved step endpoints, observed at every output node (energy where the
-    node is measured); one statistics row per node."""
+def _global_records(particles, e):
+    """``_global_particles`` (``particles.jl:116-119``): every rank's particle
+    records, owner set, ordered by id."""
+    rank = e.rank()
+    local = e.phase(lambda: [dict(_particle_record(p), owner=rank) for p in particles])
+    return sorted([r for part in e.gather(local) for r in part], key=lambda r: r["id"])
+
+
+def _replay_fresh(fresh, replay, c: RunConfig, event, sweep, ops, e):
+    """``_replay_fresh!`` (``event.jl:79-112``): the local fresh samples re-evolved
+    through the saved step endpoints, observed at every output node (energy
+    where the node is measured); one statistics row of all ranks' fresh
+    samples per node."""
     rows = []
+    records = []
     for node, segment in enumerate(replay):
         if node > 0:
-            _advance_particles(fresh, c, segment["steps"],
-                               node == len(replay) - 1 and measure_at(c, segment["beta"]), ops)
-        records = [_particle_record(p) for p in fresh]
+            e.phase(lambda: _advance_particles(fresh, c, segment["steps"],
+                                               node == len(replay) - 1 and measure_at(c, segment["beta"]), ops))
+        records = _global_records(fresh, e)
+        seconds = max(e.gather(sum(p.time_seconds for p in fresh)))
         if records:
             stats = _statistics(records, sum(r["count"] for r in records), c.lattice.Lx * c.lattice.Ly)
-            stats.update(event=event, sweep=sweep, time_seconds=sum(p.time_seconds for p in fresh),
-                         source="fresh_replay")
+            stats.update(event=event, sweep=sweep, time_seconds=seconds, source="fresh_replay")
             rows.append(dict(event=event, sweep=sweep, statistics=stats, samples=records))
-    return [_particle_record(p) for p in fresh], rows
+    return records, rows
 
 
-def _resample(particles, records, checkpoint, c: RunConfig, baseline_cache, replay, event, next_sample_id, ops):
+def _redistribute(pool_particles, pool, selection, ops, e, like):
+    """``_redistribute`` (``execution.jl:28-31``, ``ext/StoPEPSMPIExt.jl:32-51``):
+    the selected pool members, the k-th of them (in selection order) to rank
+    k % nprocs, with the selection's counts and weights.  A member held by
+    another rank moves with its state exported through the ops."""
+    rank, nprocs = e.rank(), e.nprocs()
+    held = {p.id: p for p in pool_particles}
+    nxt, outgoing = [], []
+    for position, i in enumerate(selection["active"]):
+        source, dest = pool[i]["owner"], position % nprocs
+        if rank == source and source == dest:
+            nxt.append((i, held[pool[i]["id"]]))
+        elif rank == source:
+            p = held[pool[i]["id"]]
+            blob = dict(p.__dict__)
+            blob["state"] = ops.export_state(p.state)
+            outgoing.append((dest, i, blob))
+    for part in e.gather(outgoing):
+        for dest, i, blob in part:
+            if dest == rank:
+                blob = dict(blob)
+                blob["state"] = ops.import_state(blob["state"], like)
+                nxt.append((i, Particle(**blob)))
+    out = []
+    for i, p in sorted(nxt, key=lambda t: selection["active"].index(t[0])):
+        p.count = selection["multiplicity"][i]
+        p.relative_log_weight = selection["output_relative_log_weight"][i]
+        p.weight_log_scale = selection["common_log_weight"]
+        out.append(p)
+    return out
+
+
+def _resample(particles, records, checkpoint, c: RunConfig, baseline_cache, replay, event, next_sample_id, ops,
+              e=None):
     """``_resample!`` (``event.jl:176-253``): one annealed Born resampling event.
 
     Leave-one-out plan, then up to ``max_resample_sweep`` sweeps of fresh draws
     from the mixture proposal, each sweep's distinct configurations projected
-    from the beta0 PEPO and replayed to the current beta and added to the
-    pool, with a new plan after every sweep that does not stop; finally SIR
-    selection of Ns distinct representatives from the pool with equal
-    weights.  Returns the new particles, their records and statistics, the
-    next free sample id and the event's audit record."""
+    from the beta0 PEPO (the u-th on rank (u-1) % nprocs, the representative
+    owner of ``execution.jl:34``), replayed to the current beta and added to
+    the pool, with a new plan after every sweep that does not stop; finally
+    SIR selection of Ns distinct representatives from the pool with equal
+    weights, moved to their new owners.  ``particles`` are this rank's,
+    ``records`` every rank's.  Returns this rank's new particles, every
+    rank's records and their statistics, the next free sample id and the
+    event's audit record."""
     from . import resample as rs
+    from .parallel import SerialExecution
+    e = e or SerialExecution()
+    rank, nprocs = e.rank(), e.nprocs()
     started = time.perf_counter()
     beta = replay[-1]["beta"]
-    interval_seconds = sum(p.time_seconds for p in particles)
+    interval_seconds = max(e.gather(sum(p.time_seconds for p in particles)))
     memo = rs.ScoreTable()
     caches = {0: baseline_cache}
     evaluations, sweeps, replay_rows = [], [], []
-    evaluation = _evaluate_resampling(memo, caches, particles, records, c, ops, 0)
+    evaluation = _evaluate_resampling(memo, caches, particles, records, c, ops, e, 0)
     evaluations.append(evaluation)
     plan = evaluation["plan"]
     M = rs.resample_fresh_count(plan, c.resampling)
@@ -609,8 +712,8 @@ def _resample(particles, records, checkpoint, c: RunConfig, baseline_cache, repl
     proposal_seconds = replay_seconds = 0.0
     for sweep in range(1, c.resampling.max_resample_sweep + 1):
         t = time.perf_counter()
-        batch = _draw_resampling_batch(memo, caches, pool_records, plan, M, c, event, sweep, ops)
-        proposal_time = time.perf_counter() - t
+        batch = _draw_resampling_batch(memo, caches, pool_records, plan, M, c, event, sweep, ops, e)
+        proposal_time = max(e.gather(time.perf_counter() - t))
         proposal_seconds += proposal_time
         lam = plan["selection"]["lam"]
         stop_reason = "no_fresh_draws" if M == 0 else rs.resample_stop(lam, sweep, c.resampling)
@@ -623,11 +726,11 @@ def _resample(particles, records, checkpoint, c: RunConfig, baseline_cache, repl
                       configuration=batch["configurations"][u], log_p0=batch["proposals"][u]["log_p0"],
                       log_q=batch["proposals"][u]["log_q"],
                       sampling_error=batch["proposals"][u]["max_environment_truncation"])
-                 for u, d in enumerate(batch["grouping"]["first_draw"])]
-        fresh = _new_particles(checkpoint, c, items, len(replay) == 1 and measure_at(c, beta), ops)
-        fresh_records, rows = ([], []) if M == 0 else _replay_fresh(fresh, replay, c, event, sweep, ops)
+                 for u, d in enumerate(batch["grouping"]["first_draw"]) if u % nprocs == rank]
+        fresh = e.phase(lambda: _new_particles(checkpoint, c, items, len(replay) == 1 and measure_at(c, beta), ops))
+        fresh_records, rows = ([], []) if M == 0 else _replay_fresh(fresh, replay, c, event, sweep, ops, e)
         replay_rows.extend(rows)
-        replay_time = time.perf_counter() - t
+        replay_time = max(e.gather(time.perf_counter() - t))
         replay_seconds += replay_time
         pool_particles.extend(fresh)
         all_fresh.extend(fresh_records)
@@ -639,30 +742,27 @@ def _resample(particles, records, checkpoint, c: RunConfig, baseline_cache, repl
                            timing=dict(proposal_seconds=proposal_time, replay_seconds=replay_time)))
         if stop_reason != "continue":
             break
-        evaluation = _evaluate_resampling(memo, caches, pool_particles, pool_records, c, ops, sweep)
+        evaluation = _evaluate_resampling(memo, caches, pool_particles, pool_records, c, ops, e, sweep)
         evaluations.append(evaluation)
         plan = evaluation["plan"]
         if plan["selection"]["lam"] >= c.resampling.lambda_threshold:
             stop_reason = "lambda_threshold"
             break
     caches.clear()
-    # _pool_selection (event.jl:69-77) and _redistribute (execution.jl:28-31)
     pool = list(records) + all_fresh
-    relative, scale = rs.aligned_weights(pool)
-    pivot = max(relative)
-    selection = rs.sir_select_until_unique([v - pivot for v in relative], [r["count"] for r in pool], c.Ns,
-                                           c.seed, event)
-    selection.update(common_log_weight=scale + pivot + selection["common_log_weight"],
-                     pool_statistics=_statistics(pool, c.Ns, c.lattice.Lx * c.lattice.Ly))
-    by_id = {p.id: p for p in pool_particles}
-    nxt = []
-    for i in selection["active"]:
-        p = by_id[pool[i]["id"]]
-        p.count = selection["multiplicity"][i]
-        p.relative_log_weight = selection["output_relative_log_weight"][i]
-        p.weight_log_scale = selection["common_log_weight"]
-        nxt.append(p)
-    post = sorted([_particle_record(p) for p in nxt], key=lambda r: r["id"])
+
+    def pool_selection():
+        """``_pool_selection`` (``event.jl:69-77``)."""
+        relative, scale = rs.aligned_weights(pool)
+        pivot = max(relative)
+        sel = rs.sir_select_until_unique([v - pivot for v in relative], [r["count"] for r in pool], c.Ns,
+                                         c.seed, event)
+        sel.update(common_log_weight=scale + pivot + sel["common_log_weight"],
+                   pool_statistics=_statistics(pool, c.Ns, c.lattice.Lx * c.lattice.Ly))
+        return sel
+    selection = e.broadcast(pool_selection)
+    nxt = _redistribute(pool_particles, pool, selection, ops, e, checkpoint.state)
+    post = _global_records(nxt, e)
     stats = _statistics(post, c.Ns, c.lattice.Lx * c.lattice.Ly)
     stats.update(source="sampling", time_seconds=interval_seconds)
     audit = dict(event=event, beta=beta, M=M,

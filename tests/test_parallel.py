@@ -53,6 +53,12 @@ class OracleOps:
         return dict(configuration=np.asarray(d["configuration"]), log_probability=d["log_probability"],
                     max_environment_truncation=d["max_environment_truncation"], **self._repairs(d))
 
+    def export_state(self, state):
+        return state
+
+    def import_state(self, blob, like):
+        return blob
+
     def probability(self, cache, configuration):
         from oracle import sampling as sp
         d = sp.sample_configuration(cache, configuration=np.asarray(configuration).tolist())
@@ -89,8 +95,16 @@ def _config(sps):
                          chi_environment=4, Ns=5, seed=9, resampling=sps.ResamplingOptions(enabled=False))
 
 
-def _run(sps, execution=None, fail_rank=None):
-    c = _config(sps)
+def _config_resampling(sps):
+    """An event at beta = 0.3 (eta_th = 1) with two sweeps, Ns = 6."""
+    return sps.RunConfig(lattice=sps.Lattice(2, 2), model=sps.TFIM(1.0, 0.7), beta0=0.1, beta_log=[0.1, 0.3],
+                         beta_measure=[0.1, 0.3], delta_tau_pur=0.05, delta_tau_peps=0.05, D_pur=2, D_peps=2,
+                         chi_environment=4, Ns=6, seed=5,
+                         resampling=sps.ResamplingOptions(enabled=True, eta_th=1.0, max_resample_sweep=2))
+
+
+def _run(sps, execution=None, fail_rank=None, resampling=False):
+    c = _config_resampling(sps) if resampling else _config(sps)
     ops = OracleOps(c)
     if fail_rank is not None and execution is not None and execution.rank() == fail_rank:
         def bad(*a, **k):
@@ -100,7 +114,7 @@ def _run(sps, execution=None, fail_rank=None):
     return sps.run_stochastic(c, cp, execution=execution, ops=ops)
 
 
-def _worker(rank, world, port, q, fail_rank):
+def _worker(rank, world, port, q, fail_rank, resampling=False):
     os.environ["MASTER_ADDR"] = "127.0.0.1"
     os.environ["MASTER_PORT"] = str(port)
     sys.path.insert(0, ROOT)
@@ -110,12 +124,13 @@ def _worker(rank, world, port, q, fail_rank):
         import __graft_entry__ as ge
         sps = ge.load_package()
         try:
-            res = _run(sps, sps.TorchExecution(), fail_rank)
+            res = _run(sps, sps.TorchExecution(), fail_rank, resampling)
             out = None if res is None else [(r["beta"], r["energy_per_site"], r["lnZ"], r["eta"])
                                              for r in res["observables"]["curve"]]
-            q.put((rank, "ok", out, None if res is None else res["metadata"]["mpi_size"]))
+            events = None if res is None else _event_summary(res)
+            q.put((rank, "ok", out, None if res is None else res["metadata"]["mpi_size"], events))
         except RuntimeError as ex:
-            q.put((rank, "error", str(ex), None))
+            q.put((rank, "error", str(ex), None, None))
     finally:
         dist.destroy_process_group()
 
@@ -126,11 +141,26 @@ def _free_port():
         return s.getsockname()[1]
 
 
-def _spawn(world, fail_rank=None):
+def _event_summary(res):
+    """Members, fresh draws, selected representatives and weights of each resampling event."""
+    out = []
+    for ev in res["diagnostics"]["events"]:
+        out.append(dict(members=[s["members"] for s in ev["sweeps"]],
+                        draws=[[(d["index"], tuple(np.asarray(d["configuration"]).reshape(-1).tolist()),
+                                 d["log_probability"]) for d in s["draws"]] for s in ev["sweeps"]],
+                        post=[(r["id"], r["count"], r["relative_log_weight"], r["weight_log_scale"])
+                              for r in ev["post"]],
+                        stop=ev["stop_reason"],
+                        moved=sum(1 for r in ev["post"]
+                                  if {q["id"]: q["owner"] for q in ev["pre"] + ev["fresh"]}[r["id"]] != r["owner"])))
+    return out
+
+
+def _spawn(world, fail_rank=None, resampling=False):
     ctx = mp.get_context("spawn")
     q = ctx.Queue()
     port = _free_port()
-    procs = [ctx.Process(target=_worker, args=(r, world, port, q, fail_rank)) for r in range(world)]
+    procs = [ctx.Process(target=_worker, args=(r, world, port, q, fail_rank, resampling)) for r in range(world)]
     for p in procs:
         p.start()
     results = [q.get(timeout=600) for _ in procs]
@@ -209,3 +239,30 @@ def test_batched_ops_match_single_ops(sps):
             assert (math.isnan(x) and math.isnan(y)) or abs(x - y) <= 1e-12 * max(1.0, abs(y))
     assert [d["configuration"].tolist() for d in res["diagnostics"]["born_draws"]] == \
         [d["configuration"].tolist() for d in serial["diagnostics"]["born_draws"]]
+
+
+def test_two_ranks_resampling_match_serial(sps):
+    """An annealed resampling event over two gloo ranks (scores and draws on
+    their owners, fresh samples by representative owner, selected particles
+    moved to their new ranks) gives the serial run's members, draws, selected
+    representatives with their weights, and curve."""
+    serial = _run(sps, resampling=True)
+    ref = [(r["beta"], r["energy_per_site"], r["lnZ"], r["eta"]) for r in serial["observables"]["curve"]]
+    ref_events = _event_summary(serial)
+    assert ref_events
+    results = _spawn(2, resampling=True)
+    assert [r[1] for r in results] == ["ok", "ok"], results
+    rank0 = results[0]
+    for a, b in zip(rank0[2], ref):
+        for x, y in zip(a, b):
+            assert (math.isnan(x) and math.isnan(y)) or abs(x - y) <= 1e-12 * max(1.0, abs(y))
+    for ev, rv in zip(rank0[4], ref_events):
+        assert ev["members"] == rv["members"] and ev["stop"] == rv["stop"]
+        for s1, s2 in zip(ev["draws"], rv["draws"]):
+            assert [d[:2] for d in s1] == [d[:2] for d in s2]
+            for d1, d2 in zip(s1, s2):
+                assert abs(d1[2] - d2[2]) <= 1e-12 * max(1.0, abs(d2[2]))
+        assert [p[:2] for p in ev["post"]] == [p[:2] for p in rv["post"]]
+        assert ev["moved"] > 0 and rv["moved"] == 0   # particles changed ranks on two, none on one
+        for p1, p2 in zip(ev["post"], rv["post"]):
+            assert abs(p1[2] - p2[2]) <= 1e-12 and abs(p1[3] - p2[3]) <= 1e-12 * max(1.0, abs(p2[3]))
