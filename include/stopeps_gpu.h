@@ -266,6 +266,12 @@ int sps_set_precision(sps_handle* h, int32_t mode);
  * candidates' milliseconds). */
 int sps_set_autotune(sps_handle* h, int32_t enable);
 int sps_autotune_report(sps_handle* h, char* buf, size_t n);
+/* No counterpart in the reference (MatrixAlgebraKit computes every truncated
+ * SVD from the full spectrum).  method 0 (default): truncated SVDs that keep
+ * a few vectors of a large block take the subspace iteration when no entropy
+ * is recorded; method 1: every truncated SVD from the full spectrum (the
+ * one-sided Jacobi path), slower, for comparisons with a full-spectrum SVD. */
+int sps_set_truncated_svd(sps_handle* h, int32_t method);
 /* No counterpart in the reference: host-side failure injection for tests
  * (nothing faults on the device; the library takes its ordinary error
  * paths).  force_repair != 0 treats every full-update bond fit as triggered,

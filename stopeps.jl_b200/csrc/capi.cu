@@ -126,6 +126,7 @@ void run_batch(sps_handle* h, int n, F&& fn) {
     h->workers.push_back(std::make_unique<Engine>(M.device));
     h->workers.back()->ctas_cap = M.num_sms / h->concurrency;
     h->workers.back()->force_repair = M.force_repair;
+    h->workers.back()->full_spectrum = M.full_spectrum;
     h->workers.back()->sweep_cap = M.sweep_cap;
     h->workers.back()->eigh_multi_min = M.eigh_multi_min;
     h->workers.back()->precision = M.precision;
@@ -272,6 +273,14 @@ int sps_autotune_report(sps_handle* h, char* buf, size_t n) {
     const std::string js = tune::report_json();
     if (!buf || js.size() + 1 > n) throw Error(SPS_ERR_ARGUMENT, "buffer too small");
     std::memcpy(buf, js.c_str(), js.size() + 1);
+  });
+}
+
+int sps_set_truncated_svd(sps_handle* h, int32_t method) {
+  return guarded(h, [&] {
+    if (method != 0 && method != 1) throw Error(SPS_ERR_ARGUMENT, "sps_set_truncated_svd: method is 0 or 1");
+    h->E->full_spectrum = method == 1;
+    for (auto& w : h->workers) w->full_spectrum = method == 1;
   });
 }
 

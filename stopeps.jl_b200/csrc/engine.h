@@ -177,6 +177,7 @@ class Engine {
   // every full-update bond
   int sweep_cap = 0;
   bool force_repair = false;
+  bool full_spectrum = false;    // truncated SVDs by the full spectrum (no subspace iteration)
   // eigendecompositions of blocks with at least this many rows in the PSD
   // repair take the multi-CTA route (eigh_unit_shifted); smaller ones the
   // single-CTA Jacobi eigh

@@ -1709,7 +1709,7 @@ KeptSVD svd_kept(Engine& E, const Tensor& A, const std::vector<int>& rows, const
                  const Trunc& tr, bool want_entropy, bool left) {
   BlockTables bt = tables_of(A, rows, cols);
   const int nr = (int)rows.size(), nc = (int)cols.size();
-  if (!want_entropy) {
+  if (!want_entropy && !E.full_spectrum) {
     KeptSVD res;
     if (svd_kept_topk(E, bt, A, nr, nc, tr, left, res)) return res;
   }

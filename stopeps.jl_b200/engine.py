@@ -95,6 +95,14 @@ class Engine:
             raise ValueError(f"unknown precision {mode!r}; one of {sorted(self.PRECISIONS)}")
         self.check(self.lib.sps_set_precision(self.h, self.PRECISIONS[mode]))
 
+    def set_truncated_svd(self, method="subspace"):
+        """``"subspace"`` (default): truncated SVDs keeping a few vectors of a large
+        block take the subspace iteration when no entropy is recorded;
+        ``"full"``: every truncated SVD from the full spectrum."""
+        if method not in ("subspace", "full"):
+            raise ValueError("method is 'subspace' or 'full'")
+        self.check(self.lib.sps_set_truncated_svd(self.h, 1 if method == "full" else 0))
+
     def set_autotune(self, enable=True):
         """Pick launch shapes (split-K slices, tcgen05 tile width) by timing the
         candidates on first use; the choices are shared process-wide."""
