@@ -13,11 +13,10 @@ log norms and projection norms; identical Born configurations.
 Two quantities carry looser, measured bounds.  Born log-probabilities agree to
 1e-15 for four of the six draws; one draw per absorption differs by 1e-8
 (exact compression) and 8e-6 (zip-up) relative, from the rows after the first
-truncated north boundary on: the subspace iteration of the truncated SVDs stops
-at a residual of 5e-14 (exact) or 1e-10 (zip-up) of the largest singular value,
-which allows a kept-subspace angle of residual / gap where the gap at the cut
-is small.  With every truncated SVD from the full spectrum the exact
-compression's draws agree to rounding (last test).  The bound is DRAW_TOL.  One full-update step (every ALS solve stops at its iteration limit,
+truncated north boundary on.  The difference comes from the subspace-iteration
+SVD of the truncations (the zip-up's splits also stop at a 1e-10 residual):
+with every truncated SVD from the full spectrum the exact compression's draws
+agree to rounding (last test).  The bound is DRAW_TOL.  One full-update step (every ALS solve stops at its iteration limit,
 so rounding is amplified by the conditioning of the reduced metrics): the
 oracle's own log-normalisation moves by 7e-8 under a 1e-15 perturbation of its
 input, the device differs by 3e-6; the bound is STEP_TOL.
@@ -130,10 +129,8 @@ def test_headline_projection_and_full_update_step(sps):
 
 def test_headline_draws_with_full_spectrum_svd(sps):
     """The exact-compression draws with every truncated SVD from the full
-    spectrum: all six log-probabilities to 1e-12 (measured 4e-15), where the
-    default subspace iteration leaves one draw at 1e-8 (its stopping rule, a
-    residual below 5e-14 of the largest singular value, allows a kept-subspace
-    angle of residual / gap when the gap at the cut is small)."""
+    spectrum: all log-probabilities to 1e-12 (measured 4e-15), where the
+    default subspace iteration leaves one draw at 1e-8."""
     g, e, st = _setup(sps)
     e.set_truncated_svd("full")
     cache = sps.SamplingCache(st, _method(sps, g, "plain"))

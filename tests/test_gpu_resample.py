@@ -8,9 +8,9 @@ site is bound to the PEPS's total parity, and the last row is not absorbed.
 Identical configurations; log-probabilities to 1e-10 where no north boundary
 is truncated, DRAW_TOL after one is (the rows after the first truncated north
 absorption differ by up to 5e-8 in their conditionals on the 4x4 D=4 PEPS,
-2.4e-8 relative in log p: the subspace-iteration SVD's residual stopping rule,
-as for the auxiliary draws at the headline shapes; with the full-spectrum SVD
-they agree to rounding, last test); the smallest relative eigenvalue of the site metrics to METRIC_TOL (the
+2.4e-8 relative in log p: it comes from the subspace-iteration SVD, as for
+the auxiliary draws at the headline shapes; with the full-spectrum SVD they
+agree to rounding, last test); the smallest relative eigenvalue of the site metrics to METRIC_TOL (the
 sign of eigenvalues at the rounding level, ~1e-21 here, is solver-dependent,
 so counts of clipped eigenvalues are not compared); the batched scores of
 given configurations; the exhaustive distribution of a small PEPS sums to one
@@ -152,7 +152,7 @@ def test_physical_draws_with_full_spectrum_svd_match_oracle_to_rounding(sps):
     """With every truncated SVD from the full spectrum (``set_truncated_svd("full")``)
     the physical-kind draws after a truncated north absorption agree with the
     oracle to rounding (measured 9e-15 on the 4x4 D=4 PEPS): the gap of the
-    default path comes from the subspace iteration's stopping rule."""
+    default path comes from the subspace iteration."""
     from oracle import sampling as osp
     g = golden("pepo_4x4_D4.npz")
     e, ps, ops = _projected(sps, g)
