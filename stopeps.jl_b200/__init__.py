@@ -17,6 +17,7 @@ from .driver import (run_purification, run_stochastic, ensemble_statistics, grou
 from . import _lib
 from .build import build, LIB as LIBRARY_PATH
 from .parallel import SerialExecution, TorchExecution
+from .checkpoint import save_checkpoint, load_checkpoint, CHECKPOINT_FORMAT
 from . import synthetic
 from . import bench_states
 
@@ -28,5 +29,6 @@ __all__ = [
     "measure_energy_batch", "lognorm_batch", "sample_conditionals", "sample_probability_batch",
     "run_purification", "run_stochastic",
     "ensemble_statistics", "group_configurations", "sample_uniforms", "step_schedule", "ThermalCheckpoint",
-    "Particle", "RESULT_SCHEMA_VERSION", "build", "LIBRARY_PATH",
+    "Particle", "RESULT_SCHEMA_VERSION", "build", "LIBRARY_PATH", "save_checkpoint", "load_checkpoint",
+    "CHECKPOINT_FORMAT",
 ]

@@ -157,6 +157,12 @@ class DeviceOps:
         return like.engine.upload_state(blob["sites"], blob["dims"], blob["is_pepo"], beta=blob["beta"],
                                         log_amplitude=blob["log_amplitude"])
 
+    def state_from(self, blob, c: RunConfig, engine=None):
+        """An exported state on a new engine for ``c`` (a checkpoint being loaded)."""
+        e = engine or eng.Engine.from_config(c)
+        return e.upload_state(blob["sites"], blob["dims"], blob["is_pepo"], beta=blob["beta"],
+                              log_amplitude=blob["log_amplitude"])
+
     def project(self, state, configuration):
         return eng.project_configuration(state, configuration)
 
@@ -389,7 +395,8 @@ def _advance_particles(particles, c: RunConfig, steps, energy: bool, ops=DEVICE_
         p.measurement_seconds = m["measurement_seconds"]
 
 
-def run_stochastic(c: RunConfig, checkpoint: ThermalCheckpoint, uniforms_fn=None, execution=None, ops=None):
+def run_stochastic(c: RunConfig, checkpoint: ThermalCheckpoint | None = None, uniforms_fn=None, execution=None,
+                   ops=None, checkpoint_path=None):
     """Draw Born samples from the beta0 checkpoint and evolve the weighted ensemble (``run.jl:76-134``).
 
     ``execution`` distributes the work like the reference's MPI backend
@@ -404,6 +411,12 @@ def run_stochastic(c: RunConfig, checkpoint: ThermalCheckpoint, uniforms_fn=None
     ops = ops or DEVICE_OPS
     e.phase(lambda: validate_config(c))
     e.check_arguments(repr(parameter_dict(c)))
+    if checkpoint is None:
+        # the checkpoint from disk (run.jl:79-87): every rank loads it
+        if checkpoint_path is None:
+            raise ValueError("supply a checkpoint or checkpoint_path")
+        from .checkpoint import load_checkpoint
+        checkpoint = e.phase(lambda: load_checkpoint(checkpoint_path, c, ops))
 
     def check_checkpoint():
         if not same_beta(checkpoint.state.beta, c.beta0):

@@ -54,10 +54,27 @@ class OracleOps:
                     max_environment_truncation=d["max_environment_truncation"], **self._repairs(d))
 
     def export_state(self, state):
-        return state
+        from oracle import z2
+        Lx, Ly = state.Lx, state.Ly
+        sites = [state[x, y] for y in range(Ly) for x in range(Lx)]
+        dims = [[(int(np.sum(p == 0)), int(np.sum(p == 1))) for p in A.p] for A in sites]
+        return dict(sites=[A.a.copy() for A in sites], dims=np.asarray(dims), is_pepo=state.kind == "pepo",
+                    beta=state.beta, log_amplitude=state.log_amplitude)
+
+    def _state(self, blob, Lx, Ly):
+        from oracle.model import State
+        from oracle.z2 import T, leg
+        grid = [[None] * Ly for _ in range(Lx)]
+        for i, (a, ld) in enumerate(zip(blob["sites"], blob["dims"])):
+            grid[i % Lx][i // Lx] = T(np.asarray(a, float), [leg(int(p), int(q)) for p, q in ld])
+        return State(Lx, Ly, grid, float(blob["beta"]), float(blob["log_amplitude"]),
+                     "pepo" if blob["is_pepo"] else "peps")
 
     def import_state(self, blob, like):
-        return blob
+        return self._state(blob, like.Lx, like.Ly)
+
+    def state_from(self, blob, c):
+        return self._state(blob, c.lattice.Lx, c.lattice.Ly)
 
     def probability(self, cache, configuration):
         from oracle import sampling as sp
