@@ -9,7 +9,7 @@ function.  All indices are 0-based here.
 from __future__ import annotations
 
 import math
-from dataclasses import dataclass, field
+from dataclasses import dataclass
 
 import numpy as np
 

@@ -8,7 +8,7 @@ repair path) for Z2 dense tensors.  0-based indices throughout.
 from __future__ import annotations
 
 import math
-from dataclasses import dataclass, field
+from dataclasses import dataclass
 
 import numpy as np
 

@@ -10,7 +10,7 @@ keep their field names and defaults.  Z2 spaces are written
 from __future__ import annotations
 
 import math
-from dataclasses import dataclass, field, fields, asdict
+from dataclasses import dataclass, field, fields
 from typing import Optional
 
 EPS = 2.220446049250313e-16

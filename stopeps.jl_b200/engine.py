@@ -10,7 +10,6 @@ from __future__ import annotations
 
 import ctypes as C
 import json
-import math
 
 import numpy as np
 
