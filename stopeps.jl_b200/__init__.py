@@ -18,6 +18,7 @@ from . import _lib
 from .build import build, LIB as LIBRARY_PATH
 from .parallel import SerialExecution, TorchExecution
 from .checkpoint import save_checkpoint, load_checkpoint, CHECKPOINT_FORMAT
+from .models import physical_space, dense_hamiltonian, exact_thermal_observables, identity_pepo, validate_state
 from . import synthetic
 from . import bench_states
 
@@ -30,5 +31,6 @@ __all__ = [
     "run_purification", "run_stochastic",
     "ensemble_statistics", "group_configurations", "sample_uniforms", "step_schedule", "ThermalCheckpoint",
     "Particle", "RESULT_SCHEMA_VERSION", "build", "LIBRARY_PATH", "save_checkpoint", "load_checkpoint",
-    "CHECKPOINT_FORMAT",
+    "CHECKPOINT_FORMAT", "physical_space", "dense_hamiltonian", "exact_thermal_observables", "identity_pepo",
+    "validate_state",
 ]
