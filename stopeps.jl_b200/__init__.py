@@ -19,6 +19,8 @@ from .build import build, LIB as LIBRARY_PATH
 from .parallel import SerialExecution, TorchExecution
 from .checkpoint import save_checkpoint, load_checkpoint, CHECKPOINT_FORMAT
 from .models import physical_space, dense_hamiltonian, exact_thermal_observables, identity_pepo, validate_state
+from .results import save_result, load_result, save_run_result
+from . import results as Results
 from . import synthetic
 from . import bench_states
 
@@ -32,5 +34,5 @@ __all__ = [
     "ensemble_statistics", "group_configurations", "sample_uniforms", "step_schedule", "ThermalCheckpoint",
     "Particle", "RESULT_SCHEMA_VERSION", "build", "LIBRARY_PATH", "save_checkpoint", "load_checkpoint",
     "CHECKPOINT_FORMAT", "physical_space", "dense_hamiltonian", "exact_thermal_observables", "identity_pepo",
-    "validate_state",
+    "validate_state", "save_result", "load_result", "save_run_result", "Results",
 ]

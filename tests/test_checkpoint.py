@@ -55,3 +55,28 @@ def test_checkpoint_checks(sps, tmp_path):
         sps.load_checkpoint(bad, c, ops=ops)
     with pytest.raises(ValueError, match="supply a checkpoint"):
         sps.run_stochastic(c, ops=ops)
+
+
+def test_result_record_round_trip(sps, tmp_path):
+    """``save_result`` / ``load_result`` (``src/io/results.jl:21-80``): the run record
+    comes back with the schema version and the same curve; without ``overwrite``
+    an existing file is kept; the extension is checked."""
+    import math
+    c = _config(sps)
+    ops = OracleOps(c)
+    res = sps.run_stochastic(c, sps.run_purification(c, ops=ops, identity=ops.identity), ops=ops)
+    path = str(tmp_path / "run" / "result.json")
+    dest = sps.save_run_result(path, res)
+    back = sps.load_result(dest)
+    assert back["schema_version"] == sps.RESULT_SCHEMA_VERSION == "2.7.0"
+    assert back["method"] == "stoPEPS" and "created_at" in back
+    for a, b in zip(res["observables"]["curve"], back["observables"]["curve"]):
+        for k in ("beta", "lnZ", "energy_per_site", "eta"):
+            assert (math.isnan(a[k]) and math.isnan(b[k])) or a[k] == b[k]
+    draws = back["diagnostics"]["born_draws"]
+    np.testing.assert_array_equal(np.asarray(draws[0]["configuration"]),
+                                  res["diagnostics"]["born_draws"][0]["configuration"])
+    with pytest.raises(FileExistsError):
+        sps.save_run_result(path, res, overwrite=False)
+    with pytest.raises(ValueError, match="extension"):
+        sps.save_run_result(str(tmp_path / "result.jld2"), res)
