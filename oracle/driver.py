@@ -28,6 +28,7 @@ class RunConfig:
     Ly: int = 2
     J: float = 1.0
     h: float = 0.7
+    fields: tuple | None = None   # per-site transverse fields (extension; x + y*Lx order)
     beta0: float = 0.1
     beta_log: list = field(default_factory=lambda: [0.0, 0.05, 0.1, 0.15, 0.2, 0.25, 0.3])
     beta_measure: list = field(default_factory=lambda: [0.0, 0.1, 0.2, 0.3])
@@ -102,7 +103,7 @@ def step_schedule(start, target, dtau):
 def observe(state, c, energy):
     """``_observe`` (``particles.jl:35-40``)."""
     if energy:
-        return sp.measure_energy(state, TFIM(c.J, c.h), c.boundary("measurement"),
+        return sp.measure_energy(state, TFIM(c.J, c.h, c.fields), c.boundary("measurement"),
                                  record_entropy=c.record_boundary_entropy)
     m = bm.lognorm(state, c.boundary("measurement"))
     m.update(energy_total=math.nan, energy_per_site=math.nan, magnetization=math.nan)
@@ -114,7 +115,7 @@ def evolve(state, c, steps, D, space):
     maxstate = maxenv = norml = 0.0
     reports = []
     for beta in steps:
-        r = fu.evolution_step(state, TFIM(c.J, c.h), (beta - state.beta) / 2, D, c.update,
+        r = fu.evolution_step(state, TFIM(c.J, c.h, c.fields), (beta - state.beta) / 2, D, c.update,
                               c.boundary("environment"), order=c.trotter_order, space=space,
                               record_entropy=c.record_boundary_entropy)
         state.beta = beta

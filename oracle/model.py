@@ -22,9 +22,19 @@ TRIV = leg(1, 0)     # open-boundary unit leg
 
 @dataclass
 class TFIM:
-    """``TFIM(J,h)`` with Z2 physical space (``src/models/tfim.jl:9-19``)."""
+    """``TFIM(J,h)`` with Z2 physical space (``src/models/tfim.jl:9-19``).
+
+    ``fields`` (optional, Lx*Ly values in x + y*Lx order) replaces the uniform
+    h by a field per site: the extension a per-site gradient needs (the
+    reference's model has one h).  The bond gates then split each site's own
+    field over its bonds (h_i / deg_i, as ``tfim.jl:46`` does with h)."""
     J: float = 1.0
     h: float = 0.7
+    fields: tuple | None = None
+
+    def field(self, x, y, Lx):
+        """The transverse field at 0-based site (x, y)."""
+        return self.h if self.fields is None else float(self.fields[x + y * Lx])
 
 
 def spin_operators():
@@ -46,8 +56,9 @@ def bond_hamiltonian(m: TFIM, Lx, Ly, a, b):
     I = np.eye(2)
     da = degree(Lx, Ly, *a)
     db = degree(Lx, Ly, *b)
-    return (-m.J * ZZ - (m.h / da) * np.einsum("pu,qv->pquv", X, I)
-            - (m.h / db) * np.einsum("pu,qv->pquv", I, X))
+    ha, hb = m.field(*a, Lx), m.field(*b, Lx)
+    return (-m.J * ZZ - (ha / da) * np.einsum("pu,qv->pquv", X, I)
+            - (hb / db) * np.einsum("pu,qv->pquv", I, X))
 
 
 def sym_expm(Hm: np.ndarray, t: float) -> np.ndarray:
@@ -64,8 +75,9 @@ def trotter_gate(m: TFIM, Lx, Ly, a, b, delta) -> T:
 
 
 def onsite_gate(m: TFIM, delta) -> np.ndarray:
+    """The one-site lattice's gate exp(delta h X) (the site's own field)."""
     X, _, _ = spin_operators()
-    return sym_expm(-m.h * X, -delta)
+    return sym_expm(-m.field(0, 0, 1) * X, -delta)
 
 
 @dataclass
@@ -144,7 +156,7 @@ def dense_hamiltonian(Lx, Ly, m: TFIM) -> np.ndarray:
             diag -= m.J * z(idx(x, y)) * z(idx(x, y + 1))
     H[b, b] = diag
     for i in range(N):
-        H[b ^ (1 << i), b] -= m.h
+        H[b ^ (1 << i), b] -= m.field(i % Lx, i // Lx, Lx)
     return H
 
 

@@ -421,7 +421,9 @@ def measure_energy(state: State, model: TFIM, method: bm.BoundaryMPS, record_ent
             zzsum += real_ratio(num, den)
     final = north[Ly]
     log_norm = math.log(bm.positive_real(bm.close_boundary(final.tensors), "norm")) + final.log_scale
-    et = -model.J * zzsum - model.h * xsum
+    hx = xsum * model.h if model.fields is None else float(
+        sum(model.field(x, y, Lx) * site_x[x, y] for x in range(Lx) for y in range(Ly)))
+    et = -model.J * zzsum - hx
     return dict(energy_total=et, energy_per_site=et / (Lx * Ly), log_norm=log_norm + 2 * state.log_amplitude,
                 tensor_log_norm=log_norm, max_environment_truncation=mx,
                 Se=(entropy.Se if entropy is not None else None), x_sum=xsum,

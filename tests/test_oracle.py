@@ -65,6 +65,46 @@ def test_purification_3x3_converges_to_exact_diagonalization():
         assert 3.0 < coarse / fine < 6.0
 
 
+def _site_x_exact(Lx, Ly, m, beta):
+    """<X_i> per site at inverse temperature beta by exact diagonalization."""
+    H = md.dense_hamiltonian(Lx, Ly, m)
+    e, V = np.linalg.eigh(H)
+    w = np.exp(-beta * (e - e.min()))
+    b = np.arange(1 << (Lx * Ly))
+    out = []
+    for i in range(Lx * Ly):
+        Xi = np.zeros_like(H)
+        Xi[b ^ (1 << i), b] = 1.0
+        out.append(float(w @ np.einsum("ik,ij,jk->k", V, Xi, V) / w.sum()))
+    return np.array(out)
+
+
+def test_per_site_fields_converge_to_exact_diagonalization():
+    """The per-site-field TFIM (an extension for per-site gradients; the
+    reference has one h): purification to beta=0.2 converges to the per-site ED
+    at second order in delta_tau, and the central difference of lnZ in h_i
+    (step 1e-4) gives beta <X_i> (the exact derivative) within the Trotter error."""
+    rng = np.random.default_rng(7)
+    fields = tuple(3.0 + rng.uniform(-0.5, 0.5, 6))
+    errs = []
+    for tau in (0.025, 0.0125):
+        c = _cfg(Lx=3, Ly=2, h=3.0, fields=fields, delta_tau_pur=tau, delta_tau_peps=tau)
+        r = dr.run_purification(c)[1][-1]
+        ex = md.exact_thermal_observables(3, 2, md.TFIM(1.0, 3.0, fields), 0.2)
+        errs.append(abs(r["energy_per_site"] - ex["energy_per_site"]))
+    assert errs[0] < 1e-4 and 3.0 < errs[0] / errs[1] < 6.0
+    f2 = tuple(3.0 + rng.uniform(-0.5, 0.5, 4))
+    exact = 0.2 * _site_x_exact(2, 2, md.TFIM(1.0, 3.0, f2), 0.2)
+    step = 1e-4
+    for i in range(4):
+        lz = []
+        for s in (+1, -1):
+            f = list(f2)
+            f[i] += s * step
+            lz.append(dr.run_purification(_cfg(h=3.0, fields=tuple(f), delta_tau_pur=0.0125))[1][-1]["lnZ"])
+        assert abs((lz[0] - lz[1]) / (2 * step) - exact[i]) < 1e-5   # measured 2.4e-6 (4.8e-7 at tau/2)
+
+
 def test_born_probabilities_sum_to_one_and_weights_give_Z():
     """Exhaustive 2x2: sum_k p_k = 1 and sum_k ||psi_k||^2 = Z(beta0) = ||PEPO||^2."""
     c = _cfg()
