@@ -272,6 +272,13 @@ int sps_autotune_report(sps_handle* h, char* buf, size_t n);
  * is recorded; method 1: every truncated SVD from the full spectrum (the
  * one-sided Jacobi path), slower, for comparisons with a full-spectrum SVD. */
 int sps_set_truncated_svd(sps_handle* h, int32_t method);
+/* Per-site transverse fields h_i (index x + y*Lx), an extension of the
+ * reference's uniform TFIM (src/models/tfim.jl:9-19: one h).  With fields
+ * set, the Trotter bond gates split each site's h_i over its bonds as the
+ * uniform gate splits h (src/models/tfim.jl:44-48), the 1x1 gate uses
+ * h_0, and sps_measure_energy's total is -J sum ZZ - sum_i h_i <X_i>.
+ * n = Lx*Ly sets them; n = 0 clears them (cfg.h everywhere again). */
+int sps_set_site_fields(sps_handle* h, int32_t n, const double* fields);
 /* No counterpart in the reference: host-side failure injection for tests
  * (nothing faults on the device; the library takes its ordinary error
  * paths).  force_repair != 0 treats every full-update bond fit as triggered,

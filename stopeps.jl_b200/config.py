@@ -45,14 +45,29 @@ class Lattice:
 
 @dataclass(frozen=True)
 class TFIM:
-    """H = -J sum ZZ - h sum X, Z2-symmetric physical space (X eigenbasis)."""
+    """H = -J sum ZZ - h sum X, Z2-symmetric physical space (X eigenbasis).
+
+    ``fields`` (optional, Lx*Ly values in x + y*Lx order) replaces the uniform
+    h by a transverse field per site, H = -J sum ZZ - sum_i h_i X_i: an
+    extension of the reference's model (one h) for per-site lnZ gradients
+    (d lnZ / d h_i = beta <X_i>).  ``None`` is the reference's model."""
     J: float = 1.0
     h: float = 0.7
     physical_space: Z2Space = Z2Space(1, 1)
+    fields: Optional[tuple] = None
 
     def __post_init__(self):
         if self.physical_space != Z2Space(1, 1):
             raise ValueError("TFIM supports Z2Space(0=>1,1=>1) in the X eigenbasis")
+        if self.fields is not None:
+            f = tuple(float(v) for v in self.fields)
+            if not f or not all(math.isfinite(v) for v in f):
+                raise ValueError("per-site fields must be a nonempty sequence of finite numbers")
+            object.__setattr__(self, "fields", f)
+
+    def field(self, x, y, Lx):
+        """The transverse field at 0-based site (x, y)."""
+        return self.h if self.fields is None else self.fields[x + y * Lx]
 
 
 @dataclass(frozen=True)
@@ -204,6 +219,8 @@ def validate_config(c: RunConfig) -> RunConfig:
         raise ValueError("invalid full-update options")
     if not (math.isfinite(c.model.J) and math.isfinite(c.model.h)):
         raise ValueError("nonfinite model parameter")
+    if c.model.fields is not None and len(c.model.fields) != c.lattice.Lx * c.lattice.Ly:
+        raise ValueError("per-site fields need one value per lattice site")
     for V in (c.bond_space_pur, c.bond_space_peps, c.environment_space, c.sampling_space,
               c.measurement_space, c.proposal_space):
         if V is None:
@@ -229,7 +246,8 @@ def parameter_dict(c: RunConfig) -> dict:
                     "sectors": [{"sector": "0", "multiplicity": x.n0}, {"sector": "1", "multiplicity": x.n1}]}
         if hasattr(x, "__dataclass_fields__"):
             d = {"type": type(x).__name__}
-            d.update({f.name: enc(getattr(x, f.name)) for f in fields(x)})
+            d.update({f.name: enc(getattr(x, f.name)) for f in fields(x)
+                      if not (isinstance(x, TFIM) and f.name == "fields" and x.fields is None)})
             return d
         return repr(x)
     d = {f.name: enc(getattr(c, f.name)) for f in fields(c)}

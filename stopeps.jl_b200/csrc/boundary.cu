@@ -1031,7 +1031,12 @@ EnergyResult measure_energy(Engine& E, const State& s, const Model& m, const BMP
   for (term = first_vertical; term < nterm; ++term) zzsum += real_ratio(vals[2 * term], vals[2 * term + 1]);
   const Env& fin = env.north[Ly];
   double ln = std::log(positive_real(close_boundary(E, fin.t), "norm")) + fin.log_scale;
-  out.energy_total = -m.J * zzsum - m.h * xsum;
+  double hx = m.h * xsum;
+  if (!m.fields.empty()) {   // sum_i h_i <X_i>
+    hx = 0;
+    for (int i = 0; i < Lx * Ly; ++i) hx += m.fields[i] * out.site_x[i];
+  }
+  out.energy_total = -m.J * zzsum - hx;
   out.energy_per_site = out.energy_total / (Lx * Ly);
   out.log_norm = ln + 2 * s.log_amplitude;
   out.tensor_log_norm = ln;

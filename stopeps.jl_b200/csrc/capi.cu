@@ -18,6 +18,7 @@ struct sps_handle {
   int concurrency = 1;
   cudaEvent_t t0 = nullptr, t1 = nullptr;
   sps_config cfg;
+  std::vector<double> site_fields;   // per-site transverse fields; empty: cfg.h everywhere
   std::unordered_map<int, State> states;
   std::unordered_map<int, SamplingCache> caches;
   std::unordered_map<int, int> cache_state;   // cache -> pinned state copy id
@@ -60,7 +61,13 @@ BMPS to_bmps(const sps_boundary* b) {
   return m;
 }
 
-Model model_of(const sps_handle* h) { return Model{h->cfg.J, h->cfg.h}; }
+Model model_of(const sps_handle* h) {
+  Model m;
+  m.J = h->cfg.J;
+  m.h = h->cfg.h;
+  m.fields = h->site_fields;
+  return m;
+}
 
 FUOptions fu_of(const sps_handle* h) {
   FUOptions o;
@@ -281,6 +288,21 @@ int sps_set_truncated_svd(sps_handle* h, int32_t method) {
     if (method != 0 && method != 1) throw Error(SPS_ERR_ARGUMENT, "sps_set_truncated_svd: method is 0 or 1");
     h->E->full_spectrum = method == 1;
     for (auto& w : h->workers) w->full_spectrum = method == 1;
+  });
+}
+
+int sps_set_site_fields(sps_handle* h, int32_t n, const double* fields) {
+  return guarded(h, [&] {
+    if (n == 0) {
+      h->site_fields.clear();
+      return;
+    }
+    if (n != h->cfg.Lx * h->cfg.Ly || !fields)
+      throw Error(SPS_ERR_ARGUMENT, "sps_set_site_fields: n must be Lx*Ly (or 0 to clear)");
+    std::vector<double> f(fields, fields + n);
+    for (double v : f)
+      if (!std::isfinite(v)) throw Error(SPS_ERR_ARGUMENT, "sps_set_site_fields: nonfinite field");
+    h->site_fields = std::move(f);
   });
 }
 

@@ -58,6 +58,7 @@ Tensor trotter_gate(Engine& E, const Model& m, int Lx, int Ly, int ax, int ay, i
   double X[2] = {1, -1};
   double H[16] = {0};
   double da = degree(Lx, Ly, ax, ay), db = degree(Lx, Ly, bx, by);
+  const double ha = m.field(ax, ay, Lx), hb = m.field(bx, by, Lx);   // each site's own field
   for (int p = 0; p < 2; ++p)
     for (int q = 0; q < 2; ++q)
       for (int u = 0; u < 2; ++u)
@@ -65,7 +66,7 @@ Tensor trotter_gate(Engine& E, const Model& m, int Lx, int Ly, int ax, int ay, i
           double zz = (p != u && q != v) ? 1.0 : 0.0;
           double xa = (p == u && q == v) ? X[p] : 0.0;
           double xb = (p == u && q == v) ? X[q] : 0.0;
-          H[(p * 2 + q) * 4 + (u * 2 + v)] = -m.J * zz - m.h / da * xa - m.h / db * xb;
+          H[(p * 2 + q) * 4 + (u * 2 + v)] = -m.J * zz - ha / da * xa - hb / db * xb;
         }
   double V[16], w[4], A[16];
   std::copy(H, H + 16, A);
@@ -712,7 +713,8 @@ StepReport evolution_step(Engine& E, State& s, const Model& m, double delta, int
   double gd = order == 2 ? delta / 2 : delta;
   if (s.Lx * s.Ly == 1) {
     // exp(-delta * (-h X)) on the physical leg
-    double g[4] = {std::exp(delta * m.h), 0, 0, std::exp(-delta * m.h)};
+    const double h0 = m.field(0, 0, 1);
+    double g[4] = {std::exp(delta * h0), 0, 0, std::exp(-delta * h0)};
     Par p2 = make_par(1, 1);
     Tensor G = E.upload({p2, p2}, g);
     s.sites[0] = ein(E, "pu,wnuaes->wnpaes", G, s.sites[0]);

@@ -10,6 +10,10 @@ namespace sps {
 
 struct Model {
   double J = 1.0, h = 0.7;
+  // per-site transverse fields (x + y*Lx), an extension for per-site
+  // gradients (the reference's TFIM has one h); empty: h everywhere
+  std::vector<double> fields;
+  double field(int x, int y, int Lx) const { return fields.empty() ? h : fields[x + y * Lx]; }
 };
 
 struct FUOptions {   // FullUpdate (src/evolution/full_update.jl:11-17)

@@ -56,6 +56,11 @@ class Engine:
         self.h = h
         self.Lx, self.Ly = int(Lx), int(Ly)
         self.model = model
+        if getattr(model, "fields", None) is not None:
+            f = np.ascontiguousarray(model.fields, np.float64)
+            if f.size != self.Lx * self.Ly:
+                raise ValueError("per-site fields need one value per lattice site")
+            self.check(self.lib.sps_set_site_fields(self.h, int(f.size), f.ctypes.data_as(C.POINTER(C.c_double))))
         self.update = update
 
     @classmethod

@@ -23,7 +23,8 @@ def physical_space(model: TFIM):
 
 def dense_hamiltonian(lattice: Lattice, model: TFIM) -> np.ndarray:
     """``dense_hamiltonian`` (``tfim.jl:50-64``): H = -J sum_<ij> Z_i Z_j - h sum_i X_i on
-    the open lattice, basis state b with spin i up when bit i (site x + y Lx) is 0."""
+    the open lattice, basis state b with spin i up when bit i (site x + y Lx) is 0;
+    with per-site fields the X_i term carries h_i."""
     Lx, Ly = lattice.Lx, lattice.Ly
     N = Lx * Ly
     if N > 16:
@@ -40,7 +41,7 @@ def dense_hamiltonian(lattice: Lattice, model: TFIM) -> np.ndarray:
                 diag -= model.J * spin[:, i] * spin[:, i + Lx]
     H = np.diag(diag)
     for i in range(N):
-        H[b ^ (1 << i), b] -= model.h
+        H[b ^ (1 << i), b] -= model.field(i % Lx, i // Lx, Lx)
     return H
 
 

@@ -22,6 +22,37 @@ def test_exact_diagonalization_matches_oracle(sps, Lx, Ly, h):
     assert sps.physical_space(sps.TFIM(1.0, h)) == sps.Z2Space(1, 1)
 
 
+def test_per_site_fields_config_and_exact_diagonalization(sps):
+    """The per-site-field extension: ED equals the oracle's, the uniform field
+    written out per site gives the reference's model bit for bit, the config
+    encoding of the reference's model is unchanged, and bad fields are refused."""
+    rng = np.random.default_rng(3)
+    f = tuple(0.7 + rng.uniform(-0.3, 0.3, 6))
+    H = sps.dense_hamiltonian(sps.Lattice(3, 2), sps.TFIM(1.0, 0.7, fields=f))
+    np.testing.assert_array_equal(H, md.dense_hamiltonian(3, 2, md.TFIM(1.0, 0.7, f)))
+    np.testing.assert_array_equal(sps.dense_hamiltonian(sps.Lattice(3, 2), sps.TFIM(1.0, 0.7, fields=[0.7] * 6)),
+                                  sps.dense_hamiltonian(sps.Lattice(3, 2), sps.TFIM(1.0, 0.7)))
+    # d lnZ / d h_i = beta <X_i>: the field gradient is the site magnetization
+    beta, i, eps = 0.4, 4, 1e-5
+    def lnz(fi):
+        g = list(f)
+        g[i] = fi
+        return sps.exact_thermal_observables(sps.Lattice(3, 2), sps.TFIM(1.0, 0.7, fields=g), beta)["lnZ"]
+    w, v = np.linalg.eigh(H)
+    rho = (v * np.exp(-beta * (w - w.min()))) @ v.T
+    b = np.arange(64)
+    xi = np.zeros((64, 64))
+    xi[b ^ (1 << i), b] = 1.0
+    assert abs((lnz(f[i] + eps) - lnz(f[i] - eps)) / (2 * eps) - beta * np.trace(rho @ xi) / np.trace(rho)) < 1e-7
+    assert "fields" not in sps.parameter_dict(sps.RunConfig(lattice=sps.Lattice(3, 2)))["model"]
+    assert sps.parameter_dict(sps.RunConfig(lattice=sps.Lattice(3, 2),
+                                            model=sps.TFIM(fields=f)))["model"]["fields"] == list(f)
+    with pytest.raises(ValueError):
+        sps.TFIM(fields=[1.0, float("nan")])
+    with pytest.raises(ValueError):
+        sps.validate_config(sps.RunConfig(lattice=sps.Lattice(3, 2), model=sps.TFIM(fields=[1.0] * 5)))
+
+
 class _HostState:
     """A host stand-in with the device state's interface (lattice, is_pepo, download)."""
 

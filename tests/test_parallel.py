@@ -89,7 +89,7 @@ class OracleOps:
 
     def measure_energy(self, state, method):
         from oracle import sampling as sp
-        m = sp.measure_energy(state, self.md.TFIM(self.c.model.J, self.c.model.h), self._m(method))
+        m = sp.measure_energy(state, self.md.TFIM(self.c.model.J, self.c.model.h, self.c.model.fields), self._m(method))
         return dict(m)
 
     def lognorm(self, state, method):
@@ -99,7 +99,7 @@ class OracleOps:
         u = self.c.update
         opts = self.fu.FullUpdate(u.max_iterations, u.error_tolerance, u.diagonal_shift,
                                   u.linear_max_iterations, u.linear_tolerance)
-        r = self.fu.evolution_step(state, self.md.TFIM(self.c.model.J, self.c.model.h), delta, D, opts,
+        r = self.fu.evolution_step(state, self.md.TFIM(self.c.model.J, self.c.model.h, self.c.model.fields), delta, D, opts,
                                    self._m(method), order=self.c.trotter_order,
                                    space=None if space is None else (space.n0, space.n1),
                                    record_entropy=self.c.record_boundary_entropy)
@@ -283,3 +283,24 @@ def test_two_ranks_resampling_match_serial(sps):
         assert ev["moved"] > 0 and rv["moved"] == 0   # particles changed ranks on two, none on one
         for p1, p2 in zip(ev["post"], rv["post"]):
             assert abs(p1[2] - p2[2]) <= 1e-12 and abs(p1[3] - p2[3]) <= 1e-12 * max(1.0, abs(p2[3]))
+
+
+def test_host_driver_with_site_fields(sps):
+    """The host driver carries per-site fields to the contraction ops: the
+    purification records equal the oracle driver's own run of the same model."""
+    from oracle import driver as odr
+    f = (0.5, 0.9, 0.7, 1.1)
+    c = sps.RunConfig(lattice=sps.Lattice(2, 2), model=sps.TFIM(1.0, 0.7, fields=f), beta0=0.1, beta_log=[0.1],
+                      beta_measure=[0.1], delta_tau_pur=0.05, delta_tau_peps=0.05, D_pur=2, D_peps=2,
+                      chi_environment=4, Ns=2, seed=9, resampling=sps.ResamplingOptions(enabled=False))
+    ops = OracleOps(c)
+    cp = sps.run_purification(c, ops=ops, identity=ops.identity)
+    _, rows = odr.run_purification(odr.RunConfig(Lx=2, Ly=2, J=1.0, h=0.7, fields=f, beta0=0.1, beta_log=[0.1],
+                                                 beta_measure=[0.1], delta_tau_pur=0.05, D_pur=2, D_peps=2,
+                                                 chi_environment=4, Ns=2, seed=9))
+    for a, b in zip(cp.purification, rows):
+        for k in ("lnZ", "energy_per_site"):
+            assert (math.isnan(a[k]) and math.isnan(b[k])) or abs(a[k] - b[k]) <= 1e-12 * max(1.0, abs(b[k]))
+    uniform = sps.run_purification(c.__class__(**{**c.__dict__, "model": sps.TFIM(1.0, 0.7)}), ops=OracleOps(
+        c.__class__(**{**c.__dict__, "model": sps.TFIM(1.0, 0.7)})), identity=ops.identity)
+    assert abs(uniform.purification[-1]["lnZ"] - cp.purification[-1]["lnZ"]) > 1e-6   # the fields matter
