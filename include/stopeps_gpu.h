@@ -57,7 +57,10 @@ typedef struct sps_config {
  * reference's row absorption (exact LQ sweep + truncated SVD sweep,
  * compress_boundary!, boundary_mps.jl:94-134); 1 is this library's zip-up
  * absorption (one sweep of truncated SVDs without a canonical form), which
- * has no counterpart in the reference. */
+ * has no counterpart in the reference; 2 is BoundaryMPSDiagonal
+ * (src/contraction/diagonal_mps.jl: anti-diagonal layers, site blocks,
+ * truncation of the bonds a block opens), taken by sps_lognorm,
+ * sps_measure_energy and the sampling caches, not by the full update. */
 typedef struct sps_boundary {
   int32_t chi;
   int32_t space0, space1;
@@ -205,8 +208,11 @@ int sps_evolution_step(sps_handle* h, int32_t state_id, double delta, int32_t D,
 /* lognorm(state, BoundaryMPS) (src/contraction/boundary_mps.jl:180-186) */
 int sps_lognorm(sps_handle* h, int32_t state_id, const sps_boundary* method, sps_lognorm_result* out);
 /* measure_energy(state, model, BoundaryMPS; record_entropy)
- * (src/measurement/energy.jl:31-78).  site_x (Lx*Ly), se_north/se_south
- * ((Ly-1)*(Lx-1), Se profile) may be NULL. */
+ * (src/measurement/energy.jl:31-78; the diagonal method
+ * src/measurement/diagonal_energy.jl:12-45).  site_x (Lx*Ly), se_north /
+ * se_south (the Se profile: (Ly-1)*(Lx-1) for the row methods; for the
+ * diagonal one the northwest / southeast per-site profiles, Lx*Ly each,
+ * index x + y*Lx) may be NULL. */
 int sps_measure_energy(sps_handle* h, int32_t state_id, const sps_boundary* method, sps_energy* out,
                        double* site_x, double* se_north, double* se_south);
 /* SamplingCache(state, BoundaryMPS; kind=:auxiliary) (src/sampling/born.jl:56-73) */
@@ -220,14 +226,17 @@ int sps_sampling_cache(sps_handle* h, int32_t pepo_id, const sps_boundary* metho
 int sps_sampling_cache_kind(sps_handle* h, int32_t state_id, const sps_boundary* method, int32_t kind,
                             int32_t* cache_id);
 int sps_sampling_cache_free(sps_handle* h, int32_t cache_id);
-/* sample_configuration(cache; rng) with the Lx*Ly uniforms (row-major site
- * order) in place of rand(rng) (src/sampling/born.jl:86-163).  configuration
+/* sample_configuration(cache; rng) with the Lx*Ly uniforms in place of
+ * rand(rng) (src/sampling/born.jl:86-163, src/sampling/diagonal_born.jl:24-97):
+ * uniforms[i] is consumed by the i-th site drawn, row-major for the row
+ * methods, by anti-diagonals for the diagonal one (x + y = 0, 1, ...; even
+ * diagonals by increasing x, odd ones by decreasing x).  configuration
  * receives SymmetryBasis labels 1 (even) / 2 (odd), index x + y*Lx. */
 int sps_sample(sps_handle* h, int32_t cache_id, const double* uniforms, int32_t* configuration,
                sps_sample_report* report);
 /* sample_configuration with the `conditionals` of its result (born.jl:95,
- * :146): the Lx*Ly conditional probabilities of the chosen labels in row-major
- * site order (0 past a zero-probability stop).  Draws from `uniforms`, or
+ * :146): the Lx*Ly conditional probabilities of the chosen labels in site
+ * order x + y*Lx (0 past a zero-probability stop).  Draws from `uniforms`, or
  * evaluates `given` (labels) when it is not NULL. */
 int sps_sample_conditionals(sps_handle* h, int32_t cache_id, const double* uniforms, const int32_t* given,
                             int32_t* configuration, double* conditionals, sps_sample_report* report);

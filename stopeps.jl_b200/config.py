@@ -97,6 +97,14 @@ class BoundaryMPSZipUp(BoundaryMPS):
 
 
 @dataclass(frozen=True)
+class BoundaryMPSDiagonal(BoundaryMPS):
+    """``BoundaryMPSDiagonal(chi, sector_space)`` (``src/contraction/diagonal_mps.jl:3-9``):
+    anti-diagonal layers x + y = t absorbed as site blocks, with the same ``chi``
+    and sector budget.  Taken by ``lognorm``, ``measure_energy`` and
+    ``SamplingCache``; the full update's bond environments stay row-based."""
+
+
+@dataclass(frozen=True)
 class ResamplingOptions:
     enabled: bool = True
     eta_th: float = 0.7

@@ -262,7 +262,7 @@ double close_boundary(Engine& E, const std::vector<Tensor>& B) {
   return sum_all(E, V);
 }
 
-static double positive_real(double z, const char* name) {
+double positive_real(double z, const char* name) {
   if (!(std::isfinite(z) && z > 0))
     throw Error(SPS_ERR_NUMERIC, std::string(name) + " requires a finite positive real value; received " +
                                      std::to_string(z));
@@ -271,6 +271,7 @@ static double positive_real(double z, const char* name) {
 
 // lognorm / contract_layers (boundary_mps.jl:165-186)
 LogNorm lognorm(Engine& E, const State& s, const BMPS& m) {
+  if (m.diagonal) return lognorm_diagonal(E, s, m);
   auto layers = row_layers(E, s);
   Env env = trivial_boundary(E, column(layers, s.Lx, 0), true);
   for (int y = 0; y < s.Ly; ++y) env = absorb(E, env, column(layers, s.Lx, y), m, true);
@@ -422,13 +423,13 @@ std::vector<double> normalize_state(Engine& E, State& s) {
 // ---------------------------------------------------------------------------
 // Born sampling (src/sampling/born.jl:56-163), kind = :auxiliary and :physical
 // ---------------------------------------------------------------------------
-static Tensor project_aux(Engine& E, const Tensor& A, int k) {
+Tensor project_aux(Engine& E, const Tensor& A, int k) {
   return slice_leg(E, A, 3, k, k == 0 ? make_par(1, 0) : make_par(0, 1));
 }
 
 // _project(A, B, k, :physical) for SymmetryBasis (basis.jl:87): the physical
 // leg restricted to its basis state k, a one-dimensional leg of that state's parity
-static Tensor project_physical(Engine& E, const Tensor& A, int k) {
+Tensor project_physical(Engine& E, const Tensor& A, int k) {
   const int c = (*A.legs[2])[k];
   return slice_leg(E, A, 2, k, c == 0 ? make_par(1, 0) : make_par(0, 1));
 }
@@ -451,6 +452,17 @@ SamplingCache make_sampling_cache(Engine& E, const State& s, const BMPS& m, int 
       if (A.dims[2] != 2) throw Error(SPS_ERR_ARGUMENT, "proposal sampling needs a two-state physical leg");
       c.target ^= (*A.legs[3])[0];
     }
+  }
+  if (m.diagonal) {
+    // the diagonal draw keeps the projected kets and the southeast
+    // boundaries of every layer (diagonal_born.jl:11-21)
+    for (auto& A : s.sites) {
+      std::array<Tensor, 2> kets;
+      for (int k = 0; k < 2; ++k) kets[k] = kind == KIND_PHYSICAL ? project_physical(E, A, k) : project_aux(E, A, k);
+      c.candidate_kets.push_back(kets);
+    }
+    diagonal_southeast(E, s, m, c.southeast);
+    return c;
   }
   c.layers = row_layers(E, s);
   for (auto& A : s.sites) {
@@ -480,7 +492,7 @@ static double logsumexp(const std::vector<double>& x) {
   return pivot + std::log(s);
 }
 
-static int categorical(const std::vector<double>& lm, double u, int* near) {
+int categorical(const std::vector<double>& lm, double u, int* near) {
   double z = logsumexp(lm);
   if (!std::isfinite(z)) throw Error(SPS_ERR_NUMERIC, "proposal requires positive total probability");
   double cum = 0;
@@ -666,6 +678,10 @@ static Tensor site_metric_root(Engine& E, const Tensor& left, const Tensor& top,
   Tensor H = contiguous(E, ein(E, "wbnc,bsce->wnes", X, Y));
   const int vl[4] = {0, 1, 4, 5};   // the site's virtual legs w, n, e, s
   for (int k = 3; k >= 0; --k) H = split(E, H, k, {A.legs[vl[k]], A.legs[vl[k]]});   // (wk wb nk nb ek eb sk sb)
+  return metric_root(E, H, res);
+}
+
+Tensor metric_root(Engine& E, const Tensor& H, SampleResult& res) {
   if (!all_finite(E, H)) throw Error(SPS_ERR_NUMERIC, "nonfinite norm metric");
   const double scale = norm(E, H);
   Tensor Hm = contiguous(E, perm_view(H, {1, 3, 5, 7, 0, 2, 4, 6}));   // (bras, kets)
@@ -797,6 +813,7 @@ static SampleResult sample_physical(Engine& E, const SamplingCache& c, const dou
 
 SampleResult sample_configuration(Engine& E, const SamplingCache& c, const double* uniforms,
                                   const int* configuration) {
+  if (c.method.diagonal) return sample_diagonal(E, c, uniforms, configuration);
   if (c.kind == KIND_PHYSICAL) return sample_physical(E, c, uniforms, configuration);
   if (uniforms && !configuration && c.Lx * c.Ly + 1 <= Engine::NSCAL - 64 && c.Lx + 3 <= 128)
     return sample_device(E, c, uniforms);
@@ -906,7 +923,7 @@ State project_configuration(Engine& E, const State& pepo, const int* configurati
 // _operator_factors(ZZ) for the Z2 TFIM: M[(p,u),(q,v)] = z[p,u] z[q,v] is
 // rank one in the odd block with singular value 2, so F = sqrt(2) z and
 // G = z / sqrt(2) on a one-state odd leg r (energy.jl:8-12).
-static void operator_factors(Engine& E, Tensor& F, Tensor& G) {
+void operator_factors(Engine& E, Tensor& F, Tensor& G) {
   Par p2 = make_par(1, 1), r = make_par(0, 1);
   double s2 = std::sqrt(2.0);
   double f[4] = {0, s2, s2, 0};          // F[p,u,r]: (0,1)->s2, (1,0)->s2
@@ -915,8 +932,8 @@ static void operator_factors(Engine& E, Tensor& F, Tensor& G) {
   G = E.upload({r, p2, p2}, g);
 }
 
-static void operator_pair(Engine& E, const Tensor& A, const Tensor& B, const Tensor& F, const Tensor& G,
-                          bool horizontal, Tensor& C, Tensor& D) {
+void operator_pair(Engine& E, const Tensor& A, const Tensor& B, const Tensor& F, const Tensor& G, bool horizontal,
+                   Tensor& C, Tensor& D) {
   if (horizontal) {
     C = fuse(E, ein(E, "wnuaes,pur->wnpaers", A, F), 4, 2);
     D = fuse(E, ein(E, "wnvaes,rqv->wrnqaes", B, G), 0, 2);
@@ -926,7 +943,7 @@ static void operator_pair(Engine& E, const Tensor& A, const Tensor& B, const Ten
   }
 }
 
-static double real_ratio(double a, double b) {
+double real_ratio(double a, double b) {
   if (b == 0) throw Error(SPS_ERR_NUMERIC, "zero local norm environment");
   double z = a / b;
   if (!std::isfinite(z)) throw Error(SPS_ERR_NUMERIC, "nonreal observable");
@@ -935,6 +952,7 @@ static double real_ratio(double a, double b) {
 
 EnergyResult measure_energy(Engine& E, const State& s, const Model& m, const BMPS& method,
                             bool record_entropy) {
+  if (method.diagonal) return measure_energy_diagonal(E, s, m, method, record_entropy);
   const int Lx = s.Lx, Ly = s.Ly;
   EnergyResult out;
   out.entropy.profile = record_entropy;

@@ -56,8 +56,9 @@ BMPS to_bmps(const sps_boundary* b) {
   m.chi = b->chi;
   m.space[0] = b->space0 >= 0 && b->space1 >= 0 ? b->space0 : -1;
   m.space[1] = b->space0 >= 0 && b->space1 >= 0 ? b->space1 : -1;
-  if (b->absorption != 0 && b->absorption != 1) throw Error(SPS_ERR_ARGUMENT, "unknown boundary absorption");
+  if (b->absorption < 0 || b->absorption > 2) throw Error(SPS_ERR_ARGUMENT, "unknown boundary absorption");
   m.zipup = b->absorption == 1;
+  m.diagonal = b->absorption == 2;
   return m;
 }
 
@@ -766,10 +767,11 @@ int sps_measure_energy(sps_handle* h, int32_t state_id, const sps_boundary* meth
     EnergyResult r = measure_energy(*h->E, s, model_of(h), to_bmps(method), h->cfg.record_boundary_entropy != 0);
     if (out) fill_energy(r, *out);
     if (site_x) std::memcpy(site_x, r.site_x.data(), r.site_x.size() * sizeof(double));
-    if (se_north && r.entropy.profile)
-      std::memcpy(se_north, r.entropy.north.data(), r.entropy.north.size() * sizeof(double));
-    if (se_south && r.entropy.profile)
-      std::memcpy(se_south, r.entropy.south.data(), r.entropy.south.size() * sizeof(double));
+    // the diagonal method's profiles are per site (northwest, southeast)
+    const auto& a = r.entropy.northwest.empty() ? r.entropy.north : r.entropy.northwest;
+    const auto& b = r.entropy.southeast.empty() ? r.entropy.south : r.entropy.southeast;
+    if (se_north && r.entropy.profile) std::memcpy(se_north, a.data(), a.size() * sizeof(double));
+    if (se_south && r.entropy.profile) std::memcpy(se_south, b.data(), b.size() * sizeof(double));
   });
 }
 
@@ -880,8 +882,15 @@ int sps_sample_conditionals(sps_handle* h, int32_t cache_id, const double* unifo
     SampleResult r = sample_configuration(*h->E, c, given ? nullptr : uniforms, given ? cfg.data() : nullptr);
     if (configuration)
       for (size_t i = 0; i < r.config.size(); ++i) configuration[i] = r.config[i];
-    if (conditionals)
-      for (size_t i = 0; i < r.config.size(); ++i) conditionals[i] = i < r.conditionals.size() ? r.conditionals[i] : 0.0;
+    if (conditionals) {
+      // r.conditionals follow the draw order; the diagonal draw visits the
+      // sites by anti-diagonals
+      std::vector<int> order;
+      if (c.method.diagonal) order = diagonal_draw_order(c.Lx, c.Ly);
+      for (size_t i = 0; i < r.config.size(); ++i) conditionals[i] = 0.0;
+      for (size_t i = 0; i < r.conditionals.size() && i < r.config.size(); ++i)
+        conditionals[c.method.diagonal ? order[i] : (int)i] = r.conditionals[i];
+    }
     if (report) fill_sample(r, *report);
   });
 }

@@ -1,0 +1,856 @@
+// Diagonal boundary-MPS contraction on the Z2 engine (BoundaryMPSDiagonal):
+// restates src/contraction/diagonal_mps.jl, the Born sampling of
+// src/sampling/diagonal_born.jl and the energy of
+// src/measurement/diagonal_energy.jl.
+//
+// The lattice is swept by anti-diagonal layers t = x + y (0-based sites; the
+// reference's t - 2, so the parity of t agrees).  A layer is absorbed as one
+// raw block per site: the frontier tensors of the site's input edges
+// contracted with its ket, then its bra.  The blocks are put in an exact
+// canonical form and only the bond a site opens between its two output
+// edges is truncated (the bonds between blocks already meet the budget).
+// Strips of one or two layers between cached boundaries carry the sampling
+// conditionals and the energy terms.  Networks are built from labelled
+// tensors that contract every label they share; every contraction is the
+// engine's table-addressed ein, every factorization its QR/LQ/SVD.
+#include "pipeline.h"
+#include <algorithm>
+#include <cfloat>
+
+namespace sps {
+namespace {
+
+const int VAX[4] = {0, 1, 4, 5};   // w, n, e, s legs of a site tensor (w, n, p, a, e, s)
+const int PHYS = -21, AUX = -22;   // physical and auxiliary legs shared by ket and bra
+const int LBL = 1 << 24, RBL = LBL + 1, R2L = LBL + 2;   // raw-block chain ends
+const int BOND = 1 << 20;          // strip labels of boundary bonds
+
+// _DiagonalTensor (diagonal_mps.jl:14-20): a tensor with one label per leg,
+// or a plain number
+struct LT {
+  Tensor t;
+  std::vector<int> lab;
+  bool number = false;
+  bool unit = false;   // every leg one-dimensional and even, value 1
+  double s = 1.0;
+};
+
+LT number(double v) {
+  LT a;
+  a.number = true;
+  a.s = v;
+  return a;
+}
+
+int index_of(const std::vector<int>& v, int x) {
+  auto it = std::find(v.begin(), v.end(), x);
+  return it == v.end() ? -1 : (int)(it - v.begin());
+}
+
+char letter(int i) {
+  if (i < 26) return (char)('a' + i);
+  if (i < 52) return (char)('A' + i - 26);
+  throw Error(SPS_ERR_ARGUMENT, "diagonal network: too many legs");
+}
+
+// the engine, the lattice's edge labels (_diagonal_ports,
+// diagonal_mps.jl:91-97) and a unit vector for open-boundary legs
+struct Net {
+  Engine& E;
+  int Lx, Ly;
+  Par triv;
+  Tensor u1;
+  Net(Engine& e, int lx, int ly) : E(e), Lx(lx), Ly(ly), triv(make_par(1, 0)) { u1 = unit_tensor(E, {triv}); }
+  int hedge(int x, int y) const { return 1 + x + y * (Lx + 1); }             // (x-1,y)-(x,y), x = 0..Lx
+  int vedge(int x, int y) const { return 1 + (Lx + 1) * Ly + x + y * Lx; }   // (x,y-1)-(x,y), y = 0..Ly
+  std::array<int, 4> ports(int x, int y) const { return {hedge(x, y), vedge(x, y), hedge(x + 1, y), vedge(x, y + 1)}; }
+  std::array<bool, 4> inside(int x, int y) const { return {x > 0, y > 0, x < Lx - 1, y < Ly - 1}; }
+  LT unit(int label) const {
+    LT a;
+    a.t = u1;
+    a.lab = {label};
+    a.unit = true;
+    return a;
+  }
+};
+
+// A with `count` trivial legs added in front or at the back (a view)
+Tensor with_trivial(const Tensor& A, int count, bool front, const Par& triv) {
+  Tensor t = A;
+  const int64_t size = std::max<int64_t>(A.size(), 1);
+  for (int i = 0; i < count; ++i) {
+    if (front) {
+      t.legs.insert(t.legs.begin(), triv);
+      t.dims.insert(t.dims.begin(), 1);
+      t.strides.insert(t.strides.begin(), size);
+    } else {
+      t.legs.push_back(triv);
+      t.dims.push_back(1);
+      t.strides.push_back(1);
+    }
+  }
+  return t;
+}
+
+// _diagonal_join (diagonal_mps.jl:21-28): contract the shared labels; the
+// result keeps a's free labels, then b's
+LT join(Net& n, const LT& a, const LT& b) {
+  Engine& E = n.E;
+  if (a.number || b.number) {
+    if (a.number && b.number) return number(a.s * b.s);
+    const LT& t = a.number ? b : a;
+    const double f = a.number ? a.s : b.s;
+    if (f == 1.0) return t;
+    LT r = t;
+    r.t = clone(E, t.t);
+    scale_inplace(E, r.t, f);
+    r.unit = false;
+    return r;
+  }
+  std::vector<int> common, fa, fb;
+  for (int k : a.lab) (index_of(b.lab, k) >= 0 ? common : fa).push_back(k);
+  for (int k : b.lab)
+    if (index_of(a.lab, k) < 0) fb.push_back(k);
+  if (fa.empty() && fb.empty()) {   // a closed network
+    std::vector<int> order;
+    for (int i = 0; i < (int)b.lab.size(); ++i) {
+      const int j = index_of(a.lab, b.lab[i]);
+      if (a.t.dims[j] != b.t.dims[i] || *a.t.legs[j] != *b.t.legs[i])
+        throw Error(SPS_ERR_ARGUMENT, "diagonal network: leg mismatch in a closed contraction");
+      order.push_back(j);
+    }
+    return number(dot(E, perm_view(a.t, order), b.t));
+  }
+  if (common.empty()) {
+    // outer products only meet unit vectors here: add their trivial legs
+    LT r;
+    r.lab = a.lab;
+    r.lab.insert(r.lab.end(), b.lab.begin(), b.lab.end());
+    if (b.unit) {
+      r.t = with_trivial(a.t, (int)b.lab.size(), false, n.triv);
+      r.unit = a.unit;
+    } else if (a.unit) {
+      r.t = with_trivial(b.t, (int)a.lab.size(), true, n.triv);
+    } else {
+      throw Error(SPS_ERR_ARGUMENT, "diagonal network: disconnected tensors");
+    }
+    return r;
+  }
+  std::vector<int> all = a.lab;
+  all.insert(all.end(), fb.begin(), fb.end());
+  std::string spec;
+  for (int k : a.lab) spec += letter(index_of(all, k));
+  spec += ',';
+  for (int k : b.lab) spec += letter(index_of(all, k));
+  spec += "->";
+  LT r;
+  for (int k : fa) {
+    spec += letter(index_of(all, k));
+    r.lab.push_back(k);
+  }
+  for (int k : fb) {
+    spec += letter(index_of(all, k));
+    r.lab.push_back(k);
+  }
+  r.t = ein(E, spec, a.t, b.t);
+  return r;
+}
+
+LT labelled(const Tensor& t, std::vector<int> lab) {
+  LT a;
+  a.t = t;
+  a.lab = std::move(lab);
+  return a;
+}
+
+// _diagonal_reorder (a view)
+Tensor reordered(const LT& a, const std::vector<int>& labels) {
+  if (labels.size() != a.lab.size()) throw Error(SPS_ERR_ARGUMENT, "diagonal tensor labels");
+  std::vector<int> order;
+  for (int k : labels) {
+    const int i = index_of(a.lab, k);
+    if (i < 0) throw Error(SPS_ERR_ARGUMENT, "diagonal tensor labels");
+    order.push_back(i);
+  }
+  return perm_view(a.t, order);
+}
+
+// _diagonal_apply (diagonal_mps.jl:58-88): contract the two input ports of
+// `msg` with the ket A, then the bra B; the other two virtual legs leave as
+// fused (ket, bra) ports, appended in w, n, e, s order.  `phys` (two labels)
+// keeps the physical legs open.
+LT apply(Net& n, LT msg, const Tensor& A, const Tensor& B, const std::array<int, 4>& ports,
+         const std::vector<int>& inputs, const int* phys = nullptr) {
+  if (inputs.size() != 2) throw Error(SPS_ERR_ARGUMENT, "a diagonal vertex has two input ports");
+  int rk[6] = {-1, -2, PHYS, AUX, -5, -6}, rb[6] = {-11, -12, PHYS, AUX, -15, -16};
+  if (phys) {
+    rk[2] = phys[0];
+    rb[2] = phys[1];
+  }
+  for (int port : inputs) {
+    const int j = (int)(std::find(ports.begin(), ports.end(), port) - ports.begin());
+    const int axis = VAX[j];
+    const int pos = index_of(msg.lab, port);
+    if (pos < 0 || *msg.t.legs[pos] != *fused_par({A.legs[axis], B.legs[axis]}))
+      throw Error(SPS_ERR_ARGUMENT, "diagonal network: input port does not match the site's legs");
+    msg.t = split(n.E, msg.t, pos, {A.legs[axis], B.legs[axis]});
+    msg.lab.erase(msg.lab.begin() + pos);
+    msg.lab.insert(msg.lab.begin() + pos, {rk[axis], rb[axis]});
+    msg.unit = false;
+  }
+  msg = join(n, msg, labelled(A, std::vector<int>(rk, rk + 6)));
+  msg = join(n, msg, labelled(B, std::vector<int>(rb, rb + 6)));
+  for (int j = 0; j < 4; ++j) {
+    const int port = ports[j];
+    if (std::find(inputs.begin(), inputs.end(), port) != inputs.end()) continue;
+    const int axis = VAX[j];
+    std::vector<int> others, order;
+    for (int i = 0; i < (int)msg.lab.size(); ++i)
+      if (msg.lab[i] != rk[axis] && msg.lab[i] != rb[axis]) {
+        others.push_back(msg.lab[i]);
+        order.push_back(i);
+      }
+    order.push_back(index_of(msg.lab, rk[axis]));
+    order.push_back(index_of(msg.lab, rb[axis]));
+    msg.t = fuse(n.E, perm_view(msg.t, order), (int)others.size(), 2);
+    others.push_back(port);
+    msg.lab = others;
+  }
+  return msg;
+}
+
+// sites of layer t by increasing x - y (increasing x)
+std::vector<std::array<int, 2>> layer_sites(int Lx, int Ly, int t) {
+  std::vector<std::array<int, 2>> out;
+  for (int x = std::max(0, t - Ly + 1); x <= std::min(Lx - 1, t); ++x) out.push_back({x, t - x});
+  return out;
+}
+
+struct Layout {   // _diagonal_layer_layout (diagonal_mps.jl:158-176)
+  std::vector<std::array<int, 2>> sites;
+  std::vector<std::vector<int>> inputs, outputs, ranges;
+  std::vector<int> edges;
+};
+
+Layout layer_layout(const Net& n, const DiagEnv& inp, int t, bool reverse) {
+  Layout L;
+  L.sites = layer_sites(n.Lx, n.Ly, t);
+  const int ia[2] = {reverse ? 3 : 0, reverse ? 2 : 1};
+  const int oa[2] = {reverse ? 0 : 3, reverse ? 1 : 2};
+  for (auto& s : L.sites) {
+    auto ports = n.ports(s[0], s[1]);
+    auto inside = n.inside(s[0], s[1]);
+    std::vector<int> incoming, out, idx, range;
+    for (int k : ia)
+      if (inside[k]) incoming.push_back(ports[k]);
+    const int p = incoming.empty() ? 0 : index_of(inp.edges, incoming[0]);
+    for (int i = 0; i < (int)incoming.size(); ++i) {
+      if (p < 0 || p + i >= (int)inp.edges.size() || inp.edges[p + i] != incoming[i])
+        throw Error(SPS_ERR_ARGUMENT, "nonadjacent diagonal frontier inputs");
+      idx.push_back(p + i);
+    }
+    for (int k : oa)
+      if (inside[k]) out.push_back(ports[k]);
+    for (int i = 0; i < (int)out.size(); ++i) range.push_back((int)L.edges.size() + i);
+    L.inputs.push_back(idx);
+    L.outputs.push_back(out);
+    L.ranges.push_back(range);
+    L.edges.insert(L.edges.end(), out.begin(), out.end());
+  }
+  return L;
+}
+
+// _diagonal_raw_block (diagonal_mps.jl:179-209): legs (left, outputs..., right)
+Tensor raw_block(Net& n, const DiagEnv& inp, const Tensor& A, int x, int y, const std::vector<int>& idx,
+                 const std::vector<int>& outputs, bool reverse) {
+  auto ports = n.ports(x, y);
+  auto inside = n.inside(x, y);
+  const int ia[2] = {reverse ? 3 : 0, reverse ? 2 : 1};
+  const int oa[2] = {reverse ? 0 : 3, reverse ? 1 : 2};
+  std::vector<int> inputs;
+  for (int k : ia)
+    if (inside[k]) inputs.push_back(ports[k]);
+  LT phi;
+  if (inputs.empty()) {
+    if (!inp.t.empty()) throw Error(SPS_ERR_ARGUMENT, "disconnected diagonal initialization");
+    phi = labelled(unit_tensor(n.E, {n.triv, n.triv}), {LBL, RBL});
+    phi.unit = true;
+  } else if (inputs.size() == 1) {
+    phi = labelled(inp.t[idx[0]], {LBL, inputs[0], RBL});
+  } else {
+    phi = join(n, labelled(inp.t[idx[0]], {LBL, inputs[0], R2L}), labelled(inp.t[idx[1]], {R2L, inputs[1], RBL}));
+  }
+  for (int k : ia)
+    if (!inside[k]) phi = join(n, phi, n.unit(ports[k]));
+  LT theta = apply(n, phi, A, A, ports, {ports[ia[0]], ports[ia[1]]});
+  for (int k : oa)
+    if (!inside[k]) theta = join(n, theta, n.unit(ports[k]));
+  std::vector<int> order{LBL};
+  order.insert(order.end(), outputs.begin(), outputs.end());
+  order.push_back(RBL);
+  return contiguous(n.E, reordered(theta, order));
+}
+
+// _diagonal_normalized: A / |A| in place (A owns its buffer), log |A|
+double normalize(Engine& E, Tensor& A) {
+  const double s = norm(E, A);
+  if (!std::isfinite(s)) throw Error(SPS_ERR_NUMERIC, "nonfinite diagonal boundary norm");
+  if (s == 0) return -INFINITY;
+  scale_inplace(E, A, 1.0 / s);
+  return std::log(s);
+}
+
+// c = R (k, r) times the first leg of X
+Tensor times_first(Engine& E, const Tensor& R, const Tensor& X) {
+  std::string rest;
+  for (int i = 1; i < X.rank(); ++i) rest += letter(2 + i);
+  return ein(E, "ab,b" + rest + "->a" + rest, R, X);
+}
+
+// c = the last leg of X times L (l, k)
+Tensor times_last(Engine& E, const Tensor& X, const Tensor& L) {
+  std::string rest;
+  for (int i = 0; i + 1 < X.rank(); ++i) rest += letter(2 + i);
+  return ein(E, rest + "a,ab->" + rest + "b", X, L);
+}
+
+// _diagonal_block_center_step! (diagonal_mps.jl:219-237)
+double block_center_step(Engine& E, std::vector<Tensor>& blocks, int j, bool right) {
+  const Tensor& A = blocks[j];
+  const int rank = A.rank();
+  std::vector<int> head, tail;
+  if (right) {
+    for (int i = 0; i + 1 < rank; ++i) head.push_back(i);
+    QRres f = qr(E, A, head, {rank - 1});
+    blocks[j] = f.Q;
+    Tensor R = contiguous(E, f.R);
+    const double s = normalize(E, R);
+    blocks[j + 1] = times_first(E, R, blocks[j + 1]);
+    return s;
+  }
+  for (int i = 1; i < rank; ++i) tail.push_back(i);
+  LQres f = lq(E, A, {0}, tail);
+  blocks[j] = f.Q;
+  Tensor L = contiguous(E, f.L);
+  const double s = normalize(E, L);
+  blocks[j - 1] = times_last(E, blocks[j - 1], L);
+  return s;
+}
+
+struct Compressed {
+  std::vector<Tensor> tensors;
+  double log_scale = 0, max_trunc = 0;
+};
+
+// _diagonal_compress_blocks! (diagonal_mps.jl:240-271)
+Compressed compress_blocks(Engine& E, std::vector<Tensor>& blocks, const Layout& L, const BMPS& m, bool right,
+                           bool reverse, Entropy* ent, int Lx) {
+  const int n = (int)blocks.size();
+  Compressed c;
+  if (right) {
+    for (int j = n - 1; j >= 1; --j) c.log_scale += block_center_step(E, blocks, j, false);
+  } else {
+    for (int j = 0; j < n - 1; ++j) c.log_scale += block_center_step(E, blocks, j, true);
+  }
+  Trunc tr;
+  tr.chi = m.chi;
+  tr.space[0] = m.space[0];
+  tr.space[1] = m.space[1];
+  c.tensors.resize(L.edges.size());
+  for (int step = 0; step < n; ++step) {
+    const int j = right ? step : n - 1 - step;
+    const auto& cut = L.ranges[j];
+    if (cut.empty()) throw Error(SPS_ERR_ARGUMENT, "diagonal block without outputs");
+    if (cut.size() == 2) {
+      SVDres f = svd(E, blocks[j], {0, 1}, {2, 3}, tr, ent != nullptr);
+      if (ent) {
+        const int site = L.sites[j][0] + L.sites[j][1] * Lx;
+        ent->maximum = std::max(ent->maximum, f.entropy);
+        if (ent->profile) (reverse ? ent->southeast : ent->northwest)[site] = f.entropy;
+      }
+      c.max_trunc = std::max(c.max_trunc, f.norm == 0 ? 0.0 : (f.err / f.norm) * (f.err / f.norm));
+      std::vector<double> sv(f.S[0]);
+      sv.insert(sv.end(), f.S[1].begin(), f.S[1].end());
+      if (right) {
+        c.tensors[cut[0]] = f.U;
+        blocks[j] = scale_leg(E, f.V, 0, sv);
+      } else {
+        c.tensors[cut[1]] = f.V;
+        blocks[j] = scale_leg(E, f.U, 2, sv);
+      }
+    }
+    if (j == (right ? n - 1 : 0)) {
+      blocks[j] = contiguous(E, blocks[j]);
+      c.log_scale += normalize(E, blocks[j]);
+    } else {
+      c.log_scale += block_center_step(E, blocks, j, right);
+    }
+    c.tensors[right ? cut.back() : cut.front()] = blocks[j];
+  }
+  return c;
+}
+
+// _diagonal_absorb_layer! (diagonal_mps.jl:272-297); site(x, y) gives the
+// tensor absorbed at a site
+template <class Site>
+void absorb_layer(Net& n, DiagEnv& env, Site site, int t, const BMPS& m, bool reverse, Entropy* ent) {
+  if (m.chi < 1) throw Error(SPS_ERR_ARGUMENT, "chi must be positive");
+  Layout L = layer_layout(n, env, t, reverse);
+  std::vector<Tensor> blocks;
+  double scale = env.log_scale;
+  for (size_t j = 0; j < L.sites.size(); ++j) {
+    const int x = L.sites[j][0], y = L.sites[j][1];
+    Tensor A = raw_block(n, env, site(x, y), x, y, L.inputs[j], L.outputs[j], reverse);
+    scale += normalize(n.E, A);
+    blocks.push_back(A);
+  }
+  if (L.edges.empty()) {
+    // the last corner: two unit boundary bonds
+    if (blocks.size() != 1 || blocks[0].size() != 1) throw Error(SPS_ERR_ARGUMENT, "diagonal corner is not closed");
+    env.t.clear();
+    env.scalar = sum_all(n.E, blocks[0]);
+  } else {
+    const bool right = blocks.size() < 2 ? !reverse : ((t % 2 == 0) != reverse);
+    Compressed c = compress_blocks(n.E, blocks, L, m, right, reverse, ent, n.Lx);
+    env.t = c.tensors;
+    env.max_trunc = std::max(env.max_trunc, c.max_trunc);
+    scale += c.log_scale;
+  }
+  env.edges = L.edges;
+  env.log_scale = scale;
+}
+
+}  // namespace
+
+// lognorm for the diagonal method (diagonal_mps.jl:315-323)
+LogNorm lognorm_diagonal(Engine& E, const State& s, const BMPS& m) {
+  Net n(E, s.Lx, s.Ly);
+  DiagEnv env;
+  auto site = [&](int x, int y) -> const Tensor& { return s.at(x, y); };
+  for (int t = 0; t < s.Lx + s.Ly - 1; ++t) absorb_layer(n, env, site, t, m, false, nullptr);
+  const double v = std::log(positive_real(env.scalar, "norm")) + env.log_scale;
+  return {v + 2 * s.log_amplitude, v, env.max_trunc};
+}
+
+// _diagonal_boundaries(side = :southeast) (diagonal_mps.jl:298-314)
+void diagonal_southeast(Engine& E, const State& s, const BMPS& m, std::vector<DiagEnv>& se) {
+  Net n(E, s.Lx, s.Ly);
+  const int nl = s.Lx + s.Ly - 1;
+  se.assign(nl + 1, DiagEnv());
+  auto site = [&](int x, int y) -> const Tensor& { return s.at(x, y); };
+  for (int t = nl - 1; t >= 0; --t) {
+    se[t] = se[t + 1];
+    absorb_layer(n, se[t], site, t, m, true, nullptr);
+  }
+}
+
+std::vector<int> diagonal_draw_order(int Lx, int Ly) {
+  std::vector<int> out;
+  for (int t = 0; t < Lx + Ly - 1; ++t) {
+    auto s = layer_sites(Lx, Ly, t);
+    if (t % 2 == 1) std::reverse(s.begin(), s.end());
+    for (auto& p : s) out.push_back(p[0] + p[1] * Lx);
+  }
+  return out;
+}
+
+}  // namespace sps
+
+namespace sps {
+namespace {
+
+// DiagonalStrip / _diagonal_strip (diagonal_mps.jl:325-363): the sites of
+// layers first..last by increasing x - y, the frontier tensors of the two
+// boundaries attached to the site that owns their edge, unit vectors on
+// open-boundary ports, and the unit ends of the boundary chains
+struct Strip {
+  std::vector<std::array<int, 2>> sites;
+  std::vector<std::array<int, 4>> ports;
+  std::vector<std::vector<LT>> att;
+  LT left, right;
+  double max_trunc = 0;
+};
+
+Strip make_strip(Net& n, int first, int last, const DiagEnv& nw, const DiagEnv& se) {
+  Strip s;
+  for (int t = first; t <= last; ++t)
+    for (auto& p : layer_sites(n.Lx, n.Ly, t)) s.sites.push_back(p);
+  std::stable_sort(s.sites.begin(), s.sites.end(),
+                   [](const std::array<int, 2>& a, const std::array<int, 2>& b) { return a[0] - a[1] < b[0] - b[1]; });
+  for (auto& p : s.sites) s.ports.push_back(n.ports(p[0], p[1]));
+  s.att.resize(s.sites.size());
+  s.left = number(1.0);
+  s.right = number(1.0);
+  int base = BOND;
+  for (const DiagEnv* b : {&nw, &se}) {
+    if (b->t.empty()) continue;
+    if (b->t.front().dims[0] != 1 || b->t.back().dims[2] != 1)
+      throw Error(SPS_ERR_ARGUMENT, "diagonal boundary ends are not trivial");
+    const int len = (int)b->t.size();
+    s.left = join(n, s.left, n.unit(base));
+    s.right = join(n, s.right, n.unit(base + len));
+    for (int k = 0; k < len; ++k) {
+      const int edge = b->edges[k];
+      int owner = -1;
+      for (int i = 0; i < (int)s.ports.size() && owner < 0; ++i)
+        if (std::find(s.ports[i].begin(), s.ports[i].end(), edge) != s.ports[i].end()) owner = i;
+      if (owner < 0) throw Error(SPS_ERR_ARGUMENT, "boundary edge and diagonal strip are disconnected");
+      s.att[owner].push_back(labelled(b->t[k], {base + k, edge, base + k + 1}));
+    }
+    base += len + 1;
+  }
+  for (size_t i = 0; i < s.sites.size(); ++i) {
+    auto inside = n.inside(s.sites[i][0], s.sites[i][1]);
+    for (int j = 0; j < 4; ++j)
+      if (!inside[j]) s.att[i].push_back(n.unit(s.ports[i][j]));
+  }
+  s.max_trunc = std::max(nw.max_trunc, se.max_trunc);
+  return s;
+}
+
+int shared(const LT& a, const LT& b) {
+  int c = 0;
+  for (int k : a.lab) c += index_of(b.lab, k) >= 0;
+  return c;
+}
+
+// _diagonal_attach (diagonal_mps.jl:366-378): the pending tensor sharing the
+// most labels (the first on ties); with none shared, the first unit vector
+LT attach(Net& n, const LT& msg, std::vector<LT>& pending) {
+  int best = 0, score = -1;
+  for (int i = 0; i < (int)pending.size(); ++i) {
+    const int c = shared(msg, pending[i]);
+    if (c > score) {
+      score = c;
+      best = i;
+    }
+  }
+  if (score == 0) {
+    best = -1;
+    for (int i = 0; i < (int)pending.size() && best < 0; ++i)
+      if (pending[i].lab.size() == 1) best = i;
+    if (best < 0) throw Error(SPS_ERR_ARGUMENT, "disconnected diagonal strip attachment");
+  }
+  LT a = pending[best];
+  pending.erase(pending.begin() + best);
+  return join(n, msg, a);
+}
+
+// _diagonal_step (diagonal_mps.jl:380-394)
+LT step(Net& n, LT msg, const Strip& s, int k, const Tensor& A, const Tensor& B, const int* phys = nullptr) {
+  std::vector<LT> pending = s.att[k];
+  const auto& ports = s.ports[k];
+  auto present = [&](const LT& m) {
+    int c = 0;
+    for (int p : ports) c += index_of(m.lab, p) >= 0;
+    return c;
+  };
+  while (present(msg) < 2) {
+    if (pending.empty()) throw Error(SPS_ERR_ARGUMENT, "missing diagonal strip inputs");
+    msg = attach(n, msg, pending);
+  }
+  std::vector<int> inputs;
+  for (int p : ports)
+    if (index_of(msg.lab, p) >= 0) inputs.push_back(p);
+  if (inputs.size() != 2) throw Error(SPS_ERR_ARGUMENT, "diagonal strip step has more than two inputs");
+  msg = apply(n, msg, A, B, ports, inputs, phys);
+  while (!pending.empty()) msg = attach(n, msg, pending);
+  return msg;
+}
+
+// _diagonal_scale: divide by the norm on the device (a step's result owns its buffer)
+LT scaled(Net& n, LT m) {
+  if (m.number) {
+    if (!std::isfinite(m.s)) throw Error(SPS_ERR_NUMERIC, "nonfinite diagonal environment");
+    if (m.s != 0) m.s = m.s > 0 ? 1.0 : -1.0;
+    return m;
+  }
+  safe_scale_inplace(n.E, m.t);
+  m.unit = false;
+  return m;
+}
+
+template <class Site>
+void messages(Net& n, const Strip& s, Site site, int side /*0 both, 1 left, 2 right*/, std::vector<LT>& le,
+              std::vector<LT>& ri) {
+  const int m = (int)s.sites.size();
+  le.assign(m + 1, LT());
+  ri.assign(m + 1, LT());
+  le[0] = s.left;
+  ri[m] = s.right;
+  if (side != 2)
+    for (int k = 0; k < m; ++k) {
+      const Tensor& A = site(s.sites[k][0], s.sites[k][1]);
+      le[k + 1] = scaled(n, step(n, le[k], s, k, A, A));
+    }
+  if (side != 1)
+    for (int k = m - 1; k >= 0; --k) {
+      const Tensor& A = site(s.sites[k][0], s.sites[k][1]);
+      ri[k] = scaled(n, step(n, ri[k + 1], s, k, A, A));
+    }
+}
+
+double value(Net& n, const LT& l, const LT& r) {
+  LT v = join(n, l, r);
+  if (!v.number) throw Error(SPS_ERR_ARGUMENT, "unclosed diagonal network");
+  return v.s;
+}
+
+// _diagonal_hole (diagonal_mps.jl:415-433): the attachments of site k joined
+// to whichever half shares more labels, then the halves; legs in `output` order
+Tensor hole(Net& n, LT left, LT right, const Strip& s, int k, const std::vector<int>& output) {
+  std::vector<LT> pending = s.att[k];
+  while (!pending.empty()) {
+    int li = 0, ri = 0, ls = -1, rs = -1;
+    for (int i = 0; i < (int)pending.size(); ++i) {
+      const int a = shared(left, pending[i]), b = shared(right, pending[i]);
+      if (a > ls) {
+        ls = a;
+        li = i;
+      }
+      if (b > rs) {
+        rs = b;
+        ri = i;
+      }
+    }
+    const bool useleft = ls > rs || (ls == rs && left.lab.size() <= right.lab.size());
+    const int idx = useleft ? li : ri;
+    LT a = pending[idx];
+    pending.erase(pending.begin() + idx);
+    if (useleft) left = join(n, left, a);
+    else right = join(n, right, a);
+  }
+  return contiguous(n.E, reordered(join(n, left, right), output));
+}
+
+struct SiteRef {
+  const State& s;
+  const Tensor& operator()(int x, int y) const { return s.at(x, y); }
+};
+
+}  // namespace
+
+// sample_configuration for the diagonal method (diagonal_born.jl:24-97):
+// sites are drawn layer by layer (even layers by increasing x, odd ones by
+// decreasing x; uniforms[i] is the uniform of the i-th site drawn), each
+// layer inside a strip between the projected northwest boundary and the
+// cached southeast one, then absorbed into the northwest boundary (the
+// physical kind skips the last layer)
+SampleResult sample_diagonal(Engine& E, const SamplingCache& c, const double* uniforms, const int* configuration) {
+  const State& st = *c.state_ref;
+  const int Lx = c.Lx, Ly = c.Ly, L = Lx * Ly, nl = Lx + Ly - 1;
+  const bool physical = c.kind == KIND_PHYSICAL;
+  Net n(E, Lx, Ly);
+  SampleResult res;
+  res.config.assign(L, 0);
+  double maxtr = c.southeast.empty() ? 0.0 : c.southeast[0].max_trunc;
+  res.max_env_trunc = maxtr;
+  if (configuration) {
+    int charge = 0;
+    for (int i = 0; i < L; ++i) {
+      if (configuration[i] != 1 && configuration[i] != 2)
+        throw Error(SPS_ERR_ARGUMENT, "configuration contains an unknown basis label");
+      charge ^= (*st.sites[i].legs[2])[configuration[i] - 1];
+    }
+    if (physical && charge != c.target) {
+      for (int i = 0; i < L; ++i) res.config[i] = configuration[i];
+      res.log_probability = -INFINITY;
+      return res;
+    }
+  }
+  DiagEnv nw;
+  std::vector<Tensor> projected(L);
+  auto proj_site = [&](int x, int y) -> const Tensor& { return projected[x + y * Lx]; };
+  double logp = 0;
+  int prefix = 0, position = 0;
+  for (int t = 0; t < nl; ++t) {
+    Strip s = make_strip(n, t, t, nw, c.southeast[t + 1]);
+    const bool rightward = t % 2 == 0;
+    std::vector<LT> le, ri;
+    messages(n, s, SiteRef{st}, rightward ? 2 : 1, le, ri);
+    LT msg = rightward ? s.left : s.right;
+    const int m = (int)s.sites.size();
+    for (int q = 0; q < m; ++q) {
+      const int k = rightward ? q : m - 1 - q;
+      const int x = s.sites[k][0], y = s.sites[k][1], site = x + y * Lx;
+      const Tensor& A = st.sites[site];
+      const LT& left = rightward ? msg : le[k];
+      const LT& right = rightward ? ri[k + 1] : msg;
+      bool allowed[2] = {true, true};
+      if (physical)
+        for (int j = 0; j < 2; ++j) allowed[j] = position < L - 1 || (prefix ^ (*A.legs[2])[j]) == c.target;
+      if (!allowed[0] && !allowed[1]) throw Error(SPS_ERR_BORN, "sampling prefix violates the total symmetry sector");
+      const auto& kets = c.candidate_kets[site];
+      double p[2];
+      LT next[2];
+      if (physical) {
+        std::vector<int> out(s.ports[k].begin(), s.ports[k].end());
+        Tensor H = hole(n, left, right, s, k, out);
+        for (int i = 3; i >= 0; --i) H = split(E, H, i, {A.legs[VAX[i]], A.legs[VAX[i]]});
+        Tensor root = metric_root(E, H, res);
+        double values[2] = {0, 0};
+        for (int j = 0; j < 2; ++j) {
+          if (!allowed[j]) continue;
+          Tensor u = ein(E, "wnpaes,wnesz->paz", kets[j], root);
+          values[j] = dot(E, u, u);
+        }
+        const double total = values[0] + values[1];
+        if (!std::isfinite(total)) throw Error(SPS_ERR_NUMERIC, "nonfinite proposal weight");
+        if (total == 0) {
+          const int na = (int)allowed[0] + (int)allowed[1];
+          for (int j = 0; j < 2; ++j) p[j] = allowed[j] ? 1.0 / na : 0.0;
+          res.zero_proposals++;
+        } else {
+          for (int j = 0; j < 2; ++j) p[j] = values[j] / total;
+        }
+      } else {
+        double raw[2];
+        for (int j = 0; j < 2; ++j) {
+          next[j] = step(n, left, s, k, kets[j], kets[j]);
+          raw[j] = value(n, next[j], right);
+        }
+        const double scale = std::max(std::fabs(raw[0]), std::fabs(raw[1]));
+        for (double z : raw)
+          if (!(std::isfinite(z) && z >= -64 * DBL_EPSILON * scale))
+            throw Error(SPS_ERR_BORN, "invalid Born conditional at (" + std::to_string(x + 1) + "," +
+                                          std::to_string(y + 1) + "); increase chi_sampling");
+        const double v0 = std::max(raw[0], 0.0), v1 = std::max(raw[1], 0.0), total = v0 + v1;
+        if (!(total > 0))
+          throw Error(SPS_ERR_BORN, "Born conditional has zero total mass at (" + std::to_string(x + 1) + "," +
+                                        std::to_string(y + 1) + ")");
+        p[0] = v0 / total;
+        p[1] = v1 / total;
+      }
+      int j;
+      if (configuration) {
+        j = configuration[site] - 1;
+      } else {
+        std::vector<double> lm{p[0] > 0 ? std::log(p[0]) : -INFINITY, p[1] > 0 ? std::log(p[1]) : -INFINITY};
+        j = categorical(lm, uniforms[position], &res.near_boundary);
+      }
+      res.config[site] = j + 1;
+      res.conditionals.push_back(p[j]);
+      ++position;
+      if (p[j] == 0.0) {
+        res.log_probability = -INFINITY;
+        res.max_env_trunc = maxtr;
+        return res;
+      }
+      logp += std::log(p[j]);
+      projected[site] = kets[j];
+      if (physical) prefix ^= (*A.legs[2])[j];
+      // moving from the left, the chosen candidate's step is the next message
+      msg = scaled(n, (!physical && rightward) ? next[j] : step(n, msg, s, k, kets[j], kets[j]));
+    }
+    if (!physical || t < nl - 1) {
+      absorb_layer(n, nw, proj_site, t, c.method, false, nullptr);
+      maxtr = std::max(maxtr, nw.max_trunc);
+    }
+  }
+  E.check_flag("sample_configuration");
+  res.log_probability = logp;
+  res.max_env_trunc = maxtr;
+  return res;
+}
+
+// measure_energy for the diagonal method (diagonal_energy.jl:12-45): one-site
+// terms in single-layer strips, bonds from layer t to t+1 in two-layer
+// strips (_diagonal_layer_bonds, diagonal_update.jl:54-59; the pair value
+// of diagonal_energy.jl:1-10 steps both sites with the operator kets)
+EnergyResult measure_energy_diagonal(Engine& E, const State& s, const Model& m, const BMPS& method,
+                                     bool record_entropy) {
+  const int Lx = s.Lx, Ly = s.Ly, L = Lx * Ly, nl = Lx + Ly - 1;
+  Net n(E, Lx, Ly);
+  EnergyResult out;
+  out.entropy.profile = record_entropy;
+  out.entropy.Lx = Lx;
+  out.entropy.Ly = Ly;
+  if (record_entropy) {
+    out.entropy.northwest.assign(L, NAN);
+    out.entropy.southeast.assign(L, NAN);
+  }
+  Entropy* ent = record_entropy ? &out.entropy : nullptr;
+  std::vector<DiagEnv> nw(nl + 1), se(nl + 1);
+  SiteRef site{s};
+  for (int t = 0; t < nl; ++t) {
+    nw[t + 1] = nw[t];
+    absorb_layer(n, nw[t + 1], site, t, method, false, ent);
+  }
+  for (int t = nl - 1; t >= 0; --t) {
+    se[t] = se[t + 1];
+    absorb_layer(n, se[t], site, t, method, true, ent);
+  }
+  Par p2 = make_par(1, 1);
+  double xo[4] = {1, 0, 0, -1};
+  Tensor X = E.upload({p2, p2}, xo);
+  Tensor F, G;
+  operator_factors(E, F, G);
+  out.site_x.assign(L, 0.0);
+  double xsum = 0, zzsum = 0;
+  for (int t = 0; t < nl; ++t) {
+    Strip st = make_strip(n, t, t, nw[t], se[t + 1]);
+    std::vector<LT> le, ri;
+    messages(n, st, site, 0, le, ri);
+    for (int k = 0; k < (int)st.sites.size(); ++k) {
+      const int x = st.sites[k][0], y = st.sites[k][1];
+      const Tensor& A = s.at(x, y);
+      const double den = value(n, step(n, le[k], st, k, A, A), ri[k + 1]);
+      Tensor XA = ein(E, "pu,wnuaes->wnpaes", X, A);
+      const double num = value(n, step(n, le[k], st, k, XA, A), ri[k + 1]);
+      const double r = real_ratio(num, den);
+      out.site_x[x + y * Lx] = r;
+      xsum += r;
+    }
+    if (t == nl - 1) continue;
+    Strip pst = make_strip(n, t, t + 1, nw[t], se[t + 2]);
+    messages(n, pst, site, 0, le, ri);
+    for (int dir = 0; dir < 2; ++dir) {
+      const bool horizontal = dir == 0;
+      auto sites = layer_sites(Lx, Ly, t);
+      if (t % 2 == 1) std::reverse(sites.begin(), sites.end());
+      for (auto& a : sites) {
+        const int bx = a[0] + (horizontal ? 1 : 0), by = a[1] + (horizontal ? 0 : 1);
+        if (bx >= Lx || by >= Ly) continue;
+        int ia = -1, ib = -1;
+        for (int k = 0; k < (int)pst.sites.size(); ++k) {
+          if (pst.sites[k] == a) ia = k;
+          if (pst.sites[k][0] == bx && pst.sites[k][1] == by) ib = k;
+        }
+        if (ia < 0 || ib < 0 || std::abs(ia - ib) != 1) throw Error(SPS_ERR_ARGUMENT, "nonadjacent diagonal observable");
+        const Tensor& A = s.at(a[0], a[1]);
+        const Tensor& B = s.at(bx, by);
+        Tensor Cop, Dop;
+        operator_pair(E, A, B, F, G, horizontal, Cop, Dop);
+        auto pair_value = [&](const Tensor& KA, const Tensor& KB) {
+          LT msg = le[std::min(ia, ib)];
+          for (int k = std::min(ia, ib); k <= std::max(ia, ib); ++k) {
+            const bool first = k == ia;
+            msg = step(n, msg, pst, k, first ? KA : KB, first ? A : B);
+          }
+          return value(n, msg, ri[std::max(ia, ib) + 1]);
+        };
+        const double num = pair_value(Cop, Dop);
+        const double den = pair_value(A, B);
+        zzsum += real_ratio(num, den);
+      }
+    }
+  }
+  E.check_flag("measure_energy");
+  const DiagEnv& fin = nw[nl];
+  const double lnv = std::log(positive_real(fin.scalar, "norm")) + fin.log_scale;
+  double hx = m.h * xsum;
+  if (!m.fields.empty()) {
+    hx = 0;
+    for (int i = 0; i < L; ++i) hx += m.fields[i] * out.site_x[i];
+  }
+  out.energy_total = -m.J * zzsum - hx;
+  out.energy_per_site = out.energy_total / L;
+  out.log_norm = lnv + 2 * s.log_amplitude;
+  out.tensor_log_norm = lnv;
+  out.max_env_trunc = std::max(fin.max_trunc, se[0].max_trunc);
+  out.x_sum = xsum;
+  out.zz_sum = zzsum;
+  return out;
+}
+
+}  // namespace sps

@@ -707,6 +707,9 @@ static void sweep(Engine& E, State& s, const Model& m, double delta, int D, cons
 StepReport evolution_step(Engine& E, State& s, const Model& m, double delta, int D, const FUOptions& o,
                           const BMPS& env_method, int order, const int space[2], bool record_entropy,
                           bool force_repair) {
+  if (env_method.diagonal)
+    throw Error(SPS_ERR_ARGUMENT,
+                "the full update takes row boundary-MPS environments; diagonal bond environments are not built");
   StepReport rep;
   double env_err = 0;
   Entropy ent;

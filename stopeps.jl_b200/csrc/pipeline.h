@@ -28,6 +28,9 @@ struct BMPS {        // BoundaryMPS (src/contraction/boundary_mps.jl:11-18)
   int chi = 32;
   int space[2] = {-1, -1};
   bool zipup = false;   // zip-up row absorption (this engine's variant) instead of the exact compression
+  // BoundaryMPSDiagonal (src/contraction/diagonal_mps.jl:3-9): anti-diagonal
+  // layers instead of rows, same chi and sector budget
+  bool diagonal = false;
 };
 
 struct State {       // FiniteState (src/states/finite.jl:27-49)
@@ -49,10 +52,20 @@ struct Entropy {     // BoundaryEntropy (boundary_mps.jl:44-57)
   bool profile = false;
   int Lx = 0, Ly = 0;
   std::vector<double> north, south;   // (Ly-1) x (Lx-1), row-major [row][bond]
+  // diagonal method (diagonal_mps.jl:143-157): per site x + y*Lx, the entropy
+  // of the bond its block split opened, for each sweep direction
+  std::vector<double> northwest, southeast;
   void record(bool south_side, int row, int bond, double v) {
     maximum = std::max(maximum, v);
     if (profile && row >= 1 && row <= Ly - 1) (south_side ? south : north)[(row - 1) * (Lx - 1) + bond - 1] = v;
   }
+};
+
+struct DiagEnv {     // DiagonalBoundary (diagonal_mps.jl:106-118)
+  std::vector<Tensor> t;      // (l, edge, r) per frontier edge, in frontier order
+  std::vector<int> edges;     // the frontier's edge labels
+  double log_scale = 0, max_trunc = 0;
+  double scalar = 1;          // the closed network after the last layer
 };
 
 struct Layer {       // a row entry: plain double layer or SlabColumn (boundary_mps.jl:212-215)
@@ -134,6 +147,7 @@ struct SamplingCache {
   std::vector<std::array<Tensor, 2>> candidates;
   std::vector<std::array<Tensor, 2>> candidate_kets;   // the projected single layers of the candidates
   std::vector<Env> south;
+  std::vector<DiagEnv> southeast;   // diagonal method: se[t] holds the layers from t on
   BMPS method;
   const State* state_ref = nullptr;
 };
@@ -165,5 +179,29 @@ EnergyResult measure_energy(Engine& E, const State& s, const Model& m, const BMP
                             bool record_entropy);
 
 State identity_pepo(Engine& E, int Lx, int Ly);
+
+// helpers shared by the row and diagonal methods (boundary.cu)
+double positive_real(double z, const char* name);
+Tensor project_aux(Engine& E, const Tensor& A, int k);
+Tensor project_physical(Engine& E, const Tensor& A, int k);
+int categorical(const std::vector<double>& lm, double u, int* near);
+// _positive_metric(H; square_root=true) of a site hole H with legs
+// (wk, wb, nk, nb, ek, eb, sk, sb): the eigenvectors on the ket legs scaled by
+// the square roots of the clipped eigenvalues, legs (w, n, e, s, z)
+Tensor metric_root(Engine& E, const Tensor& H, SampleResult& res);
+void operator_factors(Engine& E, Tensor& F, Tensor& G);
+void operator_pair(Engine& E, const Tensor& A, const Tensor& B, const Tensor& F, const Tensor& G, bool horizontal,
+                   Tensor& C, Tensor& D);
+double real_ratio(double a, double b);
+
+// diagonal boundary MPS (diagonal.cu; src/contraction/diagonal_mps.jl,
+// src/sampling/diagonal_born.jl, src/measurement/diagonal_energy.jl)
+LogNorm lognorm_diagonal(Engine& E, const State& s, const BMPS& m);
+void diagonal_southeast(Engine& E, const State& s, const BMPS& m, std::vector<DiagEnv>& se);
+SampleResult sample_diagonal(Engine& E, const SamplingCache& c, const double* uniforms, const int* configuration);
+EnergyResult measure_energy_diagonal(Engine& E, const State& s, const Model& m, const BMPS& method,
+                                     bool record_entropy);
+// the order in which a diagonal draw visits the sites (x + y*Lx), _diagonal_order
+std::vector<int> diagonal_draw_order(int Lx, int Ly);
 
 }  // namespace sps

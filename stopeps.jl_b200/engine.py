@@ -14,7 +14,7 @@ import json
 import numpy as np
 
 from . import _lib
-from .config import BoundaryMPS, BoundaryMPSZipUp, RunConfig, TFIM, FullUpdate, Z2Space
+from .config import BoundaryMPS, BoundaryMPSDiagonal, BoundaryMPSZipUp, RunConfig, TFIM, FullUpdate, Z2Space
 
 
 def _arr(a, ctype):
@@ -28,7 +28,7 @@ def _boundary(m: BoundaryMPS):
         b.space0 = b.space1 = -1
     else:
         b.space0, b.space1 = int(m.sector_space.n0), int(m.sector_space.n1)
-    b.absorption = 1 if isinstance(m, BoundaryMPSZipUp) else 0
+    b.absorption = 2 if isinstance(m, BoundaryMPSDiagonal) else 1 if isinstance(m, BoundaryMPSZipUp) else 0
     return b
 
 
@@ -355,7 +355,8 @@ def measure_energy(state: DeviceState, contraction: BoundaryMPS, site_profile=Fa
     b = _boundary(contraction)
     L = e.Lx * e.Ly
     sx = np.zeros(L)
-    nb = max(0, (e.Ly - 1) * (e.Lx - 1))
+    diagonal = isinstance(contraction, BoundaryMPSDiagonal)
+    nb = L if diagonal else max(0, (e.Ly - 1) * (e.Lx - 1))
     sn = np.zeros(max(nb, 1))
     ss = np.zeros(max(nb, 1))
     e.check(e.lib.sps_measure_energy(e.h, state.id, C.byref(b), C.byref(r), _arr(sx, C.c_double),
@@ -363,7 +364,10 @@ def measure_energy(state: DeviceState, contraction: BoundaryMPS, site_profile=Fa
     out = dict(energy_total=r.energy_total, energy_per_site=r.energy_per_site, log_norm=r.log_norm,
                tensor_log_norm=r.tensor_log_norm, max_environment_truncation=r.max_environment_truncation,
                x_sum=r.x_sum, zz_sum=r.zz_sum, magnetization=r.x_sum / L)
-    if site_profile:
+    if site_profile and diagonal:   # per-site profiles of the two sweeps, [x, y]
+        out["site_x"] = sx.reshape(e.Ly, e.Lx).T.copy()
+        out["Se"] = {"northwest": sn.reshape(e.Ly, e.Lx).T.copy(), "southeast": ss.reshape(e.Ly, e.Lx).T.copy()}
+    elif site_profile:
         out["site_x"] = sx.reshape(e.Ly, e.Lx).T.copy()
         out["Se"] = {"north": sn[:nb].reshape(e.Ly - 1, e.Lx - 1) if nb else np.zeros((0, 0)),
                      "south": ss[:nb].reshape(e.Ly - 1, e.Lx - 1) if nb else np.zeros((0, 0))}

@@ -12,6 +12,16 @@ def pytest_configure(config):
     config.addinivalue_line("markers", "gpu: needs a CUDA device (B200) and the built libstopeps_gpu.so")
 
 
+# Device paths added most recently run after the established parity suite, so
+# that under ``-x`` a failure of theirs is reported without hiding the results
+# of the paths before them.  The order is otherwise unchanged.
+LATE_MODULES = ("test_gpu_site_fields.py", "test_gpu_diagonal.py")
+
+
+def pytest_collection_modifyitems(config, items):
+    items.sort(key=lambda item: os.path.basename(str(item.fspath)) in LATE_MODULES)
+
+
 @pytest.fixture(scope="session")
 def sps():
     import __graft_entry__ as g

@@ -1,0 +1,105 @@
+"""The diagonal boundary MPS on the device (``BoundaryMPSDiagonal``,
+``src/contraction/diagonal_mps.jl``, ``src/sampling/diagonal_born.jl``,
+``src/measurement/diagonal_energy.jl``) against the oracle's restatement
+(``oracle/diagonal.py``, pinned on the CPU to the exact row contraction).
+
+On the stored purified PEPOs (2x3 D=2, 3x3 D=4) with their truncating chi:
+lognorm, the energy, <X> and the per-site <X> to 1e-10; auxiliary draws with
+identical configurations and log-probabilities to 1e-9 (every truncated SVD
+of the diagonal method is the full-spectrum one); the draw's conditionals
+in site order; the physical kind over a projected PEPS likewise; at a chi
+above every bond the device's diagonal values equal its row values.
+"""
+import numpy as np
+import pytest
+
+from util import golden, upload_golden, oracle_state, rel
+
+pytestmark = pytest.mark.gpu
+TOL = 1e-10
+DRAW_TOL = 1e-9
+CASES = ["pepo_2x3_D2.npz", "pepo_3x3_D4.npz"]
+
+
+def _setup(sps, case):
+    from oracle import diagonal as dg
+    g = golden(case)
+    e = sps.Engine(int(g["Lx"]), int(g["Ly"]), sps.TFIM(float(g["J"]), float(g["h"])))
+    st = upload_golden(sps, g, e)
+    chi, a, b = (int(v) for v in g["chi0"])
+    m = sps.BoundaryMPSDiagonal(chi, None if a < 0 else sps.Z2Space(a, b))
+    om = dg.BoundaryMPSDiagonal(chi, None if a < 0 else (a, b))
+    return g, e, st, m, oracle_state(g), om
+
+
+@pytest.mark.parametrize("case", CASES)
+def test_diagonal_lognorm_and_energy(sps, case):
+    from oracle import diagonal as dg, model as md
+    g, e, st, m, ost, om = _setup(sps, case)
+    ln, oln = sps.lognorm(st, m), dg.lognorm(ost, om)
+    assert rel(ln["log_norm"], oln["log_norm"]) < TOL
+    assert abs(ln["max_environment_truncation"] - oln["max_environment_truncation"]) < 1e-12
+    en = sps.measure_energy(st, m, site_profile=True)
+    oe = dg.measure_energy(ost, md.TFIM(float(g["J"]), float(g["h"])), om)
+    for k in ("energy_per_site", "log_norm", "x_sum", "zz_sum"):
+        assert rel(en[k], oe[k]) < TOL, (k, en[k], oe[k])
+    np.testing.assert_allclose(en["site_x"], oe["site_x"], atol=TOL)
+
+
+@pytest.mark.parametrize("case", CASES)
+def test_diagonal_draws(sps, case):
+    from oracle import diagonal as dg
+    g, e, st, m, ost, om = _setup(sps, case)
+    cache = sps.SamplingCache(st, m)
+    ocache = dg.DiagonalSamplingCache(ost, om)
+    Lx, Ly = int(g["Lx"]), int(g["Ly"])
+    order = dg.draw_order(Lx, Ly)
+    for u in g["uniforms"][:3]:
+        d = sps.sample_conditionals(cache, uniforms=u)
+        od = dg.sample_configuration(ocache, uniforms=u)
+        np.testing.assert_array_equal(d["configuration"], np.asarray(od["configuration"]))
+        again = sps.sample_configuration(cache, configuration=d["configuration"])
+        assert rel(again["log_probability"], od["log_probability"]) < DRAW_TOL
+        for i, (x, y) in enumerate(order):   # conditionals come back in site order
+            assert abs(d["conditionals"][x, y] - od["conditionals"][i]) < DRAW_TOL
+
+
+def test_diagonal_physical_draws(sps):
+    from oracle import diagonal as dg, sampling as osp
+    g, e, st, m, ost, om = _setup(sps, "pepo_3x3_D4.npz")
+    cfg = np.asarray(g["configs"][0])
+    ps, _ = sps.project_configuration(st, cfg)
+    ops, _ = osp.project_configuration(ost, cfg.tolist())
+    cache = sps.SamplingCache(ps, m, kind="physical")
+    ocache = dg.DiagonalSamplingCache(ops, om, kind="physical")
+    for seed in range(2):
+        u = np.random.default_rng([17, seed]).random(9)
+        d = sps.sample_configuration(cache, uniforms=u)
+        od = dg.sample_configuration(ocache, uniforms=u)
+        np.testing.assert_array_equal(d["configuration"], np.asarray(od["configuration"]))
+        assert rel(d["log_probability"], od["log_probability"]) < DRAW_TOL
+        zero = sum(1 for r in od["repairs"] if r.get("reason") == "zero_proposal_weights")
+        assert d["zero_proposals"] == zero
+
+
+def test_diagonal_exact_chi_equals_row_contraction(sps):
+    """2x3 D=2 at chi = 64 (above every bond): both device contractions are exact."""
+    g = golden("pepo_2x3_D2.npz")
+    e = sps.Engine(2, 3, sps.TFIM(float(g["J"]), float(g["h"])))
+    st = upload_golden(sps, g, e)
+    a = sps.measure_energy(st, sps.BoundaryMPS(64))
+    b = sps.measure_energy(st, sps.BoundaryMPSDiagonal(64))
+    for k in ("energy_per_site", "log_norm", "x_sum"):
+        assert rel(a[k], b[k]) < 1e-12, k
+    ca, cb = sps.SamplingCache(st, sps.BoundaryMPS(64)), sps.SamplingCache(st, sps.BoundaryMPSDiagonal(64))
+    cfgs = np.stack([np.asarray(c) for c in g["configs"][:3]])
+    la, _ = sps.sample_probability_batch(ca, cfgs)
+    lb, _ = sps.sample_probability_batch(cb, cfgs)
+    np.testing.assert_allclose(lb, la, rtol=1e-12)
+
+
+def test_diagonal_environment_is_refused_by_the_full_update(sps):
+    g, e, st, m, ost, om = _setup(sps, "pepo_2x3_D2.npz")
+    ps, _ = sps.project_configuration(st, np.asarray(g["configs"][0]))
+    with pytest.raises(sps._lib.EngineError):
+        sps.evolution_step(ps, 0.01, 2, m)
