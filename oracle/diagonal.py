@@ -716,3 +716,119 @@ def measure_energy(state, model, method: BoundaryMPSDiagonal, record_entropy=Fal
                 Se=(entropy.Se if entropy is not None else None),
                 max_boundary_entropy=(entropy.maximum if entropy is not None else math.nan),
                 x_sum=xsum, magnetization=xsum / (Lx * Ly), site_x=site_x, zz_sum=zzsum)
+
+
+# ---------------------------------------------------------------------------
+# full-update bond environments (src/evolution/diagonal_update.jl)
+# ---------------------------------------------------------------------------
+
+def external_axes(direction):
+    """``_diagonal_external_axes``: the exterior virtual legs of the bond's two
+    sites, in the order of the reduced pair's Q factors."""
+    return ((0, 1, 5), (1, 4, 5)) if direction == "horizontal" else ((0, 1, 4), (0, 4, 5))
+
+
+@dataclass
+class DiagonalBondEnvironment:
+    """``DiagonalBondEnvironment`` (diagonal_update.jl:1-20)."""
+    strip: Strip
+    left: LT
+    right: LT
+    positions: tuple
+    first: tuple
+    second: tuple
+    direction: str
+    outer: tuple   # parities of the six exterior legs
+
+
+def bond_environment(state, strip, left, right, i, j, direction):
+    """``_diagonal_bond_environment`` (diagonal_update.jl:13-20)."""
+    a, b = strip.sites.index(i), strip.sites.index(j)
+    if abs(a - b) != 1:
+        raise RuntimeError("bond sites must be adjacent in a diagonal strip")
+    ax = external_axes(direction)
+    outer = tuple(state[i[0], i[1]].p[k] for k in ax[0]) + tuple(state[j[0], j[1]].p[k] for k in ax[1])
+    return DiagonalBondEnvironment(strip, left, right, (min(a, b), max(a, b)), i, j, direction, outer)
+
+
+def bond_hole(env: DiagonalBondEnvironment) -> T:
+    """``bond_hole`` (diagonal_update.jl:21-29): the six exterior double legs of
+    the bond, each split (ket, bra), in the layout of ``boundary.bond_hole``."""
+    ax = external_axes(env.direction)
+    ports = [ports_of(env.first), ports_of(env.second)]
+    output = [ports[k][VIRTUAL_AXES.index(a)] for k in (0, 1) for a in ax[k]]
+    H = hole(env.left, env.right, env.strip, list(range(env.positions[0], env.positions[1] + 1)), output)
+    for k in range(5, -1, -1):
+        H = z2.split(H, k, [env.outer[k], env.outer[k]])
+    return H
+
+
+def core_site(Q: T, direction, first) -> T:
+    """``_diagonal_core_site`` (diagonal_update.jl:32-38): a reduced factor Q
+    (three exterior legs, auxiliary, core) as a site tensor whose physical leg
+    is the core leg and whose bond leg is trivial."""
+    ax = external_axes(direction)[0 if first else 1]
+    missing = [a for a in VIRTUAL_AXES if a not in ax][0]
+    site = join(LT(Q, list(ax) + [3, 2]), unit_lt(missing))
+    return reorder(site, [0, 1, 2, 3, 4, 5]).t
+
+
+def reduced_metric(env: DiagonalBondEnvironment, Qa: T, Qb: T) -> T:
+    """``_reduced_metric(::DiagonalBondEnvironment)`` (diagonal_update.jl:39-52):
+    each core site closed against its own half of the strip, the open core
+    pairs joined; legs (rb, sb, rk, sk) as ``full_update.reduced_metric``."""
+    A = core_site(Qa, env.direction, True)
+    B = core_site(Qb, env.direction, False)
+
+    def absorb(message, k):
+        isfirst = env.strip.sites[k] == env.first
+        return step(message, env.strip, k, A if isfirst else B,
+                    physical=(("core", "ka"), ("core", "ba")) if isfirst else (("core", "kb"), ("core", "bb")))
+
+    left = absorb(env.left, env.positions[0])
+    right = absorb(env.right, env.positions[1])
+    return reorder(join(left, right), [("core", "ba"), ("core", "bb"), ("core", "ka"), ("core", "kb")]).t
+
+
+def sweep(state, model, delta, D, method, contraction: BoundaryMPSDiagonal, direction, reverse, space=None,
+          entropy=None, force_repair_bonds=()):
+    """``_sweep!`` for the diagonal method (diagonal_update.jl:61-102): the
+    bonds from layer t to t+1 are updated in a strip of the two layers
+    between the rolling boundary of the updated layers and the cached one of
+    the others; the rolling boundary then absorbs the finished layer."""
+    from . import full_update as fu
+    from .model import trotter_gate
+    Lx, Ly = state.Lx, state.Ly
+    nl = layer_count(Lx, Ly)
+    nw, se = boundaries(state, contraction, side="northwest" if reverse else "southeast", entropy=entropy)
+    fixed = nw[1:nl + 1] if reverse else se[0:nl - 1]
+    env_err = max([e.max_truncation for e in fixed], default=0.0)
+    rolling = DiagonalBoundary()
+    records = []
+    at = lambda s: state[s[0], s[1]]
+    for t in (range(nl - 2, -1, -1) if reverse else range(nl - 1)):
+        strip = Strip(state, t, t + 1, nw[t] if reverse else rolling, rolling if reverse else se[t + 2])
+        order = draw_sites(Lx, Ly, t, reverse)
+        rightward = (not reverse) if len(order) < 2 else order[0][0] < order[-1][0]
+        le, ri = messages(state, strip, side="right" if rightward else "left")
+        message = strip.left if rightward else strip.right
+        n = len(strip.sites)
+        cursor = 0 if rightward else n - 1
+        for i, j in layer_bonds(Lx, Ly, t, direction, reverse):
+            a, b = sorted([strip.sites.index(i), strip.sites.index(j)])
+            while (cursor < a) if rightward else (cursor > b):
+                message = scale(step(message, strip, cursor, at(strip.sites[cursor])))
+                cursor += 1 if rightward else -1
+            left = message if rightward else le[a]
+            right = ri[b + 1] if rightward else message
+            env = bond_environment(state, strip, left, right, i, j, direction)
+            gate = trotter_gate(model, Lx, Ly, i, j, delta)
+            records.append(fu.update_bond(state, i, j, gate, D, method, env, direction,
+                                          boundary_error=strip.max_truncation, space=space,
+                                          force_repair=(i, j) in force_repair_bonds))
+            for k in (range(a, b + 1) if rightward else range(b, a - 1, -1)):
+                message = scale(step(message, strip, k, at(strip.sites[k])))
+            cursor = b + 1 if rightward else a - 1
+        absorb_layer(rolling, at, Lx, Ly, t + 1 if reverse else t, contraction, reverse=reverse, entropy=entropy)
+        env_err = max(env_err, rolling.max_truncation)
+    return records, env_err

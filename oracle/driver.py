@@ -17,6 +17,7 @@ import numpy as np
 from .z2 import EPS
 from . import boundary as bm
 from . import full_update as fu
+from . import diagonal as dg
 from . import sampling as sp
 from .model import TFIM, identity_pepo, normalize_state
 
@@ -49,6 +50,7 @@ class RunConfig:
     record_boundary_entropy: bool = True
     Ns: int = 16
     seed: int = 20260924
+    diagonal: bool = False   # contraction = BoundaryMPSDiagonal (src/contraction/diagonal_mps.jl)
 
     def boundary(self, role):
         chi = getattr(self, "chi_" + role)
@@ -57,7 +59,7 @@ class RunConfig:
         sp_ = getattr(self, role + "_space")
         if sp_ is None:
             sp_ = self.environment_space
-        return bm.BoundaryMPS(chi, sp_)
+        return dg.BoundaryMPSDiagonal(chi, sp_) if self.diagonal else bm.BoundaryMPS(chi, sp_)
 
 
 def sample_uniforms(seed: int, index: int, n: int) -> np.ndarray:
@@ -103,9 +105,9 @@ def step_schedule(start, target, dtau):
 def observe(state, c, energy):
     """``_observe`` (``particles.jl:35-40``)."""
     if energy:
-        return sp.measure_energy(state, TFIM(c.J, c.h, c.fields), c.boundary("measurement"),
-                                 record_entropy=c.record_boundary_entropy)
-    m = bm.lognorm(state, c.boundary("measurement"))
+        return (dg if c.diagonal else sp).measure_energy(state, TFIM(c.J, c.h, c.fields), c.boundary("measurement"),
+                                                         record_entropy=c.record_boundary_entropy)
+    m = (dg if c.diagonal else bm).lognorm(state, c.boundary("measurement"))
     m.update(energy_total=math.nan, energy_per_site=math.nan, magnetization=math.nan)
     return m
 
@@ -184,8 +186,12 @@ def run_stochastic(c: RunConfig, checkpoint, uniforms_fn=None):
     """
     if uniforms_fn is None:
         uniforms_fn = lambda i: sample_uniforms(c.seed, i, c.Lx * c.Ly)
-    cache = sp.SamplingCache(checkpoint, c.boundary("sampling"))
-    draws = [sp.sample_configuration(cache, uniforms=uniforms_fn(i)) for i in range(1, c.Ns + 1)]
+    if c.diagonal:
+        cache = dg.DiagonalSamplingCache(checkpoint, c.boundary("sampling"))
+        draws = [dg.sample_configuration(cache, uniforms=uniforms_fn(i)) for i in range(1, c.Ns + 1)]
+    else:
+        cache = sp.SamplingCache(checkpoint, c.boundary("sampling"))
+        draws = [sp.sample_configuration(cache, uniforms=uniforms_fn(i)) for i in range(1, c.Ns + 1)]
     grouping = sp.group_configurations([d["configuration"] for d in draws])
     particles = []
     for u, i in enumerate(grouping["first_draw"]):

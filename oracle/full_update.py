@@ -192,7 +192,11 @@ def reduced_layer(Q):
 
 
 def reduced_metric(env, Qa, Qb):
-    """``_reduced_metric(::BondEnvironment,...)`` (``full_update.jl:151-172``)."""
+    """``_reduced_metric(::BondEnvironment,...)`` (``full_update.jl:151-172``);
+    a diagonal bond environment takes ``diagonal.reduced_metric``."""
+    from . import diagonal as dg
+    if isinstance(env, dg.DiagonalBondEnvironment):
+        return dg.reduced_metric(env, Qa, Qb)
     A = reduced_layer(Qa)
     B = reduced_layer(Qb)
     left, right = env.left, env.right
@@ -224,7 +228,9 @@ def positive_reduced_metric(env, Qa, Qb):
     two-leg basis to save memory; the positive projection is basis
     independent, so the result agrees to roundoff.
     """
-    H = bm.bond_hole(env)           # legs (k1,b1,k2,b2,...,k6,b6)
+    from . import diagonal as dg
+    H = dg.bond_hole(env) if isinstance(env, dg.DiagonalBondEnvironment) else bm.bond_hole(env)
+    # legs (k1,b1,k2,b2,...,k6,b6)
     kets = [0, 2, 4, 6, 8, 10]
     bras = [1, 3, 5, 7, 9, 11]
     if not np.all(np.isfinite(H.a)):
@@ -508,9 +514,13 @@ def sweep(state, model, delta, D, method, contraction, direction, reverse, space
 def evolution_step(state, model: TFIM, delta, D, method: FullUpdate, contraction, order=2,
                    space=None, record_entropy=False, force_repair_bonds=()):
     """``evolution_step!`` (``full_update.jl:559-597``)."""
+    from . import diagonal as dg
+    diagonal = isinstance(contraction, dg.BoundaryMPSDiagonal)
     records = []
     env_err = 0.0
-    entropy = bm.Entropy() if record_entropy else None
+    entropy = None
+    if record_entropy:
+        entropy = dg.DiagonalEntropy(state.Lx, state.Ly) if diagonal else bm.Entropy()
     gate_delta = delta / 2 if order == 2 else delta
     sweeps = ([("horizontal", False), ("vertical", False), ("vertical", True), ("horizontal", True)]
               if order == 2 else [("horizontal", False), ("vertical", False)])
@@ -522,8 +532,9 @@ def evolution_step(state, model: TFIM, delta, D, method: FullUpdate, contraction
                 continue
             if direction == "vertical" and state.Ly < 2:
                 continue
-            r, e = sweep(state, model, gate_delta, D, method, contraction, direction, rev, space=space,
-                         entropy=entropy, force_repair_bonds=force_repair_bonds)
+            r, e = (dg.sweep if diagonal else sweep)(state, model, gate_delta, D, method, contraction, direction,
+                                                      rev, space=space, entropy=entropy,
+                                                      force_repair_bonds=force_repair_bonds)
             records.extend(r)
             env_err = max(env_err, e)
     state.beta += 2 * delta

@@ -126,3 +126,67 @@ def test_sector_budget_and_fields():
             for leg in (0, 2):
                 n0, n1 = A.sector_dims(leg)
                 assert n0 <= 2 and n1 <= 2
+
+
+def test_bond_environment_equals_row_environment():
+    """``diagonal_update.jl``'s bond environments at exact chi: on every bond of
+    a 3x3 D=3 PEPO the reduced metric and the bond hole equal the row
+    method's up to the environments' overall scale."""
+    from oracle import full_update as fu
+    st = _state(3, 3, D=3)
+    m = md.TFIM(1.0, 0.9)
+    nw, se = dg.boundaries(st, dg.BoundaryMPSDiagonal(400))
+    layers = bm.row_layers(st)
+    north, south, _ = bm.boundary_environments(layers, bm.BoundaryMPS(400))
+    seen = 0
+    for t in range(dg.layer_count(3, 3) - 1):
+        strip = dg.Strip(st, t, t + 1, nw[t], se[t + 2])
+        le, ri = dg.messages(st, strip)
+        for direction in ("horizontal", "vertical"):
+            for i, j in dg.layer_bonds(3, 3, t, direction):
+                a, b = sorted([strip.sites.index(i), strip.sites.index(j)])
+                denv = dg.bond_environment(st, strip, le[a], ri[b + 1], i, j, direction)
+                renv = bm.bond_environment(st, layers, north, south, i, j, direction)
+                pair = fu.reduced_pair(st[i], st[j], md.trotter_gate(m, 3, 3, i, j, 0.05), direction)
+                for x, y in ((fu.reduced_metric(renv, pair["Qa"], pair["Qb"]),
+                              fu.reduced_metric(denv, pair["Qa"], pair["Qb"])),
+                             (bm.bond_hole(renv), dg.bond_hole(denv))):
+                    np.testing.assert_allclose(y.a / np.abs(y.a).max(), x.a / np.abs(x.a).max(), atol=1e-13)
+                seen += 1
+    assert seen == 12
+
+
+@pytest.mark.parametrize("Lx,Ly", [(3, 3), (2, 3)])
+def test_full_update_step_without_truncation_equals_row(Lx, Ly):
+    """One second-order step from beta = 0 at D = 4 truncates nothing, so the
+    diagonal and row environments give the same state: the same lnZ and energy."""
+    from oracle import full_update as fu
+    m = md.TFIM(1.0, 0.9)
+    out = []
+    for method in (bm.BoundaryMPS(400), dg.BoundaryMPSDiagonal(400)):
+        st = md.identity_pepo(Lx, Ly)
+        md.normalize_state(st)
+        r = fu.evolution_step(st, m, 0.05, 4, fu.FullUpdate(), method, record_entropy=True)
+        assert r["bond_updates"] == 2 * ((Lx - 1) * Ly + Lx * (Ly - 1))
+        e = sp.measure_energy(st, m, bm.BoundaryMPS(400))
+        out.append((e["log_norm"], e["energy_per_site"]))
+    assert abs(out[0][0] - out[1][0]) < 1e-12 and abs(out[0][1] - out[1][1]) < 1e-12
+
+
+@pytest.mark.parametrize("h", [0.7, 3.0])
+def test_purification_with_diagonal_environments_matches_exact_diagonalization(h):
+    """``RunConfig(contraction=BoundaryMPSDiagonal)``: the purification (full
+    update and measurement on diagonal boundaries) is within the Trotter error
+    of exact diagonalisation and equals the row method's run to 1e-10."""
+    out = []
+    for diagonal in (False, True):
+        c = dr.RunConfig(Lx=3, Ly=2, J=1.0, h=h, beta0=0.2, beta_log=[0.1, 0.2], beta_measure=[0.0, 0.2],
+                         delta_tau_pur=0.025, D_pur=4, D_peps=4, chi_environment=16, Ns=4, seed=1,
+                         diagonal=diagonal)
+        out.append(dr.run_purification(c)[1][-1])
+    ex = md.exact_thermal_observables(3, 2, md.TFIM(1.0, h), out[1]["beta"])
+    tol = 2e-5 * max(1.0, h * h)
+    assert abs(out[1]["lnZ"] - ex["lnZ"]) < tol
+    assert abs(out[1]["energy_per_site"] - ex["energy_per_site"]) < tol
+    assert abs(out[0]["lnZ"] - out[1]["lnZ"]) < 1e-10
+    assert abs(out[0]["energy_per_site"] - out[1]["energy_per_site"]) < 1e-10
