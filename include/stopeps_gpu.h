@@ -60,7 +60,8 @@ typedef struct sps_config {
  * has no counterpart in the reference; 2 is BoundaryMPSDiagonal
  * (src/contraction/diagonal_mps.jl: anti-diagonal layers, site blocks,
  * truncation of the bonds a block opens), taken by sps_lognorm,
- * sps_measure_energy and the sampling caches, not by the full update. */
+ * sps_measure_energy, the sampling caches and, for its bond environments,
+ * the full update (src/evolution/diagonal_update.jl). */
 typedef struct sps_boundary {
   int32_t chi;
   int32_t space0, space1;

@@ -100,8 +100,9 @@ class BoundaryMPSZipUp(BoundaryMPS):
 class BoundaryMPSDiagonal(BoundaryMPS):
     """``BoundaryMPSDiagonal(chi, sector_space)`` (``src/contraction/diagonal_mps.jl:3-9``):
     anti-diagonal layers x + y = t absorbed as site blocks, with the same ``chi``
-    and sector budget.  Taken by ``lognorm``, ``measure_energy`` and
-    ``SamplingCache``; the full update's bond environments stay row-based."""
+    and sector budget.  Taken by ``lognorm``, ``measure_energy``,
+    ``SamplingCache`` and the full update's bond environments
+    (``src/evolution/diagonal_update.jl``); ``RunConfig(contraction=...)``."""
 
 
 @dataclass(frozen=True)
@@ -201,8 +202,9 @@ def temperature_nodes(c: RunConfig):
 
 def validate_config(c: RunConfig) -> RunConfig:
     """``validate_config`` (``config.jl:80-114``) for the row boundary-MPS path."""
-    if c.contraction is not BoundaryMPS:
-        raise ValueError("this engine implements the row boundary-MPS contraction (BoundaryMPS/BoundaryMPSRow)")
+    if c.contraction not in (BoundaryMPS, BoundaryMPSDiagonal):
+        raise ValueError("this engine implements the row and diagonal boundary-MPS contractions "
+                         "(BoundaryMPS/BoundaryMPSRow, BoundaryMPSDiagonal)")
     grid = [c.beta0] + list(c.beta_log) + list(c.beta_measure)
     if not all(math.isfinite(b) and b >= 0 for b in grid):
         raise ValueError("invalid beta grid")
@@ -240,6 +242,17 @@ def validate_config(c: RunConfig) -> RunConfig:
     return c
 
 
+def diagonal_order(Lx, Ly):
+    """``_diagonal_order`` (``src/contraction/diagonal_mps.jl:111``): the 0-based sites
+    (x, y) by anti-diagonals x + y = 0, 1, ..., even ones by increasing x, odd
+    ones by decreasing x; the order in which a diagonal draw visits them."""
+    out = []
+    for t in range(Lx + Ly - 1):
+        layer = [(x, t - x) for x in range(max(0, t - Ly + 1), min(Lx - 1, t) + 1)]
+        out.extend(reversed(layer) if t % 2 else layer)
+    return out
+
+
 def parameter_dict(c: RunConfig) -> dict:
     """Plain-container encoding of the configuration (``config.jl:117-185``, subset)."""
     def enc(x):
@@ -259,9 +272,13 @@ def parameter_dict(c: RunConfig) -> dict:
             return d
         return repr(x)
     d = {f.name: enc(getattr(c, f.name)) for f in fields(c)}
-    d["contraction"] = "BoundaryMPS-Row"
-    d["sampling_site_order"] = [(x + 1, y + 1) for y in range(c.lattice.Ly) for x in range(c.lattice.Lx)]
-    d["contraction_order"] = "row_major"
+    diagonal = c.contraction is BoundaryMPSDiagonal
+    d["contraction"] = "BoundaryMPS-Diagonal" if diagonal else "BoundaryMPS-Row"
+    d["sampling_site_order"] = (
+        [(x + 1, y + 1) for x, y in diagonal_order(c.lattice.Lx, c.lattice.Ly)] if diagonal
+        else [(x + 1, y + 1) for y in range(c.lattice.Ly) for x in range(c.lattice.Lx)])
+    d["contraction_order"] = ("x+y_ascending; even_diagonal_x_ascending; odd_diagonal_x_descending" if diagonal
+                              else "row_major")
     d["state_truncation_metric"] = "relative_squared_FU_residual"
     d["full_update_algorithm"] = "environment_gauge_SVD_ALS"
     d["full_update_algorithm_revision"] = 2

@@ -596,10 +596,13 @@ double value(Net& n, const LT& l, const LT& r) {
   return v.s;
 }
 
-// _diagonal_hole (diagonal_mps.jl:415-433): the attachments of site k joined
-// to whichever half shares more labels, then the halves; legs in `output` order
-Tensor hole(Net& n, LT left, LT right, const Strip& s, int k, const std::vector<int>& output) {
-  std::vector<LT> pending = s.att[k];
+// _diagonal_hole (diagonal_mps.jl:415-433): the attachments of the given
+// sites joined to whichever half shares more labels, then the halves; legs
+// in `output` order
+Tensor hole(Net& n, LT left, LT right, const Strip& s, const std::vector<int>& positions,
+            const std::vector<int>& output) {
+  std::vector<LT> pending;
+  for (int k : positions) pending.insert(pending.end(), s.att[k].begin(), s.att[k].end());
   while (!pending.empty()) {
     int li = 0, ri = 0, ls = -1, rs = -1;
     for (int i = 0; i < (int)pending.size(); ++i) {
@@ -685,7 +688,7 @@ SampleResult sample_diagonal(Engine& E, const SamplingCache& c, const double* un
       LT next[2];
       if (physical) {
         std::vector<int> out(s.ports[k].begin(), s.ports[k].end());
-        Tensor H = hole(n, left, right, s, k, out);
+        Tensor H = hole(n, left, right, s, {k}, out);
         for (int i = 3; i >= 0; --i) H = split(E, H, i, {A.legs[VAX[i]], A.legs[VAX[i]]});
         Tensor root = metric_root(E, H, res);
         double values[2] = {0, 0};
@@ -851,6 +854,160 @@ EnergyResult measure_energy_diagonal(Engine& E, const State& s, const Model& m, 
   out.x_sum = xsum;
   out.zz_sum = zzsum;
   return out;
+}
+
+}  // namespace sps
+
+// ---------------------------------------------------------------------------
+// full-update bond environments on diagonal boundaries
+// (src/evolution/diagonal_update.jl)
+// ---------------------------------------------------------------------------
+namespace sps {
+namespace {
+
+// _diagonal_external_axes (diagonal_update.jl:12): the exterior legs of the
+// bond's two sites, in the order of the reduced pair's Q factors
+const int EXT_H[2][3] = {{0, 1, 5}, {1, 4, 5}}, EXT_V[2][3] = {{0, 1, 4}, {0, 4, 5}};
+const int KA = -31, BA = -32, KB = -33, BB = -34;   // open core legs (ket, bra) of the two sites
+
+std::vector<std::array<int, 2>> draw_sites(int Lx, int Ly, int t, bool reverse) {
+  auto s = layer_sites(Lx, Ly, t);
+  if ((t % 2 == 1) != reverse) std::reverse(s.begin(), s.end());
+  return s;
+}
+
+// _diagonal_core_site (diagonal_update.jl:32-38): Q (three exterior legs,
+// auxiliary, core) as a site tensor (w, n, p, a, e, s) whose physical leg is
+// the core leg and whose bond leg is trivial
+Tensor core_site(Net& n, const Tensor& Q, bool horizontal, bool first) {
+  const int* ax = (horizontal ? EXT_H : EXT_V)[first ? 0 : 1];
+  int missing = -1;
+  for (int v : VAX)
+    if (v != ax[0] && v != ax[1] && v != ax[2]) missing = v;
+  Tensor t = with_trivial(Q, 1, false, n.triv);   // (x1, x2, x3, aux, core, trivial)
+  std::vector<int> order(6);
+  for (int i = 0; i < 3; ++i) order[ax[i]] = i;
+  order[2] = 4;
+  order[3] = 3;
+  order[missing] = 5;
+  return contiguous(n.E, perm_view(t, order));
+}
+
+struct DiagBond {   // DiagonalBondEnvironment (diagonal_update.jl:1-20)
+  const Strip* strip;
+  const LT* left;
+  const LT* right;
+  int a, b;                      // strip positions of the bond's sites, a < b
+  std::array<int, 2> first, second;
+  bool horizontal;
+};
+
+// _reduced_metric(::DiagonalBondEnvironment) (diagonal_update.jl:39-52): each
+// core site closed against its own half, the open core pairs joined;
+// N[rb, sb, rk, sk]
+Tensor diag_metric(Net& n, const DiagBond& d, const Tensor& Qa, const Tensor& Qb) {
+  Tensor A = core_site(n, Qa, d.horizontal, true), B = core_site(n, Qb, d.horizontal, false);
+  auto absorb = [&](const LT& msg, int k) {
+    const bool isfirst = d.strip->sites[k] == d.first;
+    const int phys[2] = {isfirst ? KA : KB, isfirst ? BA : BB};
+    const Tensor& C = isfirst ? A : B;
+    return step(n, msg, *d.strip, k, C, C, phys);
+  };
+  LT l = absorb(*d.left, d.a), r = absorb(*d.right, d.b);
+  return contiguous(n.E, reordered(join(n, l, r), {BA, BB, KA, KB}));
+}
+
+// bond_hole(::DiagonalBondEnvironment) (diagonal_update.jl:21-29): the six
+// exterior double legs, each split (ket, bra)
+Tensor diag_bond_hole(Net& n, const DiagBond& d, const State& st) {
+  const auto& ax = d.horizontal ? EXT_H : EXT_V;
+  std::vector<int> output;
+  std::vector<Par> outer;
+  for (int k = 0; k < 2; ++k) {
+    const auto& site = k == 0 ? d.first : d.second;
+    auto ports = n.ports(site[0], site[1]);
+    for (int i = 0; i < 3; ++i) {
+      const int axis = ax[k][i];
+      output.push_back(ports[std::find(VAX, VAX + 4, axis) - VAX]);
+      outer.push_back(st.at(site[0], site[1]).legs[axis]);
+    }
+  }
+  Tensor H = hole(n, *d.left, *d.right, *d.strip, {d.a, d.b}, output);
+  for (int k = 5; k >= 0; --k) H = split(n.E, H, k, {outer[k], outer[k]});
+  return H;
+}
+
+}  // namespace
+
+// _sweep! on diagonal boundaries (diagonal_update.jl:61-102): the bonds from
+// layer t to t+1 are updated inside a strip of the two layers between the
+// rolling boundary of the finished layers and the cached boundary of the
+// others; the rolling boundary then absorbs the finished layer
+void sweep_diagonal(Engine& E, State& s, const Model& m, double delta, int D, const FUOptions& o,
+                    const BMPS& method, bool horizontal, bool reverse, const int space[2], Entropy* ent,
+                    StepReport& rep, double& env_err, bool force_repair) {
+  const int Lx = s.Lx, Ly = s.Ly, nl = Lx + Ly - 1;
+  Net n(E, Lx, Ly);
+  SiteRef site{s};
+  std::vector<DiagEnv> nw(nl + 1), se(nl + 1);
+  if (reverse) {
+    for (int t = 0; t < nl; ++t) {
+      nw[t + 1] = nw[t];
+      absorb_layer(n, nw[t + 1], site, t, method, false, ent);
+      env_err = std::max(env_err, nw[t + 1].max_trunc);
+    }
+  } else {
+    for (int t = nl - 1; t >= 0; --t) {
+      se[t] = se[t + 1];
+      absorb_layer(n, se[t], site, t, method, true, ent);
+      if (t <= nl - 2) env_err = std::max(env_err, se[t].max_trunc);
+    }
+  }
+  DiagEnv rolling;
+  for (int q = 0; q + 1 < nl; ++q) {
+    const int t = reverse ? nl - 2 - q : q;
+    Strip st = make_strip(n, t, t + 1, reverse ? nw[t] : rolling, reverse ? rolling : se[t + 2]);
+    auto order = draw_sites(Lx, Ly, t, reverse);
+    const bool rightward = order.size() < 2 ? !reverse : order.front()[0] < order.back()[0];
+    std::vector<LT> le, ri;
+    messages(n, st, site, rightward ? 2 : 1, le, ri);
+    LT msg = rightward ? st.left : st.right;
+    const int ns = (int)st.sites.size();
+    int cursor = rightward ? 0 : ns - 1;
+    for (const auto& i : order) {   // _diagonal_layer_bonds(l, t, direction; reverse)
+      const std::array<int, 2> j{i[0] + (horizontal ? 1 : 0), i[1] + (horizontal ? 0 : 1)};
+      if (j[0] >= Lx || j[1] >= Ly) continue;
+      int pi = -1, pj = -1;
+      for (int k = 0; k < ns; ++k) {
+        if (st.sites[k] == i) pi = k;
+        if (st.sites[k] == j) pj = k;
+      }
+      if (pi < 0 || pj < 0 || std::abs(pi - pj) != 1)
+        throw Error(SPS_ERR_ARGUMENT, "bond sites must be adjacent in a diagonal strip");
+      const int a = std::min(pi, pj), b = std::max(pi, pj);
+      while (rightward ? cursor < a : cursor > b) {
+        const Tensor& A = s.at(st.sites[cursor][0], st.sites[cursor][1]);
+        msg = scaled(n, step(n, msg, st, cursor, A, A));
+        cursor += rightward ? 1 : -1;
+      }
+      DiagBond d{&st, rightward ? &msg : &le[a], rightward ? &ri[b + 1] : &msg, a, b, i, j, horizontal};
+      PairEnv env;
+      env.horizontal = horizontal;
+      env.metric = [&](const Tensor& Qa, const Tensor& Qb) { return diag_metric(n, d, Qa, Qb); };
+      env.hole = [&]() { return diag_bond_hole(n, d, s); };
+      Tensor gate = trotter_gate(E, m, Lx, Ly, i[0], i[1], j[0], j[1], delta);
+      BondReport br = update_bond_env(E, s, i[0], i[1], j[0], j[1], gate, D, o, env, space, force_repair);
+      br.max_env_trunc = st.max_trunc;
+      record_bond(rep, br, o);
+      for (int k = rightward ? a : b; rightward ? k <= b : k >= a; k += rightward ? 1 : -1) {
+        const Tensor& A = s.at(st.sites[k][0], st.sites[k][1]);
+        msg = scaled(n, step(n, msg, st, k, A, A));
+      }
+      cursor = rightward ? b + 1 : a - 1;
+    }
+    absorb_layer(n, rolling, site, reverse ? t + 1 : t, method, reverse, ent);
+    env_err = std::max(env_err, rolling.max_trunc);
+  }
 }
 
 }  // namespace sps

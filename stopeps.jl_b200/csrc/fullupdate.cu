@@ -435,8 +435,7 @@ static Tensor bond_hole(Engine& E, const BondEnv& env) {
 
 // _positive_reduced_metric (full_update.jl:278-340): PSD projection of the
 // complete hole (scaled by its Frobenius norm), reduced with Qa and Qb.
-static Tensor positive_reduced_metric(Engine& E, const BondEnv& env, const Tensor& Qa, const Tensor& Qb) {
-  Tensor H = bond_hole(E, env);
+static Tensor positive_reduced_metric(Engine& E, const Tensor& H, const Tensor& Qa, const Tensor& Qb) {
   if (!all_finite(E, H)) throw Error(SPS_ERR_NUMERIC, "nonfinite norm metric");
   double scale = norm(E, H);
   std::vector<int> bk{1, 3, 5, 7, 9, 11, 0, 2, 4, 6, 8, 10};
@@ -594,15 +593,15 @@ static Fit optimize_pair(Engine& E, const Pair& p, const Tensor& N, const FUOpti
 }
 
 // update_bond! (full_update.jl:484-508)
-static BondReport update_bond(Engine& E, State& s, int ix, int iy, int jx, int jy, const Tensor& gate, int D,
-                              const FUOptions& o, const BondEnv& hole, const int space[2], bool force_repair) {
-  Pair p = reduced_pair(E, s.at(ix, iy), s.at(jx, jy), gate, hole.horizontal);
-  Tensor N = reduced_metric(E, hole, p.Qa, p.Qb);
+BondReport update_bond_env(Engine& E, State& s, int ix, int iy, int jx, int jy, const Tensor& gate, int D,
+                           const FUOptions& o, const PairEnv& env, const int space[2], bool force_repair) {
+  Pair p = reduced_pair(E, s.at(ix, iy), s.at(jx, jy), gate, env.horizontal);
+  Tensor N = env.metric(p.Qa, p.Qb);
   initialize_pair(E, p, N, D, space);
   Fit fit = optimize_pair(E, p, N, o);
   int repairs = 0;
   if (fit.trigger || force_repair) {
-    Tensor Nr = positive_reduced_metric(E, hole, p.Qa, p.Qb);
+    Tensor Nr = positive_reduced_metric(E, env.hole(), p.Qa, p.Qb);
     repairs = 1;
     initialize_pair(E, p, Nr, D, space);
     fit = optimize_pair(E, p, Nr, o);
@@ -614,6 +613,30 @@ static BondReport update_bond(Engine& E, State& s, int ix, int iy, int jx, int j
   s.at(jx, jy) = sb;
   fit.rep.repairs = repairs;
   return fit.rep;
+}
+
+// update_bond! with a row bond environment
+static BondReport update_bond(Engine& E, State& s, int ix, int iy, int jx, int jy, const Tensor& gate, int D,
+                              const FUOptions& o, const BondEnv& hole, const int space[2], bool force_repair) {
+  PairEnv env;
+  env.horizontal = hole.horizontal;
+  env.metric = [&](const Tensor& Qa, const Tensor& Qb) { return reduced_metric(E, hole, Qa, Qb); };
+  env.hole = [&]() { return bond_hole(E, hole); };
+  return update_bond_env(E, s, ix, iy, jx, jy, gate, D, o, env, space, force_repair);
+}
+
+void record_bond(StepReport& rep, const BondReport& br, const FUOptions& o) {
+  rep.bond_updates++;
+  if (br.iteration_limit_reached) {
+    rep.iteration_limit_hits++;
+    rep.max_iteration_limit_error = std::max(rep.max_iteration_limit_error, br.final_cost);
+  }
+  rep.stop_reasons[br.stop_reason]++;
+  rep.max_state_truncation = std::max(rep.max_state_truncation, br.final_cost);
+  rep.max_solver_residual = std::max(rep.max_solver_residual, br.residual);
+  if (br.residual > o.linear_tolerance) rep.linear_unconverged++;
+  rep.repairs += br.repairs;
+  rep.fallbacks += br.fallbacks;
 }
 
 // _sweep! for the row method (full_update.jl:510-557)
@@ -664,17 +687,7 @@ static void sweep(Engine& E, State& s, const Model& m, double delta, int D, cons
       double err = std::max(env.north[y].max_trunc, env.south[lastrow + 1].max_trunc);
       BondReport br = update_bond(E, s, x, y, jx, jy, gate, D, o, H, space, force_repair);
       br.max_env_trunc = err;
-      rep.bond_updates++;
-      if (br.iteration_limit_reached) {
-        rep.iteration_limit_hits++;
-        rep.max_iteration_limit_error = std::max(rep.max_iteration_limit_error, br.final_cost);
-      }
-      rep.stop_reasons[br.stop_reason]++;
-      rep.max_state_truncation = std::max(rep.max_state_truncation, br.final_cost);
-      rep.max_solver_residual = std::max(rep.max_solver_residual, br.residual);
-      if (br.residual > o.linear_tolerance) rep.linear_unconverged++;
-      rep.repairs += br.repairs;
-      rep.fallbacks += br.fallbacks;
+      record_bond(rep, br, o);
       layers[x + y * Lx] = double_layer(E, s.at(x, y), s.at(x, y));
       layers[jx + jy * Lx] = double_layer(E, s.at(jx, jy), s.at(jx, jy));
       int col = reverse ? finalx : x;
@@ -707,9 +720,6 @@ static void sweep(Engine& E, State& s, const Model& m, double delta, int D, cons
 StepReport evolution_step(Engine& E, State& s, const Model& m, double delta, int D, const FUOptions& o,
                           const BMPS& env_method, int order, const int space[2], bool record_entropy,
                           bool force_repair) {
-  if (env_method.diagonal)
-    throw Error(SPS_ERR_ARGUMENT,
-                "the full update takes row boundary-MPS environments; diagonal bond environments are not built");
   StepReport rep;
   double env_err = 0;
   Entropy ent;
@@ -728,8 +738,12 @@ StepReport evolution_step(Engine& E, State& s, const Model& m, double delta, int
     for (auto sw : sweeps) {
       if (sw.h && s.Lx < 2) continue;
       if (!sw.h && s.Ly < 2) continue;
-      sweep(E, s, m, gd, D, o, env_method, sw.h, sw.r, space, record_entropy ? &ent : nullptr, rep, env_err,
-            force_repair || E.force_repair);
+      if (env_method.diagonal)
+        sweep_diagonal(E, s, m, gd, D, o, env_method, sw.h, sw.r, space, record_entropy ? &ent : nullptr, rep,
+                       env_err, force_repair || E.force_repair);
+      else
+        sweep(E, s, m, gd, D, o, env_method, sw.h, sw.r, space, record_entropy ? &ent : nullptr, rep, env_err,
+              force_repair || E.force_repair);
     }
   }
   s.beta += 2 * delta;

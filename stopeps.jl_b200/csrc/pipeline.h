@@ -4,6 +4,7 @@
 #pragma once
 #include "engine.h"
 #include <array>
+#include <functional>
 #include <cmath>
 
 namespace sps {
@@ -132,6 +133,22 @@ struct StepReport {
   int repairs = 0, fallbacks = 0, linear_unconverged = 0;
 };
 Tensor trotter_gate(Engine& E, const Model& m, int Lx, int Ly, int ax, int ay, int bx, int by, double delta);
+// a bond environment as update_bond! uses it: the reduced metric N[rb, sb, rk, sk]
+// of the reduced pair's Q factors, and the bond hole (six exterior legs, each
+// split (ket, bra)) for the PSD repair
+struct PairEnv {
+  std::function<Tensor(const Tensor& Qa, const Tensor& Qb)> metric;
+  std::function<Tensor()> hole;
+  bool horizontal = true;
+};
+// update_bond! (src/evolution/full_update.jl:484-508)
+BondReport update_bond_env(Engine& E, State& s, int ix, int iy, int jx, int jy, const Tensor& gate, int D,
+                           const FUOptions& o, const PairEnv& env, const int space[2], bool force_repair);
+void record_bond(StepReport& rep, const BondReport& br, const FUOptions& o);
+// _sweep! on diagonal boundaries (src/evolution/diagonal_update.jl:61-102)
+void sweep_diagonal(Engine& E, State& s, const Model& m, double delta, int D, const FUOptions& o,
+                    const BMPS& method, bool horizontal, bool reverse, const int space[2], Entropy* ent,
+                    StepReport& rep, double& env_err, bool force_repair);
 StepReport evolution_step(Engine& E, State& s, const Model& m, double delta, int D, const FUOptions& o,
                           const BMPS& env_method, int order, const int space[2], bool record_entropy,
                           bool force_repair = false);

@@ -8,7 +8,8 @@ lognorm, the energy, <X> and the per-site <X> to 1e-10; auxiliary draws with
 identical configurations and log-probabilities to 1e-9 (every truncated SVD
 of the diagonal method is the full-spectrum one); the draw's conditionals
 in site order; the physical kind over a projected PEPS likewise; at a chi
-above every bond the device's diagonal values equal its row values.
+above every bond the device's diagonal values equal its row values; one
+full-update step on diagonal bond environments against the oracle's.
 """
 import numpy as np
 import pytest
@@ -98,8 +99,36 @@ def test_diagonal_exact_chi_equals_row_contraction(sps):
     np.testing.assert_allclose(lb, la, rtol=1e-12)
 
 
-def test_diagonal_environment_is_refused_by_the_full_update(sps):
-    g, e, st, m, ost, om = _setup(sps, "pepo_2x3_D2.npz")
-    ps, _ = sps.project_configuration(st, np.asarray(g["configs"][0]))
-    with pytest.raises(sps._lib.EngineError):
-        sps.evolution_step(ps, 0.01, 2, m)
+@pytest.mark.parametrize("case", CASES)
+def test_diagonal_full_update_step(sps, case):
+    """One second-order full-update step of the projected PEPS on diagonal
+    bond environments (``diagonal_update.jl``) against the oracle's step:
+    bond count, stop reasons, the log normalisation and the stepped state's
+    energy and lnZ to 1e-9 (the row step's tolerance)."""
+    from oracle import diagonal as dg, full_update as fu, model as md, sampling as osp
+    g = golden(case)
+    upd = sps.FullUpdate(max_iterations=8, linear_max_iterations=40) if "2x3" in case else sps.FullUpdate()
+    e = sps.Engine(int(g["Lx"]), int(g["Ly"]), sps.TFIM(float(g["J"]), float(g["h"])), update=upd)
+    st = upload_golden(sps, g, e)
+    pc = g["peps_cfg"]
+    chi, a, b = int(pc[3]), int(pc[4]), int(pc[5])
+    m = sps.BoundaryMPSDiagonal(chi, None if a < 0 else sps.Z2Space(a, b))
+    om = dg.BoundaryMPSDiagonal(chi, None if a < 0 else (a, b))
+    space = None if pc[1] < 0 else (int(pc[1]), int(pc[2]))
+    cfg = np.asarray(g["configs"][0])
+    ps, _ = sps.project_configuration(st, cfg)
+    ops, _ = osp.project_configuration(oracle_state(g), cfg.tolist())
+    r = sps.evolution_step(ps, float(g["dtau"]), int(pc[0]), m, None if space is None else sps.Z2Space(*space))
+    opts = fu.FullUpdate(upd.max_iterations, upd.error_tolerance, upd.diagonal_shift, upd.linear_max_iterations,
+                         upd.linear_tolerance)
+    model = md.TFIM(float(g["J"]), float(g["h"]))
+    orr = fu.evolution_step(ops, model, float(g["dtau"]), int(pc[0]), opts, om, space=space)
+    assert r["bond_updates"] == orr["bond_updates"]
+    stops = [r["stop_error_tolerance"], r["stop_iteration_limit"], r["stop_residual_fallback"], r["stop_disabled"]]
+    assert stops == [orr["stop_reasons"][k] for k in ("error_tolerance", "iteration_limit", "residual_fallback",
+                                                       "disabled")]
+    assert rel(r["log_normalization_sum"], sum(v for _, v in orr["normalizations"])) < 1e-9
+    en = sps.measure_energy(ps, m)
+    oe = dg.measure_energy(ops, model, om)
+    assert rel(en["energy_per_site"], oe["energy_per_site"]) < 1e-9
+    assert rel(en["log_norm"], oe["log_norm"]) < 1e-9

@@ -27,8 +27,16 @@ class OracleOps:
         self.bm, self.fu, self.md = bm, fu, md
 
     def _m(self, m):
+        from oracle import diagonal as dg
         sp = None if m.sector_space is None else (m.sector_space.n0, m.sector_space.n1)
+        if type(m).__name__ == "BoundaryMPSDiagonal":
+            return dg.BoundaryMPSDiagonal(m.chi, sp)
         return self.bm.BoundaryMPS(m.chi, sp)
+
+    @staticmethod
+    def _sampler(cache):
+        from oracle import diagonal as dg, sampling as sp
+        return dg if isinstance(cache, dg.DiagonalSamplingCache) else sp
 
     def identity(self):
         st = self.md.identity_pepo(self.c.lattice.Lx, self.c.lattice.Ly)
@@ -36,8 +44,11 @@ class OracleOps:
         return st, [v for _, v in rec]
 
     def sampling_cache(self, state, method, kind="auxiliary"):
-        from oracle import sampling as sp
-        return sp.SamplingCache(state, self._m(method), kind=kind)
+        from oracle import diagonal as dg, sampling as sp
+        m = self._m(method)
+        if isinstance(m, dg.BoundaryMPSDiagonal):
+            return dg.DiagonalSamplingCache(state, m, kind=kind)
+        return sp.SamplingCache(state, m, kind=kind)
 
     @staticmethod
     def _repairs(d):
@@ -48,8 +59,7 @@ class OracleOps:
                     min_relative_eigenvalue=min([0.0] + [r["minimum_relative_eigenvalue"] for r in neg]))
 
     def sample(self, cache, uniforms):
-        from oracle import sampling as sp
-        d = sp.sample_configuration(cache, uniforms=uniforms)
+        d = self._sampler(cache).sample_configuration(cache, uniforms=uniforms)
         return dict(configuration=np.asarray(d["configuration"]), log_probability=d["log_probability"],
                     max_environment_truncation=d["max_environment_truncation"], **self._repairs(d))
 
@@ -77,8 +87,7 @@ class OracleOps:
         return self._state(blob, c.lattice.Lx, c.lattice.Ly)
 
     def probability(self, cache, configuration):
-        from oracle import sampling as sp
-        d = sp.sample_configuration(cache, configuration=np.asarray(configuration).tolist())
+        d = self._sampler(cache).sample_configuration(cache, configuration=np.asarray(configuration).tolist())
         return dict(log_probability=d["log_probability"],
                     max_environment_truncation=d["max_environment_truncation"], **self._repairs(d))
 
@@ -88,12 +97,15 @@ class OracleOps:
         return st, [v for _, v in rec]
 
     def measure_energy(self, state, method):
-        from oracle import sampling as sp
-        m = sp.measure_energy(state, self.md.TFIM(self.c.model.J, self.c.model.h, self.c.model.fields), self._m(method))
-        return dict(m)
+        from oracle import diagonal as dg, sampling as sp
+        m = self._m(method)
+        mod = dg if isinstance(m, dg.BoundaryMPSDiagonal) else sp
+        return dict(mod.measure_energy(state, self.md.TFIM(self.c.model.J, self.c.model.h, self.c.model.fields), m))
 
     def lognorm(self, state, method):
-        return dict(self.bm.lognorm(state, self._m(method)))
+        from oracle import diagonal as dg
+        m = self._m(method)
+        return dict((dg if isinstance(m, dg.BoundaryMPSDiagonal) else self.bm).lognorm(state, m))
 
     def evolution_step(self, state, delta, D, method, space):
         u = self.c.update
@@ -304,3 +316,29 @@ def test_host_driver_with_site_fields(sps):
     uniform = sps.run_purification(c.__class__(**{**c.__dict__, "model": sps.TFIM(1.0, 0.7)}), ops=OracleOps(
         c.__class__(**{**c.__dict__, "model": sps.TFIM(1.0, 0.7)})), identity=ops.identity)
     assert abs(uniform.purification[-1]["lnZ"] - cp.purification[-1]["lnZ"]) > 1e-6   # the fields matter
+
+
+def test_host_driver_with_diagonal_contraction(sps):
+    """``RunConfig(contraction=BoundaryMPSDiagonal)`` through the host driver:
+    purification records, draws and the sampled curve equal the oracle
+    driver's own run on diagonal boundaries (draws consume their uniforms in
+    the anti-diagonal order, the parameter record names the method)."""
+    from oracle import driver as dr
+    kw = dict(beta0=0.1, beta_log=[0.1, 0.2], beta_measure=[0.1, 0.2], delta_tau_pur=0.05, delta_tau_peps=0.05,
+              D_pur=2, D_peps=2, chi_environment=4, Ns=3, seed=9)
+    c = sps.RunConfig(lattice=sps.Lattice(2, 3), model=sps.TFIM(1.0, 0.7), contraction=sps.BoundaryMPSDiagonal,
+                      resampling=sps.ResamplingOptions(enabled=False), **kw)
+    sps.validate_config(c)
+    ops = OracleOps(c)
+    cp = sps.run_purification(c, ops=ops, identity=ops.identity)
+    oc = dr.RunConfig(Lx=2, Ly=3, J=1.0, h=0.7, diagonal=True, **{k: v for k, v in kw.items()})
+    _, rows = dr.run_purification(oc)
+    for a, b in zip(cp.purification, rows):
+        for k in ("lnZ", "energy_per_site"):
+            assert (math.isnan(a[k]) and math.isnan(b[k])) or abs(a[k] - b[k]) <= 1e-12 * max(1.0, abs(b[k]))
+    res = sps.run_stochastic(c, cp, ops=ops)
+    draws = res["diagnostics"]["born_draws"]
+    assert len(draws) == 3 and all(np.isfinite(d["log_probability"]) for d in draws)
+    p = sps.parameter_dict(c)
+    assert p["contraction"] == "BoundaryMPS-Diagonal"
+    assert p["sampling_site_order"][:3] == [(1, 1), (2, 1), (1, 2)]
