@@ -9,7 +9,7 @@ function.  All indices are 0-based here.
 from __future__ import annotations
 
 import math
-from dataclasses import dataclass
+from dataclasses import dataclass, field
 
 import numpy as np
 
@@ -32,10 +32,14 @@ class BoundaryMPS:
 
 @dataclass
 class Env:
-    """``BoundaryEnvironment`` (``boundary_mps.jl:79-83``)."""
+    """``BoundaryEnvironment`` (``boundary_mps.jl:79-83``); ``center`` and
+    ``variational`` (the fit records) are kept by the variational method
+    (``RowVariationalBoundary``, ``row_variational.jl:37-43``)."""
     tensors: list
     log_scale: float = 0.0
     max_truncation: float = 0.0
+    center: int = 0
+    variational: list = field(default_factory=list)
 
 
 class Entropy:
@@ -209,7 +213,11 @@ def absorb_zipup(env: Env, row, method: BoundaryMPS, side="north") -> Env:
 
 
 def absorb(env: Env, row, method: BoundaryMPS, side="north", entropy=None, row_cut=0) -> Env:
-    """``_absorb`` for the row method (``boundary_mps.jl:136-151``)."""
+    """``_absorb`` for the row method (``boundary_mps.jl:136-151``); the row
+    variational method absorbs by its fit (``variational.absorb_variational``)."""
+    if getattr(method, "variational", False):
+        from .variational import absorb_variational
+        return absorb_variational(env, row, method, side, entropy, row_cut)
     if method.zipup:
         return absorb_zipup(env, row, method, side)
     B = []
@@ -252,11 +260,19 @@ def positive_real(z, name):
 
 
 def lognorm(s, method):
-    """``lognorm`` (``boundary_mps.jl:180-186``)."""
-    mant, ls, mt = contract_layers(row_layers(s), method)
-    v = positive_real(mant, "norm")
-    return dict(log_norm=math.log(v) + ls + 2 * s.log_amplitude,
-                tensor_log_norm=math.log(v) + ls, max_environment_truncation=mt)
+    """``lognorm`` (``boundary_mps.jl:180-186``; the variational method adds its
+    fit summary, ``row_variational.jl:331-339``)."""
+    layers = row_layers(s)
+    env = trivial_boundary(col(layers, 0), "north")
+    for y in range(len(layers[0])):
+        env = absorb(env, col(layers, y), method, row_cut=y + 1)
+    v = positive_real(close_boundary(env.tensors), "norm")
+    out = dict(log_norm=math.log(v) + env.log_scale + 2 * s.log_amplitude,
+               tensor_log_norm=math.log(v) + env.log_scale, max_environment_truncation=env.max_truncation)
+    if getattr(method, "variational", False):
+        from .variational import summary
+        out["boundary_variational"] = summary(env.variational)
+    return out
 
 
 def boundary_environments(layers, method, side="both", entropy=None):
