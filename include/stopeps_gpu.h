@@ -61,7 +61,10 @@ typedef struct sps_config {
  * (src/contraction/diagonal_mps.jl: anti-diagonal layers, site blocks,
  * truncation of the bonds a block opens), taken by sps_lognorm,
  * sps_measure_energy, the sampling caches and, for its bond environments,
- * the full update (src/evolution/diagonal_update.jl). */
+ * the full update (src/evolution/diagonal_update.jl); 3 is
+ * BoundaryMPSRowVariational (src/contraction/row_variational.jl: every row
+ * absorbed by a two-site variational fit; its sweep options are the
+ * handle's, sps_set_variational). */
 typedef struct sps_boundary {
   int32_t chi;
   int32_t space0, space1;
@@ -289,6 +292,16 @@ int sps_set_truncated_svd(sps_handle* h, int32_t method);
  * h_0, and sps_measure_energy's total is -J sum ZZ - sum_i h_i <X_i>.
  * n = Lx*Ly sets them; n = 0 clears them (cfg.h everywhere again). */
 int sps_set_site_fields(sps_handle* h, int32_t n, const double* fields);
+/* The sweep options of BoundaryMPSRowVariational (row_variational.jl:10-25)
+ * for the handle's later calls with absorption 3: max_sweep >= 1 round trips,
+ * threshold_sweep >= 0 on the relative change of the squared norm (0 runs
+ * every sweep).  Defaults 4 and 1e-8. */
+int sps_set_variational(sps_handle* h, int32_t max_sweep, double threshold_sweep);
+/* lognorm with the fit summary of a variational method
+ * (row_variational.jl:331-339, _variational_summary): counts = {layers,
+ * max_sweeps, sweep_limit_hits, fallback_count}; max_relative_change. */
+int sps_lognorm_variational(sps_handle* h, int32_t state_id, const sps_boundary* method, sps_lognorm_result* out,
+                            int32_t* counts, double* max_relative_change);
 /* No counterpart in the reference: host-side failure injection for tests
  * (nothing faults on the device; the library takes its ordinary error
  * paths).  force_repair != 0 treats every full-update bond fit as triggered,

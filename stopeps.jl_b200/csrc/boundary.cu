@@ -235,6 +235,7 @@ static Env absorb_zipup(Engine& E, const Env& env, const std::vector<Tensor>& ro
 // _absorb for the row method (boundary_mps.jl:136-151)
 Env absorb(Engine& E, const Env& env, const std::vector<Tensor>& row, const BMPS& m, bool north,
            Entropy* ent, int row_cut, const std::vector<Tensor>* kets) {
+  if (m.variational) return absorb_variational(E, env, row, m, north, ent, row_cut);
   if (m.zipup) return absorb_zipup(E, env, row, m, north, north ? kets : nullptr);
   std::vector<Tensor> B;
   B.reserve(row.size());
@@ -274,9 +275,10 @@ LogNorm lognorm(Engine& E, const State& s, const BMPS& m) {
   if (m.diagonal) return lognorm_diagonal(E, s, m);
   auto layers = row_layers(E, s);
   Env env = trivial_boundary(E, column(layers, s.Lx, 0), true);
-  for (int y = 0; y < s.Ly; ++y) env = absorb(E, env, column(layers, s.Lx, y), m, true);
+  for (int y = 0; y < s.Ly; ++y) env = absorb(E, env, column(layers, s.Lx, y), m, true, nullptr, y + 1);
   double v = positive_real(close_boundary(E, env.t), "norm");
-  return {std::log(v) + env.log_scale + 2 * s.log_amplitude, std::log(v) + env.log_scale, env.max_trunc};
+  return {std::log(v) + env.log_scale + 2 * s.log_amplitude, std::log(v) + env.log_scale, env.max_trunc,
+          env.variational};
 }
 
 // boundary_environments (boundary_mps.jl:193-209)

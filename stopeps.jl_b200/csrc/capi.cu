@@ -19,6 +19,8 @@ struct sps_handle {
   cudaEvent_t t0 = nullptr, t1 = nullptr;
   sps_config cfg;
   std::vector<double> site_fields;   // per-site transverse fields; empty: cfg.h everywhere
+  int var_max_sweep = 4;              // the row variational method's sweep options
+  double var_threshold_sweep = 1e-8;
   std::unordered_map<int, State> states;
   std::unordered_map<int, SamplingCache> caches;
   std::unordered_map<int, int> cache_state;   // cache -> pinned state copy id
@@ -50,15 +52,18 @@ State& get_state(sps_handle* h, int id) {
   return it->second;
 }
 
-BMPS to_bmps(const sps_boundary* b) {
+BMPS to_bmps(const sps_handle* h, const sps_boundary* b) {
   if (!b) throw Error(SPS_ERR_ARGUMENT, "missing boundary method");
   BMPS m;
   m.chi = b->chi;
   m.space[0] = b->space0 >= 0 && b->space1 >= 0 ? b->space0 : -1;
   m.space[1] = b->space0 >= 0 && b->space1 >= 0 ? b->space1 : -1;
-  if (b->absorption < 0 || b->absorption > 2) throw Error(SPS_ERR_ARGUMENT, "unknown boundary absorption");
+  if (b->absorption < 0 || b->absorption > 3) throw Error(SPS_ERR_ARGUMENT, "unknown boundary absorption");
   m.zipup = b->absorption == 1;
   m.diagonal = b->absorption == 2;
+  m.variational = b->absorption == 3;
+  m.max_sweep = h->var_max_sweep;
+  m.threshold_sweep = h->var_threshold_sweep;
   return m;
 }
 
@@ -289,6 +294,44 @@ int sps_set_truncated_svd(sps_handle* h, int32_t method) {
     if (method != 0 && method != 1) throw Error(SPS_ERR_ARGUMENT, "sps_set_truncated_svd: method is 0 or 1");
     h->E->full_spectrum = method == 1;
     for (auto& w : h->workers) w->full_spectrum = method == 1;
+  });
+}
+
+int sps_set_variational(sps_handle* h, int32_t max_sweep, double threshold_sweep) {
+  return guarded(h, [&] {
+    if (max_sweep < 1) throw Error(SPS_ERR_ARGUMENT, "max_sweep must be positive");
+    if (!(std::isfinite(threshold_sweep) && threshold_sweep >= 0))
+      throw Error(SPS_ERR_ARGUMENT, "threshold_sweep must be finite and nonnegative");
+    h->var_max_sweep = max_sweep;
+    h->var_threshold_sweep = threshold_sweep;
+  });
+}
+
+int sps_lognorm_variational(sps_handle* h, int32_t state_id, const sps_boundary* method, sps_lognorm_result* out,
+                            int32_t* counts, double* max_relative_change) {
+  return guarded(h, [&] {
+    LogNorm r = lognorm(*h->E, get_state(h, state_id), to_bmps(h, method));
+    if (out) {
+      out->log_norm = r.log_norm;
+      out->tensor_log_norm = r.tensor_log_norm;
+      out->max_environment_truncation = r.max_env_trunc;
+    }
+    // _variational_summary (diagonal_variational.jl:40-46)
+    int layers = (int)r.variational.size(), max_sweeps = 0, limit = 0, fallbacks = 0;
+    double change = 0;
+    for (const auto& v : r.variational) {
+      max_sweeps = std::max(max_sweeps, v.sweeps);
+      limit += v.stop_reason == VariationalRecord::SWEEP_LIMIT;
+      fallbacks += v.fallback;
+      if (std::isfinite(v.relative_change)) change = std::max(change, v.relative_change);
+    }
+    if (counts) {
+      counts[0] = layers;
+      counts[1] = max_sweeps;
+      counts[2] = limit;
+      counts[3] = fallbacks;
+    }
+    if (max_relative_change) *max_relative_change = change;
   });
 }
 
@@ -722,7 +765,7 @@ int sps_evolution_step(sps_handle* h, int32_t state_id, double delta, int32_t D,
       sp[0] = space[0];
       sp[1] = space[1];
     }
-    StepReport r = evolution_step(*h->E, s, model_of(h), delta, D, fu_of(h), to_bmps(environment),
+    StepReport r = evolution_step(*h->E, s, model_of(h), delta, D, fu_of(h), to_bmps(h, environment),
                                   h->cfg.trotter_order, sp, h->cfg.record_boundary_entropy != 0);
     if (report) fill_report(r, *report);
   });
@@ -738,7 +781,7 @@ int sps_evolution_step_batch(sps_handle* h, int32_t n, const int32_t* state_ids,
       sp[0] = space[0];
       sp[1] = space[1];
     }
-    const BMPS m = to_bmps(environment);
+    const BMPS m = to_bmps(h, environment);
     const Model md = model_of(h);
     const FUOptions o = fu_of(h);
     run_batch(h, n, [&](Engine& E, int i) {
@@ -751,7 +794,7 @@ int sps_evolution_step_batch(sps_handle* h, int32_t n, const int32_t* state_ids,
 
 int sps_lognorm(sps_handle* h, int32_t state_id, const sps_boundary* method, sps_lognorm_result* out) {
   return guarded(h, [&] {
-    LogNorm r = lognorm(*h->E, get_state(h, state_id), to_bmps(method));
+    LogNorm r = lognorm(*h->E, get_state(h, state_id), to_bmps(h, method));
     if (out) {
       out->log_norm = r.log_norm;
       out->tensor_log_norm = r.tensor_log_norm;
@@ -764,7 +807,7 @@ int sps_measure_energy(sps_handle* h, int32_t state_id, const sps_boundary* meth
                        double* site_x, double* se_north, double* se_south) {
   return guarded(h, [&] {
     State& s = get_state(h, state_id);
-    EnergyResult r = measure_energy(*h->E, s, model_of(h), to_bmps(method), h->cfg.record_boundary_entropy != 0);
+    EnergyResult r = measure_energy(*h->E, s, model_of(h), to_bmps(h, method), h->cfg.record_boundary_entropy != 0);
     if (out) fill_energy(r, *out);
     if (site_x) std::memcpy(site_x, r.site_x.data(), r.site_x.size() * sizeof(double));
     // the diagonal method's profiles are per site (northwest, southeast)
@@ -779,7 +822,7 @@ int sps_measure_energy_batch(sps_handle* h, int32_t n, const int32_t* state_ids,
                              sps_energy* out, double* site_x) {
   return guarded(h, [&] {
     std::vector<State*> st = batch_states(h, n, state_ids);
-    const BMPS m = to_bmps(method);
+    const BMPS m = to_bmps(h, method);
     const Model md = model_of(h);
     const size_t L = (size_t)h->cfg.Lx * h->cfg.Ly;
     run_batch(h, n, [&](Engine& E, int i) {
@@ -794,7 +837,7 @@ int sps_lognorm_batch(sps_handle* h, int32_t n, const int32_t* state_ids, const 
                       sps_lognorm_result* out) {
   return guarded(h, [&] {
     std::vector<State*> st = batch_states(h, n, state_ids);
-    const BMPS m = to_bmps(method);
+    const BMPS m = to_bmps(h, method);
     run_batch(h, n, [&](Engine& E, int i) {
       LogNorm r = lognorm(E, *st[i], m);
       if (out) {
@@ -823,7 +866,7 @@ int sps_sampling_cache(sps_handle* h, int32_t pepo_id, const sps_boundary* metho
     int sid = h->next_id++;
     h->states[sid] = s;
     int id = h->next_id++;
-    h->caches[id] = make_sampling_cache(*h->E, h->states[sid], to_bmps(method));
+    h->caches[id] = make_sampling_cache(*h->E, h->states[sid], to_bmps(h, method));
     h->cache_state[id] = sid;
     *cache_id = id;
   });
@@ -838,7 +881,7 @@ int sps_sampling_cache_kind(sps_handle* h, int32_t state_id, const sps_boundary*
     int sid = h->next_id++;
     h->states[sid] = s;
     int id = h->next_id++;
-    h->caches[id] = make_sampling_cache(*h->E, h->states[sid], to_bmps(method), kind);
+    h->caches[id] = make_sampling_cache(*h->E, h->states[sid], to_bmps(h, method), kind);
     h->cache_state[id] = sid;
     *cache_id = id;
   });

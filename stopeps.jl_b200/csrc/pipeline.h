@@ -32,6 +32,25 @@ struct BMPS {        // BoundaryMPS (src/contraction/boundary_mps.jl:11-18)
   // BoundaryMPSDiagonal (src/contraction/diagonal_mps.jl:3-9): anti-diagonal
   // layers instead of rows, same chi and sector budget
   bool diagonal = false;
+  // BoundaryMPSRowVariational (src/contraction/row_variational.jl:10-25): rows
+  // absorbed by a two-site variational fit
+  bool variational = false;
+  int max_sweep = 4;
+  double threshold_sweep = 1e-8;
+};
+
+// one absorption of the row variational method (the records that
+// _variational_summary collects, diagonal_variational.jl:40-46)
+struct VariationalRecord {
+  enum { DIRECT = 0, ZERO_TARGET = 1, SWEEP_LIMIT = 2, THRESHOLD_SWEEP = 3, NUMERICAL_FALLBACK = 4 };
+  int layer = 0;
+  bool reverse = false;
+  int sweeps = 0;
+  double relative_change = 0;
+  int stop_reason = DIRECT;
+  double max_local_discarded_weight = 0;
+  bool fallback = false;
+  std::string fallback_reason;
 };
 
 struct State {       // FiniteState (src/states/finite.jl:27-49)
@@ -46,6 +65,10 @@ struct State {       // FiniteState (src/states/finite.jl:27-49)
 struct Env {         // BoundaryEnvironment (boundary_mps.jl:79-83)
   std::vector<Tensor> t;
   double log_scale = 0, max_trunc = 0;
+  // the row variational method's canonical centre and fit records
+  // (RowVariationalBoundary, row_variational.jl:37-43)
+  int center = 0;
+  std::vector<VariationalRecord> variational;
 };
 
 struct Entropy {     // BoundaryEntropy (boundary_mps.jl:44-57)
@@ -91,7 +114,13 @@ CompressReport compress_boundary(Engine& E, std::vector<Tensor>& B, const BMPS& 
 Env absorb(Engine& E, const Env& env, const std::vector<Tensor>& row, const BMPS& m, bool north,
            Entropy* ent = nullptr, int row_cut = 0, const std::vector<Tensor>* kets = nullptr);
 double close_boundary(Engine& E, const std::vector<Tensor>& B);
-struct LogNorm { double log_norm, tensor_log_norm, max_env_trunc; };
+struct LogNorm {
+  double log_norm, tensor_log_norm, max_env_trunc;
+  std::vector<VariationalRecord> variational;
+};
+// _absorb for BoundaryMPSRowVariational (variational.cu; row_variational.jl:306-329)
+Env absorb_variational(Engine& E, const Env& env, const std::vector<Tensor>& row, const BMPS& m, bool north,
+                       Entropy* ent, int row_cut);
 LogNorm lognorm(Engine& E, const State& s, const BMPS& m);
 struct Envs { std::vector<Env> north, south; double max_trunc = 0; };
 Envs boundary_environments(Engine& E, const std::vector<Tensor>& layers, int Lx, int Ly, const BMPS& m,

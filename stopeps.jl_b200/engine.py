@@ -14,14 +14,16 @@ import json
 import numpy as np
 
 from . import _lib
-from .config import BoundaryMPS, BoundaryMPSDiagonal, BoundaryMPSZipUp, RunConfig, TFIM, FullUpdate, Z2Space
+from .config import BoundaryMPS, BoundaryMPSDiagonal, BoundaryMPSRowVariational, BoundaryMPSZipUp, RunConfig, TFIM, FullUpdate, Z2Space
 
 
 def _arr(a, ctype):
     return a.ctypes.data_as(C.POINTER(ctype))
 
 
-def _boundary(m: BoundaryMPS):
+def _boundary(m: BoundaryMPS, e=None):
+    """The C ABI's sps_boundary of a method; a variational method also sets the
+    engine's sweep options (``max_sweep``, ``threshold_sweep``)."""
     b = _lib.sps_boundary()
     b.chi = int(m.chi)
     if m.sector_space is None:
@@ -29,6 +31,10 @@ def _boundary(m: BoundaryMPS):
     else:
         b.space0, b.space1 = int(m.sector_space.n0), int(m.sector_space.n1)
     b.absorption = 2 if isinstance(m, BoundaryMPSDiagonal) else 1 if isinstance(m, BoundaryMPSZipUp) else 0
+    if isinstance(m, BoundaryMPSRowVariational):
+        b.absorption = 3
+        if e is not None:
+            e.check(e.lib.sps_set_variational(e.h, int(m.max_sweep), float(m.threshold_sweep)))
     return b
 
 
@@ -330,7 +336,7 @@ def evolution_step(state: DeviceState, delta, D, contraction: BoundaryMPS, secto
     """``evolution_step!(state, model, delta, D, FullUpdate, contraction)``."""
     e = state.engine
     rep = _lib.sps_step_report()
-    b = _boundary(contraction)
+    b = _boundary(contraction, e)
     if sector_space is None:
         e.check(e.lib.sps_evolution_step(e.h, state.id, float(delta), int(D), None, C.byref(b), C.byref(rep)))
     else:
@@ -340,9 +346,20 @@ def evolution_step(state: DeviceState, delta, D, contraction: BoundaryMPS, secto
 
 
 def lognorm(state: DeviceState, contraction: BoundaryMPS):
+    """``lognorm``; a variational method adds ``boundary_variational``, the fit
+    summary (``max_sweeps``, ``sweep_limit_hits``, ``fallback_count``,
+    ``max_relative_change``, ``layers`` = the number of absorptions)."""
     e = state.engine
     r = _lib.sps_lognorm_result()
-    b = _boundary(contraction)
+    b = _boundary(contraction, e)
+    if isinstance(contraction, BoundaryMPSRowVariational):
+        counts = (C.c_int32 * 4)()
+        change = C.c_double()
+        e.check(e.lib.sps_lognorm_variational(e.h, state.id, C.byref(b), C.byref(r), counts, C.byref(change)))
+        return dict(log_norm=r.log_norm, tensor_log_norm=r.tensor_log_norm,
+                    max_environment_truncation=r.max_environment_truncation,
+                    boundary_variational=dict(layers=counts[0], max_sweeps=counts[1], sweep_limit_hits=counts[2],
+                                              fallback_count=counts[3], max_relative_change=change.value))
     e.check(e.lib.sps_lognorm(e.h, state.id, C.byref(b), C.byref(r)))
     return dict(log_norm=r.log_norm, tensor_log_norm=r.tensor_log_norm,
                 max_environment_truncation=r.max_environment_truncation)
@@ -352,7 +369,7 @@ def measure_energy(state: DeviceState, contraction: BoundaryMPS, site_profile=Fa
     """``measure_energy``; also returns ``magnetization`` = <sum_i X_i>/N."""
     e = state.engine
     r = _lib.sps_energy()
-    b = _boundary(contraction)
+    b = _boundary(contraction, e)
     L = e.Lx * e.Ly
     sx = np.zeros(L)
     diagonal = isinstance(contraction, BoundaryMPSDiagonal)
@@ -389,7 +406,7 @@ class SamplingCache:
         self.engine = state.engine
         self.kind = kind
         cid = C.c_int32()
-        b = _boundary(contraction)
+        b = _boundary(contraction, self.engine)
         self.engine.check(self.engine.lib.sps_sampling_cache_kind(self.engine.h, state.id, C.byref(b),
                                                                   SAMPLING_KINDS[kind], C.byref(cid)))
         self.id = cid.value
@@ -505,7 +522,7 @@ def evolution_step_batch(states, deltas, D, contraction: BoundaryMPS, sector_spa
     n = len(states)
     d = np.ascontiguousarray(np.broadcast_to(np.asarray(deltas, np.float64), (n,)))
     reps = (_lib.sps_step_report * n)()
-    b = _boundary(contraction)
+    b = _boundary(contraction, e)
     sp = None if sector_space is None else (C.c_int32 * 2)(sector_space.n0, sector_space.n1)
     e.check(e.lib.sps_evolution_step_batch(e.h, n, _arr(ids, C.c_int32), _arr(d, C.c_double), int(D), sp,
                                            C.byref(b), reps))
@@ -520,7 +537,7 @@ def measure_energy_batch(states, contraction: BoundaryMPS):
     n, L = len(states), e.Lx * e.Ly
     out = (_lib.sps_energy * n)()
     sx = np.zeros(n * L)
-    b = _boundary(contraction)
+    b = _boundary(contraction, e)
     e.check(e.lib.sps_measure_energy_batch(e.h, n, _arr(ids, C.c_int32), C.byref(b), out, _arr(sx, C.c_double)))
     res = []
     for i, r in enumerate(out):
@@ -538,7 +555,7 @@ def lognorm_batch(states, contraction: BoundaryMPS):
     e, ids = _ids(states)
     n = len(states)
     out = (_lib.sps_lognorm_result * n)()
-    b = _boundary(contraction)
+    b = _boundary(contraction, e)
     e.check(e.lib.sps_lognorm_batch(e.h, n, _arr(ids, C.c_int32), C.byref(b), out))
     return [dict(log_norm=r.log_norm, tensor_log_norm=r.tensor_log_norm,
                  max_environment_truncation=r.max_environment_truncation) for r in out]

@@ -31,6 +31,9 @@ class OracleOps:
         sp = None if m.sector_space is None else (m.sector_space.n0, m.sector_space.n1)
         if type(m).__name__ == "BoundaryMPSDiagonal":
             return dg.BoundaryMPSDiagonal(m.chi, sp)
+        if type(m).__name__ == "BoundaryMPSRowVariational":
+            from oracle import variational as va
+            return va.BoundaryMPSRowVariational(m.chi, sp, m.max_sweep, m.threshold_sweep)
         return self.bm.BoundaryMPS(m.chi, sp)
 
     @staticmethod
@@ -342,3 +345,23 @@ def test_host_driver_with_diagonal_contraction(sps):
     p = sps.parameter_dict(c)
     assert p["contraction"] == "BoundaryMPS-Diagonal"
     assert p["sampling_site_order"][:3] == [(1, 1), (2, 1), (1, 2)]
+
+
+def test_host_driver_with_row_variational_contraction(sps):
+    """``RunConfig(contraction=BoundaryMPSRowVariational)`` through the host
+    driver equals the oracle's exact-compression run at a chi above every bond
+    (the variational fit is then exact) and names the method in its record."""
+    from oracle import driver as dr
+    kw = dict(beta0=0.1, beta_log=[0.1, 0.2], beta_measure=[0.1, 0.2], delta_tau_pur=0.05, delta_tau_peps=0.05,
+              D_pur=2, D_peps=2, chi_environment=64, Ns=3, seed=9)
+    c = sps.RunConfig(lattice=sps.Lattice(3, 2), model=sps.TFIM(1.0, 0.7),
+                      contraction=sps.BoundaryMPSRowVariational, resampling=sps.ResamplingOptions(enabled=False),
+                      **kw)
+    sps.validate_config(c)
+    ops = OracleOps(c)
+    cp = sps.run_purification(c, ops=ops, identity=ops.identity)
+    _, rows = dr.run_purification(dr.RunConfig(Lx=3, Ly=2, J=1.0, h=0.7, **kw))
+    for a, b in zip(cp.purification, rows):
+        for k in ("lnZ", "energy_per_site"):
+            assert (math.isnan(a[k]) and math.isnan(b[k])) or abs(a[k] - b[k]) <= 1e-11 * max(1.0, abs(b[k]))
+    assert sps.parameter_dict(c)["contraction"] == "BoundaryMPS-Row-Variational"
