@@ -215,8 +215,8 @@ def absorb_zipup(env: Env, row, method: BoundaryMPS, side="north") -> Env:
 def absorb(env: Env, row, method: BoundaryMPS, side="north", entropy=None, row_cut=0) -> Env:
     """``_absorb`` for the row method (``boundary_mps.jl:136-151``); the row
     variational method absorbs by its fit (``variational.absorb_variational``)."""
-    if getattr(method, "variational", False):
-        from .variational import absorb_variational
+    from .variational import BoundaryMPSRowVariational, absorb_variational
+    if isinstance(method, BoundaryMPSRowVariational):
         return absorb_variational(env, row, method, side, entropy, row_cut)
     if method.zipup:
         return absorb_zipup(env, row, method, side)
@@ -269,7 +269,7 @@ def lognorm(s, method):
     v = positive_real(close_boundary(env.tensors), "norm")
     out = dict(log_norm=math.log(v) + env.log_scale + 2 * s.log_amplitude,
                tensor_log_norm=math.log(v) + env.log_scale, max_environment_truncation=env.max_truncation)
-    if getattr(method, "variational", False):
+    if env.variational:
         from .variational import summary
         out["boundary_variational"] = summary(env.variational)
     return out

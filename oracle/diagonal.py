@@ -191,10 +191,11 @@ class DiagonalBoundary:
     log_scale: float = 0.0
     max_truncation: float = 0.0
     scalar: float = 1.0
+    variational: list = field(default_factory=list)   # fit records of the variational method
 
     def copy(self):
         return DiagonalBoundary(list(self.tensors), list(self.edges), self.center, self.log_scale,
-                                self.max_truncation, self.scalar)
+                                self.max_truncation, self.scalar, list(self.variational))
 
 
 class DiagonalEntropy:
@@ -339,7 +340,11 @@ def compress_blocks(blocks, layout, method: BoundaryMPSDiagonal, right, reverse=
 def absorb_layer(env: DiagonalBoundary, site_tensor, Lx, Ly, t, method: BoundaryMPSDiagonal, reverse=False,
                  entropy=None) -> DiagonalBoundary:
     """``_diagonal_absorb_layer!`` (diagonal_mps.jl:272-297); ``site_tensor``
-    maps a site to its tensor.  Modifies and returns ``env``."""
+    maps a site to its tensor.  Modifies and returns ``env``.  The diagonal
+    variational method absorbs by its fit (``diagonal_variational``)."""
+    from . import diagonal_variational as dv
+    if isinstance(method, dv.BoundaryMPSDiagonalVariational):
+        return dv.absorb_layer_variational(env, site_tensor, Lx, Ly, t, method, reverse, entropy)
     if method.chi < 1:
         raise ValueError("chi must be positive")
     layout = layer_layout(env, Lx, Ly, t, reverse)
@@ -394,8 +399,12 @@ def lognorm(state, method: BoundaryMPSDiagonal):
     for t in range(layer_count(state.Lx, state.Ly)):
         absorb_layer(env, at, state.Lx, state.Ly, t, method)
     value = math.log(positive_real(env.scalar, "norm")) + env.log_scale
-    return dict(log_norm=value + 2 * state.log_amplitude, tensor_log_norm=value,
-                max_environment_truncation=env.max_truncation)
+    out = dict(log_norm=value + 2 * state.log_amplitude, tensor_log_norm=value,
+               max_environment_truncation=env.max_truncation)
+    if env.variational:
+        from .variational import summary
+        out["boundary_variational"] = summary(env.variational)
+    return out
 
 
 # ---------------------------------------------------------------------------

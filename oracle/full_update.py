@@ -514,8 +514,8 @@ def sweep(state, model, delta, D, method, contraction, direction, reverse, space
 def evolution_step(state, model: TFIM, delta, D, method: FullUpdate, contraction, order=2,
                    space=None, record_entropy=False, force_repair_bonds=()):
     """``evolution_step!`` (``full_update.jl:559-597``)."""
-    from . import diagonal as dg
-    diagonal = isinstance(contraction, dg.BoundaryMPSDiagonal)
+    from . import diagonal as dg, diagonal_variational as dv
+    diagonal = isinstance(contraction, (dg.BoundaryMPSDiagonal, dv.BoundaryMPSDiagonalVariational))
     records = []
     env_err = 0.0
     entropy = None

@@ -79,3 +79,43 @@ def test_space_map_and_options():
     for bad in (dict(chi=0), dict(chi=4, max_sweep=0), dict(chi=4, threshold_sweep=-1.0)):
         with pytest.raises(ValueError):
             va.BoundaryMPSRowVariational(**bad)
+
+
+def test_diagonal_variational_exact_and_truncated():
+    """``diagonal_variational.jl``: exact at a chi above every bond (energy and
+    every Born probability equal the row contraction's), as accurate as the
+    diagonal SVD absorption at a truncating chi, records per layer, the whole
+    sweep budget with a zero threshold, and the full update runs on it."""
+    from oracle import diagonal as dg, diagonal_variational as dv, full_update as fu
+    st = _state(3, 2, h=0.9)
+    m = md.TFIM(1.0, 0.9)
+    a = sp.measure_energy(st, m, bm.BoundaryMPS(200))
+    b = dg.measure_energy(st, m, dv.BoundaryMPSDiagonalVariational(200))
+    for k in ("energy_total", "log_norm", "x_sum", "zz_sum"):
+        assert abs(a[k] - b[k]) <= 1e-12 * max(1.0, abs(a[k])), k
+    ca = sp.SamplingCache(st, bm.BoundaryMPS(200))
+    cb = dg.DiagonalSamplingCache(st, dv.BoundaryMPSDiagonalVariational(200))
+    for bits in itertools.product([1, 2], repeat=6):
+        cfg = [[bits[x + 3 * y] for y in range(2)] for x in range(3)]
+        assert abs(sp.sample_configuration(ca, configuration=cfg)["log_probability"]
+                   - dg.sample_configuration(cb, configuration=cfg)["log_probability"]) < 1e-11
+    st = _state(4, 3)
+    exact = bm.lognorm(st, bm.BoundaryMPS(400))["log_norm"]
+    for chi in (4, 8):
+        svd = dg.lognorm(st, dg.BoundaryMPSDiagonal(chi))
+        var = dg.lognorm(st, dv.BoundaryMPSDiagonalVariational(chi))
+        assert abs(var["log_norm"] - exact) <= 1.5 * abs(svd["log_norm"] - exact) + 1e-13
+        layers = var["boundary_variational"]["layers"]
+        assert len(layers) == dg.layer_count(4, 3) and var["boundary_variational"]["fallback_count"] == 0
+        assert {r["stop_reason"] for r in layers} <= {"direct", "threshold_sweep", "sweep_limit"}
+    full = dg.lognorm(st, dv.BoundaryMPSDiagonalVariational(8, threshold_sweep=0.0, max_sweep=2))
+    assert all(r["sweeps"] == 2 for r in full["boundary_variational"]["layers"] if r["stop_reason"] != "direct")
+    out = []
+    for method in (bm.BoundaryMPS(400), dv.BoundaryMPSDiagonalVariational(400)):
+        s = md.identity_pepo(3, 2)
+        md.normalize_state(s)
+        fu.evolution_step(s, m, 0.05, 4, fu.FullUpdate(), method)
+        out.append(sp.measure_energy(s, m, bm.BoundaryMPS(400))["energy_per_site"])
+    assert abs(out[0] - out[1]) < 1e-12
+    with pytest.raises(ValueError):
+        dv.BoundaryMPSDiagonalVariational(4, None, target_cache_bytes=-1)
