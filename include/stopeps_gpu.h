@@ -64,7 +64,9 @@ typedef struct sps_config {
  * the full update (src/evolution/diagonal_update.jl); 3 is
  * BoundaryMPSRowVariational (src/contraction/row_variational.jl: every row
  * absorbed by a two-site variational fit; its sweep options are the
- * handle's, sps_set_variational). */
+ * handle's, sps_set_variational); 4 is BoundaryMPSDiagonalVariational
+ * (src/contraction/diagonal_variational.jl: every diagonal layer absorbed by
+ * a two-site variational fit, the same options). */
 typedef struct sps_boundary {
   int32_t chi;
   int32_t space0, space1;

@@ -6,7 +6,7 @@ types, the two drivers, the hot-path functions and the ensemble statistics.
 The numerical work runs in ``libstopeps_gpu.so`` (C ABI in
 ``include/stopeps_gpu.h``).
 """
-from .config import (Z2Space, Lattice, TFIM, FullUpdate, BoundaryMPS, BoundaryMPSRow, BoundaryMPSZipUp, BoundaryMPSDiagonal, BoundaryMPSRowVariational, ResamplingOptions,
+from .config import (Z2Space, Lattice, TFIM, FullUpdate, BoundaryMPS, BoundaryMPSRow, BoundaryMPSZipUp, BoundaryMPSDiagonal, BoundaryMPSRowVariational, BoundaryMPSDiagonalVariational, ResamplingOptions,
                      SymmetryBasis, RunConfig, validate_config, temperature_nodes, parameter_dict)
 from .engine import (Engine, DeviceState, SamplingCache, normalize_state, evolution_step, lognorm,
                      measure_energy, sample_configuration, sample_batch, project_configuration,

@@ -106,6 +106,27 @@ class BoundaryMPSDiagonal(BoundaryMPS):
 
 
 @dataclass(frozen=True)
+class BoundaryMPSDiagonalVariational(BoundaryMPSDiagonal):
+    """``BoundaryMPSDiagonalVariational(chi; sector_space, max_sweep=4, threshold_sweep=1e-8,
+    target_cache_bytes)`` (``src/contraction/diagonal_variational.jl:12-30``): every
+    diagonal layer absorbed by a two-site variational fit; the engine keeps no
+    target-block cache, so ``target_cache_bytes`` is only validated."""
+    max_sweep: int = 4
+    threshold_sweep: float = 1e-8
+    target_cache_bytes: int = 256 * 1024 ** 2
+
+    def __post_init__(self):
+        if self.chi < 1:
+            raise ValueError("chi must be positive")
+        if self.max_sweep < 1:
+            raise ValueError("max_sweep must be positive")
+        if not (math.isfinite(self.threshold_sweep) and self.threshold_sweep >= 0):
+            raise ValueError("threshold_sweep must be finite and nonnegative")
+        if self.target_cache_bytes < 0:
+            raise ValueError("target_cache_bytes must be nonnegative")
+
+
+@dataclass(frozen=True)
 class BoundaryMPSRowVariational(BoundaryMPS):
     """``BoundaryMPSRowVariational(chi; sector_space, max_sweep=4, threshold_sweep=1e-8)``
     (``src/contraction/row_variational.jl:10-25``): every row absorbed by a
@@ -220,9 +241,11 @@ def temperature_nodes(c: RunConfig):
 
 def validate_config(c: RunConfig) -> RunConfig:
     """``validate_config`` (``config.jl:80-114``) for the row boundary-MPS path."""
-    if c.contraction not in (BoundaryMPS, BoundaryMPSDiagonal, BoundaryMPSRowVariational):
-        raise ValueError("this engine implements the row, diagonal and row variational boundary-MPS "
-                         "contractions (BoundaryMPS/BoundaryMPSRow, BoundaryMPSDiagonal, BoundaryMPSRowVariational)")
+    if c.contraction not in (BoundaryMPS, BoundaryMPSDiagonal, BoundaryMPSRowVariational,
+                             BoundaryMPSDiagonalVariational):
+        raise ValueError("this engine implements the row, diagonal and variational boundary-MPS contractions "
+                         "(BoundaryMPS/BoundaryMPSRow, BoundaryMPSDiagonal, BoundaryMPSRowVariational, "
+                         "BoundaryMPSDiagonalVariational)")
     grid = [c.beta0] + list(c.beta_log) + list(c.beta_measure)
     if not all(math.isfinite(b) and b >= 0 for b in grid):
         raise ValueError("invalid beta grid")
@@ -290,9 +313,10 @@ def parameter_dict(c: RunConfig) -> dict:
             return d
         return repr(x)
     d = {f.name: enc(getattr(c, f.name)) for f in fields(c)}
-    diagonal = c.contraction is BoundaryMPSDiagonal
-    d["contraction"] = ("BoundaryMPS-Diagonal" if diagonal else "BoundaryMPS-Row-Variational"
-                        if c.contraction is BoundaryMPSRowVariational else "BoundaryMPS-Row")
+    diagonal = issubclass(c.contraction, BoundaryMPSDiagonal)
+    d["contraction"] = {BoundaryMPSDiagonal: "BoundaryMPS-Diagonal",
+                        BoundaryMPSDiagonalVariational: "BoundaryMPS-Diagonal-Variational",
+                        BoundaryMPSRowVariational: "BoundaryMPS-Row-Variational"}.get(c.contraction, "BoundaryMPS-Row")
     d["sampling_site_order"] = (
         [(x + 1, y + 1) for x, y in diagonal_order(c.lattice.Lx, c.lattice.Ly)] if diagonal
         else [(x + 1, y + 1) for y in range(c.lattice.Ly) for x in range(c.lattice.Lx)])

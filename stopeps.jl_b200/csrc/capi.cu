@@ -58,10 +58,10 @@ BMPS to_bmps(const sps_handle* h, const sps_boundary* b) {
   m.chi = b->chi;
   m.space[0] = b->space0 >= 0 && b->space1 >= 0 ? b->space0 : -1;
   m.space[1] = b->space0 >= 0 && b->space1 >= 0 ? b->space1 : -1;
-  if (b->absorption < 0 || b->absorption > 3) throw Error(SPS_ERR_ARGUMENT, "unknown boundary absorption");
+  if (b->absorption < 0 || b->absorption > 4) throw Error(SPS_ERR_ARGUMENT, "unknown boundary absorption");
   m.zipup = b->absorption == 1;
-  m.diagonal = b->absorption == 2;
-  m.variational = b->absorption == 3;
+  m.diagonal = b->absorption == 2 || b->absorption == 4;
+  m.variational = b->absorption == 3 || b->absorption == 4;
   m.max_sweep = h->var_max_sweep;
   m.threshold_sweep = h->var_threshold_sweep;
   return m;

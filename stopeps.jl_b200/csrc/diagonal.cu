@@ -393,7 +393,11 @@ Compressed compress_blocks(Engine& E, std::vector<Tensor>& blocks, const Layout&
 // _diagonal_absorb_layer! (diagonal_mps.jl:272-297); site(x, y) gives the
 // tensor absorbed at a site
 template <class Site>
+void absorb_layer_variational(Net& n, DiagEnv& env, Site site, int t, const BMPS& m, bool reverse, Entropy* ent);
+
+template <class Site>
 void absorb_layer(Net& n, DiagEnv& env, Site site, int t, const BMPS& m, bool reverse, Entropy* ent) {
+  if (m.variational) return absorb_layer_variational(n, env, site, t, m, reverse, ent);
   if (m.chi < 1) throw Error(SPS_ERR_ARGUMENT, "chi must be positive");
   Layout L = layer_layout(n, env, t, reverse);
   std::vector<Tensor> blocks;
@@ -413,11 +417,572 @@ void absorb_layer(Net& n, DiagEnv& env, Site site, int t, const BMPS& m, bool re
     const bool right = blocks.size() < 2 ? !reverse : ((t % 2 == 0) != reverse);
     Compressed c = compress_blocks(n.E, blocks, L, m, right, reverse, ent, n.Lx);
     env.t = c.tensors;
+    env.center = right ? (int)c.tensors.size() - 1 : 0;
     env.max_trunc = std::max(env.max_trunc, c.max_trunc);
     scale += c.log_scale;
   }
   env.edges = L.edges;
   env.log_scale = scale;
+}
+
+// ---------------------------------------------------------------------------
+// BoundaryMPSDiagonalVariational (src/contraction/diagonal_variational.jl): a
+// layer absorbed by a two-site variational fit of the candidate frontier MPS
+// to the chain of raw site blocks, normalised to unit norm.  Cross-block
+// projections take the full two-site SVD (the reference's factored SVD keeps
+// the same space or falls back to it); the target-block cache only saves work.
+// ---------------------------------------------------------------------------
+
+const int TB = 1 << 22, CB = 1 << 23;   // target and candidate bond labels
+
+struct VFail : Error {   // _VariationalNumericalError
+  std::string reason;
+  explicit VFail(const std::string& r) : Error(SPS_ERR_NUMERIC, "variational boundary: " + r), reason(r) {}
+};
+
+struct VMsg {   // _VariationalMessage
+  LT m;
+  double ls = 0;
+};
+
+VMsg vmsg(Net& n, LT t, double ls = 0.0) {
+  double s;
+  if (t.number) {
+    s = std::fabs(t.s);
+  } else {
+    t.t = contiguous(n.E, t.t);
+    s = norm(n.E, t.t);
+  }
+  if (!std::isfinite(s)) throw VFail("nonfinite_overlap");
+  if (s == 0) return {t, -INFINITY};
+  if (t.number) {
+    t.s /= s;
+  } else {
+    t.t = clone(n.E, t.t);
+    scale_inplace(n.E, t.t, 1.0 / s);
+    t.unit = false;
+  }
+  return {t, ls + std::log(s)};
+}
+
+// _diagonal_coordinate (diagonal_variational.jl:52-60): twice the transverse
+// coordinate x - y of an edge's midpoint
+int coordinate(const Net& n, int e) {
+  const int nh = (n.Lx + 1) * n.Ly;
+  if (e <= nh) {
+    const int x = (e - 1) % (n.Lx + 1), y = (e - 1) / (n.Lx + 1);
+    return 2 * x - 1 - 2 * y;
+  }
+  const int r = e - 1 - nh, x = r % n.Lx, y = r / n.Lx;
+  return 2 * x - 2 * y + 1;
+}
+
+// _variational_identity of a single-layer leg p, on its fused (ket, bra) leg
+Tensor identity_leg(Engine& E, const Par& p) {
+  const int d = (int)p->size();
+  std::vector<double> v((size_t)d * d, 0.0);
+  for (int k = 0; k < d; ++k) v[(size_t)k * d + k] = 1.0 / std::sqrt((double)d);
+  return E.upload({fused_par({p, p})}, v.data());
+}
+
+// A without its one-dimensional leg `axis` (a view)
+Tensor drop_trivial(const Tensor& A, int axis) {
+  if (A.dims[axis] != 1) throw Error(SPS_ERR_ARGUMENT, "diagonal variational: leg is not trivial");
+  Tensor t = A;
+  t.legs.erase(t.legs.begin() + axis);
+  t.dims.erase(t.dims.begin() + axis);
+  t.strides.erase(t.strides.begin() + axis);
+  return t;
+}
+
+struct VTarget {   // _DiagonalLayerTarget (diagonal_variational.jl:96-217)
+  Net& n;
+  const DiagEnv& input;
+  int t;
+  bool reverse;
+  Layout L;
+  std::vector<int> owner;
+  std::vector<Par> physical;
+  std::vector<Par> single;     // the single-layer leg of each output edge
+  std::vector<std::array<Par, 4>> legs4;   // each site's virtual legs w, n, e, s
+  std::vector<Tensor> blocks;
+  double log_scale = 0, weight = 1;
+};
+
+double chain_lognorm(Engine& E, const std::vector<Tensor>& blocks) {   // _variational_chain_lognorm
+  Tensor carry;
+  bool have = false;
+  double total = 0;
+  for (const Tensor& B : blocks) {
+    Tensor A = have ? times_first(E, carry, B) : B;
+    std::vector<int> head;
+    for (int i = 0; i + 1 < A.rank(); ++i) head.push_back(i);
+    QRres f = qr(E, A, head, {A.rank() - 1});
+    Tensor R = contiguous(E, f.R);
+    const double s = norm(E, R);
+    if (!std::isfinite(s)) throw VFail("nonfinite_norm");
+    if (s == 0) return -INFINITY;
+    total += std::log(s);
+    R = clone(E, R);
+    scale_inplace(E, R, 1.0 / s);
+    carry = R;
+    have = true;
+  }
+  return total;
+}
+
+template <class Site>
+VTarget make_target(Net& n, const DiagEnv& inp, Site site, int t, bool reverse) {
+  VTarget g{n, inp, t, reverse, layer_layout(n, inp, t, reverse)};
+  g.log_scale = inp.log_scale;
+  std::vector<double> norms;
+  for (size_t j = 0; j < g.L.sites.size(); ++j) {
+    const int x = g.L.sites[j][0], y = g.L.sites[j][1];
+    const Tensor& A = site(x, y);
+    auto ports = n.ports(x, y);
+    g.legs4.push_back({A.legs[0], A.legs[1], A.legs[4], A.legs[5]});
+    for (int port : g.L.outputs[j]) {
+      const int axis = VAX[std::find(ports.begin(), ports.end(), port) - ports.begin()];
+      g.owner.push_back((int)j);
+      g.physical.push_back(fused_par({A.legs[axis], A.legs[axis]}));
+      g.single.push_back(A.legs[axis]);
+    }
+    Tensor B = raw_block(n, inp, A, x, y, g.L.inputs[j], g.L.outputs[j], reverse);
+    const double s = norm(n.E, B);
+    if (!std::isfinite(s)) throw Error(SPS_ERR_NUMERIC, "nonfinite variational target block");
+    if (s != 0) scale_inplace(n.E, B, 1.0 / s);
+    norms.push_back(s);
+    g.blocks.push_back(B);
+  }
+  bool zero = false;
+  double sumlog = 0;
+  for (double s : norms) {
+    zero |= s == 0;
+    if (s != 0) sumlog += std::log(s);
+  }
+  if (zero) {
+    g.log_scale = -INFINITY;
+  } else if (!g.L.edges.empty()) {
+    const double ln = chain_lognorm(n.E, g.blocks);
+    g.log_scale += sumlog + ln;
+    g.weight = std::isfinite(ln) ? std::exp(-ln / (double)g.blocks.size()) : 1.0;
+    for (Tensor& B : g.blocks) scale_inplace(n.E, B, g.weight);
+  } else {
+    g.log_scale += sumlog;
+  }
+  return g;
+}
+
+LT labelled_block(const VTarget& g, int j) {
+  std::vector<int> lab{TB + j};
+  lab.insert(lab.end(), g.L.outputs[j].begin(), g.L.outputs[j].end());
+  lab.push_back(TB + j + 1);
+  return labelled(g.blocks[j], lab);
+}
+
+VMsg vedge(VTarget& g, int ncand, bool left) {   // _variational_edge
+  return vmsg(g.n, join(g.n, g.n.unit(TB + (left ? 0 : (int)g.L.sites.size())), g.n.unit(CB + (left ? 0 : ncand))));
+}
+
+VMsg vstep(VTarget& g, const VMsg& m, int i, const Tensor& A, bool left) {   // _variational_step
+  const int j = g.owner[i];
+  const auto& rng = g.L.ranges[j];
+  LT E = m.m;
+  if (i == (left ? rng.front() : rng.back())) E = join(g.n, E, labelled_block(g, j));
+  E = join(g.n, E, labelled(A, {CB + i, g.L.edges[i], CB + i + 1}));
+  return vmsg(g.n, E, m.ls);
+}
+
+std::vector<VMsg> vmessages(VTarget& g, const DiagEnv& C, bool left) {
+  const int nc = (int)C.t.size();
+  std::vector<VMsg> out(nc + 1);
+  if (left) {
+    out[0] = vedge(g, nc, true);
+    for (int i = 0; i < nc; ++i) out[i + 1] = vstep(g, out[i], i, C.t[i], true);
+  } else {
+    out[nc] = vedge(g, nc, false);
+    for (int i = nc - 1; i >= 0; --i) out[i] = vstep(g, out[i + 1], i, C.t[i], false);
+  }
+  return out;
+}
+
+// _variational_pair: the two-site projection (cb_i, e_i, e_i+1, cb_i+2)
+Tensor vpair(VTarget& g, int i, const VMsg& L, const VMsg& R) {
+  LT E = L.m;
+  std::vector<int> js{g.owner[i], g.owner[i + 1]};
+  if (js[0] == js[1]) js.pop_back();
+  for (int j : js) {
+    const auto& rng = g.L.ranges[j];
+    if (rng.front() >= i && rng.back() <= i + 1) E = join(g.n, E, labelled_block(g, j));
+  }
+  E = join(g.n, E, R.m);
+  Tensor M = clone(g.n.E, contiguous(g.n.E, reordered(E, {CB + i, g.L.edges[i], g.L.edges[i + 1], CB + i + 2})));
+  scale_inplace(g.n.E, M, std::exp(L.ls + R.ls));
+  return M;
+}
+
+void vmove_center(Engine& E, DiagEnv& C, int target) {   // _diagonal_center!
+  while (C.center < target) {
+    const int i = C.center;
+    QRres f = qr(E, C.t[i], {0, 1}, {2});
+    C.t[i] = f.Q;
+    C.t[i + 1] = ein(E, "lk,kpr->lpr", f.R, C.t[i + 1]);
+    C.center++;
+  }
+  while (C.center > target) {
+    const int i = C.center;
+    LQres f = lq(E, C.t[i], {0}, {1, 2});
+    C.t[i] = f.Q;
+    C.t[i - 1] = ein(E, "lpk,kr->lpr", C.t[i - 1], f.L);
+    C.center--;
+  }
+}
+
+DiagEnv vproduct(VTarget& g) {   // _variational_product
+  DiagEnv C;
+  for (const Par& p : g.single) {
+    Tensor v = identity_leg(g.n.E, p);
+    Tensor u = v;
+    u.legs = {g.n.triv, v.legs[0], g.n.triv};
+    u.dims = {1, v.dims[0], 1};
+    u.strides = {v.dims[0], 1, 1};
+    C.t.push_back(u);
+  }
+  C.edges = g.L.edges;
+  C.center = 0;
+  return C;
+}
+
+
+// _variational_input_identity: the identity on the leg of the layer site
+// that takes `edge` as an input
+Tensor input_identity(VTarget& g, int edge) {
+  for (size_t j = 0; j < g.L.sites.size(); ++j) {
+    auto ports = g.n.ports(g.L.sites[j][0], g.L.sites[j][1]);
+    for (int k = 0; k < 4; ++k)
+      if (ports[k] == edge) return identity_leg(g.n.E, g.legs4[j][k]);
+  }
+  throw Error(SPS_ERR_ARGUMENT, "input edge missing from variational layer");
+}
+
+// _variational_warm_start (diagonal_variational.jl:238-301)
+DiagEnv vwarm_start(VTarget& g) {
+  Engine& E = g.n.E;
+  if (g.input.t.empty()) return vproduct(g);
+  DiagEnv C;
+  C.t = g.input.t;
+  C.edges = g.input.edges;
+  C.center = std::max(g.input.center, 0);
+  std::vector<int> coords, oldc;
+  for (int e : g.L.edges) coords.push_back(coordinate(g.n, e));
+  for (int e : C.edges) oldc.push_back(coordinate(g.n, e));
+  auto has = [&](int c) { return std::find(coords.begin(), coords.end(), c) != coords.end(); };
+  // an end edge that leaves the frontier is capped with the identity
+  while (!C.t.empty() && !has(oldc.front())) {
+    vmove_center(E, C, 0);
+    Tensor h = ein(E, "pr,p->r", drop_trivial(C.t[0], 0), input_identity(g, C.edges[0]));
+    C.t.erase(C.t.begin());
+    C.edges.erase(C.edges.begin());
+    oldc.erase(oldc.begin());
+    if (C.t.empty()) break;
+    C.t[0] = with_trivial(ein(E, "r,rps->ps", h, C.t[0]), 1, true, g.n.triv);
+    C.center = 0;
+  }
+  while (!C.t.empty() && !has(oldc.back())) {
+    vmove_center(E, C, (int)C.t.size() - 1);
+    Tensor h = ein(E, "lp,p->l", drop_trivial(C.t.back(), 2), input_identity(g, C.edges.back()));
+    C.t.pop_back();
+    C.edges.pop_back();
+    oldc.pop_back();
+    if (C.t.empty()) break;
+    C.t.back() = with_trivial(ein(E, "lpr,r->lp", C.t.back(), h), 1, false, g.n.triv);
+    C.center = (int)C.t.size() - 1;
+  }
+  if (C.t.empty()) return vproduct(g);
+  // physical maps: embeddings keep the canonical form, projections first
+  // move the centre there
+  for (int i = 0; i < (int)C.t.size(); ++i) {
+    const int j = (int)(std::find(coords.begin(), coords.end(), oldc[i]) - coords.begin());
+    if (j >= (int)coords.size()) throw Error(SPS_ERR_ARGUMENT, "variational warm start: frontier edge not matched");
+    const Par& P = C.t[i].legs[1];
+    const Par& Q = g.physical[j];
+    if (*P == *Q) continue;
+    bool projects = false;
+    for (int c = 0; c < 2; ++c) projects |= par_count(P, c) > par_count(Q, c);
+    if (projects) vmove_center(E, C, i);
+    const int nq = (int)Q->size(), np = (int)P->size();
+    std::vector<double> mm((size_t)nq * np, 0.0);
+    for (int c = 0; c < 2; ++c) {
+      std::vector<int> qi, pi;
+      for (int k = 0; k < nq; ++k)
+        if ((*Q)[k] == c) qi.push_back(k);
+      for (int k = 0; k < np; ++k)
+        if ((*P)[k] == c) pi.push_back(k);
+      for (size_t k = 0; k < std::min(qi.size(), pi.size()); ++k) mm[(size_t)qi[k] * np + pi[k]] = 1.0;
+    }
+    C.t[i] = ein(E, "qp,lpr->lqr", E.upload({Q, P}, mm.data()), C.t[i]);
+  }
+  DiagEnv product = vproduct(g);
+  while (oldc.front() > coords.front()) {
+    const int j = (int)(std::find(coords.begin(), coords.end(), oldc.front()) - coords.begin()) - 1;
+    if (j < 0 || j >= (int)coords.size()) throw Error(SPS_ERR_ARGUMENT, "variational warm start: frontier edge not matched");
+    C.t.insert(C.t.begin(), product.t[j]);
+    oldc.insert(oldc.begin(), coords[j]);
+    C.center++;
+  }
+  while (oldc.back() < coords.back()) {
+    const int j = (int)(std::find(coords.begin(), coords.end(), oldc.back()) - coords.begin()) + 1;
+    if (j <= 0 || j >= (int)coords.size()) throw Error(SPS_ERR_ARGUMENT, "variational warm start: frontier edge not matched");
+    C.t.push_back(product.t[j]);
+    oldc.push_back(coords[j]);
+  }
+  C.edges = g.L.edges;
+  C.t[C.center] = contiguous(E, C.t[C.center]);
+  const double s = norm(E, C.t[C.center]);
+  if (s == 0) return product;
+  if (!std::isfinite(s)) throw Error(SPS_ERR_NUMERIC, "nonfinite variational warm start");
+  C.t[C.center] = clone(E, C.t[C.center]);
+  scale_inplace(E, C.t[C.center], 1.0 / s);
+  return C;
+}
+
+double nonnegative_residual(double value, double scale) {
+  if (!std::isfinite(value)) throw VFail("nonfinite_residual");
+  if (!(value >= -512 * DBL_EPSILON * std::max(1.0, scale))) throw VFail("negative_residual");
+  return std::max(0.0, value);
+}
+
+// _variational_overlap_residual: |C - T|^2 with |T| = 1
+double overlap_residual(VTarget& g, const DiagEnv& C, bool left, const VMsg* terminal) {
+  VMsg term;
+  if (terminal) {
+    term = *terminal;
+  } else {
+    const int nc = (int)C.t.size();
+    term = vedge(g, nc, left);
+    for (int q = 0; q < nc; ++q) {
+      const int i = left ? q : nc - 1 - q;
+      term = vstep(g, term, i, C.t[i], left);
+    }
+  }
+  VMsg edge = vedge(g, (int)C.t.size(), !left);
+  LT v = join(g.n, term.m, edge.m);
+  if (!v.number) throw Error(SPS_ERR_ARGUMENT, "unclosed variational overlap");
+  const double overlap = v.s * std::exp(term.ls + edge.ls);
+  const double nc = norm(g.n.E, C.t[C.center]);
+  const double norm2 = nc * nc;
+  if (!(std::isfinite(overlap) && std::isfinite(norm2))) throw VFail("nonfinite_overlap");
+  return nonnegative_residual(1 + norm2 - 2 * overlap, std::max(norm2, 2 * std::fabs(overlap)));
+}
+
+struct HalfOut {
+  double maxdiscard = 0, norm2 = 0;
+  std::vector<VMsg> next;
+};
+
+// _variational_half_sweep! (diagonal_variational.jl:470-499)
+HalfOut vhalf_sweep(VTarget& g, DiagEnv& C, const BMPS& m, bool right, Entropy* ent, std::vector<double>& profile,
+                    const std::vector<VMsg>& fixed) {
+  Engine& E = g.n.E;
+  const int nc = (int)C.t.size();
+  HalfOut out;
+  VMsg rolling = vedge(g, nc, right);
+  out.next.assign(nc + 1, VMsg());
+  out.next[right ? 0 : nc] = rolling;
+  Trunc tr;
+  tr.chi = m.chi;
+  tr.space[0] = m.space[0];
+  tr.space[1] = m.space[1];
+  std::vector<double> last;
+  for (int q = 0; q + 1 < nc; ++q) {
+    const int i = right ? q : nc - 2 - q;
+    const VMsg& L = right ? rolling : fixed[i];
+    const VMsg& R = right ? fixed[i + 2] : rolling;
+    Tensor M = vpair(g, i, L, R);
+    SVDres f = svd(E, M, {0, 1}, {2, 3}, tr, ent != nullptr);
+    if (ent) {
+      ent->maximum = std::max(ent->maximum, f.entropy);
+      profile[i] = f.entropy;
+    }
+    if (f.norm == 0) throw VFail("zero_local_projection");
+    last = f.S[0];
+    last.insert(last.end(), f.S[1].begin(), f.S[1].end());
+    out.maxdiscard = std::max(out.maxdiscard, (f.err / f.norm) * (f.err / f.norm));
+    if (right) {
+      C.t[i] = f.U;
+      C.t[i + 1] = scale_leg(E, f.V, 0, last);
+    } else {
+      C.t[i] = scale_leg(E, f.U, 2, last);
+      C.t[i + 1] = f.V;
+    }
+    C.center = right ? i + 1 : i;
+    const int k = right ? i : i + 1;
+    rolling = vstep(g, rolling, k, C.t[k], right);
+    out.next[right ? k + 1 : k] = rolling;
+  }
+  for (double v : last) out.norm2 += v * v;
+  if (out.norm2 == 0) throw VFail("zero_local_projection");
+  return out;
+}
+
+// _variational_fit (diagonal_variational.jl:501-539)
+DiagEnv vfit(VTarget& g, const BMPS& m, Entropy* ent, VariationalRecord& rec, std::vector<double>& bestprofile) {
+  DiagEnv C = vwarm_start(g);
+  const int nc = (int)C.t.size();
+  const bool right = C.center < nc - 1 - C.center || (C.center == nc - 1 - C.center && !g.reverse);
+  vmove_center(g.n.E, C, right ? 0 : nc - 1);
+  std::vector<VMsg> fixed = vmessages(g, C, !right);
+  const double initial = overlap_residual(g, C, !right, &fixed[right ? 0 : nc]);
+  DiagEnv best = C;
+  double cost = initial, change = INFINITY, discard = 0, previous = NAN;
+  bestprofile.assign(std::max(0, nc - 1), NAN);
+  int reason = VariationalRecord::SWEEP_LIMIT, sweeps = 0;
+  for (int sweep = 1; sweep <= m.max_sweep; ++sweep) {
+    std::vector<double> profile(nc - 1, NAN);
+    sweeps = sweep;
+    double current = INFINITY;
+    std::string failure;
+    try {
+      HalfOut a = vhalf_sweep(g, C, m, right, ent, profile, fixed);
+      HalfOut b = vhalf_sweep(g, C, m, !right, ent, profile, a.next);
+      fixed = b.next;
+      discard = std::max(discard, std::max(a.maxdiscard, b.maxdiscard));
+      if (!(std::isfinite(b.norm2) && b.norm2 >= 0)) throw VFail("nonfinite_norm");
+      current = nonnegative_residual(1 - b.norm2, b.norm2);
+      if (!(current <= cost + 512 * DBL_EPSILON * std::max(1.0, cost))) throw VFail("residual_increase");
+      change = sweep == 1 ? INFINITY : std::fabs(b.norm2 - previous) / std::max({b.norm2, previous, DBL_MIN});
+      previous = b.norm2;
+    } catch (const VFail& ex) {
+      failure = ex.reason;
+    } catch (const Error& ex) {
+      if (ex.code != SPS_ERR_CONVERGENCE) throw;
+      failure = "factorization_failure";
+    }
+    if (!failure.empty()) {
+      rec.fallback = true;
+      rec.fallback_reason = failure;
+      reason = VariationalRecord::NUMERICAL_FALLBACK;
+      break;
+    }
+    if (current <= cost) {
+      best = C;
+      cost = current;
+      bestprofile = profile;
+    }
+    if (sweep > 1 && m.threshold_sweep > 0 && change <= m.threshold_sweep) {
+      reason = VariationalRecord::THRESHOLD_SWEEP;
+      break;
+    }
+  }
+  rec.sweeps = sweeps;
+  rec.relative_change = change;
+  rec.stop_reason = reason;
+  rec.initial_residual = initial;
+  rec.residual = cost;
+  rec.max_local_discarded_weight = discard;
+  return best;
+}
+
+// _diagonal_absorb_layer! for the variational method (diagonal_variational.jl:541-614)
+template <class Site>
+void absorb_layer_variational(Net& n, DiagEnv& env, Site site, int t, const BMPS& m, bool reverse, Entropy* ent) {
+  Engine& E = n.E;
+  if (m.chi < 1) throw Error(SPS_ERR_ARGUMENT, "chi must be positive");
+  if (m.max_sweep < 1) throw Error(SPS_ERR_ARGUMENT, "max_sweep must be positive");
+  VTarget g = make_target(n, env, site, t, reverse);
+  const int ne = (int)g.L.edges.size();
+  std::vector<double> profile(std::max(0, ne - 1), NAN);
+  VariationalRecord rec;
+  rec.layer = t;
+  rec.reverse = reverse;
+  DiagEnv C;
+  bool have = true;
+  if (g.log_scale == -INFINITY) {
+    if (ne == 0) {
+      C.scalar = 0;
+    } else {
+      C = vproduct(g);
+      C.t[C.center] = clone(E, C.t[C.center]);
+      scale_inplace(E, C.t[C.center], 0.0);
+    }
+    rec.stop_reason = VariationalRecord::ZERO_TARGET;
+    rec.residual = rec.initial_residual = NAN;
+  } else if (ne <= 1) {
+    if (ne == 0) {
+      if (g.blocks.size() != 1 || g.blocks[0].size() != 1) throw Error(SPS_ERR_ARGUMENT, "diagonal corner is not closed");
+      C.scalar = sum_all(E, g.blocks[0]);
+    } else {
+      C.t = {g.blocks[0]};
+      C.edges = g.L.edges;
+      C.center = 0;
+    }
+  } else if (g.L.sites.size() == 1) {
+    Trunc tr;
+    tr.chi = m.chi;
+    tr.space[0] = m.space[0];
+    tr.space[1] = m.space[1];
+    SVDres f = svd(E, g.blocks[0], {0, 1}, {2, 3}, tr, ent != nullptr);
+    if (ent) {
+      ent->maximum = std::max(ent->maximum, f.entropy);
+      profile[0] = f.entropy;
+    }
+    std::vector<double> sv(f.S[0]);
+    sv.insert(sv.end(), f.S[1].begin(), f.S[1].end());
+    C.t = {f.U, scale_leg(E, f.V, 0, sv)};
+    C.edges = g.L.edges;
+    C.center = 1;
+    rec.residual = rec.max_local_discarded_weight = f.err * f.err;
+  } else {
+    try {
+      C = vfit(g, m, ent, rec, profile);
+    } catch (const VFail& ex) {
+      have = false;
+      rec.stop_reason = VariationalRecord::NUMERICAL_FALLBACK;
+      rec.initial_residual = NAN;
+      rec.residual = INFINITY;
+      rec.fallback = true;
+      rec.fallback_reason = ex.reason;
+    }
+    if (rec.fallback) {   // _variational_recover: the SVD absorption of the same layer
+      DiagEnv alt = env;
+      alt.max_trunc = 0;
+      alt.variational.clear();
+      BMPS plain = m;
+      plain.variational = false;
+      absorb_layer(n, alt, site, t, plain, reverse, nullptr);
+      alt.t[alt.center] = clone(E, alt.t[alt.center]);
+      scale_inplace(E, alt.t[alt.center], std::exp(alt.log_scale - g.log_scale));
+      const double cost = overlap_residual(g, alt, true, nullptr);
+      if (!std::isfinite(cost)) throw VFail("failed_svd_fallback");
+      const bool use_svd = !have || cost < rec.residual;
+      if (use_svd) {
+        C = alt;
+        rec.residual = cost;
+      }
+      rec.max_local_discarded_weight = std::max(rec.max_local_discarded_weight, alt.max_trunc);
+      rec.used_svd = use_svd;
+    }
+  }
+  double scale = 1.0;
+  if (ne > 0) {
+    C.t[C.center] = contiguous(E, C.t[C.center]);
+    scale = norm(E, C.t[C.center]);
+    if (!std::isfinite(scale)) throw Error(SPS_ERR_NUMERIC, "nonfinite variational boundary norm");
+    if (scale != 0) {
+      C.t[C.center] = clone(E, C.t[C.center]);
+      scale_inplace(E, C.t[C.center], 1.0 / scale);
+    }
+  }
+  std::vector<VariationalRecord> records = env.variational;
+  records.push_back(rec);
+  const double mt = std::isnan(rec.residual) ? env.max_trunc : std::max(env.max_trunc, rec.residual);
+  env.t = C.t;
+  env.edges = C.edges;
+  env.center = C.center;
+  env.scalar = C.scalar;
+  env.log_scale = scale == 0 ? -INFINITY : g.log_scale + std::log(scale);
+  env.max_trunc = mt;
+  env.variational = records;
 }
 
 }  // namespace
@@ -429,7 +994,7 @@ LogNorm lognorm_diagonal(Engine& E, const State& s, const BMPS& m) {
   auto site = [&](int x, int y) -> const Tensor& { return s.at(x, y); };
   for (int t = 0; t < s.Lx + s.Ly - 1; ++t) absorb_layer(n, env, site, t, m, false, nullptr);
   const double v = std::log(positive_real(env.scalar, "norm")) + env.log_scale;
-  return {v + 2 * s.log_amplitude, v, env.max_trunc};
+  return {v + 2 * s.log_amplitude, v, env.max_trunc, env.variational};
 }
 
 // _diagonal_boundaries(side = :southeast) (diagonal_mps.jl:298-314)

@@ -51,6 +51,8 @@ struct VariationalRecord {
   double max_local_discarded_weight = 0;
   bool fallback = false;
   std::string fallback_reason;
+  double initial_residual = 0, residual = 0;   // diagonal method: |C - T|^2 before and after the fit
+  bool used_svd = false;                      // diagonal method: the fallback took the SVD absorption
 };
 
 struct State {       // FiniteState (src/states/finite.jl:27-49)
@@ -90,6 +92,8 @@ struct DiagEnv {     // DiagonalBoundary (diagonal_mps.jl:106-118)
   std::vector<int> edges;     // the frontier's edge labels
   double log_scale = 0, max_trunc = 0;
   double scalar = 1;          // the closed network after the last layer
+  int center = 0;             // the canonical centre
+  std::vector<VariationalRecord> variational;   // fit records of the diagonal variational method
 };
 
 struct Layer {       // a row entry: plain double layer or SlabColumn (boundary_mps.jl:212-215)

@@ -14,7 +14,7 @@ import json
 import numpy as np
 
 from . import _lib
-from .config import BoundaryMPS, BoundaryMPSDiagonal, BoundaryMPSRowVariational, BoundaryMPSZipUp, RunConfig, TFIM, FullUpdate, Z2Space
+from .config import BoundaryMPS, BoundaryMPSDiagonal, BoundaryMPSDiagonalVariational, BoundaryMPSRowVariational, BoundaryMPSZipUp, RunConfig, TFIM, FullUpdate, Z2Space
 
 
 def _arr(a, ctype):
@@ -31,8 +31,8 @@ def _boundary(m: BoundaryMPS, e=None):
     else:
         b.space0, b.space1 = int(m.sector_space.n0), int(m.sector_space.n1)
     b.absorption = 2 if isinstance(m, BoundaryMPSDiagonal) else 1 if isinstance(m, BoundaryMPSZipUp) else 0
-    if isinstance(m, BoundaryMPSRowVariational):
-        b.absorption = 3
+    if isinstance(m, (BoundaryMPSRowVariational, BoundaryMPSDiagonalVariational)):
+        b.absorption = 4 if isinstance(m, BoundaryMPSDiagonalVariational) else 3
         if e is not None:
             e.check(e.lib.sps_set_variational(e.h, int(m.max_sweep), float(m.threshold_sweep)))
     return b
@@ -352,7 +352,7 @@ def lognorm(state: DeviceState, contraction: BoundaryMPS):
     e = state.engine
     r = _lib.sps_lognorm_result()
     b = _boundary(contraction, e)
-    if isinstance(contraction, BoundaryMPSRowVariational):
+    if isinstance(contraction, (BoundaryMPSRowVariational, BoundaryMPSDiagonalVariational)):
         counts = (C.c_int32 * 4)()
         change = C.c_double()
         e.check(e.lib.sps_lognorm_variational(e.h, state.id, C.byref(b), C.byref(r), counts, C.byref(change)))

@@ -5,7 +5,9 @@
 The sweep count is fixed (``threshold_sweep = 0``, three round trips) so that
 rounding cannot move a stopping decision; lognorm, the energy, <X> and the
 Born draws then agree to 1e-10 (draws 1e-9) on the stored purified PEPOs at
-their truncating chi, and the fit summary matches.
+their truncating chi, and the fit summary matches; likewise the diagonal
+variational method (``src/contraction/diagonal_variational.jl``) against
+``oracle/diagonal_variational.py``.
 """
 import numpy as np
 import pytest
@@ -55,3 +57,32 @@ def test_variational_options_are_checked(sps):
         e.check(e.lib.sps_set_variational(e.h, 0, 1e-8))
     with pytest.raises(ValueError):
         sps.BoundaryMPSRowVariational(4, None, max_sweep=0)
+
+
+@pytest.mark.parametrize("case", CASES)
+def test_diagonal_variational_lognorm_energy_and_draws(sps, case):
+    """``BoundaryMPSDiagonalVariational`` (``diagonal_variational.jl``) against the
+    oracle's restatement with two fixed round trips per layer."""
+    from oracle import diagonal as dg, diagonal_variational as dv, model as md
+    g = golden(case)
+    e = sps.Engine(int(g["Lx"]), int(g["Ly"]), sps.TFIM(float(g["J"]), float(g["h"])))
+    st = upload_golden(sps, g, e)
+    ost = oracle_state(g)
+    chi, a, b = (int(v) for v in g["chi0"])
+    m = sps.BoundaryMPSDiagonalVariational(chi, None if a < 0 else sps.Z2Space(a, b), max_sweep=2,
+                                           threshold_sweep=0.0)
+    om = dv.BoundaryMPSDiagonalVariational(chi, None if a < 0 else (a, b), max_sweep=2, threshold_sweep=0.0)
+    ln, oln = sps.lognorm(st, m), dg.lognorm(ost, om)
+    assert rel(ln["log_norm"], oln["log_norm"]) < TOL
+    assert ln["boundary_variational"]["layers"] == len(oln["boundary_variational"]["layers"])
+    assert ln["boundary_variational"]["fallback_count"] == oln["boundary_variational"]["fallback_count"]
+    en = sps.measure_energy(st, m)
+    oe = dg.measure_energy(ost, md.TFIM(float(g["J"]), float(g["h"])), om)
+    for k in ("energy_per_site", "log_norm", "x_sum"):
+        assert rel(en[k], oe[k]) < TOL, (k, en[k], oe[k])
+    cache, ocache = sps.SamplingCache(st, m), dg.DiagonalSamplingCache(ost, om)
+    for u in g["uniforms"][:2]:
+        d = sps.sample_configuration(cache, uniforms=u)
+        od = dg.sample_configuration(ocache, uniforms=u)
+        np.testing.assert_array_equal(d["configuration"], np.asarray(od["configuration"]))
+        assert rel(d["log_probability"], od["log_probability"]) < 1e-9

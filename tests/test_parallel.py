@@ -34,6 +34,9 @@ class OracleOps:
         if type(m).__name__ == "BoundaryMPSRowVariational":
             from oracle import variational as va
             return va.BoundaryMPSRowVariational(m.chi, sp, m.max_sweep, m.threshold_sweep)
+        if type(m).__name__ == "BoundaryMPSDiagonalVariational":
+            from oracle import diagonal_variational as dv
+            return dv.BoundaryMPSDiagonalVariational(m.chi, sp, m.max_sweep, m.threshold_sweep)
         return self.bm.BoundaryMPS(m.chi, sp)
 
     @staticmethod
@@ -48,8 +51,9 @@ class OracleOps:
 
     def sampling_cache(self, state, method, kind="auxiliary"):
         from oracle import diagonal as dg, sampling as sp
+        from oracle import diagonal_variational as dv
         m = self._m(method)
-        if isinstance(m, dg.BoundaryMPSDiagonal):
+        if isinstance(m, (dg.BoundaryMPSDiagonal, dv.BoundaryMPSDiagonalVariational)):
             return dg.DiagonalSamplingCache(state, m, kind=kind)
         return sp.SamplingCache(state, m, kind=kind)
 
@@ -101,14 +105,17 @@ class OracleOps:
 
     def measure_energy(self, state, method):
         from oracle import diagonal as dg, sampling as sp
+        from oracle import diagonal_variational as dv
         m = self._m(method)
-        mod = dg if isinstance(m, dg.BoundaryMPSDiagonal) else sp
+        mod = dg if isinstance(m, (dg.BoundaryMPSDiagonal, dv.BoundaryMPSDiagonalVariational)) else sp
         return dict(mod.measure_energy(state, self.md.TFIM(self.c.model.J, self.c.model.h, self.c.model.fields), m))
 
     def lognorm(self, state, method):
         from oracle import diagonal as dg
+        from oracle import diagonal_variational as dv
         m = self._m(method)
-        return dict((dg if isinstance(m, dg.BoundaryMPSDiagonal) else self.bm).lognorm(state, m))
+        diag = isinstance(m, (dg.BoundaryMPSDiagonal, dv.BoundaryMPSDiagonalVariational))
+        return dict((dg if diag else self.bm).lognorm(state, m))
 
     def evolution_step(self, state, delta, D, method, space):
         u = self.c.update
@@ -365,3 +372,14 @@ def test_host_driver_with_row_variational_contraction(sps):
         for k in ("lnZ", "energy_per_site"):
             assert (math.isnan(a[k]) and math.isnan(b[k])) or abs(a[k] - b[k]) <= 1e-11 * max(1.0, abs(b[k]))
     assert sps.parameter_dict(c)["contraction"] == "BoundaryMPS-Row-Variational"
+    cd = sps.RunConfig(lattice=sps.Lattice(3, 2), model=sps.TFIM(1.0, 0.7),
+                       contraction=sps.BoundaryMPSDiagonalVariational, resampling=sps.ResamplingOptions(enabled=False),
+                       **kw)
+    sps.validate_config(cd)
+    ops = OracleOps(cd)
+    cpd = sps.run_purification(cd, ops=ops, identity=ops.identity)
+    for a, b in zip(cpd.purification, rows):
+        for k in ("lnZ", "energy_per_site"):
+            assert (math.isnan(a[k]) and math.isnan(b[k])) or abs(a[k] - b[k]) <= 1e-11 * max(1.0, abs(b[k]))
+    p = sps.parameter_dict(cd)
+    assert p["contraction"] == "BoundaryMPS-Diagonal-Variational" and p["sampling_site_order"][1] == (2, 1)
