@@ -132,3 +132,35 @@ def test_diagonal_full_update_step(sps, case):
     oe = dg.measure_energy(ops, model, om)
     assert rel(en["energy_per_site"], oe["energy_per_site"]) < 1e-9
     assert rel(en["log_norm"], oe["log_norm"]) < 1e-9
+
+
+def test_diagonal_forced_psd_repair_matches_oracle(sps):
+    """update_bond!'s PSD-repair branch forced on every bond of one step on
+    diagonal bond environments: the repaired metric from the diagonal bond
+    hole and the refit, against the oracle with the same bonds forced."""
+    from oracle import diagonal as dg, full_update as fu, model as md, sampling as osp
+    g = golden("pepo_2x3_D2.npz")
+    upd = sps.FullUpdate(max_iterations=8, linear_max_iterations=40)
+    e = sps.Engine(2, 3, sps.TFIM(float(g["J"]), float(g["h"])), update=upd)
+    st = upload_golden(sps, g, e)
+    pc = g["peps_cfg"]
+    chi = int(pc[3])
+    m = sps.BoundaryMPSDiagonal(chi, None)
+    cfg = g["configs"][0]
+    ps, _ = sps.project_configuration(st, cfg)
+    e.set_injection(force_repair=True)
+    try:
+        r = sps.evolution_step(ps, float(g["dtau"]), int(pc[0]), m, None)
+    finally:
+        e.set_injection()
+    assert r["repairs"] == r["bond_updates"] > 0
+    ops, _ = osp.project_configuration(oracle_state(g), np.asarray(cfg).tolist())
+    bonds = {((0, y), (1, y)) for y in range(3)} | {((x, y), (x, y + 1)) for x in range(2) for y in range(2)}
+    model = md.TFIM(float(g["J"]), float(g["h"]))
+    ro = fu.evolution_step(ops, model, float(g["dtau"]), int(pc[0]), fu.FullUpdate(max_iterations=8,
+                           linear_max_iterations=40), dg.BoundaryMPSDiagonal(chi), force_repair_bonds=bonds)
+    assert ro["repairs"] == r["repairs"]
+    assert rel(r["log_normalization_sum"], sum(v for _, v in ro["normalizations"])) < 1e-9
+    en = sps.measure_energy(ps, m)
+    oen = dg.measure_energy(ops, model, dg.BoundaryMPSDiagonal(chi))
+    assert rel(en["energy_per_site"], oen["energy_per_site"]) < 1e-9

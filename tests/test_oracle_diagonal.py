@@ -190,3 +190,22 @@ def test_purification_with_diagonal_environments_matches_exact_diagonalization(h
     assert abs(out[1]["energy_per_site"] - ex["energy_per_site"]) < tol
     assert abs(out[0]["lnZ"] - out[1]["lnZ"]) < 1e-10
     assert abs(out[0]["energy_per_site"] - out[1]["energy_per_site"]) < 1e-10
+
+
+def test_forced_repair_on_diagonal_environments_equals_row():
+    """update_bond!'s PSD-repair branch forced on every bond: the repaired
+    metric comes from the diagonal bond hole, which equals the row hole up to
+    scale, so a step without truncation matches the row method's step."""
+    from oracle import full_update as fu
+    m = md.TFIM(1.0, 0.9)
+    bonds = {((x, y), (x + 1, y)) for x in range(2) for y in range(3)}
+    bonds |= {((x, y), (x, y + 1)) for x in range(3) for y in range(2)}
+    out = []
+    for method in (bm.BoundaryMPS(400), dg.BoundaryMPSDiagonal(400)):
+        st = md.identity_pepo(3, 3)
+        md.normalize_state(st)
+        r = fu.evolution_step(st, m, 0.05, 4, fu.FullUpdate(), method, force_repair_bonds=bonds)
+        assert r["repairs"] == r["bond_updates"] == 24
+        e = sp.measure_energy(st, m, bm.BoundaryMPS(400))
+        out.append((e["log_norm"], e["energy_per_site"]))
+    assert abs(out[0][0] - out[1][0]) < 1e-11 and abs(out[0][1] - out[1][1]) < 1e-11
