@@ -1,8 +1,9 @@
 """stopeps_b200: the StoPEPS sample-ensemble hot path on one B200.
 
 The public names mirror the reference package StoPEPS.jl v0.2.0
-(``src/StoPEPS.jl:32-42``) for the row boundary-MPS path: the configuration
-types, the two drivers, the hot-path functions and the ensemble statistics.
+(``src/StoPEPS.jl:32-42``) for the sample-ensemble path: the configuration
+types, the row, diagonal and variational boundary methods, the two drivers,
+the hot-path functions and the ensemble statistics.
 The numerical work runs in ``libstopeps_gpu.so`` (C ABI in
 ``include/stopeps_gpu.h``).
 """

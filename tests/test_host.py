@@ -107,3 +107,39 @@ def test_stored_benchmark_state_layout(sps):
             par = par + p.reshape(sh)
         assert np.all(a[par % 2 == 1] == 0.0)
         assert np.linalg.norm(a) > 0
+
+
+@pytest.mark.parametrize("Lx,Ly", [(1, 1), (1, 4), (4, 1), (3, 2), (4, 5)])
+def test_diagonal_draw_order_matches_oracle(sps, Lx, Ly):
+    """``_diagonal_order``: the host's order (used for the parameter record and
+    the uniforms of a diagonal draw) is the oracle's, a permutation of the sites."""
+    from oracle import diagonal as dg
+    order = sps.config.diagonal_order(Lx, Ly)
+    assert order == dg.draw_order(Lx, Ly)
+    assert sorted(order) == sorted((x, y) for x in range(Lx) for y in range(Ly))
+
+
+def test_boundary_methods_and_parameter_records(sps):
+    """The boundary methods a RunConfig may name, their records
+    (``config.jl:129-136``) and their option checks."""
+    names = {sps.BoundaryMPS: ("BoundaryMPS-Row", "row_major"),
+             sps.BoundaryMPSDiagonal: ("BoundaryMPS-Diagonal",
+                                       "x+y_ascending; even_diagonal_x_ascending; odd_diagonal_x_descending"),
+             sps.BoundaryMPSRowVariational: ("BoundaryMPS-Row-Variational", "row_major"),
+             sps.BoundaryMPSDiagonalVariational: ("BoundaryMPS-Diagonal-Variational",
+                                                  "x+y_ascending; even_diagonal_x_ascending; "
+                                                  "odd_diagonal_x_descending")}
+    for cls, (name, order) in names.items():
+        c = sps.RunConfig(lattice=sps.Lattice(3, 2), contraction=cls)
+        sps.validate_config(c)
+        p = sps.parameter_dict(c)
+        assert p["contraction"] == name and p["contraction_order"] == order
+        assert isinstance(c.boundary("sampling"), cls)
+    with pytest.raises(ValueError):
+        sps.validate_config(sps.RunConfig(contraction=sps.BoundaryMPSZipUp))
+    for cls in (sps.BoundaryMPSRowVariational, sps.BoundaryMPSDiagonalVariational):
+        for bad in (dict(chi=0), dict(chi=4, max_sweep=0), dict(chi=4, threshold_sweep=float("nan"))):
+            with pytest.raises(ValueError):
+                cls(**bad)
+    with pytest.raises(ValueError):
+        sps.BoundaryMPSDiagonalVariational(4, target_cache_bytes=-1)
