@@ -71,7 +71,10 @@ def test_born_draws(sps, case):
 
 
 @pytest.mark.parametrize("case", CASES)
-def test_projection_and_evolution_step(sps, case):
+def test_projection(sps, case):
+    """project_configuration (born.jl:27-36): the per-site normalisations and
+    the projected PEPS's energy and log norm; the step itself is
+    test_evolution_step."""
     g = golden(case)
     e = _engine(sps, g)
     st = upload_golden(sps, g, e)
