@@ -90,6 +90,13 @@ def test_projection(sps, case):
 
 @pytest.mark.parametrize("case", CASES)
 def test_evolution_step(sps, case):
+    """One second-order full-update step of a projected PEPS against the
+    oracle's fixture: bond count, stop reasons, the log normalisation and the
+    stepped state's energy, log norm and <X> at 1e-9.  The bar is looser than
+    the contraction's 1e-10 because each ALS solve is an iterative Jacobi-PCG
+    (full_update.jl:371-400) that stops at a relative residual of 1e-9 (the
+    FullUpdate linear tolerance): device and oracle take the same iterations,
+    but their rounding moves the stopping residual at that level."""
     g = golden(case)
     upd = sps.FullUpdate(max_iterations=8, linear_max_iterations=40) if "2x3" in case else sps.FullUpdate()
     e = _engine(sps, g, update=upd)
