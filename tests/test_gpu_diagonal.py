@@ -164,3 +164,32 @@ def test_diagonal_forced_psd_repair_matches_oracle(sps):
     en = sps.measure_energy(ps, m)
     oen = dg.measure_energy(ops, model, dg.BoundaryMPSDiagonal(chi))
     assert rel(en["energy_per_site"], oen["energy_per_site"]) < 1e-9
+
+
+@pytest.mark.parametrize("contraction", ["BoundaryMPSDiagonal", "BoundaryMPSDiagonalVariational"])
+def test_pipeline_on_diagonal_boundaries_matches_the_oracle_ops(sps, contraction):
+    """``RunConfig(contraction=...)`` end to end on the device (purification on
+    diagonal bond environments, diagonal draws, projection, evolution and
+    measurement) against the same driver with the oracle as the numerical
+    ops: the same draws and the same curve."""
+    import os
+    import sys
+    sys.path.insert(0, os.path.dirname(os.path.abspath(__file__)))
+    from test_parallel import OracleOps
+    c = sps.RunConfig(lattice=sps.Lattice(2, 3), model=sps.TFIM(1.0, 0.7), beta0=0.1, beta_log=[0.1, 0.2],
+                      beta_measure=[0.1, 0.2], delta_tau_pur=0.05, delta_tau_peps=0.05, D_pur=2, D_peps=2,
+                      chi_environment=4, Ns=4, seed=3, contraction=getattr(sps, contraction),
+                      resampling=sps.ResamplingOptions(enabled=False))
+    dev = sps.run_stochastic(c, sps.run_purification(c))
+    ops = OracleOps(c)
+    ref = sps.run_stochastic(c, sps.run_purification(c, ops=ops, identity=ops.identity), ops=ops)
+    for d, o in zip(dev["diagnostics"]["born_draws"], ref["diagnostics"]["born_draws"]):
+        np.testing.assert_array_equal(d["configuration"], o["configuration"])
+        assert rel(d["log_probability"], o["log_probability"]) < 1e-9
+    curve = [r for r in dev["observables"]["curve"] if r.get("source") == "sampling"]
+    ocurve = [r for r in ref["observables"]["curve"] if r.get("source") == "sampling"]
+    assert len(curve) == len(ocurve) > 0
+    for a, b in zip(curve, ocurve):
+        assert rel(a["lnZ"], b["lnZ"]) < 1e-9
+        assert (np.isnan(a["energy_per_site"]) and np.isnan(b["energy_per_site"])) or \
+            rel(a["energy_per_site"], b["energy_per_site"]) < 1e-9

@@ -43,3 +43,24 @@ def test_uniform_fields_written_per_site(sps):
     b = sps.run_purification(sps.RunConfig(model=sps.TFIM(1.0, 1.3, fields=[1.3] * 6), **kw)).purification[-1]
     assert rel(a["lnZ"], b["lnZ"]) < 1e-13
     assert rel(a["energy_per_site"], b["energy_per_site"]) < 1e-13
+
+
+def test_pipeline_with_site_fields_matches_the_oracle_ops(sps):
+    """run_stochastic with per-site fields on the device against the same
+    driver with the oracle as the numerical ops."""
+    import os
+    import sys
+    sys.path.insert(0, os.path.dirname(os.path.abspath(__file__)))
+    from test_parallel import OracleOps
+    f = (0.5, 0.9, 0.7, 1.1, 0.6, 1.3)
+    c = sps.RunConfig(lattice=sps.Lattice(3, 2), model=sps.TFIM(1.0, 0.7, fields=f), beta0=0.1,
+                      beta_log=[0.1, 0.2], beta_measure=[0.1, 0.2], delta_tau_pur=0.05, delta_tau_peps=0.05,
+                      D_pur=2, D_peps=2, chi_environment=4, Ns=4, seed=3,
+                      resampling=sps.ResamplingOptions(enabled=False))
+    dev = sps.run_stochastic(c, sps.run_purification(c))
+    ops = OracleOps(c)
+    ref = sps.run_stochastic(c, sps.run_purification(c, ops=ops, identity=ops.identity), ops=ops)
+    for a, b in zip([r for r in dev["observables"]["curve"] if r.get("source") == "sampling"],
+                    [r for r in ref["observables"]["curve"] if r.get("source") == "sampling"]):
+        assert rel(a["lnZ"], b["lnZ"]) < 1e-9
+        assert rel(a["energy_per_site"], b["energy_per_site"]) < 1e-9

@@ -86,3 +86,26 @@ def test_diagonal_variational_lognorm_energy_and_draws(sps, case):
         od = dg.sample_configuration(ocache, uniforms=u)
         np.testing.assert_array_equal(d["configuration"], np.asarray(od["configuration"]))
         assert rel(d["log_probability"], od["log_probability"]) < 1e-9
+
+
+def test_pipeline_on_row_variational_boundaries_matches_the_oracle_ops(sps):
+    """``RunConfig(contraction=BoundaryMPSRowVariational)`` end to end on the
+    device against the same driver with the oracle as the numerical ops."""
+    import os
+    import sys
+    sys.path.insert(0, os.path.dirname(os.path.abspath(__file__)))
+    from test_parallel import OracleOps
+    c = sps.RunConfig(lattice=sps.Lattice(3, 2), model=sps.TFIM(1.0, 0.7), beta0=0.1, beta_log=[0.1, 0.2],
+                      beta_measure=[0.1, 0.2], delta_tau_pur=0.05, delta_tau_peps=0.05, D_pur=2, D_peps=2,
+                      chi_environment=4, Ns=4, seed=3, contraction=sps.BoundaryMPSRowVariational,
+                      resampling=sps.ResamplingOptions(enabled=False))
+    dev = sps.run_stochastic(c, sps.run_purification(c))
+    ops = OracleOps(c)
+    ref = sps.run_stochastic(c, sps.run_purification(c, ops=ops, identity=ops.identity), ops=ops)
+    for d, o in zip(dev["diagnostics"]["born_draws"], ref["diagnostics"]["born_draws"]):
+        np.testing.assert_array_equal(d["configuration"], o["configuration"])
+        assert rel(d["log_probability"], o["log_probability"]) < 1e-9
+    for a, b in zip([r for r in dev["observables"]["curve"] if r.get("source") == "sampling"],
+                    [r for r in ref["observables"]["curve"] if r.get("source") == "sampling"]):
+        assert rel(a["lnZ"], b["lnZ"]) < 1e-9
+        assert rel(a["energy_per_site"], b["energy_per_site"]) < 1e-9
