@@ -1254,7 +1254,11 @@ SampleResult sample_diagonal(Engine& E, const SamplingCache& c, const double* un
       if (physical) {
         std::vector<int> out(s.ports[k].begin(), s.ports[k].end());
         Tensor H = hole(n, left, right, s, {k}, out);
-        for (int i = 3; i >= 0; --i) H = split(E, H, i, {A.legs[VAX[i]], A.legs[VAX[i]]});
+        for (int i = 3; i >= 0; --i) {
+          if (*H.legs[i] != *fused_par({A.legs[VAX[i]], A.legs[VAX[i]]}))
+            throw Error(SPS_ERR_ARGUMENT, "diagonal site hole does not match the site's legs");
+          H = split(E, H, i, {A.legs[VAX[i]], A.legs[VAX[i]]});
+        }
         Tensor root = metric_root(E, H, res);
         double values[2] = {0, 0};
         for (int j = 0; j < 2; ++j) {
@@ -1498,7 +1502,11 @@ Tensor diag_bond_hole(Net& n, const DiagBond& d, const State& st) {
     }
   }
   Tensor H = hole(n, *d.left, *d.right, *d.strip, {d.a, d.b}, output);
-  for (int k = 5; k >= 0; --k) H = split(n.E, H, k, {outer[k], outer[k]});
+  for (int k = 5; k >= 0; --k) {
+    if (*H.legs[k] != *fused_par({outer[k], outer[k]}))
+      throw Error(SPS_ERR_ARGUMENT, "diagonal bond hole does not match the sites' legs");
+    H = split(n.E, H, k, {outer[k], outer[k]});
+  }
   return H;
 }
 
