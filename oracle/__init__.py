@@ -4,7 +4,8 @@ TEST INFRASTRUCTURE ONLY: the checker, never the product.  Only ``tests/``,
 ``__graft_entry__.smoke()`` and ``bench.py``'s CPU-baseline leg may import
 anything from this package.  It is a NumPy FP64 restatement of the
 reference's Julia files cited in each module (``z2``, ``model``,
-``boundary``, ``diagonal``, ``full_update``, ``sampling``, ``driver``).
+``boundary``, ``diagonal``, ``variational``, ``diagonal_variational``,
+``full_update``, ``sampling``, ``driver``).
 
 Parity status: the reference (pure Julia over TensorKit/MatrixAlgebraKit,
 neither installed here) ships no golden vectors and cannot be run in this
