@@ -209,3 +209,24 @@ def test_forced_repair_on_diagonal_environments_equals_row():
         e = sp.measure_energy(st, m, bm.BoundaryMPS(400))
         out.append((e["log_norm"], e["energy_per_site"]))
     assert abs(out[0][0] - out[1][0]) < 1e-11 and abs(out[0][1] - out[1][1]) < 1e-11
+
+
+@pytest.mark.parametrize("Lx,Ly", [(1, 3), (3, 1), (2, 2)])
+def test_physical_kind_on_narrow_lattices(Lx, Ly):
+    """The physical kind where layers hold a single site or the frontier
+    shrinks to one edge: the same distribution as the row method's at exact chi."""
+    st = _state(Lx, Ly)
+    cfg0 = [[1 + ((x + y) % 2) for y in range(Ly)] for x in range(Lx)]
+    peps, _ = sp.project_configuration(st, cfg0)
+    ca = sp.SamplingCache(peps, bm.BoundaryMPS(200), kind="physical")
+    cb = dg.DiagonalSamplingCache(peps, dg.BoundaryMPSDiagonal(200), kind="physical")
+    total = 0.0
+    for cfg in _configs(Lx, Ly):
+        p = sp.sample_configuration(ca, configuration=cfg)["log_probability"]
+        q = dg.sample_configuration(cb, configuration=cfg)["log_probability"]
+        if p == -math.inf:
+            assert q == -math.inf
+            continue
+        assert abs(p - q) < 1e-12
+        total += math.exp(q)
+    assert abs(total - 1.0) < 1e-12
