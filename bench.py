@@ -56,7 +56,7 @@ PROBES = """probes (one hot operation on a representative input, run once to war
   fustep [L]        one full-update Trotter step + energy, L x L D=6 chi=36 (default 8): both absorptions,
                     FP64 and 3xTF32 contractions
   purify [L] [s] [p] purification of the L x L TFIM to beta0 = 0.4 at D=6 chi=36 within s seconds
-                    (precision p), the state saved under gpurun_out/"""
+                    (precision p), the state saved under --out"""
 
 
 def parse():
@@ -70,6 +70,7 @@ def parse():
     p.add_argument("--no-pipeline", action="store_true", help="skip the full-update / measurement sub-lines")
     p.add_argument("--no-cpu", action="store_true", help="skip the CPU baseline sample")
     p.add_argument("--probe", nargs="+", metavar="NAME", help="run one probe instead of the benchmark")
+    p.add_argument("--out", default="probe_out", help="directory for files a probe writes")
     return p.parse_args()
 
 
@@ -519,7 +520,7 @@ def graded(m, n, decay, seed):
     return (u * np.exp(-decay * np.arange(min(m, n)))) @ v.T
 
 
-def probe(argv):
+def probe(argv, out="probe_out"):
     import numpy as np
     import __graft_entry__ as ge
     sps = ge.load_package()
@@ -692,8 +693,8 @@ def probe(argv):
             if time.perf_counter() - t0 > budget:
                 break
         sites, dims = st.download()
-        os.makedirs(os.path.join(ROOT, "gpurun_out"), exist_ok=True)
-        np.savez_compressed(os.path.join(ROOT, "gpurun_out", f"purified_{Ls}x{Ls}_D{D}_{prec}.npz"),
+        os.makedirs(os.path.join(ROOT, out), exist_ok=True)
+        np.savez_compressed(os.path.join(ROOT, out, f"purified_{Ls}x{Ls}_D{D}_{prec}.npz"),
                             data=np.concatenate([np.asarray(a).reshape(-1) for a in sites]), dims=np.asarray(dims),
                             beta=st.beta, log_amplitude=st.log_amplitude)
         en = sps.measure_energy(st, m)
@@ -706,7 +707,7 @@ def probe(argv):
 def main():
     args = parse()
     if args.probe:
-        probe(args.probe)
+        probe(args.probe, args.out)
         return
     rank = int(os.environ.get("RANK", 0))
     world = int(os.environ.get("WORLD_SIZE", 1))
