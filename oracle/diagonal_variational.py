@@ -19,7 +19,8 @@ bond for a cheaper SVD (``_variational_small_svd``) and checks that the
 factored SVD keeps the same space, else it takes the full SVD; the oracle
 takes the full two-site SVD everywhere (the same kept space and singular
 values).  The target-block cache (``target_cache_bytes``) only saves work and
-is not restated.
+is not restated, and of the Schmidt entropies only the maximum is kept (the
+reference also lists them per cut, ``northwest_cuts`` / ``southeast_cuts``).
 """
 from __future__ import annotations
 
