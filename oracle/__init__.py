@@ -5,7 +5,8 @@ TEST INFRASTRUCTURE ONLY: the checker, never the product.  Only ``tests/``,
 anything from this package.  It is a NumPy FP64 restatement of the
 reference's Julia files cited in each module (``z2``, ``model``,
 ``boundary``, ``diagonal``, ``variational``, ``diagonal_variational``,
-``full_update``, ``sampling``, ``driver``).
+``full_update``, ``sampling``, ``driver``, and ``adjoint``: the reverse-mode
+derivative of lognorm, which the reference does not have).
 
 Parity status: the reference (pure Julia over TensorKit/MatrixAlgebraKit,
 neither installed here) ships no golden vectors and cannot be run in this
