@@ -335,6 +335,24 @@ int sps_lognorm_variational(sps_handle* h, int32_t state_id, const sps_boundary*
   });
 }
 
+int sps_lognorm_gradient(sps_handle* h, int32_t state_id, const sps_boundary* method, double* log_norm,
+                         double* grads, int64_t capacity) {
+  return guarded(h, [&] {
+    State& s = get_state(h, state_id);
+    LognormGradient r = lognorm_gradient(*h->E, s, to_bmps(h, method));
+    if (log_norm) *log_norm = r.log_norm;
+    if (grads) {
+      int64_t off = 0;
+      for (auto& t : r.grads) {
+        if (off + t.size() > capacity) throw Error(SPS_ERR_ARGUMENT, "buffer too small");
+        auto v = h->E->download(t);
+        std::memcpy(grads + off, v.data(), v.size() * sizeof(double));
+        off += t.size();
+      }
+    }
+  });
+}
+
 int sps_set_site_fields(sps_handle* h, int32_t n, const double* fields) {
   return guarded(h, [&] {
     if (n == 0) {

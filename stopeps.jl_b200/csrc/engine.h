@@ -273,6 +273,9 @@ struct KeptSVD {
 };
 KeptSVD svd_kept(Engine& E, const Tensor& A, const std::vector<int>& rows, const std::vector<int>& cols,
                  const Trunc& tr, bool want_entropy, bool left);
+// the kept index sets of a truncation over per-block singular values (each
+// block descending): truncrank & truncspace & trunctol, as svd applies them
+void truncation_keep(const std::vector<double> s[2], const Trunc& tr, std::vector<char> keep[2]);
 // true when the kept-vector path (svd_kept) beats the full SVD for this view
 bool svd_prefers_kept(const Tensor& A, const std::vector<int>& rows, const std::vector<int>& cols, const Trunc& tr,
                       bool want_entropy);

@@ -244,6 +244,14 @@ void operator_pair(Engine& E, const Tensor& A, const Tensor& B, const Tensor& F,
                    Tensor& C, Tensor& D);
 double real_ratio(double a, double b);
 
+// reverse-mode derivative of the row lognorm with respect to the site
+// tensors (adjoint.cu; exact compression only)
+struct LognormGradient {
+  double log_norm = 0;
+  std::vector<Tensor> grads;   // per site x + y*Lx, legs of the site tensor
+};
+LognormGradient lognorm_gradient(Engine& E, const State& s, const BMPS& m);
+
 // diagonal boundary MPS (diagonal.cu; src/contraction/diagonal_mps.jl,
 // src/sampling/diagonal_born.jl, src/measurement/diagonal_energy.jl)
 LogNorm lognorm_diagonal(Engine& E, const State& s, const BMPS& m);

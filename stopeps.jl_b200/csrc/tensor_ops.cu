@@ -1353,6 +1353,10 @@ static std::vector<char> select_truncation(const std::vector<double> s[2], const
   return {};
 }
 
+void truncation_keep(const std::vector<double> s[2], const Trunc& tr, std::vector<char> keep[2]) {
+  select_truncation(s, tr, keep);
+}
+
 // Device value arrays to the host after one synchronisation: through the
 // pinned scalar scratch when they fit, else by plain copies after the sync.
 // The device flag is checked (and raised as an error) on the way.

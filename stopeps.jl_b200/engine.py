@@ -365,6 +365,31 @@ def lognorm(state: DeviceState, contraction: BoundaryMPS):
                 max_environment_truncation=r.max_environment_truncation)
 
 
+def lognorm_gradient(state: DeviceState, contraction: BoundaryMPS):
+    """lognorm (row method, exact compression) and its derivative with respect
+    to every site tensor by reverse mode: (log_norm, [gradient per site in
+    x + y*Lx order, shaped like the site tensor]).  No counterpart in the
+    reference, which has no derivatives."""
+    e = state.engine
+    L = e.Lx * e.Ly
+    dims = np.zeros(L * 12, np.int32)
+    tot = C.c_int64()
+    e.check(e.lib.sps_state_layout(e.h, state.id, _arr(dims, C.c_int32), C.byref(tot)))
+    grads = np.zeros(tot.value, np.float64)
+    value = C.c_double()
+    b = _boundary(contraction, e)
+    e.check(e.lib.sps_lognorm_gradient(e.h, state.id, C.byref(b), C.byref(value), _arr(grads, C.c_double),
+                                       tot.value))
+    dims = dims.reshape(L, 6, 2)
+    out, off = [], 0
+    for i in range(L):
+        shape = [int(a + c) for a, c in dims[i]]
+        n = int(np.prod(shape))
+        out.append(grads[off:off + n].reshape(shape))
+        off += n
+    return value.value, out
+
+
 def measure_energy(state: DeviceState, contraction: BoundaryMPS, site_profile=False):
     """``measure_energy``; also returns ``magnetization`` = <sum_i X_i>/N."""
     e = state.engine

@@ -14,13 +14,17 @@ def pytest_configure(config):
 
 # Device paths added most recently run after the established parity suite, so
 # that under ``-x`` a failure of theirs is reported without hiding the results
-# of the paths before them.  The order is otherwise unchanged.
+# of the paths before them; among themselves they run in the listed order.
+# The order is otherwise unchanged.
 LATE_MODULES = ("test_gpu_site_fields.py", "test_gpu_diagonal.py", "test_gpu_variational.py",
-                "test_gpu_repair.py")
+                "test_gpu_repair.py", "test_gpu_adjoint.py")
 
 
 def pytest_collection_modifyitems(config, items):
-    items.sort(key=lambda item: os.path.basename(str(item.fspath)) in LATE_MODULES)
+    def rank(item):
+        name = os.path.basename(str(item.fspath))
+        return LATE_MODULES.index(name) + 1 if name in LATE_MODULES else 0
+    items.sort(key=rank)
 
 
 @pytest.fixture(scope="session")

@@ -6,8 +6,8 @@ grow their allocator's pool).  This entry point takes the caller's device
 buffers and keeps its scratch in a fixed file-scope device array.  The test
 checks it against the allocating entry point sps_la_svd on two calls in a
 row (the shared array keeps the previous call's contents), within the SVD
-tolerance of the linear-algebra tests.  It runs last in collection order and
-passes alone or after the other tests.
+tolerance of the linear-algebra tests.  It passes alone or after the other
+tests.
 """
 import ctypes as C
 
