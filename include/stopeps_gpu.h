@@ -303,11 +303,14 @@ int sps_set_variational(sps_handle* h, int32_t max_sweep, double threshold_sweep
  * row method's exact compression (src/contraction/boundary_mps.jl:180-186)
  * and its derivative with respect to every site tensor by reverse mode
  * (QR-free: the canonical sweep by full SVDs, a gauge choice; the SVD reverse
- * rule per parity block with Lorentzian broadening).  grads receives the
- * derivatives in the layout of sps_state_download (sites x + y*Lx, each
- * row-major); capacity is its length in doubles. */
-int sps_lognorm_gradient(sps_handle* h, int32_t state_id, const sps_boundary* method, double* log_norm,
-                         double* grads, int64_t capacity);
+ * rule per parity block with Lorentzian broadening).  checkpoint_rows != 0
+ * keeps only each row's incoming boundary and recomputes the row's
+ * factorizations in the reverse pass (memory of one row's tape instead of
+ * all rows').  grads receives the derivatives in the layout of
+ * sps_state_download (sites x + y*Lx, each row-major); capacity is its
+ * length in doubles. */
+int sps_lognorm_gradient(sps_handle* h, int32_t state_id, const sps_boundary* method, int32_t checkpoint_rows,
+                         double* log_norm, double* grads, int64_t capacity);
 /* lognorm with the fit summary of a variational method
  * (row_variational.jl:331-339, _variational_summary): counts = {layers,
  * max_sweeps, sweep_limit_hits, fallback_count}; max_relative_change. */

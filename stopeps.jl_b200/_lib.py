@@ -110,7 +110,7 @@ def load():
         "sps_set_truncated_svd": ([vp, i32], C.c_int),
         "sps_set_site_fields": ([vp, i32, C.POINTER(C.c_double)], C.c_int),
         "sps_set_variational": ([vp, i32, C.c_double], C.c_int),
-        "sps_lognorm_gradient": ([vp, i32, P(sps_boundary), C.POINTER(C.c_double), C.POINTER(C.c_double),
+        "sps_lognorm_gradient": ([vp, i32, P(sps_boundary), i32, C.POINTER(C.c_double), C.POINTER(C.c_double),
                                   C.c_int64], C.c_int),
         "sps_lognorm_variational": ([vp, i32, C.POINTER(sps_boundary), C.POINTER(sps_lognorm_result),
                                      C.POINTER(C.c_int32), C.POINTER(C.c_double)], C.c_int),

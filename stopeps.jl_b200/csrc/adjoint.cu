@@ -11,6 +11,11 @@
 // the thin SVD's, per parity block, with the couplings 1 / (s_j^2 - s_i^2)
 // and 1 / s Lorentzian-broadened.  The truncated SVDs keep the leading
 // columns of the full ones, so discarded columns get zero cotangents.
+//
+// The tape of a row (its factorizations) is the memory of the reverse pass;
+// with checkpoint_rows only each row's incoming boundary is kept and the
+// row's factorizations are recomputed from it when the reverse pass reaches
+// it (the same operations on the same boundary give the same tape).
 #include "pipeline.h"
 #include <algorithm>
 #include <cfloat>
@@ -127,7 +132,7 @@ struct RowTape {
 
 }  // namespace
 
-LognormGradient lognorm_gradient(Engine& E, const State& s, const BMPS& m) {
+LognormGradient lognorm_gradient(Engine& E, const State& s, const BMPS& m, bool checkpoint_rows) {
   if (m.zipup || m.diagonal || m.variational)
     throw Error(SPS_ERR_ARGUMENT, "the lognorm derivative takes the row method's exact compression");
   const int Lx = s.Lx, Ly = s.Ly;
@@ -137,18 +142,13 @@ LognormGradient lognorm_gradient(Engine& E, const State& s, const BMPS& m) {
   tr.space[1] = m.space[1];
   std::vector<Tensor> layers(Lx * Ly);
   for (int i = 0; i < Lx * Ly; ++i) layers[i] = double_layer(E, s.sites[i], s.sites[i]);
-  std::vector<Tensor> firstrow(layers.begin(), layers.begin() + Lx);
-  std::vector<Tensor> env = trivial_boundary(E, firstrow, true).t;
-  double log_scale = 0;
-  std::vector<RowTape> tape(Ly);
-  for (int y = 0; y < Ly; ++y) {
-    RowTape& rt = tape[y];
-    rt.env = env;
-    rt.row.assign(layers.begin() + y * Lx, layers.begin() + (y + 1) * Lx);
+  // one row's absorption and compression, recorded in rt; returns the new
+  // boundary (centre normalised) and leaves the centre's norm in rt.scale
+  auto forward_row = [&](RowTape& rt) {
     std::vector<Tensor> B(Lx);
     for (int x = 0; x < Lx; ++x)
-      B[x] = fuse(E, fuse(E, ein(E, "lnr,wnep->lwpre", env[x], rt.row[x]), 3, 2), 0, 2);
-    rt.canon.resize(Lx);
+      B[x] = fuse(E, fuse(E, ein(E, "lnr,wnep->lwpre", rt.env[x], rt.row[x]), 3, 2), 0, 2);
+    rt.canon.assign(Lx, CanonStep());
     for (int x = Lx - 1; x >= 1; --x) {
       CanonStep& c = rt.canon[x];
       c.f = full_svd(E, B[x], {0}, {1, 2});
@@ -157,7 +157,7 @@ LognormGradient lognorm_gradient(Engine& E, const State& s, const BMPS& m) {
       B[x] = c.f.Vt;
       B[x - 1] = ein(E, "lpk,kr->lpr", B[x - 1], c.L);
     }
-    rt.sweep.resize(Lx);
+    rt.sweep.assign(Lx, SweepStep());
     for (int x = 0; x + 1 < Lx; ++x) {
       SweepStep& w = rt.sweep[x];
       w.f = full_svd(E, B[x], {0, 1}, {2});
@@ -198,8 +198,23 @@ LognormGradient lognorm_gradient(Engine& E, const State& s, const BMPS& m) {
     if (!(std::isfinite(rt.scale) && rt.scale > 0)) throw Error(SPS_ERR_NUMERIC, "nonfinite boundary norm");
     B[Lx - 1] = clone(E, B[Lx - 1]);
     scale_inplace(E, B[Lx - 1], 1.0 / rt.scale);
+    return B;
+  };
+  std::vector<Tensor> firstrow(layers.begin(), layers.begin() + Lx);
+  std::vector<Tensor> env = trivial_boundary(E, firstrow, true).t;
+  double log_scale = 0;
+  std::vector<RowTape> tape(Ly);
+  for (int y = 0; y < Ly; ++y) {
+    RowTape& rt = tape[y];
+    rt.env = env;
+    rt.row.assign(layers.begin() + y * Lx, layers.begin() + (y + 1) * Lx);
+    env = forward_row(rt);
     log_scale += std::log(rt.scale);
-    env = B;
+    if (checkpoint_rows) {   // keep the row's incoming boundary only
+      rt.canon.clear();
+      rt.sweep.clear();
+      rt.center = Tensor();
+    }
   }
   // close (_close_boundary) on the host: the last boundary has one-state
   // physical legs, V_{x+1} = V_x A_x[:, 0, :], value = sum V_Lx
@@ -234,6 +249,7 @@ LognormGradient lognorm_gradient(Engine& E, const State& s, const BMPS& m) {
   std::vector<Tensor> layerbar(Lx * Ly);
   for (int y = Ly - 1; y >= 0; --y) {
     RowTape& rt = tape[y];
+    if (checkpoint_rows) forward_row(rt);   // the same operations on the same boundary
     std::vector<Tensor> Bb = envbar;
     // centre normalisation: out = B / s, and log s enters the value with weight 1
     {
@@ -279,12 +295,16 @@ LognormGradient lognorm_gradient(Engine& E, const State& s, const BMPS& m) {
       for (int i = 0; i < K; ++i) sb[i] = ul[(size_t)i * K + i];
       Bb[x] = svd_backward(E, c.f, Ub, sb, Bb[x], 1);
     }
+    if (checkpoint_rows) {
+      rt.canon.clear();
+      rt.sweep.clear();
+    }
     for (int x = 0; x < Lx; ++x) {
       Tensor C = ein(E, "lnr,wnep->lwpre", rt.env[x], rt.row[x]);
-      Tensor Cb = contiguous(E, Bb[x]);
-      Cb.legs = C.legs;
-      Cb.dims = C.dims;
-      Cb.strides = C.strides;   // the fused legs are the row-major reshape of C's
+      // the fused legs are the row-major reshape of C's: split them back
+      if (Bb[x].size() != C.size()) throw Error(SPS_ERR_ARGUMENT, "lognorm derivative: boundary size");
+      Tensor Cb = split(E, contiguous(E, Bb[x]), 2, {C.legs[3], C.legs[4]});
+      Cb = split(E, Cb, 0, {C.legs[0], C.legs[1]});
       envbar[x] = ein(E, "lwpre,wnep->lnr", Cb, rt.row[x]);
       layerbar[x + y * Lx] = ein(E, "lwpre,lnr->wnep", Cb, rt.env[x]);
     }

@@ -335,11 +335,11 @@ int sps_lognorm_variational(sps_handle* h, int32_t state_id, const sps_boundary*
   });
 }
 
-int sps_lognorm_gradient(sps_handle* h, int32_t state_id, const sps_boundary* method, double* log_norm,
-                         double* grads, int64_t capacity) {
+int sps_lognorm_gradient(sps_handle* h, int32_t state_id, const sps_boundary* method, int32_t checkpoint_rows,
+                         double* log_norm, double* grads, int64_t capacity) {
   return guarded(h, [&] {
     State& s = get_state(h, state_id);
-    LognormGradient r = lognorm_gradient(*h->E, s, to_bmps(h, method));
+    LognormGradient r = lognorm_gradient(*h->E, s, to_bmps(h, method), checkpoint_rows != 0);
     if (log_norm) *log_norm = r.log_norm;
     if (grads) {
       int64_t off = 0;

@@ -250,7 +250,7 @@ struct LognormGradient {
   double log_norm = 0;
   std::vector<Tensor> grads;   // per site x + y*Lx, legs of the site tensor
 };
-LognormGradient lognorm_gradient(Engine& E, const State& s, const BMPS& m);
+LognormGradient lognorm_gradient(Engine& E, const State& s, const BMPS& m, bool checkpoint_rows = false);
 
 // diagonal boundary MPS (diagonal.cu; src/contraction/diagonal_mps.jl,
 // src/sampling/diagonal_born.jl, src/measurement/diagonal_energy.jl)

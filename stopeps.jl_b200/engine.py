@@ -365,11 +365,13 @@ def lognorm(state: DeviceState, contraction: BoundaryMPS):
                 max_environment_truncation=r.max_environment_truncation)
 
 
-def lognorm_gradient(state: DeviceState, contraction: BoundaryMPS):
+def lognorm_gradient(state: DeviceState, contraction: BoundaryMPS, checkpoint_rows=False):
     """lognorm (row method, exact compression) and its derivative with respect
     to every site tensor by reverse mode: (log_norm, [gradient per site in
-    x + y*Lx order, shaped like the site tensor]).  No counterpart in the
-    reference, which has no derivatives."""
+    x + y*Lx order, shaped like the site tensor]).  ``checkpoint_rows`` keeps
+    only each row's incoming boundary and recomputes the row's
+    factorizations in the reverse pass.  No counterpart in the reference,
+    which has no derivatives."""
     e = state.engine
     L = e.Lx * e.Ly
     dims = np.zeros(L * 12, np.int32)
@@ -378,7 +380,8 @@ def lognorm_gradient(state: DeviceState, contraction: BoundaryMPS):
     grads = np.zeros(tot.value, np.float64)
     value = C.c_double()
     b = _boundary(contraction, e)
-    e.check(e.lib.sps_lognorm_gradient(e.h, state.id, C.byref(b), C.byref(value), _arr(grads, C.c_double),
+    e.check(e.lib.sps_lognorm_gradient(e.h, state.id, C.byref(b), int(bool(checkpoint_rows)), C.byref(value),
+                                       _arr(grads, C.c_double),
                                        tot.value))
     dims = dims.reshape(L, 6, 2)
     out, off = [], 0

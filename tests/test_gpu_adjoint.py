@@ -52,3 +52,21 @@ def test_lognorm_gradient_takes_the_row_method_only(sps):
             sps.lognorm_gradient(st, m)
     value, _ = sps.lognorm_gradient(st, sps.BoundaryMPS(4))
     assert np.isfinite(value)
+
+
+def test_row_checkpoints_give_the_same_derivative(sps):
+    """With per-row checkpoints the reverse pass recomputes each row's
+    factorizations from its incoming boundary: the same operations on the same
+    boundary, so the derivative agrees with the full tape to roundoff (bar
+    1e-8 of the largest entry: the large-block SVD sums with floating-point
+    atomics, whose order may differ between the two passes)."""
+    g = golden("pepo_3x3_D4.npz")
+    e = sps.Engine(3, 3, sps.TFIM(float(g["J"]), float(g["h"])))
+    st = upload_golden(sps, g, e)
+    chi, a, b = (int(v) for v in g["chi0"])
+    m = sps.BoundaryMPS(chi, sps.Z2Space(a, b))
+    v0, g0 = sps.lognorm_gradient(st, m)
+    v1, g1 = sps.lognorm_gradient(st, m, checkpoint_rows=True)
+    assert abs(v1 - v0) <= 1e-12 * abs(v0)
+    for x0, x1 in zip(g0, g1):
+        assert np.abs(x1 - x0).max() <= 1e-8 * np.abs(x0).max()
