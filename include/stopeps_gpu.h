@@ -311,6 +311,15 @@ int sps_set_variational(sps_handle* h, int32_t max_sweep, double threshold_sweep
  * length in doubles. */
 int sps_lognorm_gradient(sps_handle* h, int32_t state_id, const sps_boundary* method, int32_t checkpoint_rows,
                          double* log_norm, double* grads, int64_t capacity);
+/* No counterpart in the reference.  The per-site field derivatives from one
+ * reverse pass of sps_lognorm_gradient: site_x[i] = <X_i> = half the
+ * derivative of lnZ along A_i -> A_i + e X A_i (X = diag(1, -1) on the
+ * physical leg), and d_fields[i] = d lnZ / dh_i = beta <X_i> for the thermal
+ * state exp(-beta H) the PEPO represents at its beta (the reference's direct
+ * route to the same numbers is one ratio per site, measure_energy's
+ * energy.jl:43-46).  site_x and d_fields hold Lx*Ly values (x + y*Lx). */
+int sps_lognorm_field_gradient(sps_handle* h, int32_t state_id, const sps_boundary* method, int32_t checkpoint_rows,
+                               double* log_norm, double* site_x, double* d_fields);
 /* lognorm with the fit summary of a variational method
  * (row_variational.jl:331-339, _variational_summary): counts = {layers,
  * max_sweeps, sweep_limit_hits, fallback_count}; max_relative_change. */

@@ -271,3 +271,20 @@ def lognorm_with_gradient(state, chi, space=None):
             g = np.einsum("wWnNeEsS,WNpaES->wnpaes", raw, A.a) + np.einsum("wWnNeEsS,wnpaes->WNpaES", raw, A.a)
             grads[x][y] = g
     return value, grads
+
+
+def field_gradient(state, chi, space=None):
+    """Per-site <X_i> from one reverse pass (half the derivative of lnZ along
+    A_i -> A_i + e X A_i, X on the physical leg) and d lnZ/dh_i = beta <X_i>
+    of the thermal state the PEPO represents: (value, site_x[x, y],
+    d_fields in x + y*Lx order).  The reference's direct route to <X_i> is one
+    ratio per site (``src/measurement/energy.jl:43-46``)."""
+    from . import model as md
+    X = md.spin_operators()[0]
+    value, g = lognorm_with_gradient(state, chi, space)
+    site_x = np.zeros((state.Lx, state.Ly))
+    for x in range(state.Lx):
+        for y in range(state.Ly):
+            XA = np.einsum("pu,wnuaes->wnpaes", X, state[x, y].a)
+            site_x[x, y] = 0.5 * float(np.sum(g[x][y] * XA))
+    return value, site_x, state.beta * site_x.T.reshape(-1)

@@ -9,7 +9,7 @@ The numerical work runs in ``libstopeps_gpu.so`` (C ABI in
 """
 from .config import (Z2Space, Lattice, TFIM, FullUpdate, BoundaryMPS, BoundaryMPSRow, BoundaryMPSZipUp, BoundaryMPSDiagonal, BoundaryMPSRowVariational, BoundaryMPSDiagonalVariational, ResamplingOptions,
                      SymmetryBasis, RunConfig, validate_config, temperature_nodes, parameter_dict)
-from .engine import (Engine, DeviceState, SamplingCache, normalize_state, evolution_step, lognorm, lognorm_gradient,
+from .engine import (Engine, DeviceState, SamplingCache, normalize_state, evolution_step, lognorm, lognorm_gradient, lognorm_field_gradient,
                      measure_energy, sample_configuration, sample_batch, project_configuration,
                      project_batch, evolution_step_batch, measure_energy_batch, lognorm_batch,
                      sample_conditionals, sample_probability_batch)
@@ -28,7 +28,7 @@ from . import bench_states
 __all__ = [
     "Z2Space", "Lattice", "TFIM", "FullUpdate", "BoundaryMPS", "BoundaryMPSRow", "ResamplingOptions",
     "SymmetryBasis", "RunConfig", "validate_config", "temperature_nodes", "parameter_dict", "Engine",
-    "DeviceState", "SamplingCache", "normalize_state", "evolution_step", "lognorm", "lognorm_gradient", "measure_energy",
+    "DeviceState", "SamplingCache", "normalize_state", "evolution_step", "lognorm", "lognorm_gradient", "lognorm_field_gradient", "measure_energy",
     "sample_configuration", "sample_batch", "project_configuration", "project_batch", "evolution_step_batch",
     "measure_energy_batch", "lognorm_batch", "sample_conditionals", "sample_probability_batch",
     "run_purification", "run_stochastic",

@@ -17,7 +17,7 @@ EXPORTS = [
     "sps_identity_pepo", "sps_state_upload", "sps_state_layout", "sps_state_download",
     "sps_state_info", "sps_state_set_beta", "sps_state_copy", "sps_state_free",
     "sps_normalize_state", "sps_evolution_step", "sps_lognorm", "sps_measure_energy",
-    "sps_set_truncated_svd", "sps_set_site_fields", "sps_set_variational", "sps_lognorm_variational", "sps_lognorm_gradient", "sps_sampling_cache", "sps_sampling_cache_kind", "sps_sampling_cache_free", "sps_sample",
+    "sps_set_truncated_svd", "sps_set_site_fields", "sps_set_variational", "sps_lognorm_variational", "sps_lognorm_gradient", "sps_lognorm_field_gradient", "sps_sampling_cache", "sps_sampling_cache_kind", "sps_sampling_cache_free", "sps_sample",
     "sps_sample_probability", "sps_sample_probability_batch",
     "sps_sample_batch", "sps_project", "sps_set_profile", "sps_kernel_stats_json", "sps_timer_start",
     "sps_timer_stop", "sps_la_svd", "sps_la_qr", "sps_la_svd_noalloc", "sps_la_svd_left", "sps_la_svd_topk", "sps_la_gemm", "sps_set_concurrency",
@@ -110,6 +110,8 @@ def load():
         "sps_set_truncated_svd": ([vp, i32], C.c_int),
         "sps_set_site_fields": ([vp, i32, C.POINTER(C.c_double)], C.c_int),
         "sps_set_variational": ([vp, i32, C.c_double], C.c_int),
+        "sps_lognorm_field_gradient": ([vp, i32, P(sps_boundary), i32, C.POINTER(C.c_double),
+                                        C.POINTER(C.c_double), C.POINTER(C.c_double)], C.c_int),
         "sps_lognorm_gradient": ([vp, i32, P(sps_boundary), i32, C.POINTER(C.c_double), C.POINTER(C.c_double),
                                   C.c_int64], C.c_int),
         "sps_lognorm_variational": ([vp, i32, C.POINTER(sps_boundary), C.POINTER(sps_lognorm_result),

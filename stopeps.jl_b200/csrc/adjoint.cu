@@ -326,4 +326,20 @@ LognormGradient lognorm_gradient(Engine& E, const State& s, const BMPS& m, bool 
   return out;
 }
 
+FieldGradient lognorm_field_gradient(Engine& E, const State& s, const BMPS& m, bool checkpoint_rows) {
+  LognormGradient g = lognorm_gradient(E, s, m, checkpoint_rows);
+  FieldGradient out;
+  out.log_norm = g.log_norm;
+  const std::vector<double> X = {1.0, -1.0};   // X on the physical leg in the Z2 basis
+  for (size_t i = 0; i < s.sites.size(); ++i) {
+    const Tensor& A = s.sites[i];
+    if (A.dims[2] != 2) throw Error(SPS_ERR_ARGUMENT, "field derivative: the physical leg is not a spin");
+    // lnZ along A_i -> A_i + e X A_i grows by 2 e <X_i>
+    const double x = 0.5 * dot(E, g.grads[i], scale_leg(E, A, 2, X));
+    out.site_x.push_back(x);
+    out.d_fields.push_back(s.beta * x);
+  }
+  return out;
+}
+
 }  // namespace sps

@@ -353,6 +353,17 @@ int sps_lognorm_gradient(sps_handle* h, int32_t state_id, const sps_boundary* me
   });
 }
 
+int sps_lognorm_field_gradient(sps_handle* h, int32_t state_id, const sps_boundary* method, int32_t checkpoint_rows,
+                               double* log_norm, double* site_x, double* d_fields) {
+  return guarded(h, [&] {
+    State& s = get_state(h, state_id);
+    FieldGradient r = lognorm_field_gradient(*h->E, s, to_bmps(h, method), checkpoint_rows != 0);
+    if (log_norm) *log_norm = r.log_norm;
+    if (site_x) std::copy(r.site_x.begin(), r.site_x.end(), site_x);
+    if (d_fields) std::copy(r.d_fields.begin(), r.d_fields.end(), d_fields);
+  });
+}
+
 int sps_set_site_fields(sps_handle* h, int32_t n, const double* fields) {
   return guarded(h, [&] {
     if (n == 0) {

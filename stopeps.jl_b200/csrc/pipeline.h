@@ -251,6 +251,13 @@ struct LognormGradient {
   std::vector<Tensor> grads;   // per site x + y*Lx, legs of the site tensor
 };
 LognormGradient lognorm_gradient(Engine& E, const State& s, const BMPS& m, bool checkpoint_rows = false);
+// per-site <X_i> from one reverse pass (the derivative along X insertions)
+// and d lnZ/dh_i = beta <X_i> of the thermal state the PEPO represents
+struct FieldGradient {
+  double log_norm = 0;
+  std::vector<double> site_x, d_fields;
+};
+FieldGradient lognorm_field_gradient(Engine& E, const State& s, const BMPS& m, bool checkpoint_rows = false);
 
 // diagonal boundary MPS (diagonal.cu; src/contraction/diagonal_mps.jl,
 // src/sampling/diagonal_born.jl, src/measurement/diagonal_energy.jl)

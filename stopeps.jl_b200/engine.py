@@ -393,6 +393,22 @@ def lognorm_gradient(state: DeviceState, contraction: BoundaryMPS, checkpoint_ro
     return value.value, out
 
 
+def lognorm_field_gradient(state: DeviceState, contraction: BoundaryMPS, checkpoint_rows=False):
+    """Per-site field derivatives from one reverse pass of ``lognorm_gradient``:
+    ``site_x`` (<X_i>, half the derivative of lnZ along X insertions) and
+    ``d_fields`` (d lnZ/dh_i = beta <X_i> of the thermal state the PEPO
+    represents), x + y*Lx order.  The reference's direct route to the same
+    numbers is one ratio per site (``measure_energy``, ``energy.jl:43-46``)."""
+    e = state.engine
+    L = e.Lx * e.Ly
+    x, d = np.zeros(L, np.float64), np.zeros(L, np.float64)
+    value = C.c_double()
+    b = _boundary(contraction, e)
+    e.check(e.lib.sps_lognorm_field_gradient(e.h, state.id, C.byref(b), int(bool(checkpoint_rows)), C.byref(value),
+                                             _arr(x, C.c_double), _arr(d, C.c_double)))
+    return {"log_norm": value.value, "site_x": x.reshape(e.Ly, e.Lx).T.copy(), "d_fields": d}
+
+
 def measure_energy(state: DeviceState, contraction: BoundaryMPS, site_profile=False):
     """``measure_energy``; also returns ``magnetization`` = <sum_i X_i>/N."""
     e = state.engine

@@ -58,3 +58,34 @@ def test_gradient_along_x_insertions_is_twice_the_site_magnetisation():
         for y in range(3):
             XA = np.einsum("pu,wnuaes->wnpaes", X, st[x, y].a)
             assert abs(float(np.sum(g[x][y] * XA)) / 2 - e["site_x"][x, y]) < 1e-10
+
+
+def test_field_gradient_matches_finite_differences_of_the_purification():
+    """d lnZ/dh_i = beta <X_i> from one reverse pass against the central
+    difference (step 1e-4) of the purified lnZ in each site's field, on a 2x2
+    (exact chi): the Trotterized state is exp(-beta H_eff / 2) with H_eff
+    = H + O(delta_tau^2), so the two differ by the Trotter error alone,
+    measured 5.2e-6, 1.2e-6 and 2.2e-7 at delta_tau 0.025, 0.0125 and
+    0.00625 (the last is tested).  <X_i> from the reverse pass equals the
+    direct per-site ratio to 1e-10."""
+    rng = np.random.default_rng(7)
+    fields = tuple(3.0 + rng.uniform(-0.05, 0.05, 4))
+
+    def run(f):
+        c = dr.RunConfig(Lx=2, Ly=2, J=1.0, h=3.0, fields=f, beta0=0.2, beta_log=[0.2], beta_measure=[0.2],
+                         delta_tau_pur=0.00625, D_pur=4, D_peps=4, chi_environment=16, Ns=1)
+        return dr.run_purification(c)
+
+    st, rows = run(fields)
+    value, site_x, d_fields = ad.field_gradient(st, 16)
+    assert abs(value - rows[-1]["lnZ"]) < 1e-12 * abs(value)
+    e = sp.measure_energy(st, md.TFIM(1.0, 3.0, fields), bm.BoundaryMPS(16))
+    assert np.abs(site_x - e["site_x"]).max() < 1e-10
+    step = 1e-4
+    for i in range(4):
+        lz = []
+        for s in (+1, -1):
+            f = list(fields)
+            f[i] += s * step
+            lz.append(run(tuple(f))[1][-1]["lnZ"])
+        assert abs((lz[0] - lz[1]) / (2 * step) - d_fields[i]) < 5e-7
