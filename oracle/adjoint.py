@@ -126,6 +126,38 @@ def _lq_backward(info, Lbar: T, Qbar: T):
     return _scatter(v, grads, legs, [0, 1, 2])
 
 
+def _svdc_forward(t: T):
+    """Canonical step by a full thin SVD over (leg 0 | legs 1, 2) per block:
+    L = U S, Q = V^T (the gauge the device's canonical sweep takes)."""
+    v = _blocks(t, [0], [1, 2])
+    full = []
+    for c in (0, 1):
+        b = v.blocks[c]
+        if min(b.shape) == 0:
+            full.append((np.zeros((b.shape[0], 0)), np.zeros(0), np.zeros((0, b.shape[1]))))
+        else:
+            full.append(np.linalg.svd(b, full_matrices=False))
+    nl = z2.newleg(len(full[0][1]), len(full[1][1]))
+    L = z2.from_blocks([u * s[None, :] for u, s, _ in full], v.rp, [nl])
+    Q = z2.from_blocks([vt for _, _, vt in full], [nl], v.cp)
+    return L, Q, (v, full, t.p)
+
+
+def _svdc_backward(info, Lbar: T, Qbar: T):
+    """L = U S: Ubar = Lbar S, sbar = diag(U^T Lbar); Q = V^T: (V^T)bar = Qbar."""
+    v, full, legs = info
+    lb = z2.MatView(Lbar, [0], [1]).blocks
+    qb = z2.MatView(Qbar, [0], [1, 2]).blocks
+    grads = []
+    for c in (0, 1):
+        u, s, vt = full[c]
+        if s.size == 0:
+            grads.append(None)
+            continue
+        grads.append(_svd_backward(v.blocks[c], u, s, vt, lb[c] * s[None, :], np.sum(u * lb[c], axis=0), qb[c]))
+    return _scatter(v, grads, legs, [0, 1, 2])
+
+
 def _svd_forward(t: T, chi, space):
     """Truncated SVD over (legs 0, 1 | leg 2) per block, recorded."""
     v = _blocks(t, [0, 1], [2])
@@ -167,10 +199,16 @@ def _svd_backward_blocks(info, Ubar: T, sbar, Vbar: T):
     return _scatter(v, grads, legs, [0, 1, 2])
 
 
-def lognorm_with_gradient(state, chi, space=None):
+def lognorm_with_gradient(state, chi, space=None, canonical="lq"):
     """``lognorm`` of a state with the row method's exact compression and
     its derivative with respect to every site tensor: (value, grads) with
-    grads[x][y] shaped like the site tensor."""
+    grads[x][y] shaped like the site tensor.  ``canonical`` is the gauge of
+    the exact canonical sweep: "lq" as the reference, or "svd" (L = U S,
+    Q = V^T), the device's; the truncated boundary does not depend on it."""
+    if canonical not in ("lq", "svd"):
+        raise ValueError("canonical is 'lq' or 'svd'")
+    canon_forward, canon_backward = (_lq_forward, _lq_backward) if canonical == "lq" else \
+        (_svdc_forward, _svdc_backward)
     from . import boundary as bm
     Lx, Ly = state.Lx, state.Ly
     sites = [[state[x, y] for y in range(Ly)] for x in range(Lx)]
@@ -187,7 +225,7 @@ def lognorm_with_gradient(state, chi, space=None):
         rec = dict(env=env, row=row, lq=[None] * Lx, svd=[None] * Lx)
         B = list(B0)
         for x in range(Lx - 1, 0, -1):
-            L, Q, info = _lq_forward(B[x])
+            L, Q, info = canon_forward(B[x])
             rec["lq"][x] = (info, B[x - 1], L)
             B[x] = Q
             B[x - 1] = einsum("lpk,kr->lpr", B[x - 1], L)
@@ -251,7 +289,7 @@ def lognorm_with_gradient(state, chi, space=None):
             Lbar = einsum("lpr,lpk->kr", G, Bprev)
             Bbar[x - 1] = einsum("lpr,kr->lpk", G, L)
             Qbar = Bbar[x]
-            Bbar[x] = T(_lq_backward(info, Lbar, Qbar), info[2])
+            Bbar[x] = T(canon_backward(info, Lbar, Qbar), info[2])
         # absorption: B0 = fuse(fuse(einsum(env, row)))
         newenv = [None] * Lx
         for x in range(Lx):

@@ -5,9 +5,10 @@ and the direct <X_i> ratios).
 
 The device canonicalizes by full SVDs where the oracle takes LQs (a gauge
 choice the truncated state does not see, but the Lorentzian broadening of the
-SVD reverse rule does, slightly): a CPU restatement of the device's sequence
-agrees with the oracle to 2e-16 on the 2x3 D=2 fixture and 2.3e-9 of each
-site gradient's largest entry on the 3x3 D=4 one, at chi0 and exact alike.
+SVD reverse rule does, slightly): the oracle with the device's gauge
+(``canonical="svd"``) agrees with its LQ gauge to 2e-16 on the 2x3 D=2
+fixture and 2.3e-9 of each site gradient's largest entry on the 3x3 D=4 one,
+at chi0 and exact alike.
 The bar here is 1e-7 of the largest entry (the oracle itself matches central
 finite differences to 1e-7); homogeneity (<d lnZ/dA_i, A_i> = 2) holds on the
 device to 1e-9.
