@@ -15,6 +15,7 @@ from .engine import (Engine, DeviceState, SamplingCache, normalize_state, evolut
                      sample_conditionals, sample_probability_batch)
 from .driver import (run_purification, run_stochastic, ensemble_statistics, group_configurations,
                      sample_uniforms, step_schedule, ThermalCheckpoint, Particle, RESULT_SCHEMA_VERSION)
+from .autodiff import LognormFunction, lognorm_differentiable
 from . import _lib
 from .build import build, LIB as LIBRARY_PATH
 from .parallel import SerialExecution, TorchExecution
@@ -28,7 +29,7 @@ from . import bench_states
 __all__ = [
     "Z2Space", "Lattice", "TFIM", "FullUpdate", "BoundaryMPS", "BoundaryMPSRow", "ResamplingOptions",
     "SymmetryBasis", "RunConfig", "validate_config", "temperature_nodes", "parameter_dict", "Engine",
-    "DeviceState", "SamplingCache", "normalize_state", "evolution_step", "lognorm", "lognorm_gradient", "lognorm_field_gradient", "measure_energy",
+    "DeviceState", "SamplingCache", "normalize_state", "evolution_step", "lognorm", "lognorm_gradient", "lognorm_field_gradient", "LognormFunction", "lognorm_differentiable", "measure_energy",
     "sample_configuration", "sample_batch", "project_configuration", "project_batch", "evolution_step_batch",
     "measure_energy_batch", "lognorm_batch", "sample_conditionals", "sample_probability_batch",
     "run_purification", "run_stochastic",

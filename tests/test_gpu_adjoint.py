@@ -97,3 +97,21 @@ def test_field_gradient_matches_direct_ratios_and_oracle(sps):
     ov, osx, odf = ad.field_gradient(oracle_state(g), chi, (a, b))
     assert abs(r["log_norm"] - ov) <= 1e-10 * abs(ov)
     assert np.abs(r["d_fields"] - odf).max() <= 1e-7 * np.abs(odf).max()
+
+
+def test_autograd_function_on_the_device(sps):
+    """torch.autograd through LognormFunction returns the device derivative
+    scaled by the cotangent."""
+    import torch
+    g = golden("pepo_2x3_D2.npz")
+    e = sps.Engine(int(g["Lx"]), int(g["Ly"]), sps.TFIM(float(g["J"]), float(g["h"])))
+    st = upload_golden(sps, g, e)
+    sites, dims = st.download()
+    m = sps.BoundaryMPS(4)
+    value, ref = sps.lognorm_gradient(st, m)
+    ts = [torch.tensor(s, dtype=torch.float64, requires_grad=True) for s in sites]
+    out = sps.lognorm_differentiable(e, ts, dims, m, beta=float(g["beta"]), log_amplitude=float(g["log_amplitude"]))
+    assert abs(out.item() - value) <= 1e-13 * abs(value)
+    grads = torch.autograd.grad(-2.0 * out, ts)
+    for a, b in zip(grads, ref):
+        assert np.abs(a.numpy() + 2.0 * b).max() <= 1e-12 * np.abs(b).max()
