@@ -56,7 +56,9 @@ PROBES = """probes (one hot operation on a representative input, run once to war
   fustep [L]        one full-update Trotter step + energy, L x L D=6 chi=36 (default 8): both absorptions,
                     FP64 and 3xTF32 contractions
   purify [L] [s] [p] purification of the L x L TFIM to beta0 = 0.4 at D=6 chi=36 within s seconds
-                    (precision p), the state saved under --out"""
+                    (precision p), the state saved under --out
+  adjoint [L] [D] [chi] lognorm and its reverse-mode derivative (full tape and row checkpoints) and the
+                    per-site field derivatives, on the seeded synthetic L x L PEPO (default 8, D=6, chi=36)"""
 
 
 def parse():
@@ -700,6 +702,29 @@ def probe(argv, out="probe_out"):
         en = sps.measure_energy(st, m)
         print(f"beta {st.beta}: E per site {en['energy_per_site']:.12f}, lnZ {en['log_norm']:.12f}, "
               f"total {time.perf_counter() - t0:.1f} s", flush=True)
+    elif which == "adjoint":
+        # lognorm, its reverse-mode derivative and the field derivatives on the seeded synthetic PEPO
+        Ls = int(argv[1]) if len(argv) > 1 else LX
+        Dd = int(argv[2]) if len(argv) > 2 else D
+        chi = int(argv[3]) if len(argv) > 3 else CHI
+        e = sps.Engine(Ls, Ls, sps.TFIM(1.0, H_FIELD))
+        sites, dims = sps.synthetic.synthetic_pepo(Ls, Ls, Dd, PEPO_EPS, PEPO_SEED)
+        st = e.upload_state(sites, dims, True, beta=1.0)
+        sps.normalize_state(st)
+        m = sps.BoundaryMPS(chi, sps.Z2Space(chi // 2, chi // 2))
+        for label, fn in (("lognorm", lambda: sps.lognorm(st, m)["log_norm"]),
+                          ("gradient", lambda: sps.lognorm_gradient(st, m)[0]),
+                          ("gradient, row checkpoints", lambda: sps.lognorm_gradient(st, m, checkpoint_rows=True)[0]),
+                          ("field gradient", lambda: sps.lognorm_field_gradient(st, m)["log_norm"])):
+            try:
+                fn()
+                t = time.perf_counter()
+                v = fn()
+                dt = time.perf_counter() - t
+                print(f"{Ls}x{Ls} D={Dd} chi={chi} {label}: {dt:.3f} s, lnZ {v:.12f}", flush=True)
+            except Exception as ex:
+                print(f"{Ls}x{Ls} D={Dd} chi={chi} {label}: {type(ex).__name__}: {ex}", flush=True)
+        e.close()
     else:
         raise SystemExit(f"unknown probe {which}\n{PROBES}")
 
