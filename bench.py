@@ -57,8 +57,9 @@ PROBES = """probes (one hot operation on a representative input, run once to war
                     FP64 and 3xTF32 contractions
   purify [L] [s] [p] purification of the L x L TFIM to beta0 = 0.4 at D=6 chi=36 within s seconds
                     (precision p), the state saved under --out
-  adjoint [L] [D] [chi] lognorm and its reverse-mode derivative (full tape and row checkpoints) and the
-                    per-site field derivatives, on the seeded synthetic L x L PEPO (default 8, D=6, chi=36)"""
+  adjoint [L] [D] [chi] lognorm and its reverse-mode derivative (row checkpoints; the full tape where it
+                    fits in 60 GB) and the per-site field derivatives, on the seeded synthetic L x L PEPO
+                    (default 8, D=6, chi=36)"""
 
 
 def parse():
@@ -712,10 +713,18 @@ def probe(argv, out="probe_out"):
         st = e.upload_state(sites, dims, True, beta=1.0)
         sps.normalize_state(st)
         m = sps.BoundaryMPS(chi, sps.Z2Space(chi // 2, chi // 2))
-        for label, fn in (("lognorm", lambda: sps.lognorm(st, m)["log_norm"]),
-                          ("gradient", lambda: sps.lognorm_gradient(st, m)[0]),
-                          ("gradient, row checkpoints", lambda: sps.lognorm_gradient(st, m, checkpoint_rows=True)[0]),
-                          ("field gradient", lambda: sps.lognorm_field_gradient(st, m)["log_norm"])):
+        # the full tape holds about 4 absorbed-row tensors (chi D^2, D^2, chi D^2) per site for every row
+        # (about 130 GB at 8x8 D=6 chi=36); row checkpoints hold one row's
+        tape_gb = 4 * 8 * (chi * Dd * Dd) ** 2 * Dd * Dd * Ls * Ls / 1e9
+        variants = [("lognorm", lambda: sps.lognorm(st, m)["log_norm"]),
+                    ("gradient, row checkpoints", lambda: sps.lognorm_gradient(st, m, checkpoint_rows=True)[0]),
+                    ("field gradient, row checkpoints",
+                     lambda: sps.lognorm_field_gradient(st, m, checkpoint_rows=True)["log_norm"])]
+        if tape_gb < 60:
+            variants.append(("gradient, full tape", lambda: sps.lognorm_gradient(st, m)[0]))
+        else:
+            print(f"full tape skipped: about {tape_gb:.0f} GB", flush=True)
+        for label, fn in variants:
             try:
                 fn()
                 t = time.perf_counter()
