@@ -14,10 +14,11 @@ def pytest_configure(config):
 
 # Device paths added most recently run after the established parity suite, so
 # that under ``-x`` a failure of theirs is reported without hiding the results
-# of the paths before them; among themselves they run in the listed order.
+# of the paths before them; among themselves they run in the listed order
+# (the smallest changes to established paths first).
 # The order is otherwise unchanged.
-LATE_MODULES = ("test_gpu_site_fields.py", "test_gpu_diagonal.py", "test_gpu_variational.py",
-                "test_gpu_repair.py", "test_gpu_adjoint.py")
+LATE_MODULES = ("test_gpu_site_fields.py", "test_gpu_repair.py", "test_gpu_adjoint.py",
+                "test_gpu_variational.py", "test_gpu_diagonal.py")
 
 
 def pytest_collection_modifyitems(config, items):
