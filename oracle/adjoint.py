@@ -10,10 +10,11 @@ LQ sweep, the truncated SVD sweep and the centre normalisation) and
 piece of per-site-field gradients, which chain through it.
 
 Each factorization is differentiated per parity block of its matrix view:
-QR / LQ by the standard reverse rule (with the wide-matrix split), the
-truncated SVD through the thin full SVD with the discarded columns' cotangents
-zero, the coupling 1 / (s_j^2 - s_i^2) Lorentzian-broadened,
-(s_j^2 - s_i^2) / ((s_j^2 - s_i^2)^2 + eps), and 1 / s as s / (s^2 + eps).
+the canonical sweep by a full SVD (default) or by QR / LQ (the standard
+reverse rule with the wide-matrix split), the truncated SVD through the thin
+full SVD with the discarded columns' cotangents zero.  The SVD couplings
+1 / (s_j^2 - s_i^2) are split into 1 / (s_j - s_i) and 1 / (s_j + s_i) terms,
+each Lorentzian-broadened, d / (d^2 + eps), and 1 / s is s / (s^2 + eps).
 The forward pass repeats ``boundary.lognorm`` (exact compression) and keeps
 what the backward pass needs.
 """
@@ -72,14 +73,22 @@ def _svd_backward(A, U, s, Vt, Ub, sb, Vtb):
     """Reverse rule of the thin SVD A = U diag(s) Vt, all min(m, n) values."""
     m, n = A.shape
     V, Vb = Vt.T, Vtb.T
-    s2 = s * s
-    diff = s2[None, :] - s2[:, None]                   # s_j^2 - s_i^2
-    F = diff / (diff * diff + BROADENING)
-    np.fill_diagonal(F, 0.0)
-    sinv = s / (s2 + BROADENING)
-    J = F * (U.T @ Ub - Ub.T @ U)
-    K = F * (V.T @ Vb - Vb.T @ V)
-    core = J * s[None, :] + s[:, None] * K + np.diag(sb)
+    # the couplings (A_ij s_j + s_i B_ij) / (s_j^2 - s_i^2), A = U^T Ub - Ub^T U,
+    # B = V^T Vb - Vb^T V, split as (A + B)_ij / 2 (s_j - s_i) + (A - B)_ij / 2
+    # (s_j + s_i): for a gauge-invariant function A + B vanishes with s_j - s_i,
+    # so the broadening of 1 / (s_j - s_i) only removes rounding noise
+    dm = s[None, :] - s[:, None]
+    dp = s[None, :] + s[:, None]
+    Fm = dm / (dm * dm + BROADENING)
+    Fp = dp / (dp * dp + BROADENING)
+    np.fill_diagonal(Fm, 0.0)
+    np.fill_diagonal(Fp, 0.0)
+    X = U.T @ Ub
+    Y = V.T @ Vb
+    Aa = X - X.T
+    Bb = Y - Y.T
+    core = 0.5 * Fm * (Aa + Bb) + 0.5 * Fp * (Aa - Bb) + np.diag(sb)
+    sinv = s / (s * s + BROADENING)
     Ab = U @ core @ Vt
     if m > len(s):
         Ab += (np.eye(m) - U @ U.T) @ Ub * sinv[None, :] @ Vt
@@ -199,12 +208,16 @@ def _svd_backward_blocks(info, Ubar: T, sbar, Vbar: T):
     return _scatter(v, grads, legs, [0, 1, 2])
 
 
-def lognorm_with_gradient(state, chi, space=None, canonical="lq"):
+def lognorm_with_gradient(state, chi, space=None, canonical="svd"):
     """``lognorm`` of a state with the row method's exact compression and
     its derivative with respect to every site tensor: (value, grads) with
     grads[x][y] shaped like the site tensor.  ``canonical`` is the gauge of
-    the exact canonical sweep: "lq" as the reference, or "svd" (L = U S,
-    Q = V^T), the device's; the truncated boundary does not depend on it."""
+    the exact canonical sweep: "svd" (L = U S, Q = V^T, the device's) or
+    "lq" as the reference's forward pass; the truncated boundary and the value
+    do not depend on it.  The LQ reverse rule solves with L, so on boundaries
+    whose blocks are numerically rank deficient (synthetic 4x4 D=4 states)
+    it loses accuracy (1e-4 against central differences) where the SVD rule,
+    regularised by the broadening, keeps 1e-9."""
     if canonical not in ("lq", "svd"):
         raise ValueError("canonical is 'lq' or 'svd'")
     canon_forward, canon_backward = (_lq_forward, _lq_backward) if canonical == "lq" else \

@@ -9,8 +9,11 @@
 // forward pass here canonicalizes with a full SVD (L = U S, Q = V^T) where the
 // reference takes an LQ; every factorization then shares one reverse rule:
 // the thin SVD's, per parity block, with the couplings 1 / (s_j^2 - s_i^2)
-// and 1 / s Lorentzian-broadened.  The truncated SVDs keep the leading
-// columns of the full ones, so discarded columns get zero cotangents.
+// split into 1 / (s_j - s_i) and 1 / (s_j + s_i) terms; those and 1 / s are
+// Lorentzian-broadened.  (The LQ reverse rule solves with L and loses
+// accuracy on numerically rank-deficient boundary blocks; the broadened SVD
+// rule does not.)  The truncated SVDs keep the leading columns of the full
+// ones, so discarded columns get zero cotangents.
 //
 // The tape of a row (its factorizations) is the memory of the reverse pass;
 // with checkpoint_rows only each row's incoming boundary is kept and the
@@ -80,22 +83,29 @@ Tensor svd_backward(Engine& E, const FullSVD& f, const Tensor& Ub, const std::ve
                     int nrow) {
   const std::string ru = nrow == 2 ? "lp" : "l", cv = nrow == 2 ? "r" : "pr";
   const int K = (int)f.s.size();
-  std::vector<double> F((size_t)K * K, 0.0), D((size_t)K * K, 0.0), sinv(K);
+  // the couplings (A_ij s_j + s_i B_ij) / (s_j^2 - s_i^2), A = U^T Ub - Ub^T U,
+  // B = V^T Vb - Vb^T V, split as (A + B)_ij / 2 (s_j - s_i) + (A - B)_ij / 2
+  // (s_j + s_i): for a gauge-invariant function A + B vanishes with s_j - s_i,
+  // so the broadening of 1 / (s_j - s_i) only removes rounding noise
+  std::vector<double> Fmv((size_t)K * K, 0.0), Fpv((size_t)K * K, 0.0), D((size_t)K * K, 0.0), sinv(K);
   for (int i = 0; i < K; ++i) {
     D[(size_t)i * K + i] = sb[i];
     sinv[i] = f.s[i] / (f.s[i] * f.s[i] + BROADENING);
     for (int j = 0; j < K; ++j)
       if (i != j) {
-        const double d = f.s[j] * f.s[j] - f.s[i] * f.s[i];
-        F[(size_t)i * K + j] = d / (d * d + BROADENING);
+        const double dm = f.s[j] - f.s[i], dp = f.s[j] + f.s[i];
+        Fmv[(size_t)i * K + j] = 0.5 * dm / (dm * dm + BROADENING);
+        Fpv[(size_t)i * K + j] = 0.5 * dp / (dp * dp + BROADENING);
       }
   }
-  Tensor Fm = leg_matrix(E, f.leg, f.leg, F), Dm = leg_matrix(E, f.leg, f.leg, D);
+  Tensor Fm = leg_matrix(E, f.leg, f.leg, Fmv), Fp = leg_matrix(E, f.leg, f.leg, Fpv);
+  Tensor Dm = leg_matrix(E, f.leg, f.leg, D);
   Tensor X = ein(E, ru + "K," + ru + "L->KL", f.U, Ub);                 // U^T Ub
-  Tensor J = hadamard(E, Fm, axpby(E, 1.0, X, -1.0, perm_view(X, {1, 0})));
+  Tensor A = axpby(E, 1.0, X, -1.0, perm_view(X, {1, 0}));
   Tensor Y = ein(E, "K" + cv + ",L" + cv + "->KL", f.Vt, Vtb);           // V^T Vb
-  Tensor Kk = hadamard(E, Fm, axpby(E, 1.0, Y, -1.0, perm_view(Y, {1, 0})));
-  Tensor core = axpby(E, 1.0, scale_leg(E, J, 1, f.s), 1.0, scale_leg(E, Kk, 0, f.s));
+  Tensor B = axpby(E, 1.0, Y, -1.0, perm_view(Y, {1, 0}));
+  Tensor core = axpby(E, 1.0, hadamard(E, Fm, axpby(E, 1.0, A, 1.0, B)), 1.0,
+                      hadamard(E, Fp, axpby(E, 1.0, A, -1.0, B)));
   core = axpby(E, 1.0, core, 1.0, Dm);
   const std::string out = ru + cv;
   Tensor Ab = ein(E, ru + "L,L" + cv + "->" + out, ein(E, ru + "K,KL->" + ru + "L", f.U, core), f.Vt);

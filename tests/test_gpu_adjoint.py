@@ -3,15 +3,12 @@
 (``oracle/adjoint.py``, pinned on the CPU by finite differences, homogeneity
 and the direct <X_i> ratios).
 
-The device canonicalizes by full SVDs where the oracle takes LQs (a gauge
-choice the truncated state does not see, but the Lorentzian broadening of the
-SVD reverse rule does, slightly): the oracle with the device's gauge
-(``canonical="svd"``) agrees with its LQ gauge to 2e-16 on the 2x3 D=2
-fixture and 2.3e-9 of each site gradient's largest entry on the 3x3 D=4 one,
-at chi0 and exact alike.
-The bar here is 1e-7 of the largest entry (the oracle itself matches central
-finite differences to 1e-7); homogeneity (<d lnZ/dA_i, A_i> = 2) holds on the
-device to 1e-9.
+Both canonicalize by full SVDs (the oracle's default gauge) and split the SVD
+couplings into broadened 1/(s_j - s_i) and 1/(s_j + s_i) terms; what differs
+is the SVD itself (LAPACK against the device's Jacobi), which near-degenerate
+singular values turn into differences far below the bar, 1e-7 of each site
+gradient's largest entry (the oracle matches central differences to 1e-7 or
+better).  Homogeneity (<d lnZ/dA_i, A_i> = 2) holds on the device to 1e-9.
 """
 import numpy as np
 import pytest
