@@ -162,3 +162,28 @@ def test_gradient_on_rank_deficient_boundaries(sps, chi, space):
     for x in range(4):
         for y in range(4):
             assert abs(float(np.sum(g[x][y] * st[x, y].a)) - 2.0) < 1e-12
+
+
+def test_gradient_at_the_differentiation_shape(sps):
+    """The 6x6 D=4 chi=24 (12+12) shape of the differentiation workload, on a
+    seeded synthetic PEPO at beta 1: the derivative along a random direction
+    matches central differences (step 1e-5) to 1.5e-7 relative (bar 1e-6)."""
+    from oracle.model import State
+    from oracle.z2 import leg
+    L = 6
+    sites, dims = sps.synthetic.synthetic_pepo(L, L, 4, 0.3, 7)
+    dims = np.asarray(dims).reshape(L * L, 6, 2)
+    S = [[None] * L for _ in range(L)]
+    for i in range(L * L):
+        S[i % L][i // L] = T(np.asarray(sites[i]).reshape([int(a + b) for a, b in dims[i]]),
+                             [leg(int(a), int(b)) for a, b in dims[i]])
+    st = State(L, L, S, 1.0, 0.0, "pepo")
+    value, g = ad.lognorm_with_gradient(st, 24, (12, 12))
+    rng = np.random.default_rng(11)
+    dirs = [[rng.standard_normal(st[x, y].shape) * (st[x, y].a != 0) for y in range(L)] for x in range(L)]
+    eps = 1e-5
+    up = bm.lognorm(_shifted(st, dirs, eps), bm.BoundaryMPS(24, (12, 12)))["log_norm"]
+    down = bm.lognorm(_shifted(st, dirs, -eps), bm.BoundaryMPS(24, (12, 12)))["log_norm"]
+    fd = (up - down) / (2 * eps)
+    adj = sum(float(np.sum(g[x][y] * dirs[x][y])) for x in range(L) for y in range(L))
+    assert abs(fd - adj) <= 1e-6 * abs(fd)
