@@ -112,3 +112,29 @@ def test_autograd_function_on_the_device(sps):
     grads = torch.autograd.grad(-2.0 * out, ts)
     for a, b in zip(grads, ref):
         assert np.abs(a.numpy() + 2.0 * b).max() <= 1e-12 * np.abs(b).max()
+
+
+def test_lognorm_gradient_at_the_differentiation_shape(sps):
+    """6x6 D=4 chi=24 (12+12), a seeded synthetic PEPO at beta 1 whose
+    boundary blocks are numerically rank deficient: the device derivative
+    against the oracle's (which matches central differences to 1.5e-7 there),
+    1e-6 of each site gradient's largest entry, homogeneity to 1e-9."""
+    from oracle import adjoint as ad
+    from oracle.model import State
+    from oracle.z2 import T, leg
+    L = 6
+    sites, dims = sps.synthetic.synthetic_pepo(L, L, 4, 0.3, 7)
+    e = sps.Engine(L, L, sps.TFIM(1.0, 3.0))
+    st = e.upload_state(sites, dims, True, beta=1.0)
+    value, grads = sps.lognorm_gradient(st, sps.BoundaryMPS(24, sps.Z2Space(12, 12)), checkpoint_rows=True)
+    d = np.asarray(dims).reshape(L * L, 6, 2)
+    S = [[None] * L for _ in range(L)]
+    for i in range(L * L):
+        S[i % L][i // L] = T(np.asarray(sites[i]).reshape([int(a + b) for a, b in d[i]]),
+                             [leg(int(a), int(b)) for a, b in d[i]])
+    ov, og = ad.lognorm_with_gradient(State(L, L, S, 1.0, 0.0, "pepo"), 24, (12, 12))
+    assert abs(value - ov) <= 1e-10 * abs(ov)
+    for i in range(L * L):
+        ref = og[i % L][i // L]
+        assert np.abs(grads[i] - ref).max() <= 1e-6 * np.abs(ref).max()
+        assert abs(float(np.sum(grads[i] * np.asarray(sites[i]).reshape(ref.shape))) - 2.0) < 1e-9
